@@ -1,0 +1,232 @@
+/*
+ * lrt_raster.h -- C-ABI of the B200 splat tile rasteriser.
+ *
+ * Drop-in for lucabRTrender's splat raster path: packed Gaussian clouds in
+ * (the scene::GpuSplats layout), premultiplied linear colour and view-z depth
+ * out (bottom row first), and the per-stage timings `lrt bench --stages`
+ * prints. Every signature is plain C: device pointers and sizes, no C++ or
+ * torch types, so a C++, Python (ctypes) or any other FFI host can bind it.
+ *
+ * Reference interfaces replaced (paths inside the lucabRTrender tree):
+ *   lrt_rast_create        modules/render/src/TileRasterizer.cpp:59-103
+ *                          (TileRasterizer::create)
+ *   lrt_rast_render        modules/render/src/TileRasterizer.cpp:188-484
+ *                          (TileRasterizer::render(const Projection&, ...))
+ *   lrt_projection_for     modules/render/src/Camera.cpp:23-48 (projectionFor)
+ *   lrt_camera_looking_at  modules/render/src/Camera.cpp:9-13 (Camera::lookingAt)
+ *   lrt_prefix_sum         modules/gpu/src/algo/PrefixSum.cpp:58-88 (PrefixSum::apply)
+ *   lrt_radix_sort         modules/gpu/src/algo/RadixSort.cpp:80-157 (RadixSort::sort)
+ *   lrt_pack_splats        modules/scene/src/GpuClouds.cpp:151-226 and
+ *                          shaders/lrt/scene/splat_decode.slang:20-91 (CloudLoader::upload,
+ *                          host-side; the packed bytes are what the raster reads)
+ *
+ * Conventions (the reference's, shaders/lrt/splat/frame.slang:22-27):
+ * +z forward, x right, y up; screen origin bottom-left; pixel centres at +0.5;
+ * 16x16 tiles. Errors are returned as an lrt_status (the reference's
+ * lrt::ErrorCode, modules/core/include/lrt/core/Error.h:14-26, plus OVERFLOW and
+ * TIMEOUT for device-side capacity and bounded-wait failures); nothing throws,
+ * and lrt_rast_last_error() gives the message. One calling thread per handle;
+ * every call is ordered on the caller's CUDA stream.
+ */
+#ifndef LRT_RASTER_H
+#define LRT_RASTER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LRT_ABI_VERSION 1u
+#define LRT_TILE 16u
+
+typedef enum lrt_status {
+    LRT_OK = 0,
+    LRT_UNKNOWN = 1,
+    LRT_NOT_FOUND = 2,
+    LRT_INVALID_ARGUMENT = 3,
+    LRT_UNSUPPORTED = 4,
+    LRT_IO_FAILURE = 5,
+    LRT_DEVICE_FAILURE = 6,
+    LRT_OUT_OF_MEMORY = 8,
+    LRT_INTERNAL_ERROR = 10,
+    /* Not in the reference's ErrorCode: a device-side capacity check failed
+     * (more pairs were emitted than the pair buffer holds). */
+    LRT_OVERFLOW = 11,
+    /* A bounded device-side wait (decoupled look-back, bulk-copy barrier)
+     * gave up; the kernel returned instead of spinning. */
+    LRT_TIMEOUT = 12
+} lrt_status;
+
+/* Projection (modules/render/include/lrt/render/Camera.h:56-82), the part
+ * the rasteriser reads. Row-major 4x4 acting on column vectors. */
+typedef struct lrt_projection {
+    double world_to_view[16];
+    double focal_x, focal_y;     /* pixels per unit of x/z (perspective) or per unit (ortho) */
+    double centre_x, centre_y;
+    double near_z, far_z;
+    double eye_world[3];
+    uint32_t orthographic;
+    uint32_t reserved;
+} lrt_projection;
+
+/* Lens + Camera (Camera.h:23-53). */
+typedef struct lrt_lens {
+    uint32_t orthographic;
+    uint32_t reserved;
+    double focal;              /* mm */
+    double haperture;          /* mm */
+    double vaperture;          /* mm */
+    double near_z, far_z;
+    double window_translate[2];
+    double window_scale[2];
+    double window_roll;        /* degrees, counter-clockwise */
+} lrt_lens;
+
+typedef struct lrt_camera {
+    double camera_to_world[16];
+    lrt_lens lens;
+} lrt_camera;
+
+/* SplatEdit (modules/render/include/lrt/render/TileRasterizer.h:29-50). */
+typedef struct lrt_splat_edit {
+    uint32_t active;
+    uint32_t shape;   /* 0 box, 1 sphere */
+    uint32_t mode;    /* 0 keep inside, 1 remove inside, 2 grade inside */
+    uint32_t invert;
+    float centre[3];
+    float size[3];
+    float tint[3];
+    float saturation, brightness, opacity, min_opacity, max_scale;
+} lrt_splat_edit;
+
+/* scene::GpuSplats (modules/scene/include/lrt/scene/GpuClouds.h:41-76):
+ *   positions  float4 per splat: xyz, linear opacity
+ *   shape      uint32 x4 per splat: [0] smallest-three quaternion,
+ *              [1] f16 log sx | f16 log sy << 16, [2] f16 log sz | f16 base r << 16,
+ *              [3] f16 base g | f16 base b << 16
+ *   sh         sh_words uint32 per splat: f16 rest coefficients, rgb per basis
+ * All three are device pointers owned by the caller. */
+typedef struct lrt_gpu_splats {
+    uint32_t count;
+    uint32_t rest_per_colour;   /* 0, 3, 8, 15 -> degree 0..3 */
+    uint32_t sh_words;          /* (rest_per_colour * 3 + 1) / 2 */
+    uint32_t reserved;
+    const void* positions;
+    const void* shape;
+    const void* sh;
+} lrt_gpu_splats;
+
+/* SplatInstance (TileRasterizer.h:52-67) without the relight fields. */
+typedef struct lrt_splat_instance {
+    const lrt_gpu_splats* splats;
+    double object_to_world[16];
+    lrt_splat_edit edit;
+} lrt_splat_instance;
+
+/* RenderSettings (TileRasterizer.h:105-118). */
+typedef struct lrt_render_settings {
+    uint32_t width, height;
+    uint32_t antialias;
+    uint32_t max_sh_degree;
+    float background[4];        /* premultiplied, linear */
+    uint32_t depth_mode;        /* 0 alpha-weighted mean, 1 first crossing of depth_threshold */
+    float depth_threshold;
+    uint32_t linearise;
+    uint32_t time_stages;       /* record per-stage CUDA events into the stats */
+} lrt_render_settings;
+
+/* FrameStats (TileRasterizer.h:120-126). Stage times are CUDA-event times on
+ * the render stream when time_stages is set; total_ms is host wall time. The
+ * depth order is folded into the pair sort's key, so that sort is reported
+ * under tile_sort_ms (with ranges) and depth_sort_ms is 0. */
+typedef struct lrt_frame_stats {
+    uint32_t splats, visible, pairs, reserved;
+    double project_ms, depth_sort_ms, counts_ms, emit_ms, tile_sort_ms, blend_ms, total_ms;
+} lrt_frame_stats;
+
+/* RenderTargets (TileRasterizer.h:128-134): caller-owned device images,
+ * width * height, bottom row first. colour is float4 premultiplied linear,
+ * depth is float view z. */
+typedef struct lrt_targets {
+    uint32_t width, height;
+    void* colour;
+    void* depth;
+} lrt_targets;
+
+/* Device views of one frame's intermediate buffers, for parity checks. Valid
+ * until the next call on the handle. */
+typedef struct lrt_debug_view {
+    const void* proj;            /* 48-byte ProjRecord per slot (frame.slang:85-89) */
+    const void* rects;           /* uint32 x4 per slot: tile rect lo.x lo.y hi.x hi.y */
+    const void* touched;         /* uint32 per slot */
+    const void* depth_keys;      /* uint32 per slot: float bits of view z >> 7; 0x00FFFFFF culled */
+    const void* pairs;           /* uint64 per pair, sorted: tile | depth key | slot (see pair_*) */
+    const void* ranges;          /* uint32 x2 per tile: [start, end) into pairs */
+    uint32_t slots, pairs_count, tiles, slot_bits;
+    uint32_t depth_bits, tile_bits, visible, reserved;
+} lrt_debug_view;
+
+typedef struct lrt_rast lrt_rast;
+
+uint32_t lrt_abi_version(void);
+
+/* TileRasterizer::create. `device` is the CUDA ordinal the handle renders on. */
+int lrt_rast_create(lrt_rast** out, int device);
+void lrt_rast_destroy(lrt_rast* rast);
+/* The message of the last failed call on this handle ("" when none). */
+const char* lrt_rast_last_error(const lrt_rast* rast);
+
+/* TileRasterizer::render(const Projection&, instances, settings, targets).
+ * `stream` is a cudaStream_t (NULL: the legacy default stream). Instances are
+ * concatenated into slots base + i in the order given; the slot breaks depth
+ * ties. The call returns once the frame is enqueued and its counts are known
+ * (it reads back the pair count, as the reference does). */
+int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
+                    const lrt_splat_instance* instances, uint32_t instance_count,
+                    const lrt_render_settings* settings, lrt_targets* targets,
+                    lrt_frame_stats* stats, void* stream);
+
+int lrt_rast_debug_view(const lrt_rast* rast, lrt_debug_view* out);
+
+/* Camera::lookingAt and projectionFor, in double precision on the host. */
+int lrt_camera_looking_at(const double eye[3], const double target[3], const double up[3],
+                          lrt_camera* out);
+int lrt_projection_for(const lrt_camera* camera, uint32_t width, uint32_t height,
+                       lrt_projection* out);
+
+/* PrefixSum::apply: exclusive scan of `count` uint32 at `in` into `out`, the
+ * sum into `total` (all device pointers; `out` may alias `in`). Single pass,
+ * decoupled look-back; scratch is the handle's. */
+int lrt_prefix_sum(lrt_rast* rast, const void* in, void* out, void* total, uint32_t count,
+                   void* stream);
+
+/* RadixSort::sort: stable LSD sort of `count` keys (key_bytes 4 or 8) and
+ * optional uint32 values by their low `key_bits` bits, in place. Onesweep:
+ * one histogram pass, then one decoupled look-back pass per 8-bit digit. */
+int lrt_radix_sort(lrt_rast* rast, void* keys, void* values, uint32_t count, uint32_t key_bits,
+                   uint32_t key_bytes, void* stream);
+
+/* Raw 3DGS records (the PLY encoding: x y z, logit opacity, 3 log scales,
+ * rot w x y z, 3 DC, rest coefficients all red then green then blue) to the
+ * packed layout above, on the host. Invalid records (non-finite position or
+ * scale, |log scale| >= 60, opacity < 1/255) are dropped, order kept. Writes
+ * positions (float4), shape (uint32 x4) and sh (sh_words uint32; one word
+ * minimum per splat) for up to `count` splats; returns the kept count in
+ * *kept. `keep_per_colour` <= `file_per_colour` (0, 3, 8, 15). */
+int lrt_pack_splats(const float* raw, uint32_t count, uint32_t floats_per_record,
+                    uint32_t file_per_colour, uint32_t keep_per_colour, float* positions,
+                    uint32_t* shape, uint32_t* sh, uint32_t* kept);
+
+/* Diagnostic: the library's own exp (fn 0), log (1), sRGB-to-linear (2) and
+ * cut-off power (3), evaluated on the device over n floats (device pointers),
+ * for comparing their bits with a host implementation. No reference
+ * counterpart: the reference evaluates these through Slang's library. */
+int lrt_math_eval(int fn, const void* x, void* y, uint32_t n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LRT_RASTER_H */

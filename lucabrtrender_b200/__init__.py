@@ -1,0 +1,16 @@
+"""B200-native splat tile rasteriser with lucabRTrender's TileRasterizer interface.
+
+The compute path is the in-tree CUDA library ``lib/liblrt_raster.so`` (sm_100a
+kernels behind the C-ABI of ``include/lrt_raster.h``); this package is the
+Python host mirror of the reference's C++ interface over that ABI.
+"""
+from .camera import Camera, Lens, Projection, projection_for, square_pixel_camera
+from .raster import (Depth, EditMode, EditShape, FrameStats, RenderSettings, RenderTargets, SplatEdit,
+                     SplatInstance, TileRasterizer, math_eval)
+from .scene import CloudLoader, GpuSplats, PackedSplats, pack_splats, synthetic_records, to_device
+
+__all__ = [
+    "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
+    "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
+    "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device",
+]

@@ -1,0 +1,170 @@
+"""ctypes mirror of ``include/lrt_raster.h`` and the loader of the in-tree library.
+
+The library is loaded from ``lucabrtrender_b200/lib/liblrt_raster.so``; there
+is no fallback of any kind: if it is missing or does not load, every entry
+point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "lib" / "liblrt_raster.so"
+ABI_VERSION = 1
+TILE = 16
+
+# lrt_status
+OK = 0
+UNKNOWN = 1
+NOT_FOUND = 2
+INVALID_ARGUMENT = 3
+UNSUPPORTED = 4
+IO_FAILURE = 5
+DEVICE_FAILURE = 6
+OUT_OF_MEMORY = 8
+INTERNAL_ERROR = 10
+OVERFLOW = 11
+TIMEOUT = 12
+
+STATUS_NAMES = {
+    OK: "Ok", UNKNOWN: "Unknown", NOT_FOUND: "NotFound", INVALID_ARGUMENT: "InvalidArgument",
+    UNSUPPORTED: "Unsupported", IO_FAILURE: "IoFailure", DEVICE_FAILURE: "DeviceFailure",
+    OUT_OF_MEMORY: "OutOfMemory", INTERNAL_ERROR: "InternalError", OVERFLOW: "Overflow", TIMEOUT: "Timeout",
+}
+
+# Every symbol include/lrt_raster.h declares.
+EXPORTS = (
+    "lrt_abi_version", "lrt_rast_create", "lrt_rast_destroy", "lrt_rast_last_error", "lrt_rast_render",
+    "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
+    "lrt_pack_splats", "lrt_math_eval",
+)
+
+
+class Projection(C.Structure):
+    _fields_ = [
+        ("world_to_view", C.c_double * 16),
+        ("focal_x", C.c_double), ("focal_y", C.c_double),
+        ("centre_x", C.c_double), ("centre_y", C.c_double),
+        ("near_z", C.c_double), ("far_z", C.c_double),
+        ("eye_world", C.c_double * 3),
+        ("orthographic", C.c_uint32), ("reserved", C.c_uint32),
+    ]
+
+
+class Lens(C.Structure):
+    _fields_ = [
+        ("orthographic", C.c_uint32), ("reserved", C.c_uint32),
+        ("focal", C.c_double), ("haperture", C.c_double), ("vaperture", C.c_double),
+        ("near_z", C.c_double), ("far_z", C.c_double),
+        ("window_translate", C.c_double * 2), ("window_scale", C.c_double * 2),
+        ("window_roll", C.c_double),
+    ]
+
+
+class CameraStruct(C.Structure):
+    _fields_ = [("camera_to_world", C.c_double * 16), ("lens", Lens)]
+
+
+class SplatEdit(C.Structure):
+    _fields_ = [
+        ("active", C.c_uint32), ("shape", C.c_uint32), ("mode", C.c_uint32), ("invert", C.c_uint32),
+        ("centre", C.c_float * 3), ("size", C.c_float * 3), ("tint", C.c_float * 3),
+        ("saturation", C.c_float), ("brightness", C.c_float), ("opacity", C.c_float),
+        ("min_opacity", C.c_float), ("max_scale", C.c_float),
+    ]
+
+
+class GpuSplatsStruct(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint32), ("rest_per_colour", C.c_uint32), ("sh_words", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("positions", C.c_void_p), ("shape", C.c_void_p), ("sh", C.c_void_p),
+    ]
+
+
+class SplatInstanceStruct(C.Structure):
+    _fields_ = [
+        ("splats", C.POINTER(GpuSplatsStruct)),
+        ("object_to_world", C.c_double * 16),
+        ("edit", SplatEdit),
+    ]
+
+
+class RenderSettingsStruct(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32), ("antialias", C.c_uint32),
+        ("max_sh_degree", C.c_uint32), ("background", C.c_float * 4), ("depth_mode", C.c_uint32),
+        ("depth_threshold", C.c_float), ("linearise", C.c_uint32), ("time_stages", C.c_uint32),
+    ]
+
+
+class FrameStatsStruct(C.Structure):
+    _fields_ = [
+        ("splats", C.c_uint32), ("visible", C.c_uint32), ("pairs", C.c_uint32), ("reserved", C.c_uint32),
+        ("project_ms", C.c_double), ("depth_sort_ms", C.c_double), ("counts_ms", C.c_double),
+        ("emit_ms", C.c_double), ("tile_sort_ms", C.c_double), ("blend_ms", C.c_double),
+        ("total_ms", C.c_double),
+    ]
+
+
+class TargetsStruct(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("colour", C.c_void_p), ("depth", C.c_void_p)]
+
+
+class DebugView(C.Structure):
+    _fields_ = [
+        ("proj", C.c_void_p), ("rects", C.c_void_p), ("touched", C.c_void_p), ("depth_keys", C.c_void_p),
+        ("pairs", C.c_void_p), ("ranges", C.c_void_p),
+        ("slots", C.c_uint32), ("pairs_count", C.c_uint32), ("tiles", C.c_uint32), ("slot_bits", C.c_uint32),
+        ("depth_bits", C.c_uint32), ("tile_bits", C.c_uint32), ("visible", C.c_uint32), ("reserved", C.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """The loaded library; raises if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBRARY_PATH.exists():
+        raise RuntimeError(
+            f"the CUDA library {LIBRARY_PATH} is not built: run `python -m lucabrtrender_b200.build` "
+            "(or __graft_entry__.build())")
+    lib = C.CDLL(str(LIBRARY_PATH))
+    lib.lrt_abi_version.restype = C.c_uint32
+    lib.lrt_rast_create.argtypes = [C.POINTER(C.c_void_p), C.c_int]
+    lib.lrt_rast_destroy.argtypes = [C.c_void_p]
+    lib.lrt_rast_destroy.restype = None
+    lib.lrt_rast_last_error.argtypes = [C.c_void_p]
+    lib.lrt_rast_last_error.restype = C.c_char_p
+    lib.lrt_rast_render.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(SplatInstanceStruct), C.c_uint32,
+                                    C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
+                                    C.POINTER(FrameStatsStruct), C.c_void_p]
+    lib.lrt_rast_debug_view.argtypes = [C.c_void_p, C.POINTER(DebugView)]
+    lib.lrt_camera_looking_at.argtypes = [C.POINTER(C.c_double)] * 3 + [C.POINTER(CameraStruct)]
+    lib.lrt_projection_for.argtypes = [C.POINTER(CameraStruct), C.c_uint32, C.c_uint32, C.POINTER(Projection)]
+    lib.lrt_prefix_sum.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    lib.lrt_radix_sort.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                   C.c_void_p]
+    lib.lrt_pack_splats.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.lrt_math_eval.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    if lib.lrt_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"ABI version mismatch: library {lib.lrt_abi_version()}, bindings {ABI_VERSION}")
+    _lib = lib
+    return lib
+
+
+class LrtError(RuntimeError):
+    """A failed call: ``code`` is the lrt_status (the reference's ErrorCode)."""
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+
+
+def check(code: int, message: str = "") -> None:
+    if code != OK:
+        raise LrtError(code, message)

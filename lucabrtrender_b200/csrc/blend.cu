@@ -1,0 +1,243 @@
+// Stages (b) duplication, (d) tile ranges and (e) the front-to-back blend.
+//
+// Pair word (64 bits, sorted on its key bits only):
+//     tile << (24 + slotBits) | depthKey24 << slotBits | slot
+// A stable sort of the key bits [slotBits, slotBits + 24 + tileBits) over
+// pairs emitted in slot order leaves every tile's pairs in (depth key, slot)
+// order -- the order the reference gets from its depth sort followed by a
+// stable tile sort (shaders/lrt/splat/frame.slang:17-20,
+// modules/render/src/TileRasterizer.cpp:401-457).
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+namespace lrt {
+namespace {
+
+constexpr uint32_t kDupThreads = 256;
+constexpr uint32_t kBlendThreads = 256;
+constexpr uint32_t kBatch = 256;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// shaders/lrt/splat/splat_emit.slang:17-50, emitting in slot order.
+__global__ void __launch_bounds__(kDupThreads)
+duplicate_kernel(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* __restrict__ proj,
+                 const uint4* __restrict__ rects, const uint32_t* __restrict__ touched,
+                 const uint32_t* __restrict__ keys, const uint32_t* __restrict__ offsets, uint32_t slots,
+                 uint32_t slotBits, unsigned long long* __restrict__ pairs, uint32_t capacity,
+                 uint32_t* __restrict__ err) {
+    const uint32_t slot = blockIdx.x * kDupThreads + threadIdx.x;
+    if (slot >= slots) return;
+    const uint32_t expected = touched[slot];
+    if (expected == 0) return;
+    const uint32_t first = offsets[slot];
+    const float4 screen = proj[slot].screen;
+    const float4 conic = proj[slot].conic;
+    const uint4 rect = rects[slot];
+    const unsigned long long low = (static_cast<unsigned long long>(keys[slot]) << slotBits) | slot;
+    const uint32_t tileShift = 24 + slotBits;
+    uint32_t written = 0;
+    for (uint32_t ty = rect.y; ty <= rect.w && written < expected; ++ty) {
+        for (uint32_t tx = rect.x; tx <= rect.z && written < expected; ++tx) {
+            if (!tile_touched(width, height, screen.x, screen.y, conic.x, conic.y, conic.z, screen.w, tx, ty)) continue;
+            const uint32_t at = first + written;
+            if (at < capacity) {
+                pairs[at] = (static_cast<unsigned long long>(ty * tilesX + tx) << tileShift) | low;
+            } else {
+                atomicOr(err, kErrOverflow);
+            }
+            written += 1;
+        }
+    }
+}
+
+// shaders/lrt/splat/splat_ranges.slang:11-25 (after a zeroing memset,
+// splat_tiles_clear.slang:8-17).
+__global__ void ranges_kernel(const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ dCount,
+                              uint32_t cap, uint32_t tileShift, uint2* __restrict__ ranges) {
+    const uint32_t n = min(*dCount, cap);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = static_cast<uint32_t>(pairs[i] >> tileShift);
+    if (i == 0 || static_cast<uint32_t>(pairs[i - 1] >> tileShift) != t) ranges[t].x = i;
+    if (i + 1 == n || static_cast<uint32_t>(pairs[i + 1] >> tileShift) != t) ranges[t].y = i + 1;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// One record (48 bytes, 16-byte aligned at both ends) by the bulk-copy engine.
+__device__ __forceinline__ void bulk_copy_record(void* dst, const void* src, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 48, [%2];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait on a barrier phase; false when the limit passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// shaders/lrt/splat/splat_blend.slang:23-108 (splat-only entry, :110-114).
+// One block per 16x16 tile, one thread per pixel. The tile's pairs are read
+// in batches of 256: each thread copies one record into shared memory with a
+// bulk copy, completing on the batch's mbarrier; batch k+1 is in flight while
+// batch k is blended. A pixel stops at T < 1e-4 exactly as the reference's
+// loop does; the block stops when every pixel has (a block-wide vote).
+__global__ void __launch_bounds__(kBlendThreads)
+blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+             const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
+             uint32_t* __restrict__ err) {
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
+    __shared__ __align__(8) uint64_t sBar[2];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % bp.tilesX, ty = tile / bp.tilesX;
+    const uint32_t px = tx * kTile + (tid & 15u);
+    const uint32_t py = ty * kTile + (tid >> 4);
+    const bool inside = px < bp.width && py < bp.height;
+    const uint2 range = ranges[tile];
+    const uint32_t start = range.x, end = range.y;
+    const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
+    if (tid == 0) {
+        mbar_init(&sBar[0], 1);
+        mbar_init(&sBar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](uint32_t buf, uint32_t at) {
+        const uint32_t cnt = min(kBatch, end - at);
+        if (tid == 0) mbar_arrive_expect_tx(&sBar[buf], cnt * static_cast<uint32_t>(sizeof(ProjRecord)));
+        if (tid < cnt) {
+            const uint32_t slot = static_cast<uint32_t>(pairs[at + tid] & slotMask);
+            fence_proxy_async_smem();
+            bulk_copy_record(&sRec[buf][tid], proj + slot, &sBar[buf]);
+        }
+    };
+
+    const float pxf = static_cast<float>(px) + 0.5f;
+    const float pyf = static_cast<float>(py) + 0.5f;
+    float r = 0.0f, g = 0.0f, b = 0.0f;
+    float T = 1.0f;
+    float depthSum = 0.0f;
+    float depthAt = -1.0f;
+    bool done = !inside;
+    uint32_t phase0 = 0, phase1 = 0;
+    if (start < end) issue(0, start);
+    uint32_t k = 0;
+    for (uint32_t at = start; at < end; at += kBatch, ++k) {
+        const uint32_t buf = k & 1u;
+        const bool more = at + kBatch < end;
+        if (more) issue(buf ^ 1u, at + kBatch);
+        const uint32_t parity = buf == 0 ? phase0 : phase1;
+        if (!mbar_wait(&sBar[buf], parity)) {
+            atomicOr(err, kErrTimeout);
+            done = true;
+        }
+        if (buf == 0) phase0 ^= 1u; else phase1 ^= 1u;
+        const uint32_t cnt = min(kBatch, end - at);
+        if (!done) {
+            const ProjRecord* batch = sRec[buf];
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const float4 screen = batch[j].screen;
+                const float4 conic = batch[j].conic;
+                const float dx = pxf - screen.x;
+                const float dy = pyf - screen.y;
+                const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
+                if (power > screen.w) continue;
+                const float alpha = fminf(0.99f, conic.w * lrt_exp(-0.5f * power));
+                if (alpha < 1.0f / 255.0f) continue;
+                const float4 colour = batch[j].colour;
+                const float weight = T * alpha;
+                r = r + weight * colour.x;
+                g = g + weight * colour.y;
+                b = b + weight * colour.z;
+                depthSum = depthSum + weight * screen.z;
+                T = T * (1.0f - alpha);
+                if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
+                if (T < 1e-4f) {
+                    done = true;
+                    break;
+                }
+            }
+        }
+        if (__syncthreads_and(done ? 1 : 0)) {
+            if (more) {
+                const uint32_t nb = buf ^ 1u;
+                if (!mbar_wait(&sBar[nb], nb == 0 ? phase0 : phase1)) atomicOr(err, kErrTimeout);
+            }
+            break;
+        }
+    }
+    if (!inside) return;
+    const float coverage = 1.0f - T;
+    float lr = r, lg = g, lb = b;
+    if (bp.linearise != 0 && coverage > 1e-6f) {
+        lr = srgb_to_linear(r / coverage) * coverage;
+        lg = srgb_to_linear(g / coverage) * coverage;
+        lb = srgb_to_linear(b / coverage) * coverage;
+    }
+    const size_t pix = static_cast<size_t>(py) * bp.width + px;
+    colourOut[pix] = make_float4(lr + T * bp.bg[0], lg + T * bp.bg[1], lb + T * bp.bg[2], coverage + T * bp.bg[3]);
+    depthOut[pix] = bp.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f) : fmaxf(depthAt, 0.0f);
+}
+
+}  // namespace
+
+cudaError_t launch_duplicate(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* proj,
+                             const uint4* rects, const uint32_t* touched, const uint32_t* keys,
+                             const uint32_t* offsets, uint32_t slots, uint32_t slotBits, uint64_t* pairs,
+                             uint32_t capacity, uint32_t* err, cudaStream_t stream) {
+    if (slots == 0) return cudaSuccess;
+    duplicate_kernel<<<(slots + kDupThreads - 1) / kDupThreads, kDupThreads, 0, stream>>>(
+        width, height, tilesX, proj, rects, touched, keys, offsets, slots, slotBits,
+        reinterpret_cast<unsigned long long*>(pairs), capacity, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
+                          uint2* ranges, uint32_t tiles, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(ranges, 0, sizeof(uint2) * tiles, stream);
+    if (e != cudaSuccess || cap == 0) return e;
+    ranges_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs), dCount,
+                                                          cap, tileShift, ranges);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream) {
+    const uint32_t tiles = bp.tilesX * bp.tilesY;
+    if (tiles == 0) return cudaSuccess;
+    blend_kernel<<<tiles, kBlendThreads, 0, stream>>>(bp, ranges, reinterpret_cast<const unsigned long long*>(pairs),
+                                                      proj, colour, depth, err);
+    return cudaGetLastError();
+}
+
+}  // namespace lrt

@@ -1,0 +1,44 @@
+// Host-side launchers of the rasteriser's kernels (one .cu file per stage).
+#pragma once
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lrt {
+
+struct FrameParams;
+struct BlendParams;
+struct ProjRecord;
+
+cudaError_t launch_project(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
+                           ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys,
+                           uint32_t* visibleCount, cudaStream_t stream);
+
+size_t scan_scratch_bytes(uint32_t n);
+cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
+                                  uint32_t* err, cudaStream_t stream);
+
+cudaError_t launch_duplicate(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* proj,
+                             const uint4* rects, const uint32_t* touched, const uint32_t* keys,
+                             const uint32_t* offsets, uint32_t slots, uint32_t slotBits, uint64_t* pairs,
+                             uint32_t capacity, uint32_t* err, cudaStream_t stream);
+
+size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);
+cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
+                            const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream);
+cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
+                            const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream);
+
+cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
+                          uint2* ranges, uint32_t tiles, cudaStream_t stream);
+
+cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream);
+
+cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
+
+}  // namespace lrt

@@ -1,0 +1,353 @@
+// Stage (a): per-splat projection.
+//
+// Restates shaders/lrt/splat/splat_project.slang:39-221 (the splat route;
+// relighting is not part of this path): SplatEdit fate, near/far cull, 3D
+// covariance from the smallest-three quaternion and f16 log-scales, EWA
+// Jacobian clamped to 1.3x the frustum, Mip-Splatting 2D filter with the
+// opacity payback, conic and cut-off, tile rectangle, exact touched-tile
+// count, view-dependent colour from f16 spherical harmonics up to degree 3,
+// and the 24-bit depth key.
+//
+// B200 layout: one thread per splat, 256 per block. Positions and shape are
+// read as 16-byte vectors (coalesced). The block's harmonics rows (92 bytes a
+// splat at degree 3: not 16-byte aligned per splat, but 256 rows start on a
+// 16-byte boundary) are staged into shared memory by 16-byte cp.async copies
+// issued first, so they land while the geometry is computed.
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+namespace lrt {
+namespace {
+
+constexpr uint32_t kProjectThreads = 256;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
+}
+
+struct Fate {
+    bool removed, graded;
+    float opacity;
+};
+
+// shaders/lrt/common/edit.slang:46-75
+__device__ __forceinline__ Fate edit_fate(const EditParams& e, float3 p, float opacity, float3 s) {
+    Fate f{false, false, opacity};
+    if (e.active == 0) return f;
+    if (e.minOpacity > 0.0f && opacity < e.minOpacity) {
+        f.removed = true;
+        return f;
+    }
+    if (e.maxScale > 0.0f && fmaxf(fmaxf(fabsf(s.x), fabsf(s.y)), fabsf(s.z)) > e.maxScale) {
+        f.removed = true;
+        return f;
+    }
+    const float rx = p.x - e.centre[0], ry = p.y - e.centre[1], rz = p.z - e.centre[2];
+    bool inside = e.shape == 1 ? rx * rx + ry * ry + rz * rz <= e.size[0] * e.size[0]
+                               : (fabsf(rx) <= e.size[0] && fabsf(ry) <= e.size[1] && fabsf(rz) <= e.size[2]);
+    if (e.invert != 0) inside = !inside;
+    if ((e.mode == 0 && !inside) || (e.mode == 1 && inside)) {
+        f.removed = true;
+        return f;
+    }
+    if (inside) {
+        f.graded = true;
+        f.opacity = opacity * e.opacity;
+        f.removed = !(f.opacity >= 1.0f / 255.0f);
+    }
+    return f;
+}
+
+// edit.slang:78-85 (lerp(a, b, t) = a + (b - a) t)
+__device__ __forceinline__ float3 edit_grade(const EditParams& e, float3 c0) {
+    const float cx = c0.x * e.tint[0] * e.brightness;
+    const float cy = c0.y * e.tint[1] * e.brightness;
+    const float cz = c0.z * e.tint[2] * e.brightness;
+    const float luma = cx * 0.2126f + cy * 0.7152f + cz * 0.0722f;
+    return make_float3(fmaxf(luma + (cx - luma) * e.saturation, 0.0f),
+                       fmaxf(luma + (cy - luma) * e.saturation, 0.0f),
+                       fmaxf(luma + (cz - luma) * e.saturation, 0.0f));
+}
+
+// shaders/lrt/common/sh.slang:8-51, over one staged row of f16 pairs.
+__device__ __forceinline__ float half_at(const uint32_t* row, uint32_t index) {
+    const uint32_t w = row[index >> 1];
+    return (index & 1u) == 0u ? low_half(w) : high_half(w);
+}
+
+struct Basis {
+    float x, y, z;
+};
+__device__ __forceinline__ Basis basis(const uint32_t* row, uint32_t k) {
+    return {half_at(row, k * 3), half_at(row, k * 3 + 1), half_at(row, k * 3 + 2)};
+}
+
+__device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t degree, float3 dir) {
+    constexpr float kC1 = 0.4886025119029199f;
+    constexpr float kC2_0 = 1.0925484305920792f, kC2_1 = -1.0925484305920792f, kC2_2 = 0.31539156525252005f,
+                    kC2_3 = -1.0925484305920792f, kC2_4 = 0.5462742152960396f;
+    constexpr float kC3_0 = -0.5900435899266435f, kC3_1 = 2.890611442640554f, kC3_2 = -0.4570457994644658f,
+                    kC3_3 = 0.3731763325901154f, kC3_4 = -0.4570457994644658f, kC3_5 = 1.445305721320277f,
+                    kC3_6 = -0.5900435899266435f;
+    if (degree == 0) return make_float3(0.0f, 0.0f, 0.0f);
+    const float x = dir.x, y = dir.y, z = dir.z;
+    const float s0 = -kC1 * y, s1 = kC1 * z, s2 = kC1 * x;
+    const Basis b0 = basis(row, 0), b1 = basis(row, 1), b2 = basis(row, 2);
+    float3 r = make_float3(s0 * b0.x + s1 * b1.x - s2 * b2.x, s0 * b0.y + s1 * b1.y - s2 * b2.y,
+                           s0 * b0.z + s1 * b1.z - s2 * b2.z);
+    if (degree < 2) return r;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    const float xy = x * y, yz = y * z, xz = x * z;
+    {
+        const float t0 = kC2_0 * xy, t1 = kC2_1 * yz, t2 = kC2_2 * (2.0f * zz - xx - yy), t3 = kC2_3 * xz,
+                    t4 = kC2_4 * (xx - yy);
+        const Basis b3 = basis(row, 3), b4 = basis(row, 4), b5 = basis(row, 5), b6 = basis(row, 6),
+                    b7 = basis(row, 7);
+        r.x = r.x + (t0 * b3.x + t1 * b4.x + t2 * b5.x + t3 * b6.x + t4 * b7.x);
+        r.y = r.y + (t0 * b3.y + t1 * b4.y + t2 * b5.y + t3 * b6.y + t4 * b7.y);
+        r.z = r.z + (t0 * b3.z + t1 * b4.z + t2 * b5.z + t3 * b6.z + t4 * b7.z);
+    }
+    if (degree < 3) return r;
+    {
+        const float t0 = kC3_0 * y * (3.0f * xx - yy), t1 = kC3_1 * xy * z,
+                    t2 = kC3_2 * y * (4.0f * zz - xx - yy),
+                    t3 = kC3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy),
+                    t4 = kC3_4 * x * (4.0f * zz - xx - yy), t5 = kC3_5 * z * (xx - yy),
+                    t6 = kC3_6 * x * (xx - 3.0f * yy);
+        const Basis b8 = basis(row, 8), b9 = basis(row, 9), b10 = basis(row, 10), b11 = basis(row, 11),
+                    b12 = basis(row, 12), b13 = basis(row, 13), b14 = basis(row, 14);
+        r.x = r.x + (t0 * b8.x + t1 * b9.x + t2 * b10.x + t3 * b11.x + t4 * b12.x + t5 * b13.x + t6 * b14.x);
+        r.y = r.y + (t0 * b8.y + t1 * b9.y + t2 * b10.y + t3 * b11.y + t4 * b12.y + t5 * b13.y + t6 * b14.y);
+        r.z = r.z + (t0 * b8.z + t1 * b9.z + t2 * b10.z + t3 * b11.z + t4 * b12.z + t5 * b13.z + t6 * b14.z);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(kProjectThreads)
+project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4* __restrict__ shape,
+               const uint32_t* __restrict__ sh, uint32_t stageWords, uint32_t shVector,
+               ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
+               uint32_t* __restrict__ keysOut, uint32_t* __restrict__ visibleCount) {
+    extern __shared__ __align__(16) uint32_t shStage[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t blockStart = blockIdx.x * kProjectThreads;
+    const uint32_t i = blockStart + tid;
+    const bool inRange = i < f.count;
+
+    // Harmonics of the whole block, in flight while the geometry runs.
+    if (stageWords != 0) {
+        const uint32_t nBlock = min(kProjectThreads, f.count - blockStart);
+        const uint32_t words = nBlock * f.shWords;
+        const uint32_t* src = sh + static_cast<size_t>(blockStart) * f.shWords;
+        uint32_t w0 = 0;
+        if (shVector) {
+            const uint32_t nvec = words >> 2;
+            for (uint32_t v = tid; v < nvec; v += kProjectThreads) cp_async16(&shStage[v * 4], src + v * 4);
+            w0 = nvec * 4;
+        }
+        for (uint32_t w = w0 + tid; w < words; w += kProjectThreads) cp_async4(&shStage[w], src + w);
+    }
+
+    bool alive = false;
+    float3 p = make_float3(0.0f, 0.0f, 0.0f);
+    float3 t = p;
+    float cx = 0.0f, cy = 0.0f, ca = 0.0f, cb = 0.0f, cc = 0.0f, alpha = 0.0f, cutoff = 0.0f;
+    uint4 rect = make_uint4(1, 1, 0, 0);
+    uint32_t touched = 0;
+    Fate fate{true, false, 0.0f};
+    uint4 sw = make_uint4(0, 0, 0, 0);
+    if (inRange) {
+        const float4 po = __ldg(positions + i);
+        sw = __ldg(shape + i);
+        p = make_float3(po.x, po.y, po.z);
+        const float3 scale = make_float3(lrt_exp(low_half(sw.y)), lrt_exp(high_half(sw.y)), lrt_exp(low_half(sw.z)));
+        fate = edit_fate(f.edit, p, po.w, scale);
+        t = to_view(f, p);
+        alive = !fate.removed && (t.z > f.nearZ) && !(t.z > f.farZ);
+        if (alive) {
+            // decodeQuaternion, packing.slang:52-69
+            const uint32_t word = sw.x;
+            const uint32_t largest = word & 3u;
+            float sx = static_cast<float>((word >> 22) & 1023u);
+            float sy = static_cast<float>((word >> 12) & 1023u);
+            float sz = static_cast<float>((word >> 2) & 1023u);
+            sx = (sx / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+            sy = (sy / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+            sz = (sz / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+            const float rest = sqrtf(fmaxf(0.0f, 1.0f - (sx * sx + sy * sy + sz * sz)));
+            float q[4];
+            {
+                const float small[3] = {sx, sy, sz};
+                uint32_t next = 0;
+#pragma unroll
+                for (uint32_t k = 0; k < 4; ++k) {
+                    if (k == largest) {
+                        q[k] = rest;
+                    } else {
+                        q[k] = small[next == 0 ? 0 : next == 1 ? 1 : 2];
+                        next += 1;
+                    }
+                }
+            }
+            const float x = q[0], y = q[1], z = q[2], w = q[3];
+            const float r00 = 1.0f - 2.0f * (y * y + z * z), r01 = 2.0f * (x * y - w * z), r02 = 2.0f * (x * z + w * y);
+            const float r10 = 2.0f * (x * y + w * z), r11 = 1.0f - 2.0f * (x * x + z * z), r12 = 2.0f * (y * z - w * x);
+            const float r20 = 2.0f * (x * z - w * y), r21 = 2.0f * (y * z + w * x), r22 = 1.0f - 2.0f * (x * x + y * y);
+            const float m00 = r00 * scale.x, m01 = r01 * scale.y, m02 = r02 * scale.z;
+            const float m10 = r10 * scale.x, m11 = r11 * scale.y, m12 = r12 * scale.z;
+            const float m20 = r20 * scale.x, m21 = r21 * scale.y, m22 = r22 * scale.z;
+
+            float jx0, jx1, jx2, jy0, jy1, jy2;
+            if (f.ortho) {
+                jx0 = f.focalX; jx1 = 0.0f; jx2 = 0.0f;
+                jy0 = 0.0f; jy1 = f.focalY; jy2 = 0.0f;
+                cx = f.focalX * t.x + f.centreX;
+                cy = f.focalY * t.y + f.centreY;
+            } else {
+                const float invZ = 1.0f / t.z;
+                cx = f.focalX * t.x * invZ + f.centreX;
+                cy = f.focalY * t.y * invZ + f.centreY;
+                const float limLoX = (-0.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+                const float limHiX = (1.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+                const float limLoY = (-0.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+                const float limHiY = (1.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+                const float tx = clampf(t.x * invZ, limLoX, limHiX) * t.z;
+                const float ty = clampf(t.y * invZ, limLoY, limHiY) * t.z;
+                jx0 = f.focalX * invZ; jx1 = 0.0f; jx2 = -f.focalX * tx * invZ * invZ;
+                jy0 = 0.0f; jy1 = f.focalY * invZ; jy2 = -f.focalY * ty * invZ * invZ;
+            }
+            // mul(row, W), then mul(row, M): result[j] = row0 X[0][j] + row1 X[1][j] + row2 X[2][j]
+            const float tx0 = jx0 * f.m[0] + jx1 * f.m[4] + jx2 * f.m[8];
+            const float tx1 = jx0 * f.m[1] + jx1 * f.m[5] + jx2 * f.m[9];
+            const float tx2 = jx0 * f.m[2] + jx1 * f.m[6] + jx2 * f.m[10];
+            const float ty0 = jy0 * f.m[0] + jy1 * f.m[4] + jy2 * f.m[8];
+            const float ty1 = jy0 * f.m[1] + jy1 * f.m[5] + jy2 * f.m[9];
+            const float ty2 = jy0 * f.m[2] + jy1 * f.m[6] + jy2 * f.m[10];
+            const float ax0 = tx0 * m00 + tx1 * m10 + tx2 * m20;
+            const float ax1 = tx0 * m01 + tx1 * m11 + tx2 * m21;
+            const float ax2 = tx0 * m02 + tx1 * m12 + tx2 * m22;
+            const float ay0 = ty0 * m00 + ty1 * m10 + ty2 * m20;
+            const float ay1 = ty0 * m01 + ty1 * m11 + ty2 * m21;
+            const float ay2 = ty0 * m02 + ty1 * m12 + ty2 * m22;
+            float a = ax0 * ax0 + ax1 * ax1 + ax2 * ax2;
+            const float b = ax0 * ay0 + ax1 * ay1 + ax2 * ay2;
+            float c = ay0 * ay0 + ay1 * ay1 + ay2 * ay2;
+            const float detBefore = a * c - b * b;
+            a = a + 0.3f;
+            c = c + 0.3f;
+            const float det = a * c - b * b;
+            alive = det > 1e-12f;
+            if (alive) {
+                alpha = fate.opacity;
+                if (f.antialias != 0) alpha = alpha * sqrtf(fmaxf(detBefore, 0.0f) / det);
+                alive = alpha >= 1.0f / 255.0f;
+            }
+            if (alive) {
+                ca = c / det;
+                cb = -b / det;
+                cc = a / det;
+                cutoff = cutoff_power(alpha);
+                // footprintExtent, frame.slang:142-146
+                const float det2 = ca * cc - cb * cb;
+                const float inv = det2 > 1e-20f ? 1.0f / det2 : 0.0f;
+                const float ex = sqrtf(fmaxf(cutoff * cc * inv, 0.0f));
+                const float ey = sqrtf(fmaxf(cutoff * ca * inv, 0.0f));
+                // tileRect, frame.slang:149-161
+                const float x1 = cx - ex, y1 = cy - ey, x2 = cx + ex, y2 = cy + ey;
+                if (x2 < 0.0f || y2 < 0.0f || x1 >= static_cast<float>(f.width) ||
+                    y1 >= static_cast<float>(f.height)) {
+                    alive = false;
+                } else {
+                    rect = make_uint4(static_cast<uint32_t>(fmaxf(x1, 0.0f)) / kTile,
+                                      static_cast<uint32_t>(fmaxf(y1, 0.0f)) / kTile,
+                                      static_cast<uint32_t>(fminf(x2, static_cast<float>(f.width) - 1.0f)) / kTile,
+                                      static_cast<uint32_t>(fminf(y2, static_cast<float>(f.height) - 1.0f)) / kTile);
+                    alive = !(rect.x > rect.z || rect.y > rect.w);
+                }
+            }
+            if (alive) {
+                for (uint32_t ty = rect.y; ty <= rect.w; ++ty)
+                    for (uint32_t tx = rect.x; tx <= rect.z; ++tx)
+                        touched += tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, tx, ty) ? 1u : 0u;
+                alive = touched != 0;
+            }
+        }
+    }
+
+    if (stageWords != 0) cp_async_wait_all();
+    __syncthreads();
+
+    const uint32_t slot = f.base + i;
+    if (inRange) {
+        if (alive) {
+            const float3 base = make_float3(high_half(sw.z), low_half(sw.w), high_half(sw.w));
+            const uint32_t rpc = f.restPerColour;
+            const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
+            const uint32_t degree = min(stored, f.shLimit);
+            float3 colour = base;
+            float3 restc = make_float3(0.0f, 0.0f, 0.0f);
+            if (degree > 0) {
+                const float dx = p.x - f.eye[0], dy = p.y - f.eye[1], dz = p.z - f.eye[2];
+                const float l = sqrtf(dx * dx + dy * dy + dz * dz);
+                const float3 dir = make_float3(dx / l, dy / l, dz / l);
+                restc = evaluate_rest(shStage + tid * f.shWords, degree, dir);
+            }
+            colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
+                                 fmaxf(base.z + restc.z, 0.0f));
+            if (fate.graded) colour = edit_grade(f.edit, colour);
+            ProjRecord rec;
+            rec.screen = make_float4(cx, cy, t.z, cutoff);
+            rec.conic = make_float4(ca, cb, cc, alpha);
+            rec.colour = make_float4(colour.x, colour.y, colour.z, 0.0f);
+            proj[slot] = rec;
+            rects[slot] = rect;
+            touchedOut[slot] = touched;
+            keysOut[slot] = float_bits(t.z) >> 7;
+        } else {
+            // splat_project.slang:39-49, plus a zeroed record
+            ProjRecord rec;
+            rec.screen = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            rec.conic = rec.screen;
+            rec.colour = rec.screen;
+            proj[slot] = rec;
+            rects[slot] = make_uint4(1, 1, 0, 0);
+            touchedOut[slot] = 0;
+            keysOut[slot] = 0x00FFFFFFu;
+        }
+    }
+    const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, inRange && alive);
+    if ((tid & 31u) == 0 && ballot != 0) atomicAdd(visibleCount, static_cast<uint32_t>(__popc(ballot)));
+}
+
+}  // namespace
+
+cudaError_t launch_project(const FrameParams& f, const float4* positions, const uint4* shape,
+                           const uint32_t* sh, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                           uint32_t* keys, uint32_t* visibleCount, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    const uint32_t rpc = f.restPerColour;
+    const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
+    const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
+    const uint32_t stageWords = stage ? f.shWords : 0u;
+    const uint32_t shVector = (reinterpret_cast<uintptr_t>(sh) & 15u) == 0 ? 1u : 0u;
+    const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t blocks = (f.count + kProjectThreads - 1) / kProjectThreads;
+    project_kernel<<<blocks, kProjectThreads, smem, stream>>>(f, positions, shape, sh, stageWords, shVector, proj,
+                                                             rects, touched, keys, visibleCount);
+    return cudaGetLastError();
+}
+
+}  // namespace lrt

@@ -1,0 +1,483 @@
+// The C-ABI rasteriser: lrt_rast_create / lrt_rast_render / ... (see
+// include/lrt_raster.h). Host orchestration of one frame, in the reference's
+// order (modules/render/src/TileRasterizer.cpp:188-484):
+//
+//   project (per instance)  -> scan of touched counts (duplication offsets)
+//   -> one readback of the visible and pair counts -> duplicate pairs
+//   -> onesweep sort of the pairs' (tile | depth) key bits -> tile ranges
+//   -> blend
+//
+// Buffers belong to the handle and grow by 1.5x (TileRasterizer.cpp:26-32);
+// targets and clouds belong to the caller. Stage times come from CUDA events
+// on the caller's stream.
+#include "../../include/lrt_raster.h"
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct lrt_rast {
+    int device = 0;
+    std::string error;
+    DeviceBuffer proj, rects, touched, keys, offsets;   // per slot
+    DeviceBuffer pairs, pairsAlt;                        // per pair
+    DeviceBuffer ranges;                                 // per tile
+    DeviceBuffer scanScratch, sortScratch;
+    DeviceBuffer counters;                               // visible, pairs, err, algo err
+    DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers
+    uint32_t* hostCounters = nullptr;                    // pinned
+    cudaEvent_t ev[8] = {};
+    uint32_t splatCap = 0, pairCap = 0, tileCap = 0;
+    lrt_debug_view debug{};
+};
+
+namespace {
+
+using lrt::BlendParams;
+using lrt::FrameParams;
+using lrt::ProjRecord;
+
+int fail(lrt_rast* r, int code, const std::string& message) {
+    if (r != nullptr) r->error = message;
+    return code;
+}
+
+int cuda_fail(lrt_rast* r, cudaError_t e, const char* what) {
+    const int code = e == cudaErrorMemoryAllocation ? LRT_OUT_OF_MEMORY : LRT_DEVICE_FAILURE;
+    return fail(r, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define LRT_CUDA(r, call, what)                         \
+    do {                                                \
+        const cudaError_t e_ = (call);                  \
+        if (e_ != cudaSuccess) return cuda_fail(r, e_, what); \
+    } while (0)
+
+// TileRasterizer.cpp:26-32
+uint32_t grow(uint32_t have, uint32_t need) {
+    uint64_t size = std::max<uint32_t>(have, 1024);
+    while (size < need) size = size * 3 / 2;
+    return static_cast<uint32_t>(std::min<uint64_t>(size, 0xFFFFFFFFull));
+}
+
+cudaError_t ensure(DeviceBuffer& b, size_t bytes) {
+    if (b.bytes >= bytes && b.ptr != nullptr) return cudaSuccess;
+    if (b.ptr != nullptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.ptr, std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess) b.bytes = std::max<size_t>(bytes, 16);
+    return e;
+}
+
+void release(DeviceBuffer& b) {
+    if (b.ptr != nullptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+// FrameParams.h:18-24
+uint32_t bits_for(uint64_t values) {
+    uint32_t bits = 1;
+    while (bits < 32 && (uint64_t{1} << bits) < values) ++bits;
+    return bits;
+}
+
+struct M4 {
+    double m[16];
+    double at(int r, int c) const { return m[r * 4 + c]; }
+};
+
+M4 mul4(const double* a, const double* b) {
+    M4 o{};
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double s = 0.0;
+            for (int k = 0; k < 4; ++k) s += a[r * 4 + k] * b[k * 4 + c];
+            o.m[r * 4 + c] = s;
+        }
+    return o;
+}
+
+// The eye in the instance's own space: inverse(objectToWorld) applied to the
+// world eye (TileRasterizer.cpp:298-299, aofx::xform::inverseAffine).
+void eye_in_object(const double* m, const double* eye, double out[3]) {
+    auto at = [&](int r, int c) { return m[r * 4 + c]; };
+    const double a00 = at(0, 0), a01 = at(0, 1), a02 = at(0, 2);
+    const double a10 = at(1, 0), a11 = at(1, 1), a12 = at(1, 2);
+    const double a20 = at(2, 0), a21 = at(2, 1), a22 = at(2, 2);
+    const double c00 = a11 * a22 - a12 * a21;
+    const double c01 = a12 * a20 - a10 * a22;
+    const double c02 = a10 * a21 - a11 * a20;
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    const double inv = std::fabs(det) > 1e-18 ? 1.0 / det : 0.0;
+    const double i00 = c00 * inv, i01 = (a02 * a21 - a01 * a22) * inv, i02 = (a01 * a12 - a02 * a11) * inv;
+    const double i10 = c01 * inv, i11 = (a00 * a22 - a02 * a20) * inv, i12 = (a02 * a10 - a00 * a12) * inv;
+    const double i20 = c02 * inv, i21 = (a01 * a20 - a00 * a21) * inv, i22 = (a00 * a11 - a01 * a10) * inv;
+    const double tx = at(0, 3), ty = at(1, 3), tz = at(2, 3);
+    const double b0 = -(i00 * tx + i01 * ty + i02 * tz);
+    const double b1 = -(i10 * tx + i11 * ty + i12 * tz);
+    const double b2 = -(i20 * tx + i21 * ty + i22 * tz);
+    out[0] = i00 * eye[0] + i01 * eye[1] + i02 * eye[2] + b0;
+    out[1] = i10 * eye[0] + i11 * eye[1] + i12 * eye[2] + b1;
+    out[2] = i20 * eye[0] + i21 * eye[1] + i22 * eye[2] + b2;
+}
+
+float event_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.0f;
+    return ms;
+}
+
+struct DeviceScope {
+    int previous = -1;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&previous) == cudaSuccess && previous != device) {
+            cudaSetDevice(device);
+        } else {
+            previous = -1;
+        }
+    }
+    ~DeviceScope() {
+        if (previous >= 0) cudaSetDevice(previous);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+uint32_t lrt_abi_version(void) { return LRT_ABI_VERSION; }
+
+int lrt_rast_create(lrt_rast** out, int device) {
+    if (out == nullptr) return LRT_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return LRT_DEVICE_FAILURE;
+    if (device < 0 || device >= count) return LRT_INVALID_ARGUMENT;
+    DeviceScope scope(device);
+    lrt_rast* r = new lrt_rast();
+    r->device = device;
+    bool ok = cudaMallocHost(reinterpret_cast<void**>(&r->hostCounters), 64) == cudaSuccess &&
+              ensure(r->counters, 64) == cudaSuccess;
+    for (auto& e : r->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    if (!ok) {
+        lrt_rast_destroy(r);
+        cudaGetLastError();
+        return LRT_DEVICE_FAILURE;
+    }
+    *out = r;
+    return LRT_OK;
+}
+
+void lrt_rast_destroy(lrt_rast* r) {
+    if (r == nullptr) return;
+    DeviceScope scope(r->device);
+    for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->offsets, &r->pairs, &r->pairsAlt,
+                            &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
+                            &r->algoValsAlt})
+        release(*b);
+    if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
+    for (auto& e : r->ev)
+        if (e != nullptr) cudaEventDestroy(e);
+    delete r;
+}
+
+const char* lrt_rast_last_error(const lrt_rast* r) { return r == nullptr ? "no handle" : r->error.c_str(); }
+
+int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                    const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    // TileRasterizer.cpp:194-217
+    if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
+    if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
+        targets->depth == nullptr)
+        return fail(r, LRT_INVALID_ARGUMENT, "the targets are not the frame's size");
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const lrt_gpu_splats* c = instances[k].splats;
+        if (c == nullptr || c->count == 0) continue;
+        if (c->positions == nullptr || c->shape == nullptr)
+            return fail(r, LRT_INVALID_ARGUMENT, "a cloud without positions or shape");
+        if (c->rest_per_colour > 0 && c->sh == nullptr) return fail(r, LRT_INVALID_ARGUMENT, "a cloud without harmonics");
+        if (c->rest_per_colour > 0 && c->sh_words < (c->rest_per_colour * 3 + 1) / 2)
+            return fail(r, LRT_INVALID_ARGUMENT, "sh_words too small for rest_per_colour");
+        total += c->count;
+    }
+    if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one frame");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    const uint32_t slots = static_cast<uint32_t>(total);
+    const uint32_t tilesX = (s->width + lrt::kTile - 1) / lrt::kTile;
+    const uint32_t tilesY = (s->height + lrt::kTile - 1) / lrt::kTile;
+    const uint32_t tiles = tilesX * tilesY;
+    const uint32_t slotBits = bits_for(std::max<uint64_t>(slots, 1));
+    const uint32_t tileBits = bits_for(tiles);
+    const uint32_t keyBits = 24 + tileBits;
+    if (slotBits + keyBits > 64)
+        return fail(r, LRT_UNSUPPORTED, "splat slots and tile count do not fit one 64-bit pair word");
+
+    // Buffers (TileRasterizer.cpp:105-177).
+    if (slots > r->splatCap) {
+        const uint32_t cap = grow(r->splatCap, slots);
+        LRT_CUDA(r, ensure(r->proj, size_t{cap} * sizeof(ProjRecord)), "splat records");
+        LRT_CUDA(r, ensure(r->rects, size_t{cap} * 16), "tile rects");
+        LRT_CUDA(r, ensure(r->touched, size_t{cap} * 4), "touched counts");
+        LRT_CUDA(r, ensure(r->keys, size_t{cap} * 4), "depth keys");
+        LRT_CUDA(r, ensure(r->offsets, size_t{cap} * 4), "pair offsets");
+        LRT_CUDA(r, ensure(r->scanScratch, lrt::scan_scratch_bytes(cap)), "scan scratch");
+        r->splatCap = cap;
+    }
+    if (tiles > r->tileCap) {
+        LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
+        r->tileCap = tiles;
+    }
+    uint32_t* counters = static_cast<uint32_t*>(r->counters.ptr);
+    uint32_t* err = counters + 2;
+    LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
+
+    // --- project -----------------------------------------------------------
+    LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
+    uint32_t base = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const lrt_splat_instance& inst = instances[k];
+        const lrt_gpu_splats* c = inst.splats;
+        if (c == nullptr || c->count == 0) continue;
+        FrameParams f{};
+        f.width = s->width;
+        f.height = s->height;
+        f.tilesX = tilesX;
+        f.tilesY = tilesY;
+        f.focalX = static_cast<float>(pr->focal_x);
+        f.focalY = static_cast<float>(pr->focal_y);
+        f.centreX = static_cast<float>(pr->centre_x);
+        f.centreY = static_cast<float>(pr->centre_y);
+        f.nearZ = static_cast<float>(pr->near_z);
+        f.farZ = static_cast<float>(pr->far_z);
+        f.ortho = pr->orthographic ? 1u : 0u;
+        f.antialias = s->antialias ? 1u : 0u;
+        const M4 ov = mul4(pr->world_to_view, inst.object_to_world);
+        for (int row = 0; row < 3; ++row)
+            for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
+        double eye[3];
+        eye_in_object(inst.object_to_world, pr->eye_world, eye);
+        for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
+        f.count = c->count;
+        f.base = base;
+        f.restPerColour = c->rest_per_colour;
+        f.shWords = c->sh_words;
+        f.shLimit = s->max_sh_degree;
+        const lrt_splat_edit& e = inst.edit;
+        f.edit.active = e.active;
+        f.edit.shape = e.shape;
+        f.edit.mode = e.mode;
+        f.edit.invert = e.invert;
+        for (int a = 0; a < 3; ++a) {
+            f.edit.centre[a] = e.centre[a];
+            f.edit.size[a] = e.size[a];
+            f.edit.tint[a] = e.tint[a];
+        }
+        f.edit.saturation = e.saturation;
+        f.edit.brightness = e.brightness;
+        f.edit.opacity = e.opacity;
+        f.edit.minOpacity = e.min_opacity;
+        f.edit.maxScale = e.max_scale;
+        LRT_CUDA(r,
+                 lrt::launch_project(f, static_cast<const float4*>(c->positions), static_cast<const uint4*>(c->shape),
+                                     static_cast<const uint32_t*>(c->sh), static_cast<ProjRecord*>(r->proj.ptr),
+                                     static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                                     static_cast<uint32_t*>(r->keys.ptr), counters, stream),
+                 "project");
+        base += c->count;
+    }
+    LRT_CUDA(r, cudaEventRecord(r->ev[1], stream), "event");
+
+    // --- counts: duplication offsets and the pair total ---------------------
+    LRT_CUDA(r,
+             lrt::launch_exclusive_scan(static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->offsets.ptr),
+                                        counters + 1, slots, r->scanScratch.ptr, err, stream),
+             "scan");
+    LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "count readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "count readback");
+    const uint32_t visible = r->hostCounters[0];
+    const uint32_t pairs = r->hostCounters[1];
+    if (r->hostCounters[2] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "prefix sum look-back gave up");
+    if (r->hostCounters[2] & lrt::kErrTooManyPairs) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pairs in one frame");
+
+    if (pairs > r->pairCap) {
+        const uint32_t cap = grow(r->pairCap, pairs);
+        LRT_CUDA(r, ensure(r->pairs, size_t{cap} * 8), "pairs");
+        LRT_CUDA(r, ensure(r->pairsAlt, size_t{cap} * 8), "pairs");
+        r->pairCap = cap;
+    }
+    LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(std::max(pairs, 1u), keyBits)), "sort scratch");
+
+    // --- emit ---------------------------------------------------------------
+    LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
+    uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
+    LRT_CUDA(r,
+             lrt::launch_duplicate(s->width, s->height, tilesX, static_cast<ProjRecord*>(r->proj.ptr),
+                                   static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                                   static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->offsets.ptr), slots,
+                                   slotBits, pairBuf, r->pairCap, err, stream),
+             "duplicate");
+    LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
+
+    // --- sort + ranges ------------------------------------------------------
+    bool inAlt = false;
+    LRT_CUDA(r,
+             lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), nullptr, nullptr, counters + 1,
+                                  pairs, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt, stream),
+             "pair sort");
+    const uint64_t* sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
+    LRT_CUDA(r,
+             lrt::launch_ranges(sorted, counters + 1, pairs, 24 + slotBits, static_cast<uint2*>(r->ranges.ptr), tiles,
+                                stream),
+             "ranges");
+    LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
+
+    // --- blend --------------------------------------------------------------
+    BlendParams bp{};
+    bp.width = s->width;
+    bp.height = s->height;
+    bp.tilesX = tilesX;
+    bp.tilesY = tilesY;
+    bp.slotBits = slotBits;
+    bp.tileShift = 24 + slotBits;
+    bp.depthMode = s->depth_mode;
+    bp.linearise = s->linearise ? 1u : 0u;
+    bp.depthThreshold = s->depth_threshold;
+    for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
+    LRT_CUDA(r,
+             lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted, static_cast<ProjRecord*>(r->proj.ptr),
+                               static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth), err,
+                               stream),
+             "blend");
+    LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 4, err, 4, cudaMemcpyDeviceToHost, stream), "status readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "frame");
+
+    r->debug.proj = r->proj.ptr;
+    r->debug.rects = r->rects.ptr;
+    r->debug.touched = r->touched.ptr;
+    r->debug.depth_keys = r->keys.ptr;
+    r->debug.pairs = sorted;
+    r->debug.ranges = r->ranges.ptr;
+    r->debug.slots = slots;
+    r->debug.pairs_count = pairs;
+    r->debug.tiles = tiles;
+    r->debug.slot_bits = slotBits;
+    r->debug.depth_bits = 24;
+    r->debug.tile_bits = tileBits;
+    r->debug.visible = visible;
+
+    const uint32_t status = r->hostCounters[4];
+    if (stats != nullptr) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->splats = slots;
+        stats->visible = visible;
+        stats->pairs = pairs;
+        if (s->time_stages) {
+            stats->project_ms = event_ms(r->ev[0], r->ev[1]);
+            stats->counts_ms = event_ms(r->ev[1], r->ev[2]);
+            stats->emit_ms = event_ms(r->ev[3], r->ev[4]);
+            stats->tile_sort_ms = event_ms(r->ev[4], r->ev[5]);
+            stats->blend_ms = event_ms(r->ev[5], r->ev[6]);
+        }
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - frameStart).count();
+    }
+    if (status & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+    if (status & lrt::kErrOverflow) return fail(r, LRT_OVERFLOW, "pair capacity exceeded");
+    return LRT_OK;
+}
+
+int lrt_rast_debug_view(const lrt_rast* r, lrt_debug_view* out) {
+    if (r == nullptr || out == nullptr) return LRT_INVALID_ARGUMENT;
+    *out = r->debug;
+    return LRT_OK;
+}
+
+int lrt_prefix_sum(lrt_rast* r, const void* in, void* out, void* total, uint32_t count, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if ((count > 0 && (in == nullptr || out == nullptr)) || total == nullptr)
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    uint32_t* err = static_cast<uint32_t*>(r->counters.ptr) + 3;
+    LRT_CUDA(r, ensure(r->scanScratch, lrt::scan_scratch_bytes(count)), "scan scratch");
+    LRT_CUDA(r, cudaMemsetAsync(err, 0, 4, stream), "status");
+    LRT_CUDA(r,
+             lrt::launch_exclusive_scan(static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out),
+                                        static_cast<uint32_t*>(total), count, r->scanScratch.ptr, err, stream),
+             "prefix sum");
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 5, err, 4, cudaMemcpyDeviceToHost, stream), "status readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "prefix sum");
+    if (r->hostCounters[5] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "prefix sum look-back gave up");
+    if (r->hostCounters[5] & lrt::kErrTooManyPairs) return fail(r, LRT_OVERFLOW, "the sum passed 2^32 - 1");
+    return LRT_OK;
+}
+
+int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32_t keyBits, uint32_t keyBytes,
+                   void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (keyBytes != 4 && keyBytes != 8) return fail(r, LRT_INVALID_ARGUMENT, "key_bytes must be 4 or 8");
+    if (keyBits == 0 || keyBits > keyBytes * 8) return fail(r, LRT_INVALID_ARGUMENT, "key_bits out of range");
+    if (count > 0 && keys == nullptr) return fail(r, LRT_INVALID_ARGUMENT, "null keys");
+    if (count <= 1) return LRT_OK;
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    uint32_t* counters = static_cast<uint32_t*>(r->counters.ptr);
+    uint32_t* err = counters + 3;
+    LRT_CUDA(r, ensure(r->algoKeysAlt, size_t{count} * keyBytes), "sort buffers");
+    if (values != nullptr) LRT_CUDA(r, ensure(r->algoValsAlt, size_t{count} * 4), "sort buffers");
+    LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(count, keyBits)), "sort scratch");
+    // The count lives on the device so the kernels can be replayed; write it.
+    r->hostCounters[6] = count;
+    LRT_CUDA(r, cudaMemcpyAsync(counters + 4, r->hostCounters + 6, 4, cudaMemcpyHostToDevice, stream), "count");
+    LRT_CUDA(r, cudaMemsetAsync(err, 0, 4, stream), "status");
+    bool inAlt = false;
+    uint32_t* vals = static_cast<uint32_t*>(values);
+    uint32_t* valsAlt = values != nullptr ? static_cast<uint32_t*>(r->algoValsAlt.ptr) : nullptr;
+    if (keyBytes == 8) {
+        LRT_CUDA(r,
+                 lrt::launch_sort_u64(static_cast<uint64_t*>(keys), static_cast<uint64_t*>(r->algoKeysAlt.ptr), vals,
+                                      valsAlt, counters + 4, count, 0, keyBits, r->sortScratch.ptr, err, &inAlt,
+                                      stream),
+                 "radix sort");
+    } else {
+        LRT_CUDA(r,
+                 lrt::launch_sort_u32(static_cast<uint32_t*>(keys), static_cast<uint32_t*>(r->algoKeysAlt.ptr), vals,
+                                      valsAlt, counters + 4, count, 0, keyBits, r->sortScratch.ptr, err, &inAlt,
+                                      stream),
+                 "radix sort");
+    }
+    if (inAlt) {   // an odd pass count ends in the scratch buffers (RadixSort.cpp:146-155 copies back too)
+        LRT_CUDA(r, cudaMemcpyAsync(keys, r->algoKeysAlt.ptr, size_t{count} * keyBytes, cudaMemcpyDeviceToDevice, stream),
+                 "copy back");
+        if (values != nullptr)
+            LRT_CUDA(r, cudaMemcpyAsync(values, r->algoValsAlt.ptr, size_t{count} * 4, cudaMemcpyDeviceToDevice, stream),
+                     "copy back");
+    }
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 7, err, 4, cudaMemcpyDeviceToHost, stream), "status readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "radix sort");
+    if (r->hostCounters[7] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "radix sort look-back gave up");
+    return LRT_OK;
+}
+
+}  // extern "C"

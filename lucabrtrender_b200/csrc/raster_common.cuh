@@ -1,0 +1,104 @@
+// Device-side frame maths shared by the projection, duplication and blend
+// kernels. Each function restates the reference's Slang definition cited
+// beside it (paths inside the lucabRTrender tree), expression for expression:
+// the library is compiled with -fmad=false, so every product and sum rounds
+// once, in the order written, exactly as the CPU oracle's does.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lrt_math.cuh"
+
+namespace lrt {
+
+constexpr uint32_t kTile = 16;   // shaders/lrt/splat/frame.slang:31
+
+struct EditParams {   // shaders/lrt/common/edit.slang:23-37
+    uint32_t active, shape, mode, invert;
+    float centre[3], size[3], tint[3];
+    float saturation, brightness, opacity, minOpacity, maxScale;
+};
+
+// The projection's per-instance uniforms (frame.slang:33-81 without the
+// relight fields).
+struct FrameParams {
+    uint32_t width, height, tilesX, tilesY;
+    float focalX, focalY, centreX, centreY, nearZ, farZ;
+    uint32_t ortho, antialias;
+    float m[12];      // object -> view, rows of a 3x4
+    float eye[3];     // the camera in the cloud's space
+    uint32_t count, base, restPerColour, shWords, shLimit;
+    EditParams edit;
+};
+
+struct BlendParams {
+    uint32_t width, height, tilesX, tilesY;
+    uint32_t slotBits, tileShift;
+    uint32_t depthMode, linearise;
+    float depthThreshold;
+    float bg[4];
+};
+
+// frame.slang:85-89: what the projection leaves for the blend.
+struct __align__(16) ProjRecord {
+    float4 screen;   // centre.xy, view z, cutoff power
+    float4 conic;    // a, b, c, alpha
+    float4 colour;   // rgb (encoded), 0
+};
+
+// Status bits a kernel may raise in the frame's error word.
+constexpr uint32_t kErrOverflow = 1u;
+constexpr uint32_t kErrTimeout = 2u;
+constexpr uint32_t kErrTooManyPairs = 4u;
+
+__device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+
+__device__ __forceinline__ float3 to_view(const FrameParams& f, float3 p) {   // frame.slang:91-95
+    return make_float3(f.m[0] * p.x + f.m[1] * p.y + f.m[2] * p.z + f.m[3],
+                       f.m[4] * p.x + f.m[5] * p.y + f.m[6] * p.z + f.m[7],
+                       f.m[8] * p.x + f.m[9] * p.y + f.m[10] * p.z + f.m[11]);
+}
+
+__device__ __forceinline__ float cutoff_power(float alpha) {   // frame.slang:105-107
+    return fminf(2.0f * lrt_log(fmaxf(255.0f * alpha, 1.0001f)), 9.0f);
+}
+
+// frame.slang:113-130: exact minimum of the quadratic form over a box.
+__device__ __forceinline__ float min_power_over_box(float a, float b, float c, float lox, float loy,
+                                                    float hix, float hiy) {
+    if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f;
+    float best = 3.4e38f;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float x = e == 0 ? lox : hix;
+        const float y = c > 1e-12f ? clampf(-b * x / c, loy, hiy) : loy;
+        best = fminf(best, a * x * x + 2.0f * b * x * y + c * y * y);
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float y = e == 0 ? loy : hiy;
+        const float x = a > 1e-12f ? clampf(-b * y / a, lox, hix) : lox;
+        best = fminf(best, a * x * x + 2.0f * b * x * y + c * y * y);
+    }
+    return best;
+}
+
+// frame.slang:133-138: does tile (tx, ty) hold a pixel centre inside the footprint?
+__device__ __forceinline__ bool tile_touched(uint32_t width, uint32_t height, float cx, float cy,
+                                             float ca, float cb, float cc, float cutoff, uint32_t tx,
+                                             uint32_t ty) {
+    const float firstX = static_cast<float>(tx * kTile) + 0.5f;
+    const float firstY = static_cast<float>(ty * kTile) + 0.5f;
+    const float lastX = static_cast<float>(min((tx + 1) * kTile, width) - 1) + 0.5f;
+    const float lastY = static_cast<float>(min((ty + 1) * kTile, height) - 1) + 0.5f;
+    return min_power_over_box(ca, cb, cc, firstX - cx, firstY - cy, lastX - cx, lastY - cy) <= cutoff;
+}
+
+// shaders/lrt/common/color.slang:7-10
+__device__ __forceinline__ float srgb_to_linear(float c) {
+    c = fmaxf(c, 0.0f);
+    return c <= 0.04045f ? c / 12.92f : lrt_pow((c + 0.055f) / 1.055f, 2.4f);
+}
+
+}  // namespace lrt

@@ -1,0 +1,278 @@
+// Stable LSD radix sort, onesweep form (Adinets & Merrill, "Onesweep: A
+// Faster Least Significant Digit Radix Sort for GPUs", 2022), used for the
+// rasteriser's pair sort (stage c) and for the public lrt_radix_sort (the
+// reference's gpu::RadixSort, modules/gpu/src/algo/RadixSort.cpp:80-157,
+// which runs four dispatches per 8-bit pass with one thread walking each
+// chunk serially).
+//
+// Here a sort is one histogram kernel that reads the keys once and counts
+// every pass's digits, then one kernel per 8-bit digit that:
+//   1. takes the next 4096-key partition by atomic ticket (launch order),
+//   2. ranks its keys stably inside each warp with __match_any_sync (keys are
+//      warp-striped, so a warp's item j covers 32 consecutive keys and items
+//      are visited in order), and across warps with per-warp digit counts,
+//   3. publishes its per-digit counts and resolves the prefix of all earlier
+//      partitions by decoupled look-back (bounded waits),
+//   4. scatters keys (and values) into shared memory in digit order, then
+//      writes them out so that consecutive threads write consecutive slots.
+// Only the key bits asked for are sorted: the pass count is ceil(bits / 8).
+// Key types: uint32 and uint64, with or without uint32 values.
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+#include <cuda/atomic>
+
+namespace lrt {
+namespace {
+
+constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kSortWarps = kSortThreads / 32;
+constexpr uint32_t kSortItems = 16;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+constexpr uint32_t kDigits = 256;
+constexpr uint32_t kFlagAggregate = 1u << 30;
+constexpr uint32_t kFlagInclusive = 2u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1;
+constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint32_t kMaxPasses = 8;
+constexpr uint32_t kHistThreads = 512;
+
+// 256-wide exclusive scan across the block (one value per thread).
+__device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* sWarp) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= d) x += o;
+    }
+    if (lane == 31) sWarp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kSortWarps ? sWarp[lane] : 0;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= d) w += o;
+        }
+        if (lane < kSortWarps) sWarp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp == 0 ? 0 : sWarp[warp - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t digit_of(K key, uint32_t shift) {
+    return static_cast<uint32_t>(key >> shift) & 0xFFu;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kHistThreads)
+histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount, uint32_t cap,
+                 uint32_t firstBit, uint32_t passes, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sHist[kMaxPasses * kDigits];
+    for (uint32_t i = threadIdx.x; i < passes * kDigits; i += blockDim.x) sHist[i] = 0;
+    __syncthreads();
+    const uint32_t n = min(*dCount, cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const K key = keys[i];
+        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p * kDigits + digit_of(key, firstBit + 8 * p)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < passes * kDigits; i += blockDim.x)
+        if (sHist[i] != 0) atomicAdd(&hist[i], sHist[i]);
+}
+
+template <typename K, bool kValues>
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
+                uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
+                const uint32_t* __restrict__ hist, uint32_t* __restrict__ lookback,
+                uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    K* sKeys = reinterpret_cast<K*>(smem);
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * kSortTile);
+    __shared__ uint32_t sWarpHist[kSortWarps][kDigits];
+    __shared__ uint32_t sBlockStart[kDigits];
+    __shared__ uint32_t sGlobal[kDigits];
+    __shared__ uint32_t sScan[kSortWarps];
+    __shared__ uint32_t sPart;
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    if (tid == 0) sPart = atomicAdd(ticket, 1u);
+    for (uint32_t i = tid; i < kSortWarps * kDigits; i += kSortThreads) (&sWarpHist[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t n = min(*dCount, cap);
+    const uint32_t part = sPart;
+    const uint32_t base = part * kSortTile;
+    if (base >= n) return;
+
+    // Warp-striped load: item j of lane l is key base + 512 warp + 32 j + l.
+    K key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t dig[kSortItems];
+    const uint32_t wbase = base + warp * (kSortItems * 32);
+#pragma unroll
+    for (uint32_t j = 0; j < kSortItems; ++j) {
+        const uint32_t idx = wbase + j * 32 + lane;
+        const bool ok = idx < n;
+        key[j] = ok ? kin[idx] : K(0);
+        if (kValues) val[j] = ok ? vin[idx] : 0u;
+        dig[j] = ok ? digit_of(key[j], shift) : kDigits;
+    }
+
+    // Stable rank inside the warp: peers with equal digits, lower lanes first;
+    // items in order.
+    uint32_t rank[kSortItems];
+    const uint32_t lowerLanes = (1u << lane) - 1u;
+#pragma unroll
+    for (uint32_t j = 0; j < kSortItems; ++j) {
+        const uint32_t d = dig[j];
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t prior = d < kDigits ? sWarpHist[warp][d] : 0u;
+        __syncwarp();
+        const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers));
+        if (lane == leader && d < kDigits) sWarpHist[warp][d] = prior + static_cast<uint32_t>(__popc(peers));
+        rank[j] = prior + static_cast<uint32_t>(__popc(peers & lowerLanes));
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Per digit (thread = digit): warps' exclusive offsets and the block count.
+    uint32_t count = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = sWarpHist[w][tid];
+        sWarpHist[w][tid] = count;
+        count += c;
+    }
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(lookback[static_cast<size_t>(part) * kDigits + tid]);
+    if (part == 0) {
+        mine.store(kFlagInclusive | count, cuda::memory_order_relaxed);
+    } else {
+        mine.store(kFlagAggregate | count, cuda::memory_order_relaxed);
+    }
+    const uint32_t blockStart = block_exclusive_scan_256(count, sScan);
+    const uint32_t globalStart = block_exclusive_scan_256(hist[tid], sScan);
+    sBlockStart[tid] = blockStart;
+
+    uint32_t prefix = 0;
+    if (part > 0) {
+        int64_t p = static_cast<int64_t>(part) - 1;
+        uint32_t spins = 0;
+        while (p >= 0) {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> s(lookback[static_cast<size_t>(p) * kDigits + tid]);
+            const uint32_t word = s.load(cuda::memory_order_relaxed);
+            if ((word & ~kValueMask) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(err, kErrTimeout);
+                    break;
+                }
+                __nanosleep(20);
+                continue;
+            }
+            prefix += word & kValueMask;
+            if (word & kFlagInclusive) break;
+            --p;
+        }
+        mine.store(kFlagInclusive | (prefix + count), cuda::memory_order_relaxed);
+    }
+    sGlobal[tid] = globalStart + prefix - blockStart;
+    __syncthreads();
+
+    // Scatter into shared memory in digit order.
+#pragma unroll
+    for (uint32_t j = 0; j < kSortItems; ++j) {
+        const uint32_t d = dig[j];
+        if (d < kDigits) {
+            const uint32_t at = sBlockStart[d] + sWarpHist[warp][d] + rank[j];
+            sKeys[at] = key[j];
+            if (kValues) sVals[at] = val[j];
+        }
+    }
+    __syncthreads();
+
+    // Write out: slot i of the block goes to sGlobal[digit] + i.
+    const uint32_t valid = min(kSortTile, n - base);
+    for (uint32_t i = tid; i < valid; i += kSortThreads) {
+        const K k = sKeys[i];
+        const uint32_t at = sGlobal[digit_of(k, shift)] + i;
+        kout[at] = k;
+        if (kValues) vout[at] = sVals[i];
+    }
+}
+
+template <typename K, bool kValues>
+cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
+                      uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
+                      bool* resultInAlt, cudaStream_t stream) {
+    *resultInAlt = false;
+    if (cap == 0 || bits == 0) return cudaSuccess;
+    const uint32_t passes = (bits + 7) / 8;
+    const uint32_t parts = (cap + kSortTile - 1) / kSortTile;
+    char* s = static_cast<char*>(scratch);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(s);                     // kMaxPasses
+    uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
+    uint32_t* lookback = reinterpret_cast<uint32_t*>(s + 64 + kMaxPasses * kDigits * 4);
+    const size_t bytes = sort_scratch_bytes(cap, bits);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, bytes, stream);
+    if (e != cudaSuccess) return e;
+    const uint32_t histBlocks = std::max(1u, std::min(parts, 148u * 4u));
+    histogram_kernel<K><<<histBlocks, kHistThreads, 0, stream>>>(keys, dCount, cap, firstBit, passes, hist);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(K) * kSortTile + (kValues ? sizeof(uint32_t) * kSortTile : 0);
+    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    K* src = keys;
+    K* dst = keysAlt;
+    uint32_t* vsrc = vals;
+    uint32_t* vdst = valsAlt;
+    for (uint32_t p = 0; p < passes; ++p) {
+        onesweep_kernel<K, kValues><<<parts, kSortThreads, smem, stream>>>(
+            src, dst, vsrc, vdst, dCount, cap, hist + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
+            tickets + p, err, firstBit + 8 * p);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        std::swap(src, dst);
+        std::swap(vsrc, vdst);
+    }
+    *resultInAlt = (passes & 1u) != 0;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+size_t sort_scratch_bytes(uint32_t cap, uint32_t bits) {
+    const size_t passes = (bits + 7) / 8;
+    const size_t parts = (static_cast<size_t>(cap) + kSortTile - 1) / kSortTile;
+    return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * 4;
+}
+
+cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
+                            const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
+                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream) {
+    if (bits > 64 || firstBit + bits > 64 || (bits + 7) / 8 > kMaxPasses) return cudaErrorInvalidValue;
+    if (vals != nullptr)
+        return sort_impl<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
+                                         resultInAlt, stream);
+    return sort_impl<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
+                                      resultInAlt, stream);
+}
+
+cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
+                            const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
+                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream) {
+    if (bits > 32 || firstBit + bits > 32) return cudaErrorInvalidValue;
+    if (vals != nullptr)
+        return sort_impl<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
+                                         resultInAlt, stream);
+    return sort_impl<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
+                                      resultInAlt, stream);
+}
+
+}  // namespace lrt

@@ -1,0 +1,287 @@
+"""The tile rasteriser, shaped like the reference's ``lrt::render::TileRasterizer``
+(modules/render/include/lrt/render/TileRasterizer.h:26-193): ``create``, then
+``render(camera | projection, instances, settings, targets)`` returning
+``FrameStats``. Every call goes through the C-ABI of the in-tree CUDA library.
+Device memory is torch's; the rasteriser's own scratch is the library's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _abi
+from .camera import Camera, Projection, projection_for
+from .scene import GpuSplats
+
+
+class EditShape(enum.IntEnum):
+    BOX = 0
+    SPHERE = 1
+
+
+class EditMode(enum.IntEnum):
+    KEEP = 0
+    REMOVE = 1
+    GRADE = 2
+
+
+@dataclass
+class SplatEdit:
+    """SplatEdit (TileRasterizer.h:29-50)."""
+    active: bool = False
+    shape: EditShape = EditShape.BOX
+    mode: EditMode = EditMode.GRADE
+    centre: tuple[float, float, float] = (0.0, 0.0, 0.0)
+    size: tuple[float, float, float] = (1.0, 1.0, 1.0)
+    tint: tuple[float, float, float] = (1.0, 1.0, 1.0)
+    saturation: float = 1.0
+    brightness: float = 1.0
+    opacity: float = 1.0
+    min_opacity: float = 0.0
+    max_scale: float = 0.0
+    invert: bool = False
+
+    def fill(self, e: _abi.SplatEdit) -> None:
+        e.active = 1 if self.active else 0
+        e.shape = int(self.shape)
+        e.mode = int(self.mode)
+        e.invert = 1 if self.invert else 0
+        e.centre[:] = list(map(float, self.centre))
+        e.size[:] = list(map(float, self.size))
+        e.tint[:] = list(map(float, self.tint))
+        e.saturation = self.saturation
+        e.brightness = self.brightness
+        e.opacity = self.opacity
+        e.min_opacity = self.min_opacity
+        e.max_scale = self.max_scale
+
+
+@dataclass
+class SplatInstance:
+    """SplatInstance (TileRasterizer.h:52-67) without relighting."""
+    splats: GpuSplats | None
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+    edit: SplatEdit = field(default_factory=SplatEdit)
+
+
+class Depth(enum.IntEnum):
+    MEAN = 0
+    THRESHOLD = 1
+
+
+@dataclass
+class RenderSettings:
+    """RenderSettings (TileRasterizer.h:105-118), same defaults."""
+    width: int = 1920
+    height: int = 1080
+    antialias: bool = True
+    max_sh_degree: int = 3
+    background: tuple[float, float, float, float] = (0.0, 0.0, 0.0, 0.0)
+    depth: Depth = Depth.MEAN
+    depth_threshold: float = 0.5
+    linearise: bool = True
+    time_stages: bool = False
+
+    def struct(self) -> _abi.RenderSettingsStruct:
+        s = _abi.RenderSettingsStruct()
+        s.width, s.height = int(self.width), int(self.height)
+        s.antialias = 1 if self.antialias else 0
+        s.max_sh_degree = int(self.max_sh_degree)
+        s.background[:] = list(map(float, self.background))
+        s.depth_mode = int(self.depth)
+        s.depth_threshold = float(self.depth_threshold)
+        s.linearise = 1 if self.linearise else 0
+        s.time_stages = 1 if self.time_stages else 0
+        return s
+
+
+@dataclass
+class FrameStats:
+    """FrameStats (TileRasterizer.h:120-126)."""
+    splats: int = 0
+    visible: int = 0
+    pairs: int = 0
+    project_ms: float = 0.0
+    depth_sort_ms: float = 0.0
+    counts_ms: float = 0.0
+    emit_ms: float = 0.0
+    tile_sort_ms: float = 0.0
+    blend_ms: float = 0.0
+    total_ms: float = 0.0
+
+    @staticmethod
+    def from_struct(s: _abi.FrameStatsStruct) -> "FrameStats":
+        return FrameStats(s.splats, s.visible, s.pairs, s.project_ms, s.depth_sort_ms, s.counts_ms, s.emit_ms,
+                          s.tile_sort_ms, s.blend_ms, s.total_ms)
+
+    def stages_line(self) -> str:
+        """The stage breakdown `lrt bench --stages` prints (apps/lrt/src/CmdRender.cpp:412-418)."""
+        return (f"project {self.project_ms:.2f}, depth sort {self.depth_sort_ms:.2f}, counts {self.counts_ms:.2f}, "
+                f"emit {self.emit_ms:.2f}, tile sort+ranges {self.tile_sort_ms:.2f}, blend {self.blend_ms:.2f}")
+
+
+class RenderTargets:
+    """RenderTargets (TileRasterizer.h:128-134): colour float4 premultiplied
+    linear [H, W, 4] and depth [H, W], bottom row first, on the device.
+    Reallocated by the rasteriser when the frame's size changes."""
+
+    def __init__(self, width: int = 0, height: int = 0, device="cuda"):
+        self.width = 0
+        self.height = 0
+        self.device = device
+        self.colour: torch.Tensor | None = None
+        self.depth: torch.Tensor | None = None
+        if width and height:
+            self.reserve(width, height)
+
+    def reserve(self, width: int, height: int) -> None:
+        if self.width == width and self.height == height and self.colour is not None:
+            return
+        self.colour = torch.empty((height, width, 4), dtype=torch.float32, device=self.device)
+        self.depth = torch.empty((height, width), dtype=torch.float32, device=self.device)
+        self.width, self.height = width, height
+
+    def struct(self) -> _abi.TargetsStruct:
+        t = _abi.TargetsStruct()
+        t.width, t.height = self.width, self.height
+        t.colour = self.colour.data_ptr()
+        t.depth = self.depth.data_ptr()
+        return t
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, torch.cuda.Stream):
+        return stream.cuda_stream
+    return int(stream)
+
+
+class TileRasterizer:
+    """TileRasterizer::create / render over ``lrt_rast_*``."""
+
+    def __init__(self, handle: C.c_void_p, device: int):
+        self._handle = handle
+        self.device = device
+
+    @staticmethod
+    def create(device: int | None = None) -> "TileRasterizer":
+        lib = _abi.load()
+        if device is None:
+            device = torch.cuda.current_device()
+        h = C.c_void_p()
+        code = lib.lrt_rast_create(C.byref(h), int(device))
+        _abi.check(code, f"lrt_rast_create(device {device})")
+        return TileRasterizer(h, int(device))
+
+    def close(self) -> None:
+        if self._handle:
+            _abi.load().lrt_rast_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return _abi.load().lrt_rast_last_error(self._handle).decode()
+
+    def _check(self, code: int) -> None:
+        if code != _abi.OK:
+            raise _abi.LrtError(code, self.last_error())
+
+    def render(self, view: Camera | Projection, instances: Sequence[SplatInstance], settings: RenderSettings,
+               targets: RenderTargets, stream=None) -> FrameStats:
+        lib = _abi.load()
+        projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
+        targets.reserve(settings.width, settings.height)
+        clouds = []
+        arr = (_abi.SplatInstanceStruct * max(1, len(instances)))()
+        for k, inst in enumerate(instances):
+            if inst.splats is not None and inst.splats.count > 0:
+                cs = inst.splats.struct()
+                clouds.append(cs)
+                arr[k].splats = C.pointer(cs)
+            arr[k].object_to_world[:] = [float(v) for v in np.asarray(inst.object_to_world, np.float64).reshape(16)]
+            inst.edit.fill(arr[k].edit)
+        pr = projection.struct()
+        st = settings.struct()
+        tg = targets.struct()
+        stats = _abi.FrameStatsStruct()
+        code = lib.lrt_rast_render(self._handle, C.byref(pr), arr, len(instances), C.byref(st), C.byref(tg),
+                                   C.byref(stats), _stream_ptr(stream))
+        self._check(code)
+        return FrameStats.from_struct(stats)
+
+    def debug_view(self) -> _abi.DebugView:
+        v = _abi.DebugView()
+        self._check(_abi.load().lrt_rast_debug_view(self._handle, C.byref(v)))
+        return v
+
+    def debug_arrays(self) -> dict[str, torch.Tensor]:
+        """Copies of the last frame's intermediate buffers (for parity checks)."""
+        v = self.debug_view()
+        dev = torch.device("cuda", self.device)
+
+        def grab(ptr, count, dtype, cols=1):
+            shape = (count, cols) if cols > 1 else (count,)
+            if not count:
+                return torch.empty(shape, dtype=dtype, device=dev)
+            return device_view(ptr, shape, dtype, self.device).clone()
+
+        return {
+            "proj": grab(v.proj, v.slots, torch.float32, 12),
+            "rects": grab(v.rects, v.slots, torch.int32, 4),
+            "touched": grab(v.touched, v.slots, torch.int32),
+            "depth_keys": grab(v.depth_keys, v.slots, torch.int32),
+            "pairs": grab(v.pairs, v.pairs_count, torch.int64),
+            "ranges": grab(v.ranges, v.tiles, torch.int32, 2),
+            "slot_bits": v.slot_bits,
+            "tile_bits": v.tile_bits,
+            "visible": v.visible,
+        }
+
+    def prefix_sum(self, values: torch.Tensor, out: torch.Tensor, total: torch.Tensor, stream=None) -> None:
+        """PrefixSum::apply over uint32 bit patterns held in int32 tensors."""
+        n = values.numel()
+        self._check(_abi.load().lrt_prefix_sum(self._handle, values.data_ptr(), out.data_ptr(), total.data_ptr(), n,
+                                              _stream_ptr(stream)))
+
+    def radix_sort(self, keys: torch.Tensor, values: torch.Tensor | None, key_bits: int, stream=None) -> None:
+        """RadixSort::sort in place: keys int32 (4-byte) or int64 (8-byte) bit patterns."""
+        key_bytes = keys.element_size()
+        self._check(_abi.load().lrt_radix_sort(self._handle, keys.data_ptr(),
+                                              values.data_ptr() if values is not None else None, keys.numel(),
+                                              key_bits, key_bytes, _stream_ptr(stream)))
+
+
+_TYPESTR = {torch.float32: "<f4", torch.int32: "<i4", torch.int64: "<i8"}
+
+
+class _DeviceArray:
+    """A borrowed device pointer presented through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, shape: tuple, dtype: torch.dtype):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": _TYPESTR[dtype],
+                                         "data": (int(ptr), True), "version": 3, "strides": None}
+
+
+def device_view(ptr: int, shape: tuple, dtype: torch.dtype, device: int) -> torch.Tensor:
+    """A tensor viewing library-owned device memory (valid until the next call on the handle)."""
+    torch.cuda.synchronize(device)
+    return torch.as_tensor(_DeviceArray(ptr, shape, dtype), device=torch.device("cuda", device))
+
+
+def math_eval(fn: int, x: torch.Tensor) -> torch.Tensor:
+    """The library's own exp (0), log (1), sRGB-to-linear (2), cut-off power (3), on the device."""
+    y = torch.empty_like(x)
+    _abi.check(_abi.load().lrt_math_eval(fn, x.data_ptr(), y.data_ptr(), x.numel(),
+                                         torch.cuda.current_stream().cuda_stream), "math_eval")
+    return y

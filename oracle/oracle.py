@@ -1,0 +1,243 @@
+"""ORACLE -- test infrastructure, not product code.
+
+ctypes wrapper of ``oracle/_build/liblrt_oracle.so``, the CPU restatement of
+lucabRTrender's splat tile rasteriser (see ``lrt_oracle.h`` for what it
+restates and how it is pinned). Only the tests, the smoke check and the
+benchmark's CPU-baseline leg use it, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liblrt_oracle.so"
+REF_LIB = HERE / "_ref" / "libref_camera.so"
+
+import sys  # noqa: E402
+
+sys.path.insert(0, str(HERE.parent))
+from lucabrtrender_b200 import _abi  # noqa: E402  (struct layouts of the public header)
+
+
+class FrameOut(C.Structure):
+    _fields_ = [
+        ("colour", C.c_void_p), ("depth", C.c_void_p), ("proj", C.c_void_p), ("rects", C.c_void_p),
+        ("touched", C.c_void_p), ("depth_keys", C.c_void_p), ("pair_tiles", C.c_void_p),
+        ("pair_slots", C.c_void_p), ("ranges", C.c_void_p), ("pair_capacity", C.c_uint64),
+        ("pairs", C.c_uint64), ("visible", C.c_uint32), ("slots", C.c_uint32), ("stage_ms", C.c_double * 6),
+    ]
+
+
+def build() -> None:
+    """Compile the restatement (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    lib.ora_exp.argtypes = [C.c_float]
+    lib.ora_exp.restype = C.c_float
+    lib.ora_log.argtypes = [C.c_float]
+    lib.ora_log.restype = C.c_float
+    lib.ora_math_eval.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.ora_math_eval.restype = None
+    lib.ora_camera_looking_at.argtypes = [C.POINTER(C.c_double)] * 3 + [C.POINTER(_abi.CameraStruct)]
+    lib.ora_projection_for.argtypes = [C.POINTER(_abi.CameraStruct), C.c_uint32, C.c_uint32,
+                                       C.POINTER(_abi.Projection)]
+    lib.ora_pack_splats.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.ora_render.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.SplatInstanceStruct), C.c_uint32,
+                               C.POINTER(_abi.RenderSettingsStruct), C.POINTER(FrameOut), C.c_uint32]
+    lib.ora_reference_render.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.SplatInstanceStruct),
+                                         C.c_uint32, C.POINTER(_abi.RenderSettingsStruct), C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_uint32), C.c_uint32]
+    lib.ora_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                       C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_uint64)]
+    lib.ora_random_cloud.argtypes = [C.c_uint32, C.c_uint64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
+    lib.ora_f32_to_f16.argtypes = [C.c_float]
+    lib.ora_f32_to_f16.restype = C.c_uint16
+    lib.ora_f16_to_f32.argtypes = [C.c_uint16]
+    lib.ora_f16_to_f32.restype = C.c_float
+    _lib = lib
+    return lib
+
+
+def _check(code: int, what: str) -> None:
+    if code != 0:
+        raise RuntimeError(f"oracle {what} failed with status {code}")
+
+
+# ---------------------------------------------------------------- camera ----
+def looking_at(eye, target, up=(0.0, 1.0, 0.0)) -> _abi.CameraStruct:
+    out = _abi.CameraStruct()
+    arr = lambda v: (C.c_double * 3)(*map(float, v))  # noqa: E731
+    _check(load().ora_camera_looking_at(arr(eye), arr(target), arr(up), C.byref(out)), "looking_at")
+    return out
+
+
+def projection_for(camera: _abi.CameraStruct, width: int, height: int) -> _abi.Projection:
+    out = _abi.Projection()
+    _check(load().ora_projection_for(C.byref(camera), width, height, C.byref(out)), "projection_for")
+    return out
+
+
+# --------------------------------------------------------------- packing ----
+@dataclass
+class HostCloud:
+    positions: np.ndarray   # [N, 4] float32
+    shape: np.ndarray       # [N, 4] uint32
+    sh: np.ndarray          # [N, words] uint32
+    rest_per_colour: int
+
+    @property
+    def count(self) -> int:
+        return int(self.positions.shape[0])
+
+    def struct(self) -> _abi.GpuSplatsStruct:
+        s = _abi.GpuSplatsStruct()
+        s.count = self.count
+        s.rest_per_colour = self.rest_per_colour
+        s.sh_words = int(self.sh.shape[1])
+        s.positions = self.positions.ctypes.data
+        s.shape = self.shape.ctypes.data
+        s.sh = self.sh.ctypes.data
+        return s
+
+
+def pack(raw: np.ndarray, file_per_colour: int, keep: int) -> HostCloud:
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    n, fpr = raw.shape
+    words = max((keep * 3 + 1) // 2, 1)
+    pos = np.empty((n, 4), np.float32)
+    shape = np.empty((n, 4), np.uint32)
+    sh = np.empty((n, words), np.uint32)
+    kept = C.c_uint32()
+    _check(load().ora_pack_splats(raw.ctypes.data, n, fpr, file_per_colour, keep, pos.ctypes.data,
+                                  shape.ctypes.data, sh.ctypes.data, C.byref(kept)), "pack")
+    k = kept.value
+    return HostCloud(pos[:k].copy(), shape[:k].copy(), sh[:k].copy(), keep)
+
+
+def random_cloud(count: int, seed: int, min_size=0.004, max_size=0.6, min_opacity=0.02,
+                 max_opacity=0.99) -> np.ndarray:
+    """The reference tests' randomCloud (23-float degree-1 records)."""
+    raw = np.empty((count, 23), np.float32)
+    _check(load().ora_random_cloud(count, seed, min_size, max_size, min_opacity, max_opacity, raw.ctypes.data),
+           "random_cloud")
+    return raw
+
+
+# ------------------------------------------------------------- rendering ----
+def _instances(instances):
+    """instances: list of (HostCloud, object_to_world 4x4, edit lrt_splat_edit | None)."""
+    arr = (_abi.SplatInstanceStruct * max(1, len(instances)))()
+    keep = []
+    for k, (cloud, m, edit) in enumerate(instances):
+        cs = cloud.struct()
+        keep.append(cs)
+        arr[k].splats = C.pointer(cs)
+        arr[k].object_to_world[:] = [float(v) for v in np.asarray(m, np.float64).reshape(16)]
+        if edit is not None:
+            arr[k].edit = edit
+    return arr, keep
+
+
+def render(projection: _abi.Projection, instances, settings: _abi.RenderSettingsStruct, threads: int = 0,
+           want_pairs: bool = True) -> dict:
+    slots = sum(c.count for c, _, _ in instances)
+    tiles_x = (settings.width + 15) // 16
+    tiles_y = (settings.height + 15) // 16
+    w, h = settings.width, settings.height
+    colour = np.zeros((h, w, 4), np.float32)
+    depth = np.zeros((h, w), np.float32)
+    proj = np.zeros((slots, 12), np.float32)
+    rects = np.zeros((slots, 4), np.uint32)
+    touched = np.zeros(slots, np.uint32)
+    keys = np.zeros(slots, np.uint32)
+    ranges = np.zeros((tiles_x * tiles_y, 2), np.uint32)
+    cap = int(touched.size) * 0  # filled on the second call when pairs are wanted
+    out = FrameOut()
+    out.colour, out.depth = colour.ctypes.data, depth.ctypes.data
+    out.proj, out.rects = proj.ctypes.data, rects.ctypes.data
+    out.touched, out.depth_keys = touched.ctypes.data, keys.ctypes.data
+    out.ranges = ranges.ctypes.data
+    out.pair_capacity = cap
+    arr, keep = _instances(instances)
+    _check(load().ora_render(C.byref(projection), arr, len(instances), C.byref(settings), C.byref(out), threads),
+           "render")
+    pairs = int(out.pairs)
+    result = dict(colour=colour, depth=depth, proj=proj, rects=rects, touched=touched, depth_keys=keys,
+                  ranges=ranges, pairs=pairs, visible=int(out.visible), slots=int(out.slots),
+                  stage_ms=list(out.stage_ms))
+    if want_pairs:
+        # The pair list is only known after the frame: recompute it into buffers of that size
+        # (deterministic, so the second run is the same frame).
+        pt = np.zeros(pairs, np.uint32)
+        ps = np.zeros(pairs, np.uint32)
+        out2 = FrameOut()
+        out2.pair_tiles, out2.pair_slots, out2.pair_capacity = pt.ctypes.data, ps.ctypes.data, pairs
+        _check(load().ora_render(C.byref(projection), arr, len(instances), C.byref(settings), C.byref(out2),
+                                 threads), "render")
+        result["pair_tiles"] = pt
+        result["pair_slots"] = ps
+    return result
+
+
+def reference_render(projection: _abi.Projection, instances, settings: _abi.RenderSettingsStruct,
+                     threads: int = 0):
+    w, h = settings.width, settings.height
+    colour = np.zeros((h, w, 4), np.float32)
+    depth = np.zeros((h, w), np.float32)
+    over = C.c_uint32()
+    arr, keep = _instances(instances)
+    _check(load().ora_reference_render(C.byref(projection), arr, len(instances), C.byref(settings),
+                                       colour.ctypes.data, depth.ctypes.data, C.byref(over), threads),
+           "reference_render")
+    return colour, depth, int(over.value)
+
+
+@dataclass
+class ImageDifference:
+    p99: int
+    max: int
+    over2: int
+    pixels: int
+    histogram: np.ndarray
+
+
+def compare_images(a: np.ndarray, b: np.ndarray) -> ImageDifference:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    h, w = a.shape[:2]
+    hist = np.zeros(256, np.uint32)
+    p99, mx = C.c_uint32(), C.c_uint32()
+    over2, pixels = C.c_uint64(), C.c_uint64()
+    _check(load().ora_compare_images(a.ctypes.data, b.ctypes.data, w, h, hist.ctypes.data, C.byref(p99),
+                                     C.byref(mx), C.byref(over2), C.byref(pixels)), "compare_images")
+    return ImageDifference(p99.value, mx.value, over2.value, pixels.value, hist)
+
+
+def math_eval(fn: int, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty_like(x)
+    load().ora_math_eval(fn, x.ctypes.data, y.ctypes.data, x.size)
+    return y
+
+
+def threads() -> int:
+    return os.cpu_count() or 1

@@ -1,0 +1,174 @@
+"""Shared scene set-ups for the tests: the reference's own render-test scenes
+(tests/render/test_splat_render.cpp, tests/render/SplatFixtures.h in the
+lucabRTrender tree) and the benchmark's synthetic scenes, built once as packed
+bytes and handed to both the oracle (host pointers) and the CUDA path."""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+import lucabrtrender_b200 as L
+from lucabrtrender_b200 import _abi
+
+import oracle as ora
+
+SH0 = np.float32(0.28209479)
+
+
+def cloud_record(x, y, z, opacity, sx, sy, sz, wxyz, colour, rest=None) -> np.ndarray:
+    """CloudBuilder::add (SplatFixtures.h:30-45): one degree-1 record of 23 floats."""
+    f = np.float32
+    r = np.zeros(23, np.float32)
+    a = f(opacity)
+    r[:14] = [x, y, z, np.log(a / (f(1) - a)), np.log(f(sx)), np.log(f(sy)), np.log(f(sz)), *wxyz,
+              (f(colour[0]) - f(0.5)) / SH0, (f(colour[1]) - f(0.5)) / SH0, (f(colour[2]) - f(0.5)) / SH0]
+    if rest is not None:
+        r[14:] = rest
+    return r
+
+
+def packed_from_raw(raw: np.ndarray, file_per_colour: int, max_degree: int = 3) -> L.PackedSplats:
+    return L.pack_splats(raw, file_per_colour, max_degree)
+
+
+def host_cloud(p: L.PackedSplats) -> ora.HostCloud:
+    return ora.HostCloud(p.positions, p.shape, p.sh, p.rest_per_colour)
+
+
+def settings(width=250, height=190, antialias=True, linearise=True, background=(0, 0, 0, 0), depth=0,
+             threshold=0.5, max_sh_degree=3) -> L.RenderSettings:
+    return L.RenderSettings(width=width, height=height, antialias=antialias, max_sh_degree=max_sh_degree,
+                            background=background, depth=L.Depth(depth), depth_threshold=threshold,
+                            linearise=linearise)
+
+
+def camera(eye, target=(0, 0, 0), focal=50.0, orthographic=False, window_translate=(0.0, 0.0),
+           window_scale=(1.0, 1.0), roll=0.0, near=0.1) -> L.Camera:
+    c = L.Camera.looking_at(eye, target)
+    c.lens.focal = focal
+    c.lens.orthographic = orthographic
+    c.lens.window_translate = tuple(window_translate)
+    c.lens.window_scale = tuple(window_scale)
+    c.lens.window_roll = roll
+    c.lens.near_z = near
+    return c
+
+
+def translation(t) -> np.ndarray:
+    m = np.eye(4)
+    m[:3, 3] = t
+    return m
+
+
+def rotation_y(deg) -> np.ndarray:
+    c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))
+    m = np.eye(4)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c, s, -s, c
+    return m
+
+
+def scaling(s) -> np.ndarray:
+    return np.diag([s[0], s[1], s[2], 1.0])
+
+
+def edit_struct(edit: L.SplatEdit | None) -> _abi.SplatEdit | None:
+    if edit is None:
+        return None
+    e = _abi.SplatEdit()
+    edit.fill(e)
+    return e
+
+
+@dataclass
+class Scene:
+    """One frame: packed clouds with transforms and edits, a camera, settings."""
+    name: str
+    clouds: list            # [(PackedSplats, object_to_world, SplatEdit | None)]
+    camera: L.Camera
+    settings: L.RenderSettings
+    extra: dict = field(default_factory=dict)
+
+    def projection(self) -> L.Projection:
+        return L.projection_for(self.camera, self.settings.width, self.settings.height)
+
+    def oracle_instances(self):
+        return [(host_cloud(p), m, edit_struct(e)) for p, m, e in self.clouds]
+
+    def oracle_render(self, threads=0, want_pairs=True):
+        return ora.render(self.projection().struct(), self.oracle_instances(), self.settings.struct(), threads,
+                          want_pairs)
+
+    def oracle_reference(self, threads=0):
+        return ora.reference_render(self.projection().struct(), self.oracle_instances(), self.settings.struct(),
+                                    threads)
+
+    def gpu_instances(self, device="cuda"):
+        out = []
+        for p, m, e in self.clouds:
+            out.append(L.SplatInstance(L.to_device(p, device), m, e if e is not None else L.SplatEdit()))
+        return out
+
+
+_RANDOM_CACHE = {}
+
+
+def random_cloud_packed(count=3000, seed=7) -> L.PackedSplats:
+    key = (count, seed)
+    if key not in _RANDOM_CACHE:
+        _RANDOM_CACHE[key] = packed_from_raw(ora.random_cloud(count, seed), 3, 3)
+    return _RANDOM_CACHE[key]
+
+
+def reference_render_scenes() -> list[Scene]:
+    """The five sections of "the tile rasteriser renders what the GPU reference
+    renders" (test_splat_render.cpp:70-121): a 3000-splat randomCloud(seed 7),
+    degree 1, at 250x190 (partial tiles)."""
+    cloud = random_cloud_packed(3000, 7)
+    I = np.eye(4)
+    scenes = [
+        Scene("perspective", [(cloud, I, None)], camera((1.5, 1.0, 6.0), focal=30.0), settings()),
+        Scene("frustum_edge", [(cloud, I, None)], camera((0.3, -0.2, 2.2), focal=18.0), settings()),
+        Scene("orthographic", [(cloud, I, None)], camera((0.0, 3.0, 5.0), focal=5.0, orthographic=True), settings()),
+        Scene("no_aa_window_roll", [(cloud, I, None)],
+              camera((-2.0, 0.5, 5.0), window_translate=(0.2, 0.0), window_scale=(1.0, 1.3), roll=25.0),
+              settings(antialias=False)),
+        Scene("two_instances",
+              [(cloud, I, None),
+               (cloud, translation((0.5, 0.0, -1.5)) @ rotation_y(40.0) @ scaling((1.0, 0.7, 1.3)), None)],
+              camera((2.0, 1.5, 7.0), target=(0.0, 0.0, -0.5)), settings()),
+    ]
+    return scenes
+
+
+def edit_scenes() -> list[Scene]:
+    """"a SplatEdit renders as the GPU reference renders it" (test_splat_render.cpp:231-283)."""
+    cloud = random_cloud_packed(3000, 29)
+    cam = camera((1.5, 1.0, 6.0), focal=30.0)
+    edits = {
+        "keep_box": L.SplatEdit(active=True, mode=L.EditMode.KEEP, centre=(0.5, 0.0, 0.0), size=(1.0, 0.8, 1.5)),
+        "remove_sphere": L.SplatEdit(active=True, mode=L.EditMode.REMOVE, shape=L.EditShape.SPHERE,
+                                     size=(1.2, 0.0, 0.0), tint=(0.2, 1.0, 1.0)),
+        "grade_inverted_box": L.SplatEdit(active=True, mode=L.EditMode.GRADE, invert=True, size=(1.0, 1.0, 1.0),
+                                          tint=(1.0, 0.6, 0.3), saturation=0.3, brightness=1.4, opacity=0.5),
+        "haze_filters": L.SplatEdit(active=True, mode=L.EditMode.GRADE, size=(100.0, 100.0, 100.0), min_opacity=0.4,
+                                    max_scale=0.2),
+    }
+    return [Scene(name, [(cloud, np.eye(4), e)], cam, settings(), extra=dict(edit=e)) for name, e in edits.items()]
+
+
+def synthetic_scene(count: int, width: int, height: int, seed: int = 1, eye=(0.0, 0.0, 4.0), **dist) -> Scene:
+    raw = L.synthetic_records(count, seed, **dist)
+    packed = packed_from_raw(raw, 15, 3)
+    cam = L.square_pixel_camera(eye, (0.0, 0.0, 0.0), width, height, 60.0, 0.01)
+    return Scene(f"synthetic_{count}_{width}x{height}", [(packed, np.eye(4), None)], cam,
+                 settings(width=width, height=height))
+
+
+def pair_words_to_tile_slot(words: np.ndarray, slot_bits: int):
+    w = words.astype(np.uint64)
+    slots = (w & np.uint64((1 << slot_bits) - 1)).astype(np.uint32)
+    keys = ((w >> np.uint64(slot_bits)) & np.uint64(0xFFFFFF)).astype(np.uint32)
+    tiles = (w >> np.uint64(24 + slot_bits)).astype(np.uint32)
+    return tiles, keys, slots
