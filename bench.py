@@ -1,0 +1,319 @@
+"""Benchmark: the plain forward of the splat tile rasteriser at 1M splats, 1920x1080.
+
+Workload (the configuration the headline metric is quoted on): 1,000,000 seeded
+synthetic Gaussians (means N(0,1), log-scales N(-4.5,0.5), uniform rotations,
+opacity sigmoid(N(0,1)), SH degree 3 with DC N(0,0.5) and rest N(0,0.05)),
+1920x1080, 16x16 tiles, 0.3 px Mip-Splatting 2D filter, 60 degree vertical field
+of view, camera orbiting the origin at radius 4 over 20 frames. A step is one
+frame (one view) of the orbit through the rasteriser's public call.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's algorithm on the host cores: the
+reference's own kernels are Slang, which cannot run here, so its CPU arm is
+the oracle (oracle/, a C++ restatement of those kernels), multithreaded.
+Under torchrun each rank renders its own views of the orbit (replicas: the
+frames are independent, there is no data exchange); value is whole-job ms per
+view = max-over-ranks time / (steps x ranks).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ms/view @1M splats 1080p: plain fwd vs batched fwd+bwd; sort GB/s vs HBM"
+UNIT = "ms/view"
+SPLATS = 1_000_000
+WIDTH, HEIGHT = 1920, 1080
+FRAMES = 20
+RADIUS = 4.0
+SEED = 1
+L2_FLUSH_BYTES = 256 << 20
+
+
+def orbit_camera(L, k: int):
+    th = 2.0 * math.pi * (k % FRAMES) / FRAMES
+    eye = (RADIUS * math.sin(th), 0.0, RADIUS * math.cos(th))
+    return L.square_pixel_camera(eye, (0.0, 0.0, 0.0), WIDTH, HEIGHT, 60.0, 0.01)
+
+
+def workload_config(extra: dict | None = None) -> dict:
+    cfg = {"workload": "plain forward, 1M splats, 1920x1080, 20-frame orbit at radius 4",
+           "splats": SPLATS, "width": WIDTH, "height": HEIGHT, "frames": FRAMES, "tile": 16, "sh_degree": 3,
+           "seed": SEED, "l2": "flushed before every timed step (256 MB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_frames(k_frames: int, threads: int, packed, log=print) -> tuple[float, list]:
+    """The oracle (CPU restatement) rendering full frames of the orbit."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as ora
+    import lucabrtrender_b200 as L
+    from lucabrtrender_b200 import _abi  # noqa: F401
+
+    cloud = ora.HostCloud(packed.positions, packed.shape, packed.sh, packed.rest_per_colour)
+    st = L.RenderSettings(width=WIDTH, height=HEIGHT).struct()
+    times = []
+    for k in range(k_frames):
+        pr = L.projection_for(orbit_camera(L, k), WIDTH, HEIGHT).struct()
+        t = time.perf_counter()
+        ora.render(pr, [(cloud, np.eye(4), None)], st, threads, want_pairs=False)
+        times.append((time.perf_counter() - t) * 1e3)
+    return float(np.mean(times)), times
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import lucabrtrender_b200 as L
+    threads = os.cpu_count() or 1
+    packed = L.pack_splats(L.synthetic_records(SPLATS, SEED), 15, 3)
+    cpu_reference_frames(args.warmup, threads, packed)
+    mean_ms, _ = cpu_reference_frames(args.steps, threads, packed)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(mean_ms, 3), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config({"reference_arm": "oracle: C++ restatement of the reference's Slang raster "
+                                                    "kernels (the Slang itself cannot run here), CPU"}),
+        "cpu_baseline": {"value": round(mean_ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full frames of the orbit, {threads} threads"},
+        "e2e": {"value": round(mean_ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    import lucabrtrender_b200 as L
+    from lucabrtrender_b200 import _abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    packed = L.pack_splats(L.synthetic_records(SPLATS, SEED), 15, 3)
+    cloud = L.to_device(packed, dev)
+    instances = [L.SplatInstance(cloud)]
+    raster = L.TileRasterizer.create(local)
+    settings = L.RenderSettings(width=WIDTH, height=HEIGHT)
+    targets = L.RenderTargets(WIDTH, HEIGHT, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    projections = [L.projection_for(orbit_camera(L, k), WIDTH, HEIGHT) for k in range(FRAMES)]
+
+    def frame(k: int, stages: bool = False):
+        settings.time_stages = stages
+        return raster.render(projections[(k + rank * 7) % FRAMES], instances, settings, targets, stream)
+
+    for k in range(max(3, args.warmup)):
+        frame(k)
+    torch.cuda.synchronize(dev)
+
+    # --- device-timed steps: inputs resident, L2 flushed before every step ---
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stats_list = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with Clocks(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            stats_list.append(frame(k, stages=True))
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = total_ms / (args.steps * world)
+
+    # --- end to end through the public call: camera from the host, image read back to pinned memory ---
+    host_colour = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
+    host_depth = torch.empty((HEIGHT, WIDTH), dtype=torch.float32, pin_memory=True)
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e2e_ms = 0.0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e_start.record(stream)
+        cam = orbit_camera(L, k + rank * 7)
+        settings.time_stages = False
+        raster.render(cam, instances, settings, targets, stream)
+        host_colour.copy_(targets.colour, non_blocking=True)
+        host_depth.copy_(targets.depth, non_blocking=True)
+        e_end.record(stream)
+        e_end.synchronize()
+        e2e_ms += e_start.elapsed_time(e_end)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = e2e_ms / (args.steps * world)
+
+    # --- roofline of the dominant kernel, measured live over the timed steps ---
+    st = stats_list
+    mean = lambda f: float(np.mean([getattr(s, f) for s in st]))  # noqa: E731
+    stage = {k: mean(k) for k in ("project_ms", "counts_ms", "emit_ms", "tile_sort_ms", "blend_ms")}
+    pairs = float(np.mean([s.pairs for s in st]))
+    visible = float(np.mean([s.visible for s in st]))
+    tiles = ((WIDTH + 15) // 16) * ((HEIGHT + 15) // 16)
+    pixels = WIDTH * HEIGHT
+    key_bits = 24 + max(1, math.ceil(math.log2(tiles)))
+    passes = math.ceil(key_bits / 8)
+    # Algorithmic bytes per launch (per unit x units):
+    #   blend:   ranges 8 B/tile + (8 B pair word + 48 B record) per pair + 20 B per pixel written
+    #   sort:    per 8-bit pass 8 B read + 8 B written per pair, plus one 8 B/pair histogram read
+    #   project: 124 B per splat read (deg 3) + 48+16+4+4 B per slot written
+    bytes_blend = 8 * tiles + 56 * pairs + 20 * pixels
+    bytes_sort = (passes * 16 + 8) * pairs
+    bytes_project = 124 * SPLATS + 72 * SPLATS
+    peak, peak_kind = measured_peaks()
+    kernels = {
+        "blend": (stage["blend_ms"], bytes_blend),
+        "pair sort + ranges": (stage["tile_sort_ms"], bytes_sort + 8 * pairs + 8 * tiles),
+        "project": (stage["project_ms"], bytes_project),
+    }
+    dom_name = max(kernels, key=lambda n: kernels[n][0])
+    dom_ms, dom_bytes = kernels[dom_name]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    sort_gbs = bytes_sort / (stage["tile_sort_ms"] * 1e-3) / 1e9 if stage["tile_sort_ms"] > 0 else None
+    launches_per_frame = 1 + 1 + 1 + 1 + passes + 1 + 1   # project, scan, duplicate, histogram, passes, ranges, blend
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            ms, times = cpu_reference_frames(args.cpu_frames, threads, packed)
+            cpu = {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_frames} full frames of the same orbit on the oracle (C++ restatement "
+                             f"of the reference's kernels), {threads} threads"}
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                       "pairs_per_frame": int(pairs), "visible_per_frame": int(visible)}),
+            "stages_ms": {k: round(v, 4) for k, v in stage.items()},
+            "sort_gbs": round(sort_gbs, 1) if sort_gbs else None,
+            "roofline": {"kernel": dom_name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_kind": peak_kind},
+            "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
+                    "h2d_bytes_per_step": _abi.C.sizeof(_abi.Projection),
+                    "d2h_bytes_per_step": pixels * 20},
+            "gpu_launches": launches_per_frame * args.steps,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    raster.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-frames", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -270,7 +270,7 @@ class _DeviceArray:
 
     def __init__(self, ptr: int, shape: tuple, dtype: torch.dtype):
         self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": _TYPESTR[dtype],
-                                         "data": (int(ptr), True), "version": 3, "strides": None}
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
 
 
 def device_view(ptr: int, shape: tuple, dtype: torch.dtype, device: int) -> torch.Tensor:

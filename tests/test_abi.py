@@ -1,0 +1,123 @@
+"""The C-ABI boundary without a GPU: the library loads, exports every symbol
+include/lrt_raster.h declares, its struct layouts match the ctypes mirror,
+host-only entry points work, and device entry points fail cleanly."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import lucabrtrender_b200 as L
+from lucabrtrender_b200 import _abi
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "lrt_raster.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(lrt_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _abi.load()
+    assert lib.lrt_abi_version() == _abi.ABI_VERSION
+    names = declared_functions()
+    assert len(names) >= 10
+    assert sorted(names) == sorted(_abi.EXPORTS)
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_abi.LIBRARY_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (lrt_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+
+
+PROBE = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "lrt_raster.h"
+#define S(t) printf(#t " %zu\n", sizeof(t));
+#define O(t, f) printf(#t "." #f " %zu\n", offsetof(t, f));
+int main(void) {
+  S(lrt_projection) O(lrt_projection, eye_world) O(lrt_projection, orthographic)
+  S(lrt_lens) S(lrt_camera) O(lrt_camera, lens)
+  S(lrt_splat_edit) O(lrt_splat_edit, max_scale)
+  S(lrt_gpu_splats) O(lrt_gpu_splats, sh)
+  S(lrt_splat_instance) O(lrt_splat_instance, edit)
+  S(lrt_render_settings) O(lrt_render_settings, time_stages)
+  S(lrt_frame_stats) O(lrt_frame_stats, total_ms)
+  S(lrt_targets) S(lrt_debug_view) O(lrt_debug_view, visible)
+  return 0;
+}
+"""
+
+CTYPES = {
+    "lrt_projection": _abi.Projection, "lrt_lens": _abi.Lens, "lrt_camera": _abi.CameraStruct,
+    "lrt_splat_edit": _abi.SplatEdit, "lrt_gpu_splats": _abi.GpuSplatsStruct,
+    "lrt_splat_instance": _abi.SplatInstanceStruct, "lrt_render_settings": _abi.RenderSettingsStruct,
+    "lrt_frame_stats": _abi.FrameStatsStruct, "lrt_targets": _abi.TargetsStruct, "lrt_debug_view": _abi.DebugView,
+}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    src = tmp_path / "probe.c"
+    src.write_text(PROBE)
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        name, value = line.split()
+        value = int(value)
+        if "." in name:
+            t, f = name.split(".")
+            assert getattr(CTYPES[t], f).offset == value, name
+        else:
+            assert C.sizeof(CTYPES[name]) == value, name
+
+
+def test_cpp_host_compiles_against_the_header(tmp_path):
+    """A C++ host links the library through the header alone (the binding a
+    maintainer adds in the reference's C++ tree)."""
+    src = tmp_path / "host.cpp"
+    src.write_text(r"""
+#include "lrt_raster.h"
+#include <cstdio>
+int main() {
+    lrt_camera cam;
+    const double eye[3] = {0, 0, 4}, target[3] = {0, 0, 0}, up[3] = {0, 1, 0};
+    if (lrt_camera_looking_at(eye, target, up, &cam) != LRT_OK) return 1;
+    lrt_projection p;
+    if (lrt_projection_for(&cam, 512, 512, &p) != LRT_OK) return 2;
+    std::printf("%.6f %.1f\n", p.focal_x, p.centre_x);
+    return lrt_abi_version() == LRT_ABI_VERSION ? 0 : 3;
+}
+""")
+    exe = tmp_path / "host"
+    subprocess.run(["g++", "-std=c++17", "-I", str(ROOT / "include"), str(src), "-o", str(exe),
+                    str(_abi.LIBRARY_PATH), f"-Wl,-rpath,{_abi.LIBRARY_PATH.parent}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.split() == [f"{512 * 50 / 24.576:.6f}", "256.0"]
+
+
+def test_host_entry_points_validate_arguments():
+    lib = _abi.load()
+    kept = C.c_uint32()
+    assert lib.lrt_pack_splats(None, 1, 59, 15, 15, None, None, None, C.byref(kept)) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_pack_splats(None, 0, 59, 3, 15, None, None, None, C.byref(kept)) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_projection_for(None, 1, 1, None) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_rast_create(None, 0) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_rast_render(None, None, None, 0, None, None, None, None) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_math_eval(7, None, None, 0, None) == _abi.INVALID_ARGUMENT
+
+
+def test_device_entry_points_fail_cleanly_without_a_device():
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    assert _abi.load().lrt_rast_create(C.byref(h), 0) == _abi.DEVICE_FAILURE
+    assert not h.value
