@@ -104,23 +104,59 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
+// A box outside which no pixel centre can pass the record's cut, with every
+// rounding of the per-pixel test accounted for, so that skipping a record
+// for a whole warp never changes a pixel. {power <= k} is an ellipse whose
+// bounding half-widths are sqrt(k c / det) and sqrt(k a / det) for the conic
+// (a, b, c). The float power of a pixel can fall below the exact one by at
+// most ~4u (|a| dx^2 + 2|b| |dx dy| + |c| dy^2) <= 4u kappa power with
+// kappa = (|a| + 2|b| + |c|) / lambda_min; det itself carries a relative
+// error up to ~4u (|ac| + b^2) / det. delta bounds both with a factor of 8
+// to spare; the cut is widened to cutoff / (1 - delta) and the half-widths by
+// (1 + delta) plus 1e-3 px. Records where delta is not small are never skipped.
+__device__ __forceinline__ float4 cull_box(const ProjRecord& rec) {
+    const float a = rec.conic.x, b = rec.conic.y, c = rec.conic.z, cutoff = rec.screen.w;
+    const float det = a * c - b * b;
+    const float half = 0.5f * (a + c);
+    const float root = sqrtf(0.25f * (a - c) * (a - c) + b * b);
+    const float lmin = half - root;
+    const float kInf = 3.0e38f;
+    if (!(det > 0.0f) || !(lmin > 0.0f) || !(cutoff >= 0.0f)) return make_float4(-kInf, kInf, -kInf, kInf);
+    const float kappa = (fabsf(a) + 2.0f * fabsf(b) + fabsf(c)) / lmin;
+    const float cond = (fabsf(a * c) + b * b) / det;
+    const float delta = 32.0f * 5.9604645e-08f * (kappa + cond + 4.0f);
+    if (!(delta < 0.25f)) return make_float4(-kInf, kInf, -kInf, kInf);
+    const float k = cutoff / (1.0f - delta);
+    const float ex = sqrtf(k * c / det) * (1.0f + delta) + 1e-3f;
+    const float ey = sqrtf(k * a / det) * (1.0f + delta) + 1e-3f;
+    if (!(ex < kInf) || !(ey < kInf)) return make_float4(-kInf, kInf, -kInf, kInf);
+    return make_float4(rec.screen.x - ex, rec.screen.x + ex, rec.screen.y - ey, rec.screen.y + ey);
+}
+
 // shaders/lrt/splat/splat_blend.slang:23-108 (splat-only entry, :110-114).
-// One block per 16x16 tile, one thread per pixel. The tile's pairs are read
-// in batches of 256: each thread copies one record into shared memory with a
-// bulk copy, completing on the batch's mbarrier; batch k+1 is in flight while
-// batch k is blended. A pixel stops at T < 1e-4 exactly as the reference's
-// loop does; the block stops when every pixel has (a block-wide vote).
+// One block per 16x16 tile, one thread per pixel; warp w covers the 8x4
+// pixel block ((w & 1) * 8, (w >> 1) * 4). The tile's pairs are read in
+// batches of 256: each thread copies one record into shared memory with a
+// bulk copy completing on the batch's mbarrier, and batch k+1 is in flight
+// while batch k is blended. Each record gets a conservative bounding box
+// (cull_box); a warp skips, as a whole, every record whose box misses the
+// bounding box of its pixels that are still blending. Each pixel runs the
+// reference's loop unchanged over the records it is given, so it stops at
+// T < 1e-4 exactly as the reference does; a warp leaves a batch when all its
+// pixels have stopped, and the block stops when every pixel has.
 __global__ void __launch_bounds__(kBlendThreads)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
              uint32_t* __restrict__ err) {
     __shared__ __align__(128) ProjRecord sRec[2][kBatch];
+    __shared__ __align__(16) float4 sBox[kBatch];
     __shared__ __align__(8) uint64_t sBar[2];
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % bp.tilesX, ty = tile / bp.tilesX;
-    const uint32_t px = tx * kTile + (tid & 15u);
-    const uint32_t py = ty * kTile + (tid >> 4);
+    const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
     const bool inside = px < bp.width && py < bp.height;
     const uint2 range = ranges[tile];
     const uint32_t start = range.x, end = range.y;
@@ -163,9 +199,24 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
         }
         if (buf == 0) phase0 ^= 1u; else phase1 ^= 1u;
         const uint32_t cnt = min(kBatch, end - at);
-        if (!done) {
-            const ProjRecord* batch = sRec[buf];
+        const ProjRecord* batch = sRec[buf];
+        if (tid < cnt) sBox[tid] = cull_box(batch[tid]);
+        __syncthreads();
+        // The bounding box of this warp's pixels still blending.
+        const unsigned active = __ballot_sync(0xFFFFFFFFu, !done);
+        if (active != 0) {
+            const uint32_t big = 0xFFFFFFFFu;
+            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, done ? big : px);
+            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : px);
+            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, done ? big : py);
+            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : py);
+            const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
+            const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
             for (uint32_t j = 0; j < cnt; ++j) {
+                if ((j & 7u) == 0 && __all_sync(0xFFFFFFFFu, done)) break;
+                const float4 box = sBox[j];
+                if (box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0) continue;   // warp-uniform
+                if (done) continue;
                 const float4 screen = batch[j].screen;
                 const float4 conic = batch[j].conic;
                 const float dx = pxf - screen.x;
@@ -182,10 +233,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
                 depthSum = depthSum + weight * screen.z;
                 T = T * (1.0f - alpha);
                 if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
-                if (T < 1e-4f) {
-                    done = true;
-                    break;
-                }
+                if (T < 1e-4f) done = true;
             }
         }
         if (__syncthreads_and(done ? 1 : 0)) {
