@@ -208,6 +208,23 @@ int lrt_prefix_sum(lrt_rast* rast, const void* in, void* out, void* total, uint3
 int lrt_radix_sort(lrt_rast* rast, void* keys, void* values, uint32_t count, uint32_t key_bits,
                    uint32_t key_bytes, void* stream);
 
+/* The prefix sum above for callers that cannot allocate device memory: a
+ * plugin running inside a host application that owns every device allocation
+ * (and its budget), or a frame-critical path where cudaMalloc would
+ * synchronise the device. It takes no handle and allocates nothing: the
+ * caller passes input, output and total (device pointers), and the scan's
+ * look-back scratch is a fixed 128 KB array compiled into the library, which
+ * every GPU that loads the library holds until the process exits. Counts
+ * above LRT_PREFIX_SUM_NOALLOC_MAX are rejected with LRT_INVALID_ARGUMENT.
+ * The first call on each device looks up that array's device address (with
+ * the device current), so make the first call before any stream capture.
+ * All calls on a device share the array and clear it on their stream first;
+ * calls whose work overlaps on the GPU race on it. Blocks until done, like
+ * lrt_prefix_sum. No counterpart in the reference: its PrefixSum always
+ * allocates through its device. */
+#define LRT_PREFIX_SUM_NOALLOC_MAX (1u << 26)
+int lrt_prefix_sum_noalloc(const void* in, void* out, void* total, uint32_t count, void* stream);
+
 /* Raw 3DGS records (the PLY encoding: x y z, logit opacity, 3 log scales,
  * rot w x y z, 3 DC, rest coefficients all red then green then blue) to the
  * packed layout above, on the host. Invalid records (non-finite position or

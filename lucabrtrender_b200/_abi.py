@@ -36,8 +36,9 @@ STATUS_NAMES = {
 EXPORTS = (
     "lrt_abi_version", "lrt_rast_create", "lrt_rast_destroy", "lrt_rast_last_error", "lrt_rast_render",
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
-    "lrt_pack_splats", "lrt_math_eval",
+    "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc",
 )
+PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
 
 class Projection(C.Structure):
@@ -151,6 +152,7 @@ def load() -> C.CDLL:
     lib.lrt_pack_splats.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
     lib.lrt_math_eval.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    lib.lrt_prefix_sum_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     if lib.lrt_abi_version() != ABI_VERSION:
         raise RuntimeError(f"ABI version mismatch: library {lib.lrt_abi_version()}, bindings {ABI_VERSION}")
     _lib = lib
