@@ -250,21 +250,22 @@ def run_ours(args) -> None:
     # Algorithmic bytes per launch (per unit x units):
     #   blend:   ranges 8 B/tile + (8 B pair word + 48 B record) per pair + 20 B per pixel written
     #   sort:    per 8-bit pass 8 B read + 8 B written per pair, plus one 8 B/pair histogram read
-    #   project: 124 B per splat read (deg 3) + 48+16+4+4 B per slot written
+    #   project (fused with counts and emission): 124 B per splat read (deg 3),
+    #            48+16+4+4 B per slot written, 8 B per pair written
     bytes_blend = 8 * tiles + 56 * pairs + 20 * pixels
     bytes_sort = (passes * 16 + 8) * pairs
-    bytes_project = 124 * SPLATS + 72 * SPLATS
+    bytes_project = 124 * SPLATS + 72 * SPLATS + 8 * pairs
     peak, peak_kind = measured_peaks()
     kernels = {
         "blend": (stage["blend_ms"], bytes_blend),
         "pair sort + ranges": (stage["tile_sort_ms"], bytes_sort + 8 * pairs + 8 * tiles),
-        "project": (stage["project_ms"], bytes_project),
+        "project + counts + emit": (stage["project_ms"], bytes_project),
     }
     dom_name = max(kernels, key=lambda n: kernels[n][0])
     dom_ms, dom_bytes = kernels[dom_name]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     sort_gbs = bytes_sort / (stage["tile_sort_ms"] * 1e-3) / 1e9 if stage["tile_sort_ms"] > 0 else None
-    launches_per_frame = 1 + 1 + 1 + 1 + passes + 1 + 1   # project, scan, duplicate, histogram, passes, ranges, blend
+    launches_per_frame = 1 + 1 + passes + 1 + 1   # project+emit, histogram, digit passes, ranges, blend
 
     if rank == 0:
         cpu = None

@@ -138,9 +138,11 @@ typedef struct lrt_render_settings {
 } lrt_render_settings;
 
 /* FrameStats (TileRasterizer.h:120-126). Stage times are CUDA-event times on
- * the render stream when time_stages is set; total_ms is host wall time. The
- * depth order is folded into the pair sort's key, so that sort is reported
- * under tile_sort_ms (with ranges) and depth_sort_ms is 0. */
+ * the render stream when time_stages is set; total_ms is host wall time.
+ * Projection, the touched counts and pair emission are one kernel, reported
+ * as project_ms (counts_ms and emit_ms are 0); the depth order is folded into
+ * the pair sort's key, so that sort is reported under tile_sort_ms (with the
+ * ranges) and depth_sort_ms is 0. */
 typedef struct lrt_frame_stats {
     uint32_t splats, visible, pairs, reserved;
     double project_ms, depth_sort_ms, counts_ms, emit_ms, tile_sort_ms, blend_ms, total_ms;
@@ -181,8 +183,9 @@ const char* lrt_rast_last_error(const lrt_rast* rast);
 /* TileRasterizer::render(const Projection&, instances, settings, targets).
  * `stream` is a cudaStream_t (NULL: the legacy default stream). Instances are
  * concatenated into slots base + i in the order given; the slot breaks depth
- * ties. The call returns once the frame is enqueued and its counts are known
- * (it reads back the pair count, as the reference does). */
+ * ties. Like the reference's render (which ends with a blocking submit) the
+ * call returns when the frame is done; it reads back the counts and the
+ * device status once, at the end. */
 int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
                     const lrt_splat_instance* instances, uint32_t instance_count,
                     const lrt_render_settings* settings, lrt_targets* targets,

@@ -1,4 +1,4 @@
-// Stages (b) duplication, (d) tile ranges and (e) the front-to-back blend.
+// Stages (d) tile ranges and (e) the front-to-back blend.
 //
 // Pair word (64 bits, sorted on its key bits only):
 //     tile << (24 + slotBits) | depthKey24 << slotBits | slot
@@ -13,42 +13,9 @@
 namespace lrt {
 namespace {
 
-constexpr uint32_t kDupThreads = 256;
 constexpr uint32_t kBlendThreads = 256;
 constexpr uint32_t kBatch = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;
-
-// shaders/lrt/splat/splat_emit.slang:17-50, emitting in slot order.
-__global__ void __launch_bounds__(kDupThreads)
-duplicate_kernel(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* __restrict__ proj,
-                 const uint4* __restrict__ rects, const uint32_t* __restrict__ touched,
-                 const uint32_t* __restrict__ keys, const uint32_t* __restrict__ offsets, uint32_t slots,
-                 uint32_t slotBits, unsigned long long* __restrict__ pairs, uint32_t capacity,
-                 uint32_t* __restrict__ err) {
-    const uint32_t slot = blockIdx.x * kDupThreads + threadIdx.x;
-    if (slot >= slots) return;
-    const uint32_t expected = touched[slot];
-    if (expected == 0) return;
-    const uint32_t first = offsets[slot];
-    const float4 screen = proj[slot].screen;
-    const float4 conic = proj[slot].conic;
-    const uint4 rect = rects[slot];
-    const unsigned long long low = (static_cast<unsigned long long>(keys[slot]) << slotBits) | slot;
-    const uint32_t tileShift = 24 + slotBits;
-    uint32_t written = 0;
-    for (uint32_t ty = rect.y; ty <= rect.w && written < expected; ++ty) {
-        for (uint32_t tx = rect.x; tx <= rect.z && written < expected; ++tx) {
-            if (!tile_touched(width, height, screen.x, screen.y, conic.x, conic.y, conic.z, screen.w, tx, ty)) continue;
-            const uint32_t at = first + written;
-            if (at < capacity) {
-                pairs[at] = (static_cast<unsigned long long>(ty * tilesX + tx) << tileShift) | low;
-            } else {
-                atomicOr(err, kErrOverflow);
-            }
-            written += 1;
-        }
-    }
-}
 
 // shaders/lrt/splat/splat_ranges.slang:11-25 (after a zeroing memset,
 // splat_tiles_clear.slang:8-17).
@@ -258,17 +225,6 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
 }
 
 }  // namespace
-
-cudaError_t launch_duplicate(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* proj,
-                             const uint4* rects, const uint32_t* touched, const uint32_t* keys,
-                             const uint32_t* offsets, uint32_t slots, uint32_t slotBits, uint64_t* pairs,
-                             uint32_t capacity, uint32_t* err, cudaStream_t stream) {
-    if (slots == 0) return cudaSuccess;
-    duplicate_kernel<<<(slots + kDupThreads - 1) / kDupThreads, kDupThreads, 0, stream>>>(
-        width, height, tilesX, proj, rects, touched, keys, offsets, slots, slotBits,
-        reinterpret_cast<unsigned long long*>(pairs), capacity, err);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
                           uint2* ranges, uint32_t tiles, cudaStream_t stream) {

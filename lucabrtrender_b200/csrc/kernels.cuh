@@ -12,18 +12,21 @@ struct FrameParams;
 struct BlendParams;
 struct ProjRecord;
 
-cudaError_t launch_project(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
-                           ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys,
-                           uint32_t* visibleCount, cudaStream_t stream);
+// Projection fused with the touched counts, their prefix and the pair words.
+// counters: [0] visible (added to), [1] pairs (written by the frame's last
+// partition), [2] error bits. status: one zeroed word per 256-splat partition
+// of the frame; ticket: a zeroed counter per launch; partitionBase: this
+// launch's first partition in the frame; lastPartition: the frame's last.
+uint32_t project_partitions(uint32_t count);
+size_t project_status_bytes(uint32_t partitions);
+cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
+                                ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
+                                uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
+                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream);
 
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
                                   uint32_t* err, cudaStream_t stream);
-
-cudaError_t launch_duplicate(uint32_t width, uint32_t height, uint32_t tilesX, const ProjRecord* proj,
-                             const uint4* rects, const uint32_t* touched, const uint32_t* keys,
-                             const uint32_t* offsets, uint32_t slots, uint32_t slotBits, uint64_t* pairs,
-                             uint32_t capacity, uint32_t* err, cudaStream_t stream);
 
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,

@@ -1,20 +1,34 @@
-// Stage (a): per-splat projection.
+// Stages (a) and (b): per-splat projection, the touched-tile count, the
+// pairs' offsets and the pairs themselves, in one kernel.
 //
-// Restates shaders/lrt/splat/splat_project.slang:39-221 (the splat route;
-// relighting is not part of this path): SplatEdit fate, near/far cull, 3D
-// covariance from the smallest-three quaternion and f16 log-scales, EWA
+// Projection restates shaders/lrt/splat/splat_project.slang:39-221 (the splat
+// route; relighting is not part of this path): SplatEdit fate, near/far cull,
+// 3D covariance from the smallest-three quaternion and f16 log-scales, EWA
 // Jacobian clamped to 1.3x the frustum, Mip-Splatting 2D filter with the
 // opacity payback, conic and cut-off, tile rectangle, exact touched-tile
 // count, view-dependent colour from f16 spherical harmonics up to degree 3,
-// and the 24-bit depth key.
+// and the 24-bit depth key. The pairs are the reference's splat_emit
+// (shaders/lrt/splat/splat_emit.slang:17-50), written in slot order at
+// offsets that are the exclusive prefix of the touched counts
+// (TileRasterizer.cpp:383-438 computes the same with three scans and a
+// readback).
 //
-// B200 layout: one thread per splat, 256 per block. Positions and shape are
-// read as 16-byte vectors (coalesced). The block's harmonics rows (92 bytes a
-// splat at degree 3: not 16-byte aligned per splat, but 256 rows start on a
-// 16-byte boundary) are staged into shared memory by 16-byte cp.async copies
-// issued first, so they land while the geometry is computed.
+// B200 layout: one thread per splat, 256 per block; a block takes the next
+// 256 splats by atomic ticket. Positions and shape are read as 16-byte
+// vectors. The block's harmonics rows (92 bytes a splat at degree 3; 256 rows
+// start on a 16-byte boundary) are staged into shared memory by 16-byte
+// cp.async copies issued first, so they land while the geometry runs. A
+// splat's exact tile test runs per thread when its rectangle holds at most 16
+// tiles, and across its warp (32 tiles at a time, ballots) when larger; up to
+// 64 tiles the result is kept as a bitmask. The block's pair offsets come
+// from a block scan and a decoupled look-back over all partitions of the
+// frame (bounded waits). Pairs of masked splats are then written by the whole
+// block, one pair per thread per step, so writes are contiguous; larger
+// splats are written by their own warp with the tile test repeated.
 #include "kernels.cuh"
 #include "raster_common.cuh"
+
+#include <cuda/atomic>
 
 namespace lrt {
 namespace {
@@ -131,19 +145,81 @@ __device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t de
     return r;
 }
 
+constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
+constexpr uint32_t kMaskArea = 64;    // a touched-tile bitmask up to this many
+constexpr uint64_t kFlagAggregate = 1ull << 62;
+constexpr uint64_t kFlagInclusive = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sWarp, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= d) x += o;
+    }
+    if (lane == 31) sWarp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kProjectThreads / 32 ? sWarp[lane] : 0;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= d) w += o;
+        }
+        if (lane < kProjectThreads / 32) sWarp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp == 0 ? 0 : sWarp[warp - 1];
+    *total = sWarp[kProjectThreads / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+struct PairSink {
+    unsigned long long* pairs;
+    uint32_t capacity;
+    uint32_t* err;
+    __device__ __forceinline__ void put(uint64_t at, unsigned long long word) const {
+        if (at < capacity) {
+            pairs[at] = word;
+        } else {
+            atomicOr(err, kErrOverflow);
+        }
+    }
+};
+
 __global__ void __launch_bounds__(kProjectThreads)
-project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4* __restrict__ shape,
-               const uint32_t* __restrict__ sh, uint32_t stageWords, uint32_t shVector,
-               ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
-               uint32_t* __restrict__ keysOut, uint32_t* __restrict__ visibleCount) {
+project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const uint4* __restrict__ shape,
+                    const uint32_t* __restrict__ sh, uint32_t stageWords, uint32_t shVector,
+                    ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
+                    uint32_t* __restrict__ keysOut, uint32_t* __restrict__ counters, uint64_t* __restrict__ status,
+                    uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits,
+                    unsigned long long* __restrict__ pairs, uint32_t capacity) {
     extern __shared__ __align__(16) uint32_t shStage[];
+    __shared__ uint32_t sPart;
+    __shared__ uint32_t sScan[kProjectThreads / 32];
+    __shared__ uint32_t sStart[kProjectThreads + 1];       // block-relative pair offset of each splat
+    __shared__ uint32_t sSmallStart[kProjectThreads + 1];  // the same over masked splats only
+    __shared__ unsigned long long sMask[kProjectThreads];
+    __shared__ unsigned long long sLow[kProjectThreads];   // depth key << slotBits | slot
+    __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
+    __shared__ uint32_t sWidth[kProjectThreads];
+    __shared__ unsigned long long sBase;
+    uint32_t* err = counters + 2;
     const uint32_t tid = threadIdx.x;
-    const uint32_t blockStart = blockIdx.x * kProjectThreads;
+    const uint32_t lane = tid & 31u;
+    if (tid == 0) sPart = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t part = sPart;
+    const uint32_t blockStart = part * kProjectThreads;
     const uint32_t i = blockStart + tid;
     const bool inRange = i < f.count;
 
     // Harmonics of the whole block, in flight while the geometry runs.
-    if (stageWords != 0) {
+    if (stageWords != 0 && blockStart < f.count) {
         const uint32_t nBlock = min(kProjectThreads, f.count - blockStart);
         const uint32_t words = nBlock * f.shWords;
         const uint32_t* src = sh + static_cast<size_t>(blockStart) * f.shWords;
@@ -161,7 +237,6 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
     float3 t = p;
     float cx = 0.0f, cy = 0.0f, ca = 0.0f, cb = 0.0f, cc = 0.0f, alpha = 0.0f, cutoff = 0.0f;
     uint4 rect = make_uint4(1, 1, 0, 0);
-    uint32_t touched = 0;
     Fate fate{true, false, 0.0f};
     uint4 sw = make_uint4(0, 0, 0, 0);
     if (inRange) {
@@ -183,21 +258,10 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
             sy = (sy / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
             sz = (sz / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
             const float rest = sqrtf(fmaxf(0.0f, 1.0f - (sx * sx + sy * sy + sz * sz)));
-            float q[4];
-            {
-                const float small[3] = {sx, sy, sz};
-                uint32_t next = 0;
-#pragma unroll
-                for (uint32_t k = 0; k < 4; ++k) {
-                    if (k == largest) {
-                        q[k] = rest;
-                    } else {
-                        q[k] = small[next == 0 ? 0 : next == 1 ? 1 : 2];
-                        next += 1;
-                    }
-                }
-            }
-            const float x = q[0], y = q[1], z = q[2], w = q[3];
+            const float x = largest == 0 ? rest : sx;
+            const float y = largest == 1 ? rest : largest == 0 ? sx : sy;
+            const float z = largest == 2 ? rest : largest == 3 ? sz : sy;
+            const float w = largest == 3 ? rest : sz;
             const float r00 = 1.0f - 2.0f * (y * y + z * z), r01 = 2.0f * (x * y - w * z), r02 = 2.0f * (x * z + w * y);
             const float r10 = 2.0f * (x * y + w * z), r11 = 1.0f - 2.0f * (x * x + z * z), r12 = 2.0f * (y * z - w * x);
             const float r20 = 2.0f * (x * z - w * y), r21 = 2.0f * (y * z + w * x), r22 = 1.0f - 2.0f * (x * x + y * y);
@@ -273,26 +337,64 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
                     alive = !(rect.x > rect.z || rect.y > rect.w);
                 }
             }
-            if (alive) {
-                for (uint32_t ty = rect.y; ty <= rect.w; ++ty)
-                    for (uint32_t tx = rect.x; tx <= rect.z; ++tx)
-                        touched += tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, tx, ty) ? 1u : 0u;
-                alive = touched != 0;
+        }
+    }
+
+    // The exact touched count (splat_project.slang:148-160), row-major over
+    // the rectangle, with a bitmask of the touched tiles up to kMaskArea.
+    const uint32_t rw = alive ? rect.z - rect.x + 1 : 0;
+    const uint32_t area = alive ? rw * (rect.w - rect.y + 1) : 0;
+    uint32_t touched = 0;
+    unsigned long long mask = 0;
+    if (alive && area <= kSmallArea) {
+        for (uint32_t k = 0; k < area; ++k) {
+            const uint32_t tx = rect.x + k % rw, ty = rect.y + k / rw;
+            if (tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, tx, ty)) {
+                mask |= 1ull << k;
+                touched += 1;
             }
         }
     }
+    uint32_t big = __ballot_sync(0xFFFFFFFFu, alive && area > kSmallArea);
+    while (big != 0) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
+        const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
+        const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
+        const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
+        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
+        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
+        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+        uint32_t count = 0;
+        unsigned long long m = 0;
+        for (uint32_t base = 0; base < sArea; base += 32) {
+            const uint32_t k = base + lane;
+            const bool hit = k < sArea &&
+                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + k % sW, sY + k / sW);
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+            count += static_cast<uint32_t>(__popc(bal));
+            if (base < kMaskArea) m |= static_cast<unsigned long long>(bal) << base;
+        }
+        if (lane == static_cast<uint32_t>(src)) {
+            touched = count;
+            mask = sArea <= kMaskArea ? m : 0ull;
+        }
+    }
+    alive = alive && touched != 0;
+    if (!alive) touched = 0;
 
     if (stageWords != 0) cp_async_wait_all();
     __syncthreads();
 
     const uint32_t slot = f.base + i;
+    uint32_t key = 0x00FFFFFFu;
     if (inRange) {
         if (alive) {
             const float3 base = make_float3(high_half(sw.z), low_half(sw.w), high_half(sw.w));
             const uint32_t rpc = f.restPerColour;
             const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
             const uint32_t degree = min(stored, f.shLimit);
-            float3 colour = base;
             float3 restc = make_float3(0.0f, 0.0f, 0.0f);
             if (degree > 0) {
                 const float dx = p.x - f.eye[0], dy = p.y - f.eye[1], dz = p.z - f.eye[2];
@@ -300,8 +402,8 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
                 const float3 dir = make_float3(dx / l, dy / l, dz / l);
                 restc = evaluate_rest(shStage + tid * f.shWords, degree, dir);
             }
-            colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
-                                 fmaxf(base.z + restc.z, 0.0f));
+            float3 colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
+                                        fmaxf(base.z + restc.z, 0.0f));
             if (fate.graded) colour = edit_grade(f.edit, colour);
             ProjRecord rec;
             rec.screen = make_float4(cx, cy, t.z, cutoff);
@@ -309,8 +411,7 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
             rec.colour = make_float4(colour.x, colour.y, colour.z, 0.0f);
             proj[slot] = rec;
             rects[slot] = rect;
-            touchedOut[slot] = touched;
-            keysOut[slot] = float_bits(t.z) >> 7;
+            key = float_bits(t.z) >> 7;
         } else {
             // splat_project.slang:39-49, plus a zeroed record
             ProjRecord rec;
@@ -319,19 +420,120 @@ project_kernel(FrameParams f, const float4* __restrict__ positions, const uint4*
             rec.colour = rec.screen;
             proj[slot] = rec;
             rects[slot] = make_uint4(1, 1, 0, 0);
-            touchedOut[slot] = 0;
-            keysOut[slot] = 0x00FFFFFFu;
         }
+        touchedOut[slot] = touched;
+        keysOut[slot] = key;
     }
     const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, inRange && alive);
-    if ((tid & 31u) == 0 && ballot != 0) atomicAdd(visibleCount, static_cast<uint32_t>(__popc(ballot)));
+    if (lane == 0 && ballot != 0) atomicAdd(counters, static_cast<uint32_t>(__popc(ballot)));
+
+    // Offsets: block scan, then decoupled look-back over the frame's partitions.
+    const bool masked = touched != 0 && area <= kMaskArea;
+    uint32_t blockTotal = 0, smallTotal = 0;
+    const uint32_t start = block_exclusive_scan(touched, sScan, &blockTotal);
+    const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
+    sStart[tid] = start;
+    sSmallStart[tid] = smallStart;
+    sMask[tid] = mask;
+    sLow[tid] = (static_cast<unsigned long long>(key) << slotBits) | slot;
+    sRect[tid] = rect.x | (rect.y << 16);
+    sWidth[tid] = rw;
+    if (tid == 0) {
+        sStart[kProjectThreads] = blockTotal;
+        sSmallStart[kProjectThreads] = smallTotal;
+        const uint32_t g = partitionBase + part;
+        cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
+        uint64_t prefix = 0;
+        if (g == 0) {
+            mine.store(kFlagInclusive | blockTotal, cuda::memory_order_relaxed);
+        } else {
+            mine.store(kFlagAggregate | blockTotal, cuda::memory_order_relaxed);
+            int64_t q = static_cast<int64_t>(g) - 1;
+            uint32_t spins = 0;
+            while (q >= 0) {
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[q]);
+                const uint64_t word = sref.load(cuda::memory_order_relaxed);
+                if ((word & ~kValueMask) == 0) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, kErrTimeout);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                prefix += word & kValueMask;
+                if (word & kFlagInclusive) break;
+                --q;
+            }
+            mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
+        }
+        sBase = prefix;
+        if (g == lastPartition) {
+            const uint64_t all = prefix + blockTotal;
+            if (all > 0xFFFFFFFFull) atomicOr(err, kErrTooManyPairs);
+            counters[1] = static_cast<uint32_t>(all);
+        }
+    }
+    __syncthreads();
+    const unsigned long long blockBase = sBase;
+    const PairSink sink{pairs, capacity, err};
+    const uint32_t tileShift = 24 + slotBits;
+
+    // Masked splats: the whole block writes their pairs, one per thread per step.
+    for (uint32_t j = tid; j < smallTotal; j += kProjectThreads) {
+        uint32_t lo = 0, hi = kProjectThreads;   // the splat s with sSmallStart[s] <= j < sSmallStart[s + 1]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sSmallStart[mid] <= j) lo = mid; else hi = mid;
+        }
+        const uint32_t s = lo;
+        uint32_t r = j - sSmallStart[s];
+        unsigned long long m = sMask[s];
+        for (; r > 0; --r) m &= m - 1;   // drop the r lowest set bits
+        const uint32_t bit = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
+        const uint32_t w = sWidth[s];
+        const uint32_t tx = (sRect[s] & 0xFFFFu) + bit % w;
+        const uint32_t ty = (sRect[s] >> 16) + bit / w;
+        sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
+                 (static_cast<unsigned long long>(ty * f.tilesX + tx) << tileShift) | sLow[s]);
+    }
+    // Larger splats: their warp repeats the tile test 32 tiles at a time.
+    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && area > kMaskArea);
+    while (large != 0) {
+        const int src = __ffs(large) - 1;
+        large &= large - 1;
+        const uint32_t s = (tid & ~31u) + static_cast<uint32_t>(src);
+        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
+        const uint32_t sW = sWidth[s];
+        const uint32_t sX = sRect[s] & 0xFFFFu, sY = sRect[s] >> 16;
+        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
+        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
+        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+        unsigned long long at = blockBase + sStart[s];
+        const unsigned long long low = sLow[s];
+        for (uint32_t base = 0; base < sArea; base += 32) {
+            const uint32_t k = base + lane;
+            const uint32_t tx = sX + k % sW, ty = sY + k / sW;
+            const bool hit = k < sArea && tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, tx, ty);
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+            if (hit) {
+                sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
+                         (static_cast<unsigned long long>(ty * f.tilesX + tx) << tileShift) | low);
+            }
+            at += static_cast<uint32_t>(__popc(bal));
+        }
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_project(const FrameParams& f, const float4* positions, const uint4* shape,
-                           const uint32_t* sh, ProjRecord* proj, uint4* rects, uint32_t* touched,
-                           uint32_t* keys, uint32_t* visibleCount, cudaStream_t stream) {
+size_t project_status_bytes(uint32_t partitions) { return size_t{partitions} * sizeof(uint64_t); }
+uint32_t project_partitions(uint32_t count) { return (count + kProjectThreads - 1) / kProjectThreads; }
+
+cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
+                                ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
+                                uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
+                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
@@ -339,14 +541,13 @@ cudaError_t launch_project(const FrameParams& f, const float4* positions, const 
     const uint32_t stageWords = stage ? f.shWords : 0u;
     const uint32_t shVector = (reinterpret_cast<uintptr_t>(sh) & 15u) == 0 ? 1u : 0u;
     const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-    }
-    const uint32_t blocks = (f.count + kProjectThreads - 1) / kProjectThreads;
-    project_kernel<<<blocks, kProjectThreads, smem, stream>>>(f, positions, shape, sh, stageWords, shVector, proj,
-                                                             rects, touched, keys, visibleCount);
+    cudaError_t e = cudaFuncSetAttribute(project_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(std::max<size_t>(smem, 1)));
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = project_partitions(f.count);
+    project_emit_kernel<<<blocks, kProjectThreads, smem, stream>>>(
+        f, positions, shape, sh, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket,
+        partitionBase, lastPartition, slotBits, reinterpret_cast<unsigned long long*>(pairs), capacity);
     return cudaGetLastError();
 }
 

@@ -2,10 +2,14 @@
 // include/lrt_raster.h). Host orchestration of one frame, in the reference's
 // order (modules/render/src/TileRasterizer.cpp:188-484):
 //
-//   project (per instance)  -> scan of touched counts (duplication offsets)
-//   -> one readback of the visible and pair counts -> duplicate pairs
+//   project + count + emit (one kernel per instance, offsets by look-back)
 //   -> onesweep sort of the pairs' (tile | depth) key bits -> tile ranges
-//   -> blend
+//   -> blend -> one readback of the visible and pair counts and the status
+//
+// The reference reads the counts back in the middle of the frame to size the
+// pair buffers; here the pairs go into a buffer sized before the frame, and a
+// frame that reports more pairs than it held is drawn again with room for
+// them (once per growth, so steady frames never repeat).
 //
 // Buffers belong to the handle and grow by 1.5x (TileRasterizer.cpp:26-32);
 // targets and clouds belong to the caller. Stage times come from CUDA events
@@ -27,10 +31,10 @@ struct DeviceBuffer {
 struct lrt_rast {
     int device = 0;
     std::string error;
-    DeviceBuffer proj, rects, touched, keys, offsets;   // per slot
+    DeviceBuffer proj, rects, touched, keys;            // per slot
     DeviceBuffer pairs, pairsAlt;                        // per pair
     DeviceBuffer ranges;                                 // per tile
-    DeviceBuffer scanScratch, sortScratch;
+    DeviceBuffer scanScratch, sortScratch;               // look-back status words, tickets
     DeviceBuffer counters;                               // visible, pairs, err, algo err
     DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers
     uint32_t* hostCounters = nullptr;                    // pinned
@@ -181,7 +185,7 @@ int lrt_rast_create(lrt_rast** out, int device) {
 void lrt_rast_destroy(lrt_rast* r) {
     if (r == nullptr) return;
     DeviceScope scope(r->device);
-    for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->offsets, &r->pairs, &r->pairsAlt,
+    for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt})
         release(*b);
@@ -206,6 +210,8 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         targets->depth == nullptr)
         return fail(r, LRT_INVALID_ARGUMENT, "the targets are not the frame's size");
     uint64_t total = 0;
+    uint64_t partitions = 0;
+    uint32_t launches = 0;
     for (uint32_t k = 0; k < n; ++k) {
         const lrt_gpu_splats* c = instances[k].splats;
         if (c == nullptr || c->count == 0) continue;
@@ -215,6 +221,8 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         if (c->rest_per_colour > 0 && c->sh_words < (c->rest_per_colour * 3 + 1) / 2)
             return fail(r, LRT_INVALID_ARGUMENT, "sh_words too small for rest_per_colour");
         total += c->count;
+        partitions += lrt::project_partitions(c->count);
+        launches += 1;
     }
     if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one frame");
     DeviceScope scope(r->device);
@@ -236,139 +244,137 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         LRT_CUDA(r, ensure(r->rects, size_t{cap} * 16), "tile rects");
         LRT_CUDA(r, ensure(r->touched, size_t{cap} * 4), "touched counts");
         LRT_CUDA(r, ensure(r->keys, size_t{cap} * 4), "depth keys");
-        LRT_CUDA(r, ensure(r->offsets, size_t{cap} * 4), "pair offsets");
-        LRT_CUDA(r, ensure(r->scanScratch, lrt::scan_scratch_bytes(cap)), "scan scratch");
         r->splatCap = cap;
     }
+    const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches} * 4;
+    LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
         LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
         r->tileCap = tiles;
     }
+    // Pairs are emitted on the device into a buffer of the capacity known
+    // before the frame; a frame that emits more is redrawn once with the
+    // buffers grown to the count it reported.
+    if (r->pairCap == 0) r->pairCap = std::max<uint32_t>(1024, static_cast<uint32_t>(std::min<uint64_t>(
+                                                                   uint64_t{slots} * 4, 0xFFFFFFFFull)));
     uint32_t* counters = static_cast<uint32_t*>(r->counters.ptr);
     uint32_t* err = counters + 2;
-    LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
+    uint64_t* status = static_cast<uint64_t*>(r->scanScratch.ptr);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(static_cast<char*>(r->scanScratch.ptr) +
+                                                    lrt::project_status_bytes(static_cast<uint32_t>(partitions)));
+    const uint32_t lastPartition = partitions > 0 ? static_cast<uint32_t>(partitions - 1) : 0u;
+    uint32_t visible = 0, pairs = 0, statusBits = 0;
+    const uint64_t* sorted = nullptr;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        LRT_CUDA(r, ensure(r->pairs, size_t{r->pairCap} * 8), "pairs");
+        LRT_CUDA(r, ensure(r->pairsAlt, size_t{r->pairCap} * 8), "pairs");
+        LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(r->pairCap, keyBits)), "sort scratch");
+        LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
+        LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, stream), "projection scratch");
+        uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
 
-    // --- project -----------------------------------------------------------
-    LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
-    uint32_t base = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        const lrt_splat_instance& inst = instances[k];
-        const lrt_gpu_splats* c = inst.splats;
-        if (c == nullptr || c->count == 0) continue;
-        FrameParams f{};
-        f.width = s->width;
-        f.height = s->height;
-        f.tilesX = tilesX;
-        f.tilesY = tilesY;
-        f.focalX = static_cast<float>(pr->focal_x);
-        f.focalY = static_cast<float>(pr->focal_y);
-        f.centreX = static_cast<float>(pr->centre_x);
-        f.centreY = static_cast<float>(pr->centre_y);
-        f.nearZ = static_cast<float>(pr->near_z);
-        f.farZ = static_cast<float>(pr->far_z);
-        f.ortho = pr->orthographic ? 1u : 0u;
-        f.antialias = s->antialias ? 1u : 0u;
-        const M4 ov = mul4(pr->world_to_view, inst.object_to_world);
-        for (int row = 0; row < 3; ++row)
-            for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
-        double eye[3];
-        eye_in_object(inst.object_to_world, pr->eye_world, eye);
-        for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
-        f.count = c->count;
-        f.base = base;
-        f.restPerColour = c->rest_per_colour;
-        f.shWords = c->sh_words;
-        f.shLimit = s->max_sh_degree;
-        const lrt_splat_edit& e = inst.edit;
-        f.edit.active = e.active;
-        f.edit.shape = e.shape;
-        f.edit.mode = e.mode;
-        f.edit.invert = e.invert;
-        for (int a = 0; a < 3; ++a) {
-            f.edit.centre[a] = e.centre[a];
-            f.edit.size[a] = e.size[a];
-            f.edit.tint[a] = e.tint[a];
+        // --- project, count, emit ------------------------------------------
+        LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
+        uint32_t base = 0, partitionBase = 0, launch = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const lrt_splat_instance& inst = instances[k];
+            const lrt_gpu_splats* c = inst.splats;
+            if (c == nullptr || c->count == 0) continue;
+            FrameParams f{};
+            f.width = s->width;
+            f.height = s->height;
+            f.tilesX = tilesX;
+            f.tilesY = tilesY;
+            f.focalX = static_cast<float>(pr->focal_x);
+            f.focalY = static_cast<float>(pr->focal_y);
+            f.centreX = static_cast<float>(pr->centre_x);
+            f.centreY = static_cast<float>(pr->centre_y);
+            f.nearZ = static_cast<float>(pr->near_z);
+            f.farZ = static_cast<float>(pr->far_z);
+            f.ortho = pr->orthographic ? 1u : 0u;
+            f.antialias = s->antialias ? 1u : 0u;
+            const M4 ov = mul4(pr->world_to_view, inst.object_to_world);
+            for (int row = 0; row < 3; ++row)
+                for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
+            double eye[3];
+            eye_in_object(inst.object_to_world, pr->eye_world, eye);
+            for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
+            f.count = c->count;
+            f.base = base;
+            f.restPerColour = c->rest_per_colour;
+            f.shWords = c->sh_words;
+            f.shLimit = s->max_sh_degree;
+            const lrt_splat_edit& e = inst.edit;
+            f.edit.active = e.active;
+            f.edit.shape = e.shape;
+            f.edit.mode = e.mode;
+            f.edit.invert = e.invert;
+            for (int a = 0; a < 3; ++a) {
+                f.edit.centre[a] = e.centre[a];
+                f.edit.size[a] = e.size[a];
+                f.edit.tint[a] = e.tint[a];
+            }
+            f.edit.saturation = e.saturation;
+            f.edit.brightness = e.brightness;
+            f.edit.opacity = e.opacity;
+            f.edit.minOpacity = e.min_opacity;
+            f.edit.maxScale = e.max_scale;
+            LRT_CUDA(r,
+                     lrt::launch_project_emit(
+                         f, static_cast<const float4*>(c->positions), static_cast<const uint4*>(c->shape),
+                         static_cast<const uint32_t*>(c->sh), static_cast<ProjRecord*>(r->proj.ptr),
+                         static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                         static_cast<uint32_t*>(r->keys.ptr), counters, status, tickets + launch, partitionBase,
+                         lastPartition, slotBits, pairBuf, r->pairCap, stream),
+                     "project");
+            base += c->count;
+            partitionBase += lrt::project_partitions(c->count);
+            launch += 1;
         }
-        f.edit.saturation = e.saturation;
-        f.edit.brightness = e.brightness;
-        f.edit.opacity = e.opacity;
-        f.edit.minOpacity = e.min_opacity;
-        f.edit.maxScale = e.max_scale;
+        LRT_CUDA(r, cudaEventRecord(r->ev[1], stream), "event");
+
+        // --- sort + ranges ----------------------------------------------------
+        bool inAlt = false;
         LRT_CUDA(r,
-                 lrt::launch_project(f, static_cast<const float4*>(c->positions), static_cast<const uint4*>(c->shape),
-                                     static_cast<const uint32_t*>(c->sh), static_cast<ProjRecord*>(r->proj.ptr),
-                                     static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                                     static_cast<uint32_t*>(r->keys.ptr), counters, stream),
-                 "project");
-        base += c->count;
+                 lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), nullptr, nullptr,
+                                      counters + 1, r->pairCap, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt,
+                                      stream),
+                 "pair sort");
+        sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
+        LRT_CUDA(r,
+                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + slotBits,
+                                    static_cast<uint2*>(r->ranges.ptr), tiles, stream),
+                 "ranges");
+        LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
+
+        // --- blend --------------------------------------------------------------
+        BlendParams bp{};
+        bp.width = s->width;
+        bp.height = s->height;
+        bp.tilesX = tilesX;
+        bp.tilesY = tilesY;
+        bp.slotBits = slotBits;
+        bp.tileShift = 24 + slotBits;
+        bp.depthMode = s->depth_mode;
+        bp.linearise = s->linearise ? 1u : 0u;
+        bp.depthThreshold = s->depth_threshold;
+        for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
+        LRT_CUDA(r,
+                 lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
+                                   static_cast<ProjRecord*>(r->proj.ptr), static_cast<float4*>(targets->colour),
+                                   static_cast<float*>(targets->depth), err, stream),
+                 "blend");
+        LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
+        LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "readback");
+        LRT_CUDA(r, cudaStreamSynchronize(stream), "frame");
+        visible = r->hostCounters[0];
+        pairs = r->hostCounters[1];
+        statusBits = r->hostCounters[2];
+        if (statusBits & lrt::kErrTooManyPairs) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pairs in one frame");
+        if (pairs <= r->pairCap) break;
+        r->pairCap = grow(r->pairCap, pairs);   // redraw with room for every pair
+        statusBits &= ~lrt::kErrOverflow;
     }
-    LRT_CUDA(r, cudaEventRecord(r->ev[1], stream), "event");
-
-    // --- counts: duplication offsets and the pair total ---------------------
-    LRT_CUDA(r,
-             lrt::launch_exclusive_scan(static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->offsets.ptr),
-                                        counters + 1, slots, r->scanScratch.ptr, err, stream),
-             "scan");
-    LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
-    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "count readback");
-    LRT_CUDA(r, cudaStreamSynchronize(stream), "count readback");
-    const uint32_t visible = r->hostCounters[0];
-    const uint32_t pairs = r->hostCounters[1];
-    if (r->hostCounters[2] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "prefix sum look-back gave up");
-    if (r->hostCounters[2] & lrt::kErrTooManyPairs) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pairs in one frame");
-
-    if (pairs > r->pairCap) {
-        const uint32_t cap = grow(r->pairCap, pairs);
-        LRT_CUDA(r, ensure(r->pairs, size_t{cap} * 8), "pairs");
-        LRT_CUDA(r, ensure(r->pairsAlt, size_t{cap} * 8), "pairs");
-        r->pairCap = cap;
-    }
-    LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(std::max(pairs, 1u), keyBits)), "sort scratch");
-
-    // --- emit ---------------------------------------------------------------
-    LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
-    uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
-    LRT_CUDA(r,
-             lrt::launch_duplicate(s->width, s->height, tilesX, static_cast<ProjRecord*>(r->proj.ptr),
-                                   static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                                   static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->offsets.ptr), slots,
-                                   slotBits, pairBuf, r->pairCap, err, stream),
-             "duplicate");
-    LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
-
-    // --- sort + ranges ------------------------------------------------------
-    bool inAlt = false;
-    LRT_CUDA(r,
-             lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), nullptr, nullptr, counters + 1,
-                                  pairs, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt, stream),
-             "pair sort");
-    const uint64_t* sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
-    LRT_CUDA(r,
-             lrt::launch_ranges(sorted, counters + 1, pairs, 24 + slotBits, static_cast<uint2*>(r->ranges.ptr), tiles,
-                                stream),
-             "ranges");
-    LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
-
-    // --- blend --------------------------------------------------------------
-    BlendParams bp{};
-    bp.width = s->width;
-    bp.height = s->height;
-    bp.tilesX = tilesX;
-    bp.tilesY = tilesY;
-    bp.slotBits = slotBits;
-    bp.tileShift = 24 + slotBits;
-    bp.depthMode = s->depth_mode;
-    bp.linearise = s->linearise ? 1u : 0u;
-    bp.depthThreshold = s->depth_threshold;
-    for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
-    LRT_CUDA(r,
-             lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted, static_cast<ProjRecord*>(r->proj.ptr),
-                               static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth), err,
-                               stream),
-             "blend");
-    LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
-    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 4, err, 4, cudaMemcpyDeviceToHost, stream), "status readback");
-    LRT_CUDA(r, cudaStreamSynchronize(stream), "frame");
 
     r->debug.proj = r->proj.ptr;
     r->debug.rects = r->rects.ptr;
@@ -384,7 +390,6 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
     r->debug.tile_bits = tileBits;
     r->debug.visible = visible;
 
-    const uint32_t status = r->hostCounters[4];
     if (stats != nullptr) {
         std::memset(stats, 0, sizeof(*stats));
         stats->splats = slots;
@@ -392,16 +397,14 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         stats->pairs = pairs;
         if (s->time_stages) {
             stats->project_ms = event_ms(r->ev[0], r->ev[1]);
-            stats->counts_ms = event_ms(r->ev[1], r->ev[2]);
-            stats->emit_ms = event_ms(r->ev[3], r->ev[4]);
-            stats->tile_sort_ms = event_ms(r->ev[4], r->ev[5]);
-            stats->blend_ms = event_ms(r->ev[5], r->ev[6]);
+            stats->tile_sort_ms = event_ms(r->ev[1], r->ev[2]);
+            stats->blend_ms = event_ms(r->ev[2], r->ev[3]);
         }
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - frameStart).count();
     }
-    if (status & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
-    if (status & lrt::kErrOverflow) return fail(r, LRT_OVERFLOW, "pair capacity exceeded");
+    if (statusBits & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+    if (statusBits & lrt::kErrOverflow || pairs > r->pairCap) return fail(r, LRT_OVERFLOW, "pair capacity exceeded");
     return LRT_OK;
 }
 
