@@ -169,9 +169,12 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
         const ProjRecord* batch = sRec[buf];
         if (tid < cnt) sBox[tid] = cull_box(batch[tid]);
         __syncthreads();
-        // The bounding box of this warp's pixels still blending.
-        const unsigned active = __ballot_sync(0xFFFFFFFFu, !done);
-        if (active != 0) {
+        // Records in chunks of 32: each lane tests one record's box against the
+        // bounding box of this warp's pixels still blending, and the warp then
+        // walks the ballot's set bits in record order.
+        for (uint32_t c = 0; c < cnt; c += 32) {
+            const unsigned active = __ballot_sync(0xFFFFFFFFu, !done);
+            if (active == 0) break;
             const uint32_t big = 0xFFFFFFFFu;
             const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, done ? big : px);
             const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : px);
@@ -179,10 +182,15 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
             const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : py);
             const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
             const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
-            for (uint32_t j = 0; j < cnt; ++j) {
-                if ((j & 7u) == 0 && __all_sync(0xFFFFFFFFu, done)) break;
-                const float4 box = sBox[j];
-                if (box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0) continue;   // warp-uniform
+            bool overlap = false;
+            if (c + lane < cnt) {
+                const float4 box = sBox[c + lane];
+                overlap = !(box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0);
+            }
+            uint32_t todo = __ballot_sync(0xFFFFFFFFu, overlap);
+            while (todo != 0) {
+                const uint32_t j = c + static_cast<uint32_t>(__ffs(todo)) - 1u;
+                todo &= todo - 1u;
                 if (done) continue;
                 const float4 screen = batch[j].screen;
                 const float4 conic = batch[j].conic;
