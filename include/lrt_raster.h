@@ -199,6 +199,51 @@ int lrt_camera_looking_at(const double eye[3], const double target[3], const dou
 int lrt_projection_for(const lrt_camera* camera, uint32_t width, uint32_t height,
                        lrt_projection* out);
 
+/* Differentiable parameters of one cloud for the training path (device
+ * pointers; fp32 unless noted): means [n][3], log_scales [n][3], quats [n][4]
+ * as (w, x, y, z), normalised in the forward (16-byte aligned),
+ * opacity_logits [n], sh [n][16][3] fp16 (DC first, then the 15 rest
+ * coefficients, rgb per basis; 16-byte aligned). The forward is the plain
+ * forward with scale exp(log_scale), opacity sigmoid(logit) and base colour
+ * 0.5 + SH0 * DC, without the packed layout's quantisation. No reference
+ * counterpart: the reference renders only. */
+typedef struct lrt_train_params {
+    uint32_t count;
+    uint32_t reserved;
+    const void* means;
+    const void* log_scales;
+    const void* quats;
+    const void* opacity_logits;
+    const void* sh;
+} lrt_train_params;
+
+/* Gradients of the same shapes (fp32 throughout; the SH gradient is fp32
+ * over the fp16 coefficients). Written, not accumulated. */
+typedef struct lrt_train_grads {
+    void* means;
+    void* log_scales;
+    void* quats;
+    void* opacity_logits;
+    void* sh;
+} lrt_train_grads;
+
+/* The training forward: renders `params` (one cloud in world space) like
+ * lrt_rast_render and keeps on the handle what lrt_rast_train_backward needs.
+ * The parameter buffers must stay unchanged until the backward. */
+int lrt_rast_train_forward(lrt_rast* rast, const lrt_projection* projection, const lrt_train_params* params,
+                           const lrt_render_settings* settings, lrt_targets* targets, lrt_frame_stats* stats,
+                           void* stream);
+/* The backward of the last lrt_rast_train_forward on this handle (no other
+ * render in between): grad_colour is dL/d(colour) as float4 [height][width]
+ * (device); gradients of the parameters are written to `grads`. A
+ * reverse-order re-blend per pixel, per-pair partials written at each pair's
+ * emit index, then a per-splat ordered sum and the projection's chain rule:
+ * no atomics. */
+int lrt_rast_train_backward(lrt_rast* rast, const void* grad_colour, lrt_train_grads* grads, void* stream);
+/* CUDA-event times of the last backward: the blend backward and the
+ * per-splat reduction + projection backward. */
+int lrt_rast_backward_times(const lrt_rast* rast, double* blend_ms, double* project_ms);
+
 /* PrefixSum::apply: exclusive scan of `count` uint32 at `in` into `out`, the
  * sum into `total` (all device pointers; `out` may alias `in`). Single pass,
  * decoupled look-back; scratch is the handle's. */

@@ -8,9 +8,10 @@ from .camera import Camera, Lens, Projection, projection_for, square_pixel_camer
 from .raster import (Depth, EditMode, EditShape, FrameStats, RenderSettings, RenderTargets, SplatEdit,
                      SplatInstance, TileRasterizer, math_eval)
 from .scene import CloudLoader, GpuSplats, PackedSplats, pack_splats, synthetic_records, to_device
+from .train import rasterize
 
 __all__ = [
     "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
     "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
-    "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device",
+    "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
 ]

@@ -36,7 +36,8 @@ STATUS_NAMES = {
 EXPORTS = (
     "lrt_abi_version", "lrt_rast_create", "lrt_rast_destroy", "lrt_rast_last_error", "lrt_rast_render",
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
-    "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc",
+    "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
+    "lrt_rast_train_backward", "lrt_rast_backward_times",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -121,6 +122,21 @@ class DebugView(C.Structure):
     ]
 
 
+class TrainParams(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint32), ("reserved", C.c_uint32),
+        ("means", C.c_void_p), ("log_scales", C.c_void_p), ("quats", C.c_void_p),
+        ("opacity_logits", C.c_void_p), ("sh", C.c_void_p),
+    ]
+
+
+class TrainGrads(C.Structure):
+    _fields_ = [
+        ("means", C.c_void_p), ("log_scales", C.c_void_p), ("quats", C.c_void_p),
+        ("opacity_logits", C.c_void_p), ("sh", C.c_void_p),
+    ]
+
+
 _lib = None
 
 
@@ -153,6 +169,11 @@ def load() -> C.CDLL:
                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
     lib.lrt_math_eval.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     lib.lrt_prefix_sum_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    lib.lrt_rast_train_forward.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(TrainParams),
+                                           C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
+                                           C.POINTER(FrameStatsStruct), C.c_void_p]
+    lib.lrt_rast_train_backward.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TrainGrads), C.c_void_p]
+    lib.lrt_rast_backward_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if lib.lrt_abi_version() != ABI_VERSION:
         raise RuntimeError(f"ABI version mismatch: library {lib.lrt_abi_version()}, bindings {ABI_VERSION}")
     _lib = lib

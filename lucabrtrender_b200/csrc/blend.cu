@@ -111,10 +111,14 @@ __device__ __forceinline__ float4 cull_box(const ProjRecord& rec) {
 // reference's loop unchanged over the records it is given, so it stops at
 // T < 1e-4 exactly as the reference does; a warp leaves a batch when all its
 // pixels have stopped, and the block stops when every pixel has.
+// kTrain: also keep, per pixel, the blended colour before linearising with
+// the final transmittance, and one past the last pair that contributed --
+// what the backward pass re-blends from.
+template <bool kTrain>
 __global__ void __launch_bounds__(kBlendThreads)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
-             uint32_t* __restrict__ err) {
+             float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
     __shared__ __align__(128) ProjRecord sRec[2][kBatch];
     __shared__ __align__(16) float4 sBox[kBatch];
     __shared__ __align__(8) uint64_t sBar[2];
@@ -152,6 +156,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     float depthSum = 0.0f;
     float depthAt = -1.0f;
     bool done = !inside;
+    uint32_t last = start;
     uint32_t phase0 = 0, phase1 = 0;
     if (start < end) issue(0, start);
     uint32_t k = 0;
@@ -208,6 +213,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
                 depthSum = depthSum + weight * screen.z;
                 T = T * (1.0f - alpha);
                 if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
+                if (kTrain) last = at + j + 1;
                 if (T < 1e-4f) done = true;
             }
         }
@@ -230,6 +236,195 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     const size_t pix = static_cast<size_t>(py) * bp.width + px;
     colourOut[pix] = make_float4(lr + T * bp.bg[0], lg + T * bp.bg[1], lb + T * bp.bg[2], coverage + T * bp.bg[3]);
     depthOut[pix] = bp.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f) : fmaxf(depthAt, 0.0f);
+    if (kTrain) {
+        pixState[pix] = make_float4(r, g, b, T);
+        pixLast[pix] = last;
+    }
+}
+
+// d/du of the sRGB-to-linear curve (color.slang:7-10): 0 below zero, 1/12.92
+// on the linear segment, 2.4/1.055 ((u + 0.055)/1.055)^1.4 above it.
+__device__ __forceinline__ float srgb_to_linear_slope(float c) {
+    if (!(c > 0.0f)) return 0.0f;
+    if (c <= 0.04045f) return 1.0f / 12.92f;
+    return 2.4f / 1.055f * lrt_pow((c + 0.055f) / 1.055f, 1.4f);
+}
+
+constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// The backward of blend_kernel<true>: per pixel, the reference's loop run
+// backwards from the last pair that contributed, rebuilding each pair's
+// transmittance from the final one (T_i = T_{i+1} / (1 - alpha_i)) rather
+// than storing it, with B the colour behind the pair:
+//   dL/dc_i     = dL/drgb * T_i alpha_i
+//   dL/dalpha_i = T_i sum_k dL/drgb_k (c_ik - B_k) - dL/dT * T / (1 - alpha_i)
+//   B          <- alpha_i c_i + (1 - alpha_i) B
+// then through alpha = min(0.99, alpha0 exp(-power / 2)) (no gradient when
+// clamped) and power = a dx^2 + 2 b dx dy + c dy^2. A pair's nine values are
+// summed over the warp's pixels by shuffles, over the block's warps in
+// warp order through shared memory, and written at the pair's emit index: a
+// splat's pairs are contiguous there, so a per-splat sum needs no atomics.
+__global__ void __launch_bounds__(kBlendThreads)
+blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+                      const uint32_t* __restrict__ emit, const ProjRecord* __restrict__ proj,
+                      const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
+                      const float4* __restrict__ gradColour, float* __restrict__ partials) {
+    constexpr uint32_t kB = 128;
+    __shared__ __align__(16) ProjRecord sRec[kB];
+    __shared__ __align__(16) float4 sBox[kB];
+    __shared__ uint32_t sEmit[kB];
+    __shared__ float sPart[kBlendThreads / 32][kB][kGrads];
+    __shared__ uint32_t sMaxLast;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % bp.tilesX, ty = tile / bp.tilesX;
+    const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
+    const bool inside = px < bp.width && py < bp.height;
+    const uint2 range = ranges[tile];
+    const uint32_t start = range.x;
+    const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
+    const size_t pix = static_cast<size_t>(py) * bp.width + px;
+
+    uint32_t myLast = start;
+    float gr = 0.0f, gg = 0.0f, gb = 0.0f, gT = 0.0f, T = 1.0f;
+    if (inside) {
+        myLast = pixLast[pix];
+        const float4 st = pixState[pix];
+        const float4 G = gradColour[pix];
+        T = st.w;
+        const float cov = 1.0f - T;
+        if (bp.linearise != 0 && cov > 1e-6f) {
+            const float u0 = st.x / cov, u1 = st.y / cov, u2 = st.z / cov;
+            const float d0 = srgb_to_linear_slope(u0), d1 = srgb_to_linear_slope(u1), d2 = srgb_to_linear_slope(u2);
+            gr = G.x * d0;
+            gg = G.y * d1;
+            gb = G.z * d2;
+            // out_k = s(u_k) cov + T bg_k with cov = 1 - T; alpha_out = cov + T bg_a
+            gT = G.x * (bp.bg[0] - (srgb_to_linear(u0) - d0 * u0)) + G.y * (bp.bg[1] - (srgb_to_linear(u1) - d1 * u1)) +
+                 G.z * (bp.bg[2] - (srgb_to_linear(u2) - d2 * u2)) + G.w * (bp.bg[3] - 1.0f);
+        } else {
+            gr = G.x;
+            gg = G.y;
+            gb = G.z;
+            gT = G.x * bp.bg[0] + G.y * bp.bg[1] + G.z * bp.bg[2] + G.w * (bp.bg[3] - 1.0f);
+        }
+    }
+    const float Tfinal = T;
+    if (tid == 0) sMaxLast = start;
+    __syncthreads();
+    if (inside) atomicMax(&sMaxLast, myLast);
+    __syncthreads();
+    const uint32_t maxLast = sMaxLast;
+    bool live = inside && myLast > start;
+    float Br = 0.0f, Bg = 0.0f, Bb = 0.0f;
+    const float pxf = static_cast<float>(px) + 0.5f;
+    const float pyf = static_cast<float>(py) + 0.5f;
+
+    for (uint32_t bEnd = maxLast; bEnd > start;) {
+        const uint32_t bStart = bEnd - start > kB ? bEnd - kB : start;
+        const uint32_t cnt = bEnd - bStart;
+        if (tid < cnt) {
+            const unsigned long long word = pairs[bStart + tid];
+            sRec[tid] = proj[static_cast<uint32_t>(word & slotMask)];
+            sEmit[tid] = emit[bStart + tid];
+        }
+        for (uint32_t k = tid; k < (kBlendThreads / 32) * kB * kGrads; k += kBlendThreads) (&sPart[0][0][0])[k] = 0.0f;
+        __syncthreads();
+        if (tid < cnt) sBox[tid] = cull_box(sRec[tid]);
+        __syncthreads();
+        // Records from the back of the batch, 32 at a time.
+        for (int c = static_cast<int>((cnt - 1) & ~31u); c >= 0; c -= 32) {
+            const unsigned any = __ballot_sync(0xFFFFFFFFu, live);
+            if (any == 0) break;
+            const uint32_t big = 0xFFFFFFFFu;
+            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, live ? px : big);
+            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, live ? px : 0u);
+            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, live ? py : big);
+            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, live ? py : 0u);
+            const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
+            const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
+            bool overlap = false;
+            const uint32_t jl = static_cast<uint32_t>(c) + lane;
+            if (jl < cnt) {
+                const float4 box = sBox[jl];
+                overlap = !(box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0);
+            }
+            uint32_t todo = __ballot_sync(0xFFFFFFFFu, overlap);
+            while (todo != 0) {
+                const uint32_t bit = 31u - static_cast<uint32_t>(__clz(todo));
+                todo &= ~(1u << bit);
+                const uint32_t j = static_cast<uint32_t>(c) + bit;
+                float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                bool hit = false;
+                if (live && bStart + j < myLast) {
+                    const float4 screen = sRec[j].screen;
+                    const float4 conic = sRec[j].conic;
+                    const float dx = pxf - screen.x;
+                    const float dy = pyf - screen.y;
+                    const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
+                    if (!(power > screen.w)) {
+                        const float e = lrt_exp(-0.5f * power);
+                        const float raw = conic.w * e;
+                        const float alpha = fminf(0.99f, raw);
+                        if (!(alpha < 1.0f / 255.0f)) {
+                            hit = true;
+                            const float4 col = sRec[j].colour;
+                            const float oneMinus = 1.0f - alpha;
+                            const float Ti = T / oneMinus;
+                            const float w = Ti * alpha;
+                            v[6] = gr * w;
+                            v[7] = gg * w;
+                            v[8] = gb * w;
+                            const float dAlpha = Ti * (gr * (col.x - Br) + gg * (col.y - Bg) + gb * (col.z - Bb)) -
+                                                 gT * Tfinal / oneMinus;
+                            Br = alpha * col.x + oneMinus * Br;
+                            Bg = alpha * col.y + oneMinus * Bg;
+                            Bb = alpha * col.z + oneMinus * Bb;
+                            T = Ti;
+                            if (raw <= 0.99f) {
+                                v[5] = dAlpha * e;
+                                const float dPower = -0.5f * alpha * dAlpha;
+                                v[2] = dPower * dx * dx;
+                                v[3] = dPower * 2.0f * dx * dy;
+                                v[4] = dPower * dy * dy;
+                                v[0] = -dPower * (2.0f * conic.x * dx + 2.0f * conic.y * dy);
+                                v[1] = -dPower * (2.0f * conic.y * dx + 2.0f * conic.z * dy);
+                            }
+                        }
+                    }
+                }
+                const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
+                if (hits != 0) {
+#pragma unroll
+                    for (uint32_t k = 0; k < kGrads; ++k) {
+                        const float sum = warp_sum(v[k]);
+                        if (lane == 0) sPart[warp][j][k] = sum;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < cnt) {
+            float* out = partials + static_cast<size_t>(sEmit[tid]) * kGrads;
+#pragma unroll
+            for (uint32_t k = 0; k < kGrads; ++k) {
+                float sum = 0.0f;
+#pragma unroll
+                for (uint32_t w = 0; w < kBlendThreads / 32; ++w) sum += sPart[w][tid][k];
+                out[k] = sum;
+            }
+        }
+        __syncthreads();
+        bEnd = bStart;
+    }
 }
 
 }  // namespace
@@ -247,8 +442,30 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_kernel<<<tiles, kBlendThreads, 0, stream>>>(bp, ranges, reinterpret_cast<const unsigned long long*>(pairs),
-                                                      proj, colour, depth, err);
+    blend_kernel<false><<<tiles, kBlendThreads, 0, stream>>>(
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, nullptr, nullptr, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                               float4* colour, float* depth, float4* pixState, uint32_t* pixLast, uint32_t* err,
+                               cudaStream_t stream) {
+    const uint32_t tiles = bp.tilesX * bp.tilesY;
+    if (tiles == 0) return cudaSuccess;
+    blend_kernel<true><<<tiles, kBlendThreads, 0, stream>>>(
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, pixState, pixLast, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                                  const uint32_t* emit, const ProjRecord* proj, const float4* pixState,
+                                  const uint32_t* pixLast, const float4* gradColour, float* partials,
+                                  cudaStream_t stream) {
+    const uint32_t tiles = bp.tilesX * bp.tilesY;
+    if (tiles == 0) return cudaSuccess;
+    blend_backward_kernel<<<tiles, kBlendThreads, 0, stream>>>(
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, proj, pixState, pixLast, gradColour,
+        partials);
     return cudaGetLastError();
 }
 

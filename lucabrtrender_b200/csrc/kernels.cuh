@@ -24,6 +24,16 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
                                 uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
                                 uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream);
 
+// The same for the differentiable parameters (means float3, log-scales
+// float3, quaternions w x y z, opacity logits, SH fp16 [16][3]); also writes
+// each slot's first pair index and each pair's emit index into `values`.
+cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, const float* logScales,
+                                      const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
+                                      uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
+                                      uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
+                                      uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs, uint32_t* values,
+                                      uint32_t capacity, cudaStream_t stream);
+
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
                                   uint32_t* err, cudaStream_t stream);
@@ -41,6 +51,19 @@ cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_
 
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream);
+
+cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                               float4* colour, float* depth, float4* pixState, uint32_t* pixLast, uint32_t* err,
+                               cudaStream_t stream);
+cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                                  const uint32_t* emit, const ProjRecord* proj, const float4* pixState,
+                                  const uint32_t* pixLast, const float4* gradColour, float* partials,
+                                  cudaStream_t stream);
+
+cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
+                                  const float* logits, const uint16_t* sh, const uint32_t* touched,
+                                  const uint32_t* offsets, const float* partials, float* gMeans, float* gLogScales,
+                                  float* gQuats, float* gLogits, float* gSh, cudaStream_t stream);
 
 cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
 

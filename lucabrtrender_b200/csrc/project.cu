@@ -100,10 +100,14 @@ __device__ __forceinline__ float half_at(const uint32_t* row, uint32_t index) {
 struct Basis {
     float x, y, z;
 };
-__device__ __forceinline__ Basis basis(const uint32_t* row, uint32_t k) {
-    return {half_at(row, k * 3), half_at(row, k * 3 + 1), half_at(row, k * 3 + 2)};
+template <uint32_t kOff>
+__device__ __forceinline__ Basis basis_at(const uint32_t* row, uint32_t k) {
+    return {half_at(row, kOff + k * 3), half_at(row, kOff + k * 3 + 1), half_at(row, kOff + k * 3 + 2)};
 }
 
+// The rest coefficients start kOff halves into the row: 0 in the packed
+// layout, 3 (after the DC triple) in the training layout.
+template <uint32_t kOff>
 __device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t degree, float3 dir) {
     constexpr float kC1 = 0.4886025119029199f;
     constexpr float kC2_0 = 1.0925484305920792f, kC2_1 = -1.0925484305920792f, kC2_2 = 0.31539156525252005f,
@@ -111,10 +115,11 @@ __device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t de
     constexpr float kC3_0 = -0.5900435899266435f, kC3_1 = 2.890611442640554f, kC3_2 = -0.4570457994644658f,
                     kC3_3 = 0.3731763325901154f, kC3_4 = -0.4570457994644658f, kC3_5 = 1.445305721320277f,
                     kC3_6 = -0.5900435899266435f;
+    auto basis = [&](uint32_t k) { return basis_at<kOff>(row, k); };
     if (degree == 0) return make_float3(0.0f, 0.0f, 0.0f);
     const float x = dir.x, y = dir.y, z = dir.z;
     const float s0 = -kC1 * y, s1 = kC1 * z, s2 = kC1 * x;
-    const Basis b0 = basis(row, 0), b1 = basis(row, 1), b2 = basis(row, 2);
+    const Basis b0 = basis(0), b1 = basis(1), b2 = basis(2);
     float3 r = make_float3(s0 * b0.x + s1 * b1.x - s2 * b2.x, s0 * b0.y + s1 * b1.y - s2 * b2.y,
                            s0 * b0.z + s1 * b1.z - s2 * b2.z);
     if (degree < 2) return r;
@@ -123,8 +128,8 @@ __device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t de
     {
         const float t0 = kC2_0 * xy, t1 = kC2_1 * yz, t2 = kC2_2 * (2.0f * zz - xx - yy), t3 = kC2_3 * xz,
                     t4 = kC2_4 * (xx - yy);
-        const Basis b3 = basis(row, 3), b4 = basis(row, 4), b5 = basis(row, 5), b6 = basis(row, 6),
-                    b7 = basis(row, 7);
+        const Basis b3 = basis(3), b4 = basis(4), b5 = basis(5), b6 = basis(6),
+                    b7 = basis(7);
         r.x = r.x + (t0 * b3.x + t1 * b4.x + t2 * b5.x + t3 * b6.x + t4 * b7.x);
         r.y = r.y + (t0 * b3.y + t1 * b4.y + t2 * b5.y + t3 * b6.y + t4 * b7.y);
         r.z = r.z + (t0 * b3.z + t1 * b4.z + t2 * b5.z + t3 * b6.z + t4 * b7.z);
@@ -136,14 +141,107 @@ __device__ __forceinline__ float3 evaluate_rest(const uint32_t* row, uint32_t de
                     t3 = kC3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy),
                     t4 = kC3_4 * x * (4.0f * zz - xx - yy), t5 = kC3_5 * z * (xx - yy),
                     t6 = kC3_6 * x * (xx - 3.0f * yy);
-        const Basis b8 = basis(row, 8), b9 = basis(row, 9), b10 = basis(row, 10), b11 = basis(row, 11),
-                    b12 = basis(row, 12), b13 = basis(row, 13), b14 = basis(row, 14);
+        const Basis b8 = basis(8), b9 = basis(9), b10 = basis(10), b11 = basis(11),
+                    b12 = basis(12), b13 = basis(13), b14 = basis(14);
         r.x = r.x + (t0 * b8.x + t1 * b9.x + t2 * b10.x + t3 * b11.x + t4 * b12.x + t5 * b13.x + t6 * b14.x);
         r.y = r.y + (t0 * b8.y + t1 * b9.y + t2 * b10.y + t3 * b11.y + t4 * b12.y + t5 * b13.y + t6 * b14.y);
         r.z = r.z + (t0 * b8.z + t1 * b9.z + t2 * b10.z + t3 * b11.z + t4 * b12.z + t5 * b13.z + t6 * b14.z);
     }
     return r;
 }
+
+// Where a splat's parameters come from.
+//
+// PackedSource: the GpuSplats layout (positions float4, shape uint32x4, sh
+// f16 pairs), decoded as splat_project.slang does.
+// RawSource: the differentiable parameters -- means float3, log-scales
+// float3, quaternions (w, x, y, z) float4 normalised here, opacity logits,
+// SH fp16 [16][3] per splat (DC first). Scale is exp(log-scale), opacity
+// sigmoid(logit) = 1 / (1 + exp(-logit)) and the base colour 0.5 + SH0 * DC,
+// the same arithmetic the packing applies, without its quantisation.
+struct PackedSource {
+    const float4* positions;
+    const uint4* shape;
+    const uint32_t* sh;
+    static constexpr uint32_t kRestOffset = 0;
+    struct Loaded {
+        uint4 sw;
+    };
+    __device__ __forceinline__ void load(uint32_t i, Loaded& l, float3& p, float& opacity, float3& scale) const {
+        const float4 po = __ldg(positions + i);
+        l.sw = __ldg(shape + i);
+        p = make_float3(po.x, po.y, po.z);
+        opacity = po.w;
+        scale = make_float3(lrt_exp(low_half(l.sw.y)), lrt_exp(high_half(l.sw.y)), lrt_exp(low_half(l.sw.z)));
+    }
+    // decodeQuaternion, packing.slang:52-69
+    __device__ __forceinline__ void rotation(const Loaded& l, float& x, float& y, float& z, float& w) const {
+        const uint32_t word = l.sw.x;
+        const uint32_t largest = word & 3u;
+        float sx = static_cast<float>((word >> 22) & 1023u);
+        float sy = static_cast<float>((word >> 12) & 1023u);
+        float sz = static_cast<float>((word >> 2) & 1023u);
+        sx = (sx / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+        sy = (sy / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+        sz = (sz / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
+        const float rest = sqrtf(fmaxf(0.0f, 1.0f - (sx * sx + sy * sy + sz * sz)));
+        x = largest == 0 ? rest : sx;
+        y = largest == 1 ? rest : largest == 0 ? sx : sy;
+        z = largest == 2 ? rest : largest == 3 ? sz : sy;
+        w = largest == 3 ? rest : sz;
+    }
+    __device__ __forceinline__ float3 base(const Loaded& l, const uint32_t*) const {
+        return make_float3(high_half(l.sw.z), low_half(l.sw.w), high_half(l.sw.w));
+    }
+};
+
+struct RawSource {
+    const float* means;
+    const float* logScales;
+    const float* quats;
+    const float* logits;
+    const uint32_t* sh;
+    static constexpr uint32_t kRestOffset = 3;
+    struct Loaded {
+        float qw, qx, qy, qz;
+    };
+    __device__ __forceinline__ void load(uint32_t i, Loaded& l, float3& p, float& opacity, float3& scale) const {
+        p = make_float3(__ldg(means + 3 * i), __ldg(means + 3 * i + 1), __ldg(means + 3 * i + 2));
+        opacity = 1.0f / (1.0f + lrt_exp(-__ldg(logits + i)));
+        scale = make_float3(lrt_exp(__ldg(logScales + 3 * i)), lrt_exp(__ldg(logScales + 3 * i + 1)),
+                            lrt_exp(__ldg(logScales + 3 * i + 2)));
+        const float4 q = __ldg(reinterpret_cast<const float4*>(quats) + i);
+        l.qw = q.x;
+        l.qx = q.y;
+        l.qy = q.z;
+        l.qz = q.w;
+    }
+    __device__ __forceinline__ void rotation(const Loaded& l, float& x, float& y, float& z, float& w) const {
+        const float len = sqrtf(l.qw * l.qw + l.qx * l.qx + l.qy * l.qy + l.qz * l.qz);
+        if (len > 0.0f) {
+            x = l.qx / len;
+            y = l.qy / len;
+            z = l.qz / len;
+            w = l.qw / len;
+        } else {
+            x = 0.0f;
+            y = 0.0f;
+            z = 0.0f;
+            w = 1.0f;
+        }
+    }
+    __device__ __forceinline__ float3 base(const Loaded&, const uint32_t* row) const {
+        constexpr float kSH0 = 0.28209479177387814f;
+        return make_float3(0.5f + kSH0 * half_at(row, 0), 0.5f + kSH0 * half_at(row, 1), 0.5f + kSH0 * half_at(row, 2));
+    }
+};
+
+// Extra outputs of the training forward: each slot's first pair index, and
+// each pair's emit index carried through the sort as its value.
+struct TrainOutputs {
+    uint32_t* offsets;
+    uint32_t* values;
+};
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
 constexpr uint32_t kMaskArea = 64;    // a touched-tile bitmask up to this many
@@ -180,20 +278,22 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 
 struct PairSink {
     unsigned long long* pairs;
+    uint32_t* values;   // training only: the emit index of each pair
     uint32_t capacity;
     uint32_t* err;
     __device__ __forceinline__ void put(uint64_t at, unsigned long long word) const {
         if (at < capacity) {
             pairs[at] = word;
+            if (values != nullptr) values[at] = static_cast<uint32_t>(at);
         } else {
             atomicOr(err, kErrOverflow);
         }
     }
 };
 
+template <class Src>
 __global__ void __launch_bounds__(kProjectThreads)
-project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const uint4* __restrict__ shape,
-                    const uint32_t* __restrict__ sh, uint32_t stageWords, uint32_t shVector,
+project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWords, uint32_t shVector,
                     ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
                     uint32_t* __restrict__ keysOut, uint32_t* __restrict__ counters, uint64_t* __restrict__ status,
                     uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits,
@@ -222,14 +322,14 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     if (stageWords != 0 && blockStart < f.count) {
         const uint32_t nBlock = min(kProjectThreads, f.count - blockStart);
         const uint32_t words = nBlock * f.shWords;
-        const uint32_t* src = sh + static_cast<size_t>(blockStart) * f.shWords;
+        const uint32_t* rows = src.sh + static_cast<size_t>(blockStart) * f.shWords;
         uint32_t w0 = 0;
         if (shVector) {
             const uint32_t nvec = words >> 2;
-            for (uint32_t v = tid; v < nvec; v += kProjectThreads) cp_async16(&shStage[v * 4], src + v * 4);
+            for (uint32_t v = tid; v < nvec; v += kProjectThreads) cp_async16(&shStage[v * 4], rows + v * 4);
             w0 = nvec * 4;
         }
-        for (uint32_t w = w0 + tid; w < words; w += kProjectThreads) cp_async4(&shStage[w], src + w);
+        for (uint32_t w = w0 + tid; w < words; w += kProjectThreads) cp_async4(&shStage[w], rows + w);
     }
 
     bool alive = false;
@@ -238,30 +338,17 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     float cx = 0.0f, cy = 0.0f, ca = 0.0f, cb = 0.0f, cc = 0.0f, alpha = 0.0f, cutoff = 0.0f;
     uint4 rect = make_uint4(1, 1, 0, 0);
     Fate fate{true, false, 0.0f};
-    uint4 sw = make_uint4(0, 0, 0, 0);
+    typename Src::Loaded loaded{};
     if (inRange) {
-        const float4 po = __ldg(positions + i);
-        sw = __ldg(shape + i);
-        p = make_float3(po.x, po.y, po.z);
-        const float3 scale = make_float3(lrt_exp(low_half(sw.y)), lrt_exp(high_half(sw.y)), lrt_exp(low_half(sw.z)));
-        fate = edit_fate(f.edit, p, po.w, scale);
+        float opacity;
+        float3 scale;
+        src.load(i, loaded, p, opacity, scale);
+        fate = edit_fate(f.edit, p, opacity, scale);
         t = to_view(f, p);
         alive = !fate.removed && (t.z > f.nearZ) && !(t.z > f.farZ);
         if (alive) {
-            // decodeQuaternion, packing.slang:52-69
-            const uint32_t word = sw.x;
-            const uint32_t largest = word & 3u;
-            float sx = static_cast<float>((word >> 22) & 1023u);
-            float sy = static_cast<float>((word >> 12) & 1023u);
-            float sz = static_cast<float>((word >> 2) & 1023u);
-            sx = (sx / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
-            sy = (sy / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
-            sz = (sz / 1023.0f * 2.0f - 1.0f) * 0.70710678f;
-            const float rest = sqrtf(fmaxf(0.0f, 1.0f - (sx * sx + sy * sy + sz * sz)));
-            const float x = largest == 0 ? rest : sx;
-            const float y = largest == 1 ? rest : largest == 0 ? sx : sy;
-            const float z = largest == 2 ? rest : largest == 3 ? sz : sy;
-            const float w = largest == 3 ? rest : sz;
+            float x, y, z, w;
+            src.rotation(loaded, x, y, z, w);
             const float r00 = 1.0f - 2.0f * (y * y + z * z), r01 = 2.0f * (x * y - w * z), r02 = 2.0f * (x * z + w * y);
             const float r10 = 2.0f * (x * y + w * z), r11 = 1.0f - 2.0f * (x * x + z * z), r12 = 2.0f * (y * z - w * x);
             const float r20 = 2.0f * (x * z - w * y), r21 = 2.0f * (y * z + w * x), r22 = 1.0f - 2.0f * (x * x + y * y);
@@ -391,7 +478,7 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     uint32_t key = 0x00FFFFFFu;
     if (inRange) {
         if (alive) {
-            const float3 base = make_float3(high_half(sw.z), low_half(sw.w), high_half(sw.w));
+            const float3 base = src.base(loaded, shStage + tid * f.shWords);
             const uint32_t rpc = f.restPerColour;
             const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
             const uint32_t degree = min(stored, f.shLimit);
@@ -400,7 +487,7 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
                 const float dx = p.x - f.eye[0], dy = p.y - f.eye[1], dz = p.z - f.eye[2];
                 const float l = sqrtf(dx * dx + dy * dy + dz * dz);
                 const float3 dir = make_float3(dx / l, dy / l, dz / l);
-                restc = evaluate_rest(shStage + tid * f.shWords, degree, dir);
+                restc = evaluate_rest<Src::kRestOffset>(shStage + tid * f.shWords, degree, dir);
             }
             float3 colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
                                         fmaxf(base.z + restc.z, 0.0f));
@@ -434,6 +521,7 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
     sStart[tid] = start;
     sSmallStart[tid] = smallStart;
+    const bool writeOffset = train.offsets != nullptr && inRange;
     sMask[tid] = mask;
     sLow[tid] = (static_cast<unsigned long long>(key) << slotBits) | slot;
     sRect[tid] = rect.x | (rect.y << 16);
@@ -476,7 +564,8 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     }
     __syncthreads();
     const unsigned long long blockBase = sBase;
-    const PairSink sink{pairs, capacity, err};
+    if (writeOffset) train.offsets[slot] = static_cast<uint32_t>(blockBase + start);
+    const PairSink sink{pairs, train.values, capacity, err};
     const uint32_t tileShift = 24 + slotBits;
 
     // Masked splats: the whole block writes their pairs, one per thread per step.
@@ -525,6 +614,24 @@ project_emit_kernel(FrameParams f, const float4* __restrict__ positions, const u
     }
 }
 
+template <class Src>
+cudaError_t launch(const FrameParams& f, const Src& src, TrainOutputs train, bool stage, ProjRecord* proj, uint4* rects,
+                   uint32_t* touched, uint32_t* keys, uint32_t* counters, uint64_t* status, uint32_t* ticket,
+                   uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs,
+                   uint32_t capacity, cudaStream_t stream) {
+    const uint32_t stageWords = stage ? f.shWords : 0u;
+    const uint32_t shVector = (reinterpret_cast<uintptr_t>(src.sh) & 15u) == 0 ? 1u : 0u;
+    const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
+    cudaError_t e = cudaFuncSetAttribute(project_emit_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(std::max<size_t>(smem, 1)));
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = project_partitions(f.count);
+    project_emit_kernel<Src><<<blocks, kProjectThreads, smem, stream>>>(
+        f, src, train, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket, partitionBase,
+        lastPartition, slotBits, reinterpret_cast<unsigned long long*>(pairs), capacity);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t project_status_bytes(uint32_t partitions) { return size_t{partitions} * sizeof(uint64_t); }
@@ -538,17 +645,21 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
-    const uint32_t stageWords = stage ? f.shWords : 0u;
-    const uint32_t shVector = (reinterpret_cast<uintptr_t>(sh) & 15u) == 0 ? 1u : 0u;
-    const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
-    cudaError_t e = cudaFuncSetAttribute(project_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(std::max<size_t>(smem, 1)));
-    if (e != cudaSuccess) return e;
-    const uint32_t blocks = project_partitions(f.count);
-    project_emit_kernel<<<blocks, kProjectThreads, smem, stream>>>(
-        f, positions, shape, sh, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket,
-        partitionBase, lastPartition, slotBits, reinterpret_cast<unsigned long long*>(pairs), capacity);
-    return cudaGetLastError();
+    return launch(f, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr}, stage, proj, rects, touched,
+                  keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity, stream);
+}
+
+cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, const float* logScales,
+                                      const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
+                                      uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
+                                      uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
+                                      uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs, uint32_t* values,
+                                      uint32_t capacity, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    // The DC triple is read from the staged row too, so it is always staged.
+    return launch(f, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
+                  TrainOutputs{offsets, values}, true, proj, rects, touched, keys, counters, status, ticket,
+                  partitionBase, lastPartition, slotBits, pairs, capacity, stream);
 }
 
 }  // namespace lrt

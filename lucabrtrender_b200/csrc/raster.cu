@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 struct DeviceBuffer {
     void* ptr = nullptr;
@@ -41,6 +42,16 @@ struct lrt_rast {
     cudaEvent_t ev[8] = {};
     uint32_t splatCap = 0, pairCap = 0, tileCap = 0;
     lrt_debug_view debug{};
+    // Training: what the backward pass needs from its forward.
+    DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
+    bool trainReady = false;
+    lrt_train_params trainParams{};
+    lrt::FrameParams trainFrame{};
+    lrt::BlendParams trainBlend{};
+    const uint64_t* trainSorted = nullptr;
+    const uint32_t* trainSortedValues = nullptr;
+    uint32_t trainPairs = 0;
+    double lastBackwardMs[2] = {0.0, 0.0};
 };
 
 namespace {
@@ -187,7 +198,8 @@ void lrt_rast_destroy(lrt_rast* r) {
     DeviceScope scope(r->device);
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
-                            &r->algoValsAlt})
+                            &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
+                            &r->pixLast, &r->partials})
         release(*b);
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
     for (auto& e : r->ev)
@@ -197,33 +209,90 @@ void lrt_rast_destroy(lrt_rast* r) {
 
 const char* lrt_rast_last_error(const lrt_rast* r) { return r == nullptr ? "no handle" : r->error.c_str(); }
 
-int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
-                    const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr) {
-    const auto frameStart = std::chrono::steady_clock::now();
-    if (r == nullptr) return LRT_INVALID_ARGUMENT;
-    r->error.clear();
-    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
-        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
-    // TileRasterizer.cpp:194-217
+}  // extern "C"
+
+namespace {
+
+// One projection launch of a frame: a packed cloud instance, or the
+// differentiable parameters of the training path.
+struct CloudDesc {
+    const lrt_gpu_splats* packed = nullptr;
+    const lrt_train_params* train = nullptr;
+    const double* objectToWorld = nullptr;
+    const lrt_splat_edit* edit = nullptr;
+    uint32_t count = 0;
+};
+
+const double kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+
+FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s, const CloudDesc& c, uint32_t tilesX,
+                         uint32_t tilesY, uint32_t base) {
+    FrameParams f{};
+    f.width = s->width;
+    f.height = s->height;
+    f.tilesX = tilesX;
+    f.tilesY = tilesY;
+    f.focalX = static_cast<float>(pr->focal_x);
+    f.focalY = static_cast<float>(pr->focal_y);
+    f.centreX = static_cast<float>(pr->centre_x);
+    f.centreY = static_cast<float>(pr->centre_y);
+    f.nearZ = static_cast<float>(pr->near_z);
+    f.farZ = static_cast<float>(pr->far_z);
+    f.ortho = pr->orthographic ? 1u : 0u;
+    f.antialias = s->antialias ? 1u : 0u;
+    const M4 ov = mul4(pr->world_to_view, c.objectToWorld);
+    for (int row = 0; row < 3; ++row)
+        for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
+    double eye[3];
+    eye_in_object(c.objectToWorld, pr->eye_world, eye);
+    for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
+    f.count = c.count;
+    f.base = base;
+    if (c.train != nullptr) {
+        f.restPerColour = 15;
+        f.shWords = 24;
+    } else {
+        f.restPerColour = c.packed->rest_per_colour;
+        f.shWords = c.packed->sh_words;
+    }
+    f.shLimit = s->max_sh_degree;
+    if (c.edit != nullptr) {
+        const lrt_splat_edit& e = *c.edit;
+        f.edit.active = e.active;
+        f.edit.shape = e.shape;
+        f.edit.mode = e.mode;
+        f.edit.invert = e.invert;
+        for (int a = 0; a < 3; ++a) {
+            f.edit.centre[a] = e.centre[a];
+            f.edit.size[a] = e.size[a];
+            f.edit.tint[a] = e.tint[a];
+        }
+        f.edit.saturation = e.saturation;
+        f.edit.brightness = e.brightness;
+        f.edit.opacity = e.opacity;
+        f.edit.minOpacity = e.min_opacity;
+        f.edit.maxScale = e.max_scale;
+    }
+    return f;
+}
+
+// One frame, TileRasterizer.cpp:188-484 in this build's stage order. `train`
+// selects the training variants (emit indices carried through the sort,
+// per-slot pair offsets, per-pixel blend state for the backward pass).
+int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudDesc>& clouds,
+                 const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr,
+                 bool train, std::chrono::steady_clock::time_point frameStart) {
     if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
     if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
         targets->depth == nullptr)
         return fail(r, LRT_INVALID_ARGUMENT, "the targets are not the frame's size");
     uint64_t total = 0;
     uint64_t partitions = 0;
-    uint32_t launches = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        const lrt_gpu_splats* c = instances[k].splats;
-        if (c == nullptr || c->count == 0) continue;
-        if (c->positions == nullptr || c->shape == nullptr)
-            return fail(r, LRT_INVALID_ARGUMENT, "a cloud without positions or shape");
-        if (c->rest_per_colour > 0 && c->sh == nullptr) return fail(r, LRT_INVALID_ARGUMENT, "a cloud without harmonics");
-        if (c->rest_per_colour > 0 && c->sh_words < (c->rest_per_colour * 3 + 1) / 2)
-            return fail(r, LRT_INVALID_ARGUMENT, "sh_words too small for rest_per_colour");
-        total += c->count;
-        partitions += lrt::project_partitions(c->count);
-        launches += 1;
+    for (const CloudDesc& c : clouds) {
+        total += c.count;
+        partitions += lrt::project_partitions(c.count);
     }
+    const uint32_t launches = static_cast<uint32_t>(clouds.size());
     if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one frame");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
@@ -246,6 +315,11 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         LRT_CUDA(r, ensure(r->keys, size_t{cap} * 4), "depth keys");
         r->splatCap = cap;
     }
+    if (train) {
+        LRT_CUDA(r, ensure(r->trainOffsets, size_t{std::max(slots, 1u)} * 4), "pair offsets");
+        LRT_CUDA(r, ensure(r->pixState, size_t{s->width} * s->height * 16), "pixel state");
+        LRT_CUDA(r, ensure(r->pixLast, size_t{s->width} * s->height * 4), "pixel state");
+    }
     const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches} * 4;
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
@@ -253,10 +327,10 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         r->tileCap = tiles;
     }
     // Pairs are emitted on the device into a buffer of the capacity known
-    // before the frame; a frame that emits more is redrawn once with the
+    // before the frame; a frame that emits more is drawn again once, with the
     // buffers grown to the count it reported.
-    if (r->pairCap == 0) r->pairCap = std::max<uint32_t>(1024, static_cast<uint32_t>(std::min<uint64_t>(
-                                                                   uint64_t{slots} * 4, 0xFFFFFFFFull)));
+    if (r->pairCap == 0)
+        r->pairCap = std::max<uint32_t>(1024, static_cast<uint32_t>(std::min<uint64_t>(uint64_t{slots} * 4, 0xFFFFFFFFull)));
     uint32_t* counters = static_cast<uint32_t*>(r->counters.ptr);
     uint32_t* err = counters + 2;
     uint64_t* status = static_cast<uint64_t*>(r->scanScratch.ptr);
@@ -265,105 +339,98 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
     const uint32_t lastPartition = partitions > 0 ? static_cast<uint32_t>(partitions - 1) : 0u;
     uint32_t visible = 0, pairs = 0, statusBits = 0;
     const uint64_t* sorted = nullptr;
+    const uint32_t* sortedValues = nullptr;
+    BlendParams bp{};
+    bp.width = s->width;
+    bp.height = s->height;
+    bp.tilesX = tilesX;
+    bp.tilesY = tilesY;
+    bp.slotBits = slotBits;
+    bp.tileShift = 24 + slotBits;
+    bp.depthMode = s->depth_mode;
+    bp.linearise = s->linearise ? 1u : 0u;
+    bp.depthThreshold = s->depth_threshold;
+    for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
+    FrameParams lastParams{};
     for (int attempt = 0; attempt < 2; ++attempt) {
         LRT_CUDA(r, ensure(r->pairs, size_t{r->pairCap} * 8), "pairs");
         LRT_CUDA(r, ensure(r->pairsAlt, size_t{r->pairCap} * 8), "pairs");
+        if (train) {
+            LRT_CUDA(r, ensure(r->pairValues, size_t{r->pairCap} * 4), "pair values");
+            LRT_CUDA(r, ensure(r->pairValuesAlt, size_t{r->pairCap} * 4), "pair values");
+        }
         LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(r->pairCap, keyBits)), "sort scratch");
         LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
         LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, stream), "projection scratch");
         uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
+        uint32_t* valueBuf = train ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
 
-        // --- project, count, emit ------------------------------------------
+        // --- project, count, emit --------------------------------------------
         LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
         uint32_t base = 0, partitionBase = 0, launch = 0;
-        for (uint32_t k = 0; k < n; ++k) {
-            const lrt_splat_instance& inst = instances[k];
-            const lrt_gpu_splats* c = inst.splats;
-            if (c == nullptr || c->count == 0) continue;
-            FrameParams f{};
-            f.width = s->width;
-            f.height = s->height;
-            f.tilesX = tilesX;
-            f.tilesY = tilesY;
-            f.focalX = static_cast<float>(pr->focal_x);
-            f.focalY = static_cast<float>(pr->focal_y);
-            f.centreX = static_cast<float>(pr->centre_x);
-            f.centreY = static_cast<float>(pr->centre_y);
-            f.nearZ = static_cast<float>(pr->near_z);
-            f.farZ = static_cast<float>(pr->far_z);
-            f.ortho = pr->orthographic ? 1u : 0u;
-            f.antialias = s->antialias ? 1u : 0u;
-            const M4 ov = mul4(pr->world_to_view, inst.object_to_world);
-            for (int row = 0; row < 3; ++row)
-                for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
-            double eye[3];
-            eye_in_object(inst.object_to_world, pr->eye_world, eye);
-            for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
-            f.count = c->count;
-            f.base = base;
-            f.restPerColour = c->rest_per_colour;
-            f.shWords = c->sh_words;
-            f.shLimit = s->max_sh_degree;
-            const lrt_splat_edit& e = inst.edit;
-            f.edit.active = e.active;
-            f.edit.shape = e.shape;
-            f.edit.mode = e.mode;
-            f.edit.invert = e.invert;
-            for (int a = 0; a < 3; ++a) {
-                f.edit.centre[a] = e.centre[a];
-                f.edit.size[a] = e.size[a];
-                f.edit.tint[a] = e.tint[a];
+        for (const CloudDesc& c : clouds) {
+            const FrameParams f = frame_params(pr, s, c, tilesX, tilesY, base);
+            lastParams = f;
+            if (c.train != nullptr) {
+                const lrt_train_params& t = *c.train;
+                LRT_CUDA(r,
+                         lrt::launch_project_emit_train(
+                             f, static_cast<const float*>(t.means), static_cast<const float*>(t.log_scales),
+                             static_cast<const float*>(t.quats), static_cast<const float*>(t.opacity_logits),
+                             static_cast<const uint16_t*>(t.sh), static_cast<ProjRecord*>(r->proj.ptr),
+                             static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                             static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->trainOffsets.ptr),
+                             counters, status, tickets + launch, partitionBase, lastPartition, slotBits, pairBuf,
+                             valueBuf, r->pairCap, stream),
+                         "project");
+            } else {
+                LRT_CUDA(r,
+                         lrt::launch_project_emit(
+                             f, static_cast<const float4*>(c.packed->positions),
+                             static_cast<const uint4*>(c.packed->shape), static_cast<const uint32_t*>(c.packed->sh),
+                             static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
+                             static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
+                             status, tickets + launch, partitionBase, lastPartition, slotBits, pairBuf, r->pairCap,
+                             stream),
+                         "project");
             }
-            f.edit.saturation = e.saturation;
-            f.edit.brightness = e.brightness;
-            f.edit.opacity = e.opacity;
-            f.edit.minOpacity = e.min_opacity;
-            f.edit.maxScale = e.max_scale;
-            LRT_CUDA(r,
-                     lrt::launch_project_emit(
-                         f, static_cast<const float4*>(c->positions), static_cast<const uint4*>(c->shape),
-                         static_cast<const uint32_t*>(c->sh), static_cast<ProjRecord*>(r->proj.ptr),
-                         static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                         static_cast<uint32_t*>(r->keys.ptr), counters, status, tickets + launch, partitionBase,
-                         lastPartition, slotBits, pairBuf, r->pairCap, stream),
-                     "project");
-            base += c->count;
-            partitionBase += lrt::project_partitions(c->count);
+            base += c.count;
+            partitionBase += lrt::project_partitions(c.count);
             launch += 1;
         }
         LRT_CUDA(r, cudaEventRecord(r->ev[1], stream), "event");
 
-        // --- sort + ranges ----------------------------------------------------
+        // --- sort + ranges ------------------------------------------------------
         bool inAlt = false;
         LRT_CUDA(r,
-                 lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), nullptr, nullptr,
-                                      counters + 1, r->pairCap, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt,
-                                      stream),
+                 lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), valueBuf,
+                                      train ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr, counters + 1,
+                                      r->pairCap, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt, stream),
                  "pair sort");
         sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
+        if (train) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;
         LRT_CUDA(r,
                  lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + slotBits,
                                     static_cast<uint2*>(r->ranges.ptr), tiles, stream),
                  "ranges");
         LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
 
-        // --- blend --------------------------------------------------------------
-        BlendParams bp{};
-        bp.width = s->width;
-        bp.height = s->height;
-        bp.tilesX = tilesX;
-        bp.tilesY = tilesY;
-        bp.slotBits = slotBits;
-        bp.tileShift = 24 + slotBits;
-        bp.depthMode = s->depth_mode;
-        bp.linearise = s->linearise ? 1u : 0u;
-        bp.depthThreshold = s->depth_threshold;
-        for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
-        LRT_CUDA(r,
-                 lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
-                                   static_cast<ProjRecord*>(r->proj.ptr), static_cast<float4*>(targets->colour),
-                                   static_cast<float*>(targets->depth), err, stream),
-                 "blend");
+        // --- blend ------------------------------------------------------------------
+        if (train) {
+            LRT_CUDA(r,
+                     lrt::launch_blend_train(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
+                                             static_cast<ProjRecord*>(r->proj.ptr),
+                                             static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth),
+                                             static_cast<float4*>(r->pixState.ptr),
+                                             static_cast<uint32_t*>(r->pixLast.ptr), err, stream),
+                     "blend");
+        } else {
+            LRT_CUDA(r,
+                     lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
+                                       static_cast<ProjRecord*>(r->proj.ptr), static_cast<float4*>(targets->colour),
+                                       static_cast<float*>(targets->depth), err, stream),
+                     "blend");
+        }
         LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
         LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "readback");
         LRT_CUDA(r, cudaStreamSynchronize(stream), "frame");
@@ -372,7 +439,7 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         statusBits = r->hostCounters[2];
         if (statusBits & lrt::kErrTooManyPairs) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pairs in one frame");
         if (pairs <= r->pairCap) break;
-        r->pairCap = grow(r->pairCap, pairs);   // redraw with room for every pair
+        r->pairCap = grow(r->pairCap, pairs);   // draw again with room for every pair
         statusBits &= ~lrt::kErrOverflow;
     }
 
@@ -389,6 +456,15 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
     r->debug.depth_bits = 24;
     r->debug.tile_bits = tileBits;
     r->debug.visible = visible;
+    r->trainReady = false;
+    if (train) {
+        r->trainFrame = lastParams;
+        r->trainBlend = bp;
+        r->trainSorted = sorted;
+        r->trainSortedValues = sortedValues;
+        r->trainPairs = pairs;
+        r->trainReady = true;
+    }
 
     if (stats != nullptr) {
         std::memset(stats, 0, sizeof(*stats));
@@ -405,6 +481,110 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
     }
     if (statusBits & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
     if (statusBits & lrt::kErrOverflow || pairs > r->pairCap) return fail(r, LRT_OVERFLOW, "pair capacity exceeded");
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                    const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    std::vector<CloudDesc> clouds;
+    for (uint32_t k = 0; k < n; ++k) {
+        const lrt_gpu_splats* c = instances[k].splats;
+        if (c == nullptr || c->count == 0) continue;
+        if (c->positions == nullptr || c->shape == nullptr)
+            return fail(r, LRT_INVALID_ARGUMENT, "a cloud without positions or shape");
+        if (c->rest_per_colour > 0 && c->sh == nullptr) return fail(r, LRT_INVALID_ARGUMENT, "a cloud without harmonics");
+        if (c->rest_per_colour > 0 && c->sh_words < (c->rest_per_colour * 3 + 1) / 2)
+            return fail(r, LRT_INVALID_ARGUMENT, "sh_words too small for rest_per_colour");
+        CloudDesc d;
+        d.packed = c;
+        d.objectToWorld = instances[k].object_to_world;
+        d.edit = &instances[k].edit;
+        d.count = c->count;
+        clouds.push_back(d);
+    }
+    return render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart);
+}
+
+int lrt_rast_train_forward(lrt_rast* r, const lrt_projection* pr, const lrt_train_params* params,
+                           const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats,
+                           void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    r->trainReady = false;
+    if (pr == nullptr || params == nullptr || s == nullptr || targets == nullptr)
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    std::vector<CloudDesc> clouds;
+    if (params->count > 0) {
+        if (params->means == nullptr || params->log_scales == nullptr || params->quats == nullptr ||
+            params->opacity_logits == nullptr || params->sh == nullptr)
+            return fail(r, LRT_INVALID_ARGUMENT, "a null parameter buffer");
+        if ((reinterpret_cast<uintptr_t>(params->quats) & 15u) != 0 || (reinterpret_cast<uintptr_t>(params->sh) & 15u) != 0)
+            return fail(r, LRT_INVALID_ARGUMENT, "quats and sh must be 16-byte aligned");
+        CloudDesc d;
+        d.train = params;
+        d.objectToWorld = kIdentity;
+        d.count = params->count;
+        clouds.push_back(d);
+    }
+    r->trainParams = *params;
+    return render_frame(r, pr, clouds, s, targets, stats, streamPtr, true, frameStart);
+}
+
+int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads* grads, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (gradColour == nullptr || grads == nullptr) return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    if (!r->trainReady) return fail(r, LRT_INVALID_ARGUMENT, "no training forward to differentiate on this handle");
+    const lrt_train_params& p = r->trainParams;
+    if (p.count > 0 && (grads->means == nullptr || grads->log_scales == nullptr || grads->quats == nullptr ||
+                        grads->opacity_logits == nullptr || grads->sh == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "a null gradient buffer");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    const size_t partialBytes = std::max<size_t>(size_t{r->trainPairs} * 9 * sizeof(float), 16);
+    LRT_CUDA(r, ensure(r->partials, partialBytes), "partials");
+    LRT_CUDA(r, cudaMemsetAsync(r->partials.ptr, 0, partialBytes, stream), "partials");
+    LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
+    LRT_CUDA(r,
+             lrt::launch_blend_backward(r->trainBlend, static_cast<uint2*>(r->ranges.ptr), r->trainSorted,
+                                        r->trainSortedValues, static_cast<ProjRecord*>(r->proj.ptr),
+                                        static_cast<float4*>(r->pixState.ptr), static_cast<uint32_t*>(r->pixLast.ptr),
+                                        static_cast<const float4*>(gradColour), static_cast<float*>(r->partials.ptr),
+                                        stream),
+             "blend backward");
+    LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
+    LRT_CUDA(r,
+             lrt::launch_splat_backward(r->trainFrame, static_cast<const float*>(p.means),
+                                        static_cast<const float*>(p.log_scales), static_cast<const float*>(p.quats),
+                                        static_cast<const float*>(p.opacity_logits),
+                                        static_cast<const uint16_t*>(p.sh), static_cast<uint32_t*>(r->touched.ptr),
+                                        static_cast<uint32_t*>(r->trainOffsets.ptr),
+                                        static_cast<float*>(r->partials.ptr), static_cast<float*>(grads->means),
+                                        static_cast<float*>(grads->log_scales), static_cast<float*>(grads->quats),
+                                        static_cast<float*>(grads->opacity_logits), static_cast<float*>(grads->sh),
+                                        stream),
+             "projection backward");
+    LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "backward");
+    r->lastBackwardMs[0] = event_ms(r->ev[4], r->ev[5]);
+    r->lastBackwardMs[1] = event_ms(r->ev[5], r->ev[6]);
+    return LRT_OK;
+}
+
+int lrt_rast_backward_times(const lrt_rast* r, double* blendMs, double* projectMs) {
+    if (r == nullptr || blendMs == nullptr || projectMs == nullptr) return LRT_INVALID_ARGUMENT;
+    *blendMs = r->lastBackwardMs[0];
+    *projectMs = r->lastBackwardMs[1];
     return LRT_OK;
 }
 

@@ -1,0 +1,279 @@
+// The backward of the projection, per splat (no reference counterpart: the
+// reference renders only). A splat's nine per-pair partials -- d/d(centre x,
+// y, conic a, b, c, alpha, colour r, g, b), written by the blend backward at
+// the pair's emit index -- are contiguous from the splat's first pair index,
+// so one thread sums them in order (no atomics, deterministic), then carries
+// them back through the forward of splat_project.slang:72-169 to the
+// parameters: means, log-scales, quaternions (w, x, y, z; normalised in the
+// forward), opacity logits and the 16 x 3 SH coefficients (fp32 gradients of
+// fp16 values). Every forward intermediate is recomputed from the parameters
+// with the forward's own expressions.
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+namespace lrt {
+namespace {
+
+constexpr uint32_t kThreads = 128;
+constexpr float kC1 = 0.4886025119029199f;
+__device__ constexpr float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
+                          0.5462742152960396f};
+__device__ constexpr float kC3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f, 0.3731763325901154f,
+                          -0.4570457994644658f, 1.445305721320277f, -0.5900435899266435f};
+
+// The 15 rest basis functions (sh.slang:25-51 order) and their gradients.
+__device__ __forceinline__ void sh_basis(float x, float y, float z, uint32_t degree, float b[15], float gx[15],
+                                         float gy[15], float gz[15]) {
+    for (int k = 0; k < 15; ++k) b[k] = gx[k] = gy[k] = gz[k] = 0.0f;
+    if (degree == 0) return;
+    b[0] = -kC1 * y; gy[0] = -kC1;
+    b[1] = kC1 * z;  gz[1] = kC1;
+    b[2] = -kC1 * x; gx[2] = -kC1;
+    if (degree < 2) return;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    b[3] = kC2[0] * x * y;  gx[3] = kC2[0] * y; gy[3] = kC2[0] * x;
+    b[4] = kC2[1] * y * z;  gy[4] = kC2[1] * z; gz[4] = kC2[1] * y;
+    b[5] = kC2[2] * (2.0f * zz - xx - yy); gx[5] = -2.0f * kC2[2] * x; gy[5] = -2.0f * kC2[2] * y; gz[5] = 4.0f * kC2[2] * z;
+    b[6] = kC2[3] * x * z;  gx[6] = kC2[3] * z; gz[6] = kC2[3] * x;
+    b[7] = kC2[4] * (xx - yy); gx[7] = 2.0f * kC2[4] * x; gy[7] = -2.0f * kC2[4] * y;
+    if (degree < 3) return;
+    b[8] = kC3[0] * y * (3.0f * xx - yy);  gx[8] = 6.0f * kC3[0] * x * y; gy[8] = kC3[0] * (3.0f * xx - 3.0f * yy);
+    b[9] = kC3[1] * x * y * z; gx[9] = kC3[1] * y * z; gy[9] = kC3[1] * x * z; gz[9] = kC3[1] * x * y;
+    b[10] = kC3[2] * y * (4.0f * zz - xx - yy);
+    gx[10] = -2.0f * kC3[2] * x * y; gy[10] = kC3[2] * (4.0f * zz - xx - 3.0f * yy); gz[10] = 8.0f * kC3[2] * y * z;
+    b[11] = kC3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    gx[11] = -6.0f * kC3[3] * x * z; gy[11] = -6.0f * kC3[3] * y * z; gz[11] = kC3[3] * (6.0f * zz - 3.0f * xx - 3.0f * yy);
+    b[12] = kC3[4] * x * (4.0f * zz - xx - yy);
+    gx[12] = kC3[4] * (4.0f * zz - 3.0f * xx - yy); gy[12] = -2.0f * kC3[4] * x * y; gz[12] = 8.0f * kC3[4] * x * z;
+    b[13] = kC3[5] * z * (xx - yy); gx[13] = 2.0f * kC3[5] * x * z; gy[13] = -2.0f * kC3[5] * y * z; gz[13] = kC3[5] * (xx - yy);
+    b[14] = kC3[6] * x * (xx - 3.0f * yy); gx[14] = kC3[6] * (3.0f * xx - 3.0f * yy); gy[14] = -6.0f * kC3[6] * x * y;
+}
+
+__global__ void __launch_bounds__(kThreads)
+splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
+                      const float* __restrict__ quats, const float* __restrict__ logits,
+                      const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
+                      const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
+                      float* __restrict__ gMeans, float* __restrict__ gLogScales, float* __restrict__ gQuats,
+                      float* __restrict__ gLogits, float* __restrict__ gSh) {
+    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= f.count) return;
+    const uint32_t slot = f.base + i;
+    const uint32_t n = touched[slot];
+    float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
+    float gshv[48];
+    for (int k = 0; k < 48; ++k) gshv[k] = 0.0f;
+    if (n > 0) {
+        // The splat's summed partials.
+        float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const float* part = partials + static_cast<size_t>(offsets[slot]) * 9;
+        for (uint32_t k = 0; k < n; ++k)
+            for (int c = 0; c < 9; ++c) g[c] += part[k * 9 + c];
+        const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
+
+        // ---- forward intermediates ------------------------------------------
+        const float px = means[3 * i], py = means[3 * i + 1], pz = means[3 * i + 2];
+        const float sig = 1.0f / (1.0f + lrt_exp(-logits[i]));
+        const float s0 = lrt_exp(logScales[3 * i]), s1 = lrt_exp(logScales[3 * i + 1]), s2 = lrt_exp(logScales[3 * i + 2]);
+        const float qw0 = quats[4 * i], qx0 = quats[4 * i + 1], qy0 = quats[4 * i + 2], qz0 = quats[4 * i + 3];
+        const float len = sqrtf(qw0 * qw0 + qx0 * qx0 + qy0 * qy0 + qz0 * qz0);
+        const bool unitQ = len > 0.0f;
+        const float x = unitQ ? qx0 / len : 0.0f, y = unitQ ? qy0 / len : 0.0f, z = unitQ ? qz0 / len : 0.0f,
+                    w = unitQ ? qw0 / len : 1.0f;
+        const float3 t = to_view(f, make_float3(px, py, pz));
+        const float R[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
+                               {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
+                               {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}};
+        const float S[3] = {s0, s1, s2};
+        float M[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) M[a][b] = R[a][b] * S[b];
+        const float W[3][3] = {{f.m[0], f.m[1], f.m[2]}, {f.m[4], f.m[5], f.m[6]}, {f.m[8], f.m[9], f.m[10]}};
+        float jx0, jx2, jy1, jy2;
+        bool clampX = false, clampY = false;
+        float limX = 0.0f, limY = 0.0f;
+        const float invZ = 1.0f / t.z;
+        if (f.ortho) {
+            jx0 = f.focalX; jx2 = 0.0f; jy1 = f.focalY; jy2 = 0.0f;
+        } else {
+            const float limLoX = (-0.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+            const float limHiX = (1.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+            const float limLoY = (-0.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+            const float limHiY = (1.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+            const float ux = t.x * invZ, uy = t.y * invZ;
+            clampX = ux < limLoX || ux > limHiX;
+            clampY = uy < limLoY || uy > limHiY;
+            limX = ux < limLoX ? limLoX : limHiX;
+            limY = uy < limLoY ? limLoY : limHiY;
+            const float tx = clampf(ux, limLoX, limHiX) * t.z;
+            const float ty = clampf(uy, limLoY, limHiY) * t.z;
+            jx0 = f.focalX * invZ; jx2 = -f.focalX * tx * invZ * invZ;
+            jy1 = f.focalY * invZ; jy2 = -f.focalY * ty * invZ * invZ;
+        }
+        float T2x[3], T2y[3], ax[3], ay[3];
+        for (int c = 0; c < 3; ++c) {
+            T2x[c] = jx0 * W[0][c] + jx2 * W[2][c];
+            T2y[c] = jy1 * W[1][c] + jy2 * W[2][c];
+        }
+        for (int c = 0; c < 3; ++c) {
+            ax[c] = T2x[0] * M[0][c] + T2x[1] * M[1][c] + T2x[2] * M[2][c];
+            ay[c] = T2y[0] * M[0][c] + T2y[1] * M[1][c] + T2y[2] * M[2][c];
+        }
+        const float ap = ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2];
+        const float bp = ax[0] * ay[0] + ax[1] * ay[1] + ax[2] * ay[2];
+        const float cp = ay[0] * ay[0] + ay[1] * ay[1] + ay[2] * ay[2];
+        const float detB = ap * cp - bp * bp;
+        const float a = ap + 0.3f, c = cp + 0.3f, b = bp;
+        const float det = a * c - b * b;
+        const float aa = f.antialias != 0 ? sqrtf(fmaxf(detB, 0.0f) / det) : 1.0f;
+        const float QA = c / det, QB = -b / det, QC = a / det;
+
+        // ---- colour ---------------------------------------------------------------
+        const uint16_t* row = sh + static_cast<size_t>(i) * 48;
+        float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
+        const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
+        const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
+        const uint32_t degree = min(3u, f.shLimit);
+        float bas[15], bgx[15], bgy[15], bgz[15];
+        sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
+        float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
+        for (int ch = 0; ch < 3; ++ch) {
+            constexpr float kSH0 = 0.28209479177387814f;
+            const float base = 0.5f + kSH0 * half_to_float(row[ch]);
+            float rest = 0.0f;
+            for (int k = 0; k < 15; ++k) rest += bas[k] * half_to_float(row[3 + 3 * k + ch]);
+            const float gcol = g[6 + ch];
+            if (base + rest > 0.0f) {
+                gshv[ch] = kSH0 * gcol;
+                for (uint32_t k = 0; k < (degree == 3 ? 15u : degree == 2 ? 8u : degree == 1 ? 3u : 0u); ++k) {
+                    gshv[3 + 3 * k + ch] = bas[k] * gcol;
+                    const float coef = half_to_float(row[3 + 3 * k + ch]) * gcol;
+                    gdx += coef * bgx[k];
+                    gdy += coef * bgy[k];
+                    gdz += coef * bgz[k];
+                }
+            }
+        }
+        {   // dir = v / |v|, v = p - eye
+            const float dotd = gdx * dirx + gdy * diry + gdz * dirz;
+            gm[0] += (gdx - dotd * dirx) / vl;
+            gm[1] += (gdy - dotd * diry) / vl;
+            gm[2] += (gdz - dotd * dirz) / vl;
+        }
+
+        // ---- alpha0 = sigmoid(logit) * aa -----------------------------------------
+        glog = gAlpha * aa * sig * (1.0f - sig);
+        const float gAA = gAlpha * sig;
+        float gDetB = 0.0f, gDet = 0.0f;
+        if (f.antialias != 0 && detB > 0.0f && aa > 0.0f) {
+            gDetB = gAA / (2.0f * aa * det);
+            gDet = -gAA * aa / (2.0f * det);
+        }
+
+        // ---- conic = inverse of [[a, b], [b, c]] ------------------------------------
+        // G_Sigma = -Q G_Q Q with G_Q = [[gA, gB/2], [gB/2, gC]]
+        const float h = 0.5f * gB;
+        const float t00 = gA * QA + h * QB, t01 = gA * QB + h * QC;
+        const float t10 = h * QA + gC * QB, t11 = h * QB + gC * QC;
+        const float gS00 = -(QA * t00 + QB * t10), gS01 = -(QA * t01 + QB * t11);
+        const float gS11 = -(QB * t01 + QC * t11);
+        float ga = gS00 + gDet * c + gDetB * cp;
+        float gc = gS11 + gDet * a + gDetB * ap;
+        float gb = 2.0f * gS01 - gDet * 2.0f * b - gDetB * 2.0f * bp;
+
+        // ---- a' = ax.ax, b' = ax.ay, c' = ay.ay --------------------------------
+        float gax[3], gay[3];
+        for (int k = 0; k < 3; ++k) {
+            gax[k] = 2.0f * ga * ax[k] + gb * ay[k];
+            gay[k] = gb * ax[k] + 2.0f * gc * ay[k];
+        }
+        // ax = T2x M, ay = T2y M
+        float gT2x[3], gT2y[3], gM[3][3];
+        for (int r = 0; r < 3; ++r) {
+            gT2x[r] = gax[0] * M[r][0] + gax[1] * M[r][1] + gax[2] * M[r][2];
+            gT2y[r] = gay[0] * M[r][0] + gay[1] * M[r][1] + gay[2] * M[r][2];
+            for (int cc = 0; cc < 3; ++cc) gM[r][cc] = T2x[r] * gax[cc] + T2y[r] * gay[cc];
+        }
+        // M = R diag(S)
+        float gR[3][3];
+        for (int cc = 0; cc < 3; ++cc) {
+            float gs = 0.0f;
+            for (int r = 0; r < 3; ++r) {
+                gR[r][cc] = gM[r][cc] * S[cc];
+                gs += gM[r][cc] * R[r][cc];
+            }
+            gls[cc] = gs * S[cc];
+        }
+        // R(x, y, z, w)
+        const float gx = 2.0f * (gR[0][1] * y + gR[0][2] * z + gR[1][0] * y - 2.0f * gR[1][1] * x - gR[1][2] * w +
+                                 gR[2][0] * z + gR[2][1] * w - 2.0f * gR[2][2] * x);
+        const float gy = 2.0f * (-2.0f * gR[0][0] * y + gR[0][1] * x + gR[0][2] * w + gR[1][0] * x + gR[1][2] * z -
+                                 gR[2][0] * w + gR[2][1] * z - 2.0f * gR[2][2] * y);
+        const float gz = 2.0f * (-2.0f * gR[0][0] * z - gR[0][1] * w + gR[0][2] * x + gR[1][0] * w -
+                                 2.0f * gR[1][1] * z + gR[1][2] * y + gR[2][0] * x + gR[2][1] * y);
+        const float gw = 2.0f * (-gR[0][1] * z + gR[0][2] * y + gR[1][0] * z - gR[1][2] * x - gR[2][0] * y +
+                                 gR[2][1] * x);
+        if (unitQ) {   // q_n = q / |q|
+            const float dq = gx * x + gy * y + gz * z + gw * w;
+            gq[0] = (gw - dq * w) / len;
+            gq[1] = (gx - dq * x) / len;
+            gq[2] = (gy - dq * y) / len;
+            gq[3] = (gz - dq * z) / len;
+        }
+        // T2 = J W
+        float gjx0 = 0.0f, gjx2 = 0.0f, gjy1 = 0.0f, gjy2 = 0.0f;
+        for (int cc = 0; cc < 3; ++cc) {
+            gjx0 += gT2x[cc] * W[0][cc];
+            gjx2 += gT2x[cc] * W[2][cc];
+            gjy1 += gT2y[cc] * W[1][cc];
+            gjy2 += gT2y[cc] * W[2][cc];
+        }
+        float gt[3] = {0.0f, 0.0f, 0.0f};
+        if (f.ortho) {
+            gt[0] += gcx * f.focalX;
+            gt[1] += gcy * f.focalY;
+        } else {
+            // centre = focal t.xy / t.z + c
+            gt[0] += gcx * f.focalX * invZ;
+            gt[1] += gcy * f.focalY * invZ;
+            gt[2] += -(gcx * f.focalX * t.x + gcy * f.focalY * t.y) * invZ * invZ;
+            // J: jx0 = fx / tz, jx2 = -fx tx_c / tz^2 (tx_c = t.x, or lim tz when clamped)
+            gt[2] += -(gjx0 * f.focalX + gjy1 * f.focalY) * invZ * invZ;
+            if (clampX) {
+                gt[2] += gjx2 * f.focalX * limX * invZ * invZ;
+            } else {
+                gt[0] += -gjx2 * f.focalX * invZ * invZ;
+                gt[2] += 2.0f * gjx2 * f.focalX * t.x * invZ * invZ * invZ;
+            }
+            if (clampY) {
+                gt[2] += gjy2 * f.focalY * limY * invZ * invZ;
+            } else {
+                gt[1] += -gjy2 * f.focalY * invZ * invZ;
+                gt[2] += 2.0f * gjy2 * f.focalY * t.y * invZ * invZ * invZ;
+            }
+        }
+        // t = W p + t0
+        for (int k = 0; k < 3; ++k) gm[k] += W[0][k] * gt[0] + W[1][k] * gt[1] + W[2][k] * gt[2];
+    }
+    for (int k = 0; k < 3; ++k) {
+        gMeans[3 * i + k] = gm[k];
+        gLogScales[3 * i + k] = gls[k];
+    }
+    for (int k = 0; k < 4; ++k) gQuats[4 * i + k] = gq[k];
+    gLogits[i] = glog;
+    for (int k = 0; k < 48; ++k) gSh[static_cast<size_t>(i) * 48 + k] = gshv[k];
+}
+
+}  // namespace
+
+cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
+                                  const float* logits, const uint16_t* sh, const uint32_t* touched,
+                                  const uint32_t* offsets, const float* partials, float* gMeans, float* gLogScales,
+                                  float* gQuats, float* gLogits, float* gSh, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    splat_backward_kernel<<<(f.count + kThreads - 1) / kThreads, kThreads, 0, stream>>>(
+        f, means, logScales, quats, logits, sh, touched, offsets, partials, gMeans, gLogScales, gQuats, gLogits, gSh);
+    return cudaGetLastError();
+}
+
+}  // namespace lrt

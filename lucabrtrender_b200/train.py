@@ -1,0 +1,78 @@
+"""The differentiable rasteriser: a torch.autograd.Function over the C-ABI's
+training entry points (``lrt_rast_train_forward`` / ``lrt_rast_train_backward``).
+
+Parameters (one cloud, world space): means [N,3], log_scales [N,3],
+quats [N,4] as (w, x, y, z) (normalised in the forward), opacity_logits [N],
+sh [N,16,3] (DC first). The SH coefficients are kept in fp32 by the caller
+and read by the kernels as fp16; their gradient is fp32. The colour image
+[H,W,4] is differentiable; depth is not.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _abi
+from .camera import Camera, Projection, projection_for
+from .raster import FrameStats, RenderSettings, TileRasterizer, _stream_ptr
+
+
+class _Rasterize(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, means, log_scales, quats, opacity_logits, sh, raster: TileRasterizer, projection: Projection,
+                settings: RenderSettings):
+        dev = means.device
+        n = means.shape[0]
+        means = means.contiguous().float()
+        log_scales = log_scales.contiguous().float()
+        quats = quats.contiguous().float()
+        opacity_logits = opacity_logits.contiguous().float()
+        sh16 = sh.detach().reshape(n, 48).to(torch.float16).contiguous()
+        colour = torch.empty((settings.height, settings.width, 4), dtype=torch.float32, device=dev)
+        depth = torch.empty((settings.height, settings.width), dtype=torch.float32, device=dev)
+        p = _abi.TrainParams()
+        p.count = n
+        p.means, p.log_scales, p.quats = means.data_ptr(), log_scales.data_ptr(), quats.data_ptr()
+        p.opacity_logits, p.sh = opacity_logits.data_ptr(), sh16.data_ptr()
+        t = _abi.TargetsStruct()
+        t.width, t.height, t.colour, t.depth = settings.width, settings.height, colour.data_ptr(), depth.data_ptr()
+        pr = projection.struct()
+        st = settings.struct()
+        stats = _abi.FrameStatsStruct()
+        raster._check(_abi.load().lrt_rast_train_forward(raster._handle, C.byref(pr), C.byref(p), C.byref(st),
+                                                         C.byref(t), C.byref(stats), _stream_ptr(None)))
+        ctx.raster = raster
+        ctx.stats = FrameStats.from_struct(stats)
+        # The handle keeps pointers to these until the backward.
+        ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh16)
+        ctx.mark_non_differentiable(depth)
+        return colour, depth
+
+    @staticmethod
+    def backward(ctx, grad_colour, grad_depth):
+        means, log_scales, quats, opacity_logits, sh16 = ctx.saved_tensors
+        n = means.shape[0]
+        g = [torch.empty_like(means), torch.empty_like(log_scales), torch.empty_like(quats),
+             torch.empty_like(opacity_logits), torch.empty((n, 16, 3), dtype=torch.float32, device=means.device)]
+        grads = _abi.TrainGrads()
+        grads.means, grads.log_scales, grads.quats = g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr()
+        grads.opacity_logits, grads.sh = g[3].data_ptr(), g[4].data_ptr()
+        gc = grad_colour.contiguous().float()
+        raster = ctx.raster
+        raster._check(_abi.load().lrt_rast_train_backward(raster._handle, gc.data_ptr(), C.byref(grads),
+                                                          _stream_ptr(None)))
+        return g[0], g[1], g[2], g[3], g[4], None, None, None
+
+
+def rasterize(means, log_scales, quats, opacity_logits, sh, view: Camera | Projection, settings: RenderSettings,
+              raster: TileRasterizer):
+    """Render the differentiable cloud; returns (colour [H,W,4], depth [H,W])."""
+    projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
+    return _Rasterize.apply(means, log_scales, quats, opacity_logits, sh, raster, projection, settings)
+
+
+def backward_times(raster: TileRasterizer) -> tuple[float, float]:
+    a, b = C.c_double(), C.c_double()
+    raster._check(_abi.load().lrt_rast_backward_times(raster._handle, C.byref(a), C.byref(b)))
+    return a.value, b.value

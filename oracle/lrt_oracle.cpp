@@ -445,12 +445,15 @@ inline float halfAt(const uint32_t* row, uint32_t index) {
     const uint32_t w = row[index / 2];
     return (index & 1u) == 0u ? lowHalf(w) : highHalf(w);
 }
-inline F3 basis(const uint32_t* row, uint32_t k) {
-    return {halfAt(row, k * 3), halfAt(row, k * 3 + 1), halfAt(row, k * 3 + 2)};
+inline F3 basisAt(const uint32_t* row, uint32_t off, uint32_t k) {
+    return {halfAt(row, off + k * 3), halfAt(row, off + k * 3 + 1), halfAt(row, off + k * 3 + 2)};
 }
 uint32_t degreeOf(uint32_t rest) { return rest >= 15 ? 3 : rest >= 8 ? 2 : rest >= 3 ? 1 : 0; }
 
-F3 evaluateRest(const uint32_t* row, uint32_t degree, F3 dir) {
+// `off`: where the rest coefficients start in the row, in halves (0 in the
+// packed layout; 3, after the DC triple, in the training layout).
+F3 evaluateRest(const uint32_t* row, uint32_t degree, F3 dir, uint32_t off = 0) {
+    auto basis = [&](const uint32_t* rw, uint32_t k) { return basisAt(rw, off, k); };
     if (degree == 0) return {0.0f, 0.0f, 0.0f};
     const float x = dir.x, y = dir.y, z = dir.z;
     const float s0 = -kC1 * y, s1 = kC1 * z, s2 = kC1 * x;
@@ -537,9 +540,67 @@ struct Projected {
     std::vector<uint32_t> touched, visible, keys;
 };
 
+// Where a splat's parameters come from: the packed cloud (decoded as
+// splat_project.slang does) or the training path's raw parameters (means,
+// log-scales, quaternions w x y z normalised here, opacity logits, SH fp16
+// [16][3] with the DC first: scale exp(log-scale), opacity
+// 1 / (1 + exp(-logit)), base colour 0.5 + SH0 * DC).
+struct PackedSrc {
+    const lrt_gpu_splats& c;
+    void load(uint32_t i, F3& p, float& opacity, F3& scale) const {
+        const float* pos = static_cast<const float*>(c.positions) + size_t{i} * 4;
+        const uint32_t* shape = static_cast<const uint32_t*>(c.shape) + size_t{i} * 4;
+        p = {pos[0], pos[1], pos[2]};
+        opacity = pos[3];
+        scale = {expImpl(lowHalf(shape[1])), expImpl(highHalf(shape[1])), expImpl(lowHalf(shape[2]))};
+    }
+    void rotation(uint32_t i, float q[4]) const {
+        decodeQuaternion(static_cast<const uint32_t*>(c.shape)[size_t{i} * 4], q);
+    }
+    F3 base(uint32_t i) const {
+        const uint32_t* shape = static_cast<const uint32_t*>(c.shape) + size_t{i} * 4;
+        return {highHalf(shape[2]), lowHalf(shape[3]), highHalf(shape[3])};
+    }
+    const uint32_t* shRow(uint32_t i) const { return static_cast<const uint32_t*>(c.sh) + size_t{i} * c.sh_words; }
+    uint32_t restOffset() const { return 0; }
+    uint32_t restPerColour() const { return c.rest_per_colour; }
+};
+
+struct RawSrc {
+    const lrt_train_params& t;
+    void load(uint32_t i, F3& p, float& opacity, F3& scale) const {
+        const float* m = static_cast<const float*>(t.means) + size_t{i} * 3;
+        const float* ls = static_cast<const float*>(t.log_scales) + size_t{i} * 3;
+        p = {m[0], m[1], m[2]};
+        opacity = 1.0f / (1.0f + expImpl(-static_cast<const float*>(t.opacity_logits)[i]));
+        scale = {expImpl(ls[0]), expImpl(ls[1]), expImpl(ls[2])};
+    }
+    void rotation(uint32_t i, float q[4]) const {
+        const float* r = static_cast<const float*>(t.quats) + size_t{i} * 4;   // w x y z
+        const float len = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+        if (len > 0.0f) {
+            q[0] = r[1] / len;
+            q[1] = r[2] / len;
+            q[2] = r[3] / len;
+            q[3] = r[0] / len;
+        } else {
+            q[0] = q[1] = q[2] = 0.0f;
+            q[3] = 1.0f;
+        }
+    }
+    F3 base(uint32_t i) const {
+        const uint32_t* row = shRow(i);
+        return {0.5f + kSH0 * halfAt(row, 0), 0.5f + kSH0 * halfAt(row, 1), 0.5f + kSH0 * halfAt(row, 2)};
+    }
+    const uint32_t* shRow(uint32_t i) const { return static_cast<const uint32_t*>(t.sh) + size_t{i} * 24; }
+    uint32_t restOffset() const { return 3; }
+    uint32_t restPerColour() const { return 15; }
+};
+
 // shaders/lrt/splat/splat_project.slang:39-221 (relight excluded: off in
 // every configuration this build serves).
-void projectOne(const Frame& f, const lrt_gpu_splats& c, uint32_t i, Projected& out) {
+template <class Src>
+void projectOne(const Frame& f, const Src& src, uint32_t i, Projected& out) {
     const uint32_t slot = f.base + i;
     auto cull = [&] {
         out.touched[slot] = 0;
@@ -548,12 +609,9 @@ void projectOne(const Frame& f, const lrt_gpu_splats& c, uint32_t i, Projected& 
         out.rects[slot] = {1, 1, 0, 0};
         out.proj[slot] = Record{};
     };
-    const float* pos = static_cast<const float*>(c.positions) + size_t{i} * 4;
-    const uint32_t* shape = static_cast<const uint32_t*>(c.shape) + size_t{i} * 4;
-    const F3 p{pos[0], pos[1], pos[2]};
-    float opacity = pos[3];
-    const F3 scale{expImpl(lowHalf(shape[1])), expImpl(highHalf(shape[1])),
-                   expImpl(lowHalf(shape[2]))};
+    F3 p, scale;
+    float opacity;
+    src.load(i, p, opacity, scale);
     const Fate fate = editFate(f.edit, p, opacity, scale);
     if (fate.removed) return cull();
     opacity = fate.opacity;
@@ -562,7 +620,7 @@ void projectOne(const Frame& f, const lrt_gpu_splats& c, uint32_t i, Projected& 
     if (!(t.z > f.nearZ) || t.z > f.farZ) return cull();
 
     float q[4];
-    decodeQuaternion(shape[0], q);
+    src.rotation(i, q);
     const float x = q[0], y = q[1], z = q[2], w = q[3];
     const float r[3][3] = {
         {1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
@@ -632,11 +690,10 @@ void projectOne(const Frame& f, const lrt_gpu_splats& c, uint32_t i, Projected& 
             if (tileTouched(f, cx, cy, conic, cutoff, tx, ty)) touched += 1;
     if (touched == 0) return cull();
 
-    const F3 base{highHalf(shape[2]), lowHalf(shape[3]), highHalf(shape[3])};
-    const uint32_t degree = std::min(degreeOf(c.rest_per_colour), f.shLimit);
+    const F3 base = src.base(i);
+    const uint32_t degree = std::min(degreeOf(src.restPerColour()), f.shLimit);
     const F3 dir = normalize3(F3{p.x - f.eye[0], p.y - f.eye[1], p.z - f.eye[2]});
-    const uint32_t* shRow = static_cast<const uint32_t*>(c.sh) + size_t{i} * c.sh_words;
-    const F3 rest = evaluateRest(shRow, degree, dir);
+    const F3 rest = evaluateRest(src.shRow(i), degree, dir, src.restOffset());
     F3 colour{std::fmax(base.x + rest.x, 0.0f), std::fmax(base.y + rest.y, 0.0f),
               std::fmax(base.z + rest.z, 0.0f)};
     if (fate.graded) colour = editGrade(f.edit, colour);
@@ -654,7 +711,8 @@ void projectOne(const Frame& f, const lrt_gpu_splats& c, uint32_t i, Projected& 
 
 // shaders/lrt/splat/splat_blend.slang:23-108, splat-only (no composite).
 void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t* pairSlots,
-                const uint32_t* ranges, uint32_t px, uint32_t py, float* colour, float* depth) {
+                const uint32_t* ranges, uint32_t px, uint32_t py, float* colour, float* depth,
+                std::vector<uint32_t>* contributors = nullptr) {
     const uint32_t tile = (py / kTile) * f.tilesX + px / kTile;
     const uint32_t start = ranges[tile * 2];
     const uint32_t end = ranges[tile * 2 + 1];
@@ -679,6 +737,7 @@ void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t*
         depthSum = depthSum + weight * rec.screen[2];
         T = T * (1.0f - alpha);
         if (depthAt < 0.0f && 1.0f - T >= f.depthThreshold) depthAt = rec.screen[2];
+        if (contributors != nullptr) contributors->push_back(pairSlots[k]);
         if (T < 1e-4f) break;
     }
     const float coverage = 1.0f - T;
@@ -836,11 +895,25 @@ int ora_pack_splats(const float* raw, uint32_t count, uint32_t fpr, uint32_t fil
     return LRT_OK;
 }
 
-int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
-               const lrt_render_settings* s, ora_frame_out* out, uint32_t threads) {
+}  // extern "C"
+
+namespace {
+
+// The frame after projection: counts, the reference's two sorts, ranges and
+// the blend (TileRasterizer.cpp:382-484). `project` fills P. When `crop` is
+// given, the slots that contribute to each pixel inside it are recorded in
+// blend order (what a gradient check needs to hold the discrete choices of
+// the frame fixed).
+struct Crop {
+    uint32_t x0, y0, w, h;
+    std::vector<std::vector<uint32_t>> lists;
+};
+
+template <class ProjectFn>
+int renderImpl(const lrt_projection* pr, uint64_t total, const lrt_render_settings* s, ora_frame_out* out,
+               uint32_t threads, ProjectFn&& project, Crop* crop) {
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     if (s->width == 0 || s->height == 0) return LRT_INVALID_ARGUMENT;
-    const uint64_t total = totalSplats(instances, n);
     if (total > 0xFFFFFFFFull) return LRT_UNSUPPORTED;
     Frame f = frameFor(*pr, *s);
     const uint32_t tiles = f.tilesX * f.tilesY;
@@ -852,22 +925,8 @@ int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, ui
     P.visible.assign(slots, 0);
     P.keys.assign(slots, 0x00FFFFFFu);
 
-    // TileRasterizer.cpp:290-380 -- project, instance by instance.
     Clock::time_point t = Clock::now();
-    uint32_t base = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        const lrt_gpu_splats* c = instances[k].splats;
-        if (c == nullptr || c->count == 0) continue;
-        Frame fi = f;
-        setObject(fi, *pr, instances[k]);
-        fi.base = base;
-        fi.restPerColour = c->rest_per_colour;
-        fi.shWords = c->sh_words;
-        parallelFor(c->count, threads, [&](uint64_t b, uint64_t e) {
-            for (uint64_t i = b; i < e; ++i) projectOne(fi, *c, static_cast<uint32_t>(i), P);
-        });
-        base += c->count;
-    }
+    project(f, P, threads);
     out->stage_ms[0] = msSince(t);
 
     // Counts (TileRasterizer.cpp:382-397).
@@ -947,9 +1006,14 @@ int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, ui
     }
     parallelFor(f.height, threads, [&](uint64_t b, uint64_t e) {
         for (uint64_t py = b; py < e; ++py)
-            for (uint32_t px = 0; px < f.width; ++px)
-                blendPixel(f, P.proj, sortedSlots.data(), ranges.data(), px,
-                           static_cast<uint32_t>(py), colour, depth);
+            for (uint32_t px = 0; px < f.width; ++px) {
+                std::vector<uint32_t>* list = nullptr;
+                if (crop != nullptr && px >= crop->x0 && px < crop->x0 + crop->w && py >= crop->y0 &&
+                    py < crop->y0 + crop->h)
+                    list = &crop->lists[(py - crop->y0) * crop->w + (px - crop->x0)];
+                blendPixel(f, P.proj, sortedSlots.data(), ranges.data(), px, static_cast<uint32_t>(py), colour,
+                           depth, list);
+            }
     });
     out->stage_ms[5] = msSince(t);
 
@@ -965,6 +1029,66 @@ int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, ui
         if (out->pair_tiles) std::memcpy(out->pair_tiles, sortedTiles.data(), pairs * 4ull);
         if (out->pair_slots) std::memcpy(out->pair_slots, sortedSlots.data(), pairs * 4ull);
     }
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+               const lrt_render_settings* s, ora_frame_out* out, uint32_t threads) {
+    auto project = [&](const Frame& f, Projected& P, uint32_t th) {
+        // TileRasterizer.cpp:290-380 -- project, instance by instance.
+        uint32_t base = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const lrt_gpu_splats* c = instances[k].splats;
+            if (c == nullptr || c->count == 0) continue;
+            Frame fi = f;
+            setObject(fi, *pr, instances[k]);
+            fi.base = base;
+            fi.restPerColour = c->rest_per_colour;
+            fi.shWords = c->sh_words;
+            parallelFor(c->count, th, [&](uint64_t b, uint64_t e) {
+                const PackedSrc src{*c};
+                for (uint64_t i = b; i < e; ++i) projectOne(fi, src, static_cast<uint32_t>(i), P);
+            });
+            base += c->count;
+        }
+    };
+    return renderImpl(pr, totalSplats(instances, n), s, out, threads, project, nullptr);
+}
+
+int ora_train_render(const lrt_projection* pr, const lrt_train_params* params, const lrt_render_settings* s,
+                     ora_frame_out* out, uint32_t threads, uint32_t crop_x0, uint32_t crop_y0, uint32_t crop_w,
+                     uint32_t crop_h, uint32_t* list_offsets, uint32_t* list_slots, uint64_t list_capacity,
+                     uint64_t* list_total) {
+    lrt_splat_instance inst{};
+    const double identity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    std::memcpy(inst.object_to_world, identity, sizeof(identity));
+    auto project = [&](const Frame& f, Projected& P, uint32_t th) {
+        Frame fi = f;
+        setObject(fi, *pr, inst);
+        fi.base = 0;
+        parallelFor(params->count, th, [&](uint64_t b, uint64_t e) {
+            const RawSrc src{*params};
+            for (uint64_t i = b; i < e; ++i) projectOne(fi, src, static_cast<uint32_t>(i), P);
+        });
+    };
+    Crop crop{crop_x0, crop_y0, crop_w, crop_h, {}};
+    crop.lists.resize(size_t{crop_w} * crop_h);
+    const int code = renderImpl(pr, params->count, s, out, threads, project, (crop_w != 0 && crop_h != 0) ? &crop : nullptr);
+    if (code != LRT_OK) return code;
+    uint64_t at = 0;
+    for (size_t k = 0; k < crop.lists.size(); ++k) {
+        if (list_offsets) list_offsets[k] = static_cast<uint32_t>(at);
+        for (uint32_t sl : crop.lists[k]) {
+            if (list_slots && at < list_capacity) list_slots[at] = sl;
+            ++at;
+        }
+    }
+    if (list_offsets) list_offsets[crop.lists.size()] = static_cast<uint32_t>(at);
+    if (list_total) *list_total = at;
     return LRT_OK;
 }
 

@@ -68,6 +68,16 @@ int ora_render(const lrt_projection* projection, const lrt_splat_instance* insta
                uint32_t instance_count, const lrt_render_settings* settings,
                ora_frame_out* out, uint32_t threads);
 
+/* The training path's forward: one cloud of raw parameters (HOST pointers,
+ * layout of lrt_train_params) in world space, rendered like ora_render. For
+ * each pixel of the crop, the slots that contribute to it, in blend order,
+ * are written to list_slots; pixel k's list is
+ * [list_offsets[k], list_offsets[k + 1]). */
+int ora_train_render(const lrt_projection* projection, const lrt_train_params* params,
+                     const lrt_render_settings* settings, ora_frame_out* out, uint32_t threads, uint32_t crop_x0,
+                     uint32_t crop_y0, uint32_t crop_w, uint32_t crop_h, uint32_t* list_offsets,
+                     uint32_t* list_slots, uint64_t list_capacity, uint64_t* list_total);
+
 /* The brute-force ground truth (ReferenceRenderer). Returns the number of
  * pixels whose contributor count passed kMaxHits in *overflow. */
 int ora_reference_render(const lrt_projection* projection, const lrt_splat_instance* instances,

@@ -241,3 +241,63 @@ def math_eval(fn: int, x: np.ndarray) -> np.ndarray:
 
 def threads() -> int:
     return os.cpu_count() or 1
+
+
+# --------------------------------------------------------- training path ----
+@dataclass
+class RawCloud:
+    """Differentiable parameters on the host (the training path's layout)."""
+    means: np.ndarray       # [N, 3] float32
+    log_scales: np.ndarray  # [N, 3] float32
+    quats: np.ndarray       # [N, 4] float32 (w, x, y, z)
+    logits: np.ndarray      # [N] float32
+    sh16: np.ndarray        # [N, 16, 3] float16
+
+    @property
+    def count(self) -> int:
+        return int(self.means.shape[0])
+
+    def struct(self) -> _abi.TrainParams:
+        for name in ("means", "log_scales", "quats", "logits", "sh16"):
+            a = getattr(self, name)
+            assert a.flags["C_CONTIGUOUS"], name
+        p = _abi.TrainParams()
+        p.count = self.count
+        p.means, p.log_scales, p.quats = self.means.ctypes.data, self.log_scales.ctypes.data, self.quats.ctypes.data
+        p.opacity_logits, p.sh = self.logits.ctypes.data, self.sh16.ctypes.data
+        return p
+
+
+def train_render(projection: _abi.Projection, cloud: RawCloud, settings: _abi.RenderSettingsStruct,
+                 crop=(0, 0, 0, 0), threads: int = 0) -> dict:
+    lib = load()
+    lib.ora_train_render.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.TrainParams),
+                                     C.POINTER(_abi.RenderSettingsStruct), C.POINTER(FrameOut), C.c_uint32,
+                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     C.c_uint64, C.POINTER(C.c_uint64)]
+    n = cloud.count
+    w, h = settings.width, settings.height
+    tiles = ((w + 15) // 16) * ((h + 15) // 16)
+    colour = np.zeros((h, w, 4), np.float32)
+    depth = np.zeros((h, w), np.float32)
+    proj = np.zeros((n, 12), np.float32)
+    rects = np.zeros((n, 4), np.uint32)
+    touched = np.zeros(n, np.uint32)
+    keys = np.zeros(n, np.uint32)
+    ranges = np.zeros((tiles, 2), np.uint32)
+    out = FrameOut()
+    out.colour, out.depth, out.proj, out.rects = colour.ctypes.data, depth.ctypes.data, proj.ctypes.data, rects.ctypes.data
+    out.touched, out.depth_keys, out.ranges = touched.ctypes.data, keys.ctypes.data, ranges.ctypes.data
+    x0, y0, cw, ch = crop
+    offsets = np.zeros(cw * ch + 1, np.uint32)
+    total = C.c_uint64()
+    p = cloud.struct()
+    _check(lib.ora_train_render(C.byref(projection), C.byref(p), C.byref(settings), C.byref(out), threads, x0, y0, cw,
+                                ch, offsets.ctypes.data, None, 0, C.byref(total)), "train_render")
+    slots = np.zeros(max(1, total.value), np.uint32)
+    out2 = FrameOut()
+    _check(lib.ora_train_render(C.byref(projection), C.byref(p), C.byref(settings), C.byref(out2), threads, x0, y0,
+                                cw, ch, offsets.ctypes.data, slots.ctypes.data, total.value, C.byref(total)),
+           "train_render")
+    return dict(colour=colour, depth=depth, proj=proj, rects=rects, touched=touched, depth_keys=keys, ranges=ranges,
+                pairs=int(out.pairs), visible=int(out.visible), list_offsets=offsets, list_slots=slots[:total.value])

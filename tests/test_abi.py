@@ -51,6 +51,7 @@ int main(void) {
   S(lrt_render_settings) O(lrt_render_settings, time_stages)
   S(lrt_frame_stats) O(lrt_frame_stats, total_ms)
   S(lrt_targets) S(lrt_debug_view) O(lrt_debug_view, visible)
+  S(lrt_train_params) O(lrt_train_params, sh) S(lrt_train_grads) O(lrt_train_grads, sh)
   return 0;
 }
 """
@@ -60,6 +61,7 @@ CTYPES = {
     "lrt_splat_edit": _abi.SplatEdit, "lrt_gpu_splats": _abi.GpuSplatsStruct,
     "lrt_splat_instance": _abi.SplatInstanceStruct, "lrt_render_settings": _abi.RenderSettingsStruct,
     "lrt_frame_stats": _abi.FrameStatsStruct, "lrt_targets": _abi.TargetsStruct, "lrt_debug_view": _abi.DebugView,
+    "lrt_train_params": _abi.TrainParams, "lrt_train_grads": _abi.TrainGrads,
 }
 
 

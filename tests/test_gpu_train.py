@@ -1,0 +1,131 @@
+"""The differentiable path on the GPU through the C-ABI (lrt_rast_train_forward
+/ lrt_rast_train_backward, wrapped in a torch.autograd.Function):
+
+- its forward equals the oracle's restatement of the training
+  parameterisation bit for bit (records, keys, ranges, image);
+- its forward matches the plain forward of the same splats packed (the
+  packed layout quantises rotation to 10 bits and log-scales to f16) within
+  the reference's image tolerances;
+- its gradients equal the FP64 brute-force per-pixel oracle over a 64x64
+  crop (float64 autograd with the frame's discrete choices held fixed) and
+  FP64 central finite differences (h = 1e-4) on 256 random parameters,
+  within 1e-4 relative.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import lucabrtrender_b200 as L
+
+import grad_oracle as G
+import oracle as ora
+import train_fixtures as TF
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-4   # gradient tolerance, relative to the FP64 oracle
+
+
+def to_cuda(p, requires_grad=False):
+    out = {}
+    for k, v in p.items():
+        t = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+        t.requires_grad_(requires_grad)
+        out[k] = t
+    return out
+
+
+def gpu_forward(rasterizer, p, cam, settings, requires_grad=False):
+    t = to_cuda(p, requires_grad)
+    colour, depth = L.rasterize(t["means"], t["log_scales"], t["quats"], t["logits"], t["sh"], cam, settings,
+                                rasterizer)
+    return t, colour, depth
+
+
+@pytest.mark.parametrize("n,size,seed", [(3000, 96, 5), (20000, 200, 6)])
+def test_train_forward_bit_exact(rasterizer, n, size, seed):
+    p = TF.make_params(n, seed)
+    cam, settings = TF.frame(size, size)
+    _, colour, depth = gpu_forward(rasterizer, p, cam, settings)
+    dbg = rasterizer.debug_arrays()
+    pr = L.projection_for(cam, size, size).struct()
+    ref = ora.train_render(pr, TF.raw_cloud(p), settings.struct())
+    assert np.array_equal(dbg["proj"].cpu().numpy().view(np.uint32), ref["proj"].view(np.uint32))
+    assert np.array_equal(dbg["depth_keys"].cpu().numpy().view(np.uint32), ref["depth_keys"])
+    assert np.array_equal(dbg["ranges"].cpu().numpy().view(np.uint32), ref["ranges"])
+    assert np.abs(colour.detach().cpu().numpy() - ref["colour"]).max() <= 1e-5
+    assert np.abs(depth.cpu().numpy() - ref["depth"]).max() <= 1e-5
+
+
+def test_train_forward_matches_the_packed_forward(rasterizer):
+    p = TF.make_params(20000, 7)
+    cam, settings = TF.frame(160, 160)
+    _, colour, _ = gpu_forward(rasterizer, p, cam, settings)
+    packed = L.pack_splats(TF.raw_records(p), 15, 3)
+    targets = L.RenderTargets()
+    rasterizer.render(cam, [L.SplatInstance(L.to_device(packed))], settings, targets)
+    diff = ora.compare_images(colour.detach().cpu().numpy(), targets.colour.cpu().numpy())
+    assert diff.p99 <= 2 and diff.max <= 16, (diff.p99, diff.max)
+
+
+def _crop_problem(p, cam, settings, crop, target):
+    pr = L.projection_for(cam, settings.width, settings.height).struct()
+    st = settings.struct()
+    out = ora.train_render(pr, TF.raw_cloud(p), st, crop)
+    return G.CropProblem(G.camera_from(pr, st), crop, out["list_offsets"], out["list_slots"], target), out
+
+
+def _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target):
+    t, colour, _ = gpu_forward(rasterizer, p, cam, settings, requires_grad=True)
+    x0, y0, w, h = crop
+    tgt = torch.from_numpy(target).cuda()
+    loss = torch.abs(colour[y0:y0 + h, x0:x0 + w, :3] - tgt).sum() / (3.0 * w * h)
+    loss.backward()
+    return {k: v.grad.detach().cpu().numpy() for k, v in t.items()}, float(loss.detach())
+
+
+def test_gradients_match_the_fp64_per_pixel_oracle_on_a_crop(rasterizer):
+    p = TF.make_params(6000, 8)
+    cam, settings = TF.frame(128, 128)
+    crop = (32, 32, 64, 64)
+    target = np.random.default_rng(3).uniform(0, 1, (64, 64, 3))
+    prob, _ = _crop_problem(p, cam, settings, crop, target)
+    want, loss64 = G.gradients(prob, p)
+    got, loss32 = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target)
+    assert abs(loss32 - loss64) <= 1e-5 * max(1.0, abs(loss64))
+    used = prob.used
+    report = {}
+    for name in ("means", "log_scales", "quats", "logits", "sh"):
+        g = got[name].reshape(got[name].shape[0], -1)[used].astype(np.float64)
+        w = want[name].reshape(len(used), -1)
+        err = np.linalg.norm(g - w) / max(np.linalg.norm(w), 1e-30)
+        report[name] = err
+        assert err <= REL, (name, err)
+    # splats no crop pixel sees get exactly zero
+    unused = np.setdiff1d(np.arange(p["means"].shape[0]), used)
+    assert np.all(got["means"][unused] == 0) and np.all(got["logits"][unused] == 0)
+
+
+def test_gradients_match_fp64_finite_differences(rasterizer):
+    p = TF.make_params(6000, 9)
+    cam, settings = TF.frame(128, 128)
+    crop = (32, 32, 64, 64)
+    target = np.random.default_rng(4).uniform(0, 1, (64, 64, 3))
+    prob, _ = _crop_problem(p, cam, settings, crop, target)
+    got, _ = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target)
+    rng = np.random.default_rng(11)
+    names = ["means", "log_scales", "quats", "logits", "sh"]
+    picks = []
+    for _ in range(256):
+        name = names[rng.integers(len(names))]
+        row = int(rng.integers(len(prob.used)))
+        width = int(np.prod(np.asarray(p[name]).shape[1:])) if np.asarray(p[name]).ndim > 1 else 1
+        picks.append((name, row, int(rng.integers(width))))
+    fd = G.finite_difference(prob, p, picks, h=1e-4)
+    gpu = np.array([got[n].reshape(got[n].shape[0], -1)[prob.used[r], c] for n, r, c in picks], np.float64)
+    scale = np.abs(fd).max()
+    err = np.abs(gpu - fd)
+    # per parameter: within REL of its own value or of the largest sampled gradient
+    assert np.all(err <= REL * np.abs(fd) + REL * scale), (err / scale).max()
