@@ -65,17 +65,21 @@ def measured_peaks() -> tuple[float, str]:
 
 
 class Clocks:
-    """nvidia-smi clock samples while the timed region runs."""
+    """nvidia-smi clock samples (every 20 ms) for the whole run; `summary`
+    keeps the samples taken inside the timed windows (widened by 0.25 s, since
+    one timed region can be shorter than the sampling period)."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.windows = []
+        self.lines = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "20"],
@@ -84,8 +88,10 @@ class Clocks:
             self.proc = None
         return self
 
-    def __exit__(self, *exc):
-        self.lines = []
+    def window(self, t0: float, t1: float) -> None:
+        self.windows.append((t0, t1))
+
+    def stop(self):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -96,22 +102,24 @@ class Clocks:
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], 0.0, set()
+        import datetime
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
+        rows = []
+        for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if any(a - 0.25 <= r[0] <= b + 0.25 for a, b in self.windows)]
+        sm = [r[1] for r in inside]
+        reasons = sorted({n for r in inside for n, v in zip(names, r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max((r[2] for r in rows), default=None), "reasons": reasons,
+                "samples": len(sm), "samples_whole_run": len(rows)}
 
 
 def cpu_reference_frames(k_frames: int, threads: int, packed, log=print) -> tuple[float, list]:
@@ -164,6 +172,7 @@ def run_ours(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    clocks = Clocks(local).start()
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
@@ -194,13 +203,14 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    with Clocks(local) as clocks:
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            starts[k].record(stream)
-            stats_list.append(frame(k, stages=True))
-            ends[k].record(stream)
-        torch.cuda.synchronize(dev)
+    w0 = time.time()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        starts[k].record(stream)
+        stats_list.append(frame(k, stages=True))
+        ends[k].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks.window(w0, time.time())
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -220,6 +230,7 @@ def run_ours(args) -> None:
         dist.barrier()
     torch.cuda.synchronize(dev)
     e2e_ms = 0.0
+    w0 = time.time()
     for k in range(args.steps):
         flush.fill_(float(k))
         e_start.record(stream)
@@ -231,11 +242,68 @@ def run_ours(args) -> None:
         e_end.record(stream)
         e_end.synchronize()
         e2e_ms += e_start.elapsed_time(e_end)
+    clocks.window(w0, time.time())
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = e2e_ms / (args.steps * world)
+
+    # --- forward + backward (the differentiable path, same splats and views) ---
+    fwd_bwd = None
+    if not args.no_backward:
+        raw = L.synthetic_records(SPLATS, SEED)
+        keep = raw.shape[0]
+        sh = np.zeros((keep, 16, 3), np.float32)
+        sh[:, 0, :] = raw[:, 11:14]
+        for c in range(3):
+            sh[:, 1:, c] = raw[:, 14 + 15 * c:14 + 15 * (c + 1)]
+        sh = sh.astype(np.float16).astype(np.float32)
+        params = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev).requires_grad_(True) for k, v in (
+            ("means", raw[:, 0:3]), ("log_scales", raw[:, 4:7]), ("quats", raw[:, 7:11]), ("logits", raw[:, 3]),
+            ("sh", sh))}
+        gen = torch.Generator(device=dev).manual_seed(SEED)
+        target = torch.rand((HEIGHT, WIDTH, 3), generator=gen, device=dev)
+        train_settings = L.RenderSettings(width=WIDTH, height=HEIGHT)
+
+        def train_step(k: int):
+            for v in params.values():
+                v.grad = None
+            colour, _ = L.rasterize(params["means"], params["log_scales"], params["quats"], params["logits"],
+                                    params["sh"], projections[(k + rank * 7) % FRAMES], train_settings, raster)
+            loss = torch.abs(colour[..., :3] - target).mean()
+            loss.backward()
+            return loss
+
+        for k in range(max(3, args.warmup)):
+            train_step(k)
+        torch.cuda.synchronize(dev)
+        fb_ms, bwd_blend, bwd_proj = [], [], []
+        w0 = time.time()
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            train_step(k)
+            b.record(stream)
+            b.synchronize()
+            fb_ms.append(a.elapsed_time(b))
+            t_blend, t_proj = L.train.backward_times(raster)
+            bwd_blend.append(t_blend)
+            bwd_proj.append(t_proj)
+        clocks.window(w0, time.time())
+        fb_total = float(sum(fb_ms))
+        if world > 1:
+            t = torch.tensor([fb_total], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            fb_total = float(t.item())
+        fb_value = fb_total / (args.steps * world)
+        fwd_bwd = {"ms_per_view": round(fb_value, 4), "ratio_to_plain_forward": round(fb_value / value, 3),
+                   "backward_blend_ms": round(float(np.mean(bwd_blend)), 4),
+                   "backward_reduce_and_projection_ms": round(float(np.mean(bwd_proj)), 4),
+                   "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels",
+                   "params": "means, log-scales, quaternions, opacity logits, 48 SH (fp16 storage, fp32 gradients)"}
 
     # --- roofline of the dominant kernel, measured live over the timed steps ---
     st = stats_list
@@ -267,6 +335,7 @@ def run_ours(args) -> None:
     sort_gbs = bytes_sort / (stage["tile_sort_ms"] * 1e-3) / 1e9 if stage["tile_sort_ms"] > 0 else None
     launches_per_frame = 1 + 1 + passes + 1 + 1   # project+emit, histogram, digit passes, ranges, blend
 
+    clocks.stop()
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -292,6 +361,7 @@ def run_ours(args) -> None:
             "gpu_launches": launches_per_frame * args.steps,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "fwd_bwd": fwd_bwd,
         }
         print(json.dumps(line), flush=True)
     raster.close()
@@ -308,6 +378,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-frames", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-backward", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -252,10 +252,25 @@ __device__ __forceinline__ float srgb_to_linear_slope(float c) {
 
 constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
 
-__device__ __forceinline__ float warp_sum(float v) {
+// Sum of 16 values over the warp by recursive halving (a reduce-scatter):
+// at each step a lane keeps half of its vector, sends the other half to its
+// partner and adds what it receives, so 8 + 4 + 2 + 1 + 1 = 16 shuffles
+// replace 16 x 5 butterflies. Afterwards lane l holds the warp's sum of
+// value (l >> 1) & 15 (lanes l and l ^ 1 hold the same one).
+__device__ __forceinline__ float warp_reduce_scatter16(float (&v)[16], uint32_t lane) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    return v;
+    for (int level = 0; level < 4; ++level) {
+        const int o = 16 >> level;       // partner distance
+        const int half = 8 >> level;     // values kept
+        const bool upper = (lane & static_cast<uint32_t>(o)) != 0;
+#pragma unroll
+        for (int j = 0; j < half; ++j) {
+            const float send = upper ? v[j] : v[j + half];
+            const float keep = upper ? v[j + half] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 1);
 }
 
 // The backward of blend_kernel<true>: per pixel, the reference's loop run
@@ -362,7 +377,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                 const uint32_t bit = 31u - static_cast<uint32_t>(__clz(todo));
                 todo &= ~(1u << bit);
                 const uint32_t j = static_cast<uint32_t>(c) + bit;
-                float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                float v[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
                 bool hit = false;
                 if (live && bStart + j < myLast) {
                     const float4 screen = sRec[j].screen;
@@ -402,12 +417,16 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                     }
                 }
                 const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
-                if (hits != 0) {
+                if (hits != 0 && (hits & (hits - 1)) == 0) {
+                    // one pixel of the warp: its values are the warp's sums
+                    if (hit) {
 #pragma unroll
-                    for (uint32_t k = 0; k < kGrads; ++k) {
-                        const float sum = warp_sum(v[k]);
-                        if (lane == 0) sPart[warp][j][k] = sum;
+                        for (uint32_t k = 0; k < kGrads; ++k) sPart[warp][j][k] = v[k];
                     }
+                } else if (hits != 0) {
+                    const float sum = warp_reduce_scatter16(v, lane);
+                    const uint32_t idx = (lane >> 1) & 15u;
+                    if ((lane & 1u) == 0 && idx < kGrads) sPart[warp][j][idx] = sum;
                 }
             }
         }

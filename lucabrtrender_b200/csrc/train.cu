@@ -22,8 +22,9 @@ __device__ constexpr float kC3[7] = {-0.5900435899266435f, 2.890611442640554f, -
                           -0.4570457994644658f, 1.445305721320277f, -0.5900435899266435f};
 
 // The 15 rest basis functions (sh.slang:25-51 order) and their gradients.
-__device__ __forceinline__ void sh_basis(float x, float y, float z, uint32_t degree, float b[15], float gx[15],
-                                         float gy[15], float gz[15]) {
+__device__ __forceinline__ void sh_basis(float x, float y, float z, uint32_t degree, float (&b)[15], float (&gx)[15],
+                                         float (&gy)[15], float (&gz)[15]) {
+#pragma unroll
     for (int k = 0; k < 15; ++k) b[k] = gx[k] = gy[k] = gz[k] = 0.0f;
     if (degree == 0) return;
     b[0] = -kC1 * y; gy[0] = -kC1;
@@ -61,14 +62,17 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     const uint32_t slot = f.base + i;
     const uint32_t n = touched[slot];
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
-    float gshv[48];
-    for (int k = 0; k < 48; ++k) gshv[k] = 0.0f;
-    if (n > 0) {
+    float* gshRow = gSh + static_cast<size_t>(i) * 48;
+    if (n == 0) {
+        for (int k = 0; k < 48; ++k) gshRow[k] = 0.0f;
+    } else {
         // The splat's summed partials.
         float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         const float* part = partials + static_cast<size_t>(offsets[slot]) * 9;
-        for (uint32_t k = 0; k < n; ++k)
+        for (uint32_t k = 0; k < n; ++k) {
+#pragma unroll
             for (int c = 0; c < 9; ++c) g[c] += part[k * 9 + c];
+        }
         const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
 
         // ---- forward intermediates ------------------------------------------
@@ -133,25 +137,29 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
         const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
         const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
-        const uint32_t degree = min(3u, f.shLimit);
+        const uint32_t degree = min(3u, f.shLimit);   // bas[] is 0 above it
         float bas[15], bgx[15], bgy[15], bgz[15];
         sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
         float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
+#pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
             constexpr float kSH0 = 0.28209479177387814f;
             const float base = 0.5f + kSH0 * half_to_float(row[ch]);
             float rest = 0.0f;
+#pragma unroll
             for (int k = 0; k < 15; ++k) rest += bas[k] * half_to_float(row[3 + 3 * k + ch]);
-            const float gcol = g[6 + ch];
-            if (base + rest > 0.0f) {
-                gshv[ch] = kSH0 * gcol;
-                for (uint32_t k = 0; k < (degree == 3 ? 15u : degree == 2 ? 8u : degree == 1 ? 3u : 0u); ++k) {
-                    gshv[3 + 3 * k + ch] = bas[k] * gcol;
-                    const float coef = half_to_float(row[3 + 3 * k + ch]) * gcol;
-                    gdx += coef * bgx[k];
-                    gdy += coef * bgy[k];
-                    gdz += coef * bgz[k];
-                }
+            // colour = max(base + rest, 0): no gradient where clamped. Basis
+            // functions above the evaluated degree are 0, so their
+            // coefficients get 0.
+            const float gcol = base + rest > 0.0f ? g[6 + ch] : 0.0f;
+            gshRow[ch] = kSH0 * gcol;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) {
+                gshRow[3 + 3 * k + ch] = bas[k] * gcol;
+                const float coef = half_to_float(row[3 + 3 * k + ch]) * gcol;
+                gdx += coef * bgx[k];
+                gdy += coef * bgy[k];
+                gdz += coef * bgz[k];
             }
         }
         {   // dir = v / |v|, v = p - eye
@@ -261,7 +269,6 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     }
     for (int k = 0; k < 4; ++k) gQuats[4 * i + k] = gq[k];
     gLogits[i] = glog;
-    for (int k = 0; k < 48; ++k) gSh[static_cast<size_t>(i) * 48 + k] = gshv[k];
 }
 
 }  // namespace
