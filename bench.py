@@ -278,7 +278,7 @@ def run_ours(args) -> None:
         for k in range(max(3, args.warmup)):
             train_step(k)
         torch.cuda.synchronize(dev)
-        fb_ms, bwd_blend, bwd_proj = [], [], []
+        fb_ms, bwd_blend, bwd_proj, fwd_stats = [], [], [], []
         w0 = time.time()
         for k in range(args.steps):
             flush.fill_(float(k))
@@ -293,6 +293,13 @@ def run_ours(args) -> None:
             bwd_blend.append(t_blend)
             bwd_proj.append(t_proj)
         clocks.window(w0, time.time())
+        # The forward's stage breakdown, from extra steps that wait per stage
+        # (not part of the timed steps above).
+        train_settings.time_stages = True
+        for k in range(3):
+            train_step(k)
+            fwd_stats.append(raster.last_train_stats)
+        train_settings.time_stages = False
         fb_total = float(sum(fb_ms))
         if world > 1:
             t = torch.tensor([fb_total], device=dev)
@@ -300,6 +307,8 @@ def run_ours(args) -> None:
             fb_total = float(t.item())
         fb_value = fb_total / (args.steps * world)
         fwd_bwd = {"ms_per_view": round(fb_value, 4), "ratio_to_plain_forward": round(fb_value / value, 3),
+                   "forward_stages_ms": {k: round(float(np.mean([getattr(x, k) for x in fwd_stats])), 4)
+                                         for k in ("project_ms", "tile_sort_ms", "blend_ms")},
                    "backward_blend_ms": round(float(np.mean(bwd_blend)), 4),
                    "backward_reduce_and_projection_ms": round(float(np.mean(bwd_proj)), 4),
                    "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels",

@@ -191,7 +191,7 @@ int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
                     const lrt_render_settings* settings, lrt_targets* targets,
                     lrt_frame_stats* stats, void* stream);
 
-int lrt_rast_debug_view(const lrt_rast* rast, lrt_debug_view* out);
+int lrt_rast_debug_view(lrt_rast* rast, lrt_debug_view* out);
 
 /* Camera::lookingAt and projectionFor, in double precision on the host. */
 int lrt_camera_looking_at(const double eye[3], const double target[3], const double up[3],
@@ -218,7 +218,7 @@ typedef struct lrt_train_params {
 } lrt_train_params;
 
 /* Gradients of the same shapes (fp32 throughout; the SH gradient is fp32
- * over the fp16 coefficients). Written, not accumulated. */
+ * over the fp16 coefficients, 16-byte aligned). Written, not accumulated. */
 typedef struct lrt_train_grads {
     void* means;
     void* log_scales;
@@ -229,7 +229,14 @@ typedef struct lrt_train_grads {
 
 /* The training forward: renders `params` (one cloud in world space) like
  * lrt_rast_render and keeps on the handle what lrt_rast_train_backward needs.
- * The parameter buffers must stay unchanged until the backward. */
+ * The parameter buffers must stay unchanged until the backward. The first
+ * call on a handle waits for its frame (sizing the pair buffers, drawing
+ * again if they were short); later calls only enqueue it (unless
+ * settings->time_stages is set), so the caller's loss and the backward can be
+ * queued behind it, and the stats then carry only the splat count. Such a
+ * frame's counts and status are checked by lrt_rast_train_backward, which
+ * returns LRT_OVERFLOW (buffers grown; run the step again) if the frame
+ * emitted more pairs than the buffers held. */
 int lrt_rast_train_forward(lrt_rast* rast, const lrt_projection* projection, const lrt_train_params* params,
                            const lrt_render_settings* settings, lrt_targets* targets, lrt_frame_stats* stats,
                            void* stream);

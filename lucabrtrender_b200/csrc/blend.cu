@@ -251,6 +251,7 @@ __device__ __forceinline__ float srgb_to_linear_slope(float c) {
 }
 
 constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
+constexpr uint32_t kGradStride = 12;   // floats per pair in the partials buffer (three 16-byte vectors)
 
 // Sum of 16 values over the warp by recursive halving (a reduce-scatter):
 // at each step a lane keeps half of its vector, sends the other half to its
@@ -339,6 +340,14 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
     __syncthreads();
     const uint32_t maxLast = sMaxLast;
     bool live = inside && myLast > start;
+    // Pairs past every pixel's last contributor get zero partials here, so the
+    // buffer needs no clearing beforehand.
+    for (uint32_t k = maxLast + tid; k < range.y; k += kBlendThreads) {
+        float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(emit[k]) * kGradStride);
+        out[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        out[1] = out[0];
+        out[2] = out[0];
+    }
     float Br = 0.0f, Bg = 0.0f, Bb = 0.0f;
     const float pxf = static_cast<float>(px) + 0.5f;
     const float pyf = static_cast<float>(py) + 0.5f;
@@ -359,11 +368,14 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
         for (int c = static_cast<int>((cnt - 1) & ~31u); c >= 0; c -= 32) {
             const unsigned any = __ballot_sync(0xFFFFFFFFu, live);
             if (any == 0) break;
+            // Lanes whose pixel stopped before this chunk take no part in it.
+            const bool here = live && myLast > bStart + static_cast<uint32_t>(c);
+            if (__ballot_sync(0xFFFFFFFFu, here) == 0) continue;
             const uint32_t big = 0xFFFFFFFFu;
-            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, live ? px : big);
-            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, live ? px : 0u);
-            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, live ? py : big);
-            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, live ? py : 0u);
+            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, here ? px : big);
+            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, here ? px : 0u);
+            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, here ? py : big);
+            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, here ? py : 0u);
             const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
             const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
             bool overlap = false;
@@ -391,27 +403,32 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                         const float alpha = fminf(0.99f, raw);
                         if (!(alpha < 1.0f / 255.0f)) {
                             hit = true;
+                            // Gradients are checked against FP64 to a tolerance, not
+                            // bit for bit, so this part uses fused multiply-adds.
                             const float4 col = sRec[j].colour;
                             const float oneMinus = 1.0f - alpha;
-                            const float Ti = T / oneMinus;
+                            const float inv = __frcp_rn(oneMinus);
+                            const float Ti = T * inv;
                             const float w = Ti * alpha;
                             v[6] = gr * w;
                             v[7] = gg * w;
                             v[8] = gb * w;
-                            const float dAlpha = Ti * (gr * (col.x - Br) + gg * (col.y - Bg) + gb * (col.z - Bb)) -
-                                                 gT * Tfinal / oneMinus;
-                            Br = alpha * col.x + oneMinus * Br;
-                            Bg = alpha * col.y + oneMinus * Bg;
-                            Bb = alpha * col.z + oneMinus * Bb;
+                            const float behind =
+                                __fmaf_rn(gr, col.x - Br, __fmaf_rn(gg, col.y - Bg, gb * (col.z - Bb)));
+                            const float dAlpha = __fmaf_rn(Ti, behind, -gT * Tfinal * inv);
+                            Br = __fmaf_rn(alpha, col.x - Br, Br);
+                            Bg = __fmaf_rn(alpha, col.y - Bg, Bg);
+                            Bb = __fmaf_rn(alpha, col.z - Bb, Bb);
                             T = Ti;
                             if (raw <= 0.99f) {
                                 v[5] = dAlpha * e;
                                 const float dPower = -0.5f * alpha * dAlpha;
-                                v[2] = dPower * dx * dx;
-                                v[3] = dPower * 2.0f * dx * dy;
-                                v[4] = dPower * dy * dy;
-                                v[0] = -dPower * (2.0f * conic.x * dx + 2.0f * conic.y * dy);
-                                v[1] = -dPower * (2.0f * conic.y * dx + 2.0f * conic.z * dy);
+                                const float pdx = dPower * dx, pdy = dPower * dy;
+                                v[2] = pdx * dx;
+                                v[3] = 2.0f * pdx * dy;
+                                v[4] = pdy * dy;
+                                v[0] = -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
+                                v[1] = -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
                             }
                         }
                     }
@@ -432,14 +449,16 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
         }
         __syncthreads();
         if (tid < cnt) {
-            float* out = partials + static_cast<size_t>(sEmit[tid]) * kGrads;
+            float sum[kGradStride] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
             for (uint32_t k = 0; k < kGrads; ++k) {
-                float sum = 0.0f;
 #pragma unroll
-                for (uint32_t w = 0; w < kBlendThreads / 32; ++w) sum += sPart[w][tid][k];
-                out[k] = sum;
+                for (uint32_t w = 0; w < kBlendThreads / 32; ++w) sum[k] += sPart[w][tid][k];
             }
+            float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(sEmit[tid]) * kGradStride);
+            out[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
+            out[1] = make_float4(sum[4], sum[5], sum[6], sum[7]);
+            out[2] = make_float4(sum[8], 0.0f, 0.0f, 0.0f);
         }
         __syncthreads();
         bEnd = bStart;

@@ -45,6 +45,9 @@ struct lrt_rast {
     // Training: what the backward pass needs from its forward.
     DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
     bool trainReady = false;
+    bool trainPending = false;   // the forward's counts and status are not read yet
+    cudaStream_t pendingStream = nullptr;
+    bool trainSized = false;     // a training frame has run with a wait
     lrt_train_params trainParams{};
     lrt::FrameParams trainFrame{};
     lrt::BlendParams trainBlend{};
@@ -279,9 +282,12 @@ FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s,
 // One frame, TileRasterizer.cpp:188-484 in this build's stage order. `train`
 // selects the training variants (emit indices carried through the sort,
 // per-slot pair offsets, per-pixel blend state for the backward pass).
+// `deferred`: enqueue the frame and return without waiting (training frames
+// after the first); the counts and status arrive in pinned memory and the
+// backward pass checks them.
 int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudDesc>& clouds,
                  const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr,
-                 bool train, std::chrono::steady_clock::time_point frameStart) {
+                 bool train, std::chrono::steady_clock::time_point frameStart, bool deferred = false) {
     if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
     if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
         targets->depth == nullptr)
@@ -433,6 +439,36 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         }
         LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
         LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "readback");
+        if (deferred) {
+            r->debug.proj = r->proj.ptr;
+            r->debug.rects = r->rects.ptr;
+            r->debug.touched = r->touched.ptr;
+            r->debug.depth_keys = r->keys.ptr;
+            r->debug.pairs = sorted;
+            r->debug.ranges = r->ranges.ptr;
+            r->debug.slots = slots;
+            r->debug.tiles = tiles;
+            r->debug.slot_bits = slotBits;
+            r->debug.depth_bits = 24;
+            r->debug.tile_bits = tileBits;
+            r->pendingStream = stream;
+            if (train) {
+                r->trainFrame = lastParams;
+                r->trainBlend = bp;
+                r->trainSorted = sorted;
+                r->trainSortedValues = sortedValues;
+                r->trainPairs = r->pairCap;   // an upper bound until the status is read
+                r->trainReady = true;
+                r->trainPending = true;
+            }
+            if (stats != nullptr) {
+                std::memset(stats, 0, sizeof(*stats));
+                stats->splats = slots;
+                stats->total_ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - frameStart).count();
+            }
+            return LRT_OK;
+        }
         LRT_CUDA(r, cudaStreamSynchronize(stream), "frame");
         visible = r->hostCounters[0];
         pairs = r->hostCounters[1];
@@ -457,6 +493,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     r->debug.tile_bits = tileBits;
     r->debug.visible = visible;
     r->trainReady = false;
+    r->trainPending = false;
     if (train) {
         r->trainFrame = lastParams;
         r->trainBlend = bp;
@@ -537,7 +574,13 @@ int lrt_rast_train_forward(lrt_rast* r, const lrt_projection* pr, const lrt_trai
         clouds.push_back(d);
     }
     r->trainParams = *params;
-    return render_frame(r, pr, clouds, s, targets, stats, streamPtr, true, frameStart);
+    // The first training frame waits (and redraws if its pairs overflowed) so
+    // that the pair buffers are sized; later ones are only enqueued, unless
+    // stage times are asked for.
+    const bool deferred = r->trainSized && !s->time_stages;
+    const int code = render_frame(r, pr, clouds, s, targets, stats, streamPtr, true, frameStart, deferred);
+    if (code == LRT_OK && !deferred) r->trainSized = true;
+    return code;
 }
 
 int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads* grads, void* streamPtr) {
@@ -549,11 +592,14 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
     if (p.count > 0 && (grads->means == nullptr || grads->log_scales == nullptr || grads->quats == nullptr ||
                         grads->opacity_logits == nullptr || grads->sh == nullptr))
         return fail(r, LRT_INVALID_ARGUMENT, "a null gradient buffer");
+    if ((reinterpret_cast<uintptr_t>(grads->sh) & 15u) != 0)
+        return fail(r, LRT_INVALID_ARGUMENT, "the SH gradient must be 16-byte aligned");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
-    const size_t partialBytes = std::max<size_t>(size_t{r->trainPairs} * 9 * sizeof(float), 16);
+    // Every pair's partials are written by the blend backward (zeros for those
+    // it does not walk), so the buffer is not cleared.
+    const size_t partialBytes = std::max<size_t>(size_t{r->trainPairs} * 12 * sizeof(float), 16);
     LRT_CUDA(r, ensure(r->partials, partialBytes), "partials");
-    LRT_CUDA(r, cudaMemsetAsync(r->partials.ptr, 0, partialBytes, stream), "partials");
     LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
     LRT_CUDA(r,
              lrt::launch_blend_backward(r->trainBlend, static_cast<uint2*>(r->ranges.ptr), r->trainSorted,
@@ -576,6 +622,21 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
              "projection backward");
     LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
     LRT_CUDA(r, cudaStreamSynchronize(stream), "backward");
+    if (r->trainPending) {
+        // The forward ran without waiting: its status is read here.
+        r->trainPending = false;
+        const uint32_t pairs = r->hostCounters[1], status = r->hostCounters[2];
+        r->trainPairs = pairs;
+        r->debug.pairs_count = pairs;
+        r->debug.visible = r->hostCounters[0];
+        if (pairs > r->pairCap) {
+            r->pairCap = grow(r->pairCap, pairs);
+            r->trainReady = false;
+            return fail(r, LRT_OVERFLOW, "the training forward emitted more pairs than its buffer held; "
+                                         "the buffers are grown, run the step again");
+        }
+        if (status & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+    }
     r->lastBackwardMs[0] = event_ms(r->ev[4], r->ev[5]);
     r->lastBackwardMs[1] = event_ms(r->ev[5], r->ev[6]);
     return LRT_OK;
@@ -588,8 +649,14 @@ int lrt_rast_backward_times(const lrt_rast* r, double* blendMs, double* projectM
     return LRT_OK;
 }
 
-int lrt_rast_debug_view(const lrt_rast* r, lrt_debug_view* out) {
+int lrt_rast_debug_view(lrt_rast* r, lrt_debug_view* out) {
     if (r == nullptr || out == nullptr) return LRT_INVALID_ARGUMENT;
+    if (r->trainPending) {   // an enqueued training frame: wait for its counts
+        DeviceScope scope(r->device);
+        LRT_CUDA(r, cudaStreamSynchronize(r->pendingStream), "frame");
+        r->debug.visible = r->hostCounters[0];
+        r->debug.pairs_count = std::min(r->hostCounters[1], r->pairCap);
+    }
     *out = r->debug;
     return LRT_OK;
 }

@@ -64,14 +64,18 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
     float* gshRow = gSh + static_cast<size_t>(i) * 48;
     if (n == 0) {
-        for (int k = 0; k < 48; ++k) gshRow[k] = 0.0f;
+        float4* out = reinterpret_cast<float4*>(gshRow);
+#pragma unroll
+        for (int q = 0; q < 12; ++q) out[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
         // The splat's summed partials.
         float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const float* part = partials + static_cast<size_t>(offsets[slot]) * 9;
+        const float4* part = reinterpret_cast<const float4*>(partials) + static_cast<size_t>(offsets[slot]) * 3;
         for (uint32_t k = 0; k < n; ++k) {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) g[c] += part[k * 9 + c];
+            const float4 a = part[3 * k], b = part[3 * k + 1], c = part[3 * k + 2];
+            g[0] += a.x; g[1] += a.y; g[2] += a.z; g[3] += a.w;
+            g[4] += b.x; g[5] += b.y; g[6] += b.z; g[7] += b.w;
+            g[8] += c.x;
         }
         const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
 
@@ -133,7 +137,20 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         const float QA = c / det, QB = -b / det, QC = a / det;
 
         // ---- colour ---------------------------------------------------------------
-        const uint16_t* row = sh + static_cast<size_t>(i) * 48;
+        float coef[48];   // the fp16 coefficients, read as six 16-byte vectors
+        {
+            const uint4* rv = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(i) * 48);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const uint4 w4 = __ldg(rv + q);
+                const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    coef[q * 8 + 2 * h] = low_half(ws[h]);
+                    coef[q * 8 + 2 * h + 1] = high_half(ws[h]);
+                }
+            }
+        }
         float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
         const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
         const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
@@ -141,26 +158,32 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         float bas[15], bgx[15], bgy[15], bgz[15];
         sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
         float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
+        float gsh[48];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
             constexpr float kSH0 = 0.28209479177387814f;
-            const float base = 0.5f + kSH0 * half_to_float(row[ch]);
+            const float base = 0.5f + kSH0 * coef[ch];
             float rest = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 15; ++k) rest += bas[k] * half_to_float(row[3 + 3 * k + ch]);
+            for (int k = 0; k < 15; ++k) rest += bas[k] * coef[3 + 3 * k + ch];
             // colour = max(base + rest, 0): no gradient where clamped. Basis
             // functions above the evaluated degree are 0, so their
             // coefficients get 0.
             const float gcol = base + rest > 0.0f ? g[6 + ch] : 0.0f;
-            gshRow[ch] = kSH0 * gcol;
+            gsh[ch] = kSH0 * gcol;
 #pragma unroll
             for (int k = 0; k < 15; ++k) {
-                gshRow[3 + 3 * k + ch] = bas[k] * gcol;
-                const float coef = half_to_float(row[3 + 3 * k + ch]) * gcol;
-                gdx += coef * bgx[k];
-                gdy += coef * bgy[k];
-                gdz += coef * bgz[k];
+                gsh[3 + 3 * k + ch] = bas[k] * gcol;
+                const float cg = coef[3 + 3 * k + ch] * gcol;
+                gdx += cg * bgx[k];
+                gdy += cg * bgy[k];
+                gdz += cg * bgz[k];
             }
+        }
+        {
+            float4* out = reinterpret_cast<float4*>(gshRow);
+#pragma unroll
+            for (int q = 0; q < 12; ++q) out[q] = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
         }
         {   // dir = v / |v|, v = p - eye
             const float dotd = gdx * dirx + gdy * diry + gdz * dirz;

@@ -43,7 +43,7 @@ class _Rasterize(torch.autograd.Function):
         raster._check(_abi.load().lrt_rast_train_forward(raster._handle, C.byref(pr), C.byref(p), C.byref(st),
                                                          C.byref(t), C.byref(stats), _stream_ptr(None)))
         ctx.raster = raster
-        ctx.stats = FrameStats.from_struct(stats)
+        raster.last_train_stats = FrameStats.from_struct(stats)
         # The handle keeps pointers to these until the backward.
         ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh16)
         ctx.mark_non_differentiable(depth)
