@@ -193,6 +193,41 @@ int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
 
 int lrt_rast_debug_view(lrt_rast* rast, lrt_debug_view* out);
 
+/* One view of a batch: its projection, size and caller-owned device images
+ * (colour float4 and depth float, width * height, bottom row first). */
+typedef struct lrt_view {
+    lrt_projection projection;
+    uint32_t width, height;
+    void* colour;
+    void* depth;
+} lrt_view;
+
+/* How a batch was run: views per chunk (each chunk is one projection pass,
+ * one sort and one persistent blend launch) and blend blocks per SM, chosen
+ * by the autotuner on the first batch of a given shape; whether the chunks
+ * were replayed from a captured CUDA graph. */
+typedef struct lrt_batch_stats {
+    uint32_t views, splats, pairs, chunks;
+    uint32_t views_per_chunk, blend_blocks_per_sm, graph_replayed, reserved;
+    double device_ms;   /* CUDA-event time of the batch on the device */
+    double total_ms;    /* host wall time of the call */
+} lrt_batch_stats;
+
+/* Many views of the same instances in one call (no reference counterpart:
+ * the reference renders one view per call). Every view is the frame
+ * lrt_rast_render would draw -- the same pixels, bit for bit -- with the
+ * settings' width and height replaced by the view's. Each chunk of views is
+ * projected view by view into one pair buffer whose tile ids number the
+ * chunk's tiles one view after another, sorted once, and blended by one
+ * persistent launch that takes (view, tile) work items from a queue. The
+ * first batch of a given shape (view count and sizes, splat count) is timed
+ * under a few chunk sizes and blend grid sizes and the fastest kept; the
+ * next one is captured into a CUDA graph, and later ones replay it with the
+ * new cameras. Returns when the batch is done. */
+int lrt_rast_render_batch(lrt_rast* rast, const lrt_splat_instance* instances, uint32_t instance_count,
+                          const lrt_view* views, uint32_t view_count, const lrt_render_settings* settings,
+                          lrt_batch_stats* stats, void* stream);
+
 /* Camera::lookingAt and projectionFor, in double precision on the host. */
 int lrt_camera_looking_at(const double eye[3], const double target[3], const double up[3],
                           lrt_camera* out);

@@ -37,7 +37,7 @@ EXPORTS = (
     "lrt_abi_version", "lrt_rast_create", "lrt_rast_destroy", "lrt_rast_last_error", "lrt_rast_render",
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
     "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
-    "lrt_rast_train_backward", "lrt_rast_backward_times",
+    "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -122,6 +122,19 @@ class DebugView(C.Structure):
     ]
 
 
+class View(C.Structure):
+    _fields_ = [("projection", Projection), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("colour", C.c_void_p), ("depth", C.c_void_p)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("views", C.c_uint32), ("splats", C.c_uint32), ("pairs", C.c_uint32), ("chunks", C.c_uint32),
+        ("views_per_chunk", C.c_uint32), ("blend_blocks_per_sm", C.c_uint32), ("graph_replayed", C.c_uint32),
+        ("reserved", C.c_uint32), ("device_ms", C.c_double), ("total_ms", C.c_double),
+    ]
+
+
 class TrainParams(C.Structure):
     _fields_ = [
         ("count", C.c_uint32), ("reserved", C.c_uint32),
@@ -173,6 +186,9 @@ def load() -> C.CDLL:
                                            C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
                                            C.POINTER(FrameStatsStruct), C.c_void_p]
     lib.lrt_rast_train_backward.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TrainGrads), C.c_void_p]
+    lib.lrt_rast_render_batch.argtypes = [C.c_void_p, C.POINTER(SplatInstanceStruct), C.c_uint32, C.POINTER(View),
+                                          C.c_uint32, C.POINTER(RenderSettingsStruct), C.POINTER(BatchStats),
+                                          C.c_void_p]
     lib.lrt_rast_backward_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if lib.lrt_abi_version() != ABI_VERSION:
         raise RuntimeError(f"ABI version mismatch: library {lib.lrt_abi_version()}, bindings {ABI_VERSION}")

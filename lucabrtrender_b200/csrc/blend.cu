@@ -115,29 +115,22 @@ __device__ __forceinline__ float4 cull_box(const ProjRecord& rec) {
 // the final transmittance, and one past the last pair that contributed --
 // what the backward pass re-blends from.
 template <bool kTrain>
-__global__ void __launch_bounds__(kBlendThreads)
-blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
-             const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
-             float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
-    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
-    __shared__ __align__(16) float4 sBox[kBatch];
-    __shared__ __align__(8) uint64_t sBar[2];
+__device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
+                                           const uint2* __restrict__ ranges,
+                                           const unsigned long long* __restrict__ pairs,
+                                           const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut,
+                                           float* __restrict__ depthOut, float4* __restrict__ pixState,
+                                           uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
+                                           ProjRecord (&sRec)[2][kBatch], float4 (&sBox)[kBatch],
+                                           uint64_t (&sBar)[2], uint32_t& phase0, uint32_t& phase1) {
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x;
-    const uint32_t tx = tile % bp.tilesX, ty = tile / bp.tilesX;
     const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
     const bool inside = px < bp.width && py < bp.height;
     const uint2 range = ranges[tile];
     const uint32_t start = range.x, end = range.y;
     const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
-    if (tid == 0) {
-        mbar_init(&sBar[0], 1);
-        mbar_init(&sBar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
 
     auto issue = [&](uint32_t buf, uint32_t at) {
         const uint32_t cnt = min(kBatch, end - at);
@@ -157,7 +150,6 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     float depthAt = -1.0f;
     bool done = !inside;
     uint32_t last = start;
-    uint32_t phase0 = 0, phase1 = 0;
     if (start < end) issue(0, start);
     uint32_t k = 0;
     for (uint32_t at = start; at < end; at += kBatch, ++k) {
@@ -219,8 +211,11 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
         }
         if (__syncthreads_and(done ? 1 : 0)) {
             if (more) {
+                // Drain the batch already in flight, and count its phase: a
+                // persistent block blends its next tile with the same barriers.
                 const uint32_t nb = buf ^ 1u;
                 if (!mbar_wait(&sBar[nb], nb == 0 ? phase0 : phase1)) atomicOr(err, kErrTimeout);
+                if (nb == 0) phase0 ^= 1u; else phase1 ^= 1u;
             }
             break;
         }
@@ -239,6 +234,67 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     if (kTrain) {
         pixState[pix] = make_float4(r, g, b, T);
         pixLast[pix] = last;
+    }
+}
+
+
+template <bool kTrain>
+__global__ void __launch_bounds__(kBlendThreads)
+blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+             const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
+             float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
+    __shared__ __align__(16) float4 sBox[kBatch];
+    __shared__ __align__(8) uint64_t sBar[2];
+    if (threadIdx.x == 0) {
+        mbar_init(&sBar[0], 1);
+        mbar_init(&sBar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t phase0 = 0, phase1 = 0;
+    const uint32_t tile = blockIdx.x;
+    blend_tile<kTrain>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, proj, colourOut, depthOut,
+                       pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
+}
+
+// Many views in one launch: a persistent grid whose blocks take (view, tile)
+// work items from a queue in order -- the views' tiles numbered one after
+// another, largest views first -- and blend each as blend_kernel does.
+__global__ void __launch_bounds__(kBlendThreads)
+blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_t viewCount,
+                   const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+                   const ProjRecord* __restrict__ proj, uint32_t totalTiles, uint32_t* __restrict__ queue,
+                   uint32_t* __restrict__ err) {
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
+    __shared__ __align__(16) float4 sBox[kBatch];
+    __shared__ __align__(8) uint64_t sBar[2];
+    __shared__ uint32_t sItem;
+    if (threadIdx.x == 0) {
+        mbar_init(&sBar[0], 1);
+        mbar_init(&sBar[1], 1);
+        mbar_fence_init();
+    }
+    uint32_t phase0 = 0, phase1 = 0;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) sItem = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t item = sItem;
+        if (item >= totalTiles) break;
+        uint32_t lo = 0, hi = viewCount;   // the view whose tiles hold `item`
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (views[mid].tileBase <= item) lo = mid; else hi = mid;
+        }
+        const ViewParams v = views[lo];
+        BlendParams vbp = bp;
+        vbp.width = v.width;
+        vbp.height = v.height;
+        vbp.tilesX = v.tilesX;
+        const uint32_t local = item - v.tileBase;
+        blend_tile<false>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, proj + v.recordBase,
+                          v.colour, v.depth, nullptr, nullptr, err, sRec, sBox, sBar, phase0, phase1);
     }
 }
 
@@ -482,6 +538,15 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
     if (tiles == 0) return cudaSuccess;
     blend_kernel<false><<<tiles, kBlendThreads, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, nullptr, nullptr, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
+                               const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
+                               uint32_t* err, uint32_t blocks, cudaStream_t stream) {
+    if (totalTiles == 0) return cudaSuccess;
+    blend_batch_kernel<<<blocks, kBlendThreads, 0, stream>>>(
+        bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, totalTiles, queue, err);
     return cudaGetLastError();
 }
 

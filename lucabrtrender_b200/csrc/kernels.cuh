@@ -11,6 +11,7 @@ namespace lrt {
 struct FrameParams;
 struct BlendParams;
 struct ProjRecord;
+struct ViewParams;
 
 // Projection fused with the touched counts, their prefix and the pair words.
 // counters: [0] visible (added to), [1] pairs (written by the frame's last
@@ -22,7 +23,8 @@ size_t project_status_bytes(uint32_t partitions);
 cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
                                 ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                 uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
-                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream);
+                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
+                                const FrameParams* fDev = nullptr);
 
 // The same for the differentiable parameters (means float3, log-scales
 // float3, quaternions w x y z, opacity logits, SH fp16 [16][3]); also writes
@@ -52,6 +54,11 @@ cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream);
 
+// The views' tiles in one persistent launch; `queue` is a zeroed counter and
+// `blocks` the grid size (a multiple of the SM count).
+cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
+                               const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
+                               uint32_t* err, uint32_t blocks, cudaStream_t stream);
 cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
                                float4* colour, float* depth, float4* pixState, uint32_t* pixLast, uint32_t* err,
                                cudaStream_t stream);

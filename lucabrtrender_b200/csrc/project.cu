@@ -293,7 +293,8 @@ struct PairSink {
 
 template <class Src>
 __global__ void __launch_bounds__(kProjectThreads)
-project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWords, uint32_t shVector,
+project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
+                    uint32_t stageWords, uint32_t shVector,
                     ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
                     uint32_t* __restrict__ keysOut, uint32_t* __restrict__ counters, uint64_t* __restrict__ status,
                     uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits,
@@ -308,11 +309,18 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
     __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
     __shared__ uint32_t sWidth[kProjectThreads];
     __shared__ unsigned long long sBase;
+    // The frame's parameters: by value, or (when a captured graph replays a
+    // batch with new cameras) read from device memory, once per block.
+    __shared__ FrameParams sF;
     uint32_t* err = counters + 2;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
-    if (tid == 0) sPart = atomicAdd(ticket, 1u);
+    if (tid == 0) {
+        sPart = atomicAdd(ticket, 1u);
+        sF = fDev != nullptr ? *fDev : fArg;
+    }
     __syncthreads();
+    const FrameParams& f = sF;
     const uint32_t part = sPart;
     const uint32_t blockStart = part * kProjectThreads;
     const uint32_t i = blockStart + tid;
@@ -474,7 +482,8 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
     if (stageWords != 0) cp_async_wait_all();
     __syncthreads();
 
-    const uint32_t slot = f.base + i;
+    const uint32_t slot = f.base + i;          // the slot in its view (pair words carry this)
+    const uint32_t record = f.recordBase + slot;
     uint32_t key = 0x00FFFFFFu;
     if (inRange) {
         if (alive) {
@@ -496,8 +505,8 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
             rec.screen = make_float4(cx, cy, t.z, cutoff);
             rec.conic = make_float4(ca, cb, cc, alpha);
             rec.colour = make_float4(colour.x, colour.y, colour.z, 0.0f);
-            proj[slot] = rec;
-            rects[slot] = rect;
+            proj[record] = rec;
+            if (f.writeDebug) rects[record] = rect;
             key = float_bits(t.z) >> 7;
         } else {
             // splat_project.slang:39-49, plus a zeroed record
@@ -505,11 +514,11 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
             rec.screen = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             rec.conic = rec.screen;
             rec.colour = rec.screen;
-            proj[slot] = rec;
-            rects[slot] = make_uint4(1, 1, 0, 0);
+            proj[record] = rec;
+            if (f.writeDebug) rects[record] = make_uint4(1, 1, 0, 0);
         }
-        touchedOut[slot] = touched;
-        keysOut[slot] = key;
+        if (f.writeDebug || train.offsets != nullptr) touchedOut[record] = touched;
+        if (f.writeDebug) keysOut[record] = key;
     }
     const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, inRange && alive);
     if (lane == 0 && ballot != 0) atomicAdd(counters, static_cast<uint32_t>(__popc(ballot)));
@@ -584,7 +593,7 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
         const uint32_t tx = (sRect[s] & 0xFFFFu) + bit % w;
         const uint32_t ty = (sRect[s] >> 16) + bit / w;
         sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
-                 (static_cast<unsigned long long>(ty * f.tilesX + tx) << tileShift) | sLow[s]);
+                 (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s]);
     }
     // Larger splats: their warp repeats the tile test 32 tiles at a time.
     uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && area > kMaskArea);
@@ -607,7 +616,7 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
             const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
             if (hit) {
                 sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
-                         (static_cast<unsigned long long>(ty * f.tilesX + tx) << tileShift) | low);
+                         (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | low);
             }
             at += static_cast<uint32_t>(__popc(bal));
         }
@@ -615,7 +624,8 @@ project_emit_kernel(FrameParams f, Src src, TrainOutputs train, uint32_t stageWo
 }
 
 template <class Src>
-cudaError_t launch(const FrameParams& f, const Src& src, TrainOutputs train, bool stage, ProjRecord* proj, uint4* rects,
+cudaError_t launch(const FrameParams& f, const FrameParams* fDev, const Src& src, TrainOutputs train, bool stage,
+                   ProjRecord* proj, uint4* rects,
                    uint32_t* touched, uint32_t* keys, uint32_t* counters, uint64_t* status, uint32_t* ticket,
                    uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs,
                    uint32_t capacity, cudaStream_t stream) {
@@ -627,7 +637,7 @@ cudaError_t launch(const FrameParams& f, const Src& src, TrainOutputs train, boo
     if (e != cudaSuccess) return e;
     const uint32_t blocks = project_partitions(f.count);
     project_emit_kernel<Src><<<blocks, kProjectThreads, smem, stream>>>(
-        f, src, train, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket, partitionBase,
+        f, fDev, src, train, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket, partitionBase,
         lastPartition, slotBits, reinterpret_cast<unsigned long long*>(pairs), capacity);
     return cudaGetLastError();
 }
@@ -640,13 +650,15 @@ uint32_t project_partitions(uint32_t count) { return (count + kProjectThreads - 
 cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
                                 ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                 uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
-                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream) {
+                                uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
+                                const FrameParams* fDev) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
-    return launch(f, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr}, stage, proj, rects, touched,
-                  keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity, stream);
+    return launch(f, fDev, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr}, stage, proj, rects,
+                  touched, keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity,
+                  stream);
 }
 
 cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, const float* logScales,
@@ -657,7 +669,7 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       uint32_t capacity, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     // The DC triple is read from the staged row too, so it is always staged.
-    return launch(f, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
+    return launch(f, nullptr, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
                   TrainOutputs{offsets, values}, true, proj, rects, touched, keys, counters, status, ticket,
                   partitionBase, lastPartition, slotBits, pairs, capacity, stream);
 }

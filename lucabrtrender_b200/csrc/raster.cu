@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 struct DeviceBuffer {
@@ -55,6 +56,21 @@ struct lrt_rast {
     const uint32_t* trainSortedValues = nullptr;
     uint32_t trainPairs = 0;
     double lastBackwardMs[2] = {0.0, 0.0};
+    // Batches of views.
+    struct Batch {
+        cudaStream_t stream = nullptr;
+        cudaEvent_t in = nullptr, out = nullptr, start = nullptr, end = nullptr;
+        DeviceBuffer records, ranges, params, counters, queue;
+        void* hostParams = nullptr;   // pinned: FrameParams per (view, instance), then ViewParams per view
+        size_t hostParamsBytes = 0;
+        uint32_t* hostCounters = nullptr;   // pinned: 4 words per chunk
+        uint32_t hostCounterChunks = 0;
+        uint64_t generation = 0;            // bumped whenever a buffer the graph uses moves
+        cudaGraphExec_t graph = nullptr;
+        uint64_t graphKey = 0, graphGeneration = 0;
+        bool graphFailed = false;
+        std::vector<std::pair<uint64_t, std::pair<uint32_t, uint32_t>>> tuned;   // shape -> (views per chunk, blocks/SM)
+    } batch;
 };
 
 namespace {
@@ -207,6 +223,14 @@ void lrt_rast_destroy(lrt_rast* r) {
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
     for (auto& e : r->ev)
         if (e != nullptr) cudaEventDestroy(e);
+    auto& B = r->batch;
+    for (DeviceBuffer* b : {&B.records, &B.ranges, &B.params, &B.counters, &B.queue}) release(*b);
+    if (B.hostParams != nullptr) cudaFreeHost(B.hostParams);
+    if (B.hostCounters != nullptr) cudaFreeHost(B.hostCounters);
+    if (B.graph != nullptr) cudaGraphExecDestroy(B.graph);
+    for (cudaEvent_t e : {B.in, B.out, B.start, B.end})
+        if (e != nullptr) cudaEventDestroy(e);
+    if (B.stream != nullptr) cudaStreamDestroy(B.stream);
     delete r;
 }
 
@@ -259,6 +283,7 @@ FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s,
         f.shWords = c.packed->sh_words;
     }
     f.shLimit = s->max_sh_degree;
+    f.writeDebug = 1;
     if (c.edit != nullptr) {
         const lrt_splat_edit& e = *c.edit;
         f.edit.active = e.active;
@@ -731,3 +756,422 @@ int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32
 }
 
 }  // extern "C"
+
+// --------------------------------------------------------------- batches ----
+namespace {
+
+struct BatchShape {
+    std::vector<uint32_t> order;   // views, largest first
+    uint32_t slots = 0, launchesPerView = 0;
+    uint64_t key = 0;
+};
+
+uint64_t mix(uint64_t h, uint64_t v) {
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    return h;
+}
+
+// Grows a buffer and, when it moves, invalidates the batch graph.
+cudaError_t ensure_batch(lrt_rast* r, DeviceBuffer& b, size_t bytes) {
+    if (b.bytes >= bytes && b.ptr != nullptr) return cudaSuccess;
+    r->batch.generation += 1;
+    return ensure(b, bytes);
+}
+
+// Enqueues the whole batch (all chunks) on the batch stream. Host-side
+// parameters must already be in batch.hostParams; the first operation copies
+// them to the device, so a captured graph replays with whatever cameras the
+// pinned buffer holds at launch.
+int enqueue_batch(lrt_rast* r, const std::vector<CloudDesc>& clouds, const lrt_view* views, const BatchShape& shape,
+                  const lrt_render_settings* s, uint32_t perChunk, uint32_t blocksPerSM, uint32_t numSMs) {
+    auto& B = r->batch;
+    const uint32_t nViews = static_cast<uint32_t>(shape.order.size());
+    const uint32_t nLaunch = nViews * shape.launchesPerView;
+    const size_t paramsBytes = size_t{nLaunch} * sizeof(FrameParams) + size_t{nViews} * sizeof(lrt::ViewParams);
+    LRT_CUDA(r, cudaMemcpyAsync(B.params.ptr, B.hostParams, paramsBytes, cudaMemcpyHostToDevice, B.stream), "params");
+    const FrameParams* devF = static_cast<const FrameParams*>(B.params.ptr);
+    const lrt::ViewParams* devV = reinterpret_cast<const lrt::ViewParams*>(static_cast<const char*>(B.params.ptr) +
+                                                                          size_t{nLaunch} * sizeof(FrameParams));
+    const FrameParams* hostF = static_cast<const FrameParams*>(B.hostParams);
+    const lrt::ViewParams* hostV = reinterpret_cast<const lrt::ViewParams*>(static_cast<const char*>(B.hostParams) +
+                                                                           size_t{nLaunch} * sizeof(FrameParams));
+    const uint32_t slotBits = bits_for(std::max<uint32_t>(shape.slots, 1));
+    BlendParams bp{};
+    bp.slotBits = slotBits;
+    bp.tileShift = 24 + slotBits;
+    bp.depthMode = s->depth_mode;
+    bp.linearise = s->linearise ? 1u : 0u;
+    bp.depthThreshold = s->depth_threshold;
+    for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
+    uint32_t chunk = 0;
+    for (uint32_t v0 = 0; v0 < nViews; v0 += perChunk, ++chunk) {
+        const uint32_t v1 = std::min(nViews, v0 + perChunk);
+        uint32_t chunkTiles = 0;
+        uint64_t partitions = 0;
+        for (uint32_t v = v0; v < v1; ++v) {
+            chunkTiles += hostV[v].tilesX * ((hostV[v].height + lrt::kTile - 1) / lrt::kTile);
+            for (const CloudDesc& c : clouds) partitions += lrt::project_partitions(c.count);
+        }
+        const uint32_t keyBits = 24 + bits_for(chunkTiles);
+        uint32_t* counters = static_cast<uint32_t*>(B.counters.ptr) + 4 * chunk;
+        uint32_t* err = counters + 2;
+        const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) +
+                                   size_t{(v1 - v0) * shape.launchesPerView} * 4;
+        uint64_t* status = static_cast<uint64_t*>(r->scanScratch.ptr);
+        uint32_t* tickets = reinterpret_cast<uint32_t*>(static_cast<char*>(r->scanScratch.ptr) +
+                                                        lrt::project_status_bytes(static_cast<uint32_t>(partitions)));
+        LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, B.stream), "counters");
+        LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, B.stream), "projection scratch");
+        LRT_CUDA(r, cudaMemsetAsync(static_cast<uint32_t*>(B.queue.ptr) + chunk, 0, 4, B.stream), "queue");
+        const uint32_t lastPartition = static_cast<uint32_t>(partitions - 1);
+        uint32_t partitionBase = 0, launch = 0;
+        for (uint32_t v = v0; v < v1; ++v) {
+            for (uint32_t k = 0; k < shape.launchesPerView; ++k) {
+                const uint32_t li = v * shape.launchesPerView + k;
+                const CloudDesc& c = clouds[k];
+                LRT_CUDA(r,
+                         lrt::launch_project_emit(
+                             hostF[li], static_cast<const float4*>(c.packed->positions),
+                             static_cast<const uint4*>(c.packed->shape), static_cast<const uint32_t*>(c.packed->sh),
+                             static_cast<ProjRecord*>(B.records.ptr), nullptr, nullptr, nullptr, counters, status,
+                             tickets + launch, partitionBase, lastPartition, slotBits,
+                             static_cast<uint64_t*>(r->pairs.ptr), r->pairCap, B.stream, devF + li),
+                         "project");
+                partitionBase += lrt::project_partitions(c.count);
+                launch += 1;
+            }
+        }
+        bool inAlt = false;
+        LRT_CUDA(r,
+                 lrt::launch_sort_u64(static_cast<uint64_t*>(r->pairs.ptr), static_cast<uint64_t*>(r->pairsAlt.ptr),
+                                      nullptr, nullptr, counters + 1, r->pairCap, slotBits, keyBits,
+                                      r->sortScratch.ptr, err, &inAlt, B.stream),
+                 "pair sort");
+        const uint64_t* sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : static_cast<uint64_t*>(r->pairs.ptr);
+        LRT_CUDA(r,
+                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + slotBits, static_cast<uint2*>(B.ranges.ptr),
+                                    chunkTiles, B.stream),
+                 "ranges");
+        LRT_CUDA(r,
+                 lrt::launch_blend_batch(bp, devV + v0, v1 - v0, static_cast<uint2*>(B.ranges.ptr), sorted,
+                                         static_cast<ProjRecord*>(B.records.ptr), chunkTiles,
+                                         static_cast<uint32_t*>(B.queue.ptr) + chunk, err, numSMs * blocksPerSM,
+                                         B.stream),
+                 "blend");
+        LRT_CUDA(r, cudaMemcpyAsync(B.hostCounters + 4 * chunk, counters, 16, cudaMemcpyDeviceToHost, B.stream),
+                 "readback");
+    }
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* instances, uint32_t n,
+                                     const lrt_view* views, uint32_t nViews, const lrt_render_settings* s,
+                                     lrt_batch_stats* stats, void* streamPtr) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (s == nullptr || (n > 0 && instances == nullptr) || (nViews > 0 && views == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    std::vector<CloudDesc> clouds;
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const lrt_gpu_splats* c = instances[k].splats;
+        if (c == nullptr || c->count == 0) continue;
+        if (c->positions == nullptr || c->shape == nullptr || (c->rest_per_colour > 0 && c->sh == nullptr))
+            return fail(r, LRT_INVALID_ARGUMENT, "a cloud without its buffers");
+        CloudDesc d;
+        d.packed = c;
+        d.objectToWorld = instances[k].object_to_world;
+        d.edit = &instances[k].edit;
+        d.count = c->count;
+        clouds.push_back(d);
+        total += c->count;
+    }
+    if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one view");
+    for (uint32_t v = 0; v < nViews; ++v) {
+        if (views[v].width == 0 || views[v].height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a view needs a size");
+        if (views[v].colour == nullptr || views[v].depth == nullptr)
+            return fail(r, LRT_INVALID_ARGUMENT, "a view without its images");
+    }
+    if (stats != nullptr) std::memset(stats, 0, sizeof(*stats));
+    if (nViews == 0) return LRT_OK;
+    DeviceScope scope(r->device);
+    auto& B = r->batch;
+    cudaStream_t caller = static_cast<cudaStream_t>(streamPtr);
+    if (B.stream == nullptr) {
+        LRT_CUDA(r, cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking), "batch stream");
+        for (cudaEvent_t* e : {&B.in, &B.out, &B.start, &B.end}) LRT_CUDA(r, cudaEventCreate(e), "batch event");
+    }
+    int numSMs = 148;
+    cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, r->device);
+
+    // Shape: views largest first; everything a captured graph depends on.
+    BatchShape shape;
+    shape.slots = static_cast<uint32_t>(total);
+    shape.launchesPerView = static_cast<uint32_t>(clouds.size());
+    shape.order.resize(nViews);
+    for (uint32_t v = 0; v < nViews; ++v) shape.order[v] = v;
+    std::stable_sort(shape.order.begin(), shape.order.end(), [&](uint32_t a, uint32_t b) {
+        return uint64_t{views[a].width} * views[a].height > uint64_t{views[b].width} * views[b].height;
+    });
+    uint64_t key = mix(0, nViews);
+    key = mix(key, total);
+    for (uint32_t v : shape.order) key = mix(mix(key, views[v].width), views[v].height);
+    for (const CloudDesc& c : clouds) key = mix(mix(key, reinterpret_cast<uintptr_t>(c.packed->positions)), c.count);
+    key = mix(key, (uint64_t{s->antialias} << 1) ^ (uint64_t{s->max_sh_degree} << 3) ^ (uint64_t{s->linearise} << 7) ^
+                       (uint64_t{s->depth_mode} << 9));
+    shape.key = key;
+    if (clouds.empty() || total == 0) {
+        // Nothing to draw: the background.
+        for (uint32_t v = 0; v < nViews; ++v) {
+            lrt_targets t{views[v].width, views[v].height, views[v].colour, views[v].depth};
+            lrt_render_settings sv = *s;
+            sv.width = views[v].width;
+            sv.height = views[v].height;
+            const int code = lrt_rast_render(r, &views[v].projection, nullptr, 0, &sv, &t, nullptr, streamPtr);
+            if (code != LRT_OK) return code;
+        }
+        if (stats != nullptr) stats->views = nViews;
+        return LRT_OK;
+    }
+    const uint32_t slotBits = bits_for(total);
+
+    // Per (view, instance) projection parameters and per view blend parameters,
+    // written to pinned memory in view order (largest first).
+    const uint32_t nLaunch = nViews * shape.launchesPerView;
+    const size_t paramsBytes = size_t{nLaunch} * sizeof(FrameParams) + size_t{nViews} * sizeof(lrt::ViewParams);
+    if (B.hostParamsBytes < paramsBytes) {
+        if (B.hostParams != nullptr) cudaFreeHost(B.hostParams);
+        B.hostParams = nullptr;
+        B.hostParamsBytes = 0;
+        LRT_CUDA(r, cudaMallocHost(&B.hostParams, paramsBytes), "batch parameters");
+        B.hostParamsBytes = paramsBytes;
+        B.generation += 1;
+    }
+    LRT_CUDA(r, ensure_batch(r, B.params, paramsBytes), "batch parameters");
+    FrameParams* hostF = static_cast<FrameParams*>(B.hostParams);
+    lrt::ViewParams* hostV = reinterpret_cast<lrt::ViewParams*>(static_cast<char*>(B.hostParams) +
+                                                               size_t{nLaunch} * sizeof(FrameParams));
+
+    // The chunking the autotuner picked for this shape (tune on first sight).
+    uint32_t perChunk = 0, blocksPerSM = 0;
+    for (auto& t : B.tuned)
+        if (t.first == key) {
+            perChunk = t.second.first;
+            blocksPerSM = t.second.second;
+        }
+    const bool tuning = perChunk == 0;
+
+    auto fill = [&](uint32_t chunkViews) {
+        // Tile numbering restarts at each chunk; records are per chunk slot.
+        uint32_t tileBase = 0;
+        for (uint32_t i = 0; i < nViews; ++i) {
+            if (i % chunkViews == 0) tileBase = 0;
+            const lrt_view& vw = views[shape.order[i]];
+            lrt_render_settings sv = *s;
+            sv.width = vw.width;
+            sv.height = vw.height;
+            const uint32_t tilesX = (vw.width + lrt::kTile - 1) / lrt::kTile;
+            const uint32_t tilesY = (vw.height + lrt::kTile - 1) / lrt::kTile;
+            const uint32_t recordBase = (i % chunkViews) * shape.slots;
+            uint32_t base = 0;
+            for (uint32_t k = 0; k < shape.launchesPerView; ++k) {
+                FrameParams f = frame_params(&vw.projection, &sv, clouds[k], tilesX, tilesY, base);
+                f.tileBase = tileBase;
+                f.recordBase = recordBase;
+                f.writeDebug = 0;
+                hostF[i * shape.launchesPerView + k] = f;
+                base += clouds[k].count;
+            }
+            lrt::ViewParams vp{};
+            vp.width = vw.width;
+            vp.height = vw.height;
+            vp.tilesX = tilesX;
+            vp.tileBase = tileBase;
+            vp.recordBase = recordBase;
+            vp.colour = static_cast<float4*>(vw.colour);
+            vp.depth = static_cast<float*>(vw.depth);
+            hostV[i] = vp;
+            tileBase += tilesX * tilesY;
+        }
+    };
+
+    // Buffers for a chunk size; false and an error when something failed.
+    auto reserve = [&](uint32_t chunkViews) -> int {
+        uint32_t maxTiles = 0, tiles = 0;
+        for (uint32_t i = 0; i < nViews; ++i) {
+            if (i % chunkViews == 0) tiles = 0;
+            const lrt_view& vw = views[shape.order[i]];
+            tiles += ((vw.width + 15) / 16) * ((vw.height + 15) / 16);
+            maxTiles = std::max(maxTiles, tiles);
+        }
+        if (slotBits + 24 + bits_for(maxTiles) > 64)
+            return fail(r, LRT_UNSUPPORTED, "splat slots and a chunk's tiles do not fit one 64-bit pair word");
+        const uint64_t partitions = uint64_t{chunkViews} * [&] {
+            uint64_t p = 0;
+            for (const CloudDesc& c : clouds) p += lrt::project_partitions(c.count);
+            return p;
+        }();
+        const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) +
+                                   size_t{chunkViews * shape.launchesPerView} * 4;
+        if (r->scanScratch.bytes < statusBytes) {
+            r->batch.generation += 1;
+            LRT_CUDA(r, ensure(r->scanScratch, statusBytes), "projection scratch");
+        }
+        LRT_CUDA(r, ensure_batch(r, B.records, size_t{chunkViews} * shape.slots * sizeof(ProjRecord)), "records");
+        LRT_CUDA(r, ensure_batch(r, B.ranges, size_t{maxTiles} * 8), "ranges");
+        const uint32_t chunks = (nViews + chunkViews - 1) / chunkViews;
+        LRT_CUDA(r, ensure_batch(r, B.counters, size_t{chunks} * 16), "counters");
+        LRT_CUDA(r, ensure_batch(r, B.queue, size_t{chunks} * 4), "queue");
+        if (B.hostCounterChunks < chunks) {
+            if (B.hostCounters != nullptr) cudaFreeHost(B.hostCounters);
+            B.hostCounters = nullptr;
+            LRT_CUDA(r, cudaMallocHost(reinterpret_cast<void**>(&B.hostCounters), size_t{chunks} * 16), "counters");
+            B.hostCounterChunks = chunks;
+            B.generation += 1;
+        }
+        if (r->pairCap == 0) {
+            uint64_t pixels = 0;
+            for (uint32_t i = 0; i < std::min(nViews, chunkViews); ++i)
+                pixels += uint64_t{views[shape.order[i]].width} * views[shape.order[i]].height;
+            r->pairCap = static_cast<uint32_t>(std::min<uint64_t>(std::max<uint64_t>(pixels, 1024), 0xFFFFFFFFull));
+        }
+        if (r->pairs.bytes < size_t{r->pairCap} * 8 || r->pairsAlt.bytes < size_t{r->pairCap} * 8) r->batch.generation += 1;
+        LRT_CUDA(r, ensure(r->pairs, size_t{r->pairCap} * 8), "pairs");
+        LRT_CUDA(r, ensure(r->pairsAlt, size_t{r->pairCap} * 8), "pairs");
+        const size_t sortBytes = lrt::sort_scratch_bytes(r->pairCap, 24 + bits_for(maxTiles));
+        if (r->sortScratch.bytes < sortBytes) r->batch.generation += 1;
+        LRT_CUDA(r, ensure(r->sortScratch, sortBytes), "sort scratch");
+        return LRT_OK;
+    };
+
+    // One eager run of the batch: returns the status, sets *overflowed and
+    // the device time.
+    auto eager = [&](uint32_t chunkViews, uint32_t bps, bool* overflowed, float* ms) -> int {
+        for (int attempt = 0; attempt < 3; ++attempt) {
+            int code = reserve(chunkViews);
+            if (code != LRT_OK) return code;
+            fill(chunkViews);
+            LRT_CUDA(r, cudaEventRecord(B.start, B.stream), "event");
+            code = enqueue_batch(r, clouds, views, shape, s, chunkViews, bps, static_cast<uint32_t>(numSMs));
+            if (code != LRT_OK) return code;
+            LRT_CUDA(r, cudaEventRecord(B.end, B.stream), "event");
+            LRT_CUDA(r, cudaStreamSynchronize(B.stream), "batch");
+            LRT_CUDA(r, cudaEventElapsedTime(ms, B.start, B.end), "event");
+            const uint32_t chunks = (nViews + chunkViews - 1) / chunkViews;
+            uint32_t worst = 0, statusBits = 0;
+            for (uint32_t c = 0; c < chunks; ++c) {
+                worst = std::max(worst, B.hostCounters[4 * c + 1]);
+                statusBits |= B.hostCounters[4 * c + 2];
+            }
+            if (statusBits & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+            if (statusBits & lrt::kErrTooManyPairs) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pairs in a chunk");
+            *overflowed = worst > r->pairCap;
+            if (!*overflowed) return LRT_OK;
+            r->pairCap = grow(r->pairCap, worst);
+        }
+        return fail(r, LRT_OVERFLOW, "pair capacity exceeded");
+    };
+
+    LRT_CUDA(r, cudaEventRecord(B.in, caller), "event");
+    LRT_CUDA(r, cudaStreamWaitEvent(B.stream, B.in, 0), "event");
+    bool replayed = false;
+    float deviceMs = 0.0f;
+    if (tuning) {
+        // Autotune: views per chunk x blend blocks per SM, fastest of one timed run each.
+        std::vector<uint32_t> chunkSizes;
+        for (uint32_t c : {nViews, 32u, 16u, 8u, 4u})
+            if (c <= nViews && c >= 1 && std::find(chunkSizes.begin(), chunkSizes.end(), c) == chunkSizes.end())
+                chunkSizes.push_back(c);
+        float best = 3.4e38f;
+        for (uint32_t c : chunkSizes) {
+            for (uint32_t bps : {4u, 8u}) {
+                bool over = false;
+                float ms = 0.0f;
+                int code = eager(c, bps, &over, &ms);   // sizes the buffers
+                if (code != LRT_OK) return code;
+                code = eager(c, bps, &over, &ms);
+                if (code != LRT_OK) return code;
+                if (ms < best) {
+                    best = ms;
+                    perChunk = c;
+                    blocksPerSM = bps;
+                }
+            }
+        }
+        B.tuned.push_back({key, {perChunk, blocksPerSM}});
+        bool over = false;
+        const int code = eager(perChunk, blocksPerSM, &over, &deviceMs);   // the frame itself, with the choice
+        if (code != LRT_OK) return code;
+    } else {
+        int code = reserve(perChunk);
+        if (code != LRT_OK) return code;
+        fill(perChunk);
+        const bool haveGraph = B.graph != nullptr && B.graphKey == key && B.graphGeneration == B.generation;
+        if (!haveGraph && !B.graphFailed) {
+            // Capture this shape's batch into a graph.
+            if (B.graph != nullptr) {
+                cudaGraphExecDestroy(B.graph);
+                B.graph = nullptr;
+            }
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                code = enqueue_batch(r, clouds, views, shape, s, perChunk, blocksPerSM, static_cast<uint32_t>(numSMs));
+                ok = cudaStreamEndCapture(B.stream, &graph) == cudaSuccess && code == LRT_OK;
+            }
+            if (ok) ok = cudaGraphInstantiate(&B.graph, graph, 0) == cudaSuccess;
+            if (graph != nullptr) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            if (ok) {
+                B.graphKey = key;
+                B.graphGeneration = B.generation;
+            } else {
+                B.graph = nullptr;
+                B.graphFailed = true;   // keep running eagerly
+                r->error.clear();
+            }
+        }
+        bool over = false;
+        if (B.graph != nullptr && B.graphKey == key && B.graphGeneration == B.generation) {
+            LRT_CUDA(r, cudaEventRecord(B.start, B.stream), "event");
+            LRT_CUDA(r, cudaGraphLaunch(B.graph, B.stream), "graph launch");
+            LRT_CUDA(r, cudaEventRecord(B.end, B.stream), "event");
+            LRT_CUDA(r, cudaStreamSynchronize(B.stream), "batch");
+            LRT_CUDA(r, cudaEventElapsedTime(&deviceMs, B.start, B.end), "event");
+            const uint32_t chunks = (nViews + perChunk - 1) / perChunk;
+            uint32_t worst = 0, statusBits = 0;
+            for (uint32_t c = 0; c < chunks; ++c) {
+                worst = std::max(worst, B.hostCounters[4 * c + 1]);
+                statusBits |= B.hostCounters[4 * c + 2];
+            }
+            if (statusBits & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+            over = worst > r->pairCap;
+            replayed = !over;
+            if (over) r->pairCap = grow(r->pairCap, worst);
+        }
+        if (!replayed) {
+            code = eager(perChunk, blocksPerSM, &over, &deviceMs);
+            if (code != LRT_OK) return code;
+        }
+    }
+    LRT_CUDA(r, cudaEventRecord(B.out, B.stream), "event");
+    LRT_CUDA(r, cudaStreamWaitEvent(caller, B.out, 0), "event");
+    if (stats != nullptr) {
+        const uint32_t chunks = (nViews + perChunk - 1) / perChunk;
+        uint64_t pairs = 0;
+        for (uint32_t c = 0; c < chunks; ++c) pairs += B.hostCounters[4 * c + 1];
+        stats->views = nViews;
+        stats->splats = static_cast<uint32_t>(total);
+        stats->pairs = static_cast<uint32_t>(std::min<uint64_t>(pairs, 0xFFFFFFFFull));
+        stats->chunks = chunks;
+        stats->views_per_chunk = perChunk;
+        stats->blend_blocks_per_sm = blocksPerSM;
+        stats->graph_replayed = replayed ? 1u : 0u;
+        stats->device_ms = deviceMs;
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return LRT_OK;
+}

@@ -29,6 +29,9 @@ struct FrameParams {
     float m[12];      // object -> view, rows of a 3x4
     float eye[3];     // the camera in the cloud's space
     uint32_t count, base, restPerColour, shWords, shLimit;
+    uint32_t tileBase;     // added to every tile id (the view's first tile in a batch; 0 for one view)
+    uint32_t recordBase;   // the view's first record in a batch (0 for one view)
+    uint32_t writeDebug;   // 1: write rects, touched counts and depth keys per slot
     EditParams edit;
 };
 
@@ -38,6 +41,14 @@ struct BlendParams {
     uint32_t depthMode, linearise;
     float depthThreshold;
     float bg[4];
+};
+
+// One view of a batch, as the batched blend reads it.
+struct ViewParams {
+    uint32_t width, height, tilesX, tileBase;   // tileBase: the view's first tile in the batch
+    uint32_t recordBase, reserved0, reserved1, reserved2;
+    float4* colour;
+    float* depth;
 };
 
 // frame.slang:85-89: what the projection leaves for the blend.

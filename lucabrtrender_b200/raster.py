@@ -220,6 +220,36 @@ class TileRasterizer:
         self._check(code)
         return FrameStats.from_struct(stats)
 
+    def render_batch(self, views: Sequence[tuple], instances: Sequence[SplatInstance], settings: RenderSettings,
+                     targets: Sequence[RenderTargets] | None = None, stream=None):
+        """Many views in one call (lrt_rast_render_batch). `views` holds
+        (camera | projection, width, height) per view; returns (targets, stats)."""
+        lib = _abi.load()
+        n = len(views)
+        if targets is None:
+            targets = [RenderTargets() for _ in range(n)]
+        arr_v = (_abi.View * max(1, n))()
+        for k, (view, w, h) in enumerate(views):
+            projection = view if isinstance(view, Projection) else projection_for(view, w, h)
+            targets[k].reserve(w, h)
+            arr_v[k].projection = projection.struct()
+            arr_v[k].width, arr_v[k].height = w, h
+            arr_v[k].colour, arr_v[k].depth = targets[k].colour.data_ptr(), targets[k].depth.data_ptr()
+        clouds = []
+        arr = (_abi.SplatInstanceStruct * max(1, len(instances)))()
+        for k, inst in enumerate(instances):
+            if inst.splats is not None and inst.splats.count > 0:
+                cs = inst.splats.struct()
+                clouds.append(cs)
+                arr[k].splats = C.pointer(cs)
+            arr[k].object_to_world[:] = [float(v) for v in np.asarray(inst.object_to_world, np.float64).reshape(16)]
+            inst.edit.fill(arr[k].edit)
+        st = settings.struct()
+        stats = _abi.BatchStats()
+        self._check(lib.lrt_rast_render_batch(self._handle, arr, len(instances), arr_v, n, C.byref(st),
+                                              C.byref(stats), _stream_ptr(stream)))
+        return targets, stats
+
     def debug_view(self) -> _abi.DebugView:
         v = _abi.DebugView()
         self._check(_abi.load().lrt_rast_debug_view(self._handle, C.byref(v)))
