@@ -40,6 +40,10 @@ FRAMES = 20
 RADIUS = 4.0
 SEED = 1
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + written) of one launch, from ncu (`dram__bytes_read.sum +
+# dram__bytes_write.sum`) on frame 3 of this orbit; the capture and its command
+# are summarised under profiles/.
+PROFILED_DRAM_BYTES = {"blend": 63.688192e6 + 16.780544e6}
 
 
 def orbit_camera(L, k: int):
@@ -160,6 +164,85 @@ def run_reference(args) -> None:
         "e2e": {"value": round(mean_ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+BATCH_SPLATS = 2_000_000
+BATCH_VIEWS = 64
+BATCH_SIZES = [(256, 256), (640, 480), (1280, 720), (1920, 1080)]
+
+
+def batch_views(L, seed: int):
+    """64 cameras looking at the origin from directions uniform on the sphere,
+    at radius U(3, 6), each with a resolution drawn uniformly from four."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    views = []
+    for _ in range(BATCH_VIEWS):
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        r = rng.uniform(3.0, 6.0)
+        w, h = BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+        up = (0.0, 1.0, 0.0) if abs(d[1]) < 0.99 else (1.0, 0.0, 0.0)
+        views.append((L.square_pixel_camera(tuple(d * r), (0.0, 0.0, 0.0), w, h, 60.0, 0.01, up), w, h))
+    return views
+
+
+def run_batch(L, torch, dev, rank, raster, args, clocks) -> dict:
+    """2M splats, 64 views of mixed resolution: one lrt_rast_render_batch call
+    per step against 64 sequential lrt_rast_render calls, ms per view, with
+    the batched images checked equal to the sequential ones bit for bit."""
+    packed = L.pack_splats(L.synthetic_records(BATCH_SPLATS, SEED + 1), 15, 3)
+    cloud = L.to_device(packed, dev)
+    instances = [L.SplatInstance(cloud)]
+    settings = L.RenderSettings()
+    views = batch_views(L, SEED + rank)
+    projections = [(L.projection_for(c, w, h), w, h) for c, w, h in views]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    singles = [L.RenderTargets(w, h, device=dev) for _, w, h in views]
+    batched = [L.RenderTargets(w, h, device=dev) for _, w, h in views]
+
+    def sequential():
+        for (p, w, h), t in zip(projections, singles):
+            st = L.RenderSettings(width=w, height=h)
+            raster.render(p, instances, st, t, stream)
+
+    def one_batch():
+        return raster.render_batch(projections, instances, settings, batched, stream)[1]
+
+    for _ in range(2):
+        sequential()
+    stats = None
+    for _ in range(3):          # tune, capture, replay
+        stats = one_batch()
+    torch.cuda.synchronize(dev)
+    steps = max(3, args.steps // 4)
+    seq_ms = bat_ms = 0.0
+    w0 = time.time()
+    for _ in range(steps):
+        flush.fill_(1.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sequential()
+        b.record(stream)
+        b.synchronize()
+        seq_ms += a.elapsed_time(b)
+        flush.fill_(2.0)
+        a.record(stream)
+        stats = one_batch()
+        b.record(stream)
+        b.synchronize()
+        bat_ms += a.elapsed_time(b)
+    clocks.window(w0, time.time())
+    equal = all(torch.equal(x.colour, y.colour) and torch.equal(x.depth, y.depth) for x, y in zip(singles, batched))
+    per_seq = seq_ms / (steps * BATCH_VIEWS)
+    per_bat = bat_ms / (steps * BATCH_VIEWS)
+    return {"workload": "2M splats, 64 views on a sphere of radius U(3,6), resolutions uniform over 256x256, "
+                        "640x480, 1280x720, 1920x1080", "steps": steps,
+            "batched_ms_per_view": round(per_bat, 4), "sequential_ms_per_view": round(per_seq, 4),
+            "speedup": round(per_seq / per_bat, 3), "images_equal_bit_for_bit": bool(equal),
+            "pairs_per_batch": int(stats.pairs), "views_per_chunk": int(stats.views_per_chunk),
+            "blend_blocks_per_sm": int(stats.blend_blocks_per_sm), "graph_replayed": int(stats.graph_replayed)}
 
 
 def run_ours(args) -> None:
@@ -314,6 +397,11 @@ def run_ours(args) -> None:
                    "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels",
                    "params": "means, log-scales, quaternions, opacity logits, 48 SH (fp16 storage, fp32 gradients)"}
 
+    # --- many views: one batched call against sequential renders ---
+    batch = None
+    if not args.no_batch:
+        batch = run_batch(L, torch, dev, rank, raster, args, clocks)
+
     # --- roofline of the dominant kernel, measured live over the timed steps ---
     st = stats_list
     mean = lambda f: float(np.mean([getattr(s, f) for s in st]))  # noqa: E731
@@ -362,7 +450,7 @@ def run_ours(args) -> None:
             "stages_ms": {k: round(v, 4) for k, v in stage.items()},
             "sort_gbs": round(sort_gbs, 1) if sort_gbs else None,
             "roofline": {"kernel": dom_name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": PROFILED_DRAM_BYTES.get(dom_name),
                          "peak_kind": peak_kind},
             "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
                     "h2d_bytes_per_step": _abi.C.sizeof(_abi.Projection),
@@ -371,6 +459,7 @@ def run_ours(args) -> None:
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "fwd_bwd": fwd_bwd,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     raster.close()
@@ -388,6 +477,7 @@ def main() -> None:
     ap.add_argument("--cpu-frames", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-backward", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
