@@ -4,6 +4,7 @@ The compute path is the in-tree CUDA library ``lib/liblrt_raster.so`` (sm_100a
 kernels behind the C-ABI of ``include/lrt_raster.h``); this package is the
 Python host mirror of the reference's C++ interface over that ABI.
 """
+from ._abi import LrtError
 from .camera import Camera, Lens, Projection, projection_for, square_pixel_camera
 from .raster import (Depth, EditMode, EditShape, FrameStats, RenderSettings, RenderTargets, SplatEdit,
                      SplatInstance, TileRasterizer, math_eval)
@@ -11,7 +12,7 @@ from .scene import CloudLoader, GpuSplats, PackedSplats, pack_splats, synthetic_
 from .train import rasterize
 
 __all__ = [
-    "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
+    "LrtError", "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
     "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
     "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
 ]

@@ -309,25 +309,38 @@ __device__ __forceinline__ float srgb_to_linear_slope(float c) {
 constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
 constexpr uint32_t kGradStride = 12;   // floats per pair in the partials buffer (three 16-byte vectors)
 
-// Sum of 16 values over the warp by recursive halving (a reduce-scatter):
-// at each step a lane keeps half of its vector, sends the other half to its
-// partner and adds what it receives, so 8 + 4 + 2 + 1 + 1 = 16 shuffles
-// replace 16 x 5 butterflies. Afterwards lane l holds the warp's sum of
-// value (l >> 1) & 15 (lanes l and l ^ 1 hold the same one).
-__device__ __forceinline__ float warp_reduce_scatter16(float (&v)[16], uint32_t lane) {
+// Sum of nine values over the warp by recursive halving (a reduce-scatter):
+// at each step a lane keeps part of its list, sends the rest to its partner
+// and adds what it receives. The list shrinks 9 -> 5 -> 3 -> 2 -> 1 (lists
+// padded with zeros where a half is shorter), so 5 + 3 + 2 + 1 shuffles and a
+// last butterfly (12 in all) replace 9 x 5 butterflies. Afterwards lanes l
+// and l ^ 1 hold the warp's sum of value `idx` (or idx >= 9: nothing).
+__device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], uint32_t lane, uint32_t& idx) {
+    constexpr unsigned kAll = 0xFFFFFFFFu;
+    const bool u16 = (lane & 16u) != 0, u8 = (lane & 8u) != 0, u4 = (lane & 4u) != 0, u2 = (lane & 2u) != 0;
+    float a[5];
 #pragma unroll
-    for (int level = 0; level < 4; ++level) {
-        const int o = 16 >> level;       // partner distance
-        const int half = 8 >> level;     // values kept
-        const bool upper = (lane & static_cast<uint32_t>(o)) != 0;
-#pragma unroll
-        for (int j = 0; j < half; ++j) {
-            const float send = upper ? v[j] : v[j + half];
-            const float keep = upper ? v[j + half] : v[j];
-            v[j] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
-        }
+    for (int j = 0; j < 5; ++j) {   // [0..4] | [5..8, -]
+        const float lo = v[j], hi = j < 4 ? v[5 + j] : 0.0f;
+        a[j] = (u16 ? hi : lo) + __shfl_xor_sync(kAll, u16 ? lo : hi, 16);
     }
-    return v[0] + __shfl_xor_sync(0xFFFFFFFFu, v[0], 1);
+    float b[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {   // [0, 1, 2] | [3, 4, -]
+        const float lo = a[j], hi = j < 2 ? a[3 + j] : 0.0f;
+        b[j] = (u8 ? hi : lo) + __shfl_xor_sync(kAll, u8 ? lo : hi, 8);
+    }
+    float c[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {   // [0, 1] | [2, -]
+        const float lo = b[j], hi = j < 1 ? b[2] : 0.0f;
+        c[j] = (u4 ? hi : lo) + __shfl_xor_sync(kAll, u4 ? lo : hi, 4);
+    }
+    const float d = (u2 ? c[1] : c[0]) + __shfl_xor_sync(kAll, u2 ? c[0] : c[1], 2);   // [0] | [1]
+    const uint32_t b1 = u2 ? 1u : 0u;
+    const uint32_t pos = u8 ? (u4 ? 5u : 3u + b1) : (u4 ? (b1 != 0 ? 5u : 2u) : b1);   // 5: a padding slot
+    idx = pos >= (u16 ? 4u : 5u) ? 9u : (u16 ? 5u : 0u) + pos;
+    return d + __shfl_xor_sync(kAll, d, 1);
 }
 
 // The backward of blend_kernel<true>: per pixel, the reference's loop run
@@ -352,6 +365,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
     __shared__ __align__(16) float4 sBox[kB];
     __shared__ uint32_t sEmit[kB];
     __shared__ float sPart[kBlendThreads / 32][kB][kGrads];
+    __shared__ uint32_t sHit[kBlendThreads / 32][kB / 32];   // which sPart slots a warp wrote this batch
     __shared__ uint32_t sMaxLast;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
@@ -416,7 +430,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
             sRec[tid] = proj[static_cast<uint32_t>(word & slotMask)];
             sEmit[tid] = emit[bStart + tid];
         }
-        for (uint32_t k = tid; k < (kBlendThreads / 32) * kB * kGrads; k += kBlendThreads) (&sPart[0][0][0])[k] = 0.0f;
+        if (tid < (kBlendThreads / 32) * (kB / 32)) (&sHit[0][0])[tid] = 0u;
         __syncthreads();
         if (tid < cnt) sBox[tid] = cull_box(sRec[tid]);
         __syncthreads();
@@ -441,11 +455,12 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                 overlap = !(box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0);
             }
             uint32_t todo = __ballot_sync(0xFFFFFFFFu, overlap);
+            uint32_t written = 0;
             while (todo != 0) {
                 const uint32_t bit = 31u - static_cast<uint32_t>(__clz(todo));
                 todo &= ~(1u << bit);
                 const uint32_t j = static_cast<uint32_t>(c) + bit;
-                float v[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+                float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                 bool hit = false;
                 if (live && bStart + j < myLast) {
                     const float4 screen = sRec[j].screen;
@@ -454,8 +469,17 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                     const float dy = pyf - screen.y;
                     const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
                     if (!(power > screen.w)) {
-                        const float e = lrt_exp(-0.5f * power);
-                        const float raw = conic.w * e;
+                        // The forward's alpha decides who contributed, so it is
+                        // taken from the exact exponential wherever the fast one
+                        // (relative error below 1e-6 for these arguments) lies
+                        // within 1e-5 of either threshold; elsewhere both sides
+                        // of a threshold agree and the fast value serves.
+                        float e = __expf(-0.5f * power);
+                        float raw = conic.w * e;
+                        if (fabsf(raw - 1.0f / 255.0f) <= 1e-5f / 255.0f || fabsf(raw - 0.99f) <= 0.99e-5f) {
+                            e = lrt_exp(-0.5f * power);
+                            raw = conic.w * e;
+                        }
                         const float alpha = fminf(0.99f, raw);
                         if (!(alpha < 1.0f / 255.0f)) {
                             hit = true;
@@ -490,6 +514,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                     }
                 }
                 const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
+                if (hits != 0) written |= 1u << bit;
                 if (hits != 0 && (hits & (hits - 1)) == 0) {
                     // one pixel of the warp: its values are the warp's sums
                     if (hit) {
@@ -497,19 +522,24 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                         for (uint32_t k = 0; k < kGrads; ++k) sPart[warp][j][k] = v[k];
                     }
                 } else if (hits != 0) {
-                    const float sum = warp_reduce_scatter16(v, lane);
-                    const uint32_t idx = (lane >> 1) & 15u;
+                    uint32_t idx;
+                    const float sum = warp_reduce_scatter9(v, lane, idx);
                     if ((lane & 1u) == 0 && idx < kGrads) sPart[warp][j][idx] = sum;
                 }
             }
+            if (lane == 0) sHit[warp][static_cast<uint32_t>(c) >> 5] = written;
         }
         __syncthreads();
         if (tid < cnt) {
+            // Warps that wrote nothing for this record are skipped: adding
+            // their zeros would not change the sum.
             float sum[kGradStride] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (uint32_t k = 0; k < kGrads; ++k) {
+            for (uint32_t w = 0; w < kBlendThreads / 32; ++w) {
+                if ((sHit[w][tid >> 5] >> (tid & 31u)) & 1u) {
 #pragma unroll
-                for (uint32_t w = 0; w < kBlendThreads / 32; ++w) sum[k] += sPart[w][tid][k];
+                    for (uint32_t k = 0; k < kGrads; ++k) sum[k] += sPart[w][tid][k];
+                }
             }
             float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(sEmit[tid]) * kGradStride);
             out[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);

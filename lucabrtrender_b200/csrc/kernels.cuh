@@ -69,8 +69,9 @@ cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, co
 
 cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
-                                  const uint32_t* offsets, const float* partials, float* gMeans, float* gLogScales,
-                                  float* gQuats, float* gLogits, float* gSh, cudaStream_t stream);
+                                  const uint32_t* offsets, const float* partials, uint32_t partialPairs,
+                                  float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
+                                  cudaStream_t stream);
 
 cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
 

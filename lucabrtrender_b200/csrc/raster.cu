@@ -49,6 +49,8 @@ struct lrt_rast {
     bool trainPending = false;   // the forward's counts and status are not read yet
     cudaStream_t pendingStream = nullptr;
     bool trainSized = false;     // a training frame has run with a wait
+    uint32_t trainSlots = 0, trainWidth = 0, trainHeight = 0;   // that frame's shape
+    uint32_t trainSeenPairs = 0;  // the pairs of the last training frame whose counts were read
     lrt_train_params trainParams{};
     lrt::FrameParams trainFrame{};
     lrt::BlendParams trainBlend{};
@@ -599,13 +601,48 @@ int lrt_rast_train_forward(lrt_rast* r, const lrt_projection* pr, const lrt_trai
         clouds.push_back(d);
     }
     r->trainParams = *params;
-    // The first training frame waits (and redraws if its pairs overflowed) so
-    // that the pair buffers are sized; later ones are only enqueued, unless
-    // stage times are asked for.
-    const bool deferred = r->trainSized && !s->time_stages;
+    // A training frame waits (and redraws if its pairs overflowed) when it is
+    // the first of its shape, when stage times are asked for, or when the last
+    // frame whose counts were read left less than a quarter of the pair buffer
+    // free. Otherwise it is only enqueued; the backward reads its counts, and
+    // an overflow is reported there (and by the debug view) as OVERFLOW, with
+    // the buffers grown for the next try.
+    const bool sameShape = r->trainSized && r->trainSlots == params->count && r->trainWidth == s->width &&
+                           r->trainHeight == s->height;
+    const uint64_t wanted = uint64_t{r->trainSeenPairs} + r->trainSeenPairs / 4;
+    const bool deferred = sameShape && !s->time_stages && wanted <= r->pairCap;
+    if (sameShape && wanted > r->pairCap) r->pairCap = grow(r->pairCap, static_cast<uint32_t>(std::min<uint64_t>(wanted, 0xFFFFFFFFull)));
     const int code = render_frame(r, pr, clouds, s, targets, stats, streamPtr, true, frameStart, deferred);
-    if (code == LRT_OK && !deferred) r->trainSized = true;
+    if (code == LRT_OK && !deferred) {
+        r->trainSized = true;
+        r->trainSlots = params->count;
+        r->trainWidth = s->width;
+        r->trainHeight = s->height;
+        r->trainSeenPairs = r->trainPairs;
+    }
     return code;
+}
+
+// Reads the counts of an enqueued training frame once its stream has drained:
+// LRT_OVERFLOW (buffers grown, the frame must be drawn again) or LRT_TIMEOUT.
+static int settle_pending_frame(lrt_rast* r) {
+    r->trainPending = false;
+    const uint32_t pairs = r->hostCounters[1], status = r->hostCounters[2];
+    r->trainPairs = std::min(pairs, r->pairCap);
+    r->trainSeenPairs = pairs;
+    r->debug.pairs_count = std::min(pairs, r->pairCap);
+    r->debug.visible = r->hostCounters[0];
+    if (pairs > r->pairCap) {
+        r->pairCap = grow(r->pairCap, pairs);
+        r->trainReady = false;
+        return fail(r, LRT_OVERFLOW, "the training forward emitted more pairs than its buffer held; "
+                                     "the buffers are grown, run the step again");
+    }
+    if (status & lrt::kErrTimeout) {
+        r->trainReady = false;
+        return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+    }
+    return LRT_OK;
 }
 
 int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads* grads, void* streamPtr) {
@@ -640,27 +677,17 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
                                         static_cast<const float*>(p.opacity_logits),
                                         static_cast<const uint16_t*>(p.sh), static_cast<uint32_t*>(r->touched.ptr),
                                         static_cast<uint32_t*>(r->trainOffsets.ptr),
-                                        static_cast<float*>(r->partials.ptr), static_cast<float*>(grads->means),
+                                        static_cast<float*>(r->partials.ptr), r->trainPairs,
+                                        static_cast<float*>(grads->means),
                                         static_cast<float*>(grads->log_scales), static_cast<float*>(grads->quats),
                                         static_cast<float*>(grads->opacity_logits), static_cast<float*>(grads->sh),
                                         stream),
              "projection backward");
     LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
     LRT_CUDA(r, cudaStreamSynchronize(stream), "backward");
-    if (r->trainPending) {
-        // The forward ran without waiting: its status is read here.
-        r->trainPending = false;
-        const uint32_t pairs = r->hostCounters[1], status = r->hostCounters[2];
-        r->trainPairs = pairs;
-        r->debug.pairs_count = pairs;
-        r->debug.visible = r->hostCounters[0];
-        if (pairs > r->pairCap) {
-            r->pairCap = grow(r->pairCap, pairs);
-            r->trainReady = false;
-            return fail(r, LRT_OVERFLOW, "the training forward emitted more pairs than its buffer held; "
-                                         "the buffers are grown, run the step again");
-        }
-        if (status & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up");
+    if (r->trainPending) {   // the forward ran without waiting: its status is read here
+        const int code = settle_pending_frame(r);
+        if (code != LRT_OK) return code;
     }
     r->lastBackwardMs[0] = event_ms(r->ev[4], r->ev[5]);
     r->lastBackwardMs[1] = event_ms(r->ev[5], r->ev[6]);
@@ -676,11 +703,12 @@ int lrt_rast_backward_times(const lrt_rast* r, double* blendMs, double* projectM
 
 int lrt_rast_debug_view(lrt_rast* r, lrt_debug_view* out) {
     if (r == nullptr || out == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
     if (r->trainPending) {   // an enqueued training frame: wait for its counts
         DeviceScope scope(r->device);
         LRT_CUDA(r, cudaStreamSynchronize(r->pendingStream), "frame");
-        r->debug.visible = r->hostCounters[0];
-        r->debug.pairs_count = std::min(r->hostCounters[1], r->pairCap);
+        const int code = settle_pending_frame(r);
+        if (code != LRT_OK) return code;
     }
     *out = r->debug;
     return LRT_OK;

@@ -2,8 +2,8 @@
 // reference renders only). A splat's nine per-pair partials -- d/d(centre x,
 // y, conic a, b, c, alpha, colour r, g, b), written by the blend backward at
 // the pair's emit index -- are contiguous from the splat's first pair index,
-// so one thread sums them in order (no atomics, deterministic), then carries
-// them back through the forward of splat_project.slang:72-169 to the
+// so they are summed in a fixed order (no atomics, deterministic), then carried
+// back through the forward of splat_project.slang:72-169 to the
 // parameters: means, log-scales, quaternions (w, x, y, z; normalised in the
 // forward), opacity logits and the 16 x 3 SH coefficients (fp32 gradients of
 // fp16 values). Every forward intermediate is recomputed from the parameters
@@ -50,17 +50,67 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, uint32_t deg
     b[14] = kC3[6] * x * (xx - 3.0f * yy); gx[14] = kC3[6] * (3.0f * xx - 3.0f * yy); gy[14] = -6.0f * kC3[6] * x * y;
 }
 
-__global__ void __launch_bounds__(kThreads)
+// A splat's partials summed in a fixed order. Splats with few pairs are summed
+// by their own lane; the warp then sums each splat with more than kSolo pairs
+// together (lane l takes pairs l, l + 32, ..., then a butterfly over the
+// lanes), so a splat that touches hundreds of tiles does not hold its warp
+// for hundreds of dependent iterations.
+constexpr uint32_t kSolo = 16;
+
+__device__ __forceinline__ void sum_partials(const float4* __restrict__ part, uint32_t n, float (&g)[9]) {
+#pragma unroll 4
+    for (uint32_t k = 0; k < n; ++k) {
+        const float4 a = __ldg(part + 3 * k), b = __ldg(part + 3 * k + 1), c = __ldg(part + 3 * k + 2);
+        g[0] += a.x; g[1] += a.y; g[2] += a.z; g[3] += a.w;
+        g[4] += b.x; g[5] += b.y; g[6] += b.z; g[7] += b.w;
+        g[8] += c.x;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 4)
 splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
                       const float* __restrict__ quats, const float* __restrict__ logits,
                       const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
                       const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
-                      float* __restrict__ gMeans, float* __restrict__ gLogScales, float* __restrict__ gQuats,
-                      float* __restrict__ gLogits, float* __restrict__ gSh) {
+                      uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
+                      float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh) {
     const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= f.count) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool live = i < f.count;
     const uint32_t slot = f.base + i;
-    const uint32_t n = touched[slot];
+    uint32_t n = live ? touched[slot] : 0u;
+    const uint32_t first = n != 0 ? offsets[slot] : 0u;
+    // Reads stay inside the partials buffer even for a frame whose pairs
+    // overflowed their buffer (the host reports that frame as an error).
+    n = first >= partialPairs ? 0u : min(n, partialPairs - first);
+    float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const float4* part4 = reinterpret_cast<const float4*>(partials);
+    if (n <= kSolo) sum_partials(part4 + static_cast<size_t>(first) * 3, n, g);
+    uint32_t many = __ballot_sync(0xFFFFFFFFu, n > kSolo);
+    while (many != 0) {
+        const int owner = __ffs(many) - 1;
+        many &= many - 1;
+        const uint32_t on = __shfl_sync(0xFFFFFFFFu, n, owner);
+        const uint32_t of = __shfl_sync(0xFFFFFFFFu, first, owner);
+        float h[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const float4* p = part4 + static_cast<size_t>(of) * 3;
+        for (uint32_t k = lane; k < on; k += 32) {
+            const float4 a = __ldg(p + 3 * k), b = __ldg(p + 3 * k + 1), c = __ldg(p + 3 * k + 2);
+            h[0] += a.x; h[1] += a.y; h[2] += a.z; h[3] += a.w;
+            h[4] += b.x; h[5] += b.y; h[6] += b.z; h[7] += b.w;
+            h[8] += c.x;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) h[q] += __shfl_xor_sync(0xFFFFFFFFu, h[q], d);
+        }
+        if (static_cast<int>(lane) == owner) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) g[q] = h[q];
+        }
+    }
+    if (!live) return;
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
     float* gshRow = gSh + static_cast<size_t>(i) * 48;
     if (n == 0) {
@@ -68,15 +118,6 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
 #pragma unroll
         for (int q = 0; q < 12; ++q) out[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
-        // The splat's summed partials.
-        float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const float4* part = reinterpret_cast<const float4*>(partials) + static_cast<size_t>(offsets[slot]) * 3;
-        for (uint32_t k = 0; k < n; ++k) {
-            const float4 a = part[3 * k], b = part[3 * k + 1], c = part[3 * k + 2];
-            g[0] += a.x; g[1] += a.y; g[2] += a.z; g[3] += a.w;
-            g[4] += b.x; g[5] += b.y; g[6] += b.z; g[7] += b.w;
-            g[8] += c.x;
-        }
         const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
 
         // ---- forward intermediates ------------------------------------------
@@ -298,11 +339,13 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
 
 cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
-                                  const uint32_t* offsets, const float* partials, float* gMeans, float* gLogScales,
-                                  float* gQuats, float* gLogits, float* gSh, cudaStream_t stream) {
+                                  const uint32_t* offsets, const float* partials, uint32_t partialPairs,
+                                  float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
+                                  cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     splat_backward_kernel<<<(f.count + kThreads - 1) / kThreads, kThreads, 0, stream>>>(
-        f, means, logScales, quats, logits, sh, touched, offsets, partials, gMeans, gLogScales, gQuats, gLogits, gSh);
+        f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales, gQuats,
+        gLogits, gSh);
     return cudaGetLastError();
 }
 

@@ -129,3 +129,31 @@ def test_gradients_match_fp64_finite_differences(rasterizer):
     err = np.abs(gpu - fd)
     # per parameter: within REL of its own value or of the largest sampled gradient
     assert np.all(err <= REL * np.abs(fd) + REL * scale), (err / scale).max()
+
+
+def test_an_enqueued_frame_that_overflows_is_reported_and_the_redraw_is_exact():
+    """Training frames after the first of a shape are only enqueued. One that
+    emits more pairs than the buffer holds is reported as OVERFLOW when its
+    counts are read (here by the debug view), with the buffers grown, and the
+    same frame drawn again equals the oracle bit for bit."""
+    from lucabrtrender_b200 import _abi
+    raster = L.TileRasterizer.create(0)
+    try:
+        p = TF.make_params(3000, 12, log_scale_mean=-2.0)
+        far, settings = TF.frame(96, 96, eye=(0.0, 0.0, 8.0))     # ~7.1k pairs: sizes the buffers (12k)
+        near, _ = TF.frame(96, 96, eye=(0.0, 0.0, 1.2))           # ~21k pairs
+        gpu_forward(raster, p, far, settings)
+        gpu_forward(raster, p, far, settings)
+        raster.debug_arrays()
+        gpu_forward(raster, p, near, settings)
+        with pytest.raises(L.LrtError) as info:
+            raster.debug_arrays()
+        assert info.value.code == _abi.OVERFLOW
+        _, colour, _ = gpu_forward(raster, p, near, settings)
+        dbg = raster.debug_arrays()
+        pr = L.projection_for(near, 96, 96).struct()
+        ref = ora.train_render(pr, TF.raw_cloud(p), settings.struct())
+        assert np.array_equal(dbg["ranges"].cpu().numpy().view(np.uint32), ref["ranges"])
+        assert np.abs(colour.detach().cpu().numpy() - ref["colour"]).max() <= 1e-5
+    finally:
+        raster.close()
