@@ -241,10 +241,19 @@ int lrt_projection_for(const lrt_camera* camera, uint32_t width, uint32_t height
  * coefficients, rgb per basis; 16-byte aligned). The forward is the plain
  * forward with scale exp(log_scale), opacity sigmoid(logit) and base colour
  * 0.5 + SH0 * DC, without the packed layout's quantisation. No reference
- * counterpart: the reference renders only. */
+ * counterpart: the reference renders only.
+ *
+ * flags: LRT_TRAIN_SORT_VALUES carries each pair's emit index (what the
+ * backward pass indexes its per-pair partials by) through the pair sort as a
+ * 32-bit value. By default it is the pair word's low field instead, with a
+ * 4-byte emit-index -> slot map the blend reads, which makes the sort move
+ * 8 bytes per pair, not 12; the value form is chosen by itself when tile,
+ * depth key and emit index do not fit 64 bits (beyond 2^(40 - tile bits)
+ * pairs). Both give the same images and gradients. */
+#define LRT_TRAIN_SORT_VALUES 1u
 typedef struct lrt_train_params {
     uint32_t count;
-    uint32_t reserved;
+    uint32_t flags;
     const void* means;
     const void* log_scales;
     const void* quats;

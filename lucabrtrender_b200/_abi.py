@@ -24,6 +24,7 @@ DEVICE_FAILURE = 6
 OUT_OF_MEMORY = 8
 INTERNAL_ERROR = 10
 OVERFLOW = 11
+TRAIN_SORT_VALUES = 1   # lrt_train_params.flags
 TIMEOUT = 12
 
 STATUS_NAMES = {
@@ -137,7 +138,7 @@ class BatchStats(C.Structure):
 
 class TrainParams(C.Structure):
     _fields_ = [
-        ("count", C.c_uint32), ("reserved", C.c_uint32),
+        ("count", C.c_uint32), ("flags", C.c_uint32),
         ("means", C.c_void_p), ("log_scales", C.c_void_p), ("quats", C.c_void_p),
         ("opacity_logits", C.c_void_p), ("sh", C.c_void_p),
     ]

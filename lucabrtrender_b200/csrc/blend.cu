@@ -118,6 +118,7 @@ template <bool kTrain>
 __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
                                            const uint2* __restrict__ ranges,
                                            const unsigned long long* __restrict__ pairs,
+                                           const uint32_t* __restrict__ emitSlot,
                                            const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut,
                                            float* __restrict__ depthOut, float4* __restrict__ pixState,
                                            uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
@@ -136,7 +137,10 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         const uint32_t cnt = min(kBatch, end - at);
         if (tid == 0) mbar_arrive_expect_tx(&sBar[buf], cnt * static_cast<uint32_t>(sizeof(ProjRecord)));
         if (tid < cnt) {
-            const uint32_t slot = static_cast<uint32_t>(pairs[at + tid] & slotMask);
+            uint32_t slot = static_cast<uint32_t>(pairs[at + tid] & slotMask);
+            if constexpr (kTrain) {
+                if (emitSlot != nullptr) slot = emitSlot[slot];   // the low field is the emit index
+            }
             fence_proxy_async_smem();
             bulk_copy_record(&sRec[buf][tid], proj + slot, &sBar[buf]);
         }
@@ -241,6 +245,7 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
 template <bool kTrain>
 __global__ void __launch_bounds__(kBlendThreads)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+             const uint32_t* __restrict__ emitSlot,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
              float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
     __shared__ __align__(128) ProjRecord sRec[2][kBatch];
@@ -254,7 +259,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
     const uint32_t tile = blockIdx.x;
-    blend_tile<kTrain>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, proj, colourOut, depthOut,
+    blend_tile<kTrain>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emitSlot, proj, colourOut, depthOut,
                        pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
 }
 
@@ -293,7 +298,7 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
         vbp.height = v.height;
         vbp.tilesX = v.tilesX;
         const uint32_t local = item - v.tileBase;
-        blend_tile<false>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, proj + v.recordBase,
+        blend_tile<false>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr, proj + v.recordBase,
                           v.colour, v.depth, nullptr, nullptr, err, sRec, sBox, sBar, phase0, phase1);
     }
 }
@@ -357,7 +362,8 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], uint3
 // splat's pairs are contiguous there, so a per-splat sum needs no atomics.
 __global__ void __launch_bounds__(kBlendThreads)
 blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
-                      const uint32_t* __restrict__ emit, const ProjRecord* __restrict__ proj,
+                      const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
+                      const ProjRecord* __restrict__ proj,
                       const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
                       const float4* __restrict__ gradColour, float* __restrict__ partials) {
     constexpr uint32_t kB = 128;
@@ -413,7 +419,8 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
     // Pairs past every pixel's last contributor get zero partials here, so the
     // buffer needs no clearing beforehand.
     for (uint32_t k = maxLast + tid; k < range.y; k += kBlendThreads) {
-        float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(emit[k]) * kGradStride);
+        const uint32_t e = emitSlot != nullptr ? static_cast<uint32_t>(pairs[k] & slotMask) : emit[k];
+        float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(e) * kGradStride);
         out[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         out[1] = out[0];
         out[2] = out[0];
@@ -426,9 +433,12 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
         const uint32_t bStart = bEnd - start > kB ? bEnd - kB : start;
         const uint32_t cnt = bEnd - bStart;
         if (tid < cnt) {
-            const unsigned long long word = pairs[bStart + tid];
-            sRec[tid] = proj[static_cast<uint32_t>(word & slotMask)];
-            sEmit[tid] = emit[bStart + tid];
+            const uint32_t low = static_cast<uint32_t>(pairs[bStart + tid] & slotMask);
+            // The emit index is the word's low field (and the slot comes from
+            // the emit-slot map), or it travelled through the sort as a value.
+            const uint32_t slot = emitSlot != nullptr ? emitSlot[low] : low;
+            sRec[tid] = proj[slot];
+            sEmit[tid] = emitSlot != nullptr ? low : emit[bStart + tid];
         }
         if (tid < (kBlendThreads / 32) * (kB / 32)) (&sHit[0][0])[tid] = 0u;
         __syncthreads();
@@ -567,7 +577,8 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_kernel<false><<<tiles, kBlendThreads, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, nullptr, nullptr, err);
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), nullptr, proj, colour, depth, nullptr, nullptr,
+        err);
     return cudaGetLastError();
 }
 
@@ -580,25 +591,26 @@ cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, u
     return cudaGetLastError();
 }
 
-cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
-                               float4* colour, float* depth, float4* pixState, uint32_t* pixLast, uint32_t* err,
-                               cudaStream_t stream) {
+cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                               const uint32_t* emitSlot, const ProjRecord* proj, float4* colour, float* depth,
+                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_kernel<true><<<tiles, kBlendThreads, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, pixState, pixLast, err);
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
+        pixLast, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
-                                  const uint32_t* emit, const ProjRecord* proj, const float4* pixState,
-                                  const uint32_t* pixLast, const float4* gradColour, float* partials,
-                                  cudaStream_t stream) {
+                                  const uint32_t* emit, const uint32_t* emitSlot, const ProjRecord* proj,
+                                  const float4* pixState, const uint32_t* pixLast, const float4* gradColour,
+                                  float* partials, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_backward_kernel<<<tiles, kBlendThreads, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, proj, pixState, pixLast, gradColour,
-        partials);
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
+        gradColour, partials);
     return cudaGetLastError();
 }
 

@@ -33,8 +33,8 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
                                       uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
-                                      uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs, uint32_t* values,
-                                      uint32_t capacity, cudaStream_t stream);
+                                      uint32_t lastPartition, uint32_t lowBits, uint64_t* pairs, uint32_t* values,
+                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream);
 
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
@@ -59,13 +59,16 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
 cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
                                const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
                                uint32_t* err, uint32_t blocks, cudaStream_t stream);
-cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
-                               float4* colour, float* depth, float4* pixState, uint32_t* pixLast, uint32_t* err,
-                               cudaStream_t stream);
+// Training frames: `emitSlot` (when not null) maps a pair word's low field,
+// the pair's emit index, to its slot; otherwise the low field is the slot and
+// `emit` holds each sorted pair's emit index.
+cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                               const uint32_t* emitSlot, const ProjRecord* proj, float4* colour, float* depth,
+                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream);
 cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
-                                  const uint32_t* emit, const ProjRecord* proj, const float4* pixState,
-                                  const uint32_t* pixLast, const float4* gradColour, float* partials,
-                                  cudaStream_t stream);
+                                  const uint32_t* emit, const uint32_t* emitSlot, const ProjRecord* proj,
+                                  const float4* pixState, const uint32_t* pixLast, const float4* gradColour,
+                                  float* partials, cudaStream_t stream);
 
 cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,

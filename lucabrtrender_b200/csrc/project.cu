@@ -236,11 +236,14 @@ struct RawSource {
     }
 };
 
-// Extra outputs of the training forward: each slot's first pair index, and
-// each pair's emit index carried through the sort as its value.
+// Extra outputs of the training forward: each slot's first pair index, and a
+// way back from each sorted pair to its emit index. Either the emit index
+// rides through the sort as the pair's value (`values`), or it is the pair
+// word's low field and `emitSlot` maps it to the slot (`emitSlot`).
 struct TrainOutputs {
     uint32_t* offsets;
     uint32_t* values;
+    uint32_t* emitSlot;
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
@@ -278,13 +281,21 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 
 struct PairSink {
     unsigned long long* pairs;
-    uint32_t* values;   // training only: the emit index of each pair
+    uint32_t* values;     // training, emit index as a sort value
+    uint32_t* emitSlot;   // training, emit index as the low field
     uint32_t capacity;
     uint32_t* err;
-    __device__ __forceinline__ void put(uint64_t at, unsigned long long word) const {
+    // `word` holds the tile and the depth key above the low field, which is
+    // filled here: the slot, or the emit index itself.
+    __device__ __forceinline__ void put(uint64_t at, unsigned long long word, uint32_t slot) const {
         if (at < capacity) {
-            pairs[at] = word;
-            if (values != nullptr) values[at] = static_cast<uint32_t>(at);
+            if (emitSlot != nullptr) {
+                pairs[at] = word | at;
+                emitSlot[at] = slot;
+            } else {
+                pairs[at] = word | slot;
+                if (values != nullptr) values[at] = static_cast<uint32_t>(at);
+            }
         } else {
             atomicOr(err, kErrOverflow);
         }
@@ -297,7 +308,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                     uint32_t stageWords, uint32_t shVector,
                     ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
                     uint32_t* __restrict__ keysOut, uint32_t* __restrict__ counters, uint64_t* __restrict__ status,
-                    uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits,
+                    uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t lowBits,
                     unsigned long long* __restrict__ pairs, uint32_t capacity) {
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
@@ -305,7 +316,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     __shared__ uint32_t sStart[kProjectThreads + 1];       // block-relative pair offset of each splat
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];  // the same over masked splats only
     __shared__ unsigned long long sMask[kProjectThreads];
-    __shared__ unsigned long long sLow[kProjectThreads];   // depth key << slotBits | slot
+    __shared__ unsigned long long sLow[kProjectThreads];   // depth key << lowBits
     __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
     __shared__ uint32_t sWidth[kProjectThreads];
     __shared__ unsigned long long sBase;
@@ -532,7 +543,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     sSmallStart[tid] = smallStart;
     const bool writeOffset = train.offsets != nullptr && inRange;
     sMask[tid] = mask;
-    sLow[tid] = (static_cast<unsigned long long>(key) << slotBits) | slot;
+    sLow[tid] = static_cast<unsigned long long>(key) << lowBits;
     sRect[tid] = rect.x | (rect.y << 16);
     sWidth[tid] = rw;
     if (tid == 0) {
@@ -574,8 +585,9 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     __syncthreads();
     const unsigned long long blockBase = sBase;
     if (writeOffset) train.offsets[slot] = static_cast<uint32_t>(blockBase + start);
-    const PairSink sink{pairs, train.values, capacity, err};
-    const uint32_t tileShift = 24 + slotBits;
+    const PairSink sink{pairs, train.values, train.emitSlot, capacity, err};
+    const uint32_t tileShift = 24 + lowBits;
+    const uint32_t slotBase = slot - tid;   // the slot of the block's first splat
 
     // Masked splats: the whole block writes their pairs, one per thread per step.
     for (uint32_t j = tid; j < smallTotal; j += kProjectThreads) {
@@ -593,7 +605,8 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         const uint32_t tx = (sRect[s] & 0xFFFFu) + bit % w;
         const uint32_t ty = (sRect[s] >> 16) + bit / w;
         sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
-                 (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s]);
+                 (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s],
+                 slotBase + s);
     }
     // Larger splats: their warp repeats the tile test 32 tiles at a time.
     uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && area > kMaskArea);
@@ -616,7 +629,8 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
             if (hit) {
                 sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
-                         (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | low);
+                         (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | low,
+                         slotBase + s);
             }
             at += static_cast<uint32_t>(__popc(bal));
         }
@@ -656,7 +670,7 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
-    return launch(f, fDev, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr}, stage, proj, rects,
+    return launch(f, fDev, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr, nullptr}, stage, proj, rects,
                   touched, keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity,
                   stream);
 }
@@ -665,13 +679,13 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
                                       uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
-                                      uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs, uint32_t* values,
-                                      uint32_t capacity, cudaStream_t stream) {
+                                      uint32_t lastPartition, uint32_t lowBits, uint64_t* pairs, uint32_t* values,
+                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     // The DC triple is read from the staged row too, so it is always staged.
     return launch(f, nullptr, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
-                  TrainOutputs{offsets, values}, true, proj, rects, touched, keys, counters, status, ticket,
-                  partitionBase, lastPartition, slotBits, pairs, capacity, stream);
+                  TrainOutputs{offsets, values, emitSlot}, true, proj, rects, touched, keys, counters, status, ticket,
+                  partitionBase, lastPartition, lowBits, pairs, capacity, stream);
 }
 
 }  // namespace lrt

@@ -55,7 +55,8 @@ struct lrt_rast {
     lrt::FrameParams trainFrame{};
     lrt::BlendParams trainBlend{};
     const uint64_t* trainSorted = nullptr;
-    const uint32_t* trainSortedValues = nullptr;
+    const uint32_t* trainSortedValues = nullptr;   // emit index per sorted pair (value layout)
+    const uint32_t* trainEmitSlot = nullptr;       // slot per emit index (low-field layout)
     uint32_t trainPairs = 0;
     double lastBackwardMs[2] = {0.0, 0.0};
     // Batches of views.
@@ -378,25 +379,36 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     bp.height = s->height;
     bp.tilesX = tilesX;
     bp.tilesY = tilesY;
-    bp.slotBits = slotBits;
-    bp.tileShift = 24 + slotBits;
     bp.depthMode = s->depth_mode;
     bp.linearise = s->linearise ? 1u : 0u;
     bp.depthThreshold = s->depth_threshold;
     for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
     FrameParams lastParams{};
+    // Training frames carry each pair's emit index to the backward pass. It is
+    // the pair word's low field (with an emit-index -> slot map for the blend)
+    // when tile, depth key and index fit 64 bits, else a sort value beside the
+    // word. The low field is the slot otherwise.
+    const bool valuesAsked = train && !clouds.empty() && clouds[0].train != nullptr &&
+                             (clouds[0].train->flags & LRT_TRAIN_SORT_VALUES) != 0;
+    bool lowIsEmit = false;
+    uint32_t lowBits = slotBits;
     for (int attempt = 0; attempt < 2; ++attempt) {
+        lowIsEmit = train && !valuesAsked && keyBits + bits_for(r->pairCap) <= 64;
+        lowBits = lowIsEmit ? bits_for(r->pairCap) : slotBits;
+        bp.slotBits = lowBits;
+        bp.tileShift = 24 + lowBits;
         LRT_CUDA(r, ensure(r->pairs, size_t{r->pairCap} * 8), "pairs");
         LRT_CUDA(r, ensure(r->pairsAlt, size_t{r->pairCap} * 8), "pairs");
         if (train) {
             LRT_CUDA(r, ensure(r->pairValues, size_t{r->pairCap} * 4), "pair values");
-            LRT_CUDA(r, ensure(r->pairValuesAlt, size_t{r->pairCap} * 4), "pair values");
+            if (!lowIsEmit) LRT_CUDA(r, ensure(r->pairValuesAlt, size_t{r->pairCap} * 4), "pair values");
         }
         LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(r->pairCap, keyBits)), "sort scratch");
         LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
         LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, stream), "projection scratch");
         uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
-        uint32_t* valueBuf = train ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
+        uint32_t* valueBuf = train && !lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
+        uint32_t* emitSlot = train && lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
 
         // --- project, count, emit --------------------------------------------
         LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
@@ -413,8 +425,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<const uint16_t*>(t.sh), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
                              static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->trainOffsets.ptr),
-                             counters, status, tickets + launch, partitionBase, lastPartition, slotBits, pairBuf,
-                             valueBuf, r->pairCap, stream),
+                             counters, status, tickets + launch, partitionBase, lastPartition, lowBits, pairBuf,
+                             valueBuf, emitSlot, r->pairCap, stream),
                          "project");
             } else {
                 LRT_CUDA(r,
@@ -437,13 +449,14 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         bool inAlt = false;
         LRT_CUDA(r,
                  lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), valueBuf,
-                                      train ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr, counters + 1,
-                                      r->pairCap, slotBits, keyBits, r->sortScratch.ptr, err, &inAlt, stream),
+                                      valueBuf != nullptr ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr,
+                                      counters + 1, r->pairCap, lowBits, keyBits, r->sortScratch.ptr, err, &inAlt,
+                                      stream),
                  "pair sort");
         sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
-        if (train) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;
+        if (valueBuf != nullptr) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;
         LRT_CUDA(r,
-                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + slotBits,
+                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + lowBits,
                                     static_cast<uint2*>(r->ranges.ptr), tiles, stream),
                  "ranges");
         LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
@@ -451,7 +464,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         // --- blend ------------------------------------------------------------------
         if (train) {
             LRT_CUDA(r,
-                     lrt::launch_blend_train(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
+                     lrt::launch_blend_train(bp, static_cast<uint2*>(r->ranges.ptr), sorted, emitSlot,
                                              static_cast<ProjRecord*>(r->proj.ptr),
                                              static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth),
                                              static_cast<float4*>(r->pixState.ptr),
@@ -475,7 +488,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
             r->debug.ranges = r->ranges.ptr;
             r->debug.slots = slots;
             r->debug.tiles = tiles;
-            r->debug.slot_bits = slotBits;
+            r->debug.slot_bits = lowBits;
             r->debug.depth_bits = 24;
             r->debug.tile_bits = tileBits;
             r->pendingStream = stream;
@@ -484,6 +497,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                 r->trainBlend = bp;
                 r->trainSorted = sorted;
                 r->trainSortedValues = sortedValues;
+                r->trainEmitSlot = emitSlot;
                 r->trainPairs = r->pairCap;   // an upper bound until the status is read
                 r->trainReady = true;
                 r->trainPending = true;
@@ -515,7 +529,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     r->debug.slots = slots;
     r->debug.pairs_count = pairs;
     r->debug.tiles = tiles;
-    r->debug.slot_bits = slotBits;
+    r->debug.slot_bits = lowBits;
     r->debug.depth_bits = 24;
     r->debug.tile_bits = tileBits;
     r->debug.visible = visible;
@@ -526,6 +540,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         r->trainBlend = bp;
         r->trainSorted = sorted;
         r->trainSortedValues = sortedValues;
+        r->trainEmitSlot = lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
         r->trainPairs = pairs;
         r->trainReady = true;
     }
@@ -665,7 +680,7 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
     LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
     LRT_CUDA(r,
              lrt::launch_blend_backward(r->trainBlend, static_cast<uint2*>(r->ranges.ptr), r->trainSorted,
-                                        r->trainSortedValues, static_cast<ProjRecord*>(r->proj.ptr),
+                                        r->trainSortedValues, r->trainEmitSlot, static_cast<ProjRecord*>(r->proj.ptr),
                                         static_cast<float4*>(r->pixState.ptr), static_cast<uint32_t*>(r->pixLast.ptr),
                                         static_cast<const float4*>(gradColour), static_cast<float*>(r->partials.ptr),
                                         stream),

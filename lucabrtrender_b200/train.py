@@ -6,6 +6,10 @@ quats [N,4] as (w, x, y, z) (normalised in the forward), opacity_logits [N],
 sh [N,16,3] (DC first). The SH coefficients are kept in fp32 by the caller
 and read by the kernels as fp16; their gradient is fp32. The colour image
 [H,W,4] is differentiable; depth is not.
+
+``sort_values=True`` makes the pair sort carry each pair's emit index as a
+value (``LRT_TRAIN_SORT_VALUES``) instead of in the pair word's low field;
+images and gradients are the same either way.
 """
 from __future__ import annotations
 
@@ -21,7 +25,7 @@ from .raster import FrameStats, RenderSettings, TileRasterizer, _stream_ptr
 class _Rasterize(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, log_scales, quats, opacity_logits, sh, raster: TileRasterizer, projection: Projection,
-                settings: RenderSettings):
+                settings: RenderSettings, sort_values: bool):
         dev = means.device
         n = means.shape[0]
         means = means.contiguous().float()
@@ -33,6 +37,7 @@ class _Rasterize(torch.autograd.Function):
         depth = torch.empty((settings.height, settings.width), dtype=torch.float32, device=dev)
         p = _abi.TrainParams()
         p.count = n
+        p.flags = _abi.TRAIN_SORT_VALUES if sort_values else 0
         p.means, p.log_scales, p.quats = means.data_ptr(), log_scales.data_ptr(), quats.data_ptr()
         p.opacity_logits, p.sh = opacity_logits.data_ptr(), sh16.data_ptr()
         t = _abi.TargetsStruct()
@@ -62,14 +67,14 @@ class _Rasterize(torch.autograd.Function):
         raster = ctx.raster
         raster._check(_abi.load().lrt_rast_train_backward(raster._handle, gc.data_ptr(), C.byref(grads),
                                                           _stream_ptr(None)))
-        return g[0], g[1], g[2], g[3], g[4], None, None, None
+        return g[0], g[1], g[2], g[3], g[4], None, None, None, None
 
 
 def rasterize(means, log_scales, quats, opacity_logits, sh, view: Camera | Projection, settings: RenderSettings,
-              raster: TileRasterizer):
+              raster: TileRasterizer, sort_values: bool = False):
     """Render the differentiable cloud; returns (colour [H,W,4], depth [H,W])."""
     projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
-    return _Rasterize.apply(means, log_scales, quats, opacity_logits, sh, raster, projection, settings)
+    return _Rasterize.apply(means, log_scales, quats, opacity_logits, sh, raster, projection, settings, sort_values)
 
 
 def backward_times(raster: TileRasterizer) -> tuple[float, float]:

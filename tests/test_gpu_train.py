@@ -37,18 +37,19 @@ def to_cuda(p, requires_grad=False):
     return out
 
 
-def gpu_forward(rasterizer, p, cam, settings, requires_grad=False):
+def gpu_forward(rasterizer, p, cam, settings, requires_grad=False, sort_values=False):
     t = to_cuda(p, requires_grad)
     colour, depth = L.rasterize(t["means"], t["log_scales"], t["quats"], t["logits"], t["sh"], cam, settings,
-                                rasterizer)
+                                rasterizer, sort_values=sort_values)
     return t, colour, depth
 
 
+@pytest.mark.parametrize("sort_values", [False, True], ids=["emit-low-field", "emit-sort-value"])
 @pytest.mark.parametrize("n,size,seed", [(3000, 96, 5), (20000, 200, 6)])
-def test_train_forward_bit_exact(rasterizer, n, size, seed):
+def test_train_forward_bit_exact(rasterizer, n, size, seed, sort_values):
     p = TF.make_params(n, seed)
     cam, settings = TF.frame(size, size)
-    _, colour, depth = gpu_forward(rasterizer, p, cam, settings)
+    _, colour, depth = gpu_forward(rasterizer, p, cam, settings, sort_values=sort_values)
     dbg = rasterizer.debug_arrays()
     pr = L.projection_for(cam, size, size).struct()
     ref = ora.train_render(pr, TF.raw_cloud(p), settings.struct())
@@ -77,8 +78,8 @@ def _crop_problem(p, cam, settings, crop, target):
     return G.CropProblem(G.camera_from(pr, st), crop, out["list_offsets"], out["list_slots"], target), out
 
 
-def _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target):
-    t, colour, _ = gpu_forward(rasterizer, p, cam, settings, requires_grad=True)
+def _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target, sort_values=False):
+    t, colour, _ = gpu_forward(rasterizer, p, cam, settings, requires_grad=True, sort_values=sort_values)
     x0, y0, w, h = crop
     tgt = torch.from_numpy(target).cuda()
     loss = torch.abs(colour[y0:y0 + h, x0:x0 + w, :3] - tgt).sum() / (3.0 * w * h)
@@ -86,14 +87,15 @@ def _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target):
     return {k: v.grad.detach().cpu().numpy() for k, v in t.items()}, float(loss.detach())
 
 
-def test_gradients_match_the_fp64_per_pixel_oracle_on_a_crop(rasterizer):
+@pytest.mark.parametrize("sort_values", [False, True], ids=["emit-low-field", "emit-sort-value"])
+def test_gradients_match_the_fp64_per_pixel_oracle_on_a_crop(rasterizer, sort_values):
     p = TF.make_params(6000, 8)
     cam, settings = TF.frame(128, 128)
     crop = (32, 32, 64, 64)
     target = np.random.default_rng(3).uniform(0, 1, (64, 64, 3))
     prob, _ = _crop_problem(p, cam, settings, crop, target)
     want, loss64 = G.gradients(prob, p)
-    got, loss32 = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target)
+    got, loss32 = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target, sort_values)
     assert abs(loss32 - loss64) <= 1e-5 * max(1.0, abs(loss64))
     used = prob.used
     report = {}
@@ -157,3 +159,17 @@ def test_an_enqueued_frame_that_overflows_is_reported_and_the_redraw_is_exact():
         assert np.abs(colour.detach().cpu().numpy() - ref["colour"]).max() <= 1e-5
     finally:
         raster.close()
+
+
+def test_both_emit_index_layouts_give_the_same_gradients_bit_for_bit(rasterizer):
+    """The emit index as the pair word's low field or as a sort value: the same
+    pair order, the same partial slots, so the same sums in the same order."""
+    p = TF.make_params(20000, 13)
+    cam, settings = TF.frame(200, 200)
+    crop = (0, 0, 200, 200)
+    target = np.random.default_rng(5).uniform(0, 1, (200, 200, 3))
+    a, la = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target, sort_values=False)
+    b, lb = _gpu_crop_gradients(rasterizer, p, cam, settings, crop, target, sort_values=True)
+    assert la == lb
+    for name in a:
+        assert np.array_equal(a[name].view(np.uint32), b[name].view(np.uint32)), name
