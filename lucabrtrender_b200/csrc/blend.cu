@@ -189,28 +189,34 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                 overlap = !(box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0);
             }
             uint32_t todo = __ballot_sync(0xFFFFFFFFu, overlap);
+            // Straight-line body with one warp-uniform skip: every lane computes
+            // the power, lanes still blending that pass the cut are candidates,
+            // and the rest of the reference's step runs predicated on a hit.
             while (todo != 0) {
                 const uint32_t j = c + static_cast<uint32_t>(__ffs(todo)) - 1u;
                 todo &= todo - 1u;
-                if (done) continue;
                 const float4 screen = batch[j].screen;
                 const float4 conic = batch[j].conic;
                 const float dx = pxf - screen.x;
                 const float dy = pyf - screen.y;
                 const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
-                if (power > screen.w) continue;
-                const float alpha = fminf(0.99f, conic.w * lrt_exp(-0.5f * power));
-                if (alpha < 1.0f / 255.0f) continue;
-                const float4 colour = batch[j].colour;
-                const float weight = T * alpha;
-                r = r + weight * colour.x;
-                g = g + weight * colour.y;
-                b = b + weight * colour.z;
-                depthSum = depthSum + weight * screen.z;
-                T = T * (1.0f - alpha);
-                if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
-                if (kTrain) last = at + j + 1;
-                if (T < 1e-4f) done = true;
+                const bool candidate = !done && !(power > screen.w);
+                if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
+                // A candidate's power lies in [0, 9] (the cut is at most 9), so
+                // the exponent's argument is in range; others discard it.
+                const float alpha = fminf(0.99f, conic.w * lrt_exp_in_range(-0.5f * power));
+                if (candidate && !(alpha < 1.0f / 255.0f)) {
+                    const float4 colour = batch[j].colour;
+                    const float weight = T * alpha;
+                    r = r + weight * colour.x;
+                    g = g + weight * colour.y;
+                    b = b + weight * colour.z;
+                    depthSum = depthSum + weight * screen.z;
+                    T = T * (1.0f - alpha);
+                    if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
+                    if (kTrain) last = at + j + 1;
+                    if (T < 1e-4f) done = true;
+                }
             }
         }
         if (__syncthreads_and(done ? 1 : 0)) {

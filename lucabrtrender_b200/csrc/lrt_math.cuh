@@ -99,6 +99,25 @@ LRT_HD float lrt_exp(float x) {
     return p * bits_float(static_cast<uint32_t>(e + 127) << 23);
 }
 
+// lrt_exp without its range checks, for -87 <= x <= 88 (where no check
+// fires, so the result has the same bits); outside that range it returns an
+// unspecified value. For hot loops whose argument is known to be in range.
+LRT_HD float lrt_exp_in_range(float x) {
+    const float n = lrt_rint(x * 1.44269504088896340736f);
+    float r = lrt_fma(-n, 0.693147182464599609375f, x);
+    r = lrt_fma(-n, -1.904654299957768e-09f, r);
+    float p = 1.984126984126984e-4f;
+    p = lrt_fma(p, r, 1.388888888888889e-3f);
+    p = lrt_fma(p, r, 8.333333333333333e-3f);
+    p = lrt_fma(p, r, 4.166666666666666e-2f);
+    p = lrt_fma(p, r, 1.666666666666667e-1f);
+    p = lrt_fma(p, r, 0.5f);
+    p = lrt_fma(p, r, 1.0f);
+    p = lrt_fma(p, r, 1.0f);
+    const int e = static_cast<int>(n);
+    return p * bits_float(static_cast<uint32_t>(e + 127) << 23);
+}
+
 LRT_HD float lrt_log(float x) {
     if (x != x) return x;
     if (x < 0.0f) return NAN;
