@@ -416,6 +416,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
         }
     }
     const float Tfinal = T;
+    const float gTT = -gT * Tfinal;   // the final transmittance's share of every dL/dalpha
     if (tid == 0) sMaxLast = start;
     __syncthreads();
     if (inside) atomicMax(&sMaxLast, myLast);
@@ -477,67 +478,66 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                 todo &= ~(1u << bit);
                 const uint32_t j = static_cast<uint32_t>(c) + bit;
                 float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-                bool hit = false;
-                if (live && bStart + j < myLast) {
-                    const float4 screen = sRec[j].screen;
-                    const float4 conic = sRec[j].conic;
-                    const float dx = pxf - screen.x;
-                    const float dy = pyf - screen.y;
-                    const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
-                    if (!(power > screen.w)) {
-                        // The forward's alpha decides who contributed, so it is
-                        // taken from the exact exponential wherever the fast one
-                        // (relative error below 1e-6 for these arguments) lies
-                        // within 1e-5 of either threshold; elsewhere both sides
-                        // of a threshold agree and the fast value serves.
-                        float e = __expf(-0.5f * power);
-                        float raw = conic.w * e;
-                        if (fabsf(raw - 1.0f / 255.0f) <= 1e-5f / 255.0f || fabsf(raw - 0.99f) <= 0.99e-5f) {
-                            e = lrt_exp(-0.5f * power);
-                            raw = conic.w * e;
-                        }
-                        const float alpha = fminf(0.99f, raw);
-                        if (!(alpha < 1.0f / 255.0f)) {
-                            hit = true;
-                            // Gradients are checked against FP64 to a tolerance, not
-                            // bit for bit, so this part uses fused multiply-adds.
-                            const float4 col = sRec[j].colour;
-                            const float oneMinus = 1.0f - alpha;
-                            const float inv = __frcp_rn(oneMinus);
-                            const float Ti = T * inv;
-                            const float w = Ti * alpha;
-                            v[6] = gr * w;
-                            v[7] = gg * w;
-                            v[8] = gb * w;
-                            const float behind =
-                                __fmaf_rn(gr, col.x - Br, __fmaf_rn(gg, col.y - Bg, gb * (col.z - Bb)));
-                            const float dAlpha = __fmaf_rn(Ti, behind, -gT * Tfinal * inv);
-                            Br = __fmaf_rn(alpha, col.x - Br, Br);
-                            Bg = __fmaf_rn(alpha, col.y - Bg, Bg);
-                            Bb = __fmaf_rn(alpha, col.z - Bb, Bb);
-                            T = Ti;
-                            if (raw <= 0.99f) {
-                                v[5] = dAlpha * e;
-                                const float dPower = -0.5f * alpha * dAlpha;
-                                const float pdx = dPower * dx, pdy = dPower * dy;
-                                v[2] = pdx * dx;
-                                v[3] = 2.0f * pdx * dy;
-                                v[4] = pdy * dy;
-                                v[0] = -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
-                                v[1] = -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
-                            }
-                        }
+                const float4 screen = sRec[j].screen;
+                const float4 conic = sRec[j].conic;
+                const float dx = pxf - screen.x;
+                const float dy = pyf - screen.y;
+                const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
+                const bool candidate = live && bStart + j < myLast && !(power > screen.w);
+                if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
+                // The forward's alpha decides who contributed, so it is taken
+                // from the exact exponential wherever the fast one (relative
+                // error below 1e-6 for these arguments) lies within 1e-5 of
+                // either threshold; elsewhere both sides of a threshold agree
+                // and the fast value serves.
+                float e = __expf(-0.5f * power);
+                float raw = conic.w * e;
+                if (candidate && (fabsf(raw - 1.0f / 255.0f) <= 1e-5f / 255.0f || fabsf(raw - 0.99f) <= 0.99e-5f)) {
+                    e = lrt_exp(-0.5f * power);
+                    raw = conic.w * e;
+                }
+                const float alpha = fminf(0.99f, raw);
+                const bool hit = candidate && !(alpha < 1.0f / 255.0f);
+                const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
+                if (hits == 0) continue;
+                written |= 1u << bit;
+                if (hit) {
+                    // Gradients are checked against FP64 to a tolerance, not
+                    // bit for bit, so this part uses fused multiply-adds.
+                    const float4 col = sRec[j].colour;
+                    const float oneMinus = 1.0f - alpha;   // in [0.01, 1]
+                    float inv;   // 1 / (1 - alpha) to about 1 ulp
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(oneMinus));
+                    const float Ti = T * inv;
+                    const float w = Ti * alpha;
+                    v[6] = gr * w;
+                    v[7] = gg * w;
+                    v[8] = gb * w;
+                    const float behind =
+                        __fmaf_rn(gr, col.x - Br, __fmaf_rn(gg, col.y - Bg, gb * (col.z - Bb)));
+                    const float dAlpha = __fmaf_rn(Ti, behind, gTT * inv);
+                    Br = __fmaf_rn(alpha, col.x - Br, Br);
+                    Bg = __fmaf_rn(alpha, col.y - Bg, Bg);
+                    Bb = __fmaf_rn(alpha, col.z - Bb, Bb);
+                    T = Ti;
+                    if (raw <= 0.99f) {
+                        v[5] = dAlpha * e;
+                        const float dPower = -0.5f * alpha * dAlpha;
+                        const float pdx = dPower * dx, pdy = dPower * dy;
+                        v[2] = pdx * dx;
+                        v[3] = 2.0f * pdx * dy;
+                        v[4] = pdy * dy;
+                        v[0] = -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
+                        v[1] = -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
                     }
                 }
-                const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
-                if (hits != 0) written |= 1u << bit;
-                if (hits != 0 && (hits & (hits - 1)) == 0) {
+                if ((hits & (hits - 1)) == 0) {
                     // one pixel of the warp: its values are the warp's sums
                     if (hit) {
 #pragma unroll
                         for (uint32_t k = 0; k < kGrads; ++k) sPart[warp][j][k] = v[k];
                     }
-                } else if (hits != 0) {
+                } else {
                     uint32_t idx;
                     const float sum = warp_reduce_scatter9(v, lane, idx);
                     if ((lane & 1u) == 0 && idx < kGrads) sPart[warp][j][idx] = sum;
