@@ -549,37 +549,60 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     if (tid == 0) {
         sStart[kProjectThreads] = blockTotal;
         sSmallStart[kProjectThreads] = smallTotal;
+    }
+    if (tid < 32) {
+        // Warp 0 looks back 32 partitions at a time: lane l reads the status
+        // of partition q - l; the nearest inclusive prefix ends the walk, and
+        // the aggregates up to it are summed across the warp. A partition in
+        // the window that has published nothing yet makes the warp read the
+        // window again (bounded).
         const uint32_t g = partitionBase + part;
-        cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
         uint64_t prefix = 0;
-        if (g == 0) {
-            mine.store(kFlagInclusive | blockTotal, cuda::memory_order_relaxed);
-        } else {
-            mine.store(kFlagAggregate | blockTotal, cuda::memory_order_relaxed);
+        if (lane == 0) {
+            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
+            mine.store((g == 0 ? kFlagInclusive : kFlagAggregate) | blockTotal, cuda::memory_order_relaxed);
+        }
+        if (g > 0) {
             int64_t q = static_cast<int64_t>(g) - 1;
             uint32_t spins = 0;
-            while (q >= 0) {
-                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[q]);
-                const uint64_t word = sref.load(cuda::memory_order_relaxed);
-                if ((word & ~kValueMask) == 0) {
+            while (true) {
+                const int64_t idx = q - static_cast<int64_t>(lane);
+                uint64_t word = kFlagInclusive;   // before partition 0: an empty inclusive prefix
+                if (idx >= 0) {
+                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[idx]);
+                    word = sref.load(cuda::memory_order_relaxed);
+                }
+                const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, (word & kFlagInclusive) != 0);
+                const uint32_t empty = __ballot_sync(0xFFFFFFFFu, (word & ~kValueMask) == 0);
+                const uint32_t first = inclusive != 0 ? static_cast<uint32_t>(__ffs(inclusive)) - 1u : 32u;
+                const uint32_t upTo = first < 32u ? (2u << first) - 1u : 0xFFFFFFFFu;   // lanes 0..first
+                if ((empty & upTo) != 0) {
                     if (++spins > kSpinLimit) {
-                        atomicOr(err, kErrTimeout);
+                        if (lane == 0) atomicOr(err, kErrTimeout);
                         break;
                     }
                     __nanosleep(32);
                     continue;
                 }
-                prefix += word & kValueMask;
-                if (word & kFlagInclusive) break;
-                --q;
+                uint64_t v = ((upTo >> lane) & 1u) ? (word & kValueMask) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                prefix += v;
+                if (first < 32u) break;
+                q -= 32;
             }
-            mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
+            if (lane == 0) {
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
+                mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
+            }
         }
-        sBase = prefix;
-        if (g == lastPartition) {
-            const uint64_t all = prefix + blockTotal;
-            if (all > 0xFFFFFFFFull) atomicOr(err, kErrTooManyPairs);
-            counters[1] = static_cast<uint32_t>(all);
+        if (lane == 0) {
+            sBase = prefix;
+            if (g == lastPartition) {
+                const uint64_t all = prefix + blockTotal;
+                if (all > 0xFFFFFFFFull) atomicOr(err, kErrTooManyPairs);
+                counters[1] = static_cast<uint32_t>(all);
+            }
         }
     }
     __syncthreads();

@@ -86,7 +86,7 @@ histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount
 }
 
 template <typename K, bool kValues>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
 onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
                 const uint32_t* __restrict__ hist, uint32_t* __restrict__ lookback,
@@ -125,19 +125,22 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     }
 
     // Stable rank inside the warp: peers with equal digits, lower lanes first;
-    // items in order.
+    // items in order. Each item's group leader adds the group's size to the
+    // warp's digit counter with a shared-memory atomic and passes the old
+    // count to its peers. A warp's atomics on one address take effect in
+    // issue order, so the items need no barrier between them and their
+    // latencies overlap.
     uint32_t rank[kSortItems];
     const uint32_t lowerLanes = (1u << lane) - 1u;
 #pragma unroll
     for (uint32_t j = 0; j < kSortItems; ++j) {
         const uint32_t d = dig[j];
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t prior = d < kDigits ? sWarpHist[warp][d] : 0u;
-        __syncwarp();
         const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers));
-        if (lane == leader && d < kDigits) sWarpHist[warp][d] = prior + static_cast<uint32_t>(__popc(peers));
-        rank[j] = prior + static_cast<uint32_t>(__popc(peers & lowerLanes));
-        __syncwarp();
+        uint32_t prior = 0;
+        if (lane == leader && d < kDigits) prior = atomicAdd(&sWarpHist[warp][d], static_cast<uint32_t>(__popc(peers)));
+        rank[j] = __shfl_sync(0xFFFFFFFFu, prior, static_cast<int>(leader)) +
+                  static_cast<uint32_t>(__popc(peers & lowerLanes));
     }
     __syncthreads();
 
