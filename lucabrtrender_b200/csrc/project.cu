@@ -247,7 +247,6 @@ struct TrainOutputs {
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
-constexpr uint32_t kMaskArea = 64;    // a touched-tile bitmask up to this many
 constexpr uint64_t kFlagAggregate = 1ull << 62;
 constexpr uint64_t kFlagInclusive = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
@@ -303,7 +302,7 @@ struct PairSink {
 };
 
 template <class Src>
-__global__ void __launch_bounds__(kProjectThreads)
+__global__ void __launch_bounds__(kProjectThreads, 4)
 project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
                     uint32_t stageWords, uint32_t shVector,
                     ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
@@ -447,17 +446,26 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
 
     // The exact touched count (splat_project.slang:148-160), row-major over
-    // the rectangle, with a bitmask of the touched tiles up to kMaskArea.
+    // the rectangle. Where it fits, a bitmask of the touched tiles is kept with
+    // rows `1 << sh` bits apart (sh: bits of the rectangle's width), so that a
+    // bit's tile is found by shifts; such splats are "masked".
     const uint32_t rw = alive ? rect.z - rect.x + 1 : 0;
-    const uint32_t area = alive ? rw * (rect.w - rect.y + 1) : 0;
+    const uint32_t rh = alive ? rect.w - rect.y + 1 : 0;
+    const uint32_t area = rw * rh;
+    const uint32_t sh = rw <= 1 ? 0u : 32u - static_cast<uint32_t>(__clz(rw - 1));
+    const bool masked = alive && rh <= (64u >> sh);
     uint32_t touched = 0;
     unsigned long long mask = 0;
-    if (alive && area <= kSmallArea) {
+    if (alive && area <= kSmallArea) {   // always masked: rh * 2^sh < 2 * area
+        uint32_t dx = 0, dy = 0;
         for (uint32_t k = 0; k < area; ++k) {
-            const uint32_t tx = rect.x + k % rw, ty = rect.y + k / rw;
-            if (tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, tx, ty)) {
-                mask |= 1ull << k;
+            if (tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, rect.x + dx, rect.y + dy)) {
+                mask |= 1ull << ((dy << sh) | dx);
                 touched += 1;
+            }
+            if (++dx == rw) {
+                dx = 0;
+                ++dy;
             }
         }
     }
@@ -467,24 +475,38 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         big &= big - 1;
         const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
         const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
+        const uint32_t sSh = __shfl_sync(0xFFFFFFFFu, sh, src);
+        const bool sMasked = __shfl_sync(0xFFFFFFFFu, masked ? 1u : 0u, src) != 0;
         const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
         const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
         const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
         const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
         const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+        // Lane l tests tiles l, l + 32, ... of the rectangle, row-major; its
+        // column and row advance by 32 tiles per step without a division.
+        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
+        uint32_t dx = lane % sW, dy = lane / sW;
         uint32_t count = 0;
-        unsigned long long m = 0;
+        uint32_t mLo = 0, mHi = 0;
         for (uint32_t base = 0; base < sArea; base += 32) {
-            const uint32_t k = base + lane;
-            const bool hit = k < sArea &&
-                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + k % sW, sY + k / sW);
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
-            count += static_cast<uint32_t>(__popc(bal));
-            if (base < kMaskArea) m |= static_cast<unsigned long long>(bal) << base;
+            const bool hit = base + lane < sArea &&
+                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + dx, sY + dy);
+            count += static_cast<uint32_t>(__popc(__ballot_sync(0xFFFFFFFFu, hit)));
+            if (sMasked) {
+                const uint32_t bit = (dy << sSh) | dx;
+                mLo |= __reduce_or_sync(0xFFFFFFFFu, hit && bit < 32u ? 1u << bit : 0u);
+                mHi |= __reduce_or_sync(0xFFFFFFFFu, hit && bit >= 32u ? 1u << (bit - 32u) : 0u);
+            }
+            dx += stepDx;
+            dy += stepDy;
+            if (dx >= sW) {
+                dx -= sW;
+                dy += 1;
+            }
         }
         if (lane == static_cast<uint32_t>(src)) {
             touched = count;
-            mask = sArea <= kMaskArea ? m : 0ull;
+            mask = sMasked ? (static_cast<unsigned long long>(mHi) << 32) | mLo : 0ull;
         }
     }
     alive = alive && touched != 0;
@@ -535,7 +557,6 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     if (lane == 0 && ballot != 0) atomicAdd(counters, static_cast<uint32_t>(__popc(ballot)));
 
     // Offsets: block scan, then decoupled look-back over the frame's partitions.
-    const bool masked = touched != 0 && area <= kMaskArea;
     uint32_t blockTotal = 0, smallTotal = 0;
     const uint32_t start = block_exclusive_scan(touched, sScan, &blockTotal);
     const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
@@ -545,7 +566,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     sMask[tid] = mask;
     sLow[tid] = static_cast<unsigned long long>(key) << lowBits;
     sRect[tid] = rect.x | (rect.y << 16);
-    sWidth[tid] = rw;
+    sWidth[tid] = rw | (sh << 16);
     if (tid == 0) {
         sStart[kProjectThreads] = blockTotal;
         sSmallStart[kProjectThreads] = smallTotal;
@@ -624,31 +645,32 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         unsigned long long m = sMask[s];
         for (; r > 0; --r) m &= m - 1;   // drop the r lowest set bits
         const uint32_t bit = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
-        const uint32_t w = sWidth[s];
-        const uint32_t tx = (sRect[s] & 0xFFFFu) + bit % w;
-        const uint32_t ty = (sRect[s] >> 16) + bit / w;
+        const uint32_t bsh = sWidth[s] >> 16;
+        const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
+        const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
         sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
                  (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s],
                  slotBase + s);
     }
-    // Larger splats: their warp repeats the tile test 32 tiles at a time.
-    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && area > kMaskArea);
+    // The rest: their warp repeats the tile test 32 tiles at a time.
+    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && !masked);
     while (large != 0) {
         const int src = __ffs(large) - 1;
         large &= large - 1;
         const uint32_t s = (tid & ~31u) + static_cast<uint32_t>(src);
         const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
-        const uint32_t sW = sWidth[s];
+        const uint32_t sW = sWidth[s] & 0xFFFFu;
         const uint32_t sX = sRect[s] & 0xFFFFu, sY = sRect[s] >> 16;
         const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
         const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
         const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
         unsigned long long at = blockBase + sStart[s];
         const unsigned long long low = sLow[s];
+        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
+        uint32_t dx = lane % sW, dy = lane / sW;
         for (uint32_t base = 0; base < sArea; base += 32) {
-            const uint32_t k = base + lane;
-            const uint32_t tx = sX + k % sW, ty = sY + k / sW;
-            const bool hit = k < sArea && tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, tx, ty);
+            const uint32_t tx = sX + dx, ty = sY + dy;
+            const bool hit = base + lane < sArea && tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, tx, ty);
             const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
             if (hit) {
                 sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
@@ -656,6 +678,12 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                          slotBase + s);
             }
             at += static_cast<uint32_t>(__popc(bal));
+            dx += stepDx;
+            dy += stepDy;
+            if (dx >= sW) {
+                dx -= sW;
+                dy += 1;
+            }
         }
     }
 }
