@@ -191,6 +191,28 @@ int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
                     const lrt_render_settings* settings, lrt_targets* targets,
                     lrt_frame_stats* stats, void* stream);
 
+/* The same frame, returning once it is enqueued on `stream`, so the host can
+ * prepare the next frame (or read back the last one) while the device
+ * renders. No reference counterpart: the reference's render always ends with
+ * a blocking submit. A frame is only enqueued when a frame of the same shape
+ * (splat count, width, height) has run with lrt_rast_render or this call's
+ * waiting path and the last pair count read leaves a quarter of the pair
+ * buffer free; otherwise this call waits like lrt_rast_render. time_stages
+ * also makes it wait. Enqueued frames are ordered after every earlier call on
+ * the handle, on any stream; targets belong to the caller until the frame is
+ * done (an event the caller records on `stream` after this call marks it).
+ * Counts and device status of enqueued frames are read by lrt_rast_settle. */
+int lrt_rast_render_async(lrt_rast* rast, const lrt_projection* projection,
+                          const lrt_splat_instance* instances, uint32_t instance_count,
+                          const lrt_render_settings* settings, lrt_targets* targets, void* stream);
+
+/* Waits for every enqueued frame. Returns LRT_OVERFLOW when any of them
+ * emitted more pairs than the buffer held (their images are incomplete; the
+ * buffers are grown, so drawing them again succeeds), LRT_TIMEOUT when a
+ * bounded device wait gave up, else LRT_OK. `stats` (may be NULL) receives
+ * the splats, visible splats and pairs of the last frame. */
+int lrt_rast_settle(lrt_rast* rast, lrt_frame_stats* stats);
+
 int lrt_rast_debug_view(lrt_rast* rast, lrt_debug_view* out);
 
 /* One view of a batch: its projection, size and caller-owned device images

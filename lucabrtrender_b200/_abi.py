@@ -38,7 +38,8 @@ EXPORTS = (
     "lrt_abi_version", "lrt_rast_create", "lrt_rast_destroy", "lrt_rast_last_error", "lrt_rast_render",
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
     "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
-    "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch",
+    "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
+    "lrt_rast_settle",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -173,6 +174,10 @@ def load() -> C.CDLL:
     lib.lrt_rast_render.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(SplatInstanceStruct), C.c_uint32,
                                     C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
                                     C.POINTER(FrameStatsStruct), C.c_void_p]
+    lib.lrt_rast_render_async.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(SplatInstanceStruct),
+                                          C.c_uint32, C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
+                                          C.c_void_p]
+    lib.lrt_rast_settle.argtypes = [C.c_void_p, C.POINTER(FrameStatsStruct)]
     lib.lrt_rast_debug_view.argtypes = [C.c_void_p, C.POINTER(DebugView)]
     lib.lrt_camera_looking_at.argtypes = [C.POINTER(C.c_double)] * 3 + [C.POINTER(CameraStruct)]
     lib.lrt_projection_for.argtypes = [C.POINTER(CameraStruct), C.c_uint32, C.c_uint32, C.POINTER(Projection)]

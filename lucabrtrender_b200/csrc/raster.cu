@@ -59,6 +59,19 @@ struct lrt_rast {
     const uint32_t* trainEmitSlot = nullptr;       // slot per emit index (low-field layout)
     uint32_t trainPairs = 0;
     double lastBackwardMs[2] = {0.0, 0.0};
+    // Plain frames enqueued by lrt_rast_render_async: their counts land in a
+    // ring of pinned slots, each with the event that marks its frame done.
+    static constexpr uint32_t kRing = 16;
+    uint32_t* ringHost = nullptr;               // pinned, 4 words per slot
+    cudaEvent_t ringEvent[kRing] = {};
+    uint32_t ringCap[kRing] = {};               // the pair capacity each frame ran with
+    uint64_t ringHead = 0, ringTail = 0;        // next slot to fill; oldest slot not read
+    bool plainSized = false;                    // a plain frame of this shape has run with a wait
+    uint32_t plainSlots = 0, plainWidth = 0, plainHeight = 0, plainSeenPairs = 0;
+    uint32_t asyncOverflows = 0, asyncTimeouts = 0;   // among the frames read since the last settle
+    uint32_t asyncVisible = 0, asyncPairs = 0, asyncSplats = 0;   // the last frame read
+    cudaEvent_t frameDone = nullptr;            // end of the last frame, on its stream
+    bool frameDoneSet = false;
     // Batches of views.
     struct Batch {
         cudaStream_t stream = nullptr;
@@ -204,8 +217,11 @@ int lrt_rast_create(lrt_rast** out, int device) {
     lrt_rast* r = new lrt_rast();
     r->device = device;
     bool ok = cudaMallocHost(reinterpret_cast<void**>(&r->hostCounters), 64) == cudaSuccess &&
+              cudaMallocHost(reinterpret_cast<void**>(&r->ringHost), lrt_rast::kRing * 16) == cudaSuccess &&
               ensure(r->counters, 64) == cudaSuccess;
     for (auto& e : r->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    for (auto& e : r->ringEvent) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&r->frameDone, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         lrt_rast_destroy(r);
         cudaGetLastError();
@@ -223,9 +239,14 @@ void lrt_rast_destroy(lrt_rast* r) {
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
                             &r->pixLast, &r->partials})
         release(*b);
+    if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
+    if (r->ringHost != nullptr) cudaFreeHost(r->ringHost);
     for (auto& e : r->ev)
         if (e != nullptr) cudaEventDestroy(e);
+    for (auto& e : r->ringEvent)
+        if (e != nullptr) cudaEventDestroy(e);
+    if (r->frameDone != nullptr) cudaEventDestroy(r->frameDone);
     auto& B = r->batch;
     for (DeviceBuffer* b : {&B.records, &B.ranges, &B.params, &B.counters, &B.queue}) release(*b);
     if (B.hostParams != nullptr) cudaFreeHost(B.hostParams);
@@ -330,6 +351,9 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one frame");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    // The handle's buffers serve one frame at a time: a frame on another
+    // stream than the last one waits for it.
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
     const uint32_t slots = static_cast<uint32_t>(total);
     const uint32_t tilesX = (s->width + lrt::kTile - 1) / lrt::kTile;
     const uint32_t tilesY = (s->height + lrt::kTile - 1) / lrt::kTile;
@@ -478,7 +502,19 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                      "blend");
         }
         LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
-        LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters, counters, 16, cudaMemcpyDeviceToHost, stream), "readback");
+        const bool ring = deferred && !train;
+        const uint32_t slot = static_cast<uint32_t>(r->ringHead % lrt_rast::kRing);
+        LRT_CUDA(r,
+                 cudaMemcpyAsync(ring ? r->ringHost + 4 * slot : r->hostCounters, counters, 16,
+                                 cudaMemcpyDeviceToHost, stream),
+                 "readback");
+        LRT_CUDA(r, cudaEventRecord(r->frameDone, stream), "event");
+        r->frameDoneSet = true;
+        if (ring) {
+            LRT_CUDA(r, cudaEventRecord(r->ringEvent[slot], stream), "event");
+            r->ringCap[slot] = r->pairCap;
+            r->ringHead += 1;
+        }
         if (deferred) {
             r->debug.proj = r->proj.ptr;
             r->debug.rects = r->rects.ptr;
@@ -567,14 +603,11 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
 
 extern "C" {
 
-int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
-                    const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr) {
-    const auto frameStart = std::chrono::steady_clock::now();
-    if (r == nullptr) return LRT_INVALID_ARGUMENT;
-    r->error.clear();
-    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
-        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
-    std::vector<CloudDesc> clouds;
+}  // extern "C"
+
+namespace {
+
+int collect_clouds(lrt_rast* r, const lrt_splat_instance* instances, uint32_t n, std::vector<CloudDesc>& clouds) {
     for (uint32_t k = 0; k < n; ++k) {
         const lrt_gpu_splats* c = instances[k].splats;
         if (c == nullptr || c->count == 0) continue;
@@ -590,7 +623,134 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         d.count = c->count;
         clouds.push_back(d);
     }
-    return render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart);
+    return LRT_OK;
+}
+
+uint32_t total_slots(const std::vector<CloudDesc>& clouds) {
+    uint64_t total = 0;
+    for (const CloudDesc& c : clouds) total += c.count;
+    return static_cast<uint32_t>(std::min<uint64_t>(total, 0xFFFFFFFFull));
+}
+
+// Reads the counts of the oldest enqueued plain frame (waiting for it when
+// `wait`); false when it has not finished and `wait` is not set.
+bool read_oldest(lrt_rast* r, bool wait) {
+    const uint32_t slot = static_cast<uint32_t>(r->ringTail % lrt_rast::kRing);
+    if (wait) {
+        if (cudaEventSynchronize(r->ringEvent[slot]) != cudaSuccess) return false;
+    } else if (cudaEventQuery(r->ringEvent[slot]) != cudaSuccess) {
+        cudaGetLastError();   // cudaErrorNotReady is not an error to keep
+        return false;
+    }
+    const uint32_t* c = r->ringHost + 4 * slot;
+    r->asyncVisible = c[0];
+    r->asyncPairs = c[1];
+    r->plainSeenPairs = c[1];
+    if (c[1] > r->ringCap[slot] || (c[2] & lrt::kErrTooManyPairs) != 0) {
+        r->asyncOverflows += 1;
+        r->pairCap = std::max(r->pairCap, grow(r->pairCap, c[1]));
+    }
+    if (c[2] & lrt::kErrTimeout) r->asyncTimeouts += 1;
+    r->debug.visible = c[0];
+    r->debug.pairs_count = std::min(c[1], r->ringCap[slot]);
+    r->ringTail += 1;
+    return true;
+}
+
+// Waits for every enqueued plain frame and reports what they met since the
+// last report: OVERFLOW (those frames' images are incomplete; the buffers are
+// grown) or TIMEOUT.
+int settle_async(lrt_rast* r) {
+    DeviceScope scope(r->device);
+    while (r->ringTail < r->ringHead) {
+        if (!read_oldest(r, true)) return fail(r, LRT_DEVICE_FAILURE, "waiting for an enqueued frame failed");
+    }
+    const uint32_t overflows = r->asyncOverflows, timeouts = r->asyncTimeouts;
+    r->asyncOverflows = 0;
+    r->asyncTimeouts = 0;
+    if (overflows != 0)
+        return fail(r, LRT_OVERFLOW,
+                    std::to_string(overflows) + " enqueued frame(s) emitted more pairs than their buffer held; "
+                    "the buffers are grown, draw them again");
+    if (timeouts != 0) return fail(r, LRT_TIMEOUT, "a bounded device wait gave up in an enqueued frame");
+    return LRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                    const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    std::vector<CloudDesc> clouds;
+    if (const int code = collect_clouds(r, instances, n, clouds); code != LRT_OK) return code;
+    const int code = render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart);
+    if (code == LRT_OK) {   // a frame that waited sizes the buffers for its shape
+        r->plainSized = true;
+        r->plainSlots = total_slots(clouds);
+        r->plainWidth = s->width;
+        r->plainHeight = s->height;
+        r->plainSeenPairs = r->debug.pairs_count;
+    }
+    return code;
+}
+
+int lrt_rast_render_async(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                          const lrt_render_settings* s, lrt_targets* targets, void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    std::vector<CloudDesc> clouds;
+    if (const int code = collect_clouds(r, instances, n, clouds); code != LRT_OK) return code;
+    DeviceScope scope(r->device);
+    while (r->ringTail < r->ringHead && read_oldest(r, false)) {
+    }
+    if (r->ringHead - r->ringTail == lrt_rast::kRing && !read_oldest(r, true))
+        return fail(r, LRT_DEVICE_FAILURE, "waiting for an enqueued frame failed");
+    // Enqueued only when a frame of this shape has run with a wait and the
+    // last counts read leave a quarter of the pair buffer free; otherwise the
+    // frame waits (and draws again with grown buffers if it has to).
+    const uint32_t slots = total_slots(clouds);
+    const uint64_t wanted = uint64_t{r->plainSeenPairs} + r->plainSeenPairs / 4;
+    const bool deferred = r->plainSized && r->plainSlots == slots && r->plainWidth == s->width &&
+                          r->plainHeight == s->height && !s->time_stages && wanted <= r->pairCap;
+    if (!deferred) {
+        lrt_frame_stats stats{};
+        const int code = render_frame(r, pr, clouds, s, targets, &stats, streamPtr, false, frameStart);
+        if (code == LRT_OK) {
+            r->plainSized = true;
+            r->plainSlots = slots;
+            r->plainWidth = s->width;
+            r->plainHeight = s->height;
+            r->plainSeenPairs = stats.pairs;
+            r->asyncSplats = stats.splats;
+            r->asyncVisible = stats.visible;
+            r->asyncPairs = stats.pairs;
+        }
+        return code;
+    }
+    r->asyncSplats = slots;
+    return render_frame(r, pr, clouds, s, targets, nullptr, streamPtr, false, frameStart, true);
+}
+
+int lrt_rast_settle(lrt_rast* r, lrt_frame_stats* stats) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    const int code = settle_async(r);
+    if (stats != nullptr) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->splats = r->asyncSplats;
+        stats->visible = r->asyncVisible;
+        stats->pairs = r->asyncPairs;
+    }
+    return code;
 }
 
 int lrt_rast_train_forward(lrt_rast* r, const lrt_projection* pr, const lrt_train_params* params,
@@ -719,6 +879,10 @@ int lrt_rast_backward_times(const lrt_rast* r, double* blendMs, double* projectM
 int lrt_rast_debug_view(lrt_rast* r, lrt_debug_view* out) {
     if (r == nullptr || out == nullptr) return LRT_INVALID_ARGUMENT;
     r->error.clear();
+    if (r->ringTail < r->ringHead) {   // enqueued plain frames: wait for them
+        const int code = settle_async(r);
+        if (code != LRT_OK) return code;
+    }
     if (r->trainPending) {   // an enqueued training frame: wait for its counts
         DeviceScope scope(r->device);
         LRT_CUDA(r, cudaStreamSynchronize(r->pendingStream), "frame");
@@ -736,6 +900,7 @@ int lrt_prefix_sum(lrt_rast* r, const void* in, void* out, void* total, uint32_t
         return fail(r, LRT_INVALID_ARGUMENT, "null argument");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
     uint32_t* err = static_cast<uint32_t*>(r->counters.ptr) + 3;
     LRT_CUDA(r, ensure(r->scanScratch, lrt::scan_scratch_bytes(count)), "scan scratch");
     LRT_CUDA(r, cudaMemsetAsync(err, 0, 4, stream), "status");
@@ -760,6 +925,7 @@ int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32
     if (count <= 1) return LRT_OK;
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
     uint32_t* counters = static_cast<uint32_t*>(r->counters.ptr);
     uint32_t* err = counters + 3;
     LRT_CUDA(r, ensure(r->algoKeysAlt, size_t{count} * keyBytes), "sort buffers");
@@ -1120,6 +1286,7 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
 
     LRT_CUDA(r, cudaEventRecord(B.in, caller), "event");
     LRT_CUDA(r, cudaStreamWaitEvent(B.stream, B.in, 0), "event");
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(B.stream, r->frameDone, 0), "frame order");
     bool replayed = false;
     float deviceMs = 0.0f;
     if (tuning) {
@@ -1202,6 +1369,8 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
     }
     LRT_CUDA(r, cudaEventRecord(B.out, B.stream), "event");
     LRT_CUDA(r, cudaStreamWaitEvent(caller, B.out, 0), "event");
+    LRT_CUDA(r, cudaEventRecord(r->frameDone, B.stream), "event");
+    r->frameDoneSet = true;
     if (stats != nullptr) {
         const uint32_t chunks = (nViews + perChunk - 1) / perChunk;
         uint64_t pairs = 0;

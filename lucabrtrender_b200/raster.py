@@ -220,6 +220,35 @@ class TileRasterizer:
         self._check(code)
         return FrameStats.from_struct(stats)
 
+    def render_async(self, view: Camera | Projection, instances: Sequence[SplatInstance], settings: RenderSettings,
+                     targets: RenderTargets, stream=None) -> None:
+        """The frame, returning once it is enqueued (lrt_rast_render_async);
+        its counts and status are read by settle()."""
+        lib = _abi.load()
+        projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
+        targets.reserve(settings.width, settings.height)
+        clouds = []
+        arr = (_abi.SplatInstanceStruct * max(1, len(instances)))()
+        for k, inst in enumerate(instances):
+            if inst.splats is not None and inst.splats.count > 0:
+                cs = inst.splats.struct()
+                clouds.append(cs)
+                arr[k].splats = C.pointer(cs)
+            arr[k].object_to_world[:] = [float(v) for v in np.asarray(inst.object_to_world, np.float64).reshape(16)]
+            inst.edit.fill(arr[k].edit)
+        pr = projection.struct()
+        st = settings.struct()
+        tg = targets.struct()
+        self._check(lib.lrt_rast_render_async(self._handle, C.byref(pr), arr, len(instances), C.byref(st), C.byref(tg),
+                                              _stream_ptr(stream)))
+
+    def settle(self) -> FrameStats:
+        """Waits for the enqueued frames (lrt_rast_settle); raises LrtError
+        with OVERFLOW when one of them ran out of pair buffer."""
+        stats = _abi.FrameStatsStruct()
+        self._check(_abi.load().lrt_rast_settle(self._handle, C.byref(stats)))
+        return FrameStats.from_struct(stats)
+
     def render_batch(self, views: Sequence[tuple], instances: Sequence[SplatInstance], settings: RenderSettings,
                      targets: Sequence[RenderTargets] | None = None, stream=None):
         """Many views in one call (lrt_rast_render_batch). `views` holds

@@ -1,0 +1,96 @@
+"""Frames returned as soon as they are enqueued (lrt_rast_render_async, read
+back by lrt_rast_settle): every image equals the waiting render of the same
+view bit for bit, frames on other streams are ordered after them, and an
+enqueued frame that runs out of pair buffer is reported by settle, after which
+the frame drawn again is exact."""
+from __future__ import annotations
+
+import math
+
+import pytest
+import torch
+
+import lucabrtrender_b200 as L
+from lucabrtrender_b200 import _abi
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def orbit(k: int, w: int, h: int, radius: float = 4.0):
+    th = 2.0 * math.pi * k / 12
+    return L.square_pixel_camera((radius * math.sin(th), 0.3, radius * math.cos(th)), (0.0, 0.0, 0.0), w, h)
+
+
+def test_enqueued_frames_equal_waiting_frames():
+    scene = H.synthetic_scene(60_000, 64, 64, seed=31)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings(width=320, height=240)
+    raster = L.TileRasterizer.create(0)
+    try:
+        want = []
+        for k in range(8):
+            t = L.RenderTargets()
+            raster.render(orbit(k, 320, 240), instances, settings, t)
+            want.append((t.colour.clone(), t.depth.clone()))
+        got = [L.RenderTargets(320, 240) for _ in range(8)]
+        for k in range(8):
+            raster.render_async(orbit(k, 320, 240), instances, settings, got[k])
+        stats = raster.settle()
+        assert stats.splats == 60_000 and stats.pairs > 0
+        for (colour, depth), t in zip(want, got):
+            assert torch.equal(t.colour, colour)
+            assert torch.equal(t.depth, depth)
+    finally:
+        raster.close()
+
+
+def test_a_frame_on_another_stream_waits_for_the_enqueued_ones():
+    scene = H.synthetic_scene(60_000, 64, 64, seed=32)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings(width=320, height=240)
+    raster = L.TileRasterizer.create(0)
+    try:
+        want = L.RenderTargets()
+        raster.render(orbit(5, 320, 240), instances, settings, want)
+        want = (want.colour.clone(), want.depth.clone())
+        first = L.RenderTargets(320, 240)
+        raster.render(orbit(0, 320, 240), instances, settings, first)   # sizes the shape
+        side = torch.cuda.Stream()
+        for k in range(4):
+            raster.render_async(orbit(k, 320, 240), instances, settings, first)
+        other = L.RenderTargets(320, 240)
+        raster.render(orbit(5, 320, 240), instances, settings, other, side)
+        torch.cuda.synchronize()
+        raster.settle()
+        assert torch.equal(other.colour, want[0]) and torch.equal(other.depth, want[1])
+    finally:
+        raster.close()
+
+
+def test_an_enqueued_frame_that_overflows_is_reported_and_redrawn_exactly():
+    # 20k splats: the first frame's pair buffer holds 80k pairs; the far view
+    # emits about 45k (so frames of this shape are enqueued), the near one 107k.
+    scene = H.synthetic_scene(20_000, 64, 64, seed=33, log_scale_mean=-3.0)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings(width=256, height=256)
+    far, near = orbit(0, 256, 256, radius=9.0), orbit(0, 256, 256, radius=1.6)
+    raster = L.TileRasterizer.create(0)
+    reference = L.TileRasterizer.create(0)
+    try:
+        t = L.RenderTargets(256, 256)
+        first = raster.render(far, instances, settings, t)   # sizes the pair buffer
+        raster.render_async(far, instances, settings, t)
+        assert raster.settle().pairs == first.pairs
+        raster.render_async(near, instances, settings, t)
+        with pytest.raises(L.LrtError) as info:
+            raster.settle()
+        assert info.value.code == _abi.OVERFLOW
+        raster.render(near, instances, settings, t)
+        want = L.RenderTargets(256, 256)
+        reference.render(near, instances, settings, want)
+        assert torch.equal(t.colour, want.colour) and torch.equal(t.depth, want.depth)
+    finally:
+        raster.close()
+        reference.close()
