@@ -18,15 +18,43 @@ constexpr uint32_t kBatch = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 // shaders/lrt/splat/splat_ranges.slang:11-25 (after a zeroing memset,
-// splat_tiles_clear.slang:8-17).
+// splat_tiles_clear.slang:8-17). Each thread takes kRangeRun consecutive
+// pairs (two 16-byte loads per pair pair) and the one before them.
+constexpr uint32_t kRangeRun = 8;
 __global__ void ranges_kernel(const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ dCount,
                               uint32_t cap, uint32_t tileShift, uint2* __restrict__ ranges) {
     const uint32_t n = min(*dCount, cap);
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t t = static_cast<uint32_t>(pairs[i] >> tileShift);
-    if (i == 0 || static_cast<uint32_t>(pairs[i - 1] >> tileShift) != t) ranges[t].x = i;
-    if (i + 1 == n || static_cast<uint32_t>(pairs[i + 1] >> tileShift) != t) ranges[t].y = i + 1;
+    const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) * kRangeRun;
+    if (first >= n) return;
+    uint32_t prev = first == 0 ? 0xFFFFFFFFu : static_cast<uint32_t>(__ldg(pairs + first - 1) >> tileShift);
+    unsigned long long w[kRangeRun];
+    if (first + kRangeRun <= n) {
+        const ulonglong2* v = reinterpret_cast<const ulonglong2*>(pairs + first);
+#pragma unroll
+        for (uint32_t k = 0; k < kRangeRun / 2; ++k) {
+            const ulonglong2 q = __ldg(v + k);
+            w[2 * k] = q.x;
+            w[2 * k + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (uint32_t k = 0; k < kRangeRun; ++k) w[k] = first + k < n ? __ldg(pairs + first + k) : 0ull;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kRangeRun; ++k) {
+        const uint32_t i = first + k;
+        if (i < n) {
+            const uint32_t t = static_cast<uint32_t>(w[k] >> tileShift);
+            if (t != prev) {
+                ranges[t].x = i;
+                if (i > 0) ranges[prev].y = i;
+            }
+            prev = t;
+        }
+    }
+    // The run's last pair closes its tile when the pair after it (or the end) differs.
+    const uint32_t last = min(first + kRangeRun, n) - 1;
+    if (last + 1 == n || static_cast<uint32_t>(__ldg(pairs + last + 1) >> tileShift) != prev) ranges[prev].y = last + 1;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -573,8 +601,9 @@ cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_
                           uint2* ranges, uint32_t tiles, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(ranges, 0, sizeof(uint2) * tiles, stream);
     if (e != cudaSuccess || cap == 0) return e;
-    ranges_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs), dCount,
-                                                          cap, tileShift, ranges);
+    const uint32_t threads = (cap + kRangeRun - 1) / kRangeRun;
+    ranges_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs),
+                                                             dCount, cap, tileShift, ranges);
     return cudaGetLastError();
 }
 
