@@ -125,6 +125,35 @@ typedef struct lrt_splat_instance {
     lrt_splat_edit edit;
 } lrt_splat_instance;
 
+/* scene::GpuPoints (GpuClouds.h:78-85): `count` points, positions float4
+ * (x, y, z, 1) and colours two uint32 words each of fp16 halves, r | g << 16
+ * and b | a << 16, linear. Device pointers. */
+typedef struct lrt_gpu_points {
+    uint32_t count;
+    uint32_t reserved;
+    const void* positions;
+    const void* colours;
+} lrt_gpu_points;
+
+/* PointStyle (Points.h), the fields the disc route reads: size_mode 0 world
+ * units, 1 pixels; size the diameter; constant_colour 1 draws every point
+ * in colour[] (linear). The raster route's eye-dome lighting and surface
+ * splatting need a rasterisation pipeline and are not part of this path. */
+typedef struct lrt_point_style {
+    uint32_t size_mode;
+    float size;
+    uint32_t constant_colour;
+    float colour[3];
+} lrt_point_style;
+
+/* PointInstance (Points.h): points drawn as opaque discs, sorted with the
+ * splats (shaders/lrt/splat/points_project.slang). */
+typedef struct lrt_point_instance {
+    const lrt_gpu_points* points;
+    double object_to_world[16];
+    lrt_point_style style;
+} lrt_point_instance;
+
 /* RenderSettings (TileRasterizer.h:105-118). */
 typedef struct lrt_render_settings {
     uint32_t width, height;
@@ -202,6 +231,21 @@ int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
  * the handle, on any stream; targets belong to the caller until the frame is
  * done (an event the caller records on `stream` after this call marks it).
  * Counts and device status of enqueued frames are read by lrt_rast_settle. */
+/* TileRasterizer::render with its `points` and `under` arguments
+ * (TileRasterizer.cpp:188-484): the point instances are projected as opaque
+ * discs into slots after the splats and sorted with them, and `under` (may be
+ * NULL; the frame's size, linear premultiplied colour and view depth, bottom
+ * row first) is a layer the splats composite over: a pixel stops at the
+ * first pair at or behind the layer's depth there, or at the first disc it
+ * touches, and what stopped it shows through the remaining transmittance
+ * (shaders/lrt/splat/splat_blend.slang:23-120, splatBlendComposite). With no
+ * points and no layer it is lrt_rast_render. */
+int lrt_rast_render_composite(lrt_rast* rast, const lrt_projection* projection,
+                              const lrt_splat_instance* instances, uint32_t instance_count,
+                              const lrt_point_instance* points, uint32_t point_count,
+                              const lrt_targets* under, const lrt_render_settings* settings,
+                              lrt_targets* targets, lrt_frame_stats* stats, void* stream);
+
 int lrt_rast_render_async(lrt_rast* rast, const lrt_projection* projection,
                           const lrt_splat_instance* instances, uint32_t instance_count,
                           const lrt_render_settings* settings, lrt_targets* targets, void* stream);
@@ -356,6 +400,15 @@ int lrt_prefix_sum_noalloc(const void* in, void* out, void* total, uint32_t coun
 int lrt_pack_splats(const float* raw, uint32_t count, uint32_t floats_per_record,
                     uint32_t file_per_colour, uint32_t keep_per_colour, float* positions,
                     uint32_t* shape, uint32_t* sh, uint32_t* kept);
+
+/* Raw point records (x y z r g b, 6 floats) to the GpuPoints layout above, on
+ * the host (the upload half of CloudLoader for points: points_validate.slang
+ * and points_decode.slang). colour_kind: 0 none (white), 1 sRGB bytes in
+ * 0..255, 2 linear floats. Points with a non-finite position are dropped,
+ * and with detail < 1 only those whose index hash falls below it are kept,
+ * order kept. Writes up to `count` points; the kept count in *kept. */
+int lrt_pack_points(const float* raw, uint32_t count, uint32_t colour_kind, float detail,
+                    float* positions, uint32_t* colours, uint32_t* kept);
 
 /* Diagnostic: the library's own exp (fn 0), log (1), sRGB-to-linear (2) and
  * cut-off power (3), evaluated on the device over n floats (device pointers),

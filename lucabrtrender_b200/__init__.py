@@ -6,13 +6,15 @@ Python host mirror of the reference's C++ interface over that ABI.
 """
 from ._abi import LrtError
 from .camera import Camera, Lens, Projection, projection_for, square_pixel_camera
-from .raster import (Depth, EditMode, EditShape, FrameStats, RenderSettings, RenderTargets, SplatEdit,
-                     SplatInstance, TileRasterizer, math_eval)
-from .scene import CloudLoader, GpuSplats, PackedSplats, pack_splats, synthetic_records, to_device
+from .raster import (Depth, EditMode, EditShape, FrameStats, PointInstance, PointStyle, RenderSettings, RenderTargets,
+                     SplatEdit, SplatInstance, TileRasterizer, math_eval)
+from .scene import (CloudLoader, GpuPoints, GpuSplats, PackedPoints, PackedSplats, pack_points, pack_splats,
+                    points_to_device, synthetic_records, to_device)
 from .train import rasterize
 
 __all__ = [
     "LrtError", "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
     "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
     "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
+    "PointInstance", "PointStyle", "GpuPoints", "PackedPoints", "pack_points", "points_to_device",
 ]

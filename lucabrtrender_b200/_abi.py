@@ -39,7 +39,7 @@ EXPORTS = (
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
     "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
     "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
-    "lrt_rast_settle",
+    "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -91,6 +91,23 @@ class SplatInstanceStruct(C.Structure):
         ("splats", C.POINTER(GpuSplatsStruct)),
         ("object_to_world", C.c_double * 16),
         ("edit", SplatEdit),
+    ]
+
+
+class GpuPointsStruct(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("reserved", C.c_uint32), ("positions", C.c_void_p), ("colours", C.c_void_p)]
+
+
+class PointStyleStruct(C.Structure):
+    _fields_ = [("size_mode", C.c_uint32), ("size", C.c_float), ("constant_colour", C.c_uint32),
+                ("colour", C.c_float * 3)]
+
+
+class PointInstanceStruct(C.Structure):
+    _fields_ = [
+        ("points", C.POINTER(GpuPointsStruct)),
+        ("object_to_world", C.c_double * 16),
+        ("style", PointStyleStruct),
     ]
 
 
@@ -178,6 +195,12 @@ def load() -> C.CDLL:
                                           C.c_uint32, C.POINTER(RenderSettingsStruct), C.POINTER(TargetsStruct),
                                           C.c_void_p]
     lib.lrt_rast_settle.argtypes = [C.c_void_p, C.POINTER(FrameStatsStruct)]
+    lib.lrt_rast_render_composite.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(SplatInstanceStruct),
+                                              C.c_uint32, C.POINTER(PointInstanceStruct), C.c_uint32,
+                                              C.POINTER(TargetsStruct), C.POINTER(RenderSettingsStruct),
+                                              C.POINTER(TargetsStruct), C.POINTER(FrameStatsStruct), C.c_void_p]
+    lib.lrt_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_uint32)]
     lib.lrt_rast_debug_view.argtypes = [C.c_void_p, C.POINTER(DebugView)]
     lib.lrt_camera_looking_at.argtypes = [C.POINTER(C.c_double)] * 3 + [C.POINTER(CameraStruct)]
     lib.lrt_projection_for.argtypes = [C.POINTER(CameraStruct), C.c_uint32, C.c_uint32, C.POINTER(Projection)]

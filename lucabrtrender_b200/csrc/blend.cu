@@ -142,7 +142,14 @@ __device__ __forceinline__ float4 cull_box(const ProjRecord& rec) {
 // kTrain: also keep, per pixel, the blended colour before linearising with
 // the final transmittance, and one past the last pair that contributed --
 // what the backward pass re-blends from.
-template <bool kTrain>
+// kComposite: splatBlendComposite (splat_blend.slang:116-120). A disc record
+// (colour.w > 0.5) that passes a pixel's cut ends its walk as an opaque hit,
+// and with an under layer a pixel stops at the first pair of the tile whose
+// depth is at or behind the layer's there -- whether or not that pair touches
+// the pixel. Pairs are in depth-key order, not exactly depth order, so that
+// first pair is found from a running maximum of the batch's depths (the first
+// index where it reaches the layer's depth), not from depth order.
+template <bool kTrain, bool kComposite = false>
 __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
                                            const uint2* __restrict__ ranges,
                                            const unsigned long long* __restrict__ pairs,
@@ -151,7 +158,10 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                                            float* __restrict__ depthOut, float4* __restrict__ pixState,
                                            uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
                                            ProjRecord (&sRec)[2][kBatch], float4 (&sBox)[kBatch],
-                                           uint64_t (&sBar)[2], uint32_t& phase0, uint32_t& phase1) {
+                                           uint64_t (&sBar)[2], uint32_t& phase0, uint32_t& phase1,
+                                           const float4* __restrict__ underColour = nullptr,
+                                           const float* __restrict__ underDepth = nullptr,
+                                           float* sZMax = nullptr, float* sWarpMax = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
     const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
@@ -160,6 +170,22 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
     const uint2 range = ranges[tile];
     const uint32_t start = range.x, end = range.y;
     const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
+    const size_t pix = static_cast<size_t>(py) * bp.width + px;
+    // Composite state: the under layer's depth here, where the layer stops
+    // this pixel's walk (a pair index), and what ended the walk opaquely.
+    bool underHit = false;
+    float underZ = 0.0f;
+    if constexpr (kComposite) {
+        if (underColour != nullptr && inside) {
+            underZ = underDepth[pix];
+            underHit = underZ > 0.0f;
+        }
+    }
+    uint32_t stopAt = 0xFFFFFFFFu;
+    bool opaqueHit = false;
+    float4 opaque = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float opaqueZ = 0.0f;
+    float zCarry = -3.4e38f;   // the largest depth of the tile's earlier batches
 
     auto issue = [&](uint32_t buf, uint32_t at) {
         const uint32_t cnt = min(kBatch, end - at);
@@ -197,11 +223,40 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         const uint32_t cnt = min(kBatch, end - at);
         const ProjRecord* batch = sRec[buf];
         if (tid < cnt) sBox[tid] = cull_box(batch[tid]);
+        if constexpr (kComposite) {
+            if (underColour != nullptr) {
+                // Running maximum of the depths, tile order, across batches.
+                float v = tid < cnt ? batch[tid].screen.z : -3.4e38f;
+#pragma unroll
+                for (uint32_t d = 1; d < 32; d <<= 1) {
+                    const float o = __shfl_up_sync(0xFFFFFFFFu, v, d);
+                    if (lane >= d) v = fmaxf(v, o);
+                }
+                if (lane == 31) sWarpMax[warp] = v;
+                __syncthreads();
+                float prior = zCarry;
+                for (uint32_t w = 0; w < warp; ++w) prior = fmaxf(prior, sWarpMax[w]);
+                sZMax[tid] = fmaxf(v, prior);
+                __syncthreads();
+                zCarry = sZMax[cnt - 1];
+                if (underHit && stopAt == 0xFFFFFFFFu && zCarry >= underZ) {
+                    uint32_t lo = 0, hi = cnt - 1;   // sZMax[hi] >= underZ
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (sZMax[mid] >= underZ) hi = mid; else lo = mid + 1;
+                    }
+                    stopAt = at + lo;
+                }
+            }
+        }
         __syncthreads();
         // Records in chunks of 32: each lane tests one record's box against the
         // bounding box of this warp's pixels still blending, and the warp then
         // walks the ballot's set bits in record order.
         for (uint32_t c = 0; c < cnt; c += 32) {
+            if constexpr (kComposite) {
+                if (at + c >= stopAt) done = true;
+            }
             const unsigned active = __ballot_sync(0xFFFFFFFFu, !done);
             if (active == 0) break;
             const uint32_t big = 0xFFFFFFFFu;
@@ -228,12 +283,25 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                 const float dx = pxf - screen.x;
                 const float dy = pyf - screen.y;
                 const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
-                const bool candidate = !done && !(power > screen.w);
+                const bool candidate = !done && !(power > screen.w) && (!kComposite || at + j < stopAt);
                 if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
+                bool blendIt = candidate;
+                if constexpr (kComposite) {
+                    if (candidate) {
+                        const float4 col = batch[j].colour;
+                        if (col.w > 0.5f) {   // a disc: opaque, the walk ends here
+                            opaqueHit = true;
+                            opaque = make_float4(col.x, col.y, col.z, 1.0f);
+                            opaqueZ = screen.z;
+                            done = true;
+                            blendIt = false;
+                        }
+                    }
+                }
                 // A candidate's power lies in [0, 9] (the cut is at most 9), so
                 // the exponent's argument is in range; others discard it.
                 const float alpha = fminf(0.99f, conic.w * lrt_exp_in_range(-0.5f * power));
-                if (candidate && !(alpha < 1.0f / 255.0f)) {
+                if (blendIt && !(alpha < 1.0f / 255.0f)) {
                     const float4 colour = batch[j].colour;
                     const float weight = T * alpha;
                     r = r + weight * colour.x;
@@ -259,6 +327,13 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         }
     }
     if (!inside) return;
+    if constexpr (kComposite) {
+        if (!opaqueHit && underHit) {
+            opaqueHit = true;
+            opaque = underColour[pix];
+            opaqueZ = underZ;
+        }
+    }
     const float coverage = 1.0f - T;
     float lr = r, lg = g, lb = b;
     if (bp.linearise != 0 && coverage > 1e-6f) {
@@ -266,9 +341,15 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         lg = srgb_to_linear(g / coverage) * coverage;
         lb = srgb_to_linear(b / coverage) * coverage;
     }
-    const size_t pix = static_cast<size_t>(py) * bp.width + px;
-    colourOut[pix] = make_float4(lr + T * bp.bg[0], lg + T * bp.bg[1], lb + T * bp.bg[2], coverage + T * bp.bg[3]);
-    depthOut[pix] = bp.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f) : fmaxf(depthAt, 0.0f);
+    float4 behind = make_float4(bp.bg[0], bp.bg[1], bp.bg[2], bp.bg[3]);
+    if (opaqueHit) {
+        behind = opaque;
+        depthSum = depthSum + T * opaqueZ;
+        if (depthAt < 0.0f) depthAt = opaqueZ;
+    }
+    const float total = opaqueHit ? 1.0f : coverage;
+    colourOut[pix] = make_float4(lr + T * behind.x, lg + T * behind.y, lb + T * behind.z, coverage + T * behind.w);
+    depthOut[pix] = bp.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f) : fmaxf(depthAt, 0.0f);
     if (kTrain) {
         pixState[pix] = make_float4(r, g, b, T);
         pixLast[pix] = last;
@@ -295,6 +376,31 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     const uint32_t tile = blockIdx.x;
     blend_tile<kTrain>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emitSlot, proj, colourOut, depthOut,
                        pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
+}
+
+// splatBlendComposite (splat_blend.slang:116-120): discs and an optional
+// under layer (colour may be null).
+__global__ void __launch_bounds__(kBlendThreads)
+blend_composite_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+                       const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut,
+                       float* __restrict__ depthOut, const float4* __restrict__ underColour,
+                       const float* __restrict__ underDepth, uint32_t* __restrict__ err) {
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
+    __shared__ __align__(16) float4 sBox[kBatch];
+    __shared__ __align__(8) uint64_t sBar[2];
+    __shared__ float sZMax[kBatch];
+    __shared__ float sWarpMax[kBlendThreads / 32];
+    if (threadIdx.x == 0) {
+        mbar_init(&sBar[0], 1);
+        mbar_init(&sBar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t phase0 = 0, phase1 = 0;
+    const uint32_t tile = blockIdx.x;
+    blend_tile<false, true>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, nullptr, proj, colourOut,
+                            depthOut, nullptr, nullptr, err, sRec, sBox, sBar, phase0, phase1, underColour,
+                            underDepth, sZMax, sWarpMax);
 }
 
 // Many views in one launch: a persistent grid whose blocks take (view, tile)
@@ -613,6 +719,17 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
     if (tiles == 0) return cudaSuccess;
     blend_kernel<false><<<tiles, kBlendThreads, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), nullptr, proj, colour, depth, nullptr, nullptr,
+        err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_composite(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                                  const ProjRecord* proj, float4* colour, float* depth, const float4* underColour,
+                                  const float* underDepth, uint32_t* err, cudaStream_t stream) {
+    const uint32_t tiles = bp.tilesX * bp.tilesY;
+    if (tiles == 0) return cudaSuccess;
+    blend_composite_kernel<<<tiles, kBlendThreads, 0, stream>>>(
+        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, colour, depth, underColour, underDepth,
         err);
     return cudaGetLastError();
 }

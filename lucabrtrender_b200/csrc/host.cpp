@@ -251,3 +251,52 @@ int lrt_pack_splats(const float* raw, uint32_t count, uint32_t fpr, uint32_t fil
 }
 
 }  // extern "C"
+
+namespace {
+
+// shaders/lrt/common/color.slang:7-10 and :30-34, on the host.
+float srgb_to_linear_host(float c) {
+    c = std::fmax(c, 0.0f);
+    return c <= 0.04045f ? c / 12.92f : lrt::lrt_pow((c + 0.055f) / 1.055f, 2.4f);
+}
+
+float index_hash01(uint32_t v) {
+    const uint32_t state = v * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return static_cast<float>((word >> 22u) ^ word) / 4294967295.0f;
+}
+
+}  // namespace
+
+extern "C" int lrt_pack_points(const float* raw, uint32_t count, uint32_t colourKind, float detail, float* positions,
+                               uint32_t* colours, uint32_t* kept) {
+    // The points half of CloudLoader::upload (GpuClouds.cpp:369-430): which
+    // points stay (points_validate.slang:19-28: finite, and thinned to
+    // `detail` by an index hash), compacted in order, then their layout
+    // (points_decode.slang:24-41).
+    if (kept == nullptr) return LRT_INVALID_ARGUMENT;
+    *kept = 0;
+    if (count > 0 && (raw == nullptr || positions == nullptr || colours == nullptr)) return LRT_INVALID_ARGUMENT;
+    if (colourKind > 2) return LRT_INVALID_ARGUMENT;
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* r = raw + static_cast<size_t>(i) * 6;
+        if (!(std::isfinite(r[0]) && std::isfinite(r[1]) && std::isfinite(r[2]))) continue;
+        if (!(detail >= 1.0f || index_hash01(i) < detail)) continue;
+        float* p = positions + static_cast<size_t>(j) * 4;
+        p[0] = r[0];
+        p[1] = r[1];
+        p[2] = r[2];
+        p[3] = 1.0f;
+        float rgb[3] = {1.0f, 1.0f, 1.0f};
+        for (int c = 0; c < 3; ++c) {
+            if (colourKind == 1) rgb[c] = srgb_to_linear_host(r[3 + c] / 255.0f);
+            if (colourKind == 2) rgb[c] = r[3 + c];
+        }
+        colours[static_cast<size_t>(j) * 2] = pack_halves(rgb[0], rgb[1]);
+        colours[static_cast<size_t>(j) * 2 + 1] = pack_halves(rgb[2], 1.0f);
+        ++j;
+    }
+    *kept = j;
+    return LRT_OK;
+}

@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/lrt_raster.h"
+
 namespace lrt {
 
 struct FrameParams;
@@ -29,6 +31,12 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
 // The same for the differentiable parameters (means float3, log-scales
 // float3, quaternions w x y z, opacity logits, SH fp16 [16][3]); also writes
 // each slot's first pair index and each pair's emit index into `values`.
+// Point instances as opaque discs, into the same records and pair stream.
+cudaError_t launch_project_points(const FrameParams& f, const float4* positions, const uint32_t* colours,
+                                  const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                  uint32_t* keys, uint32_t* counters, uint64_t* status, uint32_t* ticket,
+                                  uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs,
+                                  uint32_t capacity, cudaStream_t stream);
 cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, const float* logScales,
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
@@ -56,6 +64,11 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
 
 // The views' tiles in one persistent launch; `queue` is a zeroed counter and
 // `blocks` the grid size (a multiple of the SM count).
+// The composite blend: disc records end a pixel's walk, and so does an under
+// layer (underColour may be null: discs only).
+cudaError_t launch_blend_composite(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
+                                  const ProjRecord* proj, float4* colour, float* depth, const float4* underColour,
+                                  const float* underDepth, uint32_t* err, cudaStream_t stream);
 cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
                                const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
                                uint32_t* err, uint32_t blocks, cudaStream_t stream);

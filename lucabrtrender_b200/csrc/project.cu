@@ -163,6 +163,7 @@ struct PackedSource {
     const float4* positions;
     const uint4* shape;
     const uint32_t* sh;
+    static constexpr bool kDisc = false;
     static constexpr uint32_t kRestOffset = 0;
     struct Loaded {
         uint4 sw;
@@ -201,6 +202,7 @@ struct RawSource {
     const float* quats;
     const float* logits;
     const uint32_t* sh;
+    static constexpr bool kDisc = false;
     static constexpr uint32_t kRestOffset = 3;
     struct Loaded {
         float qw, qx, qy, qz;
@@ -233,6 +235,33 @@ struct RawSource {
     __device__ __forceinline__ float3 base(const Loaded&, const uint32_t* row) const {
         constexpr float kSH0 = 0.28209479177387814f;
         return make_float3(0.5f + kSH0 * half_at(row, 0), 0.5f + kSH0 * half_at(row, 1), 0.5f + kSH0 * half_at(row, 2));
+    }
+};
+
+// PointSource: a point cloud drawn as opaque discs in the same sort as the
+// splats (shaders/lrt/splat/points_project.slang:35-86): positions float4,
+// colours two words of fp16 halves per point, and the instance's style.
+struct PointSource {
+    const float4* positions;
+    const uint2* colours;
+    const uint32_t* sh;   // none: points carry no harmonics
+    uint32_t sizeMode;    // 0 world units, 1 pixels
+    float size;           // diameter
+    uint32_t constantColour;
+    float rgb[3];
+    static constexpr bool kDisc = true;
+    static constexpr uint32_t kRestOffset = 0;
+    struct Loaded {};
+    // pointRadius, shaders/lrt/points/point_frame.slang:38-44
+    __device__ __forceinline__ float radius(const FrameParams& f, float viewZ) const {
+        const float r = sizeMode == 1 ? size * 0.5f
+                                      : (f.ortho != 0 ? size * 0.5f * f.focalX : size * 0.5f * f.focalX / viewZ);
+        return fmaxf(r, 0.5f);
+    }
+    __device__ __forceinline__ float3 colour(uint32_t i) const {
+        if (constantColour != 0) return make_float3(rgb[0], rgb[1], rgb[2]);
+        const uint2 w = __ldg(colours + i);
+        return make_float3(low_half(w.x), high_half(w.x), low_half(w.y));
     }
 };
 
@@ -357,7 +386,39 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     uint4 rect = make_uint4(1, 1, 0, 0);
     Fate fate{true, false, 0.0f};
     typename Src::Loaded loaded{};
-    if (inRange) {
+    if constexpr (Src::kDisc) {
+        // points_project.slang:40-70: a disc of the point's radius, cut at
+        // one radius (conic 1/r^2 on the diagonal), alpha one.
+        if (inRange) {
+            const float4 po = __ldg(src.positions + i);
+            p = make_float3(po.x, po.y, po.z);
+            t = to_view(f, p);
+            alive = (t.z > f.nearZ) && !(t.z > f.farZ);
+            if (alive) {
+                const float radius = src.radius(f, t.z);
+                const float invZ = f.ortho != 0 ? 1.0f : 1.0f / t.z;
+                cx = f.focalX * t.x * invZ + f.centreX;
+                cy = f.focalY * t.y * invZ + f.centreY;
+                ca = 1.0f / (radius * radius);
+                cb = 0.0f;
+                cc = 1.0f / (radius * radius);
+                alpha = 1.0f;
+                cutoff = 1.0f;
+                // tileRect, frame.slang:149-161, with the radius as the extent
+                const float x1 = cx - radius, y1 = cy - radius, x2 = cx + radius, y2 = cy + radius;
+                if (x2 < 0.0f || y2 < 0.0f || x1 >= static_cast<float>(f.width) ||
+                    y1 >= static_cast<float>(f.height)) {
+                    alive = false;
+                } else {
+                    rect = make_uint4(static_cast<uint32_t>(fmaxf(x1, 0.0f)) / kTile,
+                                      static_cast<uint32_t>(fmaxf(y1, 0.0f)) / kTile,
+                                      static_cast<uint32_t>(fminf(x2, static_cast<float>(f.width) - 1.0f)) / kTile,
+                                      static_cast<uint32_t>(fminf(y2, static_cast<float>(f.height) - 1.0f)) / kTile);
+                    alive = !(rect.x > rect.z || rect.y > rect.w);
+                }
+            }
+        }
+    } else if (inRange) {
         float opacity;
         float3 scale;
         src.load(i, loaded, p, opacity, scale);
@@ -520,27 +581,38 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     uint32_t key = 0x00FFFFFFu;
     if (inRange) {
         if (alive) {
-            const float3 base = src.base(loaded, shStage + tid * f.shWords);
-            const uint32_t rpc = f.restPerColour;
-            const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
-            const uint32_t degree = min(stored, f.shLimit);
-            float3 restc = make_float3(0.0f, 0.0f, 0.0f);
-            if (degree > 0) {
-                const float dx = p.x - f.eye[0], dy = p.y - f.eye[1], dz = p.z - f.eye[2];
-                const float l = sqrtf(dx * dx + dy * dy + dz * dz);
-                const float3 dir = make_float3(dx / l, dy / l, dz / l);
-                restc = evaluate_rest<Src::kRestOffset>(shStage + tid * f.shWords, degree, dir);
+            if constexpr (Src::kDisc) {
+                ProjRecord rec;
+                rec.screen = make_float4(cx, cy, t.z, cutoff);
+                rec.conic = make_float4(ca, cb, cc, alpha);
+                const float3 rgb = src.colour(i);   // colour.w one: an opaque disc
+                rec.colour = make_float4(rgb.x, rgb.y, rgb.z, 1.0f);
+                proj[record] = rec;
+                if (f.writeDebug) rects[record] = rect;
+                key = float_bits(t.z) >> 7;
+            } else {
+                const float3 base = src.base(loaded, shStage + tid * f.shWords);
+                const uint32_t rpc = f.restPerColour;
+                const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
+                const uint32_t degree = min(stored, f.shLimit);
+                float3 restc = make_float3(0.0f, 0.0f, 0.0f);
+                if (degree > 0) {
+                    const float dx = p.x - f.eye[0], dy = p.y - f.eye[1], dz = p.z - f.eye[2];
+                    const float l = sqrtf(dx * dx + dy * dy + dz * dz);
+                    const float3 dir = make_float3(dx / l, dy / l, dz / l);
+                    restc = evaluate_rest<Src::kRestOffset>(shStage + tid * f.shWords, degree, dir);
+                }
+                float3 colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
+                                            fmaxf(base.z + restc.z, 0.0f));
+                if (fate.graded) colour = edit_grade(f.edit, colour);
+                ProjRecord rec;
+                rec.screen = make_float4(cx, cy, t.z, cutoff);
+                rec.conic = make_float4(ca, cb, cc, alpha);
+                rec.colour = make_float4(colour.x, colour.y, colour.z, 0.0f);
+                proj[record] = rec;
+                if (f.writeDebug) rects[record] = rect;
+                key = float_bits(t.z) >> 7;
             }
-            float3 colour = make_float3(fmaxf(base.x + restc.x, 0.0f), fmaxf(base.y + restc.y, 0.0f),
-                                        fmaxf(base.z + restc.z, 0.0f));
-            if (fate.graded) colour = edit_grade(f.edit, colour);
-            ProjRecord rec;
-            rec.screen = make_float4(cx, cy, t.z, cutoff);
-            rec.conic = make_float4(ca, cb, cc, alpha);
-            rec.colour = make_float4(colour.x, colour.y, colour.z, 0.0f);
-            proj[record] = rec;
-            if (f.writeDebug) rects[record] = rect;
-            key = float_bits(t.z) >> 7;
         } else {
             // splat_project.slang:39-49, plus a zeroed record
             ProjRecord rec;
@@ -724,6 +796,18 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
     return launch(f, fDev, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr, nullptr}, stage, proj, rects,
                   touched, keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity,
                   stream);
+}
+
+cudaError_t launch_project_points(const FrameParams& f, const float4* positions, const uint32_t* colours,
+                                  const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                  uint32_t* keys, uint32_t* counters, uint64_t* status, uint32_t* ticket,
+                                  uint32_t partitionBase, uint32_t lastPartition, uint32_t slotBits, uint64_t* pairs,
+                                  uint32_t capacity, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    PointSource src{positions, reinterpret_cast<const uint2*>(colours), nullptr, style.size_mode, style.size,
+                    style.constant_colour, {style.colour[0], style.colour[1], style.colour[2]}};
+    return launch(f, nullptr, src, TrainOutputs{nullptr, nullptr, nullptr}, false, proj, rects, touched, keys,
+                  counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity, stream);
 }
 
 cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, const float* logScales,

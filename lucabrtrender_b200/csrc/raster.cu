@@ -269,6 +269,7 @@ namespace {
 struct CloudDesc {
     const lrt_gpu_splats* packed = nullptr;
     const lrt_train_params* train = nullptr;
+    const lrt_point_instance* point = nullptr;   // points drawn as discs
     const double* objectToWorld = nullptr;
     const lrt_splat_edit* edit = nullptr;
     uint32_t count = 0;
@@ -302,7 +303,7 @@ FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s,
     if (c.train != nullptr) {
         f.restPerColour = 15;
         f.shWords = 24;
-    } else {
+    } else if (c.packed != nullptr) {
         f.restPerColour = c.packed->rest_per_colour;
         f.shWords = c.packed->sh_words;
     }
@@ -336,7 +337,8 @@ FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s,
 // backward pass checks them.
 int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudDesc>& clouds,
                  const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats, void* streamPtr,
-                 bool train, std::chrono::steady_clock::time_point frameStart, bool deferred = false) {
+                 bool train, std::chrono::steady_clock::time_point frameStart, bool deferred = false,
+                 const lrt_targets* under = nullptr, bool composite = false) {
     if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
     if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
         targets->depth == nullptr)
@@ -440,7 +442,17 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         for (const CloudDesc& c : clouds) {
             const FrameParams f = frame_params(pr, s, c, tilesX, tilesY, base);
             lastParams = f;
-            if (c.train != nullptr) {
+            if (c.point != nullptr) {
+                const lrt_gpu_points& g = *c.point->points;
+                LRT_CUDA(r,
+                         lrt::launch_project_points(
+                             f, static_cast<const float4*>(g.positions), static_cast<const uint32_t*>(g.colours),
+                             c.point->style, static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
+                             static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
+                             status, tickets + launch, partitionBase, lastPartition, lowBits, pairBuf, r->pairCap,
+                             stream),
+                         "points");
+            } else if (c.train != nullptr) {
                 const lrt_train_params& t = *c.train;
                 LRT_CUDA(r,
                          lrt::launch_project_emit_train(
@@ -493,6 +505,14 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                                              static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth),
                                              static_cast<float4*>(r->pixState.ptr),
                                              static_cast<uint32_t*>(r->pixLast.ptr), err, stream),
+                     "blend");
+        } else if (composite) {
+            LRT_CUDA(r,
+                     lrt::launch_blend_composite(
+                         bp, static_cast<uint2*>(r->ranges.ptr), sorted, static_cast<ProjRecord*>(r->proj.ptr),
+                         static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth),
+                         under != nullptr ? static_cast<const float4*>(under->colour) : nullptr,
+                         under != nullptr ? static_cast<const float*>(under->depth) : nullptr, err, stream),
                      "blend");
         } else {
             LRT_CUDA(r,
@@ -698,6 +718,39 @@ int lrt_rast_render(lrt_rast* r, const lrt_projection* pr, const lrt_splat_insta
         r->plainSeenPairs = r->debug.pairs_count;
     }
     return code;
+}
+
+int lrt_rast_render_composite(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                              const lrt_point_instance* points, uint32_t pointCount, const lrt_targets* under,
+                              const lrt_render_settings* s, lrt_targets* targets, lrt_frame_stats* stats,
+                              void* streamPtr) {
+    const auto frameStart = std::chrono::steady_clock::now();
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (pr == nullptr || s == nullptr || targets == nullptr || (n > 0 && instances == nullptr) ||
+        (pointCount > 0 && points == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    // TileRasterizer.cpp:211-213
+    if (under != nullptr && (under->width != s->width || under->height != s->height || under->colour == nullptr ||
+                             under->depth == nullptr))
+        return fail(r, LRT_INVALID_ARGUMENT, "the under-layer is not the frame's size");
+    std::vector<CloudDesc> clouds;
+    if (const int code = collect_clouds(r, instances, n, clouds); code != LRT_OK) return code;
+    for (uint32_t k = 0; k < pointCount; ++k) {
+        const lrt_gpu_points* g = points[k].points;
+        if (g == nullptr || g->count == 0) continue;
+        if (g->positions == nullptr || (reinterpret_cast<uintptr_t>(g->positions) & 15u) != 0 ||
+            (points[k].style.constant_colour == 0 &&
+             (g->colours == nullptr || (reinterpret_cast<uintptr_t>(g->colours) & 7u) != 0)))
+            return fail(r, LRT_INVALID_ARGUMENT, "points need 16-byte aligned positions and 8-byte aligned colours");
+        CloudDesc d;
+        d.point = &points[k];
+        d.objectToWorld = points[k].object_to_world;
+        d.count = g->count;
+        clouds.push_back(d);
+    }
+    const bool composite = under != nullptr || pointCount > 0;
+    return render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart, false, under, composite);
 }
 
 int lrt_rast_render_async(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,

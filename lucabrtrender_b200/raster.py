@@ -16,7 +16,7 @@ import torch
 
 from . import _abi
 from .camera import Camera, Projection, projection_for
-from .scene import GpuSplats
+from .scene import GpuPoints, GpuSplats
 
 
 class EditShape(enum.IntEnum):
@@ -67,6 +67,30 @@ class SplatInstance:
     splats: GpuSplats | None
     object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
     edit: SplatEdit = field(default_factory=SplatEdit)
+
+
+@dataclass
+class PointStyle:
+    """PointStyle (Points.h): what the disc route reads. size_mode 0 world
+    units, 1 pixels; size is the diameter."""
+    size_mode: int = 0
+    size: float = 0.01
+    constant_colour: bool = False
+    colour: tuple[float, float, float] = (1.0, 1.0, 1.0)
+
+    def fill(self, s: _abi.PointStyleStruct) -> None:
+        s.size_mode = int(self.size_mode)
+        s.size = float(self.size)
+        s.constant_colour = 1 if self.constant_colour else 0
+        s.colour[:] = list(map(float, self.colour))
+
+
+@dataclass
+class PointInstance:
+    """PointInstance (Points.h): a point cloud drawn as opaque discs."""
+    points: GpuPoints | None
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4))
+    style: PointStyle = field(default_factory=PointStyle)
 
 
 class Depth(enum.IntEnum):
@@ -198,7 +222,11 @@ class TileRasterizer:
             raise _abi.LrtError(code, self.last_error())
 
     def render(self, view: Camera | Projection, instances: Sequence[SplatInstance], settings: RenderSettings,
-               targets: RenderTargets, stream=None) -> FrameStats:
+               targets: RenderTargets, stream=None, points: Sequence[PointInstance] = (),
+               under: RenderTargets | None = None) -> FrameStats:
+        """TileRasterizer::render. `points` are drawn as opaque discs sorted
+        with the splats; `under` (the frame's size) is a layer the splats
+        composite over (lrt_rast_render_composite)."""
         lib = _abi.load()
         projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
         targets.reserve(settings.width, settings.height)
@@ -215,8 +243,23 @@ class TileRasterizer:
         st = settings.struct()
         tg = targets.struct()
         stats = _abi.FrameStatsStruct()
-        code = lib.lrt_rast_render(self._handle, C.byref(pr), arr, len(instances), C.byref(st), C.byref(tg),
-                                   C.byref(stats), _stream_ptr(stream))
+        if points or under is not None:
+            parr = (_abi.PointInstanceStruct * max(1, len(points)))()
+            for k, inst in enumerate(points):
+                if inst.points is not None and inst.points.count > 0:
+                    ps = inst.points.struct()
+                    clouds.append(ps)
+                    parr[k].points = C.pointer(ps)
+                parr[k].object_to_world[:] = [float(v) for v in
+                                              np.asarray(inst.object_to_world, np.float64).reshape(16)]
+                inst.style.fill(parr[k].style)
+            ut = under.struct() if under is not None else None
+            code = lib.lrt_rast_render_composite(self._handle, C.byref(pr), arr, len(instances), parr, len(points),
+                                                 C.byref(ut) if ut is not None else None, C.byref(st), C.byref(tg),
+                                                 C.byref(stats), _stream_ptr(stream))
+        else:
+            code = lib.lrt_rast_render(self._handle, C.byref(pr), arr, len(instances), C.byref(st), C.byref(tg),
+                                       C.byref(stats), _stream_ptr(stream))
         self._check(code)
         return FrameStats.from_struct(stats)
 

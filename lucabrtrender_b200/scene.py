@@ -109,14 +109,67 @@ def to_device(packed: PackedSplats, device="cuda") -> GpuSplats:
     return GpuSplats(pos, shape, sh, packed.rest_per_colour)
 
 
+@dataclass
+class PackedPoints:
+    """Host copy of a point cloud's layout: positions (x, y, z, 1) and two
+    words of fp16 halves per point (r | g, b | a), linear."""
+    positions: np.ndarray   # [N, 4] float32
+    colours: np.ndarray     # [N, 2] uint32
+
+    @property
+    def count(self) -> int:
+        return int(self.positions.shape[0])
+
+
+@dataclass
+class GpuPoints:
+    """scene::GpuPoints (GpuClouds.h:78-85) on the device."""
+    positions: torch.Tensor   # [N, 4] float32
+    colours: torch.Tensor     # [N, 2] int32 (bit patterns)
+
+    @property
+    def count(self) -> int:
+        return int(self.positions.shape[0])
+
+    def struct(self) -> _abi.GpuPointsStruct:
+        s = _abi.GpuPointsStruct()
+        s.count = self.count
+        s.positions = self.positions.data_ptr() if self.count else None
+        s.colours = self.colours.data_ptr() if self.count else None
+        return s
+
+
+def pack_points(raw: np.ndarray, colour_kind: int = 2, detail: float = 1.0) -> PackedPoints:
+    """Raw (x y z r g b) records to the point layout on the host
+    (lrt_pack_points). colour_kind: 0 none, 1 sRGB bytes, 2 linear floats."""
+    raw = np.ascontiguousarray(raw, dtype=np.float32).reshape(-1, 6)
+    n = raw.shape[0]
+    positions = np.empty((n, 4), np.float32)
+    colours = np.empty((n, 2), np.uint32)
+    kept = C.c_uint32(0)
+    _abi.check(_abi.load().lrt_pack_points(raw.ctypes.data, n, colour_kind, float(detail), positions.ctypes.data,
+                                           colours.ctypes.data, C.byref(kept)), "pack_points")
+    k = kept.value
+    return PackedPoints(positions[:k].copy(), colours[:k].copy())
+
+
+def points_to_device(packed: PackedPoints, device="cuda") -> GpuPoints:
+    return GpuPoints(torch.from_numpy(packed.positions).to(device),
+                     torch.from_numpy(packed.colours.view(np.int32)).to(device))
+
+
 class CloudLoader:
-    """CloudLoader (GpuClouds.h:126-175): raw records in, a GpuSplats out."""
+    """CloudLoader (GpuClouds.h:126-175): raw records in, a GpuSplats (or,
+    for points, a GpuPoints) out."""
 
     def __init__(self, device="cuda"):
         self.device = device
 
     def upload(self, raw: np.ndarray, file_per_colour: int, max_degree: int = 3) -> GpuSplats:
         return to_device(pack_splats(raw, file_per_colour, max_degree), self.device)
+
+    def upload_points(self, raw: np.ndarray, colour_kind: int = 2, detail: float = 1.0) -> GpuPoints:
+        return points_to_device(pack_points(raw, colour_kind, detail), self.device)
 
 
 def synthetic_records(count: int, seed: int, *, mean_sigma: float = 1.0, log_scale_mean: float = -4.5,

@@ -709,25 +709,111 @@ void projectOne(const Frame& f, const Src& src, uint32_t i, Projected& out) {
     out.keys[slot] = fbits(t.z) >> 7;
 }
 
-// shaders/lrt/splat/splat_blend.slang:23-108, splat-only (no composite).
+// A point instance's object-to-view rows (TileRasterizer.cpp:357-358); points
+// take no edit and need no eye.
+void setPointObject(Frame& f, const lrt_projection& pr, const lrt_point_instance& inst) {
+    const M4 objectToView = mul4(toM4(pr.world_to_view), toM4(inst.object_to_world));
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) f.m[r * 4 + c] = static_cast<float>(objectToView.at(r, c));
+    f.edit = lrt_splat_edit{};
+}
+
+// shaders/lrt/splat/points_project.slang:35-86, with pointRadius from
+// shaders/lrt/points/point_frame.slang:38-44: an opaque disc of the point's
+// radius in pixels (never below half a pixel), cut at one radius, alpha one,
+// colour.w one. A culled point's record is zeros (the reference leaves it
+// unwritten; nothing reads it).
+void projectPoint(const Frame& f, const lrt_gpu_points& c, const lrt_point_style& st, uint32_t i, Projected& out) {
+    const uint32_t slot = f.base + i;
+    auto cull = [&] {
+        out.touched[slot] = 0;
+        out.visible[slot] = 0;
+        out.keys[slot] = 0x00FFFFFFu;
+        out.rects[slot] = {1, 1, 0, 0};
+        out.proj[slot] = Record{};
+    };
+    const float* pos = static_cast<const float*>(c.positions) + size_t{i} * 4;
+    const F3 t = toView(f, F3{pos[0], pos[1], pos[2]});
+    if (!(t.z > f.nearZ) || t.z > f.farZ) return cull();
+    float radius = st.size_mode == 1 ? st.size * 0.5f
+                                     : (f.ortho != 0 ? st.size * 0.5f * f.focalX : st.size * 0.5f * f.focalX / t.z);
+    radius = std::fmax(radius, 0.5f);
+    const float invZ = f.ortho != 0 ? 1.0f : 1.0f / t.z;
+    const float cx = f.focalX * t.x * invZ + f.centreX;
+    const float cy = f.focalY * t.y * invZ + f.centreY;
+    const F3 conic{1.0f / (radius * radius), 0.0f, 1.0f / (radius * radius)};
+    const float cutoff = 1.0f;
+    const Rect rect = tileRect(f, cx, cy, radius, radius);
+    if (rect.x0 > rect.x1 || rect.y0 > rect.y1) return cull();
+    uint32_t touched = 0;
+    for (uint32_t ty = rect.y0; ty <= rect.y1; ++ty)
+        for (uint32_t tx = rect.x0; tx <= rect.x1; ++tx)
+            if (tileTouched(f, cx, cy, conic, cutoff, tx, ty)) touched += 1;
+    if (touched == 0) return cull();
+    float rgb[3] = {st.colour[0], st.colour[1], st.colour[2]};
+    if (st.constant_colour == 0) {
+        const uint32_t* col = static_cast<const uint32_t*>(c.colours) + size_t{i} * 2;
+        rgb[0] = lowHalf(col[0]);
+        rgb[1] = highHalf(col[0]);
+        rgb[2] = lowHalf(col[1]);
+    }
+    Record rec;
+    rec.screen[0] = cx; rec.screen[1] = cy; rec.screen[2] = t.z; rec.screen[3] = cutoff;
+    rec.conic[0] = conic.x; rec.conic[1] = conic.y; rec.conic[2] = conic.z; rec.conic[3] = 1.0f;
+    rec.colour[0] = rgb[0]; rec.colour[1] = rgb[1]; rec.colour[2] = rgb[2]; rec.colour[3] = 1.0f;
+    out.proj[slot] = rec;
+    out.rects[slot] = rect;
+    out.touched[slot] = touched;
+    out.visible[slot] = 1;
+    out.keys[slot] = fbits(t.z) >> 7;
+}
+
+// What a composite frame has under its splats (splat_blend.slang:11-16):
+// the layer's linear premultiplied colour and view depth, or nothing.
+struct Under {
+    const float* colour = nullptr;   // width*height float4
+    const float* depth = nullptr;    // width*height
+};
+
+// shaders/lrt/splat/splat_blend.slang:23-108. `composite` is the
+// splatBlendComposite entry (:116-120): discs (colour.w > 0.5) end the walk as
+// an opaque hit, and so does the under layer (a pair at or behind its depth).
 void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t* pairSlots,
                 const uint32_t* ranges, uint32_t px, uint32_t py, float* colour, float* depth,
-                std::vector<uint32_t>* contributors = nullptr) {
+                std::vector<uint32_t>* contributors = nullptr, bool composite = false,
+                const Under* under = nullptr) {
     const uint32_t tile = (py / kTile) * f.tilesX + px / kTile;
     const uint32_t start = ranges[tile * 2];
     const uint32_t end = ranges[tile * 2 + 1];
     const float pxf = static_cast<float>(px) + 0.5f;
     const float pyf = static_cast<float>(py) + 0.5f;
+    const uint64_t at = uint64_t{py} * f.width + px;
+    const bool hasUnder = composite && under != nullptr && under->colour != nullptr;
+    const float underZ = hasUnder ? under->depth[at] : 0.0f;
+    const bool underHit = hasUnder && underZ > 0.0f;
     float rgb[3] = {0.0f, 0.0f, 0.0f};
     float T = 1.0f;
     float depthSum = 0.0f;
     float depthAt = -1.0f;
+    bool opaqueHit = false;
+    float opaque[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float opaqueZ = 0.0f;
     for (uint32_t k = start; k < end; ++k) {
         const Record& rec = proj[pairSlots[k]];
+        if (underHit && rec.screen[2] >= underZ) break;
         const float dx = pxf - rec.screen[0];
         const float dy = pyf - rec.screen[1];
         const float power = rec.conic[0] * dx * dx + 2.0f * rec.conic[1] * dx * dy + rec.conic[2] * dy * dy;
         if (power > rec.screen[3]) continue;
+        if (composite && rec.colour[3] > 0.5f) {
+            opaqueHit = true;
+            opaque[0] = rec.colour[0];
+            opaque[1] = rec.colour[1];
+            opaque[2] = rec.colour[2];
+            opaque[3] = 1.0f;
+            opaqueZ = rec.screen[2];
+            break;
+        }
         const float alpha = std::fmin(0.99f, rec.conic[3] * expImpl(-0.5f * power));
         if (alpha < 1.0f / 255.0f) continue;
         const float weight = T * alpha;
@@ -740,17 +826,27 @@ void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t*
         if (contributors != nullptr) contributors->push_back(pairSlots[k]);
         if (T < 1e-4f) break;
     }
+    if (!opaqueHit && underHit) {
+        opaqueHit = true;
+        for (int c = 0; c < 4; ++c) opaque[c] = under->colour[at * 4 + c];
+        opaqueZ = underZ;
+    }
     const float coverage = 1.0f - T;
     float lin[3] = {rgb[0], rgb[1], rgb[2]};
     if (f.linearise != 0 && coverage > 1e-6f) {
         for (int k = 0; k < 3; ++k) lin[k] = srgbToLinear(rgb[k] / coverage) * coverage;
     }
-    const uint64_t at = uint64_t{py} * f.width + px;
-    colour[at * 4 + 0] = lin[0] + T * f.bg[0];
-    colour[at * 4 + 1] = lin[1] + T * f.bg[1];
-    colour[at * 4 + 2] = lin[2] + T * f.bg[2];
-    colour[at * 4 + 3] = coverage + T * f.bg[3];
-    const float total = coverage;
+    float behind[4] = {f.bg[0], f.bg[1], f.bg[2], f.bg[3]};
+    if (opaqueHit) {
+        for (int c = 0; c < 4; ++c) behind[c] = opaque[c];
+        depthSum = depthSum + T * opaqueZ;
+        if (depthAt < 0.0f) depthAt = opaqueZ;
+    }
+    colour[at * 4 + 0] = lin[0] + T * behind[0];
+    colour[at * 4 + 1] = lin[1] + T * behind[1];
+    colour[at * 4 + 2] = lin[2] + T * behind[2];
+    colour[at * 4 + 3] = coverage + T * behind[3];
+    const float total = opaqueHit ? 1.0f : coverage;
     depth[at] = f.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f) : std::fmax(depthAt, 0.0f);
 }
 
@@ -911,7 +1007,8 @@ struct Crop {
 
 template <class ProjectFn>
 int renderImpl(const lrt_projection* pr, uint64_t total, const lrt_render_settings* s, ora_frame_out* out,
-               uint32_t threads, ProjectFn&& project, Crop* crop) {
+               uint32_t threads, ProjectFn&& project, Crop* crop, bool composite = false,
+               const Under* under = nullptr) {
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     if (s->width == 0 || s->height == 0) return LRT_INVALID_ARGUMENT;
     if (total > 0xFFFFFFFFull) return LRT_UNSUPPORTED;
@@ -1012,7 +1109,7 @@ int renderImpl(const lrt_projection* pr, uint64_t total, const lrt_render_settin
                     py < crop->y0 + crop->h)
                     list = &crop->lists[(py - crop->y0) * crop->w + (px - crop->x0)];
                 blendPixel(f, P.proj, sortedSlots.data(), ranges.data(), px, static_cast<uint32_t>(py), colour,
-                           depth, list);
+                           depth, list, composite, under);
             }
     });
     out->stage_ms[5] = msSince(t);
@@ -1059,6 +1156,49 @@ int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, ui
     return renderImpl(pr, totalSplats(instances, n), s, out, threads, project, nullptr);
 }
 
+int ora_render_composite(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                         const lrt_point_instance* points, uint32_t pointCount, const float* underColour,
+                         const float* underDepth, const lrt_render_settings* s, ora_frame_out* out,
+                         uint32_t threads) {
+    // TileRasterizer.cpp:188-484 with its `points` and `under` arguments:
+    // splats first, then the point instances in slots after them (:355-377),
+    // and the composite blend when either is given (:464-475).
+    uint64_t total = totalSplats(instances, n);
+    for (uint32_t k = 0; k < pointCount; ++k)
+        if (points[k].points != nullptr) total += points[k].points->count;
+    auto project = [&](const Frame& f, Projected& P, uint32_t th) {
+        uint32_t base = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const lrt_gpu_splats* c = instances[k].splats;
+            if (c == nullptr || c->count == 0) continue;
+            Frame fi = f;
+            setObject(fi, *pr, instances[k]);
+            fi.base = base;
+            fi.restPerColour = c->rest_per_colour;
+            fi.shWords = c->sh_words;
+            parallelFor(c->count, th, [&](uint64_t b, uint64_t e) {
+                const PackedSrc src{*c};
+                for (uint64_t i = b; i < e; ++i) projectOne(fi, src, static_cast<uint32_t>(i), P);
+            });
+            base += c->count;
+        }
+        for (uint32_t k = 0; k < pointCount; ++k) {
+            const lrt_gpu_points* c = points[k].points;
+            if (c == nullptr || c->count == 0) continue;
+            Frame fi = f;
+            setPointObject(fi, *pr, points[k]);
+            fi.base = base;
+            parallelFor(c->count, th, [&](uint64_t b, uint64_t e) {
+                for (uint64_t i = b; i < e; ++i) projectPoint(fi, *c, points[k].style, static_cast<uint32_t>(i), P);
+            });
+            base += c->count;
+        }
+    };
+    const Under under{underColour, underDepth};
+    const bool composite = underColour != nullptr || pointCount > 0;
+    return renderImpl(pr, total, s, out, threads, project, nullptr, composite, &under);
+}
+
 int ora_train_render(const lrt_projection* pr, const lrt_train_params* params, const lrt_render_settings* s,
                      ora_frame_out* out, uint32_t threads, uint32_t crop_x0, uint32_t crop_y0, uint32_t crop_w,
                      uint32_t crop_h, uint32_t* list_offsets, uint32_t* list_slots, uint64_t list_capacity,
@@ -1095,11 +1235,21 @@ int ora_train_render(const lrt_projection* pr, const lrt_train_params* params, c
 int ora_reference_render(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
                          const lrt_render_settings* s, float* colour, float* depth,
                          uint32_t* overflow, uint32_t threads) {
+    return ora_reference_render_composite(pr, instances, n, nullptr, 0, s, colour, depth, overflow, threads);
+}
+
+int ora_reference_render_composite(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
+                                   const lrt_point_instance* points, uint32_t pointCount,
+                                   const lrt_render_settings* s, float* colour, float* depth, uint32_t* overflow,
+                                   uint32_t threads) {
     // modules/render/src/ReferenceRenderer.cpp:54-160 with
-    // shaders/lrt/reference/reference_project.slang:31-105 and reference_blend.slang:24-119.
+    // shaders/lrt/reference/reference_project.slang:31-105,
+    // reference_points_project.slang:19-41 and reference_blend.slang:24-119.
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     if (s->width == 0 || s->height == 0) return LRT_INVALID_ARGUMENT;
-    const uint64_t total = totalSplats(instances, n);
+    uint64_t total = totalSplats(instances, n);
+    for (uint32_t k = 0; k < pointCount; ++k)
+        if (points[k].points != nullptr) total += points[k].points->count;
     Frame f = frameFor(*pr, *s);
     std::vector<std::array<float, 4>> refScreen(total, {0.0f, 0.0f, -1.0f, 0.0f});
     std::vector<std::array<float, 4>> refConic(total), refColour(total);
@@ -1200,12 +1350,46 @@ int ora_reference_render(const lrt_projection* pr, const lrt_splat_instance* ins
         });
         base += c->count;
     }
+    for (uint32_t k = 0; k < pointCount; ++k) {
+        const lrt_gpu_points* c = points[k].points;
+        if (c == nullptr || c->count == 0) continue;
+        Frame fi = f;
+        setPointObject(fi, *pr, points[k]);
+        const lrt_point_style& st = points[k].style;
+        parallelFor(c->count, threads, [&](uint64_t b, uint64_t e) {
+            for (uint64_t ii = b; ii < e; ++ii) {
+                const uint32_t i = static_cast<uint32_t>(ii);
+                const uint32_t slot = base + i;
+                const float* pos = static_cast<const float*>(c->positions) + size_t{i} * 4;
+                const F3 v = toView(fi, F3{pos[0], pos[1], pos[2]});
+                if (!(v.z > fi.nearZ) || v.z > fi.farZ) continue;
+                const float r = st.size_mode == 1
+                                    ? std::fmax(st.size * 0.5f, 0.5f)
+                                    : std::fmax(fi.ortho != 0 ? st.size * 0.5f * fi.focalX
+                                                              : st.size * 0.5f * fi.focalX / v.z,
+                                                0.5f);
+                const float cx = fi.ortho != 0 ? fi.focalX * v.x + fi.centreX : fi.focalX * v.x / v.z + fi.centreX;
+                const float cy = fi.ortho != 0 ? fi.focalY * v.y + fi.centreY : fi.focalY * v.y / v.z + fi.centreY;
+                float rgb[3] = {st.colour[0], st.colour[1], st.colour[2]};
+                if (st.constant_colour == 0) {
+                    const uint32_t* col = static_cast<const uint32_t*>(c->colours) + size_t{i} * 2;
+                    rgb[0] = lowHalf(col[0]);
+                    rgb[1] = highHalf(col[0]);
+                    rgb[2] = lowHalf(col[1]);
+                }
+                refScreen[slot] = {cx, cy, v.z, 1.0f};
+                refConic[slot] = {1.0f / (r * r), 0.0f, 1.0f / (r * r), 1.0f};
+                refColour[slot] = {rgb[0], rgb[1], rgb[2], 1.0f};
+            }
+        });
+        base += c->count;
+    }
 
     constexpr uint32_t kMaxHits = 1024;
     std::atomic<uint32_t> over{0};
     parallelFor(f.height, threads, [&](uint64_t b, uint64_t e) {
         std::vector<float> hitDepth(kMaxHits), hitAlpha(kMaxHits);
-        std::vector<uint32_t> hitIndex(kMaxHits);
+        std::vector<uint32_t> hitIndex(kMaxHits), hitDisc(kMaxHits);
         for (uint64_t py = b; py < e; ++py) {
             for (uint32_t px = 0; px < f.width; ++px) {
                 const float pxf = static_cast<float>(px) + 0.5f;
@@ -1220,7 +1404,8 @@ int ora_reference_render(const lrt_projection* pr, const lrt_splat_instance* ins
                     const float dy = pyf - sc[1];
                     const float power = cn[0] * dx * dx + 2.0f * cn[1] * dx * dy + cn[2] * dy * dy;
                     if (power > sc[3]) continue;
-                    const float alpha = std::fmin(0.99f, cn[3] * expImpl(-0.5f * power));
+                    const bool disc = refColour[sI][3] > 0.5f;
+                    const float alpha = disc ? 1.0f : std::fmin(0.99f, cn[3] * expImpl(-0.5f * power));
                     if (alpha < 1.0f / 255.0f) continue;
                     if (hits == kMaxHits) {
                         overflowed = true;
@@ -1231,16 +1416,27 @@ int ora_reference_render(const lrt_projection* pr, const lrt_splat_instance* ins
                         hitDepth[at] = hitDepth[at - 1];
                         hitIndex[at] = hitIndex[at - 1];
                         hitAlpha[at] = hitAlpha[at - 1];
+                        hitDisc[at] = hitDisc[at - 1];
                         --at;
                     }
                     hitDepth[at] = sc[2];
                     hitIndex[at] = static_cast<uint32_t>(sI);
                     hitAlpha[at] = alpha;
+                    hitDisc[at] = disc ? 1u : 0u;
                     ++hits;
                 }
                 float rgb[3] = {0, 0, 0};
                 float T = 1.0f, depthSum = 0.0f, depthAt = -1.0f;
+                bool discHit = false;
+                float discColour[3] = {0, 0, 0};
+                float discZ = 0.0f;
                 for (uint32_t k = 0; k < hits; ++k) {
+                    if (hitDisc[k] != 0) {
+                        discHit = true;
+                        for (int c = 0; c < 3; ++c) discColour[c] = refColour[hitIndex[k]][c];
+                        discZ = hitDepth[k];
+                        break;
+                    }
                     const float weight = T * hitAlpha[k];
                     const auto& col = refColour[hitIndex[k]];
                     rgb[0] = rgb[0] + weight * col[0];
@@ -1256,11 +1452,21 @@ int ora_reference_render(const lrt_projection* pr, const lrt_splat_instance* ins
                 if (f.linearise != 0 && coverage > 1e-6f)
                     for (int k = 0; k < 3; ++k) lin[k] = srgbToLinear(rgb[k] / coverage) * coverage;
                 const uint64_t at = py * f.width + px;
-                colour[at * 4 + 0] = lin[0] + T * f.bg[0];
-                colour[at * 4 + 1] = lin[1] + T * f.bg[1];
-                colour[at * 4 + 2] = lin[2] + T * f.bg[2];
-                colour[at * 4 + 3] = coverage + T * f.bg[3];
-                depth[at] = f.depthMode == 0 ? (coverage > 1e-6f ? depthSum / coverage : 0.0f)
+                float behind[4] = {f.bg[0], f.bg[1], f.bg[2], f.bg[3]};
+                if (discHit) {
+                    behind[0] = discColour[0];
+                    behind[1] = discColour[1];
+                    behind[2] = discColour[2];
+                    behind[3] = 1.0f;
+                    depthSum = depthSum + T * discZ;
+                    if (depthAt < 0.0f) depthAt = discZ;
+                }
+                const float total = discHit ? 1.0f : coverage;
+                colour[at * 4 + 0] = lin[0] + T * behind[0];
+                colour[at * 4 + 1] = lin[1] + T * behind[1];
+                colour[at * 4 + 2] = lin[2] + T * behind[2];
+                colour[at * 4 + 3] = coverage + T * behind[3];
+                depth[at] = f.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f)
                                              : std::fmax(depthAt, 0.0f);
                 if (overflowed) over.fetch_add(1);
             }
@@ -1345,6 +1551,64 @@ int ora_random_cloud(uint32_t count, uint64_t seed, float minSize, float maxSize
                                 (dc[0] - 0.5F) / sh0, (dc[1] - 0.5F) / sh0, (dc[2] - 0.5F) / sh0};
         for (int k = 0; k < 14; ++k) r[k] = vals[k];
         for (int k = 0; k < 9; ++k) r[14 + k] = rest[k];
+    }
+    return LRT_OK;
+}
+
+int ora_pack_points(const float* raw, uint32_t count, uint32_t colourKind, float detail, float* positions,
+                    uint32_t* colours, uint32_t* kept) {
+    // shaders/lrt/scene/points_validate.slang:19-28 (which points stay),
+    // points_decode.slang:24-41 (their layout) and the in-order compaction
+    // between them (GpuClouds.cpp:369-430); hash01 from
+    // shaders/lrt/common/color.slang:30-34.
+    auto hash01 = [](uint32_t v) {
+        const uint32_t state = v * 747796405u + 2891336453u;
+        const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+        return static_cast<float>((word >> 22u) ^ word) / 4294967295.0f;
+    };
+    if (kept == nullptr || (count > 0 && (raw == nullptr || positions == nullptr || colours == nullptr)))
+        return LRT_INVALID_ARGUMENT;
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* r = raw + size_t{i} * 6;
+        const bool finite = std::isfinite(r[0]) && std::isfinite(r[1]) && std::isfinite(r[2]);
+        const bool keep = detail >= 1.0f || hash01(i) < detail;
+        if (!(finite && keep)) continue;
+        positions[size_t{j} * 4 + 0] = r[0];
+        positions[size_t{j} * 4 + 1] = r[1];
+        positions[size_t{j} * 4 + 2] = r[2];
+        positions[size_t{j} * 4 + 3] = 1.0f;
+        float rgb[3] = {1.0f, 1.0f, 1.0f};
+        if (colourKind == 1) {
+            for (int c = 0; c < 3; ++c) rgb[c] = srgbToLinear(r[3 + c] / 255.0f);
+        } else if (colourKind == 2) {
+            for (int c = 0; c < 3; ++c) rgb[c] = r[3 + c];
+        }
+        colours[size_t{j} * 2] = floatToHalf(rgb[0]) | (floatToHalf(rgb[1]) << 16);
+        colours[size_t{j} * 2 + 1] = floatToHalf(rgb[2]) | (floatToHalf(1.0f) << 16);
+        ++j;
+    }
+    *kept = j;
+    return LRT_OK;
+}
+
+int ora_random_points(uint32_t count, uint64_t seed, float* raw) {
+    // tests/render/test_points.cpp:22-44 (Lcg + randomPoints): x in [-2, 2],
+    // y in [-1.5, 1.5], z in [-2, 2], linear rgb in [0, 1].
+    uint64_t state = 0x2545F4914F6CDD1DULL ^ seed;
+    auto next = [&]() {
+        state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+        return static_cast<float>((state >> 40) & 0xFFFFFF) / 16777216.0F;
+    };
+    auto range = [&](float lo, float hi) { return lo + (hi - lo) * next(); };
+    for (uint32_t i = 0; i < count; ++i) {
+        float* r = raw + size_t{i} * 6;
+        r[0] = range(-2.0F, 2.0F);
+        r[1] = range(-1.5F, 1.5F);
+        r[2] = range(-2.0F, 2.0F);
+        r[3] = range(0.0F, 1.0F);
+        r[4] = range(0.0F, 1.0F);
+        r[5] = range(0.0F, 1.0F);
     }
     return LRT_OK;
 }

@@ -78,6 +78,28 @@ int ora_train_render(const lrt_projection* projection, const lrt_train_params* p
                      uint32_t crop_y0, uint32_t crop_w, uint32_t crop_h, uint32_t* list_offsets,
                      uint32_t* list_slots, uint64_t list_capacity, uint64_t* list_total);
 
+/* The rasteriser with point instances drawn as opaque discs and an optional
+ * under layer (TileRasterizer::render's `points` and `under`,
+ * splatBlendComposite). Points and the under layer are HOST pointers;
+ * under_colour / under_depth may be NULL. */
+int ora_render_composite(const lrt_projection* projection, const lrt_splat_instance* instances,
+                         uint32_t instance_count, const lrt_point_instance* points, uint32_t point_count,
+                         const float* under_colour, const float* under_depth, const lrt_render_settings* settings,
+                         ora_frame_out* out, uint32_t threads);
+
+/* The brute force with point discs (ReferenceRenderer::render's `points`). */
+int ora_reference_render_composite(const lrt_projection* projection, const lrt_splat_instance* instances,
+                                   uint32_t instance_count, const lrt_point_instance* points, uint32_t point_count,
+                                   const lrt_render_settings* settings, float* colour, float* depth,
+                                   uint32_t* overflow, uint32_t threads);
+
+/* Raw point records (x y z r g b) to positions/colours, as lrt_pack_points. */
+int ora_pack_points(const float* raw, uint32_t count, uint32_t colour_kind, float detail, float* positions,
+                    uint32_t* colours, uint32_t* kept);
+
+/* The reference points test's randomPoints (tests/render/test_points.cpp:22-44). */
+int ora_random_points(uint32_t count, uint64_t seed, float* raw);
+
 /* The brute-force ground truth (ReferenceRenderer). Returns the number of
  * pixels whose contributor count passed kMaxHits in *overflow. */
 int ora_reference_render(const lrt_projection* projection, const lrt_splat_instance* instances,

@@ -65,6 +65,16 @@ def load() -> C.CDLL:
     lib.ora_reference_render.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.SplatInstanceStruct),
                                          C.c_uint32, C.POINTER(_abi.RenderSettingsStruct), C.c_void_p, C.c_void_p,
                                          C.POINTER(C.c_uint32), C.c_uint32]
+    lib.ora_render_composite.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.SplatInstanceStruct), C.c_uint32,
+                                         C.POINTER(_abi.PointInstanceStruct), C.c_uint32, C.c_void_p, C.c_void_p,
+                                         C.POINTER(_abi.RenderSettingsStruct), C.POINTER(FrameOut), C.c_uint32]
+    lib.ora_reference_render_composite.argtypes = [
+        C.POINTER(_abi.Projection), C.POINTER(_abi.SplatInstanceStruct), C.c_uint32,
+        C.POINTER(_abi.PointInstanceStruct), C.c_uint32, C.POINTER(_abi.RenderSettingsStruct), C.c_void_p,
+        C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32]
+    lib.ora_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_uint32)]
+    lib.ora_random_points.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p]
     lib.ora_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint64)]
@@ -142,6 +152,55 @@ def random_cloud(count: int, seed: int, min_size=0.004, max_size=0.6, min_opacit
     return raw
 
 
+@dataclass
+class HostPoints:
+    positions: np.ndarray   # [N, 4] float32
+    colours: np.ndarray     # [N, 2] uint32 (f16 r|g, b|a)
+
+    @property
+    def count(self) -> int:
+        return int(self.positions.shape[0])
+
+    def struct(self) -> _abi.GpuPointsStruct:
+        s = _abi.GpuPointsStruct()
+        s.count = self.count
+        s.positions = self.positions.ctypes.data
+        s.colours = self.colours.ctypes.data
+        return s
+
+
+def pack_points(raw: np.ndarray, colour_kind: int = 2, detail: float = 1.0) -> HostPoints:
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    n = raw.shape[0]
+    pos = np.empty((n, 4), np.float32)
+    col = np.empty((n, 2), np.uint32)
+    kept = C.c_uint32()
+    _check(load().ora_pack_points(raw.ctypes.data, n, colour_kind, detail, pos.ctypes.data, col.ctypes.data,
+                                  C.byref(kept)), "pack_points")
+    k = kept.value
+    return HostPoints(pos[:k].copy(), col[:k].copy())
+
+
+def random_points(count: int, seed: int) -> np.ndarray:
+    """The reference points test's randomPoints (x y z r g b records)."""
+    raw = np.empty((count, 6), np.float32)
+    _check(load().ora_random_points(count, seed, raw.ctypes.data), "random_points")
+    return raw
+
+
+def _points(points):
+    """points: list of (HostPoints, object_to_world 4x4, lrt_point_style)."""
+    arr = (_abi.PointInstanceStruct * max(1, len(points)))()
+    keep = []
+    for k, (cloud, m, style) in enumerate(points):
+        cs = cloud.struct()
+        keep.append(cs)
+        arr[k].points = C.pointer(cs)
+        arr[k].object_to_world[:] = [float(v) for v in np.asarray(m, np.float64).reshape(16)]
+        arr[k].style = style
+    return arr, keep
+
+
 # ------------------------------------------------------------- rendering ----
 def _instances(instances):
     """instances: list of (HostCloud, object_to_world 4x4, edit lrt_splat_edit | None)."""
@@ -158,8 +217,11 @@ def _instances(instances):
 
 
 def render(projection: _abi.Projection, instances, settings: _abi.RenderSettingsStruct, threads: int = 0,
-           want_pairs: bool = True) -> dict:
-    slots = sum(c.count for c, _, _ in instances)
+           want_pairs: bool = True, points=(), under=None) -> dict:
+    """The restated rasteriser; `points` (HostPoints, matrix, style) are drawn
+    as discs after the splats, `under` is an optional (colour [H,W,4], depth
+    [H,W]) layer -- either makes the frame a composite one."""
+    slots = sum(c.count for c, _, _ in instances) + sum(p.count for p, _, _ in points)
     tiles_x = (settings.width + 15) // 16
     tiles_y = (settings.height + 15) // 16
     w, h = settings.width, settings.height
@@ -178,8 +240,19 @@ def render(projection: _abi.Projection, instances, settings: _abi.RenderSettings
     out.ranges = ranges.ctypes.data
     out.pair_capacity = cap
     arr, keep = _instances(instances)
-    _check(load().ora_render(C.byref(projection), arr, len(instances), C.byref(settings), C.byref(out), threads),
-           "render")
+    parr, pkeep = _points(points)
+    if under is not None:
+        under = (np.ascontiguousarray(under[0], np.float32), np.ascontiguousarray(under[1], np.float32))
+
+    def run(o):
+        if not points and under is None:
+            return load().ora_render(C.byref(projection), arr, len(instances), C.byref(settings), C.byref(o), threads)
+        uc = under[0].ctypes.data if under is not None else None
+        ud = under[1].ctypes.data if under is not None else None
+        return load().ora_render_composite(C.byref(projection), arr, len(instances), parr, len(points), uc, ud,
+                                           C.byref(settings), C.byref(o), threads)
+
+    _check(run(out), "render")
     pairs = int(out.pairs)
     result = dict(colour=colour, depth=depth, proj=proj, rects=rects, touched=touched, depth_keys=keys,
                   ranges=ranges, pairs=pairs, visible=int(out.visible), slots=int(out.slots),
@@ -191,23 +264,28 @@ def render(projection: _abi.Projection, instances, settings: _abi.RenderSettings
         ps = np.zeros(pairs, np.uint32)
         out2 = FrameOut()
         out2.pair_tiles, out2.pair_slots, out2.pair_capacity = pt.ctypes.data, ps.ctypes.data, pairs
-        _check(load().ora_render(C.byref(projection), arr, len(instances), C.byref(settings), C.byref(out2),
-                                 threads), "render")
+        _check(run(out2), "render")
         result["pair_tiles"] = pt
         result["pair_slots"] = ps
     return result
 
 
 def reference_render(projection: _abi.Projection, instances, settings: _abi.RenderSettingsStruct,
-                     threads: int = 0):
+                     threads: int = 0, points=()):
     w, h = settings.width, settings.height
     colour = np.zeros((h, w, 4), np.float32)
     depth = np.zeros((h, w), np.float32)
     over = C.c_uint32()
     arr, keep = _instances(instances)
-    _check(load().ora_reference_render(C.byref(projection), arr, len(instances), C.byref(settings),
-                                       colour.ctypes.data, depth.ctypes.data, C.byref(over), threads),
-           "reference_render")
+    if points:
+        parr, pkeep = _points(points)
+        _check(load().ora_reference_render_composite(C.byref(projection), arr, len(instances), parr, len(points),
+                                                     C.byref(settings), colour.ctypes.data, depth.ctypes.data,
+                                                     C.byref(over), threads), "reference_render")
+    else:
+        _check(load().ora_reference_render(C.byref(projection), arr, len(instances), C.byref(settings),
+                                           colour.ctypes.data, depth.ctypes.data, C.byref(over), threads),
+               "reference_render")
     return colour, depth, int(over.value)
 
 

@@ -172,3 +172,44 @@ def pair_words_to_tile_slot(words: np.ndarray, slot_bits: int):
     keys = ((w >> np.uint64(slot_bits)) & np.uint64(0xFFFFFF)).astype(np.uint32)
     tiles = (w >> np.uint64(24 + slot_bits)).astype(np.uint32)
     return tiles, keys, slots
+
+
+# ------------------------------------------------------------------ points --
+def point_style(size_mode: int = 0, size: float = 0.01, constant_colour: bool = False,
+                colour=(1.0, 1.0, 1.0)) -> _abi.PointStyleStruct:
+    s = _abi.PointStyleStruct()
+    s.size_mode = size_mode
+    s.size = size
+    s.constant_colour = 1 if constant_colour else 0
+    s.colour[:] = list(map(float, colour))
+    return s
+
+
+class Lcg:
+    """tests/render/test_points.cpp:22-30 in float32 arithmetic."""
+
+    def __init__(self, seed: int = 0):
+        self.state = 0x2545F4914F6CDD1D ^ seed
+
+    def next(self) -> np.float32:
+        self.state = (self.state * 6364136223846793005 + 1442695040888963407) & 0xFFFFFFFFFFFFFFFF
+        return np.float32((self.state >> 40) & 0xFFFFFF) / np.float32(16777216.0)
+
+    def range(self, lo, hi) -> np.float32:
+        lo, hi = np.float32(lo), np.float32(hi)
+        return lo + (hi - lo) * self.next()
+
+
+def fog_records(count: int = 40) -> np.ndarray:
+    """The 40 large translucent splats of tests/render/test_points.cpp:164-178,
+    the same draws written in the PLY encoding (logit opacity, log scales,
+    identity rotation, base colour through the DC term)."""
+    rng = Lcg()
+    out = []
+    for _ in range(count):
+        x, y, z = rng.range(-2, 2), rng.range(-1, 1), rng.range(-2, 3)
+        opacity = rng.range(0.1, 0.6)
+        sx, sy, sz = rng.range(0.1, 0.5), rng.range(0.1, 0.5), rng.range(0.1, 0.5)
+        colour = (rng.range(0, 1), rng.range(0, 1), rng.range(0, 1))
+        out.append(cloud_record(x, y, z, opacity, sx, sy, sz, (1, 0, 0, 0), colour))
+    return np.stack(out)

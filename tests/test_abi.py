@@ -52,6 +52,8 @@ int main(void) {
   S(lrt_frame_stats) O(lrt_frame_stats, total_ms)
   S(lrt_targets) S(lrt_debug_view) O(lrt_debug_view, visible)
   S(lrt_train_params) O(lrt_train_params, sh) S(lrt_train_grads) O(lrt_train_grads, sh)
+  S(lrt_gpu_points) O(lrt_gpu_points, colours) S(lrt_point_style) O(lrt_point_style, colour)
+  S(lrt_point_instance) O(lrt_point_instance, style)
   return 0;
 }
 """
@@ -62,6 +64,8 @@ CTYPES = {
     "lrt_splat_instance": _abi.SplatInstanceStruct, "lrt_render_settings": _abi.RenderSettingsStruct,
     "lrt_frame_stats": _abi.FrameStatsStruct, "lrt_targets": _abi.TargetsStruct, "lrt_debug_view": _abi.DebugView,
     "lrt_train_params": _abi.TrainParams, "lrt_train_grads": _abi.TrainGrads,
+    "lrt_gpu_points": _abi.GpuPointsStruct, "lrt_point_style": _abi.PointStyleStruct,
+    "lrt_point_instance": _abi.PointInstanceStruct,
 }
 
 
