@@ -401,6 +401,54 @@ int lrt_pack_splats(const float* raw, uint32_t count, uint32_t floats_per_record
                     uint32_t file_per_colour, uint32_t keep_per_colour, float* positions,
                     uint32_t* shape, uint32_t* sh, uint32_t* kept);
 
+/* io::SplatEncoding (io/RawSplats.h:15-70): where a raw record's fields are,
+ * in floats from its start, and how each is encoded. Modes:
+ *   opacity_mode  0 logit, 1 linear, 2 byte (v / 255)
+ *   scale_mode    0 log, 1 linear, 2 SPZ byte (log scale = v / 16 - 10)
+ *   colour_mode   0 SH DC (0.5 + SH0 v), 1 linear, 2 byte, 3 SPZ byte,
+ *                 4 linear light (taken to the sRGB curve the blend undoes)
+ *   rotation_mode 0 floats w x y z, 1 bytes ((v - 128) / 128),
+ *                 2 SPZ first three (x y z bytes, w from unit length),
+ *                 3 SPZ smallest three (a uint32 in two 16-bit halves at
+ *                 rot_x and rot_y)
+ *   rest_mode     0 floats, 1 bytes ((v - 128) / 128)
+ * rest_colour_outer 1: the rest coefficients are all red, then green, then
+ * blue (3DGS PLY), 0: rgb per basis (SPZ). flip_yz: the file is right-up-
+ * back, and y and z of positions, rotations and harmonics change sign.
+ * lrt_splat_encoding_ply fills the 3DGS PLY layout. */
+typedef struct lrt_splat_encoding {
+    uint32_t floats_per_record;
+    uint32_t x, y, z, opacity;
+    uint32_t scale0, scale1, scale2;
+    uint32_t rot_w, rot_x, rot_y, rot_z;
+    uint32_t dc0, dc1, dc2;
+    uint32_t rest_base, rest_per_colour, rest_colour_outer;
+    uint32_t opacity_mode, scale_mode, colour_mode, rotation_mode, rest_mode;
+    float position_scale;
+    uint32_t flip_yz;
+} lrt_splat_encoding;
+
+int lrt_splat_encoding_ply(uint32_t rest_per_colour, lrt_splat_encoding* out);
+
+/* CloudLoader::upload's decode on the device (GpuClouds.cpp:151-226,
+ * splat_validate.slang, splat_decode.slang): `count` raw records (a device
+ * pointer, floats_per_record floats each) are validated (finite position and
+ * log scales under 60 in size, opacity at least 1/255), compacted in order
+ * and packed into the caller's device buffers of `count` capacity
+ * (positions float4, shape uint32 x4, sh (keep_per_colour * 3 + 1) / 2 words,
+ * one minimum), in one kernel. Returns the kept count in *kept (the call
+ * waits for it). keep_per_colour <= rest_per_colour. The per-splat material
+ * words of converted meshes (relighting) are not produced. */
+int lrt_rast_decode_splats(lrt_rast* rast, const void* raw, uint32_t count, const lrt_splat_encoding* encoding,
+                           uint32_t keep_per_colour, void* positions, void* shape, void* sh, uint32_t* kept,
+                           void* stream);
+
+/* The same for points (points_validate.slang, points_decode.slang): `count`
+ * raw x y z r g b records on the device into positions and colours, as
+ * lrt_pack_points does on the host. */
+int lrt_rast_decode_points(lrt_rast* rast, const void* raw, uint32_t count, uint32_t colour_kind, float detail,
+                           void* positions, void* colours, uint32_t* kept, void* stream);
+
 /* Raw point records (x y z r g b, 6 floats) to the GpuPoints layout above, on
  * the host (the upload half of CloudLoader for points: points_validate.slang
  * and points_decode.slang). colour_kind: 0 none (white), 1 sRGB bytes in

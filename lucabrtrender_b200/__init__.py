@@ -8,8 +8,9 @@ from ._abi import LrtError
 from .camera import Camera, Lens, Projection, projection_for, square_pixel_camera
 from .raster import (Depth, EditMode, EditShape, FrameStats, PointInstance, PointStyle, RenderSettings, RenderTargets,
                      SplatEdit, SplatInstance, TileRasterizer, math_eval)
+from ._abi import SplatEncoding
 from .scene import (CloudLoader, GpuPoints, GpuSplats, PackedPoints, PackedSplats, pack_points, pack_splats,
-                    points_to_device, synthetic_records, to_device)
+                    ply_encoding, points_to_device, synthetic_records, to_device)
 from .train import rasterize
 
 __all__ = [
@@ -17,4 +18,5 @@ __all__ = [
     "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
     "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
     "PointInstance", "PointStyle", "GpuPoints", "PackedPoints", "pack_points", "points_to_device",
+    "SplatEncoding", "ply_encoding",
 ]

@@ -39,7 +39,8 @@ EXPORTS = (
     "lrt_rast_debug_view", "lrt_camera_looking_at", "lrt_projection_for", "lrt_prefix_sum", "lrt_radix_sort",
     "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
     "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
-    "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points",
+    "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points", "lrt_splat_encoding_ply",
+    "lrt_rast_decode_splats", "lrt_rast_decode_points",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -109,6 +110,15 @@ class PointInstanceStruct(C.Structure):
         ("object_to_world", C.c_double * 16),
         ("style", PointStyleStruct),
     ]
+
+
+class SplatEncoding(C.Structure):
+    """lrt_splat_encoding (io::SplatEncoding): field offsets and modes."""
+    _fields_ = [(n, C.c_uint32) for n in (
+        "floats_per_record", "x", "y", "z", "opacity", "scale0", "scale1", "scale2", "rot_w", "rot_x", "rot_y",
+        "rot_z", "dc0", "dc1", "dc2", "rest_base", "rest_per_colour", "rest_colour_outer", "opacity_mode",
+        "scale_mode", "colour_mode", "rotation_mode", "rest_mode")] + [("position_scale", C.c_float),
+                                                                        ("flip_yz", C.c_uint32)]
 
 
 class RenderSettingsStruct(C.Structure):
@@ -201,6 +211,11 @@ def load() -> C.CDLL:
                                               C.POINTER(TargetsStruct), C.POINTER(FrameStatsStruct), C.c_void_p]
     lib.lrt_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_uint32)]
+    lib.lrt_splat_encoding_ply.argtypes = [C.c_uint32, C.POINTER(SplatEncoding)]
+    lib.lrt_rast_decode_splats.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(SplatEncoding), C.c_uint32,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
+    lib.lrt_rast_decode_points.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p,
+                                           C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
     lib.lrt_rast_debug_view.argtypes = [C.c_void_p, C.POINTER(DebugView)]
     lib.lrt_camera_looking_at.argtypes = [C.POINTER(C.c_double)] * 3 + [C.POINTER(CameraStruct)]
     lib.lrt_projection_for.argtypes = [C.POINTER(CameraStruct), C.c_uint32, C.c_uint32, C.POINTER(Projection)]

@@ -1,0 +1,359 @@
+// Cloud decode on the device: raw records to the packed layout the projection
+// reads (CloudLoader::upload, modules/scene/src/GpuClouds.cpp:151-226).
+//
+// The reference runs three dispatches per slice: validate (a flag per
+// record, shaders/lrt/scene/splat_validate.slang:14-29), a prefix sum of the
+// flags, and decode (splat_decode.slang:20-91, which writes record i at
+// base + dest[i] when it is valid). Here one kernel does all three: a block
+// validates its 256 records, scans their flags, takes the count of kept
+// records before it from a decoupled look-back over the earlier blocks
+// (taken in ticket order), and decodes its kept records straight to their
+// places. The decode arithmetic restates splat_encoding.slang:21-115 and
+// packing.slang:26-50,104-113 expression for expression; the library is built
+// with -fmad=false, so it rounds as the CPU restatement does.
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+#include <cuda/atomic>
+
+namespace lrt {
+namespace {
+
+constexpr uint32_t kDecodeThreads = 256;
+constexpr uint64_t kFlagAggregate = 1ull << 62;
+constexpr uint64_t kFlagInclusive = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
+constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr float kSH0 = 0.28209479177387814f;
+constexpr float kSqrtHalf = 0.70710678f;
+
+__device__ __forceinline__ float field_of(const float* raw, uint32_t record, uint32_t stride, uint32_t field) {
+    return raw[static_cast<size_t>(record) * stride + field];
+}
+
+__device__ __forceinline__ float decode_opacity(float v, uint32_t mode) {
+    if (mode == 0) return 1.0f / (1.0f + lrt_exp(-v));
+    if (mode == 2) return v / 255.0f;
+    return v;
+}
+
+__device__ __forceinline__ float3 decode_position(const float* raw, uint32_t i, const lrt_splat_encoding& e) {
+    const uint32_t s = e.floats_per_record;
+    const float3 v = make_float3(field_of(raw, i, s, e.x) * e.position_scale, field_of(raw, i, s, e.y) * e.position_scale,
+                                 field_of(raw, i, s, e.z) * e.position_scale);
+    return e.flip_yz != 0 ? make_float3(v.x, -v.y, -v.z) : v;
+}
+
+__device__ __forceinline__ float decode_log_scale(float v, uint32_t mode) {
+    if (mode == 2) return v / 16.0f - 10.0f;
+    return mode == 0 ? v : lrt_log(fmaxf(v, 1e-30f));
+}
+
+// color.slang:21-24
+__device__ __forceinline__ float linear_to_srgb(float c) {
+    c = fmaxf(c, 0.0f);
+    return c <= 0.0031308f ? c * 12.92f : 1.055f * lrt_pow(c, 1.0f / 2.4f) - 0.055f;
+}
+
+__device__ __forceinline__ float decode_colour(float v, uint32_t mode) {
+    if (mode == 0) return 0.5f + kSH0 * v;
+    if (mode == 2) return v / 255.0f;
+    if (mode == 3) return 0.5f + kSH0 * ((v / 255.0f - 0.5f) / 0.15f);
+    if (mode == 4) return linear_to_srgb(v);
+    return v;
+}
+
+__device__ __forceinline__ float decode_byte_unit(float v, uint32_t mode) { return mode == 1 ? (v - 128.0f) / 128.0f : v; }
+
+// splat_encoding.slang:80-85: the sign of a rest coefficient under y, z -> -y, -z.
+__device__ __forceinline__ float rest_flip_sign(uint32_t basis) {
+    constexpr uint32_t kNegative = 0x2D4Bu;   // bases 0 1 3 6 8 10 11 13 are odd in y xor z
+    return (kNegative >> min(basis, 14u)) & 1u ? -1.0f : 1.0f;
+}
+
+// splat_encoding.slang:91-126: (x, y, z, w), not yet normalised.
+__device__ __forceinline__ float4 decode_quaternion(const float* raw, uint32_t i, const lrt_splat_encoding& e) {
+    const uint32_t s = e.floats_per_record;
+    float q[4];
+    if (e.rotation_mode == 2) {
+        const float x = field_of(raw, i, s, e.rot_x) / 127.5f - 1.0f;
+        const float y = field_of(raw, i, s, e.rot_y) / 127.5f - 1.0f;
+        const float z = field_of(raw, i, s, e.rot_z) / 127.5f - 1.0f;
+        q[0] = x;
+        q[1] = y;
+        q[2] = z;
+        q[3] = sqrtf(fmaxf(0.0f, 1.0f - (x * x + y * y + z * z)));
+    } else if (e.rotation_mode == 3) {
+        uint32_t comp = static_cast<uint32_t>(field_of(raw, i, s, e.rot_x)) |
+                        (static_cast<uint32_t>(field_of(raw, i, s, e.rot_y)) << 16);
+        const uint32_t largest = comp >> 30;
+        q[0] = q[1] = q[2] = q[3] = 0.0f;
+        float sum = 0.0f;
+        for (int k = 3; k >= 0; --k) {
+            if (static_cast<uint32_t>(k) == largest) continue;
+            const float magnitude = kSqrtHalf * static_cast<float>(comp & 511u) / 511.0f;
+            q[k] = ((comp >> 9) & 1u) != 0 ? -magnitude : magnitude;
+            sum = sum + q[k] * q[k];
+            comp = comp >> 10;
+        }
+        q[largest] = sqrtf(fmaxf(0.0f, 1.0f - sum));
+    } else {
+        q[0] = decode_byte_unit(field_of(raw, i, s, e.rot_x), e.rotation_mode);
+        q[1] = decode_byte_unit(field_of(raw, i, s, e.rot_y), e.rotation_mode);
+        q[2] = decode_byte_unit(field_of(raw, i, s, e.rot_z), e.rotation_mode);
+        q[3] = decode_byte_unit(field_of(raw, i, s, e.rot_w), e.rotation_mode);
+    }
+    if (e.flip_yz != 0) return make_float4(q[0], -q[1], -q[2], q[3]);
+    return make_float4(q[0], q[1], q[2], q[3]);
+}
+
+// packing.slang:26-50: smallest three of the normalised quaternion.
+__device__ __forceinline__ uint32_t encode_quaternion(float4 q0) {
+    const float l = sqrtf(q0.x * q0.x + q0.y * q0.y + q0.z * q0.z + q0.w * q0.w);
+    float q[4] = {q0.x / l, q0.y / l, q0.z / l, q0.w / l};
+    uint32_t largest = 0;
+    float best = fabsf(q[0]);
+    for (uint32_t k = 1; k < 4; ++k) {
+        if (fabsf(q[k]) > best) {
+            best = fabsf(q[k]);
+            largest = k;
+        }
+    }
+    if (q[largest] < 0.0f) {
+        for (float& v : q) v = -v;
+    }
+    uint32_t word = largest;
+    uint32_t shift = 22;
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (k == largest) continue;
+        const float unit = fminf(fmaxf(q[k] / kSqrtHalf * 0.5f + 0.5f, 0.0f), 1.0f);
+        word |= static_cast<uint32_t>(roundf(unit * 1023.0f)) << shift;
+        shift -= 10;
+    }
+    return word;
+}
+
+__device__ __forceinline__ float half_safe(float v) { return fminf(fmaxf(v, -65000.0f), 65000.0f); }
+__device__ __forceinline__ uint32_t pack_halves(float a, float b) {
+    return (float_to_half(a) & 0xFFFFu) | ((float_to_half(b) & 0xFFFFu) << 16);
+}
+
+// One block's exclusive scan of a flag per thread; *total gets the block's sum.
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* sWarp, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= d) x += o;
+    }
+    if (lane == 31) sWarp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kDecodeThreads / 32 ? sWarp[lane] : 0;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= d) w += o;
+        }
+        if (lane < kDecodeThreads / 32) sWarp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp == 0 ? 0 : sWarp[warp - 1];
+    *total = sWarp[kDecodeThreads / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+// The kept records before this block: decoupled look-back by warp 0 over a
+// window of 32 earlier blocks at a time (bounded waits). Returns the prefix
+// to every thread; the last block also writes the grand total.
+__device__ __forceinline__ uint32_t block_base(uint32_t part, uint32_t lastPart, uint32_t blockTotal,
+                                               uint64_t* status, uint32_t* total, uint32_t* err, uint32_t* sBase) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (threadIdx.x < 32) {
+        uint64_t prefix = 0;
+        if (lane == 0) {
+            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[part]);
+            mine.store((part == 0 ? kFlagInclusive : kFlagAggregate) | blockTotal, cuda::memory_order_relaxed);
+        }
+        if (part > 0) {
+            int64_t q = static_cast<int64_t>(part) - 1;
+            uint32_t spins = 0;
+            while (true) {
+                const int64_t idx = q - static_cast<int64_t>(lane);
+                uint64_t word = kFlagInclusive;
+                if (idx >= 0) {
+                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[idx]);
+                    word = sref.load(cuda::memory_order_relaxed);
+                }
+                const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, (word & kFlagInclusive) != 0);
+                const uint32_t empty = __ballot_sync(0xFFFFFFFFu, (word & ~kValueMask) == 0);
+                const uint32_t first = inclusive != 0 ? static_cast<uint32_t>(__ffs(inclusive)) - 1u : 32u;
+                const uint32_t upTo = first < 32u ? (2u << first) - 1u : 0xFFFFFFFFu;
+                if ((empty & upTo) != 0) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) atomicOr(err, kErrTimeout);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                uint64_t v = ((upTo >> lane) & 1u) ? (word & kValueMask) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                prefix += v;
+                if (first < 32u) break;
+                q -= 32;
+            }
+            if (lane == 0) {
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[part]);
+                mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
+            }
+        }
+        if (lane == 0) {
+            *sBase = static_cast<uint32_t>(prefix);
+            if (part == lastPart) *total = static_cast<uint32_t>(prefix + blockTotal);
+        }
+    }
+    __syncthreads();
+    return *sBase;
+}
+
+__global__ void __launch_bounds__(kDecodeThreads)
+decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_encoding e, uint32_t keep,
+                     uint32_t shWords, float4* __restrict__ positions, uint4* __restrict__ shape,
+                     uint32_t* __restrict__ sh, uint64_t* __restrict__ status, uint32_t* __restrict__ ticket,
+                     uint32_t* __restrict__ total, uint32_t* __restrict__ err) {
+    __shared__ uint32_t sPart, sBase;
+    __shared__ uint32_t sWarp[kDecodeThreads / 32];
+    if (threadIdx.x == 0) sPart = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t part = sPart;
+    const uint32_t i = part * kDecodeThreads + threadIdx.x;
+    const bool inRange = i < count;
+    const uint32_t s = e.floats_per_record;
+
+    // splat_validate.slang:19-28
+    bool valid = false;
+    float3 p = make_float3(0.0f, 0.0f, 0.0f);
+    float a = 0.0f, ls0 = 0.0f, ls1 = 0.0f, ls2 = 0.0f;
+    if (inRange) {
+        p = decode_position(raw, i, e);
+        a = decode_opacity(field_of(raw, i, s, e.opacity), e.opacity_mode);
+        ls0 = decode_log_scale(field_of(raw, i, s, e.scale0), e.scale_mode);
+        ls1 = decode_log_scale(field_of(raw, i, s, e.scale1), e.scale_mode);
+        ls2 = decode_log_scale(field_of(raw, i, s, e.scale2), e.scale_mode);
+        const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(ls0) && isfinite(ls1) &&
+                            isfinite(ls2) && fabsf(ls0) < 60.0f && fabsf(ls1) < 60.0f && fabsf(ls2) < 60.0f;
+        valid = finite && a >= 1.0f / 255.0f;
+    }
+    uint32_t blockTotal = 0;
+    const uint32_t local = block_scan(valid ? 1u : 0u, sWarp, &blockTotal);
+    const uint32_t lastPart = (count + kDecodeThreads - 1) / kDecodeThreads - 1;
+    const uint32_t base = block_base(part, lastPart, blockTotal, status, total, err, &sBase);
+    if (!valid) return;
+
+    // splat_decode.slang:30-90
+    const uint32_t j = base + local;
+    positions[j] = make_float4(p.x, p.y, p.z, fminf(fmaxf(a, 0.0f), 1.0f));
+    const float4 q = decode_quaternion(raw, i, e);
+    const float qLength = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    const uint32_t rotation = encode_quaternion(qLength > 1e-8f ? q : make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+    const float b0 = decode_colour(field_of(raw, i, s, e.dc0), e.colour_mode);
+    const float b1 = decode_colour(field_of(raw, i, s, e.dc1), e.colour_mode);
+    const float b2 = decode_colour(field_of(raw, i, s, e.dc2), e.colour_mode);
+    shape[j] = make_uint4(rotation, pack_halves(half_safe(ls0), half_safe(ls1)), pack_halves(half_safe(ls2), half_safe(b0)),
+                          pack_halves(half_safe(b1), half_safe(b2)));
+    // Rest coefficients, rgb per basis; every word of the row is written
+    // (unused halves zero).
+    uint32_t* row = sh + static_cast<size_t>(j) * shWords;
+    uint32_t word = 0, filled = 0, at = 0;
+    for (uint32_t basis = 0; basis < keep; ++basis) {
+        for (uint32_t colour = 0; colour < 3; ++colour) {
+            const uint32_t field = e.rest_colour_outer != 0 ? e.rest_base + colour * e.rest_per_colour + basis
+                                                            : e.rest_base + basis * 3 + colour;
+            float value = decode_byte_unit(field_of(raw, i, s, field), e.rest_mode);
+            if (e.flip_yz != 0) value = value * rest_flip_sign(basis);
+            word |= (float_to_half(half_safe(value)) & 0xFFFFu) << (filled * 16);
+            if (++filled == 2) {
+                row[at++] = word;
+                word = 0;
+                filled = 0;
+            }
+        }
+    }
+    if (filled == 1) row[at++] = word;
+    for (; at < shWords; ++at) row[at] = 0u;
+}
+
+// points_validate.slang:19-28 and points_decode.slang:24-41, fused the same way.
+__global__ void __launch_bounds__(kDecodeThreads)
+decode_points_kernel(const float* __restrict__ raw, uint32_t count, uint32_t colourKind, float detail,
+                     float4* __restrict__ positions, uint2* __restrict__ colours, uint64_t* __restrict__ status,
+                     uint32_t* __restrict__ ticket, uint32_t* __restrict__ total, uint32_t* __restrict__ err) {
+    __shared__ uint32_t sPart, sBase;
+    __shared__ uint32_t sWarp[kDecodeThreads / 32];
+    if (threadIdx.x == 0) sPart = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t part = sPart;
+    const uint32_t i = part * kDecodeThreads + threadIdx.x;
+    bool valid = false;
+    float r[6] = {0, 0, 0, 0, 0, 0};
+    if (i < count) {
+        for (int k = 0; k < 6; ++k) r[k] = raw[static_cast<size_t>(i) * 6 + k];
+        const uint32_t state = i * 747796405u + 2891336453u;   // hash01, color.slang:30-34
+        const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+        const float hash = static_cast<float>((word >> 22u) ^ word) / 4294967295.0f;
+        const bool kept = detail >= 1.0f || hash < detail;
+        valid = isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]) && kept;
+    }
+    uint32_t blockTotal = 0;
+    const uint32_t local = block_scan(valid ? 1u : 0u, sWarp, &blockTotal);
+    const uint32_t lastPart = (count + kDecodeThreads - 1) / kDecodeThreads - 1;
+    const uint32_t base = block_base(part, lastPart, blockTotal, status, total, err, &sBase);
+    if (!valid) return;
+    const uint32_t j = base + local;
+    positions[j] = make_float4(r[0], r[1], r[2], 1.0f);
+    float rgb[3] = {1.0f, 1.0f, 1.0f};
+    for (int c = 0; c < 3; ++c) {
+        if (colourKind == 1) rgb[c] = srgb_to_linear(r[3 + c] / 255.0f);
+        if (colourKind == 2) rgb[c] = r[3 + c];
+    }
+    colours[j] = make_uint2(pack_halves(rgb[0], rgb[1]), pack_halves(rgb[2], 1.0f));
+}
+
+}  // namespace
+
+size_t decode_status_bytes(uint32_t count) {
+    return size_t{std::max<uint32_t>((count + kDecodeThreads - 1) / kDecodeThreads, 1u)} * sizeof(uint64_t) + 16;
+}
+
+// scratch: decode_status_bytes(count) bytes, zeroed by the caller; its last
+// 16 bytes hold the ticket and the total.
+cudaError_t launch_decode_splats(const float* raw, uint32_t count, const lrt_splat_encoding& e, uint32_t keep,
+                                 uint32_t shWords, float4* positions, uint4* shape, uint32_t* sh, void* scratch,
+                                 uint32_t* err, cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    const uint32_t blocks = (count + kDecodeThreads - 1) / kDecodeThreads;
+    uint64_t* status = static_cast<uint64_t*>(scratch);
+    uint32_t* tail = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + size_t{blocks} * 8);
+    decode_splats_kernel<<<blocks, kDecodeThreads, 0, stream>>>(raw, count, e, keep, shWords, positions, shape, sh,
+                                                                status, tail, tail + 1, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_points(const float* raw, uint32_t count, uint32_t colourKind, float detail,
+                                 float4* positions, uint32_t* colours, void* scratch, uint32_t* err,
+                                 cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    const uint32_t blocks = (count + kDecodeThreads - 1) / kDecodeThreads;
+    uint64_t* status = static_cast<uint64_t*>(scratch);
+    uint32_t* tail = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + size_t{blocks} * 8);
+    decode_points_kernel<<<blocks, kDecodeThreads, 0, stream>>>(raw, count, colourKind, detail, positions,
+                                                                reinterpret_cast<uint2*>(colours), status, tail,
+                                                                tail + 1, err);
+    return cudaGetLastError();
+}
+
+}  // namespace lrt

@@ -300,3 +300,32 @@ extern "C" int lrt_pack_points(const float* raw, uint32_t count, uint32_t colour
     *kept = j;
     return LRT_OK;
 }
+
+extern "C" int lrt_splat_encoding_ply(uint32_t restPerColour, lrt_splat_encoding* out) {
+    // io::SplatEncoding as the PLY reader fills it for a 3DGS file: x y z,
+    // logit opacity, three log scales, rotation w x y z, three DC terms, then
+    // the rest coefficients all red, then green, then blue.
+    if (out == nullptr || !(restPerColour == 0 || restPerColour == 3 || restPerColour == 8 || restPerColour == 15))
+        return LRT_INVALID_ARGUMENT;
+    *out = lrt_splat_encoding{};
+    out->floats_per_record = 14 + 3 * restPerColour;
+    out->x = 0;
+    out->y = 1;
+    out->z = 2;
+    out->opacity = 3;
+    out->scale0 = 4;
+    out->scale1 = 5;
+    out->scale2 = 6;
+    out->rot_w = 7;
+    out->rot_x = 8;
+    out->rot_y = 9;
+    out->rot_z = 10;
+    out->dc0 = 11;
+    out->dc1 = 12;
+    out->dc2 = 13;
+    out->rest_base = 14;
+    out->rest_per_colour = restPerColour;
+    out->rest_colour_outer = 1;
+    out->position_scale = 1.0f;
+    return LRT_OK;
+}

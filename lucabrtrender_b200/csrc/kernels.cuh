@@ -91,4 +91,14 @@ cudaError_t launch_splat_backward(const FrameParams& f, const float* means, cons
 
 cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
 
+// Cloud decode (decode.cu): validate, compact and pack in one kernel.
+// scratch: decode_status_bytes(count) bytes, zeroed; err: the status word.
+size_t decode_status_bytes(uint32_t count);
+cudaError_t launch_decode_splats(const float* raw, uint32_t count, const lrt_splat_encoding& e, uint32_t keep,
+                                 uint32_t shWords, float4* positions, uint4* shape, uint32_t* sh, void* scratch,
+                                 uint32_t* err, cudaStream_t stream);
+cudaError_t launch_decode_points(const float* raw, uint32_t count, uint32_t colourKind, float detail,
+                                 float4* positions, uint32_t* colours, void* scratch, uint32_t* err,
+                                 cudaStream_t stream);
+
 }  // namespace lrt

@@ -753,6 +753,82 @@ int lrt_rast_render_composite(lrt_rast* r, const lrt_projection* pr, const lrt_s
     return render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart, false, under, composite);
 }
 
+int lrt_rast_decode_splats(lrt_rast* r, const void* raw, uint32_t count, const lrt_splat_encoding* e,
+                           uint32_t keep, void* positions, void* shape, void* sh, uint32_t* kept, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (e == nullptr || kept == nullptr ||
+        (count > 0 && (raw == nullptr || positions == nullptr || shape == nullptr || sh == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    *kept = 0;
+    if (keep > e->rest_per_colour || !(keep == 0 || keep == 3 || keep == 8 || keep == 15))
+        return fail(r, LRT_INVALID_ARGUMENT, "keep_per_colour must be 0, 3, 8 or 15 and at most the file's");
+    const uint32_t fields[] = {e->x, e->y, e->z, e->opacity, e->scale0, e->scale1, e->scale2, e->rot_w, e->rot_x,
+                               e->rot_y, e->rot_z, e->dc0, e->dc1, e->dc2};
+    for (uint32_t f : fields)
+        if (f >= e->floats_per_record) return fail(r, LRT_INVALID_ARGUMENT, "a field lies past the record");
+    const uint64_t restEnd = uint64_t{e->rest_base} + 3ull * e->rest_per_colour;
+    if (e->rest_per_colour > 0 && restEnd > e->floats_per_record)
+        return fail(r, LRT_INVALID_ARGUMENT, "the rest coefficients lie past the record");
+    if ((reinterpret_cast<uintptr_t>(positions) & 15u) != 0 || (reinterpret_cast<uintptr_t>(shape) & 15u) != 0)
+        return fail(r, LRT_INVALID_ARGUMENT, "positions and shape must be 16-byte aligned");
+    if (count == 0) return LRT_OK;
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
+    const size_t bytes = lrt::decode_status_bytes(count);
+    LRT_CUDA(r, ensure(r->scanScratch, bytes), "decode scratch");
+    uint32_t* err = static_cast<uint32_t*>(r->counters.ptr) + 3;
+    LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, bytes, stream), "decode scratch");
+    LRT_CUDA(r, cudaMemsetAsync(err, 0, 4, stream), "status");
+    const uint32_t shWords = std::max<uint32_t>((keep * 3 + 1) / 2, 1);
+    LRT_CUDA(r,
+             lrt::launch_decode_splats(static_cast<const float*>(raw), count, *e, keep, shWords,
+                                       static_cast<float4*>(positions), static_cast<uint4*>(shape),
+                                       static_cast<uint32_t*>(sh), r->scanScratch.ptr, err, stream),
+             "decode");
+    const uint32_t* total = reinterpret_cast<const uint32_t*>(static_cast<char*>(r->scanScratch.ptr) + bytes - 16) + 1;
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 8, total, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 9, err, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "decode");
+    if (r->hostCounters[9] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "decode look-back gave up");
+    *kept = r->hostCounters[8];
+    return LRT_OK;
+}
+
+int lrt_rast_decode_points(lrt_rast* r, const void* raw, uint32_t count, uint32_t colourKind, float detail,
+                           void* positions, void* colours, uint32_t* kept, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (kept == nullptr || (count > 0 && (raw == nullptr || positions == nullptr || colours == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    *kept = 0;
+    if (colourKind > 2) return fail(r, LRT_INVALID_ARGUMENT, "colour_kind must be 0, 1 or 2");
+    if ((reinterpret_cast<uintptr_t>(positions) & 15u) != 0 || (reinterpret_cast<uintptr_t>(colours) & 7u) != 0)
+        return fail(r, LRT_INVALID_ARGUMENT, "positions must be 16-byte and colours 8-byte aligned");
+    if (count == 0) return LRT_OK;
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
+    const size_t bytes = lrt::decode_status_bytes(count);
+    LRT_CUDA(r, ensure(r->scanScratch, bytes), "decode scratch");
+    uint32_t* err = static_cast<uint32_t*>(r->counters.ptr) + 3;
+    LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, bytes, stream), "decode scratch");
+    LRT_CUDA(r, cudaMemsetAsync(err, 0, 4, stream), "status");
+    LRT_CUDA(r,
+             lrt::launch_decode_points(static_cast<const float*>(raw), count, colourKind, detail,
+                                       static_cast<float4*>(positions), static_cast<uint32_t*>(colours),
+                                       r->scanScratch.ptr, err, stream),
+             "decode");
+    const uint32_t* total = reinterpret_cast<const uint32_t*>(static_cast<char*>(r->scanScratch.ptr) + bytes - 16) + 1;
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 8, total, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 9, err, 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "decode");
+    if (r->hostCounters[9] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "decode look-back gave up");
+    *kept = r->hostCounters[8];
+    return LRT_OK;
+}
+
 int lrt_rast_render_async(lrt_rast* r, const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
                           const lrt_render_settings* s, lrt_targets* targets, void* streamPtr) {
     const auto frameStart = std::chrono::steady_clock::now();

@@ -322,6 +322,43 @@ class TileRasterizer:
                                               C.byref(stats), _stream_ptr(stream)))
         return targets, stats
 
+    def decode_splats(self, raw: torch.Tensor, encoding: _abi.SplatEncoding, keep_per_colour: int,
+                      stream=None) -> GpuSplats:
+        """CloudLoader::upload's decode on the device (lrt_rast_decode_splats):
+        raw records [N, floats_per_record] float32 on this device, validated,
+        compacted and packed in one kernel."""
+        raw = raw.contiguous().float()
+        n = raw.shape[0] if raw.dim() > 0 else 0
+        dev = raw.device
+        words = max((keep_per_colour * 3 + 1) // 2, 1)
+        pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        shape = torch.empty((n, 4), dtype=torch.int32, device=dev)
+        sh = torch.empty((n, words), dtype=torch.int32, device=dev)
+        kept = C.c_uint32(0)
+        self._check(_abi.load().lrt_rast_decode_splats(self._handle, raw.data_ptr() if n else None, n,
+                                                       C.byref(encoding), keep_per_colour,
+                                                       pos.data_ptr() if n else None, shape.data_ptr() if n else None,
+                                                       sh.data_ptr() if n else None, C.byref(kept),
+                                                       _stream_ptr(stream)))
+        k = kept.value
+        return GpuSplats(pos[:k], shape[:k], sh[:k], keep_per_colour)
+
+    def decode_points(self, raw: torch.Tensor, colour_kind: int = 2, detail: float = 1.0, stream=None) -> GpuPoints:
+        """Raw x y z r g b point records on this device to a GpuPoints
+        (lrt_rast_decode_points)."""
+        raw = raw.contiguous().float().reshape(-1, 6)
+        n = raw.shape[0]
+        dev = raw.device
+        pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        col = torch.empty((n, 2), dtype=torch.int32, device=dev)
+        kept = C.c_uint32(0)
+        self._check(_abi.load().lrt_rast_decode_points(self._handle, raw.data_ptr() if n else None, n, colour_kind,
+                                                       float(detail), pos.data_ptr() if n else None,
+                                                       col.data_ptr() if n else None, C.byref(kept),
+                                                       _stream_ptr(stream)))
+        k = kept.value
+        return GpuPoints(pos[:k], col[:k])
+
     def debug_view(self) -> _abi.DebugView:
         v = _abi.DebugView()
         self._check(_abi.load().lrt_rast_debug_view(self._handle, C.byref(v)))

@@ -83,6 +83,13 @@ class GpuSplats:
         return self.count * (16 + 16 + 4 * self.sh_words)
 
 
+def ply_encoding(rest_per_colour: int) -> _abi.SplatEncoding:
+    """The 3DGS PLY record layout (lrt_splat_encoding_ply)."""
+    e = _abi.SplatEncoding()
+    _abi.check(_abi.load().lrt_splat_encoding_ply(rest_per_colour, C.byref(e)), "ply_encoding")
+    return e
+
+
 def pack_splats(raw: np.ndarray, file_per_colour: int, max_degree: int = 3) -> PackedSplats:
     """Validate, compact and pack raw records on the host (lrt_pack_splats)."""
     lib = _abi.load()

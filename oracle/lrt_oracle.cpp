@@ -1555,6 +1555,112 @@ int ora_random_cloud(uint32_t count, uint64_t seed, float minSize, float maxSize
     return LRT_OK;
 }
 
+int ora_decode_splats(const float* raw, uint32_t count, const lrt_splat_encoding* e, uint32_t keep,
+                      float* positions, uint32_t* shape, uint32_t* sh, uint32_t* kept) {
+    // CloudLoader::upload for any encoding (GpuClouds.cpp:151-226):
+    // shaders/lrt/scene/splat_validate.slang:19-28, compaction in record
+    // order, splat_decode.slang:30-90 with splat_encoding.slang:21-126.
+    // Every word of a splat's sh row is written (unused halves zero).
+    if (e == nullptr || kept == nullptr) return LRT_INVALID_ARGUMENT;
+    const uint32_t s = e->floats_per_record;
+    const uint32_t shWords = std::max<uint32_t>((keep * 3 + 1) / 2, 1);
+    constexpr float kSH0 = 0.28209479177387814f;
+    constexpr float kSqrtHalf = 0.70710678f;
+    auto field = [&](uint32_t i, uint32_t f) { return raw[size_t{i} * s + f]; };
+    auto opacityOf = [&](float v) {
+        if (e->opacity_mode == 0) return 1.0f / (1.0f + expImpl(-v));
+        if (e->opacity_mode == 2) return v / 255.0f;
+        return v;
+    };
+    auto logScaleOf = [&](float v) {
+        if (e->scale_mode == 2) return v / 16.0f - 10.0f;
+        return e->scale_mode == 0 ? v : logImpl(std::fmax(v, 1e-30f));
+    };
+    auto colourOf = [&](float v) {
+        switch (e->colour_mode) {
+            case 0: return 0.5f + kSH0 * v;
+            case 2: return v / 255.0f;
+            case 3: return 0.5f + kSH0 * ((v / 255.0f - 0.5f) / 0.15f);
+            case 4: {
+                const float c = std::fmax(v, 0.0f);   // linearToSrgb, color.slang:21-24
+                return c <= 0.0031308f ? c * 12.92f : 1.055f * powImpl(c, 1.0f / 2.4f) - 0.055f;
+            }
+            default: return v;
+        }
+    };
+    auto unitOf = [](float v, uint32_t mode) { return mode == 1 ? (v - 128.0f) / 128.0f : v; };
+    static const float kSigns[15] = {-1, -1, 1, -1, 1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        F3 p{field(i, e->x) * e->position_scale, field(i, e->y) * e->position_scale,
+             field(i, e->z) * e->position_scale};
+        if (e->flip_yz != 0) p = F3{p.x, -p.y, -p.z};
+        const float a = opacityOf(field(i, e->opacity));
+        const float ls[3] = {logScaleOf(field(i, e->scale0)), logScaleOf(field(i, e->scale1)),
+                             logScaleOf(field(i, e->scale2))};
+        bool finite = std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(p.z);
+        for (float v : ls) finite = finite && std::isfinite(v) && std::fabs(v) < 60.0f;
+        if (!(finite && a >= 1.0f / 255.0f)) continue;
+
+        float* pos = positions + size_t{j} * 4;
+        pos[0] = p.x;
+        pos[1] = p.y;
+        pos[2] = p.z;
+        pos[3] = saturatef(a);
+        float q[4];   // x y z w
+        if (e->rotation_mode == 2) {
+            q[0] = field(i, e->rot_x) / 127.5f - 1.0f;
+            q[1] = field(i, e->rot_y) / 127.5f - 1.0f;
+            q[2] = field(i, e->rot_z) / 127.5f - 1.0f;
+            q[3] = std::sqrt(std::fmax(0.0f, 1.0f - (q[0] * q[0] + q[1] * q[1] + q[2] * q[2])));
+        } else if (e->rotation_mode == 3) {
+            uint32_t comp = static_cast<uint32_t>(field(i, e->rot_x)) | (static_cast<uint32_t>(field(i, e->rot_y)) << 16);
+            const uint32_t largest = comp >> 30;
+            q[0] = q[1] = q[2] = q[3] = 0.0f;
+            float sum = 0.0f;
+            for (int k = 3; k >= 0; --k) {
+                if (static_cast<uint32_t>(k) == largest) continue;
+                const float magnitude = kSqrtHalf * static_cast<float>(comp & 511u) / 511.0f;
+                q[k] = ((comp >> 9) & 1u) != 0 ? -magnitude : magnitude;
+                sum = sum + q[k] * q[k];
+                comp = comp >> 10;
+            }
+            q[largest] = std::sqrt(std::fmax(0.0f, 1.0f - sum));
+        } else {
+            q[0] = unitOf(field(i, e->rot_x), e->rotation_mode);
+            q[1] = unitOf(field(i, e->rot_y), e->rotation_mode);
+            q[2] = unitOf(field(i, e->rot_z), e->rotation_mode);
+            q[3] = unitOf(field(i, e->rot_w), e->rotation_mode);
+        }
+        if (e->flip_yz != 0) {
+            q[1] = -q[1];
+            q[2] = -q[2];
+        }
+        const float qLength = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        const float unit[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+        uint32_t* sw = shape + size_t{j} * 4;
+        sw[0] = encodeQuaternion(qLength > 1e-8f ? q : unit);
+        const float base[3] = {colourOf(field(i, e->dc0)), colourOf(field(i, e->dc1)), colourOf(field(i, e->dc2))};
+        sw[1] = packHalves(halfSafe(ls[0]), halfSafe(ls[1]));
+        sw[2] = packHalves(halfSafe(ls[2]), halfSafe(base[0]));
+        sw[3] = packHalves(halfSafe(base[1]), halfSafe(base[2]));
+        uint32_t* row = sh + size_t{j} * shWords;
+        std::fill(row, row + shWords, 0u);
+        uint32_t n = 0;
+        for (uint32_t basis = 0; basis < keep; ++basis)
+            for (uint32_t colour = 0; colour < 3; ++colour, ++n) {
+                const uint32_t f = e->rest_colour_outer != 0 ? e->rest_base + colour * e->rest_per_colour + basis
+                                                             : e->rest_base + basis * 3 + colour;
+                float v = unitOf(field(i, f), e->rest_mode);
+                if (e->flip_yz != 0) v = v * kSigns[std::min(basis, 14u)];
+                row[n / 2] |= (floatToHalf(halfSafe(v)) & 0xFFFFu) << ((n & 1u) * 16);
+            }
+        ++j;
+    }
+    *kept = j;
+    return LRT_OK;
+}
+
 int ora_pack_points(const float* raw, uint32_t count, uint32_t colourKind, float detail, float* positions,
                     uint32_t* colours, uint32_t* kept) {
     // shaders/lrt/scene/points_validate.slang:19-28 (which points stay),

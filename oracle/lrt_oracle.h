@@ -93,6 +93,11 @@ int ora_reference_render_composite(const lrt_projection* projection, const lrt_s
                                    const lrt_render_settings* settings, float* colour, float* depth,
                                    uint32_t* overflow, uint32_t threads);
 
+/* Raw splat records of any encoding to the packed layout (as
+ * lrt_rast_decode_splats does on the device), host pointers. */
+int ora_decode_splats(const float* raw, uint32_t count, const lrt_splat_encoding* encoding, uint32_t keep,
+                      float* positions, uint32_t* shape, uint32_t* sh, uint32_t* kept);
+
 /* Raw point records (x y z r g b) to positions/colours, as lrt_pack_points. */
 int ora_pack_points(const float* raw, uint32_t count, uint32_t colour_kind, float detail, float* positions,
                     uint32_t* colours, uint32_t* kept);

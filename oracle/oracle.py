@@ -75,6 +75,8 @@ def load() -> C.CDLL:
     lib.ora_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_uint32)]
     lib.ora_random_points.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p]
+    lib.ora_decode_splats.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_abi.SplatEncoding), C.c_uint32, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
     lib.ora_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint64)]
@@ -139,6 +141,22 @@ def pack(raw: np.ndarray, file_per_colour: int, keep: int) -> HostCloud:
     kept = C.c_uint32()
     _check(load().ora_pack_splats(raw.ctypes.data, n, fpr, file_per_colour, keep, pos.ctypes.data,
                                   shape.ctypes.data, sh.ctypes.data, C.byref(kept)), "pack")
+    k = kept.value
+    return HostCloud(pos[:k].copy(), shape[:k].copy(), sh[:k].copy(), keep)
+
+
+def decode_splats(raw: np.ndarray, encoding: _abi.SplatEncoding, keep: int) -> HostCloud:
+    """Raw records of any encoding to the packed layout (the restatement of
+    the device decode)."""
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    n = raw.shape[0]
+    words = max((keep * 3 + 1) // 2, 1)
+    pos = np.empty((n, 4), np.float32)
+    shape = np.empty((n, 4), np.uint32)
+    sh = np.empty((n, words), np.uint32)
+    kept = C.c_uint32()
+    _check(load().ora_decode_splats(raw.ctypes.data, n, C.byref(encoding), keep, pos.ctypes.data, shape.ctypes.data,
+                                    sh.ctypes.data, C.byref(kept)), "decode_splats")
     k = kept.value
     return HostCloud(pos[:k].copy(), shape[:k].copy(), sh[:k].copy(), keep)
 
