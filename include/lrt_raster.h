@@ -449,6 +449,36 @@ int lrt_rast_decode_splats(lrt_rast* rast, const void* raw, uint32_t count, cons
 int lrt_rast_decode_points(lrt_rast* rast, const void* raw, uint32_t count, uint32_t colour_kind, float detail,
                            void* positions, void* colours, uint32_t* kept, void* stream);
 
+/* ImageDifference and HdrDifference (ReferenceRenderer.h:50-64). */
+typedef struct lrt_image_difference {
+    uint64_t pixels;
+    uint32_t p99;        /* 99th percentile of the per-pixel largest code difference */
+    uint32_t max;
+    uint64_t over2;      /* pixels differing by more than 2 code values */
+} lrt_image_difference;
+
+typedef struct lrt_hdr_difference {
+    uint64_t pixels;
+    double rel_mse;      /* mean over pixels of the channel mean (a - b)^2 / (b^2 + 1e-2) */
+    double p99_relative; /* 99th percentile of max_c |a - b| / max(|b|, 1e-3), to 9% */
+    double max_relative;
+} lrt_hdr_difference;
+
+/* compareImages (ReferenceRenderer.cpp:248-297) on the device: two float4
+ * images (device pointers, linear premultiplied) in 8-bit sRGB code values.
+ * `histogram` (may be NULL) receives the 256 bins on the host. */
+int lrt_rast_compare_images(lrt_rast* rast, const void* a, const void* b, uint32_t width, uint32_t height,
+                            lrt_image_difference* out, uint32_t* histogram, void* stream);
+
+/* compareHdr (ReferenceRenderer.cpp:299-362) on the device. */
+int lrt_rast_compare_hdr(lrt_rast* rast, const void* a, const void* b, uint32_t width, uint32_t height,
+                         lrt_hdr_difference* out, void* stream);
+
+/* countDifferent (ReferenceRenderer.cpp:364-396): differing entries of two
+ * uint32 device buffers. */
+int lrt_rast_count_different(lrt_rast* rast, const void* a, const void* b, uint32_t count, uint64_t* out,
+                             void* stream);
+
 /* Raw point records (x y z r g b, 6 floats) to the GpuPoints layout above, on
  * the host (the upload half of CloudLoader for points: points_validate.slang
  * and points_decode.slang). colour_kind: 0 none (white), 1 sRGB bytes in

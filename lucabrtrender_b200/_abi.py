@@ -40,7 +40,8 @@ EXPORTS = (
     "lrt_pack_splats", "lrt_math_eval", "lrt_prefix_sum_noalloc", "lrt_rast_train_forward",
     "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
     "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points", "lrt_splat_encoding_ply",
-    "lrt_rast_decode_splats", "lrt_rast_decode_points",
+    "lrt_rast_decode_splats", "lrt_rast_decode_points", "lrt_rast_compare_images", "lrt_rast_compare_hdr",
+    "lrt_rast_count_different",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -119,6 +120,15 @@ class SplatEncoding(C.Structure):
         "rot_z", "dc0", "dc1", "dc2", "rest_base", "rest_per_colour", "rest_colour_outer", "opacity_mode",
         "scale_mode", "colour_mode", "rotation_mode", "rest_mode")] + [("position_scale", C.c_float),
                                                                         ("flip_yz", C.c_uint32)]
+
+
+class ImageDifferenceStruct(C.Structure):
+    _fields_ = [("pixels", C.c_uint64), ("p99", C.c_uint32), ("max", C.c_uint32), ("over2", C.c_uint64)]
+
+
+class HdrDifferenceStruct(C.Structure):
+    _fields_ = [("pixels", C.c_uint64), ("rel_mse", C.c_double), ("p99_relative", C.c_double),
+                ("max_relative", C.c_double)]
 
 
 class RenderSettingsStruct(C.Structure):
@@ -212,6 +222,12 @@ def load() -> C.CDLL:
     lib.lrt_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_uint32)]
     lib.lrt_splat_encoding_ply.argtypes = [C.c_uint32, C.POINTER(SplatEncoding)]
+    lib.lrt_rast_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                            C.POINTER(ImageDifferenceStruct), C.c_void_p, C.c_void_p]
+    lib.lrt_rast_compare_hdr.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                         C.POINTER(HdrDifferenceStruct), C.c_void_p]
+    lib.lrt_rast_count_different.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                             C.POINTER(C.c_uint64), C.c_void_p]
     lib.lrt_rast_decode_splats.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(SplatEncoding), C.c_uint32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
     lib.lrt_rast_decode_points.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p,

@@ -101,4 +101,12 @@ cudaError_t launch_decode_points(const float* raw, uint32_t count, uint32_t colo
                                  float4* positions, uint32_t* colours, void* scratch, uint32_t* err,
                                  cudaStream_t stream);
 
+// Parity metrics (compare.cu).
+cudaError_t launch_compare_images(const float4* a, const float4* b, uint32_t pixels, uint32_t* histogram,
+                                  cudaStream_t stream);
+cudaError_t launch_compare_hdr(const float4* a, const float4* b, uint32_t width, uint32_t height, uint32_t* histogram,
+                               float* rowError, float* total, cudaStream_t stream);
+cudaError_t launch_count_different(const uint32_t* a, const uint32_t* b, uint32_t count, uint64_t* total,
+                                   cudaStream_t stream);
+
 }  // namespace lrt

@@ -45,6 +45,9 @@ struct lrt_rast {
     lrt_debug_view debug{};
     // Training: what the backward pass needs from its forward.
     DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
+    DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
+    void* metricHost = nullptr;                          // pinned readback of the metrics
+    size_t metricHostBytes = 0;
     bool trainReady = false;
     bool trainPending = false;   // the forward's counts and status are not read yet
     cudaStream_t pendingStream = nullptr;
@@ -125,6 +128,16 @@ cudaError_t ensure(DeviceBuffer& b, size_t bytes) {
     b.bytes = 0;
     cudaError_t e = cudaMalloc(&b.ptr, std::max<size_t>(bytes, 16));
     if (e == cudaSuccess) b.bytes = std::max<size_t>(bytes, 16);
+    return e;
+}
+
+cudaError_t ensure_host(lrt_rast* r, size_t bytes) {
+    if (r->metricHostBytes >= bytes && r->metricHost != nullptr) return cudaSuccess;
+    if (r->metricHost != nullptr) cudaFreeHost(r->metricHost);
+    r->metricHost = nullptr;
+    r->metricHostBytes = 0;
+    cudaError_t e = cudaMallocHost(&r->metricHost, bytes);
+    if (e == cudaSuccess) r->metricHostBytes = bytes;
     return e;
 }
 
@@ -237,11 +250,12 @@ void lrt_rast_destroy(lrt_rast* r) {
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
-                            &r->pixLast, &r->partials})
+                            &r->pixLast, &r->partials, &r->metricScratch})
         release(*b);
     if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
     if (r->ringHost != nullptr) cudaFreeHost(r->ringHost);
+    if (r->metricHost != nullptr) cudaFreeHost(r->metricHost);
     for (auto& e : r->ev)
         if (e != nullptr) cudaEventDestroy(e);
     for (auto& e : r->ringEvent)
@@ -751,6 +765,128 @@ int lrt_rast_render_composite(lrt_rast* r, const lrt_projection* pr, const lrt_s
     }
     const bool composite = under != nullptr || pointCount > 0;
     return render_frame(r, pr, clouds, s, targets, stats, streamPtr, false, frameStart, false, under, composite);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The percentiles the reference takes from a 256-bin histogram
+// (ReferenceRenderer.cpp:276-296): the bin where the running count reaches
+// pixels - pixels / 100, and the highest non-empty bin.
+void histogram_stats(const uint32_t* h, uint64_t& pixels, uint32_t& p99, uint32_t& maxBin, uint64_t* over2) {
+    pixels = 0;
+    maxBin = 0;
+    uint64_t o2 = 0;
+    for (uint32_t k = 0; k < 256; ++k) {
+        pixels += h[k];
+        if (h[k] > 0) maxBin = k;
+        if (k > 2) o2 += h[k];
+    }
+    if (over2 != nullptr) *over2 = o2;
+    const uint64_t at = pixels - pixels / 100;
+    uint64_t running = 0;
+    p99 = 0;
+    for (uint32_t k = 0; k < 256; ++k) {
+        running += h[k];
+        if (running >= at) {
+            p99 = k;
+            break;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrt_rast_compare_images(lrt_rast* r, const void* a, const void* b, uint32_t width, uint32_t height,
+                            lrt_image_difference* out, uint32_t* histogram, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (out == nullptr || (uint64_t{width} * height > 0 && (a == nullptr || b == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    if (uint64_t{width} * height > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pixels");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
+    LRT_CUDA(r, ensure(r->metricScratch, 256 * 4 + 16), "metric scratch");
+    uint32_t* bins = static_cast<uint32_t*>(r->metricScratch.ptr);
+    LRT_CUDA(r, cudaMemsetAsync(bins, 0, 256 * 4, stream), "histogram");
+    LRT_CUDA(r,
+             lrt::launch_compare_images(static_cast<const float4*>(a), static_cast<const float4*>(b), width * height,
+                                        bins, stream),
+             "compare");
+    LRT_CUDA(r, ensure_host(r, 256 * 4 + 16), "metric readback");
+    LRT_CUDA(r, cudaMemcpyAsync(r->metricHost, bins, 256 * 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "compare");
+    const uint32_t* h = static_cast<const uint32_t*>(r->metricHost);
+    *out = lrt_image_difference{};
+    histogram_stats(h, out->pixels, out->p99, out->max, &out->over2);
+    if (histogram != nullptr) std::memcpy(histogram, h, 256 * 4);
+    return LRT_OK;
+}
+
+int lrt_rast_compare_hdr(lrt_rast* r, const void* a, const void* b, uint32_t width, uint32_t height,
+                         lrt_hdr_difference* out, void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (out == nullptr || (uint64_t{width} * height > 0 && (a == nullptr || b == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    if (uint64_t{width} * height > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 pixels");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
+    const size_t bytes = 256 * 4 + 16 + size_t{height} * 4;
+    LRT_CUDA(r, ensure(r->metricScratch, bytes), "metric scratch");
+    uint32_t* bins = static_cast<uint32_t*>(r->metricScratch.ptr);
+    float* total = reinterpret_cast<float*>(bins + 256);
+    float* rows = reinterpret_cast<float*>(bins + 260);
+    LRT_CUDA(r, cudaMemsetAsync(bins, 0, 256 * 4 + 16, stream), "histogram");
+    LRT_CUDA(r,
+             lrt::launch_compare_hdr(static_cast<const float4*>(a), static_cast<const float4*>(b), width, height, bins,
+                                     rows, total, stream),
+             "compare");
+    LRT_CUDA(r, ensure_host(r, 256 * 4 + 16), "metric readback");
+    LRT_CUDA(r, cudaMemcpyAsync(r->metricHost, bins, 256 * 4 + 4, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "compare");
+    const uint32_t* h = static_cast<const uint32_t*>(r->metricHost);
+    float error = 0.0f;
+    std::memcpy(&error, h + 256, 4);
+    uint32_t p99 = 0, maxBin = 0;
+    *out = lrt_hdr_difference{};
+    histogram_stats(h, out->pixels, p99, maxBin, nullptr);
+    // Bin k > 0 holds relative differences in [2^((k-1)/8 - 16), 2^(k/8 - 16)) (ReferenceRenderer.cpp:339-360).
+    const auto upper = [](uint32_t bin) { return bin == 0 ? 0.0 : std::pow(2.0, bin / 8.0 - 16.0); };
+    out->max_relative = out->pixels > 0 ? upper(maxBin) : 0.0;
+    out->p99_relative = out->pixels > 0 ? upper(p99) : 0.0;
+    out->rel_mse = out->pixels > 0 ? static_cast<double>(error) / static_cast<double>(out->pixels) : 0.0;
+    return LRT_OK;
+}
+
+int lrt_rast_count_different(lrt_rast* r, const void* a, const void* b, uint32_t count, uint64_t* out,
+                             void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (out == nullptr || (count > 0 && (a == nullptr || b == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    *out = 0;
+    if (count == 0) return LRT_OK;
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->frameDoneSet) LRT_CUDA(r, cudaStreamWaitEvent(stream, r->frameDone, 0), "frame order");
+    LRT_CUDA(r, ensure(r->metricScratch, 256 * 4 + 16), "metric scratch");
+    uint64_t* total = static_cast<uint64_t*>(r->metricScratch.ptr);
+    LRT_CUDA(r, cudaMemsetAsync(total, 0, 8, stream), "count");
+    LRT_CUDA(r,
+             lrt::launch_count_different(static_cast<const uint32_t*>(a), static_cast<const uint32_t*>(b), count,
+                                         total, stream),
+             "count");
+    LRT_CUDA(r, ensure_host(r, 256 * 4 + 16), "metric readback");
+    LRT_CUDA(r, cudaMemcpyAsync(r->metricHost, total, 8, cudaMemcpyDeviceToHost, stream), "readback");
+    LRT_CUDA(r, cudaStreamSynchronize(stream), "count");
+    std::memcpy(out, r->metricHost, 8);
+    return LRT_OK;
 }
 
 int lrt_rast_decode_splats(lrt_rast* r, const void* raw, uint32_t count, const lrt_splat_encoding* e,

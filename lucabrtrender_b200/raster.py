@@ -149,6 +149,24 @@ class FrameStats:
                 f"emit {self.emit_ms:.2f}, tile sort+ranges {self.tile_sort_ms:.2f}, blend {self.blend_ms:.2f}")
 
 
+@dataclass
+class ImageDifference:
+    """ImageDifference (ReferenceRenderer.h:50-55), in 8-bit sRGB code values."""
+    pixels: int
+    p99: int
+    max: int
+    over2: int
+
+
+@dataclass
+class HdrDifference:
+    """HdrDifference (ReferenceRenderer.h:59-64)."""
+    pixels: int
+    rel_mse: float
+    p99_relative: float
+    max_relative: float
+
+
 class RenderTargets:
     """RenderTargets (TileRasterizer.h:128-134): colour float4 premultiplied
     linear [H, W, 4] and depth [H, W], bottom row first, on the device.
@@ -358,6 +376,31 @@ class TileRasterizer:
                                                        _stream_ptr(stream)))
         k = kept.value
         return GpuPoints(pos[:k], col[:k])
+
+    def compare_images(self, a: torch.Tensor, b: torch.Tensor, stream=None):
+        """compareImages on the device: (ImageDifference fields, histogram)."""
+        h, w = a.shape[:2]
+        a, b = a.contiguous(), b.contiguous()
+        out = _abi.ImageDifferenceStruct()
+        hist = np.zeros(256, np.uint32)
+        self._check(_abi.load().lrt_rast_compare_images(self._handle, a.data_ptr(), b.data_ptr(), w, h, C.byref(out),
+                                                        hist.ctypes.data, _stream_ptr(stream)))
+        return ImageDifference(out.pixels, out.p99, out.max, out.over2), hist
+
+    def compare_hdr(self, a: torch.Tensor, b: torch.Tensor, stream=None) -> "HdrDifference":
+        h, w = a.shape[:2]
+        a, b = a.contiguous(), b.contiguous()
+        out = _abi.HdrDifferenceStruct()
+        self._check(_abi.load().lrt_rast_compare_hdr(self._handle, a.data_ptr(), b.data_ptr(), w, h, C.byref(out),
+                                                     _stream_ptr(stream)))
+        return HdrDifference(out.pixels, out.rel_mse, out.p99_relative, out.max_relative)
+
+    def count_different(self, a: torch.Tensor, b: torch.Tensor, stream=None) -> int:
+        a, b = a.contiguous(), b.contiguous()
+        n = C.c_uint64()
+        self._check(_abi.load().lrt_rast_count_different(self._handle, a.data_ptr(), b.data_ptr(), a.numel(),
+                                                         C.byref(n), _stream_ptr(stream)))
+        return int(n.value)
 
     def debug_view(self) -> _abi.DebugView:
         v = _abi.DebugView()

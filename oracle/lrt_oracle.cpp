@@ -1520,6 +1520,50 @@ int ora_compare_images(const float* a, const float* b, uint32_t width, uint32_t 
     return LRT_OK;
 }
 
+int ora_compare_hdr(const float* a, const float* b, uint32_t width, uint32_t height, uint32_t* histogram,
+                    float* error) {
+    // shaders/lrt/reference/image_compare_hdr.slang:20-60 and floatSum
+    // (:82-100): bins eight to an octave from 2^-16 (log2 taken through this
+    // restatement's log, as the device takes it), and the relative squared
+    // error summed per row, then over rows, with compensated addition.
+    uint32_t hist[256] = {};
+    auto kahan = [](float& sum, float& carry, float term) {
+        const float t = sum + term;
+        carry += std::fabs(sum) >= std::fabs(term) ? (sum - t) + term : (term - t) + sum;
+        sum = t;
+    };
+    float total = 0.0f, totalCarry = 0.0f;
+    for (uint32_t y = 0; y < height; ++y) {
+        float sum = 0.0f, carry = 0.0f;
+        for (uint32_t x = 0; x < width; ++x) {
+            const float* pa = a + (size_t{y} * width + x) * 4;
+            const float* pb = b + (size_t{y} * width + x) * 4;
+            float worst = 0.0f, squared = 0.0f;
+            for (int c = 0; c < 4; ++c) {
+                const float d = std::fabs(pa[c] - pb[c]);
+                worst = std::fmax(worst, d / std::fmax(std::fabs(pb[c]), 1e-3f));
+                squared += d * d / (pb[c] * pb[c] + 1e-2f);
+            }
+            const uint32_t bin =
+                worst <= 0.0f ? 0u
+                              : static_cast<uint32_t>(clampf(std::floor((logImpl(worst) / kLn2Hi + 16.0f) * 8.0f) + 1.0f,
+                                                             1.0f, 255.0f));
+            hist[bin] += 1;
+            kahan(sum, carry, squared * 0.25f);
+        }
+        kahan(total, totalCarry, sum + carry);
+    }
+    if (histogram) std::memcpy(histogram, hist, sizeof(hist));
+    if (error) *error = total + totalCarry;
+    return LRT_OK;
+}
+
+uint64_t ora_count_different(const uint32_t* a, const uint32_t* b, uint32_t count) {
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < count; ++i) n += a[i] != b[i] ? 1 : 0;
+    return n;
+}
+
 int ora_random_cloud(uint32_t count, uint64_t seed, float minSize, float maxSize, float minOpacity,
                      float maxOpacity, float* raw) {
     // tests/render/SplatFixtures.h:16-85 (CloudBuilder::add + Lcg + randomCloud).

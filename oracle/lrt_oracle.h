@@ -116,6 +116,11 @@ int ora_compare_images(const float* a, const float* b, uint32_t width, uint32_t 
                        uint32_t* histogram256, uint32_t* p99, uint32_t* max, uint64_t* over2,
                        uint64_t* pixels);
 
+/* compareHdr's histogram and relative squared error (the device's order). */
+int ora_compare_hdr(const float* a, const float* b, uint32_t width, uint32_t height, uint32_t* histogram256,
+                    float* error);
+uint64_t ora_count_different(const uint32_t* a, const uint32_t* b, uint32_t count);
+
 /* The reference test fixture's randomCloud (tests/render/SplatFixtures.h:48-85):
  * `count` degree-1 raw records of 23 floats. */
 int ora_random_cloud(uint32_t count, uint64_t seed, float min_size, float max_size,

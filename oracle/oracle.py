@@ -75,6 +75,10 @@ def load() -> C.CDLL:
     lib.ora_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_uint32)]
     lib.ora_random_points.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p]
+    lib.ora_compare_hdr.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.POINTER(C.c_float)]
+    lib.ora_count_different.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.ora_count_different.restype = C.c_uint64
     lib.ora_decode_splats.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_abi.SplatEncoding), C.c_uint32, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
     lib.ora_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
@@ -326,6 +330,23 @@ def compare_images(a: np.ndarray, b: np.ndarray) -> ImageDifference:
     _check(load().ora_compare_images(a.ctypes.data, b.ctypes.data, w, h, hist.ctypes.data, C.byref(p99),
                                      C.byref(mx), C.byref(over2), C.byref(pixels)), "compare_images")
     return ImageDifference(p99.value, mx.value, over2.value, pixels.value, hist)
+
+
+def compare_hdr(a: np.ndarray, b: np.ndarray):
+    """(histogram [256], summed relative squared error) of compareHdr."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    h, w = a.shape[:2]
+    hist = np.zeros(256, np.uint32)
+    err = C.c_float()
+    _check(load().ora_compare_hdr(a.ctypes.data, b.ctypes.data, w, h, hist.ctypes.data, C.byref(err)), "compare_hdr")
+    return hist, err.value
+
+
+def count_different(a: np.ndarray, b: np.ndarray) -> int:
+    a = np.ascontiguousarray(a, np.uint32)
+    b = np.ascontiguousarray(b, np.uint32)
+    return int(load().ora_count_different(a.ctypes.data, b.ctypes.data, a.size))
 
 
 def math_eval(fn: int, x: np.ndarray) -> np.ndarray:
