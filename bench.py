@@ -246,6 +246,57 @@ def run_batch(L, torch, dev, rank, raster, args, clocks) -> dict:
             "blend_blocks_per_sm": int(stats.blend_blocks_per_sm), "graph_replayed": int(stats.graph_replayed)}
 
 
+def time_device(torch, stream, fn, reps: int) -> float:
+    """Mean ms of `fn` over `reps` calls, CUDA events on `stream`, after one warm call."""
+    fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def run_next_rows(L, torch, dev, raster, packed, cloud, peak) -> dict:
+    """The rows around the hot path: device decode of the benchmark cloud's
+    raw records, the composite frame (the same splats with a million point
+    discs, and over an under layer), and the on-device image metric."""
+    stream = torch.cuda.current_stream(dev)
+    raw = L.synthetic_records(SPLATS, SEED)
+    raw_dev = torch.from_numpy(raw).to(dev)
+    enc = L.ply_encoding(15)
+    decode_ms = time_device(torch, stream, lambda: raster.decode_splats(raw_dev, enc, 15, stream), 5)
+    decode_bytes = raw.nbytes + SPLATS * (16 + 16 + 4 * 23)
+    rng = np.random.default_rng(SEED)
+    pts_raw = np.concatenate([rng.normal(0.0, 1.0, (SPLATS, 3)), rng.uniform(0.0, 1.0, (SPLATS, 3))], 1)
+    points = raster.decode_points(torch.from_numpy(pts_raw.astype(np.float32)).to(dev), 2, 1.0, stream)
+    settings = L.RenderSettings(width=WIDTH, height=HEIGHT)
+    cam = orbit_camera(L, 0)
+    inst = [L.SplatInstance(cloud)]
+    pinst = [L.PointInstance(points, np.eye(4), L.PointStyle(size_mode=0, size=0.004))]
+    layer, out = L.RenderTargets(WIDTH, HEIGHT, device=dev), L.RenderTargets(WIDTH, HEIGHT, device=dev)
+    raster.render(cam, [], settings, layer, stream, points=pinst)
+    mixed_ms = time_device(torch, stream, lambda: raster.render(cam, inst, settings, out, stream, points=pinst), 5)
+    under_ms = time_device(torch, stream, lambda: raster.render(cam, inst, settings, out, stream, under=layer), 5)
+    plain_ms = time_device(torch, stream, lambda: raster.render(cam, inst, settings, out, stream), 5)
+    cmp_ms = time_device(torch, stream, lambda: raster.compare_images(out.colour, layer.colour, stream), 5)
+    cmp_bytes = 2 * WIDTH * HEIGHT * 16
+    return {
+        "decode": {"workload": "1M raw 3DGS PLY records (236 B) to the packed layout, on the device",
+                   "ms": round(decode_ms, 4), "gbs": round(decode_bytes / (decode_ms * 1e-3) / 1e9, 1),
+                   "frac_of_hbm": round(decode_bytes / (decode_ms * 1e-3) / 1e9 / peak, 4)},
+        "composite": {"workload": "frame 0 of the orbit, 1M splats: alone, with 1M point discs (0.004 world units), "
+                                  "and over an under layer of those discs; 1920x1080",
+                      "plain_ms": round(plain_ms, 4), "with_discs_ms": round(mixed_ms, 4),
+                      "over_layer_ms": round(under_ms, 4)},
+        "compare_images": {"workload": "two 1920x1080 float4 images, 8-bit code histogram on the device",
+                           "ms": round(cmp_ms, 4), "gbs": round(cmp_bytes / (cmp_ms * 1e-3) / 1e9, 1)},
+    }
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -378,7 +429,7 @@ def run_ours(args) -> None:
                 v.grad = None
             colour, _ = L.rasterize(params["means"], params["log_scales"], params["quats"], params["logits"],
                                     params["sh"], projections[(k + rank * 7) % FRAMES], train_settings, raster)
-            loss = torch.abs(colour[..., :3] - target).mean()
+            loss = L.l1_loss(colour, target, raster)
             loss.backward()
             return loss
 
@@ -418,8 +469,14 @@ def run_ours(args) -> None:
                                          for k in ("project_ms", "tile_sort_ms", "blend_ms")},
                    "backward_blend_ms": round(float(np.mean(bwd_blend)), 4),
                    "backward_reduce_and_projection_ms": round(float(np.mean(bwd_proj)), 4),
-                   "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels",
+                   "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels "
+                           "(lucabrtrender_b200.l1_loss: one kernel each way)",
                    "params": "means, log-scales, quaternions, opacity logits, 48 SH (fp16 storage, fp32 gradients)"}
+
+    # --- the rows around the hot path ---
+    next_rows = None
+    if not args.no_next:
+        next_rows = run_next_rows(L, torch, dev, raster, packed, cloud, measured_peaks()[0])
 
     # --- many views: one batched call against sequential renders ---
     batch = None
@@ -484,6 +541,7 @@ def run_ours(args) -> None:
             "cpu_baseline": cpu,
             "fwd_bwd": fwd_bwd,
             "batch": batch,
+            "next_rows": next_rows,
         }
         print(json.dumps(line), flush=True)
     raster.close()
@@ -502,6 +560,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-backward", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-next", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

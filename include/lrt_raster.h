@@ -479,6 +479,18 @@ int lrt_rast_compare_hdr(lrt_rast* rast, const void* a, const void* b, uint32_t 
 int lrt_rast_count_different(lrt_rast* rast, const void* a, const void* b, uint32_t count, uint64_t* out,
                              void* stream);
 
+/* The photometric L1 loss of a training step (no reference counterpart):
+ * mean |colour.rgb - target| over `pixels` pixels and 3 channels, colour a
+ * float4 image and target a float3 image (device pointers), written to the
+ * device float *loss, summed in a fixed order. Enqueued only. */
+int lrt_rast_l1_loss(lrt_rast* rast, const void* colour, const void* target, uint32_t pixels, void* loss,
+                     void* stream);
+
+/* Its gradient: grad_colour (float4 per pixel) = sign(colour.rgb - target)
+ * / (3 pixels) scaled by *grad_loss (a device float; NULL: 1), alpha 0. */
+int lrt_l1_loss_grad(const void* colour, const void* target, uint32_t pixels, const void* grad_loss,
+                     void* grad_colour, void* stream);
+
 /* Raw point records (x y z r g b, 6 floats) to the GpuPoints layout above, on
  * the host (the upload half of CloudLoader for points: points_validate.slang
  * and points_decode.slang). colour_kind: 0 none (white), 1 sRGB bytes in

@@ -41,7 +41,7 @@ EXPORTS = (
     "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
     "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points", "lrt_splat_encoding_ply",
     "lrt_rast_decode_splats", "lrt_rast_decode_points", "lrt_rast_compare_images", "lrt_rast_compare_hdr",
-    "lrt_rast_count_different",
+    "lrt_rast_count_different", "lrt_rast_l1_loss", "lrt_l1_loss_grad",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -222,6 +222,8 @@ def load() -> C.CDLL:
     lib.lrt_pack_points.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_uint32)]
     lib.lrt_splat_encoding_ply.argtypes = [C.c_uint32, C.POINTER(SplatEncoding)]
+    lib.lrt_rast_l1_loss.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    lib.lrt_l1_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lrt_rast_compare_images.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                             C.POINTER(ImageDifferenceStruct), C.c_void_p, C.c_void_p]
     lib.lrt_rast_compare_hdr.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,

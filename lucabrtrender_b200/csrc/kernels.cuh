@@ -109,4 +109,11 @@ cudaError_t launch_compare_hdr(const float4* a, const float4* b, uint32_t width,
 cudaError_t launch_count_different(const uint32_t* a, const uint32_t* b, uint32_t count, uint64_t* total,
                                    cudaStream_t stream);
 
+// The L1 training loss (loss.cu).
+size_t l1_scratch_bytes();
+cudaError_t launch_l1_loss(const float4* colour, const float* target, uint32_t pixels, float* scratch, float* loss,
+                           cudaStream_t stream);
+cudaError_t launch_l1_grad(const float4* colour, const float* target, uint32_t pixels, const float* gradLoss,
+                           float4* gradColour, cudaStream_t stream);
+
 }  // namespace lrt

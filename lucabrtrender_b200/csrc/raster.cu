@@ -46,6 +46,7 @@ struct lrt_rast {
     // Training: what the backward pass needs from its forward.
     DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
     DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
+    DeviceBuffer lossScratch;                            // the L1 loss's per-block sums
     void* metricHost = nullptr;                          // pinned readback of the metrics
     size_t metricHostBytes = 0;
     bool trainReady = false;
@@ -250,7 +251,7 @@ void lrt_rast_destroy(lrt_rast* r) {
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
-                            &r->pixLast, &r->partials, &r->metricScratch})
+                            &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch})
         release(*b);
     if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
@@ -799,6 +800,31 @@ void histogram_stats(const uint32_t* h, uint64_t& pixels, uint32_t& p99, uint32_
 }  // namespace
 
 extern "C" {
+
+int lrt_rast_l1_loss(lrt_rast* r, const void* colour, const void* target, uint32_t pixels, void* loss,
+                     void* streamPtr) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    if (loss == nullptr || (pixels > 0 && (colour == nullptr || target == nullptr)))
+        return fail(r, LRT_INVALID_ARGUMENT, "null argument");
+    DeviceScope scope(r->device);
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    LRT_CUDA(r, ensure(r->lossScratch, lrt::l1_scratch_bytes()), "loss scratch");
+    LRT_CUDA(r,
+             lrt::launch_l1_loss(static_cast<const float4*>(colour), static_cast<const float*>(target), pixels,
+                                 static_cast<float*>(r->lossScratch.ptr), static_cast<float*>(loss), stream),
+             "loss");
+    return LRT_OK;
+}
+
+int lrt_l1_loss_grad(const void* colour, const void* target, uint32_t pixels, const void* gradLoss, void* gradColour,
+                     void* streamPtr) {
+    if (pixels > 0 && (colour == nullptr || target == nullptr || gradColour == nullptr)) return LRT_INVALID_ARGUMENT;
+    const cudaError_t e = lrt::launch_l1_grad(static_cast<const float4*>(colour), static_cast<const float*>(target),
+                                              pixels, static_cast<const float*>(gradLoss),
+                                              static_cast<float4*>(gradColour), static_cast<cudaStream_t>(streamPtr));
+    return e == cudaSuccess ? LRT_OK : LRT_DEVICE_FAILURE;
+}
 
 int lrt_rast_compare_images(lrt_rast* r, const void* a, const void* b, uint32_t width, uint32_t height,
                             lrt_image_difference* out, uint32_t* histogram, void* streamPtr) {

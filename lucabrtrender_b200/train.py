@@ -70,6 +70,37 @@ class _Rasterize(torch.autograd.Function):
         return g[0], g[1], g[2], g[3], g[4], None, None, None, None
 
 
+class _L1Loss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, colour, target, raster: TileRasterizer):
+        colour = colour.contiguous().float()
+        target = target.contiguous().float()
+        if colour.shape[:-1] != target.shape[:-1] or colour.shape[-1] != 4 or target.shape[-1] != 3:
+            raise ValueError("colour must be [..., 4] and target [..., 3] over the same pixels")
+        pixels = colour.numel() // 4
+        loss = torch.empty((), dtype=torch.float32, device=colour.device)
+        raster._check(_abi.load().lrt_rast_l1_loss(raster._handle, colour.data_ptr(), target.data_ptr(), pixels,
+                                                   loss.data_ptr(), _stream_ptr(None)))
+        ctx.save_for_backward(colour, target)
+        return loss
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        colour, target = ctx.saved_tensors
+        grad_loss = grad_loss.contiguous().float()
+        grad = torch.empty_like(colour)
+        code = _abi.load().lrt_l1_loss_grad(colour.data_ptr(), target.data_ptr(), colour.numel() // 4,
+                                            grad_loss.data_ptr(), grad.data_ptr(), _stream_ptr(None))
+        _abi.check(code, "l1_loss backward")
+        return grad, None, None
+
+
+def l1_loss(colour: torch.Tensor, target: torch.Tensor, raster: TileRasterizer) -> torch.Tensor:
+    """mean |colour.rgb - target| (colour [..., 4] from rasterize, target
+    [..., 3]), one kernel each way, summed in a fixed order."""
+    return _L1Loss.apply(colour, target, raster)
+
+
 def rasterize(means, log_scales, quats, opacity_logits, sh, view: Camera | Projection, settings: RenderSettings,
               raster: TileRasterizer, sort_values: bool = False):
     """Render the differentiable cloud; returns (colour [H,W,4], depth [H,W])."""

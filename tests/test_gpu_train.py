@@ -173,3 +173,17 @@ def test_both_emit_index_layouts_give_the_same_gradients_bit_for_bit(rasterizer)
     assert la == lb
     for name in a:
         assert np.array_equal(a[name].view(np.uint32), b[name].view(np.uint32)), name
+
+
+def test_the_l1_loss_equals_torch_and_its_gradient_is_the_same(rasterizer):
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    colour = torch.rand((181, 243, 4), generator=gen, device="cuda", requires_grad=True)
+    target = torch.rand((181, 243, 3), generator=gen, device="cuda")
+    loss = L.l1_loss(colour, target, rasterizer)
+    (2.5 * loss).backward()
+    ours = colour.grad.clone()
+    colour.grad = None
+    want = torch.abs(colour[..., :3] - target).mean()
+    (2.5 * want).backward()
+    assert abs(float(loss.detach()) - float(want.detach().double())) <= 2e-6 * float(want.detach())
+    assert torch.equal(ours, colour.grad)
