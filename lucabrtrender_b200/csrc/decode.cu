@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(kDecodeThreads)
 decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_encoding e, uint32_t keep,
                      uint32_t shWords, float4* __restrict__ positions, uint4* __restrict__ shape,
                      uint32_t* __restrict__ sh, uint64_t* __restrict__ status, uint32_t* __restrict__ ticket,
-                     uint32_t* __restrict__ total, uint32_t* __restrict__ err) {
+                     uint32_t* __restrict__ total, uint32_t* __restrict__ err, uint32_t stage) {
+    extern __shared__ __align__(16) float sRaw[];
     __shared__ uint32_t sPart, sBase;
     __shared__ uint32_t sWarp[kDecodeThreads / 32];
     if (threadIdx.x == 0) sPart = atomicAdd(ticket, 1u);
@@ -233,17 +234,36 @@ decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_en
     const uint32_t i = part * kDecodeThreads + threadIdx.x;
     const bool inRange = i < count;
     const uint32_t s = e.floats_per_record;
+    // With `stage`, the block's records (contiguous in memory) are first
+    // copied to shared memory with 16-byte loads, consecutive threads taking
+    // consecutive vectors, and each thread then reads its record's fields
+    // there rather than 32 scattered lines a warp.
+    const float* src = raw;
+    uint32_t at = i;
+    if (stage != 0) {
+        const uint32_t first = part * kDecodeThreads;
+        const uint32_t n = min(kDecodeThreads, count - min(first, count));
+        const size_t floats = static_cast<size_t>(n) * s;
+        const float4* g = reinterpret_cast<const float4*>(raw + static_cast<size_t>(first) * s);
+        float4* d = reinterpret_cast<float4*>(sRaw);
+        for (size_t v = threadIdx.x; v < floats / 4; v += kDecodeThreads) d[v] = __ldg(g + v);
+        for (size_t f = (floats / 4) * 4 + threadIdx.x; f < floats; f += kDecodeThreads)
+            sRaw[f] = __ldg(raw + static_cast<size_t>(first) * s + f);
+        __syncthreads();
+        src = sRaw;
+        at = threadIdx.x;
+    }
 
     // splat_validate.slang:19-28
     bool valid = false;
     float3 p = make_float3(0.0f, 0.0f, 0.0f);
     float a = 0.0f, ls0 = 0.0f, ls1 = 0.0f, ls2 = 0.0f;
     if (inRange) {
-        p = decode_position(raw, i, e);
-        a = decode_opacity(field_of(raw, i, s, e.opacity), e.opacity_mode);
-        ls0 = decode_log_scale(field_of(raw, i, s, e.scale0), e.scale_mode);
-        ls1 = decode_log_scale(field_of(raw, i, s, e.scale1), e.scale_mode);
-        ls2 = decode_log_scale(field_of(raw, i, s, e.scale2), e.scale_mode);
+        p = decode_position(src, at, e);
+        a = decode_opacity(field_of(src, at, s, e.opacity), e.opacity_mode);
+        ls0 = decode_log_scale(field_of(src, at, s, e.scale0), e.scale_mode);
+        ls1 = decode_log_scale(field_of(src, at, s, e.scale1), e.scale_mode);
+        ls2 = decode_log_scale(field_of(src, at, s, e.scale2), e.scale_mode);
         const bool finite = isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(ls0) && isfinite(ls1) &&
                             isfinite(ls2) && fabsf(ls0) < 60.0f && fabsf(ls1) < 60.0f && fabsf(ls2) < 60.0f;
         valid = finite && a >= 1.0f / 255.0f;
@@ -257,34 +277,34 @@ decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_en
     // splat_decode.slang:30-90
     const uint32_t j = base + local;
     positions[j] = make_float4(p.x, p.y, p.z, fminf(fmaxf(a, 0.0f), 1.0f));
-    const float4 q = decode_quaternion(raw, i, e);
+    const float4 q = decode_quaternion(src, at, e);
     const float qLength = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
     const uint32_t rotation = encode_quaternion(qLength > 1e-8f ? q : make_float4(0.0f, 0.0f, 0.0f, 1.0f));
-    const float b0 = decode_colour(field_of(raw, i, s, e.dc0), e.colour_mode);
-    const float b1 = decode_colour(field_of(raw, i, s, e.dc1), e.colour_mode);
-    const float b2 = decode_colour(field_of(raw, i, s, e.dc2), e.colour_mode);
+    const float b0 = decode_colour(field_of(src, at, s, e.dc0), e.colour_mode);
+    const float b1 = decode_colour(field_of(src, at, s, e.dc1), e.colour_mode);
+    const float b2 = decode_colour(field_of(src, at, s, e.dc2), e.colour_mode);
     shape[j] = make_uint4(rotation, pack_halves(half_safe(ls0), half_safe(ls1)), pack_halves(half_safe(ls2), half_safe(b0)),
                           pack_halves(half_safe(b1), half_safe(b2)));
     // Rest coefficients, rgb per basis; every word of the row is written
     // (unused halves zero).
     uint32_t* row = sh + static_cast<size_t>(j) * shWords;
-    uint32_t word = 0, filled = 0, at = 0;
+    uint32_t word = 0, filled = 0, w = 0;
     for (uint32_t basis = 0; basis < keep; ++basis) {
         for (uint32_t colour = 0; colour < 3; ++colour) {
             const uint32_t field = e.rest_colour_outer != 0 ? e.rest_base + colour * e.rest_per_colour + basis
                                                             : e.rest_base + basis * 3 + colour;
-            float value = decode_byte_unit(field_of(raw, i, s, field), e.rest_mode);
+            float value = decode_byte_unit(field_of(src, at, s, field), e.rest_mode);
             if (e.flip_yz != 0) value = value * rest_flip_sign(basis);
             word |= (float_to_half(half_safe(value)) & 0xFFFFu) << (filled * 16);
             if (++filled == 2) {
-                row[at++] = word;
+                row[w++] = word;
                 word = 0;
                 filled = 0;
             }
         }
     }
-    if (filled == 1) row[at++] = word;
-    for (; at < shWords; ++at) row[at] = 0u;
+    if (filled == 1) row[w++] = word;
+    for (; w < shWords; ++w) row[w] = 0u;
 }
 
 // points_validate.slang:19-28 and points_decode.slang:24-41, fused the same way.
@@ -338,8 +358,17 @@ cudaError_t launch_decode_splats(const float* raw, uint32_t count, const lrt_spl
     const uint32_t blocks = (count + kDecodeThreads - 1) / kDecodeThreads;
     uint64_t* status = static_cast<uint64_t*>(scratch);
     uint32_t* tail = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + size_t{blocks} * 8);
-    decode_splats_kernel<<<blocks, kDecodeThreads, 0, stream>>>(raw, count, e, keep, shWords, positions, shape, sh,
-                                                                status, tail, tail + 1, err);
+    // Stage the records through shared memory when a block's fit (and the
+    // records start 16-byte aligned); otherwise read them in place.
+    const size_t smem = size_t{kDecodeThreads} * e.floats_per_record * sizeof(float);
+    const bool stage = smem <= 160 * 1024 && (reinterpret_cast<uintptr_t>(raw) & 15u) == 0;
+    if (stage) {
+        const cudaError_t a = cudaFuncSetAttribute(decode_splats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(smem));
+        if (a != cudaSuccess) return a;
+    }
+    decode_splats_kernel<<<blocks, kDecodeThreads, stage ? smem : 0, stream>>>(
+        raw, count, e, keep, shWords, positions, shape, sh, status, tail, tail + 1, err, stage ? 1u : 0u);
     return cudaGetLastError();
 }
 

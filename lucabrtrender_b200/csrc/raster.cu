@@ -132,6 +132,13 @@ cudaError_t ensure(DeviceBuffer& b, size_t bytes) {
     return e;
 }
 
+// Where a batch's ViewParams start in its parameter block: after the
+// FrameParams of every (view, instance), rounded up to 16 bytes, since a
+// ViewParams holds 8-byte pointers (a FrameParams is 212 bytes).
+size_t view_params_offset(uint32_t launches) {
+    return (size_t{launches} * sizeof(lrt::FrameParams) + 15) & ~size_t{15};
+}
+
 cudaError_t ensure_host(lrt_rast* r, size_t bytes) {
     if (r->metricHostBytes >= bytes && r->metricHost != nullptr) return cudaSuccess;
     if (r->metricHost != nullptr) cudaFreeHost(r->metricHost);
@@ -1287,14 +1294,14 @@ int enqueue_batch(lrt_rast* r, const std::vector<CloudDesc>& clouds, const lrt_v
     auto& B = r->batch;
     const uint32_t nViews = static_cast<uint32_t>(shape.order.size());
     const uint32_t nLaunch = nViews * shape.launchesPerView;
-    const size_t paramsBytes = size_t{nLaunch} * sizeof(FrameParams) + size_t{nViews} * sizeof(lrt::ViewParams);
+    const size_t paramsBytes = view_params_offset(nLaunch) + size_t{nViews} * sizeof(lrt::ViewParams);
     LRT_CUDA(r, cudaMemcpyAsync(B.params.ptr, B.hostParams, paramsBytes, cudaMemcpyHostToDevice, B.stream), "params");
     const FrameParams* devF = static_cast<const FrameParams*>(B.params.ptr);
     const lrt::ViewParams* devV = reinterpret_cast<const lrt::ViewParams*>(static_cast<const char*>(B.params.ptr) +
-                                                                          size_t{nLaunch} * sizeof(FrameParams));
+                                                                          view_params_offset(nLaunch));
     const FrameParams* hostF = static_cast<const FrameParams*>(B.hostParams);
     const lrt::ViewParams* hostV = reinterpret_cast<const lrt::ViewParams*>(static_cast<const char*>(B.hostParams) +
-                                                                           size_t{nLaunch} * sizeof(FrameParams));
+                                                                           view_params_offset(nLaunch));
     const uint32_t slotBits = bits_for(std::max<uint32_t>(shape.slots, 1));
     BlendParams bp{};
     bp.slotBits = slotBits;
@@ -1441,7 +1448,7 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
     // Per (view, instance) projection parameters and per view blend parameters,
     // written to pinned memory in view order (largest first).
     const uint32_t nLaunch = nViews * shape.launchesPerView;
-    const size_t paramsBytes = size_t{nLaunch} * sizeof(FrameParams) + size_t{nViews} * sizeof(lrt::ViewParams);
+    const size_t paramsBytes = view_params_offset(nLaunch) + size_t{nViews} * sizeof(lrt::ViewParams);
     if (B.hostParamsBytes < paramsBytes) {
         if (B.hostParams != nullptr) cudaFreeHost(B.hostParams);
         B.hostParams = nullptr;
@@ -1453,7 +1460,7 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
     LRT_CUDA(r, ensure_batch(r, B.params, paramsBytes), "batch parameters");
     FrameParams* hostF = static_cast<FrameParams*>(B.hostParams);
     lrt::ViewParams* hostV = reinterpret_cast<lrt::ViewParams*>(static_cast<char*>(B.hostParams) +
-                                                               size_t{nLaunch} * sizeof(FrameParams));
+                                                               view_params_offset(nLaunch));
 
     // The chunking the autotuner picked for this shape (tune on first sight).
     uint32_t perChunk = 0, blocksPerSM = 0;

@@ -83,3 +83,17 @@ def test_batch_with_two_instances_and_an_edit(rasterizer):
     want = singles(rasterizer, views, instances, settings)
     for (colour, depth), t in zip(want, targets):
         assert torch.equal(t.colour, colour) and torch.equal(t.depth, depth)
+
+
+@pytest.mark.parametrize("views", [1, 3])
+def test_a_batch_of_one_or_an_odd_number_of_views(rasterizer, views):
+    """Any number of (view, instance) parameter blocks: their per-view
+    records after them stay aligned for the pointers they hold."""
+    scene = H.synthetic_scene(20_000, 64, 64, seed=23)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings()
+    vs = cameras(views, 9)
+    for _ in range(3):   # tuning, capture, replay
+        targets, _ = rasterizer.render_batch(vs, instances, settings)
+    for (colour, depth), t in zip(singles(rasterizer, vs, instances, settings), targets):
+        assert torch.equal(t.colour, colour) and torch.equal(t.depth, depth)
