@@ -284,7 +284,9 @@ def run_next_rows(L, torch, dev, raster, packed, cloud, peak) -> dict:
     plain_ms = time_device(torch, stream, lambda: raster.render(cam, inst, settings, out, stream), 5)
     cmp_ms = time_device(torch, stream, lambda: raster.compare_images(out.colour, layer.colour, stream), 5)
     cmp_bytes = 2 * WIDTH * HEIGHT * 16
+    lod = run_lod(L, torch, stream, raster, cloud, settings, peak)
     return {
+        "lod": lod,
         "decode": {"workload": "1M raw 3DGS PLY records (236 B) to the packed layout, on the device",
                    "ms": round(decode_ms, 4), "gbs": round(decode_bytes / (decode_ms * 1e-3) / 1e9, 1),
                    "frac_of_hbm": round(decode_bytes / (decode_ms * 1e-3) / 1e9 / peak, 4)},
@@ -295,6 +297,43 @@ def run_next_rows(L, torch, dev, raster, packed, cloud, peak) -> dict:
         "compare_images": {"workload": "two 1920x1080 float4 images, 8-bit code histogram on the device",
                            "ms": round(cmp_ms, 4), "gbs": round(cmp_bytes / (cmp_ms * 1e-3) / 1e9, 1)},
     }
+
+
+def run_lod(L, torch, stream, raster, cloud, settings, peak) -> dict:
+    """Levels of detail of the benchmark cloud: the build, and per frame the
+    cut (one kernel and one count read) at a far view, 30 units out, where the
+    finest cells span 9-12 pixels; the frame drawn from each cut."""
+    import time
+    builder, selector = L.LodBuilder.create(raster), L.CutSelector.create(raster)
+    builds = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        lod = builder.build(cloud, stream=stream)
+        builds.append((time.perf_counter() - t0) * 1e3)
+        if len(builds) < 3:
+            lod.close()
+    far = L.projection_for(L.Camera.looking_at((6.0, 4.0, 30.0), (0.0, 0.0, 0.0)), WIDTH, HEIGHT)
+    out = L.RenderTargets(WIDTH, HEIGHT, device=cloud.positions.device)
+    full_ms = time_device(torch, stream, lambda: raster.render(far, [L.SplatInstance(cloud)], settings, out, stream), 5)
+    shw = cloud.sh_words
+    cuts = []
+    for threshold in (0.0, 10.0, 20.0, 40.0):
+        stats = []
+        inst = [L.LodInstance(lod)]
+        cut_ms = time_device(torch, stream, lambda: selector.select(far, inst, threshold, stats, stream), 5)
+        drawn = selector.select(far, inst, threshold, stats, stream)
+        frame_ms = time_device(torch, stream, lambda: raster.render(far, drawn, settings, out, stream), 5)
+        n_drawn = stats[0].splats + stats[0].merged
+        moved = (lod.merged_gaussians() + lod.count) * 4 + 2 * n_drawn * (32 + 4 * shw)
+        cuts.append({"threshold_px": threshold, "splats": stats[0].splats, "merged": stats[0].merged,
+                     "select_ms": round(cut_ms, 4), "select_gbs": round(moved / (cut_ms * 1e-3) / 1e9, 1),
+                     "frame_ms": round(frame_ms, 4)})
+    return {"workload": "the 1M-splat benchmark cloud (SH degree 3): LodBuilder.build, then CutSelector.select "
+                        "from (6, 4, 30) at 1920x1080 and the frame drawn from each cut",
+            "build_ms": round(float(np.median(builds)), 3), "levels": [lv.gaussians.count for lv in lod.levels],
+            "full_frame_ms": round(full_ms, 4), "cuts": cuts,
+            "select_bytes": "cells + codes read, drawn records read and written (32 + 4 sh_words B each); "
+                            "select_ms includes its one count read back"}
 
 
 def run_ours(args) -> None:

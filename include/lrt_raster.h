@@ -500,6 +500,92 @@ int lrt_l1_loss_grad(const void* colour, const void* target, uint32_t pixels, co
 int lrt_pack_points(const float* raw, uint32_t count, uint32_t colour_kind, float detail,
                     float* positions, uint32_t* colours, uint32_t* kept);
 
+/* ---- Levels of detail (modules/lod/include/lrt/lod/Lod.h) ----------------
+ * A cloud's octree levels of detail, built and cut on the device. The method
+ * is the reference's (shaders/lrt/lod/lod_common.slang:1-33): splats in
+ * Morton order; per octree cell the additive moments of its splats turned
+ * back into one Gaussian; per frame, a cell is drawn merged when it projects
+ * to at most `threshold` pixels and its parent does not, a splat when its
+ * finest merged cell does not. In memory only: every chunk of splats is
+ * resident (the .lrtc streaming store is not provided). */
+
+/* LodBuildSettings (Lod.h:83-93). */
+typedef struct lrt_lod_build_settings {
+    float max_group_fraction;   /* 0.5: the finest stored level is the deepest whose groups
+                                   number at most this fraction of the splats */
+    uint32_t coarsest_level;    /* 1 (clamped to 1..10) */
+    uint32_t chunk_splats;      /* 65536: splats per chunk, reported only */
+    uint32_t reserved;
+} lrt_lod_build_settings;
+
+int lrt_lod_build_settings_default(lrt_lod_build_settings* out);
+
+/* LodCloud (Lod.h:41-80): library-owned device buffers. */
+typedef struct lrt_lod lrt_lod;
+
+typedef struct lrt_lod_info {
+    uint32_t count;             /* splats */
+    uint32_t rest_per_colour, sh_words;
+    uint32_t levels;            /* stored merged levels, consecutive octree levels */
+    uint32_t coarsest, finest;  /* their octree levels */
+    uint32_t merged;            /* merged Gaussians over all stored levels */
+    uint32_t chunk_splats;
+    float bounds_lo[3], bounds_hi[3];
+    float extent;               /* the bounds' largest edge (x 1.0001): cells are cubes */
+    uint32_t level_groups[10];  /* per stored level, coarsest first */
+} lrt_lod_info;
+
+/* LodBuilder::build (Lod.cpp:86-300). `cloud` holds device pointers in the
+ * packed layout (rest_per_colour 0, 3, 8 or 15; sh_words at least
+ * (rest_per_colour * 3 + 1) / 2, and the merged levels' rows take as many
+ * words, zero past the coefficients); `bounds` (host, may be NULL:
+ * computed from the positions) is lo xyz then hi xyz; `settings` may be NULL
+ * (the defaults). The cloud is not changed; the result owns a Morton-ordered
+ * copy. Waits for the build. An empty cloud is LRT_INVALID_ARGUMENT. */
+int lrt_lod_build(lrt_rast* rast, const lrt_gpu_splats* cloud, const float* bounds,
+                  const lrt_lod_build_settings* settings, lrt_lod** out, void* stream);
+void lrt_lod_destroy(lrt_lod* lod);
+int lrt_lod_get_info(const lrt_lod* lod, lrt_lod_info* out);
+
+/* The Morton-ordered splats (LodCloud::splats) and each one's 30-bit code. */
+int lrt_lod_splats(const lrt_lod* lod, lrt_gpu_splats* out, const uint32_t** codes);
+
+/* Stored level `index` (0 = coarsest): its octree level, its merged Gaussians
+ * (LodLevel::gaussians) and per Gaussian its cell code (LodLevel::cells). */
+int lrt_lod_level(const lrt_lod* lod, uint32_t index, uint32_t* level, lrt_gpu_splats* gaussians,
+                  const uint32_t** cells);
+
+/* The finest stored level's groups' first splats (LodCloud::starts). */
+int lrt_lod_starts(const lrt_lod* lod, const uint32_t** starts, uint32_t* groups);
+
+/* LodInstance (Lod.h:106-111). threshold < 0: the call's. */
+typedef struct lrt_lod_instance {
+    const lrt_lod* cloud;
+    double object_to_world[16];
+    lrt_splat_edit edit;
+    float threshold;
+    uint32_t reserved;
+} lrt_lod_instance;
+
+/* CutStats (Lod.h:113-124) without the streaming needs. */
+typedef struct lrt_cut_stats {
+    uint32_t splats;      /* the cloud's own splats drawn */
+    uint32_t merged;      /* merged Gaussians drawn */
+    uint32_t available;   /* splats in the cloud */
+    uint32_t reserved;
+} lrt_cut_stats;
+
+/* CutSelector::select (Lod.cpp:349-547): each instance's cut for this view
+ * as instances the rasteriser draws. out receives up to `count` instances
+ * (those drawing anything, in order; *out_count of them); their clouds belong
+ * to `rast` and are rewritten by its next lrt_lod_select. stats (may be NULL)
+ * receives one entry per instance. The drawn cloud lists the merged
+ * Gaussians, coarsest level first, then the splats, in Morton order. One
+ * kernel per instance and one wait for all of them. */
+int lrt_lod_select(lrt_rast* rast, const lrt_projection* projection, const lrt_lod_instance* instances,
+                   uint32_t count, float threshold, lrt_splat_instance* out, uint32_t* out_count,
+                   lrt_cut_stats* stats, void* stream);
+
 /* Diagnostic: the library's own exp (fn 0), log (1), sRGB-to-linear (2) and
  * cut-off power (3), evaluated on the device over n floats (device pointers),
  * for comparing their bits with a host implementation. No reference

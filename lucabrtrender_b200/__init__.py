@@ -12,11 +12,13 @@ from ._abi import SplatEncoding
 from .scene import (CloudLoader, GpuPoints, GpuSplats, PackedPoints, PackedSplats, pack_points, pack_splats,
                     ply_encoding, points_to_device, synthetic_records, to_device)
 from .train import l1_loss, rasterize
+from .lod import CutSelector, CutStats, LodBuildSettings, LodBuilder, LodCloud, LodInstance, LodLevel
 
 __all__ = [
     "LrtError", "Camera", "Lens", "Projection", "projection_for", "square_pixel_camera", "Depth", "EditMode", "EditShape",
     "FrameStats", "RenderSettings", "RenderTargets", "SplatEdit", "SplatInstance", "TileRasterizer", "math_eval",
     "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
     "PointInstance", "PointStyle", "GpuPoints", "PackedPoints", "pack_points", "points_to_device",
-    "SplatEncoding", "ply_encoding", "l1_loss",
+    "SplatEncoding", "ply_encoding", "l1_loss", "CutSelector", "CutStats", "LodBuildSettings", "LodBuilder",
+    "LodCloud", "LodInstance", "LodLevel",
 ]

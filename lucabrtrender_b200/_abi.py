@@ -41,7 +41,9 @@ EXPORTS = (
     "lrt_rast_train_backward", "lrt_rast_backward_times", "lrt_rast_render_batch", "lrt_rast_render_async",
     "lrt_rast_settle", "lrt_rast_render_composite", "lrt_pack_points", "lrt_splat_encoding_ply",
     "lrt_rast_decode_splats", "lrt_rast_decode_points", "lrt_rast_compare_images", "lrt_rast_compare_hdr",
-    "lrt_rast_count_different", "lrt_rast_l1_loss", "lrt_l1_loss_grad",
+    "lrt_rast_count_different", "lrt_rast_l1_loss", "lrt_l1_loss_grad", "lrt_lod_build_settings_default",
+    "lrt_lod_build", "lrt_lod_destroy", "lrt_lod_get_info", "lrt_lod_splats", "lrt_lod_level", "lrt_lod_starts",
+    "lrt_lod_select",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -192,6 +194,27 @@ class TrainGrads(C.Structure):
 _lib = None
 
 
+class LodBuildSettings(C.Structure):
+    _fields_ = [("max_group_fraction", C.c_float), ("coarsest_level", C.c_uint32), ("chunk_splats", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class LodInfo(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("rest_per_colour", C.c_uint32), ("sh_words", C.c_uint32),
+                ("levels", C.c_uint32), ("coarsest", C.c_uint32), ("finest", C.c_uint32), ("merged", C.c_uint32),
+                ("chunk_splats", C.c_uint32), ("bounds_lo", C.c_float * 3), ("bounds_hi", C.c_float * 3),
+                ("extent", C.c_float), ("level_groups", C.c_uint32 * 10)]
+
+
+class LodInstanceStruct(C.Structure):
+    _fields_ = [("cloud", C.c_void_p), ("object_to_world", C.c_double * 16), ("edit", SplatEdit),
+                ("threshold", C.c_float), ("reserved", C.c_uint32)]
+
+
+class CutStatsStruct(C.Structure):
+    _fields_ = [("splats", C.c_uint32), ("merged", C.c_uint32), ("available", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 def load() -> C.CDLL:
     """The loaded library; raises if it is missing (no fallback path exists)."""
     global _lib
@@ -252,6 +275,19 @@ def load() -> C.CDLL:
                                           C.c_uint32, C.POINTER(RenderSettingsStruct), C.POINTER(BatchStats),
                                           C.c_void_p]
     lib.lrt_rast_backward_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.lrt_lod_build_settings_default.argtypes = [C.POINTER(LodBuildSettings)]
+    lib.lrt_lod_build.argtypes = [C.c_void_p, C.POINTER(GpuSplatsStruct), C.c_void_p, C.POINTER(LodBuildSettings),
+                                  C.POINTER(C.c_void_p), C.c_void_p]
+    lib.lrt_lod_destroy.argtypes = [C.c_void_p]
+    lib.lrt_lod_destroy.restype = None
+    lib.lrt_lod_get_info.argtypes = [C.c_void_p, C.POINTER(LodInfo)]
+    lib.lrt_lod_splats.argtypes = [C.c_void_p, C.POINTER(GpuSplatsStruct), C.POINTER(C.c_void_p)]
+    lib.lrt_lod_level.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(GpuSplatsStruct),
+                                  C.POINTER(C.c_void_p)]
+    lib.lrt_lod_starts.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32)]
+    lib.lrt_lod_select.argtypes = [C.c_void_p, C.POINTER(Projection), C.POINTER(LodInstanceStruct), C.c_uint32,
+                                   C.c_float, C.POINTER(SplatInstanceStruct), C.POINTER(C.c_uint32),
+                                   C.POINTER(CutStatsStruct), C.c_void_p]
     if lib.lrt_abi_version() != ABI_VERSION:
         raise RuntimeError(f"ABI version mismatch: library {lib.lrt_abi_version()}, bindings {ABI_VERSION}")
     _lib = lib

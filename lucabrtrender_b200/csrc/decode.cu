@@ -13,19 +13,13 @@
 // with -fmad=false, so it rounds as the CPU restatement does.
 #include "kernels.cuh"
 #include "raster_common.cuh"
-
-#include <cuda/atomic>
+#include "lookback.cuh"
 
 namespace lrt {
 namespace {
 
 constexpr uint32_t kDecodeThreads = 256;
-constexpr uint64_t kFlagAggregate = 1ull << 62;
-constexpr uint64_t kFlagInclusive = 2ull << 62;
-constexpr uint64_t kValueMask = (1ull << 62) - 1;
-constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr float kSH0 = 0.28209479177387814f;
-constexpr float kSqrtHalf = 0.70710678f;
 
 __device__ __forceinline__ float field_of(const float* raw, uint32_t record, uint32_t stride, uint32_t field) {
     return raw[static_cast<size_t>(record) * stride + field];
@@ -91,7 +85,7 @@ __device__ __forceinline__ float4 decode_quaternion(const float* raw, uint32_t i
         float sum = 0.0f;
         for (int k = 3; k >= 0; --k) {
             if (static_cast<uint32_t>(k) == largest) continue;
-            const float magnitude = kSqrtHalf * static_cast<float>(comp & 511u) / 511.0f;
+            const float magnitude = kSqrtHalfF * static_cast<float>(comp & 511u) / 511.0f;
             q[k] = ((comp >> 9) & 1u) != 0 ? -magnitude : magnitude;
             sum = sum + q[k] * q[k];
             comp = comp >> 10;
@@ -107,118 +101,6 @@ __device__ __forceinline__ float4 decode_quaternion(const float* raw, uint32_t i
     return make_float4(q[0], q[1], q[2], q[3]);
 }
 
-// packing.slang:26-50: smallest three of the normalised quaternion.
-__device__ __forceinline__ uint32_t encode_quaternion(float4 q0) {
-    const float l = sqrtf(q0.x * q0.x + q0.y * q0.y + q0.z * q0.z + q0.w * q0.w);
-    float q[4] = {q0.x / l, q0.y / l, q0.z / l, q0.w / l};
-    uint32_t largest = 0;
-    float best = fabsf(q[0]);
-    for (uint32_t k = 1; k < 4; ++k) {
-        if (fabsf(q[k]) > best) {
-            best = fabsf(q[k]);
-            largest = k;
-        }
-    }
-    if (q[largest] < 0.0f) {
-        for (float& v : q) v = -v;
-    }
-    uint32_t word = largest;
-    uint32_t shift = 22;
-    for (uint32_t k = 0; k < 4; ++k) {
-        if (k == largest) continue;
-        const float unit = fminf(fmaxf(q[k] / kSqrtHalf * 0.5f + 0.5f, 0.0f), 1.0f);
-        word |= static_cast<uint32_t>(roundf(unit * 1023.0f)) << shift;
-        shift -= 10;
-    }
-    return word;
-}
-
-__device__ __forceinline__ float half_safe(float v) { return fminf(fmaxf(v, -65000.0f), 65000.0f); }
-__device__ __forceinline__ uint32_t pack_halves(float a, float b) {
-    return (float_to_half(a) & 0xFFFFu) | ((float_to_half(b) & 0xFFFFu) << 16);
-}
-
-// One block's exclusive scan of a flag per thread; *total gets the block's sum.
-__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* sWarp, uint32_t* total) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (uint32_t d = 1; d < 32; d <<= 1) {
-        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, x, d);
-        if (lane >= d) x += o;
-    }
-    if (lane == 31) sWarp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < kDecodeThreads / 32 ? sWarp[lane] : 0;
-#pragma unroll
-        for (uint32_t d = 1; d < 32; d <<= 1) {
-            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
-            if (lane >= d) w += o;
-        }
-        if (lane < kDecodeThreads / 32) sWarp[lane] = w;
-    }
-    __syncthreads();
-    const uint32_t before = warp == 0 ? 0 : sWarp[warp - 1];
-    *total = sWarp[kDecodeThreads / 32 - 1];
-    __syncthreads();
-    return before + x - v;
-}
-
-// The kept records before this block: decoupled look-back by warp 0 over a
-// window of 32 earlier blocks at a time (bounded waits). Returns the prefix
-// to every thread; the last block also writes the grand total.
-__device__ __forceinline__ uint32_t block_base(uint32_t part, uint32_t lastPart, uint32_t blockTotal,
-                                               uint64_t* status, uint32_t* total, uint32_t* err, uint32_t* sBase) {
-    const uint32_t lane = threadIdx.x & 31u;
-    if (threadIdx.x < 32) {
-        uint64_t prefix = 0;
-        if (lane == 0) {
-            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[part]);
-            mine.store((part == 0 ? kFlagInclusive : kFlagAggregate) | blockTotal, cuda::memory_order_relaxed);
-        }
-        if (part > 0) {
-            int64_t q = static_cast<int64_t>(part) - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const int64_t idx = q - static_cast<int64_t>(lane);
-                uint64_t word = kFlagInclusive;
-                if (idx >= 0) {
-                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[idx]);
-                    word = sref.load(cuda::memory_order_relaxed);
-                }
-                const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, (word & kFlagInclusive) != 0);
-                const uint32_t empty = __ballot_sync(0xFFFFFFFFu, (word & ~kValueMask) == 0);
-                const uint32_t first = inclusive != 0 ? static_cast<uint32_t>(__ffs(inclusive)) - 1u : 32u;
-                const uint32_t upTo = first < 32u ? (2u << first) - 1u : 0xFFFFFFFFu;
-                if ((empty & upTo) != 0) {
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0) atomicOr(err, kErrTimeout);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                uint64_t v = ((upTo >> lane) & 1u) ? (word & kValueMask) : 0ull;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-                prefix += v;
-                if (first < 32u) break;
-                q -= 32;
-            }
-            if (lane == 0) {
-                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[part]);
-                mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
-            }
-        }
-        if (lane == 0) {
-            *sBase = static_cast<uint32_t>(prefix);
-            if (part == lastPart) *total = static_cast<uint32_t>(prefix + blockTotal);
-        }
-    }
-    __syncthreads();
-    return *sBase;
-}
 
 __global__ void __launch_bounds__(kDecodeThreads)
 decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_encoding e, uint32_t keep,
@@ -269,7 +151,7 @@ decode_splats_kernel(const float* __restrict__ raw, uint32_t count, lrt_splat_en
         valid = finite && a >= 1.0f / 255.0f;
     }
     uint32_t blockTotal = 0;
-    const uint32_t local = block_scan(valid ? 1u : 0u, sWarp, &blockTotal);
+    const uint32_t local = block_scan<kDecodeThreads>(valid ? 1u : 0u, sWarp, &blockTotal);
     const uint32_t lastPart = (count + kDecodeThreads - 1) / kDecodeThreads - 1;
     const uint32_t base = block_base(part, lastPart, blockTotal, status, total, err, &sBase);
     if (!valid) return;
@@ -329,7 +211,7 @@ decode_points_kernel(const float* __restrict__ raw, uint32_t count, uint32_t col
         valid = isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]) && kept;
     }
     uint32_t blockTotal = 0;
-    const uint32_t local = block_scan(valid ? 1u : 0u, sWarp, &blockTotal);
+    const uint32_t local = block_scan<kDecodeThreads>(valid ? 1u : 0u, sWarp, &blockTotal);
     const uint32_t lastPart = (count + kDecodeThreads - 1) / kDecodeThreads - 1;
     const uint32_t base = block_base(part, lastPart, blockTotal, status, total, err, &sBase);
     if (!valid) return;

@@ -116,4 +116,66 @@ cudaError_t launch_l1_loss(const float4* colour, const float* target, uint32_t p
 cudaError_t launch_l1_grad(const float4* colour, const float* target, uint32_t pixels, const float* gradLoss,
                            float4* gradColour, cudaStream_t stream);
 
+
+// Levels of detail (lod.cu).
+constexpr uint32_t kLodLevels = 10;   // 30-bit Morton codes, lod_common.slang:36
+constexpr uint32_t kLodMomentsHead = 13;   // lod_common.slang:38-40
+
+// What the build keeps on the device between its kernels: the bounds, the
+// cubic extent, the splat count the sort reads, and per level the number of
+// splats that begin a group there and at no coarser level (index = level;
+// kLodLevels + 1 counts splats whose codes equal their predecessor's).
+struct LodGlobals {
+    float lo[3], hi[3], extent;
+    uint32_t count;
+    uint32_t firstLevel[kLodLevels + 2];
+    uint32_t groupTotals[kLodLevels + 1];   // per level: the groups its compaction found
+    uint32_t pad[3];
+};
+
+// One instance's cut: the cloud's layout and this view's test.
+struct LodCutParams {
+    uint32_t merged, count, levels, coarsest;   // coarsest: octree level of stored level 0
+    uint32_t levelBase[kLodLevels + 2];         // first merged Gaussian of each stored level; [levels] = merged
+    uint32_t shWords, capacity, ortho, pad0;
+    float lo[3], extent;
+    float eye[3], pixelsPerUnit;
+    float threshold, pad1, pad2, pad3;
+};
+
+struct LodSplatArrays {
+    float4* positions;
+    uint4* shape;
+    uint32_t* sh;
+};
+
+cudaError_t launch_lod_bounds(const float4* positions, uint32_t count, const float* given, LodGlobals* globals,
+                              float* partial, cudaStream_t stream);
+size_t lod_bounds_partial_bytes();
+cudaError_t launch_lod_morton(const float4* positions, uint32_t count, const LodGlobals* globals, uint32_t* keys,
+                              uint32_t* order, cudaStream_t stream);
+cudaError_t launch_lod_reorder(const uint32_t* order, const uint32_t* codes, uint32_t count, uint32_t shWords,
+                               const float4* srcPositions, const uint4* srcShape, const uint32_t* srcSh,
+                               LodSplatArrays store, LodGlobals* globals, cudaStream_t stream);
+// status: compaction_status_bytes(count, lod_compaction_threads()) zeroed bytes.
+uint32_t lod_compaction_threads();
+// capacity: the groups the output arrays hold (writes past it are dropped).
+cudaError_t launch_lod_finest_groups(const uint32_t* codes, uint32_t count, uint32_t level, uint32_t capacity,
+                                     uint32_t* starts, uint32_t* cells, void* status, uint32_t* total, uint32_t* err,
+                                     cudaStream_t stream);
+cudaError_t launch_lod_parent_groups(const uint32_t* fineCells, uint32_t fineCount, uint32_t capacity,
+                                     uint32_t* cells, uint32_t* firstChild, void* status, uint32_t* total,
+                                     uint32_t* err, cudaStream_t stream);
+cudaError_t launch_lod_leaf_moments(const LodSplatArrays store, uint32_t count, uint32_t restPerColour,
+                                    uint32_t shWords, const uint32_t* starts, uint32_t groups, float* moments,
+                                    cudaStream_t stream);
+cudaError_t launch_lod_merge_moments(const uint32_t* firstChild, uint32_t groups, uint32_t fineGroups,
+                                     const float* fineMoments, float* moments, uint32_t stride, cudaStream_t stream);
+cudaError_t launch_lod_finalize(const float* moments, uint32_t groups, uint32_t restPerColour, uint32_t shWords,
+                                LodSplatArrays merged, cudaStream_t stream);
+// counts: two zeroed words (drawn, of which merged); status as above over merged + count items.
+cudaError_t launch_lod_cut(const LodCutParams& c, const uint32_t* cells, const uint32_t* codes,
+                           const LodSplatArrays merged, const LodSplatArrays store, LodSplatArrays out,
+                           void* status, uint32_t* counts, uint32_t* err, cudaStream_t stream);
+
 }  // namespace lrt

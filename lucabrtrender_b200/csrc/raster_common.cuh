@@ -112,4 +112,54 @@ __device__ __forceinline__ float srgb_to_linear(float c) {
     return c <= 0.04045f ? c / 12.92f : lrt_pow((c + 0.055f) / 1.055f, 2.4f);
 }
 
+
+constexpr float kSqrtHalfF = 0.70710678f;
+
+// decodeQuaternion, packing.slang:52-69: the smallest-three word to (x, y, z, w).
+__device__ __forceinline__ void decode_rotation_word(uint32_t word, float& x, float& y, float& z, float& w) {
+    const uint32_t largest = word & 3u;
+    float sx = static_cast<float>((word >> 22) & 1023u);
+    float sy = static_cast<float>((word >> 12) & 1023u);
+    float sz = static_cast<float>((word >> 2) & 1023u);
+    sx = (sx / 1023.0f * 2.0f - 1.0f) * kSqrtHalfF;
+    sy = (sy / 1023.0f * 2.0f - 1.0f) * kSqrtHalfF;
+    sz = (sz / 1023.0f * 2.0f - 1.0f) * kSqrtHalfF;
+    const float rest = sqrtf(fmaxf(0.0f, 1.0f - (sx * sx + sy * sy + sz * sz)));
+    x = largest == 0 ? rest : sx;
+    y = largest == 1 ? rest : largest == 0 ? sx : sy;
+    z = largest == 2 ? rest : largest == 3 ? sz : sy;
+    w = largest == 3 ? rest : sz;
+}
+
+// packing.slang:26-50: smallest three of the normalised quaternion.
+__device__ __forceinline__ uint32_t encode_quaternion(float4 q0) {
+    const float l = sqrtf(q0.x * q0.x + q0.y * q0.y + q0.z * q0.z + q0.w * q0.w);
+    float q[4] = {q0.x / l, q0.y / l, q0.z / l, q0.w / l};
+    uint32_t largest = 0;
+    float best = fabsf(q[0]);
+    for (uint32_t k = 1; k < 4; ++k) {
+        if (fabsf(q[k]) > best) {
+            best = fabsf(q[k]);
+            largest = k;
+        }
+    }
+    if (q[largest] < 0.0f) {
+        for (float& v : q) v = -v;
+    }
+    uint32_t word = largest;
+    uint32_t shift = 22;
+    for (uint32_t k = 0; k < 4; ++k) {
+        if (k == largest) continue;
+        const float unit = fminf(fmaxf(q[k] / kSqrtHalfF * 0.5f + 0.5f, 0.0f), 1.0f);
+        word |= static_cast<uint32_t>(roundf(unit * 1023.0f)) << shift;
+        shift -= 10;
+    }
+    return word;
+}
+
+__device__ __forceinline__ float half_safe(float v) { return fminf(fmaxf(v, -65000.0f), 65000.0f); }
+__device__ __forceinline__ uint32_t pack_halves(float a, float b) {
+    return (float_to_half(a) & 0xFFFFu) | ((float_to_half(b) & 0xFFFFu) << 16);
+}
+
 }  // namespace lrt

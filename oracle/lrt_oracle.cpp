@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -1764,3 +1765,442 @@ int ora_random_points(uint32_t count, uint64_t seed, float* raw) {
 }
 
 }   // extern "C"
+
+// =================================================================== LOD ====
+// Levels of detail, restated on the host in the reference's own schedule
+// (modules/lod/src/Lod.cpp:86-300 and 349-547 over shaders/lrt/lod/*.slang):
+// a stable sort by Morton code, then per level a boundary pass, an exclusive
+// prefix sum and the groups pass; leaf moments, merges through the finer
+// level's per-splat group index, finalize; per frame the per-level
+// selections, the finest level's state, the per-splat selection, and the
+// gather in part order.
+struct ora_lod {
+    uint32_t count = 0, rest = 0, shWords = 0, coarsest = 0, finest = 0;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, extent = 0.0f;
+    std::vector<float> positions;               // the store, Morton order: 4 per splat
+    std::vector<uint32_t> shape, sh, codes;     // 4, shWords, 1 per splat
+    std::vector<uint32_t> groups, starts;       // finest level: group per splat, first splat per group
+    struct Level {
+        uint32_t level = 0;
+        std::vector<float> positions;
+        std::vector<uint32_t> shape, sh, cells;
+    };
+    std::vector<Level> levels;                  // coarsest first
+};
+
+namespace {
+
+constexpr uint32_t kOraLodLevels = 10;        // lod_common.slang:36
+constexpr uint32_t kOraMomentsHead = 13;      // lod_common.slang:38-40
+
+uint32_t levelShiftOf(uint32_t level) { return 3 * (kOraLodLevels - level); }   // lod_common.slang:64-66
+
+// morton.slang:23-28 by one bit at a time: bit b of x, y, z to bits 3b+2,
+// 3b+1, 3b of the code.
+uint32_t mortonOf(uint32_t qx, uint32_t qy, uint32_t qz) {
+    uint32_t code = 0;
+    for (uint32_t b = 0; b < 10; ++b) {
+        code |= ((qx >> b) & 1u) << (3 * b + 2);
+        code |= ((qy >> b) & 1u) << (3 * b + 1);
+        code |= ((qz >> b) & 1u) << (3 * b);
+    }
+    return code;
+}
+
+// morton.slang:30-33.
+void cellIndexOf(uint32_t cell, uint32_t idx[3]) {
+    idx[0] = idx[1] = idx[2] = 0;
+    for (uint32_t b = 0; b < 10; ++b) {
+        idx[0] |= ((cell >> (3 * b + 2)) & 1u) << b;
+        idx[1] |= ((cell >> (3 * b + 1)) & 1u) << b;
+        idx[2] |= ((cell >> (3 * b)) & 1u) << b;
+    }
+}
+
+uint32_t quantiseUnit(float v, float lo, float extent) {   // morton.slang:25
+    const float unit = saturatef((v - lo) / extent);
+    const uint32_t q = static_cast<uint32_t>(unit * 1024.0f);
+    return q < 1023u ? q : 1023u;
+}
+
+// lod_leaf_moments.slang:26-64 for one group [first, end).
+void leafMomentsOf(const ora_lod& d, uint32_t first, uint32_t end, float* m) {
+    const uint32_t stride = kOraMomentsHead + 3 * d.rest;
+    for (uint32_t k = 0; k < stride; ++k) m[k] = 0.0f;
+    for (uint32_t i = first; i < end; ++i) {
+        const float* p = &d.positions[size_t{i} * 4];
+        const uint32_t* row = &d.shape[size_t{i} * 4];
+        const float s[3] = {expImpl(lowHalf(row[1])), expImpl(highHalf(row[1])), expImpl(lowHalf(row[2]))};
+        float q[4];
+        decodeQuaternion(row[0], q);
+        const float x = q[0], y = q[1], z = q[2], w = q[3];
+        const float r[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
+                               {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
+                               {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}};
+        float ms[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) ms[a][b] = r[a][b] * s[b];
+        float cov[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) cov[a][b] = ms[a][0] * ms[b][0] + ms[a][1] * ms[b][1] + ms[a][2] * ms[b][2];
+        const float smallest = std::fmin(std::fmin(s[0], s[1]), s[2]);
+        const float area = s[0] * s[1] * s[2] / std::fmax(smallest, 1e-20f);
+        const float weight = p[3] * area;
+        m[0] += weight;
+        m[1] += weight * p[0];
+        m[2] += weight * p[1];
+        m[3] += weight * p[2];
+        m[4] += weight * (cov[0][0] + p[0] * p[0]);
+        m[5] += weight * (cov[0][1] + p[0] * p[1]);
+        m[6] += weight * (cov[0][2] + p[0] * p[2]);
+        m[7] += weight * (cov[1][1] + p[1] * p[1]);
+        m[8] += weight * (cov[1][2] + p[1] * p[2]);
+        m[9] += weight * (cov[2][2] + p[2] * p[2]);
+        m[10] += weight * highHalf(row[2]);
+        m[11] += weight * lowHalf(row[3]);
+        m[12] += weight * highHalf(row[3]);
+        const uint32_t* shRow = d.sh.data() + size_t{i} * d.shWords;
+        for (uint32_t h = 0; h < d.rest * 3; ++h) m[kOraMomentsHead + h] += weight * halfAt(shRow, h);
+    }
+}
+
+void mul3(const float a[3][3], const float b[3][3], float o[3][3]) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o[r][c] = a[r][0] * b[0][c] + a[r][1] * b[1][c] + a[r][2] * b[2][c];
+}
+
+float signOf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+// lod_finalize.slang:16-40.
+void jacobiOf(float a[3][3], float v[3][3]) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) v[r][c] = r == c ? 1.0f : 0.0f;
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        for (int pq = 0; pq < 3; ++pq) {
+            const int p = pq == 2 ? 1 : 0;
+            const int q = pq == 0 ? 1 : 2;
+            const float apq = a[p][q];
+            if (std::fabs(apq) < 1e-30f) continue;
+            const float theta = (a[q][q] - a[p][p]) / (2.0f * apq);
+            const float t = signOf(theta + 1e-30f) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0f));
+            const float c = 1.0f / std::sqrt(t * t + 1.0f);
+            const float s = t * c;
+            float j[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+            j[p][p] = c;
+            j[q][q] = c;
+            j[p][q] = s;
+            j[q][p] = -s;
+            float jt[3][3], b[3][3], o[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int cc = 0; cc < 3; ++cc) jt[r][cc] = j[cc][r];
+            mul3(a, j, b);
+            mul3(jt, b, a);
+            mul3(v, j, o);
+            std::memcpy(v, o, sizeof(o));
+        }
+    }
+}
+
+// packing.slang:76-93.
+void quaternionOfAxesOf(const float m[3][3], float q[4]) {
+    const float trace = m[0][0] + m[1][1] + m[2][2];
+    if (trace > 0.0f) {
+        const float s = 0.5f / std::sqrt(trace + 1.0f);
+        q[0] = (m[2][1] - m[1][2]) * s, q[1] = (m[0][2] - m[2][0]) * s, q[2] = (m[1][0] - m[0][1]) * s, q[3] = 0.25f / s;
+    } else if (m[0][0] > m[1][1] && m[0][0] > m[2][2]) {
+        const float s = 2.0f * std::sqrt(1.0f + m[0][0] - m[1][1] - m[2][2]);
+        q[0] = 0.25f * s, q[1] = (m[1][0] + m[0][1]) / s, q[2] = (m[0][2] + m[2][0]) / s, q[3] = (m[2][1] - m[1][2]) / s;
+    } else if (m[1][1] > m[2][2]) {
+        const float s = 2.0f * std::sqrt(1.0f - m[0][0] + m[1][1] - m[2][2]);
+        q[0] = (m[1][0] + m[0][1]) / s, q[1] = 0.25f * s, q[2] = (m[2][1] + m[1][2]) / s, q[3] = (m[0][2] - m[2][0]) / s;
+    } else {
+        const float s = 2.0f * std::sqrt(1.0f - m[0][0] - m[1][1] + m[2][2]);
+        q[0] = (m[0][2] + m[2][0]) / s, q[1] = (m[2][1] + m[1][2]) / s, q[2] = 0.25f * s, q[3] = (m[1][0] - m[0][1]) / s;
+    }
+    const float l = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (int k = 0; k < 4; ++k) q[k] = q[k] / l;
+}
+
+// lod_finalize.slang:42-96: one group's moments to a packed Gaussian.
+void finalizeOf(const float* at, uint32_t rest, uint32_t shWords, float* pos, uint32_t* shape, uint32_t* sh) {
+    const float weight = std::fmax(at[0], 1e-30f);
+    const float mu[3] = {at[1] / weight, at[2] / weight, at[3] / weight};
+    float a[3][3] = {{at[4] / weight, at[5] / weight, at[6] / weight},
+                     {at[5] / weight, at[7] / weight, at[8] / weight},
+                     {at[6] / weight, at[8] / weight, at[9] / weight}};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) a[r][c] = a[r][c] - mu[r] * mu[c];
+    float axes[3][3];
+    jacobiOf(a, axes);
+    const float det = axes[0][0] * (axes[1][1] * axes[2][2] - axes[1][2] * axes[2][1]) -
+                      axes[0][1] * (axes[1][0] * axes[2][2] - axes[1][2] * axes[2][0]) +
+                      axes[0][2] * (axes[1][0] * axes[2][1] - axes[1][1] * axes[2][0]);
+    if (det < 0.0f)
+        for (int r = 0; r < 3; ++r) axes[r][2] = -axes[r][2];
+    const float s[3] = {std::sqrt(std::fmax(a[0][0], 1e-14f)), std::sqrt(std::fmax(a[1][1], 1e-14f)),
+                        std::sqrt(std::fmax(a[2][2], 1e-14f))};
+    const float smallest = std::fmin(std::fmin(s[0], s[1]), s[2]);
+    const float area = s[0] * s[1] * s[2] / std::fmax(smallest, 1e-20f);
+    const float opacity = std::fmin(at[0] / std::fmax(area, 1e-30f), 0.99f);
+    const float base[3] = {at[10] / weight, at[11] / weight, at[12] / weight};
+    pos[0] = mu[0], pos[1] = mu[1], pos[2] = mu[2], pos[3] = opacity;
+    float q[4];
+    quaternionOfAxesOf(axes, q);
+    shape[0] = encodeQuaternion(q);
+    shape[1] = packHalves(halfSafe(logImpl(s[0])), halfSafe(logImpl(s[1])));
+    shape[2] = packHalves(halfSafe(logImpl(s[2])), halfSafe(base[0]));
+    shape[3] = packHalves(halfSafe(base[1]), halfSafe(base[2]));
+    for (uint32_t w = 0; w < shWords; ++w) sh[w] = 0;
+    for (uint32_t h = 0; h < rest * 3; ++h) {
+        const uint32_t bits = floatToHalf(halfSafe(at[kOraMomentsHead + h] / weight)) & 0xFFFFu;
+        sh[h / 2] |= bits << ((h & 1u) * 16);
+    }
+}
+
+// lod_cut.slang:12-30.
+struct OraCut {
+    float lo[3], extent, eye[3], pixelsPerUnit, threshold;
+    bool ortho;
+    float projectedEdge(uint32_t cell, uint32_t level) const {
+        const float edge = extent / static_cast<float>(1u << level);
+        if (ortho) return edge * pixelsPerUnit;
+        uint32_t idx[3];
+        cellIndexOf(cell, idx);
+        float d[3];
+        for (int k = 0; k < 3; ++k) {
+            const float l = lo[k] + static_cast<float>(idx[k]) * edge;
+            const float nearest = std::fmin(std::fmax(eye[k], l), l + edge);
+            d[k] = nearest - eye[k];
+        }
+        const float distance = std::fmax(std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), 1e-6f);
+        return edge * pixelsPerUnit / distance;
+    }
+    bool small(uint32_t cell, uint32_t level) const { return threshold > 0.0f && projectedEdge(cell, level) <= threshold; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int ora_lod_build(const lrt_gpu_splats* cloud, const float* bounds, float maxGroupFraction, uint32_t coarsestLevel,
+                  ora_lod** out) {
+    if (cloud == nullptr || out == nullptr || cloud->count == 0) return LRT_INVALID_ARGUMENT;
+    const uint32_t n = cloud->count;
+    auto d = std::make_unique<ora_lod>();
+    d->count = n;
+    d->rest = cloud->rest_per_colour;
+    d->shWords = cloud->sh_words;
+    const float* srcPos = static_cast<const float*>(cloud->positions);
+    const uint32_t* srcShape = static_cast<const uint32_t*>(cloud->shape);
+    const uint32_t* srcSh = static_cast<const uint32_t*>(cloud->sh);
+    // CloudLoader::boundsOf (GpuClouds.cpp:93-125), then Lod.cpp:91-97.
+    for (int k = 0; k < 3; ++k) {
+        if (bounds != nullptr) {
+            d->lo[k] = bounds[k], d->hi[k] = bounds[3 + k];
+            continue;
+        }
+        float lo = 3.4e38f, hi = -3.4e38f;
+        for (uint32_t i = 0; i < n; ++i) lo = std::fmin(lo, srcPos[size_t{i} * 4 + k]), hi = std::fmax(hi, srcPos[size_t{i} * 4 + k]);
+        d->lo[k] = lo, d->hi[k] = hi;
+    }
+    float extent = 0.0f;
+    for (int k = 0; k < 3; ++k) extent = std::max(extent, d->hi[k] - d->lo[k]);
+    extent = std::max(extent, 1e-6f);
+    extent *= 1.0001f;
+    d->extent = extent;
+    // Morton order (lod_morton.slang; RadixSort is stable: ties keep index order).
+    std::vector<uint32_t> keys(n), order(n);
+    const float e = std::fmax(extent, 1e-20f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* p = srcPos + size_t{i} * 4;
+        keys[i] = mortonOf(quantiseUnit(p[0], d->lo[0], e), quantiseUnit(p[1], d->lo[1], e), quantiseUnit(p[2], d->lo[2], e));
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+    d->positions.resize(size_t{n} * 4);
+    d->shape.resize(size_t{n} * 4);
+    d->sh.resize(size_t{n} * d->shWords);
+    d->codes.resize(n);
+    for (uint32_t k = 0; k < n; ++k) {   // lod_reorder.slang
+        const uint32_t i = order[k];
+        d->codes[k] = keys[i];
+        std::memcpy(&d->positions[size_t{k} * 4], srcPos + size_t{i} * 4, 16);
+        std::memcpy(&d->shape[size_t{k} * 4], srcShape + size_t{i} * 4, 16);
+        if (d->shWords > 0) std::memcpy(&d->sh[size_t{k} * d->shWords], srcSh + size_t{i} * d->shWords, d->shWords * 4);
+    }
+    // Every level's groups (Lod.cpp:151-211).
+    struct LevelGroups {
+        uint32_t groups = 0;
+        std::vector<uint32_t> group, starts, cells;
+    };
+    std::vector<LevelGroups> lv(kOraLodLevels + 1);
+    auto groupsOf = [&](uint32_t level) {
+        const uint32_t shift = levelShiftOf(level);
+        std::vector<uint32_t> boundary(n), before(n);
+        for (uint32_t i = 0; i < n; ++i)   // lod_boundaries.slang
+            boundary[i] = (i == 0 || (d->codes[i] >> shift) != (d->codes[i - 1] >> shift)) ? 1u : 0u;
+        uint32_t total = 0;
+        for (uint32_t i = 0; i < n; ++i) before[i] = total, total += boundary[i];
+        LevelGroups& g = lv[level];
+        g.groups = total;
+        g.group.resize(n);
+        g.starts.resize(total);
+        g.cells.resize(total);
+        for (uint32_t i = 0; i < n; ++i) {   // lod_groups.slang
+            const uint32_t grp = before[i] + boundary[i] - 1;
+            g.group[i] = grp;
+            if (boundary[i] != 0) g.starts[grp] = i, g.cells[grp] = d->codes[i] >> shift;
+        }
+    };
+    const uint32_t coarsest = std::clamp<uint32_t>(coarsestLevel, 1, kOraLodLevels);
+    uint32_t finest = coarsest;
+    for (uint32_t level = coarsest; level <= kOraLodLevels; ++level) {
+        groupsOf(level);
+        if (static_cast<float>(lv[level].groups) > maxGroupFraction * static_cast<float>(n) && level > coarsest) break;
+        finest = level;
+    }
+    d->coarsest = coarsest;
+    d->finest = finest;
+    // Moments from the finest level up, a Gaussian per group (Lod.cpp:213-266).
+    const uint32_t stride = kOraMomentsHead + 3 * d->rest;
+    std::vector<float> fine;
+    std::vector<ora_lod::Level> stored;
+    for (uint32_t level = finest + 1; level-- > coarsest;) {
+        const LevelGroups& g = lv[level];
+        std::vector<float> moments(size_t{g.groups} * stride, 0.0f);
+        if (level == finest) {
+            for (uint32_t grp = 0; grp < g.groups; ++grp) {
+                const uint32_t end = grp + 1 < g.groups ? g.starts[grp + 1] : n;
+                leafMomentsOf(*d, g.starts[grp], end, &moments[size_t{grp} * stride]);
+            }
+        } else {   // lod_merge_moments.slang
+            const LevelGroups& f = lv[level + 1];
+            for (uint32_t grp = 0; grp < g.groups; ++grp) {
+                const uint32_t first = f.group[g.starts[grp]];
+                const uint32_t end = grp + 1 < g.groups ? f.group[g.starts[grp + 1]] : f.groups;
+                for (uint32_t k = 0; k < stride; ++k) {
+                    float sum = 0.0f;
+                    for (uint32_t h = first; h < end; ++h) sum += fine[size_t{h} * stride + k];
+                    moments[size_t{grp} * stride + k] = sum;
+                }
+            }
+        }
+        ora_lod::Level out;
+        out.level = level;
+        out.positions.resize(size_t{g.groups} * 4);
+        out.shape.resize(size_t{g.groups} * 4);
+        out.sh.resize(size_t{g.groups} * d->shWords);
+        out.cells = g.cells;
+        for (uint32_t grp = 0; grp < g.groups; ++grp)
+            finalizeOf(&moments[size_t{grp} * stride], d->rest, d->shWords, &out.positions[size_t{grp} * 4],
+                       &out.shape[size_t{grp} * 4], out.sh.data() + size_t{grp} * d->shWords);
+        if (level == finest) d->groups = g.group, d->starts = g.starts;
+        stored.push_back(std::move(out));
+        fine = std::move(moments);
+    }
+    std::reverse(stored.begin(), stored.end());
+    d->levels = std::move(stored);
+    *out = d.release();
+    return LRT_OK;
+}
+
+void ora_lod_free(ora_lod* d) { delete d; }
+
+int ora_lod_describe(const ora_lod* d, lrt_lod_info* out) {
+    if (d == nullptr || out == nullptr) return LRT_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    out->count = d->count;
+    out->rest_per_colour = d->rest;
+    out->sh_words = d->shWords;
+    out->levels = static_cast<uint32_t>(d->levels.size());
+    out->coarsest = d->coarsest;
+    out->finest = d->finest;
+    for (int k = 0; k < 3; ++k) out->bounds_lo[k] = d->lo[k], out->bounds_hi[k] = d->hi[k];
+    out->extent = d->extent;
+    for (size_t l = 0; l < d->levels.size(); ++l) {
+        out->level_groups[l] = static_cast<uint32_t>(d->levels[l].cells.size());
+        out->merged += out->level_groups[l];
+    }
+    return LRT_OK;
+}
+
+// which: 0 store positions, 1 store shape, 2 store sh, 3 codes, 4 finest starts,
+// 5 merged positions, 6 merged shape, 7 merged sh, 8 cells (all levels, coarsest first).
+int ora_lod_copy(const ora_lod* d, int which, void* dst) {
+    if (d == nullptr || dst == nullptr) return LRT_INVALID_ARGUMENT;
+    auto put = [&](const void* src, size_t bytes) {
+        if (bytes > 0) std::memcpy(dst, src, bytes);
+        dst = static_cast<char*>(dst) + bytes;
+    };
+    switch (which) {
+        case 0: put(d->positions.data(), d->positions.size() * 4); break;
+        case 1: put(d->shape.data(), d->shape.size() * 4); break;
+        case 2: put(d->sh.data(), d->sh.size() * 4); break;
+        case 3: put(d->codes.data(), d->codes.size() * 4); break;
+        case 4: put(d->starts.data(), d->starts.size() * 4); break;
+        case 5: for (const auto& l : d->levels) put(l.positions.data(), l.positions.size() * 4); break;
+        case 6: for (const auto& l : d->levels) put(l.shape.data(), l.shape.size() * 4); break;
+        case 7: for (const auto& l : d->levels) put(l.sh.data(), l.sh.size() * 4); break;
+        case 8: for (const auto& l : d->levels) put(l.cells.data(), l.cells.size() * 4); break;
+        default: return LRT_INVALID_ARGUMENT;
+    }
+    return LRT_OK;
+}
+
+// CutSelector::select for one instance, every chunk resident: the drawn cloud
+// (capacity: the cloud's splat count) and its counts.
+int ora_lod_cut(const ora_lod* d, const lrt_projection* pr, const double objectToWorld[16], float threshold,
+                float* positions, uint32_t* shape, uint32_t* sh, uint32_t* splats, uint32_t* merged) {
+    if (d == nullptr || pr == nullptr || objectToWorld == nullptr) return LRT_INVALID_ARGUMENT;
+    OraCut c{};
+    for (int k = 0; k < 3; ++k) c.lo[k] = d->lo[k];
+    c.extent = d->extent;
+    const M4 toWorld = toM4(objectToWorld);   // Lod.cpp:400-408
+    const D3 eye = pointOf(inverseAffine(toWorld), D3{pr->eye_world[0], pr->eye_world[1], pr->eye_world[2]});
+    c.eye[0] = static_cast<float>(eye.x), c.eye[1] = static_cast<float>(eye.y), c.eye[2] = static_cast<float>(eye.z);
+    double scale = 0.0;
+    for (int col = 0; col < 3; ++col)
+        scale = std::max(scale, lengthd(D3{toWorld.at(0, col), toWorld.at(1, col), toWorld.at(2, col)}));
+    c.pixelsPerUnit = static_cast<float>(pr->orthographic ? pr->focal_x * scale : pr->focal_x);
+    c.threshold = threshold;
+    c.ortho = pr->orthographic != 0;
+    const size_t parts = d->levels.size();
+    std::vector<std::vector<uint32_t>> selected(parts + 1);
+    std::vector<uint32_t> state;
+    for (size_t part = 0; part < parts; ++part) {   // lodCutGroups, lodCutFinest
+        const ora_lod::Level& l = d->levels[part];
+        selected[part].resize(l.cells.size());
+        const bool finest = part + 1 == parts;
+        if (finest) state.resize(l.cells.size());
+        for (size_t g = 0; g < l.cells.size(); ++g) {
+            const bool here = c.small(l.cells[g], l.level);
+            const bool above = part != 0 && c.small(l.cells[g] >> 3, l.level - 1);
+            selected[part][g] = (here && !above) ? 1u : 0u;
+            if (finest) state[g] = (here ? 0u : 1u) | (!here ? 2u : 0u);
+        }
+    }
+    selected[parts].resize(d->count);   // lodCutSplats
+    for (uint32_t i = 0; i < d->count; ++i) selected[parts][i] = (state[d->groups[i]] & 2u) != 0 ? 1u : 0u;
+    uint32_t drawn = 0, drawnMerged = 0;
+    for (size_t part = 0; part <= parts; ++part) {   // prefix sums and lodGather, in part order
+        const bool isMerged = part < parts;
+        const float* srcPos = isMerged ? d->levels[part].positions.data() : d->positions.data();
+        const uint32_t* srcShape = isMerged ? d->levels[part].shape.data() : d->shape.data();
+        const uint32_t* srcSh = isMerged ? d->levels[part].sh.data() : d->sh.data();
+        for (size_t i = 0; i < selected[part].size(); ++i) {
+            if (selected[part][i] == 0) continue;
+            if (drawn < d->count) {
+                if (positions) std::memcpy(positions + size_t{drawn} * 4, srcPos + i * 4, 16);
+                if (shape) std::memcpy(shape + size_t{drawn} * 4, srcShape + i * 4, 16);
+                if (sh && d->shWords > 0) std::memcpy(sh + size_t{drawn} * d->shWords, srcSh + i * d->shWords, d->shWords * 4);
+            }
+            ++drawn;
+            if (isMerged) ++drawnMerged;
+        }
+    }
+    if (splats) *splats = drawn - drawnMerged;
+    if (merged) *merged = drawnMerged;
+    return drawn <= d->count ? LRT_OK : LRT_INTERNAL_ERROR;
+}
+
+}  // extern "C"

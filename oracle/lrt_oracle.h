@@ -126,6 +126,24 @@ uint64_t ora_count_different(const uint32_t* a, const uint32_t* b, uint32_t coun
 int ora_random_cloud(uint32_t count, uint64_t seed, float min_size, float max_size,
                      float min_opacity, float max_opacity, float* raw);
 
+/* Levels of detail (LodBuilder::build, CutSelector::select), host pointers
+ * in `cloud`. Built in the reference's own schedule: a stable sort, one
+ * boundary pass and prefix sum per level, merges through the per-splat group
+ * index. ora_lod_describe fills an lrt_lod_info (chunk_splats 0). */
+typedef struct ora_lod ora_lod;
+int ora_lod_build(const lrt_gpu_splats* cloud, const float* bounds, float max_group_fraction,
+                  uint32_t coarsest_level, ora_lod** out);
+void ora_lod_free(ora_lod* lod);
+int ora_lod_describe(const ora_lod* lod, lrt_lod_info* out);
+/* which: 0 store positions, 1 store shape, 2 store sh, 3 codes, 4 finest
+ * starts, 5 merged positions, 6 merged shape, 7 merged sh, 8 cells (all
+ * levels, coarsest first). */
+int ora_lod_copy(const ora_lod* lod, int which, void* dst);
+/* One instance's cut; the outputs hold the cloud's splat count. */
+int ora_lod_cut(const ora_lod* lod, const lrt_projection* projection, const double object_to_world[16],
+                float threshold, float* positions, uint32_t* shape, uint32_t* sh, uint32_t* splats,
+                uint32_t* merged);
+
 #ifdef __cplusplus
 }
 #endif

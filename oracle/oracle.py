@@ -89,6 +89,14 @@ def load() -> C.CDLL:
     lib.ora_f32_to_f16.restype = C.c_uint16
     lib.ora_f16_to_f32.argtypes = [C.c_uint16]
     lib.ora_f16_to_f32.restype = C.c_float
+    lib.ora_lod_build.argtypes = [C.POINTER(_abi.GpuSplatsStruct), C.c_void_p, C.c_float, C.c_uint32,
+                                  C.POINTER(C.c_void_p)]
+    lib.ora_lod_free.argtypes = [C.c_void_p]
+    lib.ora_lod_free.restype = None
+    lib.ora_lod_describe.argtypes = [C.c_void_p, C.POINTER(_abi.LodInfo)]
+    lib.ora_lod_copy.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    lib.ora_lod_cut.argtypes = [C.c_void_p, C.POINTER(_abi.Projection), C.POINTER(C.c_double), C.c_float, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     _lib = lib
     return lib
 
@@ -418,3 +426,86 @@ def train_render(projection: _abi.Projection, cloud: RawCloud, settings: _abi.Re
            "train_render")
     return dict(colour=colour, depth=depth, proj=proj, rects=rects, touched=touched, depth_keys=keys, ranges=ranges,
                 pairs=int(out.pairs), visible=int(out.visible), list_offsets=offsets, list_slots=slots[:total.value])
+
+
+# ------------------------------------------------------------------- LOD ----
+class OracleLod:
+    """The restated levels of detail of one host cloud (ora_lod_build)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        self.info = _abi.LodInfo()
+        _check(load().ora_lod_describe(handle, C.byref(self.info)), "lod_describe")
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                load().ora_lod_free(self._h)
+                self._h = None
+        except Exception:   # at interpreter exit the module may be gone
+            pass
+
+    def _copy(self, which: int, shape: tuple, dtype) -> np.ndarray:
+        out = np.zeros(shape, dtype)
+        _check(load().ora_lod_copy(self._h, which, out.ctypes.data), "lod_copy")
+        return out
+
+    @property
+    def count(self) -> int:
+        return int(self.info.count)
+
+    @property
+    def level_groups(self) -> list[int]:
+        return [int(v) for v in self.info.level_groups[:self.info.levels]]
+
+    @property
+    def store(self) -> HostCloud:
+        """The splats in Morton order."""
+        n, w = self.count, int(self.info.sh_words)
+        return HostCloud(self._copy(0, (n, 4), np.float32), self._copy(1, (n, 4), np.uint32),
+                         self._copy(2, (n, w), np.uint32), int(self.info.rest_per_colour))
+
+    @property
+    def codes(self) -> np.ndarray:
+        return self._copy(3, (self.count,), np.uint32)
+
+    @property
+    def starts(self) -> np.ndarray:
+        return self._copy(4, (self.level_groups[-1],), np.uint32)
+
+    @property
+    def merged(self) -> HostCloud:
+        """Every stored level's Gaussians, coarsest level first."""
+        m, w = int(self.info.merged), int(self.info.sh_words)
+        return HostCloud(self._copy(5, (m, 4), np.float32), self._copy(6, (m, 4), np.uint32),
+                         self._copy(7, (m, w), np.uint32), int(self.info.rest_per_colour))
+
+    @property
+    def cells(self) -> np.ndarray:
+        return self._copy(8, (int(self.info.merged),), np.uint32)
+
+    def cut(self, projection: _abi.Projection, object_to_world=None, threshold: float = 0.0):
+        """The drawn cloud of one instance and (splats, merged) drawn."""
+        n, w = self.count, int(self.info.sh_words)
+        pos = np.zeros((n, 4), np.float32)
+        shape = np.zeros((n, 4), np.uint32)
+        sh = np.zeros((n, w), np.uint32)
+        m = np.eye(4) if object_to_world is None else np.asarray(object_to_world, np.float64)
+        mat = (C.c_double * 16)(*[float(v) for v in m.reshape(16)])
+        splats, merged = C.c_uint32(), C.c_uint32()
+        _check(load().ora_lod_cut(self._h, C.byref(projection), mat, float(threshold), pos.ctypes.data,
+                                  shape.ctypes.data, sh.ctypes.data, C.byref(splats), C.byref(merged)), "lod_cut")
+        k = splats.value + merged.value
+        return HostCloud(pos[:k].copy(), shape[:k].copy(), sh[:k].copy(), int(self.info.rest_per_colour)), \
+            splats.value, merged.value
+
+
+def lod_build(cloud: HostCloud, bounds=None, max_group_fraction: float = 0.5, coarsest_level: int = 1) -> OracleLod:
+    cs = cloud.struct()
+    b = None
+    if bounds is not None:
+        b = (C.c_float * 6)(*[float(v) for v in np.asarray(bounds, np.float32).reshape(6)])
+    h = C.c_void_p()
+    _check(load().ora_lod_build(C.byref(cs), b, float(max_group_fraction), int(coarsest_level), C.byref(h)),
+           "lod_build")
+    return OracleLod(h)

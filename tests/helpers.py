@@ -213,3 +213,65 @@ def fog_records(count: int = 40) -> np.ndarray:
         colour = (rng.range(0, 1), rng.range(0, 1), rng.range(0, 1))
         out.append(cloud_record(x, y, z, opacity, sx, sy, sz, (1, 0, 0, 0), colour))
     return np.stack(out)
+
+
+class FixtureLcg(Lcg):
+    """tests/render/SplatFixtures.h:48-55: the same generator from its own state."""
+
+    def __init__(self):
+        self.state = 0x853C49E6748FEA9B
+
+
+def single_splat_cells_records() -> np.ndarray:
+    """tests/lod/test_lod.cpp:112-130: six splats, one to a level-1 cell, drawn
+    in the order the reference names them (opacity, three sizes, the turn, the
+    colour)."""
+    rng = FixtureLcg()
+    at = [(-2, -2, -2), (2, -2, -2), (-2, 2, -2), (2, 2, 2), (-2, 2, 2), (2, -2, 2)]
+    rest = [0.2, -0.1, 0.3, 0.0, 0.1, -0.2, 0.1, 0.0, -0.3]
+    out = []
+    for p in at:
+        opacity = rng.range(0.3, 0.95)
+        sx, sy, sz = rng.range(0.1, 0.5), rng.range(0.1, 0.5), rng.range(0.1, 0.5)
+        turn = (rng.range(-1, 1), rng.range(-1, 1), rng.range(-1, 1), rng.range(-1, 1))
+        colour = (rng.range(0.1, 1.0), rng.range(0.1, 1.0), rng.range(0.1, 1.0))
+        out.append(cloud_record(*p, opacity, sx, sy, sz, turn, colour, rest))
+    return np.stack(out)
+
+
+def morton_codes(positions: np.ndarray, lo, extent) -> np.ndarray:
+    """morton.slang:23-28 in numpy float32: 10 bits an axis, x highest."""
+    unit = (positions[:, :3].astype(np.float32) - np.asarray(lo, np.float32)) / np.float32(max(extent, 1e-20))
+    q = np.minimum((np.clip(unit, 0, 1) * np.float32(1024.0)).astype(np.uint32), 1023)
+    code = np.zeros(len(positions), np.uint32)
+    for b in range(10):
+        for axis, shift in ((0, 2), (1, 1), (2, 0)):
+            code |= ((q[:, axis] >> b) & 1) << np.uint32(3 * b + shift)
+    return code
+
+
+def cell_axes(cells: np.ndarray, level: int) -> np.ndarray:
+    """morton.slang:30-33: per cell its index on x, y, z."""
+    out = np.zeros((len(cells), 3), np.uint32)
+    for b in range(level):
+        for axis, shift in ((0, 2), (1, 1), (2, 0)):
+            out[:, axis] |= ((cells >> np.uint32(3 * b + shift)) & 1) << np.uint32(b)
+    return out
+
+
+def projected_edge(cells: np.ndarray, level: int, lo, extent: float, eye, pixels_per_unit: float,
+                   orthographic: bool = False) -> np.ndarray:
+    """lod_cut.slang:15-26 in numpy float32, one rounding per operation."""
+    f = np.float32
+    edge = f(extent) / f(1 << level)
+    if orthographic:
+        return np.full(len(cells), edge * f(pixels_per_unit), np.float32)
+    idx = cell_axes(cells, level).astype(np.float32)
+    eye = np.asarray(eye, np.float32)
+    d = []
+    for k in range(3):
+        low = f(lo[k]) + idx[:, k] * edge
+        nearest = np.minimum(np.maximum(eye[k], low), low + edge)
+        d.append(nearest - eye[k])
+    dist = np.maximum(np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), f(1e-6))
+    return (edge * f(pixels_per_unit)) / dist

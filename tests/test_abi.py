@@ -54,6 +54,10 @@ int main(void) {
   S(lrt_train_params) O(lrt_train_params, sh) S(lrt_train_grads) O(lrt_train_grads, sh)
   S(lrt_gpu_points) O(lrt_gpu_points, colours) S(lrt_point_style) O(lrt_point_style, colour)
   S(lrt_point_instance) O(lrt_point_instance, style)
+  S(lrt_lod_build_settings) O(lrt_lod_build_settings, chunk_splats)
+  S(lrt_lod_info) O(lrt_lod_info, extent) O(lrt_lod_info, level_groups)
+  S(lrt_lod_instance) O(lrt_lod_instance, edit) O(lrt_lod_instance, threshold)
+  S(lrt_cut_stats) O(lrt_cut_stats, available)
   return 0;
 }
 """
@@ -65,7 +69,8 @@ CTYPES = {
     "lrt_frame_stats": _abi.FrameStatsStruct, "lrt_targets": _abi.TargetsStruct, "lrt_debug_view": _abi.DebugView,
     "lrt_train_params": _abi.TrainParams, "lrt_train_grads": _abi.TrainGrads,
     "lrt_gpu_points": _abi.GpuPointsStruct, "lrt_point_style": _abi.PointStyleStruct,
-    "lrt_point_instance": _abi.PointInstanceStruct,
+    "lrt_point_instance": _abi.PointInstanceStruct, "lrt_lod_build_settings": _abi.LodBuildSettings,
+    "lrt_lod_info": _abi.LodInfo, "lrt_lod_instance": _abi.LodInstanceStruct, "lrt_cut_stats": _abi.CutStatsStruct,
 }
 
 
@@ -118,6 +123,13 @@ def test_host_entry_points_validate_arguments():
     assert lib.lrt_rast_create(None, 0) == _abi.INVALID_ARGUMENT
     assert lib.lrt_rast_render(None, None, None, 0, None, None, None, None) == _abi.INVALID_ARGUMENT
     assert lib.lrt_math_eval(7, None, None, 0, None) == _abi.INVALID_ARGUMENT
+    settings = _abi.LodBuildSettings()
+    assert lib.lrt_lod_build_settings_default(C.byref(settings)) == _abi.OK
+    assert (round(settings.max_group_fraction, 6), settings.coarsest_level, settings.chunk_splats) == (0.5, 1, 65536)
+    assert lib.lrt_lod_build(None, None, None, None, None, None) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_lod_select(None, None, None, 0, 0.0, None, None, None, None) == _abi.INVALID_ARGUMENT
+    assert lib.lrt_lod_get_info(None, None) == _abi.INVALID_ARGUMENT
+    lib.lrt_lod_destroy(None)
 
 
 def test_device_entry_points_fail_cleanly_without_a_device():
