@@ -43,7 +43,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + written) of one launch, from ncu (`dram__bytes_read.sum +
 # dram__bytes_write.sum`) on frame 3 of this orbit; the capture and its command
 # are summarised under profiles/.
-PROFILED_DRAM_BYTES = {"blend": 63.688192e6 + 16.780544e6}
+PROFILED_DRAM_BYTES = {"blend": 63.371776e6 + 15.835392e6}
 
 
 def orbit_camera(L, k: int):

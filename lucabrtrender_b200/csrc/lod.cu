@@ -97,23 +97,36 @@ lod_bounds_partial_kernel(const float4* __restrict__ positions, uint32_t count, 
 // The cloud's bounds (the caller's when given) and the cubic extent of
 // Lod.cpp:91-97: the largest edge, at least 1e-6, times 1.0001 so the far
 // corner quantises inside the last cell.
-__global__ void lod_bounds_final_kernel(const float* __restrict__ partial, uint32_t blocks,
-                                        const float* __restrict__ given, LodGlobals* __restrict__ g) {
-    if (threadIdx.x != 0) return;
-    float lo[3], hi[3];
-    for (int k = 0; k < 3; ++k) {
-        if (given != nullptr) {
-            lo[k] = given[k], hi[k] = given[3 + k];
-        } else {
-            lo[k] = 3.4e38f, hi[k] = -3.4e38f;
-            for (uint32_t b = 0; b < blocks; ++b)
-                lo[k] = fminf(lo[k], partial[b * 6 + k]), hi[k] = fmaxf(hi[k], partial[b * 6 + 3 + k]);
-        }
+__global__ void __launch_bounds__(kLodThreads)
+lod_bounds_final_kernel(const float* __restrict__ partial, uint32_t blocks, const float* __restrict__ given,
+                        LodGlobals* __restrict__ g) {
+    __shared__ float sLo[3][kLodThreads / 32], sHi[3][kLodThreads / 32];
+    float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (uint32_t b = threadIdx.x; given == nullptr && b < blocks; b += kLodThreads) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) lo[k] = fminf(lo[k], partial[b * 6 + k]), hi[k] = fmaxf(hi[k], partial[b * 6 + 3 + k]);
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fminf(lo[k], __shfl_xor_sync(0xFFFFFFFFu, lo[k], o));
+            hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xFFFFFFFFu, hi[k], o));
+        }
+        if ((threadIdx.x & 31u) == 0) sLo[k][threadIdx.x >> 5] = lo[k], sHi[k][threadIdx.x >> 5] = hi[k];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     float extent = 0.0f;
     for (int k = 0; k < 3; ++k) {
-        g->lo[k] = lo[k], g->hi[k] = hi[k];
-        const float edge = hi[k] - lo[k];
+        float l = 3.4e38f, h = -3.4e38f;
+        if (given != nullptr) {
+            l = given[k], h = given[3 + k];
+        } else {
+            for (uint32_t w = 0; w < kLodThreads / 32; ++w) l = fminf(l, sLo[k][w]), h = fmaxf(h, sHi[k][w]);
+        }
+        g->lo[k] = l, g->hi[k] = h;
+        const float edge = h - l;
         extent = extent < edge ? edge : extent;
     }
     extent = extent < 1e-6f ? 1e-6f : extent;
@@ -302,19 +315,21 @@ lod_leaf_moments_kernel(LodSplatArrays store, uint32_t count, uint32_t shWords, 
 }
 
 // lod_merge_moments.slang:19-31: a coarser group's moments, its children's
-// summed in child order.
-__global__ void __launch_bounds__(kMomentThreads)
+// summed in child order. One thread per (group, moment), moments fastest, so
+// a warp's loads of one child's row are contiguous; each sum still runs over
+// the children in order, as the reference's per-group loop does.
+__global__ void __launch_bounds__(kLodThreads)
 lod_merge_moments_kernel(const uint32_t* __restrict__ firstChild, uint32_t groups, uint32_t fineGroups,
                          const float* __restrict__ fine, float* __restrict__ moments, uint32_t stride) {
-    const uint32_t g = blockIdx.x * kMomentThreads + threadIdx.x;
-    if (g >= groups) return;
+    const size_t t = static_cast<size_t>(blockIdx.x) * kLodThreads + threadIdx.x;
+    if (t >= static_cast<size_t>(groups) * stride) return;
+    const uint32_t g = static_cast<uint32_t>(t / stride);
+    const uint32_t k = static_cast<uint32_t>(t - static_cast<size_t>(g) * stride);
     const uint32_t first = min(__ldg(firstChild + g), fineGroups);
     const uint32_t end = min(g + 1 < groups ? __ldg(firstChild + g + 1) : fineGroups, fineGroups);
-    for (uint32_t k = 0; k < stride; ++k) {
-        float sum = 0.0f;
-        for (uint32_t h = first; h < end; ++h) sum = sum + __ldg(fine + static_cast<size_t>(h) * stride + k);
-        moments[static_cast<size_t>(g) * stride + k] = sum;
-    }
+    float sum = 0.0f;
+    for (uint32_t h = first; h < end; ++h) sum = sum + __ldg(fine + static_cast<size_t>(h) * stride + k);
+    moments[t] = sum;
 }
 
 // ----------------------------------------------------------- finalize ------
@@ -551,7 +566,7 @@ cudaError_t launch_lod_bounds(const float4* positions, uint32_t count, const flo
         blocks = std::max<uint32_t>(1u, std::min(kBoundsBlocks, blocks_for(count, kLodThreads)));
         lod_bounds_partial_kernel<<<blocks, kLodThreads, 0, stream>>>(positions, count, partial);
     }
-    lod_bounds_final_kernel<<<1, 32, 0, stream>>>(partial, blocks, given, globals);
+    lod_bounds_final_kernel<<<1, kLodThreads, 0, stream>>>(partial, blocks, given, globals);
     return cudaGetLastError();
 }
 
@@ -613,8 +628,9 @@ cudaError_t launch_lod_leaf_moments(const LodSplatArrays store, uint32_t count, 
 cudaError_t launch_lod_merge_moments(const uint32_t* firstChild, uint32_t groups, uint32_t fineGroups,
                                      const float* fineMoments, float* moments, uint32_t stride, cudaStream_t stream) {
     if (groups == 0) return cudaSuccess;
-    lod_merge_moments_kernel<<<blocks_for(groups, kMomentThreads), kMomentThreads, 0, stream>>>(
-        firstChild, groups, fineGroups, fineMoments, moments, stride);
+    const size_t threads = static_cast<size_t>(groups) * stride;
+    lod_merge_moments_kernel<<<static_cast<uint32_t>((threads + kLodThreads - 1) / kLodThreads), kLodThreads, 0,
+                               stream>>>(firstChild, groups, fineGroups, fineMoments, moments, stride);
     return cudaGetLastError();
 }
 

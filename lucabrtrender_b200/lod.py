@@ -45,16 +45,17 @@ class LodBuildSettings:
 
 
 def _view(s: _abi.GpuSplatsStruct, device: int) -> GpuSplats:
-    """A GpuSplats whose tensors view library-owned memory."""
+    """A GpuSplats whose tensors view library-owned memory (the calls that
+    return these clouds have waited for them)."""
     n, words = int(s.count), int(s.sh_words)
     if n == 0:
         dev = torch.device("cuda", device)
         return GpuSplats(torch.empty((0, 4), dtype=torch.float32, device=dev),
                          torch.empty((0, 4), dtype=torch.int32, device=dev),
                          torch.empty((0, words), dtype=torch.int32, device=dev), int(s.rest_per_colour))
-    return GpuSplats(device_view(s.positions, (n, 4), torch.float32, device),
-                     device_view(s.shape, (n, 4), torch.int32, device),
-                     device_view(s.sh, (n, words), torch.int32, device) if words else
+    return GpuSplats(device_view(s.positions, (n, 4), torch.float32, device, sync=False),
+                     device_view(s.shape, (n, 4), torch.int32, device, sync=False),
+                     device_view(s.sh, (n, words), torch.int32, device, sync=False) if words else
                      torch.empty((n, 0), dtype=torch.int32, device=torch.device("cuda", device)),
                      int(s.rest_per_colour))
 

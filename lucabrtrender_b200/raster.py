@@ -455,9 +455,11 @@ class _DeviceArray:
                                          "data": (int(ptr), False), "version": 3, "strides": None}
 
 
-def device_view(ptr: int, shape: tuple, dtype: torch.dtype, device: int) -> torch.Tensor:
-    """A tensor viewing library-owned device memory (valid until the next call on the handle)."""
-    torch.cuda.synchronize(device)
+def device_view(ptr: int, shape: tuple, dtype: torch.dtype, device: int, sync: bool = True) -> torch.Tensor:
+    """A tensor viewing library-owned device memory (valid until the next call on the handle).
+    `sync`: wait for the device first (callers whose call already waited pass False)."""
+    if sync:
+        torch.cuda.synchronize(device)
     return torch.as_tensor(_DeviceArray(ptr, shape, dtype), device=torch.device("cuda", device))
 
 
