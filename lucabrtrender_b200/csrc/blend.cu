@@ -282,7 +282,7 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                 const float4 conic = batch[j].conic;
                 const float dx = pxf - screen.x;
                 const float dy = pyf - screen.y;
-                const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
+                const float power = splat_power(conic, dx, dy);
                 const bool candidate = !done && !(power > screen.w) && (!kComposite || at + j < stopAt);
                 if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
                 bool blendIt = candidate;
@@ -304,10 +304,12 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                 if (blendIt && !(alpha < 1.0f / 255.0f)) {
                     const float4 colour = batch[j].colour;
                     const float weight = T * alpha;
-                    r = r + weight * colour.x;
-                    g = g + weight * colour.y;
-                    b = b + weight * colour.z;
-                    depthSum = depthSum + weight * screen.z;
+                    // rgb += weight colour, depthSum += weight z
+                    // (splat_blend.slang:72-74), each one multiply-add.
+                    r = __fmaf_rn(weight, colour.x, r);
+                    g = __fmaf_rn(weight, colour.y, g);
+                    b = __fmaf_rn(weight, colour.z, b);
+                    depthSum = __fmaf_rn(weight, screen.z, depthSum);
                     T = T * (1.0f - alpha);
                     if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
                     if (kTrain) last = at + j + 1;
@@ -616,7 +618,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                 const float4 conic = sRec[j].conic;
                 const float dx = pxf - screen.x;
                 const float dy = pyf - screen.y;
-                const float power = conic.x * dx * dx + 2.0f * conic.y * dx * dy + conic.z * dy * dy;
+                const float power = splat_power(conic, dx, dy);
                 const bool candidate = live && bStart + j < myLast && !(power > screen.w);
                 if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
                 // The forward's alpha decides who contributed, so it is taken

@@ -58,6 +58,17 @@ struct __align__(16) ProjRecord {
     float4 colour;   // rgb (encoded), 0
 };
 
+// splat_blend.slang:58: a Gaussian's power at pixel offset (dx, dy),
+// a dx^2 + 2 b dx dy + c dy^2, evaluated left to right with its two sums
+// fused into multiply-adds (the contraction a GPU compiler makes of the
+// reference's expression). The blend, its backward and the CPU restatement
+// all use this form, so they agree on every pair's contribution bit for bit.
+__device__ __forceinline__ float splat_power(float4 conic, float dx, float dy) {
+    const float t = conic.x * dx * dx;
+    const float u = __fmaf_rn(2.0f * conic.y * dx, dy, t);
+    return __fmaf_rn(conic.z * dy, dy, u);
+}
+
 // Status bits a kernel may raise in the frame's error word.
 constexpr uint32_t kErrOverflow = 1u;
 constexpr uint32_t kErrTimeout = 2u;

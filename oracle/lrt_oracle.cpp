@@ -804,7 +804,10 @@ void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t*
         if (underHit && rec.screen[2] >= underZ) break;
         const float dx = pxf - rec.screen[0];
         const float dy = pyf - rec.screen[1];
-        const float power = rec.conic[0] * dx * dx + 2.0f * rec.conic[1] * dx * dy + rec.conic[2] * dy * dy;
+        // splat_blend.slang:58, its two sums fused as a GPU compiler contracts them.
+        const float t = rec.conic[0] * dx * dx;
+        const float u = std::fma(2.0f * rec.conic[1] * dx, dy, t);
+        const float power = std::fma(rec.conic[2] * dy, dy, u);
         if (power > rec.screen[3]) continue;
         if (composite && rec.colour[3] > 0.5f) {
             opaqueHit = true;
@@ -818,10 +821,10 @@ void blendPixel(const Frame& f, const std::vector<Record>& proj, const uint32_t*
         const float alpha = std::fmin(0.99f, rec.conic[3] * expImpl(-0.5f * power));
         if (alpha < 1.0f / 255.0f) continue;
         const float weight = T * alpha;
-        rgb[0] = rgb[0] + weight * rec.colour[0];
-        rgb[1] = rgb[1] + weight * rec.colour[1];
-        rgb[2] = rgb[2] + weight * rec.colour[2];
-        depthSum = depthSum + weight * rec.screen[2];
+        rgb[0] = std::fma(weight, rec.colour[0], rgb[0]);   // splat_blend.slang:72-74, fused
+        rgb[1] = std::fma(weight, rec.colour[1], rgb[1]);
+        rgb[2] = std::fma(weight, rec.colour[2], rgb[2]);
+        depthSum = std::fma(weight, rec.screen[2], depthSum);
         T = T * (1.0f - alpha);
         if (depthAt < 0.0f && 1.0f - T >= f.depthThreshold) depthAt = rec.screen[2];
         if (contributors != nullptr) contributors->push_back(pairSlots[k]);
