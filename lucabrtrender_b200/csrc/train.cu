@@ -67,6 +67,10 @@ __device__ __forceinline__ void sum_partials(const float4* __restrict__ part, ui
     }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __global__ void __launch_bounds__(kThreads, 4)
 splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
                       const float* __restrict__ quats, const float* __restrict__ logits,
@@ -78,8 +82,20 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     const uint32_t lane = threadIdx.x & 31u;
     const bool live = i < f.count;
     const uint32_t slot = f.base + i;
+    // The parameters and SH row are read only after the partials are summed;
+    // ask for them now (into L2, no registers held), so their DRAM latency
+    // overlaps the count, offset and partial loads that each wait on the last.
+    if (live) {
+        prefetch_l2(means + 3 * static_cast<size_t>(i));
+        prefetch_l2(logScales + 3 * static_cast<size_t>(i));
+        prefetch_l2(quats + 4 * static_cast<size_t>(i));
+        prefetch_l2(logits + i);
+        prefetch_l2(sh + 48 * static_cast<size_t>(i));
+        prefetch_l2(sh + 48 * static_cast<size_t>(i) + 40);
+    }
     uint32_t n = live ? touched[slot] : 0u;
-    const uint32_t first = n != 0 ? offsets[slot] : 0u;
+    const uint32_t firstRaw = live ? offsets[slot] : 0u;   // loaded beside the count, not after it
+    const uint32_t first = n != 0 ? firstRaw : 0u;
     // Reads stay inside the partials buffer even for a frame whose pairs
     // overflowed their buffer (the host reports that frame as an error).
     n = first >= partialPairs ? 0u : min(n, partialPairs - first);

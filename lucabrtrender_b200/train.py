@@ -25,21 +25,31 @@ from .raster import FrameStats, RenderSettings, TileRasterizer, _stream_ptr
 class _Rasterize(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, log_scales, quats, opacity_logits, sh, raster: TileRasterizer, projection: Projection,
-                settings: RenderSettings, sort_values: bool):
+                settings: RenderSettings, sort_values: bool, grad_bucket, sh_storage):
         dev = means.device
         n = means.shape[0]
         means = means.contiguous().float()
         log_scales = log_scales.contiguous().float()
         quats = quats.contiguous().float()
         opacity_logits = opacity_logits.contiguous().float()
-        sh16 = sh.detach().reshape(n, 48).to(torch.float16).contiguous()
+        if sh_storage is not None:
+            # The caller's fp16 working copy of `sh` (kept in step with it by
+            # the optimizer): read as it is, no conversion this step.
+            if (sh_storage.dtype != torch.float16 or sh_storage.numel() != n * 48 or
+                    not sh_storage.is_contiguous() or sh_storage.data_ptr() % 16 != 0 or
+                    sh_storage.device != sh.device):
+                raise ValueError("sh_storage must be a contiguous, 16-byte aligned fp16 tensor of N x 48 "
+                                 "coefficients on the parameters' device")
+            shk = sh_storage.detach().reshape(n, 48)
+        else:
+            shk = sh.detach().reshape(n, 48).to(torch.float16).contiguous()
         colour = torch.empty((settings.height, settings.width, 4), dtype=torch.float32, device=dev)
         depth = torch.empty((settings.height, settings.width), dtype=torch.float32, device=dev)
         p = _abi.TrainParams()
         p.count = n
         p.flags = _abi.TRAIN_SORT_VALUES if sort_values else 0
         p.means, p.log_scales, p.quats = means.data_ptr(), log_scales.data_ptr(), quats.data_ptr()
-        p.opacity_logits, p.sh = opacity_logits.data_ptr(), sh16.data_ptr()
+        p.opacity_logits, p.sh = opacity_logits.data_ptr(), shk.data_ptr()
         t = _abi.TargetsStruct()
         t.width, t.height, t.colour, t.depth = settings.width, settings.height, colour.data_ptr(), depth.data_ptr()
         pr = projection.struct()
@@ -48,18 +58,29 @@ class _Rasterize(torch.autograd.Function):
         raster._check(_abi.load().lrt_rast_train_forward(raster._handle, C.byref(pr), C.byref(p), C.byref(st),
                                                          C.byref(t), C.byref(stats), _stream_ptr(None)))
         ctx.raster = raster
+        ctx.grad_bucket = grad_bucket
+        ctx.shapes = [t.shape for t in (means, log_scales, quats, opacity_logits, sh)]
         raster.last_train_stats = FrameStats.from_struct(stats)
         # The handle keeps pointers to these until the backward.
-        ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh16)
+        ctx.save_for_backward(means, log_scales, quats, opacity_logits, shk)
         ctx.mark_non_differentiable(depth)
+        ctx.set_materialize_grads(False)   # no zero image for the depth's gradient
         return colour, depth
 
     @staticmethod
     def backward(ctx, grad_colour, grad_depth):
-        means, log_scales, quats, opacity_logits, sh16 = ctx.saved_tensors
+        means, log_scales, quats, opacity_logits, _ = ctx.saved_tensors
+        if grad_colour is None:
+            return None, None, None, None, None, None, None, None, None, None, None
         n = means.shape[0]
-        g = [torch.empty_like(means), torch.empty_like(log_scales), torch.empty_like(quats),
-             torch.empty_like(opacity_logits), torch.empty((n, 16, 3), dtype=torch.float32, device=means.device)]
+        bucket = ctx.grad_bucket
+        if bucket is not None and bucket.count == n:
+            # Fresh views of the bucket (no other reference), so autograd keeps
+            # them as the parameters' .grad rather than copying.
+            g = [bucket.slice(name).view(shape) for name, shape in zip(bucket.ORDER, ctx.shapes)]
+        else:
+            g = [torch.empty_like(means), torch.empty_like(log_scales), torch.empty_like(quats),
+                 torch.empty_like(opacity_logits), torch.empty((n, 16, 3), dtype=torch.float32, device=means.device)]
         grads = _abi.TrainGrads()
         grads.means, grads.log_scales, grads.quats = g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr()
         grads.opacity_logits, grads.sh = g[3].data_ptr(), g[4].data_ptr()
@@ -67,7 +88,7 @@ class _Rasterize(torch.autograd.Function):
         raster = ctx.raster
         raster._check(_abi.load().lrt_rast_train_backward(raster._handle, gc.data_ptr(), C.byref(grads),
                                                           _stream_ptr(None)))
-        return g[0], g[1], g[2], g[3], g[4], None, None, None, None
+        return g[0], g[1], g[2], g[3], g[4], None, None, None, None, None, None
 
 
 class _L1Loss(torch.autograd.Function):
@@ -102,10 +123,17 @@ def l1_loss(colour: torch.Tensor, target: torch.Tensor, raster: TileRasterizer) 
 
 
 def rasterize(means, log_scales, quats, opacity_logits, sh, view: Camera | Projection, settings: RenderSettings,
-              raster: TileRasterizer, sort_values: bool = False):
-    """Render the differentiable cloud; returns (colour [H,W,4], depth [H,W])."""
+              raster: TileRasterizer, sort_values: bool = False, grad_bucket=None, sh_storage=None):
+    """Render the differentiable cloud; returns (colour [H,W,4], depth [H,W]).
+    The kernels read the SH coefficients as fp16 (the gradient with respect to
+    `sh` is fp32): by default `sh` is converted every call; `sh_storage`, an
+    fp16 copy of `sh` the caller keeps in step with it (a mixed-precision
+    optimizer writes both), is read as it is instead.
+    `grad_bucket` (a replicas.GradientBucket for this cloud): the backward
+    writes every gradient into it, ready for one all-reduce over ranks."""
     projection = view if isinstance(view, Projection) else projection_for(view, settings.width, settings.height)
-    return _Rasterize.apply(means, log_scales, quats, opacity_logits, sh, raster, projection, settings, sort_values)
+    return _Rasterize.apply(means, log_scales, quats, opacity_logits, sh, raster, projection, settings, sort_values,
+                            grad_bucket, sh_storage)
 
 
 def backward_times(raster: TileRasterizer) -> tuple[float, float]:

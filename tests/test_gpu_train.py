@@ -187,3 +187,58 @@ def test_the_l1_loss_equals_torch_and_its_gradient_is_the_same(rasterizer):
     (2.5 * want).backward()
     assert abs(float(loss.detach()) - float(want.detach().double())) <= 2e-6 * float(want.detach())
     assert torch.equal(ours, colour.grad)
+
+
+def test_gradients_written_into_a_bucket_are_the_same_and_stay_there(rasterizer):
+    """rasterize(..., grad_bucket=): the backward writes every gradient into one
+    flat buffer (ready for a single all-reduce over ranks); the gradients equal
+    the unbucketed ones bit for bit and autograd keeps them in the bucket."""
+    from lucabrtrender_b200.replicas import GradientBucket
+    p = TF.make_params(20001, 17)   # an odd count: the SH gradient still starts aligned
+    cam, settings = TF.frame(200, 200)
+    target = torch.from_numpy(np.random.default_rng(17).uniform(0, 1, (200, 200, 3)).astype(np.float32)).cuda()
+    names = ("means", "log_scales", "quats", "logits", "sh")
+    out = []
+    for bucket in (None, GradientBucket(20001, torch.device("cuda"))):
+        for _ in range(2):   # a second step rewrites the same bucket
+            t = to_cuda(p, requires_grad=True)
+            colour, _ = L.rasterize(t["means"], t["log_scales"], t["quats"], t["logits"], t["sh"], cam, settings,
+                                    rasterizer, grad_bucket=bucket)
+            L.l1_loss(colour, target, rasterizer).backward()
+            if bucket is not None:
+                assert bucket.holds([t[k].grad for k in names])
+                bucket.all_reduce([t[k] for k in names])   # one rank: nothing to sum
+        out.append({k: t[k].grad.detach().cpu().numpy().copy() for k in names})
+    for k in names:
+        assert np.array_equal(out[0][k].view(np.uint32), out[1][k].view(np.uint32)), k
+
+
+def test_an_fp16_working_copy_of_the_coefficients_gives_the_same_step(rasterizer):
+    """rasterize(..., sh_storage=): the kernels read the caller's fp16 copy of
+    the coefficients instead of converting `sh` each call; image, loss and
+    gradients (the SH one still with respect to the fp32 `sh`) are the same
+    bit for bit. A copy of the wrong type is refused."""
+    p = TF.make_params(20000, 23)
+    p["sh"] = np.random.default_rng(23).normal(0.0, 0.5, p["sh"].shape).astype(np.float32)   # needs rounding
+    cam, settings = TF.frame(200, 200)
+    target = torch.from_numpy(np.random.default_rng(23).uniform(0, 1, (200, 200, 3)).astype(np.float32)).cuda()
+    names = ("means", "log_scales", "quats", "logits", "sh")
+    out = []
+    for working in (False, True):
+        t = to_cuda(p, requires_grad=True)
+        sh16 = t["sh"].detach().reshape(-1, 48).half().contiguous() if working else None
+        colour, _ = L.rasterize(t["means"], t["log_scales"], t["quats"], t["logits"], t["sh"], cam, settings,
+                                rasterizer, sh_storage=sh16)
+        loss = L.l1_loss(colour, target, rasterizer)
+        loss.backward()
+        assert t["sh"].grad.dtype == torch.float32
+        out.append((colour.detach().cpu().numpy(), float(loss.detach()),
+                    {k: t[k].grad.detach().cpu().numpy() for k in names}))
+    (ca, la, ga), (cb, lb, gb) = out
+    assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32)) and la == lb
+    for k in names:
+        assert np.array_equal(ga[k].view(np.uint32), gb[k].view(np.uint32)), k
+    t = to_cuda(p, requires_grad=True)
+    with pytest.raises(ValueError):
+        L.rasterize(t["means"], t["log_scales"], t["quats"], t["logits"], t["sh"], cam, settings, rasterizer,
+                    sh_storage=t["sh"].detach())
