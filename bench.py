@@ -238,12 +238,82 @@ def run_batch(L, torch, dev, rank, raster, args, clocks) -> dict:
     equal = all(torch.equal(x.colour, y.colour) and torch.equal(x.depth, y.depth) for x, y in zip(singles, batched))
     per_seq = seq_ms / (steps * BATCH_VIEWS)
     per_bat = bat_ms / (steps * BATCH_VIEWS)
-    return {"workload": "2M splats, 64 views on a sphere of radius U(3,6), resolutions uniform over 256x256, "
-                        "640x480, 1280x720, 1920x1080", "steps": steps,
-            "batched_ms_per_view": round(per_bat, 4), "sequential_ms_per_view": round(per_seq, 4),
-            "speedup": round(per_seq / per_bat, 3), "images_equal_bit_for_bit": bool(equal),
-            "pairs_per_batch": int(stats.pairs), "views_per_chunk": int(stats.views_per_chunk),
-            "blend_blocks_per_sm": int(stats.blend_blocks_per_sm), "graph_replayed": int(stats.graph_replayed)}
+    out = {"workload": "2M splats, 64 views on a sphere of radius U(3,6), resolutions uniform over 256x256, "
+                       "640x480, 1280x720, 1920x1080", "steps": steps,
+           "batched_ms_per_view": round(per_bat, 4), "sequential_ms_per_view": round(per_seq, 4),
+           "speedup": round(per_seq / per_bat, 3), "images_equal_bit_for_bit": bool(equal),
+           "pairs_per_batch": int(stats.pairs), "views_per_chunk": int(stats.views_per_chunk),
+           "blend_blocks_per_sm": int(stats.blend_blocks_per_sm), "graph_replayed": int(stats.graph_replayed)}
+    del cloud, instances, singles, batched
+    out["fwd_bwd"] = run_batch_train(L, torch, dev, raster, views, projections, flush, stream, steps, per_seq, clocks)
+    return out
+
+
+def run_batch_train(L, torch, dev, raster, views, projections, flush, stream, steps, per_plain, clocks) -> dict:
+    """The 64 views' forward+backward: one lrt_rast_train_batch call per step
+    (each view's L1 loss against a seeded uniform target, gradients of their
+    sum over the same 2M splats' raw parameters) against 64 sequential
+    single-view steps (rasterize + l1_loss + backward), in ms per view."""
+    raw = L.synthetic_records(BATCH_SPLATS, SEED + 1)
+    keep = raw.shape[0]
+    sh = np.zeros((keep, 16, 3), np.float32)
+    sh[:, 0, :] = raw[:, 11:14]
+    for c in range(3):
+        sh[:, 1:, c] = raw[:, 14 + 15 * c:14 + 15 * (c + 1)]
+    sh = sh.astype(np.float16).astype(np.float32)
+    params = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in (
+        ("means", raw[:, 0:3]), ("log_scales", raw[:, 4:7]), ("quats", raw[:, 7:11]), ("logits", raw[:, 3]),
+        ("sh", sh))}
+    sh16 = params["sh"].reshape(keep, 48).half().contiguous()
+    gen = torch.Generator(device=dev).manual_seed(SEED)
+    tviews = [(p, torch.rand((h, w, 3), generator=gen, device=dev)) for p, w, h in projections]
+    ordered = [params[k] for k in ("means", "log_scales", "quats", "logits", "sh")]
+
+    def batch_step():
+        return L.train_batch(*ordered, tviews, L.RenderSettings(), raster, sh_storage=sh16, stream=stream)
+
+    leaves = {k: v.clone().requires_grad_(True) for k, v in params.items()}
+    lordered = [leaves[k] for k in ("means", "log_scales", "quats", "logits", "sh")]
+
+    def sequential_steps():
+        for p, target in tviews:
+            for v in lordered:
+                v.grad = None
+            h, w = target.shape[:2]
+            colour, _ = L.rasterize(*lordered, p, L.RenderSettings(width=w, height=h), raster, sh_storage=sh16)
+            L.l1_loss(colour, target, raster).backward()
+
+    for _ in range(2):
+        stats = batch_step()[4]
+        sequential_steps()
+    torch.cuda.synchronize(dev)
+    bat_ms = seq_ms = 0.0
+    w0 = time.time()
+    for _ in range(steps):
+        flush.fill_(3.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        stats = batch_step()[4]
+        b.record(stream)
+        b.synchronize()
+        bat_ms += a.elapsed_time(b)
+        flush.fill_(4.0)
+        a.record(stream)
+        sequential_steps()
+        b.record(stream)
+        b.synchronize()
+        seq_ms += a.elapsed_time(b)
+    clocks.window(w0, time.time())
+    per_bat = bat_ms / (steps * BATCH_VIEWS)
+    per_seq = seq_ms / (steps * BATCH_VIEWS)
+    return {"workload": "the same 64 views and 2M splats as raw parameters; per view an L1 loss against a seeded "
+                        "uniform [0,1]^3 target; gradients of the views' summed loss",
+            "batched_ms_per_view": round(per_bat, 4), "sequential_fwd_bwd_ms_per_view": round(per_seq, 4),
+            "speedup_vs_sequential_fwd_bwd": round(per_seq / per_bat, 3),
+            "ratio_to_sequential_plain_forward": round(per_bat / per_plain, 3),
+            "views_per_chunk": int(stats.views_per_chunk), "chunks": int(stats.chunks),
+            "pairs_per_batch": int(stats.pairs)}
 
 
 def time_device(torch, stream, fn, reps: int) -> float:

@@ -361,6 +361,37 @@ int lrt_rast_train_backward(lrt_rast* rast, const void* grad_colour, lrt_train_g
  * per-splat reduction + projection backward. */
 int lrt_rast_backward_times(const lrt_rast* rast, double* blend_ms, double* project_ms);
 
+/* One view of a training batch: a batch view (its images written by the
+ * forward) plus the loss's target image, float3 per pixel (width * height,
+ * bottom row first), and where its loss goes (a device float; may be NULL). */
+typedef struct lrt_train_view {
+    lrt_projection projection;
+    uint32_t width, height;
+    void* colour;
+    void* depth;
+    const void* target;
+    void* loss;
+} lrt_train_view;
+
+/* A training step over many views of one cloud of raw parameters, in one
+ * call (no reference counterpart): for each view, the forward of
+ * lrt_rast_train_forward (its colour and depth written, the same pixels bit
+ * for bit), the L1 loss of lrt_rast_l1_loss against the view's target, and
+ * the backward of that loss; `grads` receives the gradients of the sum of the
+ * views' losses (written, not added to), accumulated view by view in the
+ * given order, so they are the sum of the single-view gradients taken in that
+ * order, bit for bit. Views go in chunks: each chunk is projected view by
+ * view into one pair buffer (the views' tiles numbered one after another),
+ * sorted once, blended by one persistent launch over (view, tile) items,
+ * and taken back through one backward-blend launch over those items and one
+ * per-splat backward per view. The settings' width and height are replaced
+ * by each view's. Returns when the step is done; OVERFLOW cannot happen (a
+ * chunk whose pairs outgrow their buffer is drawn again with more room). */
+int lrt_rast_train_batch(lrt_rast* rast, const lrt_train_params* params, const lrt_train_view* views,
+                         uint32_t view_count, const lrt_render_settings* settings, lrt_train_grads* grads,
+                         lrt_batch_stats* stats, void* stream);
+
+
 /* PrefixSum::apply: exclusive scan of `count` uint32 at `in` into `out`, the
  * sum into `total` (all device pointers; `out` may alias `in`). Single pass,
  * decoupled look-back; scratch is the handle's. */

@@ -11,7 +11,7 @@ from .raster import (Depth, EditMode, EditShape, FrameStats, PointInstance, Poin
 from ._abi import SplatEncoding
 from .scene import (CloudLoader, GpuPoints, GpuSplats, PackedPoints, PackedSplats, pack_points, pack_splats,
                     ply_encoding, points_to_device, synthetic_records, to_device)
-from .train import l1_loss, rasterize
+from .train import l1_loss, rasterize, train_batch
 from .lod import CutSelector, CutStats, LodBuildSettings, LodBuilder, LodCloud, LodInstance, LodLevel
 
 __all__ = [
@@ -20,5 +20,5 @@ __all__ = [
     "CloudLoader", "GpuSplats", "PackedSplats", "pack_splats", "synthetic_records", "to_device", "rasterize",
     "PointInstance", "PointStyle", "GpuPoints", "PackedPoints", "pack_points", "points_to_device",
     "SplatEncoding", "ply_encoding", "l1_loss", "CutSelector", "CutStats", "LodBuildSettings", "LodBuilder",
-    "LodCloud", "LodInstance", "LodLevel",
+    "LodCloud", "LodInstance", "LodLevel", "train_batch",
 ]

@@ -43,7 +43,7 @@ EXPORTS = (
     "lrt_rast_decode_splats", "lrt_rast_decode_points", "lrt_rast_compare_images", "lrt_rast_compare_hdr",
     "lrt_rast_count_different", "lrt_rast_l1_loss", "lrt_l1_loss_grad", "lrt_lod_build_settings_default",
     "lrt_lod_build", "lrt_lod_destroy", "lrt_lod_get_info", "lrt_lod_splats", "lrt_lod_level", "lrt_lod_starts",
-    "lrt_lod_select",
+    "lrt_lod_select", "lrt_rast_train_batch",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 
@@ -194,6 +194,11 @@ class TrainGrads(C.Structure):
 _lib = None
 
 
+class TrainViewStruct(C.Structure):
+    _fields_ = [("projection", Projection), ("width", C.c_uint32), ("height", C.c_uint32), ("colour", C.c_void_p),
+                ("depth", C.c_void_p), ("target", C.c_void_p), ("loss", C.c_void_p)]
+
+
 class LodBuildSettings(C.Structure):
     _fields_ = [("max_group_fraction", C.c_float), ("coarsest_level", C.c_uint32), ("chunk_splats", C.c_uint32),
                 ("reserved", C.c_uint32)]
@@ -275,6 +280,9 @@ def load() -> C.CDLL:
                                           C.c_uint32, C.POINTER(RenderSettingsStruct), C.POINTER(BatchStats),
                                           C.c_void_p]
     lib.lrt_rast_backward_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.lrt_rast_train_batch.argtypes = [C.c_void_p, C.POINTER(TrainParams), C.POINTER(TrainViewStruct), C.c_uint32,
+                                         C.POINTER(RenderSettingsStruct), C.POINTER(TrainGrads),
+                                         C.POINTER(BatchStats), C.c_void_p]
     lib.lrt_lod_build_settings_default.argtypes = [C.POINTER(LodBuildSettings)]
     lib.lrt_lod_build.argtypes = [C.c_void_p, C.POINTER(GpuSplatsStruct), C.c_void_p, C.POINTER(LodBuildSettings),
                                   C.POINTER(C.c_void_p), C.c_void_p]

@@ -407,7 +407,9 @@ blend_composite_kernel(BlendParams bp, const uint2* __restrict__ ranges, const u
 
 // Many views in one launch: a persistent grid whose blocks take (view, tile)
 // work items from a queue in order -- the views' tiles numbered one after
-// another, largest views first -- and blend each as blend_kernel does.
+// another, largest views first -- and blend each as blend_kernel does
+// (kTrain: as blend_kernel<true>, keeping each view's per-pixel state).
+template <bool kTrain>
 __global__ void __launch_bounds__(kBlendThreads)
 blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_t viewCount,
                    const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
@@ -440,8 +442,9 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
         vbp.height = v.height;
         vbp.tilesX = v.tilesX;
         const uint32_t local = item - v.tileBase;
-        blend_tile<false>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr, proj + v.recordBase,
-                          v.colour, v.depth, nullptr, nullptr, err, sRec, sBox, sBar, phase0, phase1);
+        blend_tile<kTrain>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr, proj + v.recordBase,
+                           v.colour, v.depth, kTrain ? v.pixState : nullptr, kTrain ? v.pixLast : nullptr, err, sRec,
+                           sBox, sBar, phase0, phase1);
     }
 }
 
@@ -502,12 +505,18 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], uint3
 // summed over the warp's pixels by shuffles, over the block's warps in
 // warp order through shared memory, and written at the pair's emit index: a
 // splat's pairs are contiguous there, so a per-splat sum needs no atomics.
-__global__ void __launch_bounds__(kBlendThreads)
-blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
-                      const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
-                      const ProjRecord* __restrict__ proj,
-                      const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
-                      const float4* __restrict__ gradColour, float* __restrict__ partials) {
+// One tile: `item` indexes the ranges (the frame's tile, or a batch's
+// (view, tile) item); (tx, ty) is the tile within its view.
+__device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint32_t item, uint32_t tx, uint32_t ty,
+                                                    const uint2* __restrict__ ranges,
+                                                    const unsigned long long* __restrict__ pairs,
+                                                    const uint32_t* __restrict__ emit,
+                                                    const uint32_t* __restrict__ emitSlot,
+                                                    const ProjRecord* __restrict__ proj,
+                                                    const float4* __restrict__ pixState,
+                                                    const uint32_t* __restrict__ pixLast,
+                                                    const float4* __restrict__ gradColour,
+                                                    float* __restrict__ partials) {
     constexpr uint32_t kB = 128;
     __shared__ __align__(16) ProjRecord sRec[kB];
     __shared__ __align__(16) float4 sBox[kB];
@@ -517,12 +526,10 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
     __shared__ uint32_t sMaxLast;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x;
-    const uint32_t tx = tile % bp.tilesX, ty = tile / bp.tilesX;
     const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
     const bool inside = px < bp.width && py < bp.height;
-    const uint2 range = ranges[tile];
+    const uint2 range = ranges[item];
     const uint32_t start = range.x;
     const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
     const size_t pix = static_cast<size_t>(py) * bp.width + px;
@@ -703,6 +710,41 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
     }
 }
 
+__global__ void __launch_bounds__(kBlendThreads)
+blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+                      const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
+                      const ProjRecord* __restrict__ proj,
+                      const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
+                      const float4* __restrict__ gradColour, float* __restrict__ partials) {
+    const uint32_t tile = blockIdx.x;
+    blend_backward_tile(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emit, emitSlot, proj, pixState,
+                        pixLast, gradColour, partials);
+}
+
+// The backward of a training batch: one block per (view, tile) item of the
+// chunk, each the tile of blend_backward_kernel in its own view (records at
+// the view's base, pixel state and colour gradient from the view's buffers).
+__global__ void __launch_bounds__(kBlendThreads)
+blend_backward_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_t viewCount,
+                            const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
+                            const uint32_t* __restrict__ emit, const ProjRecord* __restrict__ proj,
+                            float* __restrict__ partials) {
+    const uint32_t item = blockIdx.x;
+    uint32_t lo = 0, hi = viewCount;   // the view whose tiles hold `item`
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (views[mid].tileBase <= item) lo = mid; else hi = mid;
+    }
+    const ViewParams v = views[lo];
+    BlendParams vbp = bp;
+    vbp.width = v.width;
+    vbp.height = v.height;
+    vbp.tilesX = v.tilesX;
+    const uint32_t local = item - v.tileBase;
+    blend_backward_tile(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, emit, nullptr,
+                        proj + v.recordBase, v.pixState, v.pixLast, v.gradColour, partials);
+}
+
 }  // namespace
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
@@ -740,8 +782,28 @@ cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, u
                                const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
                                uint32_t* err, uint32_t blocks, cudaStream_t stream) {
     if (totalTiles == 0) return cudaSuccess;
-    blend_batch_kernel<<<blocks, kBlendThreads, 0, stream>>>(
+    blend_batch_kernel<false><<<blocks, kBlendThreads, 0, stream>>>(
         bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, totalTiles, queue, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_batch_train(const BlendParams& bp, const ViewParams* views, uint32_t viewCount,
+                                     const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                                     uint32_t totalTiles, uint32_t* queue, uint32_t* err, uint32_t blocks,
+                                     cudaStream_t stream) {
+    if (totalTiles == 0) return cudaSuccess;
+    blend_batch_kernel<true><<<blocks, kBlendThreads, 0, stream>>>(
+        bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, totalTiles, queue, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blend_backward_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount,
+                                        const uint2* ranges, const uint64_t* pairs, const uint32_t* emit,
+                                        const ProjRecord* proj, uint32_t totalTiles, float* partials,
+                                        cudaStream_t stream) {
+    if (totalTiles == 0) return cudaSuccess;
+    blend_backward_batch_kernel<<<totalTiles, kBlendThreads, 0, stream>>>(
+        bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, proj, partials);
     return cudaGetLastError();
 }
 

@@ -72,6 +72,17 @@ cudaError_t launch_blend_composite(const BlendParams& bp, const uint2* ranges, c
 cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
                                const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
                                uint32_t* err, uint32_t blocks, cudaStream_t stream);
+// A training batch: blend_kernel<true> per (view, tile) item, and the backward
+// per item (views carry pixState, pixLast and gradColour; emit: the sorted
+// pairs' emit indices).
+cudaError_t launch_blend_batch_train(const BlendParams& bp, const ViewParams* views, uint32_t viewCount,
+                                     const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
+                                     uint32_t totalTiles, uint32_t* queue, uint32_t* err, uint32_t blocks,
+                                     cudaStream_t stream);
+cudaError_t launch_blend_backward_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount,
+                                        const uint2* ranges, const uint64_t* pairs, const uint32_t* emit,
+                                        const ProjRecord* proj, uint32_t totalTiles, float* partials,
+                                        cudaStream_t stream);
 // Training frames: `emitSlot` (when not null) maps a pair word's low field,
 // the pair's emit index, to its slot; otherwise the low field is the slot and
 // `emit` holds each sorted pair's emit index.
@@ -87,7 +98,7 @@ cudaError_t launch_splat_backward(const FrameParams& f, const float* means, cons
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
                                   const uint32_t* offsets, const float* partials, uint32_t partialPairs,
                                   float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, bool accumulate = false);
 
 cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
 

@@ -36,6 +36,10 @@ struct lrt_rast {
     DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
     DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
     DeviceBuffer lossScratch;                            // the L1 loss's per-block sums
+    // Training batches (train_batch.cu): colour gradients, view parameters
+    // and queue, losses with no caller buffer; their pair capacity.
+    DeviceBuffer trainBatchGrad, trainBatchViews, trainBatchLoss;
+    uint32_t trainBatchPairCap = 0;
     void* metricHost = nullptr;                          // pinned readback of the metrics
     size_t metricHostBytes = 0;
     bool trainReady = false;
@@ -216,5 +220,70 @@ struct DeviceScope {
         if (previous >= 0) cudaSetDevice(previous);
     }
 };
+
+// One cloud of a frame, whichever its kind, and the projection uniforms of a
+// view of it (FrameParams.h:32-93).
+struct CloudDesc {
+    const lrt_gpu_splats* packed = nullptr;
+    const lrt_train_params* train = nullptr;
+    const lrt_point_instance* point = nullptr;   // points drawn as discs
+    const double* objectToWorld = nullptr;
+    const lrt_splat_edit* edit = nullptr;
+    uint32_t count = 0;
+};
+
+inline constexpr double kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+
+inline FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s, const CloudDesc& c, uint32_t tilesX,
+                         uint32_t tilesY, uint32_t base) {
+    FrameParams f{};
+    f.width = s->width;
+    f.height = s->height;
+    f.tilesX = tilesX;
+    f.tilesY = tilesY;
+    f.focalX = static_cast<float>(pr->focal_x);
+    f.focalY = static_cast<float>(pr->focal_y);
+    f.centreX = static_cast<float>(pr->centre_x);
+    f.centreY = static_cast<float>(pr->centre_y);
+    f.nearZ = static_cast<float>(pr->near_z);
+    f.farZ = static_cast<float>(pr->far_z);
+    f.ortho = pr->orthographic ? 1u : 0u;
+    f.antialias = s->antialias ? 1u : 0u;
+    const M4 ov = mul4(pr->world_to_view, c.objectToWorld);
+    for (int row = 0; row < 3; ++row)
+        for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
+    double eye[3];
+    eye_in_object(c.objectToWorld, pr->eye_world, eye);
+    for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
+    f.count = c.count;
+    f.base = base;
+    if (c.train != nullptr) {
+        f.restPerColour = 15;
+        f.shWords = 24;
+    } else if (c.packed != nullptr) {
+        f.restPerColour = c.packed->rest_per_colour;
+        f.shWords = c.packed->sh_words;
+    }
+    f.shLimit = s->max_sh_degree;
+    f.writeDebug = 1;
+    if (c.edit != nullptr) {
+        const lrt_splat_edit& e = *c.edit;
+        f.edit.active = e.active;
+        f.edit.shape = e.shape;
+        f.edit.mode = e.mode;
+        f.edit.invert = e.invert;
+        for (int a = 0; a < 3; ++a) {
+            f.edit.centre[a] = e.centre[a];
+            f.edit.size[a] = e.size[a];
+            f.edit.tint[a] = e.tint[a];
+        }
+        f.edit.saturation = e.saturation;
+        f.edit.brightness = e.brightness;
+        f.edit.opacity = e.opacity;
+        f.edit.minOpacity = e.min_opacity;
+        f.edit.maxScale = e.max_scale;
+    }
+    return f;
+}
 
 }  // namespace

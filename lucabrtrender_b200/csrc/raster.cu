@@ -61,7 +61,8 @@ void lrt_rast_destroy(lrt_rast* r) {
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
-                            &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch})
+                            &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
+                            &r->trainBatchViews, &r->trainBatchLoss})
         release(*b);
     if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
@@ -92,69 +93,6 @@ namespace {
 
 // One projection launch of a frame: a packed cloud instance, or the
 // differentiable parameters of the training path.
-struct CloudDesc {
-    const lrt_gpu_splats* packed = nullptr;
-    const lrt_train_params* train = nullptr;
-    const lrt_point_instance* point = nullptr;   // points drawn as discs
-    const double* objectToWorld = nullptr;
-    const lrt_splat_edit* edit = nullptr;
-    uint32_t count = 0;
-};
-
-const double kIdentity[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
-
-FrameParams frame_params(const lrt_projection* pr, const lrt_render_settings* s, const CloudDesc& c, uint32_t tilesX,
-                         uint32_t tilesY, uint32_t base) {
-    FrameParams f{};
-    f.width = s->width;
-    f.height = s->height;
-    f.tilesX = tilesX;
-    f.tilesY = tilesY;
-    f.focalX = static_cast<float>(pr->focal_x);
-    f.focalY = static_cast<float>(pr->focal_y);
-    f.centreX = static_cast<float>(pr->centre_x);
-    f.centreY = static_cast<float>(pr->centre_y);
-    f.nearZ = static_cast<float>(pr->near_z);
-    f.farZ = static_cast<float>(pr->far_z);
-    f.ortho = pr->orthographic ? 1u : 0u;
-    f.antialias = s->antialias ? 1u : 0u;
-    const M4 ov = mul4(pr->world_to_view, c.objectToWorld);
-    for (int row = 0; row < 3; ++row)
-        for (int col = 0; col < 4; ++col) f.m[row * 4 + col] = static_cast<float>(ov.at(row, col));
-    double eye[3];
-    eye_in_object(c.objectToWorld, pr->eye_world, eye);
-    for (int a = 0; a < 3; ++a) f.eye[a] = static_cast<float>(eye[a]);
-    f.count = c.count;
-    f.base = base;
-    if (c.train != nullptr) {
-        f.restPerColour = 15;
-        f.shWords = 24;
-    } else if (c.packed != nullptr) {
-        f.restPerColour = c.packed->rest_per_colour;
-        f.shWords = c.packed->sh_words;
-    }
-    f.shLimit = s->max_sh_degree;
-    f.writeDebug = 1;
-    if (c.edit != nullptr) {
-        const lrt_splat_edit& e = *c.edit;
-        f.edit.active = e.active;
-        f.edit.shape = e.shape;
-        f.edit.mode = e.mode;
-        f.edit.invert = e.invert;
-        for (int a = 0; a < 3; ++a) {
-            f.edit.centre[a] = e.centre[a];
-            f.edit.size[a] = e.size[a];
-            f.edit.tint[a] = e.tint[a];
-        }
-        f.edit.saturation = e.saturation;
-        f.edit.brightness = e.brightness;
-        f.edit.opacity = e.opacity;
-        f.edit.minOpacity = e.min_opacity;
-        f.edit.maxScale = e.max_scale;
-    }
-    return f;
-}
-
 // One frame, TileRasterizer.cpp:188-484 in this build's stage order. `train`
 // selects the training variants (emit indices carried through the sort,
 // per-slot pair offsets, per-pixel blend state for the backward pass).

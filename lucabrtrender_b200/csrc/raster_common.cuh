@@ -49,6 +49,11 @@ struct ViewParams {
     uint32_t recordBase, reserved0, reserved1, reserved2;
     float4* colour;
     float* depth;
+    // Training batches: the view's per-pixel blend state, and the gradient of
+    // the loss with respect to its colour image.
+    float4* pixState;
+    uint32_t* pixLast;
+    const float4* gradColour;
 };
 
 // frame.slang:85-89: what the projection leaves for the blend.

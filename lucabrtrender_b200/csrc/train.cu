@@ -71,6 +71,10 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// kAccumulate: add this frame's gradients to what the buffers hold (the
+// views of a batch after the first, in view order); a splat this frame does
+// not touch then adds nothing and writes nothing.
+template <bool kAccumulate>
 __global__ void __launch_bounds__(kThreads, 4)
 splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
                       const float* __restrict__ quats, const float* __restrict__ logits,
@@ -127,6 +131,7 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         }
     }
     if (!live) return;
+    if (kAccumulate && n == 0) return;
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
     float* gshRow = gSh + static_cast<size_t>(i) * 48;
     if (n == 0) {
@@ -240,7 +245,14 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         {
             float4* out = reinterpret_cast<float4*>(gshRow);
 #pragma unroll
-            for (int q = 0; q < 12; ++q) out[q] = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
+            for (int q = 0; q < 12; ++q) {
+                float4 v = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
+                if (kAccumulate) {
+                    const float4 o = out[q];
+                    v = make_float4(o.x + v.x, o.y + v.y, o.z + v.z, o.w + v.w);
+                }
+                out[q] = v;
+            }
         }
         {   // dir = v / |v|, v = p - eye
             const float dotd = gdx * dirx + gdy * diry + gdz * dirz;
@@ -343,6 +355,15 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
         // t = W p + t0
         for (int k = 0; k < 3; ++k) gm[k] += W[0][k] * gt[0] + W[1][k] * gt[1] + W[2][k] * gt[2];
     }
+    if (kAccumulate) {
+        for (int k = 0; k < 3; ++k) {
+            gMeans[3 * i + k] = gMeans[3 * i + k] + gm[k];
+            gLogScales[3 * i + k] = gLogScales[3 * i + k] + gls[k];
+        }
+        for (int k = 0; k < 4; ++k) gQuats[4 * i + k] = gQuats[4 * i + k] + gq[k];
+        gLogits[i] = gLogits[i] + glog;
+        return;
+    }
     for (int k = 0; k < 3; ++k) {
         gMeans[3 * i + k] = gm[k];
         gLogScales[3 * i + k] = gls[k];
@@ -357,11 +378,17 @@ cudaError_t launch_splat_backward(const FrameParams& f, const float* means, cons
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
                                   const uint32_t* offsets, const float* partials, uint32_t partialPairs,
                                   float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
-                                  cudaStream_t stream) {
+                                  cudaStream_t stream, bool accumulate) {
     if (f.count == 0) return cudaSuccess;
-    splat_backward_kernel<<<(f.count + kThreads - 1) / kThreads, kThreads, 0, stream>>>(
-        f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales, gQuats,
-        gLogits, gSh);
+    const uint32_t blocks = (f.count + kThreads - 1) / kThreads;
+    if (accumulate)
+        splat_backward_kernel<true><<<blocks, kThreads, 0, stream>>>(
+            f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales,
+            gQuats, gLogits, gSh);
+    else
+        splat_backward_kernel<false><<<blocks, kThreads, 0, stream>>>(
+            f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales,
+            gQuats, gLogits, gSh);
     return cudaGetLastError();
 }
 

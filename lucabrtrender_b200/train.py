@@ -140,3 +140,68 @@ def backward_times(raster: TileRasterizer) -> tuple[float, float]:
     a, b = C.c_double(), C.c_double()
     raster._check(_abi.load().lrt_rast_backward_times(raster._handle, C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+def train_batch(means, log_scales, quats, opacity_logits, sh, views, settings: RenderSettings, raster: TileRasterizer,
+                sh_storage=None, grad_bucket=None, stream=None):
+    """One training step over many views in one call (lrt_rast_train_batch):
+    each view rendered as `rasterize` renders it, its L1 loss against its
+    target taken as `l1_loss` takes it, and the gradients of the sum of the
+    views' losses accumulated view by view, in the given order.
+
+    views: a sequence of (Camera | Projection, target [H, W, 3] float32 on the
+    device); each view's size is its target's. The settings' size is ignored.
+    sh_storage: as for `rasterize` (the fp16 copy the kernels read; made here
+    when not given). grad_bucket: a replicas.GradientBucket to write the
+    gradients into (else new tensors).
+
+    Returns (colours [list of [H, W, 4]], depths [list of [H, W]], losses [V]
+    tensor, grads: dict of means, log_scales, quats, opacity_logits, sh, each
+    shaped like its parameter) and the batch's stats (BatchStats).
+    """
+    dev = means.device
+    n = means.shape[0]
+    means = means.detach().contiguous().float()
+    log_scales = log_scales.detach().contiguous().float()
+    quats = quats.detach().contiguous().float()
+    opacity_logits = opacity_logits.detach().contiguous().float()
+    if sh_storage is None:
+        sh_storage = sh.detach().reshape(n, 48).to(torch.float16).contiguous()
+    elif sh_storage.dtype != torch.float16 or sh_storage.numel() != n * 48 or not sh_storage.is_contiguous():
+        raise ValueError("sh_storage must be a contiguous fp16 tensor of N x 48 coefficients")
+    p = _abi.TrainParams()
+    p.count = n
+    p.means, p.log_scales, p.quats = means.data_ptr(), log_scales.data_ptr(), quats.data_ptr()
+    p.opacity_logits, p.sh = opacity_logits.data_ptr(), sh_storage.data_ptr()
+    colours, depths, targets = [], [], []
+    losses = torch.zeros(len(views), dtype=torch.float32, device=dev)
+    arr = (_abi.TrainViewStruct * max(1, len(views)))()
+    for k, (view, target) in enumerate(views):
+        h, w = int(target.shape[0]), int(target.shape[1])
+        if target.shape[-1] != 3:
+            raise ValueError("a view's target must be [H, W, 3]")
+        target = target.contiguous().float()
+        targets.append(target)
+        pr = view if isinstance(view, Projection) else projection_for(view, w, h)
+        colour = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
+        depth = torch.empty((h, w), dtype=torch.float32, device=dev)
+        colours.append(colour)
+        depths.append(depth)
+        arr[k].projection = pr.struct()
+        arr[k].width, arr[k].height = w, h
+        arr[k].colour, arr[k].depth, arr[k].target = colour.data_ptr(), depth.data_ptr(), target.data_ptr()
+        arr[k].loss = losses.data_ptr() + 4 * k
+    shapes = {"means": means.shape, "log_scales": log_scales.shape, "quats": quats.shape,
+              "opacity_logits": opacity_logits.shape, "sh": sh.shape}
+    if grad_bucket is not None and grad_bucket.count == n:
+        grads = {k: grad_bucket.slice(k).view(shapes[k]) for k in grad_bucket.ORDER}
+    else:
+        grads = {k: torch.empty(shapes[k], dtype=torch.float32, device=dev) for k in shapes}
+    g = _abi.TrainGrads()
+    g.means, g.log_scales, g.quats = grads["means"].data_ptr(), grads["log_scales"].data_ptr(), grads["quats"].data_ptr()
+    g.opacity_logits, g.sh = grads["opacity_logits"].data_ptr(), grads["sh"].data_ptr()
+    st = settings.struct()
+    stats = _abi.BatchStats()
+    raster._check(_abi.load().lrt_rast_train_batch(raster._handle, C.byref(p), arr, len(views), C.byref(st),
+                                                   C.byref(g), C.byref(stats), _stream_ptr(stream)))
+    return colours, depths, losses, grads, stats
