@@ -91,24 +91,33 @@ __device__ __forceinline__ float cutoff_power(float alpha) {   // frame.slang:10
     return fminf(2.0f * lrt_log(fmaxf(255.0f * alpha, 1.0001f)), 9.0f);
 }
 
-// frame.slang:113-130: exact minimum of the quadratic form over a box.
-__device__ __forceinline__ float min_power_over_box(float a, float b, float c, float lox, float loy,
-                                                    float hix, float hiy) {
-    if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f;
-    float best = 3.4e38f;
+// frame.slang:113-130 decides a tile by the exact minimum of the quadratic
+// form over the box of its pixel centres: 0 when the box holds the centre,
+// else the least of four candidates (each edge at its clamped stationary
+// point), compared with the cutoff. That minimum is at most the cutoff
+// exactly when one candidate is (fminf skips a NaN candidate, and so does the
+// <= test), so here the candidates are tested one by one, each computed with
+// the reference's expression, and the first within the cutoff answers. The edges nearer the centre go
+// first, since a touched tile is usually decided by one of them; an untouched
+// tile still evaluates all four.
+__device__ __forceinline__ bool power_within_over_box(float a, float b, float c, float lox, float loy, float hix,
+                                                      float hiy, float cutoff) {
+    if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f <= cutoff;
+    const bool xNearHi = fabsf(hix) < fabsf(lox), yNearHi = fabsf(hiy) < fabsf(loy);
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-        const float x = e == 0 ? lox : hix;
-        const float y = c > 1e-12f ? clampf(-b * x / c, loy, hiy) : loy;
-        best = fminf(best, a * x * x + 2.0f * b * x * y + c * y * y);
+        {
+            const float x = (e == 0) == xNearHi ? hix : lox;
+            const float y = c > 1e-12f ? clampf(-b * x / c, loy, hiy) : loy;
+            if (a * x * x + 2.0f * b * x * y + c * y * y <= cutoff) return true;
+        }
+        {
+            const float y = (e == 0) == yNearHi ? hiy : loy;
+            const float x = a > 1e-12f ? clampf(-b * y / a, lox, hix) : lox;
+            if (a * x * x + 2.0f * b * x * y + c * y * y <= cutoff) return true;
+        }
     }
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        const float y = e == 0 ? loy : hiy;
-        const float x = a > 1e-12f ? clampf(-b * y / a, lox, hix) : lox;
-        best = fminf(best, a * x * x + 2.0f * b * x * y + c * y * y);
-    }
-    return best;
+    return false;
 }
 
 // frame.slang:133-138: does tile (tx, ty) hold a pixel centre inside the footprint?
@@ -119,7 +128,7 @@ __device__ __forceinline__ bool tile_touched(uint32_t width, uint32_t height, fl
     const float firstY = static_cast<float>(ty * kTile) + 0.5f;
     const float lastX = static_cast<float>(min((tx + 1) * kTile, width) - 1) + 0.5f;
     const float lastY = static_cast<float>(min((ty + 1) * kTile, height) - 1) + 0.5f;
-    return min_power_over_box(ca, cb, cc, firstX - cx, firstY - cy, lastX - cx, lastY - cy) <= cutoff;
+    return power_within_over_box(ca, cb, cc, firstX - cx, firstY - cy, lastX - cx, lastY - cy, cutoff);
 }
 
 // shaders/lrt/common/color.slang:7-10
