@@ -184,9 +184,12 @@ cudaError_t launch_lod_merge_moments(const uint32_t* firstChild, uint32_t groups
                                      const float* fineMoments, float* moments, uint32_t stride, cudaStream_t stream);
 cudaError_t launch_lod_finalize(const float* moments, uint32_t groups, uint32_t restPerColour, uint32_t shWords,
                                 LodSplatArrays merged, cudaStream_t stream);
-// counts: two zeroed words (drawn, of which merged); status as above over merged + count items.
+// scratch: lod_cut_scratch_bytes(merged + count) bytes (per block a bitmask
+// and a count, all written by the cut); counts: two words (drawn, of which
+// merged), written by the cut.
+size_t lod_cut_scratch_bytes(uint32_t items);
 cudaError_t launch_lod_cut(const LodCutParams& c, const uint32_t* cells, const uint32_t* codes,
                            const LodSplatArrays merged, const LodSplatArrays store, LodSplatArrays out,
-                           void* status, uint32_t* counts, uint32_t* err, cudaStream_t stream);
+                           void* scratch, uint32_t* counts, cudaStream_t stream);
 
 }  // namespace lrt

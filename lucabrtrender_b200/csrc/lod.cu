@@ -485,70 +485,133 @@ __device__ __forceinline__ bool cell_small(const LodCutParams& c, uint32_t cell,
     return c.threshold > 0.0f && projected_edge(c, cell, level) <= c.threshold;
 }
 
-// lodCutGroups / lodCutFinest / lodCutSplats (lod_cut.slang:32-86, every
-// chunk resident) + the prefix sums and lodGather (lod_gather.slang:18-33)
-// in one pass. Items: the merged Gaussians, stored levels coarsest first,
-// then the splats. A group is drawn when its cell is small and its parent's
-// is not (or it is on the coarsest level); a splat when its finest-level
-// cell is not small. Drawn items land in order from 0; items past
-// `capacity` are counted, not written.
-__global__ void __launch_bounds__(kLodThreads)
-lod_cut_kernel(LodCutParams c, const uint32_t* __restrict__ cells, const uint32_t* __restrict__ codes,
-               LodSplatArrays merged, LodSplatArrays store, LodSplatArrays out, uint64_t* __restrict__ status,
-               uint32_t* __restrict__ ticket, uint32_t* __restrict__ counts, uint32_t* __restrict__ err) {
-    __shared__ uint32_t sPart, sBase;
-    __shared__ uint32_t sWarp[kLodThreads / 32];
-    __shared__ uint32_t sItem[kLodThreads];
-    if (threadIdx.x == 0) sPart = atomicAdd(ticket, 1u);
-    __syncthreads();
-    const uint32_t part = sPart;
-    const uint32_t items = c.merged + c.count;
-    const uint32_t j = part * kLodThreads + threadIdx.x;
-    bool drawn = false;
+constexpr uint32_t kCutItems = 4;                        // consecutive items per thread
+constexpr uint32_t kCutTile = kLodThreads * kCutItems;   // items per block
+constexpr uint32_t kCutMaskWords = kCutTile / 32;
+
+// Whether item j of the cut is drawn (lodCutGroups / lodCutFinest /
+// lodCutSplats, lod_cut.slang:32-86, every chunk resident): a merged
+// Gaussian when its cell is small and its parent's is not (or it is on the
+// coarsest stored level), a splat when its finest-level cell is not small.
+__device__ __forceinline__ bool cut_drawn(const LodCutParams& c, uint32_t j, uint32_t key) {
     if (j < c.merged) {
-        // The stored level holding j (constant indices keep the table in
-        // the parameter bank).
+        // The stored level holding j (constant indices keep the table in the
+        // parameter bank).
         uint32_t level = 0;
 #pragma unroll
         for (uint32_t l = 1; l <= kLodLevels; ++l) level += (l < c.levels && j >= c.levelBase[l]) ? 1u : 0u;
         const uint32_t octree = c.coarsest + level;
-        const uint32_t cell = __ldg(cells + j);
-        const bool here = cell_small(c, cell, octree);
-        const bool above = level > 0 && cell_small(c, cell >> 3, octree - 1);
-        drawn = here && !above;
-    } else if (j < items) {
-        const uint32_t finest = c.coarsest + c.levels - 1;
-        drawn = !cell_small(c, __ldg(codes + (j - c.merged)) >> (3 * (kLodLevels - finest)), finest);
+        const bool here = cell_small(c, key, octree);
+        const bool above = level > 0 && cell_small(c, key >> 3, octree - 1);
+        return here && !above;
     }
-    const uint32_t mergedDrawn = __syncthreads_count(drawn && j < c.merged);
+    const uint32_t finest = c.coarsest + c.levels - 1;
+    return !cell_small(c, key >> (3 * (kLodLevels - finest)), finest);
+}
+
+// The cut in three passes, none waiting on another block. Items: the merged
+// Gaussians, stored levels coarsest first, then the splats (the reference's
+// output order, Lod.cpp:486-514). First every block decides its 1024 items
+// (four consecutive a thread, their cell or code loads in flight together)
+// and writes them as a 32-word bitmask and a count.
+__global__ void __launch_bounds__(kLodThreads)
+lod_cut_decide_kernel(LodCutParams c, const uint32_t* __restrict__ cells, const uint32_t* __restrict__ codes,
+                      uint32_t* __restrict__ flags, uint32_t* __restrict__ blockCounts) {
+    __shared__ uint32_t sMask[kCutMaskWords];
+    __shared__ uint32_t sWarp[kLodThreads / 32];
+    if (threadIdx.x < kCutMaskWords) sMask[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t items = c.merged + c.count;
+    const uint32_t j0 = blockIdx.x * kCutTile + threadIdx.x * kCutItems;
+    uint32_t key[kCutItems];
+#pragma unroll
+    for (uint32_t i = 0; i < kCutItems; ++i) {
+        const uint32_t j = j0 + i;
+        key[i] = j < c.merged ? __ldg(cells + j) : (j < items ? __ldg(codes + (j - c.merged)) : 0u);
+    }
+    uint32_t f = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < kCutItems; ++i)
+        if (j0 + i < items && cut_drawn(c, j0 + i, key[i])) f |= 1u << i;
+    if (f != 0) atomicOr(&sMask[threadIdx.x >> 3], f << ((threadIdx.x & 7u) * kCutItems));
+    const uint32_t n = __reduce_add_sync(0xFFFFFFFFu, static_cast<uint32_t>(__popc(f)));
+    if ((threadIdx.x & 31u) == 0) sWarp[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x < kCutMaskWords) flags[static_cast<size_t>(blockIdx.x) * kCutMaskWords + threadIdx.x] = sMask[threadIdx.x];
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (uint32_t w = 0; w < kLodThreads / 32; ++w) total += sWarp[w];
+        blockCounts[blockIdx.x] = total;
+    }
+}
+
+// Then the tiles' counts become their first output slots (one block; integer
+// sums, so the order does not matter), and the last one the drawn total.
+constexpr uint32_t kCutScanThreads = 1024;
+__global__ void __launch_bounds__(kCutScanThreads)
+lod_cut_bases_kernel(const uint32_t* __restrict__ blockCounts, uint32_t tiles, uint32_t* __restrict__ tileBase,
+                     uint32_t* __restrict__ counts) {
+    __shared__ uint32_t sWarp[kCutScanThreads / 32];
+    uint32_t carry = 0;
+    for (uint32_t at = 0; at < tiles; at += kCutScanThreads) {
+        const uint32_t t = at + threadIdx.x;
+        const uint32_t v = t < tiles ? blockCounts[t] : 0u;
+        uint32_t total = 0;
+        const uint32_t ex = block_scan<kCutScanThreads>(v, sWarp, &total);
+        if (t < tiles) tileBase[t] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) counts[0] = carry;
+}
+
+// Last, every 256 items gather their drawn records (lod_gather.slang:18-33):
+// the tile's first slot plus the drawn items of the tile's earlier quarters
+// give the block's base; a ballot per warp and a block scan rank its items,
+// listed in order in shared memory; consecutive threads copy consecutive
+// outputs, the harmonics rows word by word. Drawn items past `capacity` are
+// counted, not written. counts[1] gets the merged Gaussians drawn (the rank
+// of the first splat item).
+constexpr uint32_t kCutGather = kLodThreads;   // items per gather block
+__global__ void __launch_bounds__(kLodThreads)
+lod_cut_gather_kernel(LodCutParams c, const uint32_t* __restrict__ flags, const uint32_t* __restrict__ tileBase,
+                      LodSplatArrays merged, LodSplatArrays store, LodSplatArrays out,
+                      uint32_t* __restrict__ counts) {
+    __shared__ uint32_t sWarp[kLodThreads / 32];
+    __shared__ uint32_t sItem[kCutGather];
+    constexpr uint32_t kQuarters = kCutTile / kCutGather;
+    constexpr uint32_t kQuarterWords = kCutGather / 32;
+    const uint32_t tile = blockIdx.x / kQuarters, quarter = blockIdx.x % kQuarters;
+    const uint32_t* mask = flags + static_cast<size_t>(tile) * kCutMaskWords;
+    uint32_t earlier = 0;   // drawn items of the tile's earlier quarters
+    for (uint32_t w = 0; w < quarter * kQuarterWords; ++w) earlier += static_cast<uint32_t>(__popc(__ldg(mask + w)));
+    const uint32_t base = __ldg(tileBase + tile) + earlier;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t bits = __ldg(mask + quarter * kQuarterWords + (threadIdx.x >> 5));
+    const bool drawn = (bits >> lane) & 1u;
+    const uint32_t j = blockIdx.x * kCutGather + threadIdx.x;
     uint32_t blockTotal = 0;
     const uint32_t local = block_scan<kLodThreads>(drawn ? 1u : 0u, sWarp, &blockTotal);
-    const uint32_t lastPart = (items + kLodThreads - 1) / kLodThreads - 1;
-    const uint32_t base = block_base(part, lastPart, blockTotal, status, counts, err, &sBase);
-    if (threadIdx.x == 0 && mergedDrawn != 0) atomicAdd(counts + 1, mergedDrawn);
-    if (drawn) {
-        sItem[local] = j;
-        const uint32_t o = base + local;
-        if (o < c.capacity) {
-            const bool isMerged = j < c.merged;
-            const uint32_t k = isMerged ? j : j - c.merged;
-            out.positions[o] = isMerged ? merged.positions[k] : store.positions[k];
-            out.shape[o] = isMerged ? merged.shape[k] : store.shape[k];
-        }
+    if (j == c.merged) counts[1] = base + local;
+    if (drawn) sItem[local] = j;
+    __syncthreads();
+    const uint32_t room = c.capacity > base ? min(blockTotal, c.capacity - base) : 0u;
+    for (uint32_t r = threadIdx.x; r < room; r += kLodThreads) {
+        const uint32_t o = base + r;
+        const uint32_t item = sItem[r];
+        const bool isMerged = item < c.merged;
+        const uint32_t k = isMerged ? item : item - c.merged;
+        out.positions[o] = isMerged ? merged.positions[k] : store.positions[k];
+        out.shape[o] = isMerged ? merged.shape[k] : store.shape[k];
     }
     if (c.shWords == 0) return;
-    __syncthreads();
-    // The drawn items' harmonics rows, copied by the whole block word by word.
-    const uint32_t words = blockTotal * c.shWords;
+    const uint32_t words = room * c.shWords;
     for (uint32_t w = threadIdx.x; w < words; w += kLodThreads) {
         const uint32_t r = w / c.shWords;
         const uint32_t col = w - r * c.shWords;
-        const uint32_t o = base + r;
-        if (o >= c.capacity) continue;
         const uint32_t item = sItem[r];
         const uint32_t* src = item < c.merged ? merged.sh + static_cast<size_t>(item) * c.shWords
                                               : store.sh + static_cast<size_t>(item - c.merged) * c.shWords;
-        out.sh[static_cast<size_t>(o) * c.shWords + col] = src[col];
+        out.sh[static_cast<size_t>(base + r) * c.shWords + col] = src[col];
     }
 }
 
@@ -642,15 +705,24 @@ cudaError_t launch_lod_finalize(const float* moments, uint32_t groups, uint32_t 
     return cudaGetLastError();
 }
 
+size_t lod_cut_scratch_bytes(uint32_t items) {
+    const size_t tiles = std::max<uint32_t>(blocks_for(items, kCutTile), 1u);
+    return tiles * (kCutMaskWords + 2) * sizeof(uint32_t) + 16;
+}
+
 cudaError_t launch_lod_cut(const LodCutParams& c, const uint32_t* cells, const uint32_t* codes,
                            const LodSplatArrays merged, const LodSplatArrays store, LodSplatArrays out,
-                           void* status, uint32_t* counts, uint32_t* err, cudaStream_t stream) {
+                           void* scratch, uint32_t* counts, cudaStream_t stream) {
     const uint32_t items = c.merged + c.count;
     if (items == 0) return cudaSuccess;
-    const uint32_t blocks = blocks_for(items, kLodThreads);
-    uint64_t* words = static_cast<uint64_t*>(status);
-    uint32_t* ticket = reinterpret_cast<uint32_t*>(words + blocks);
-    lod_cut_kernel<<<blocks, kLodThreads, 0, stream>>>(c, cells, codes, merged, store, out, words, ticket, counts, err);
+    const uint32_t tiles = blocks_for(items, kCutTile);
+    uint32_t* flags = static_cast<uint32_t*>(scratch);
+    uint32_t* tileCounts = flags + size_t{tiles} * kCutMaskWords;
+    uint32_t* tileBase = tileCounts + tiles;
+    lod_cut_decide_kernel<<<tiles, kLodThreads, 0, stream>>>(c, cells, codes, flags, tileCounts);
+    lod_cut_bases_kernel<<<1, kCutScanThreads, 0, stream>>>(tileCounts, tiles, tileBase, counts);
+    lod_cut_gather_kernel<<<blocks_for(items, kCutGather), kLodThreads, 0, stream>>>(c, flags, tileBase, merged,
+                                                                                     store, out, counts);
     return cudaGetLastError();
 }
 

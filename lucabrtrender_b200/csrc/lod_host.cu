@@ -4,8 +4,8 @@
 // A build waits twice: once for the bounds and every level's group count
 // (which size the levels' buffers), once at its end, when the group counts
 // the compactions found are checked against them. The reference waits and
-// reads once per level and once per stage. A select runs one kernel per
-// instance and waits once for all their counts; a cut whose drawn count
+// reads once per level and once per stage. A select runs one cut (two
+// kernels) per instance and waits once for all their counts; a cut whose drawn count
 // passes its cloud's capacity (possible only if the float size test were
 // not monotone down the tree) is grown and run again.
 #include "rast_handle.h"
@@ -83,8 +83,9 @@ lrt_gpu_splats view_of(uint32_t count, uint32_t rest, uint32_t shWords, const vo
     return s;
 }
 
-// Status bytes of one cut: the look-back words, then 4 words of counts.
-size_t cut_status_bytes(uint32_t items) { return lrt::compaction_status_bytes(items, lrt::lod_compaction_threads()) + 16; }
+// Scratch bytes of one cut: the cut's per-block bitmasks and counts, then 4
+// words: the drawn count, the merged count and an always-zero error word.
+size_t cut_status_bytes(uint32_t items) { return lrt::lod_cut_scratch_bytes(items) + 16; }
 
 // The cut's parameters for one instance in this view (Lod.cpp:400-426): the
 // eye in the cloud's space, and pixels per unit (the transform's largest
@@ -119,8 +120,8 @@ int run_cut(lrt_rast* r, const lrt_lod& lod, LodCutFrame& frame, const LodCutPar
     const uint32_t items = lod.merged + lod.count;
     const size_t statusBytes = cut_status_bytes(items);
     LRT_CUDA(r, ensure(frame.status, statusBytes), "cut scratch");
-    LRT_CUDA(r, cudaMemsetAsync(frame.status.ptr, 0, statusBytes, stream), "cut scratch");
     uint32_t* counts = reinterpret_cast<uint32_t*>(static_cast<char*>(frame.status.ptr) + statusBytes - 16);
+    LRT_CUDA(r, cudaMemsetAsync(counts, 0, 16, stream), "cut scratch");
     LodSplatArrays merged = {static_cast<float4*>(lod.mPositions.ptr), static_cast<uint4*>(lod.mShape.ptr),
                              static_cast<uint32_t*>(lod.mSh.ptr)};
     LodSplatArrays store = {static_cast<float4*>(lod.positions.ptr), static_cast<uint4*>(lod.shape.ptr),
@@ -128,7 +129,7 @@ int run_cut(lrt_rast* r, const lrt_lod& lod, LodCutFrame& frame, const LodCutPar
     LRT_CUDA(r, lrt::launch_lod_cut(c, static_cast<const uint32_t*>(lod.cells.ptr),
                                     static_cast<const uint32_t*>(lod.codes.ptr), merged, store,
                                     arrays_of(frame.positions, frame.shape, frame.sh), frame.status.ptr, counts,
-                                    counts + 2, stream),
+                                    stream),
              "cut");
     LRT_CUDA(r, cudaMemcpyAsync(hostCounts, counts, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "cut counts");
     return LRT_OK;
