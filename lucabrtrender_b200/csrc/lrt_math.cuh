@@ -176,6 +176,12 @@ LRT_HD uint32_t float_to_half(float f) {
     const uint32_t sign = (u >> 16) & 0x8000u;
     const uint32_t a = u & 0x7FFFFFFFu;
     if (a >= 0x7F800000u) return sign | (a > 0x7F800000u ? 0x7E00u : 0x7C00u);
+#if defined(__CUDA_ARCH__)
+    // The device's conversion instruction rounds to nearest even too
+    // (overflow to infinity, subnormal results exact), so only NaN, whose
+    // payload it would keep, takes the line above.
+    return __half_as_ushort(__float2half_rn(f));
+#else
     if (a >= 0x477FF000u) return sign | 0x7C00u;
     if (a < 0x38800000u) {
         const float v = bits_float(a) * 16777216.0f;
@@ -186,6 +192,7 @@ LRT_HD uint32_t float_to_half(float f) {
     const uint32_t rem = mant & 0x1FFFu;
     if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) h += 1;
     return sign | h;
+#endif
 }
 
 LRT_HD float low_half(uint32_t w) { return half_to_float(w & 0xFFFFu); }

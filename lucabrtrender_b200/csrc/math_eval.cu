@@ -1,4 +1,5 @@
-// Diagnostic: the rasteriser's own exp / log / sRGB / cut-off functions
+// Diagnostic: the rasteriser's own exp / log / sRGB / cut-off / float-to-half
+// functions
 // evaluated on the device, so tests can compare their bits with the host's.
 #include "../../include/lrt_raster.h"
 #include "kernels.cuh"
@@ -17,6 +18,8 @@ __global__ void math_eval_kernel(int fn, const float* __restrict__ x, float* __r
         case 1: out = lrt_log(v); break;
         case 2: out = srgb_to_linear(v); break;
         case 3: out = cutoff_power(v); break;
+        case 4: out = __uint_as_float(float_to_half(v)); break;
+        case 5: out = __uint_as_float(pack_halves(v, -0.5f * v)); break;
         default: out = NAN; break;
     }
     y[i] = out;
@@ -33,7 +36,7 @@ cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaS
 }  // namespace lrt
 
 extern "C" int lrt_math_eval(int fn, const void* x, void* y, uint32_t n, void* stream) {
-    if (fn < 0 || fn > 3 || (n > 0 && (x == nullptr || y == nullptr))) return LRT_INVALID_ARGUMENT;
+    if (fn < 0 || fn > 5 || (n > 0 && (x == nullptr || y == nullptr))) return LRT_INVALID_ARGUMENT;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = lrt::launch_math_eval(fn, static_cast<const float*>(x), static_cast<float*>(y), n, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

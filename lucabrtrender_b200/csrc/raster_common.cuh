@@ -183,8 +183,28 @@ __device__ __forceinline__ uint32_t encode_quaternion(float4 q0) {
 }
 
 __device__ __forceinline__ float half_safe(float v) { return fminf(fmaxf(v, -65000.0f), 65000.0f); }
+// a in the low half, b in the high one, each rounded to nearest even. The
+// paired conversion is one instruction on the arithmetic pipe (two scalar
+// conversions would take the slower conversion unit); a NaN takes the scalar
+// path, which gives the quiet NaN 0x7E00 the host restatement gives.
 __device__ __forceinline__ uint32_t pack_halves(float a, float b) {
-    return (float_to_half(a) & 0xFFFFu) | ((float_to_half(b) & 0xFFFFu) << 16);
+    if (isnan(a) || isnan(b)) return (float_to_half(a) & 0xFFFFu) | ((float_to_half(b) & 0xFFFFu) << 16);
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Asynchronous global -> shared copies (cp.async): a thread issues all of its
+// copies before it waits, so many lines are in flight at once.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
 }
 
 }  // namespace lrt

@@ -464,7 +464,8 @@ def device_view(ptr: int, shape: tuple, dtype: torch.dtype, device: int, sync: b
 
 
 def math_eval(fn: int, x: torch.Tensor) -> torch.Tensor:
-    """The library's own exp (0), log (1), sRGB-to-linear (2), cut-off power (3), on the device."""
+    """The library's own exp (0), log (1), sRGB-to-linear (2), cut-off power (3), float-to-half
+    bits (4) and the half pair (x, -x/2) (5), both as uint32 words in a float tensor, on the device."""
     y = torch.empty_like(x)
     _abi.check(_abi.load().lrt_math_eval(fn, x.data_ptr(), y.data_ptr(), x.numel(),
                                          torch.cuda.current_stream().cuda_stream), "math_eval")

@@ -879,6 +879,16 @@ void ora_math_eval(int fn, const float* x, float* y, uint32_t n) {
             case 1: y[i] = logImpl(x[i]); break;
             case 2: y[i] = srgbToLinear(x[i]); break;
             case 3: y[i] = cutoffPower(x[i]); break;
+            case 4: {
+                const uint32_t h = floatToHalf(x[i]);
+                std::memcpy(&y[i], &h, 4);
+                break;
+            }
+            case 5: {
+                const uint32_t h = packHalves(x[i], -0.5f * x[i]);
+                std::memcpy(&y[i], &h, 4);
+                break;
+            }
             default: y[i] = NAN; break;
         }
     }

@@ -275,3 +275,15 @@ def projected_edge(cells: np.ndarray, level: int, lo, extent: float, eye, pixels
         d.append(nearest - eye[k])
     dist = np.maximum(np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), f(1e-6))
     return (edge * f(pixels_per_unit)) / dist
+
+
+def half_sweep() -> np.ndarray:
+    """Floats for the float-to-half check: random bit patterns, every exponent,
+    the overflow and subnormal edges, and exact ties."""
+    rng = np.random.default_rng(5)
+    bits = rng.integers(0, 2**32, 400000, dtype=np.uint64).astype(np.uint32)
+    edges = np.float32([65504.0, 65519.996, 65520.0, 65536.0, 6.1035156e-05, 6.097555e-05, 5.9604645e-08,
+                        2.9802322e-08, 2.9802326e-08, 1e-45, 0.0, np.inf, 1.0 + 2.0**-11, 1.0 + 3 * 2.0**-11])
+    ties = ((rng.integers(0x1C400, 0x23C00, 20000, dtype=np.uint32) << np.uint32(13)) | np.uint32(0x1000)).view(np.float32)
+    x = np.concatenate([bits.view(np.float32), edges, -edges, ties])
+    return x[~np.isnan(x)]

@@ -107,6 +107,21 @@ def test_oracle_exp_log_accuracy():
     assert np.isnan(ora.math_eval(1, np.float32([-1.0]))[0])
 
 
+def test_oracle_half_rounding_is_ieee_nearest_even():
+    """fn 4 (the packing's float-to-half) rounds as IEEE binary16 nearest-even
+    (numpy's float16 conversion); NaN becomes the quiet NaN 0x7E00."""
+    x = H.half_sweep()
+    got = ora.math_eval(4, x).view(np.uint32)
+    with np.errstate(over="ignore"):
+        want = x.astype(np.float16).view(np.uint16).astype(np.uint32)
+    assert np.array_equal(got, want)
+    assert ora.math_eval(4, np.float32([np.nan])).view(np.uint32).tolist() == [0x7E00]
+    pair = ora.math_eval(5, x).view(np.uint32)
+    with np.errstate(over="ignore"):
+        high = (np.float32(-0.5) * x).astype(np.float16).view(np.uint16).astype(np.uint32)
+    assert np.array_equal(pair, want | (high << np.uint32(16)))
+
+
 # ------------------------------------------------------------- packing -----
 def _decode_splat(p: L.PackedSplats, i: int):
     """What shaders/lrt/test/splat_inspect.slang reads back: position, opacity,
