@@ -98,7 +98,17 @@ cudaError_t launch_splat_backward(const FrameParams& f, const float* means, cons
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
                                   const uint32_t* offsets, const float* partials, uint32_t partialPairs,
                                   float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
-                                  cudaStream_t stream, bool accumulate = false);
+                                  cudaStream_t stream);
+// The same over a chunk of up to 16 views (FrameParams in device memory,
+// touched and offsets one array of `count` per view), adding the views'
+// gradients in view order and writing each buffer once; accumulate: add to
+// what the buffers hold.
+cudaError_t launch_splat_backward_views(const FrameParams* framesDev, uint32_t views, uint32_t count,
+                                        const float* means, const float* logScales, const float* quats,
+                                        const float* logits, const uint16_t* sh, const uint32_t* touched,
+                                        const uint32_t* offsets, const float* partials, uint32_t partialPairs,
+                                        float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
+                                        bool accumulate, cudaStream_t stream);
 
 cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaStream_t stream);
 

@@ -37,8 +37,9 @@ struct lrt_rast {
     DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
     DeviceBuffer lossScratch;                            // the L1 loss's per-block sums
     // Training batches (train_batch.cu): colour gradients, view parameters
-    // and queue, losses with no caller buffer; their pair capacity.
-    DeviceBuffer trainBatchGrad, trainBatchViews, trainBatchLoss;
+    // and queue, losses with no caller buffer, the chunk's frame parameters;
+    // their pair capacity.
+    DeviceBuffer trainBatchGrad, trainBatchViews, trainBatchLoss, trainBatchFrames;
     uint32_t trainBatchPairCap = 0;
     void* metricHost = nullptr;                          // pinned readback of the metrics
     size_t metricHostBytes = 0;

@@ -62,7 +62,7 @@ void lrt_rast_destroy(lrt_rast* r) {
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
                             &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
-                            &r->trainBatchViews, &r->trainBatchLoss})
+                            &r->trainBatchViews, &r->trainBatchLoss, &r->trainBatchFrames})
         release(*b);
     if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);

@@ -15,6 +15,7 @@ namespace lrt {
 namespace {
 
 constexpr uint32_t kThreads = 128;
+constexpr uint32_t kMaxChunkViews = 16;   // views one splat_backward_views launch takes
 constexpr float kC1 = 0.4886025119029199f;
 __device__ constexpr float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
                           0.5462742152960396f};
@@ -71,39 +72,235 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-// kAccumulate: add this frame's gradients to what the buffers hold (the
-// views of a batch after the first, in view order); a splat this frame does
-// not touch then adds nothing and writes nothing.
-template <bool kAccumulate>
-__global__ void __launch_bounds__(kThreads, 4)
-splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
-                      const float* __restrict__ quats, const float* __restrict__ logits,
-                      const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
-                      const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
-                      uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
-                      float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh) {
-    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31u;
-    const bool live = i < f.count;
-    const uint32_t slot = f.base + i;
-    // The parameters and SH row are read only after the partials are summed;
-    // ask for them now (into L2, no registers held), so their DRAM latency
-    // overlaps the count, offset and partial loads that each wait on the last.
-    if (live) {
-        prefetch_l2(means + 3 * static_cast<size_t>(i));
-        prefetch_l2(logScales + 3 * static_cast<size_t>(i));
-        prefetch_l2(quats + 4 * static_cast<size_t>(i));
-        prefetch_l2(logits + i);
-        prefetch_l2(sh + 48 * static_cast<size_t>(i));
-        prefetch_l2(sh + 48 * static_cast<size_t>(i) + 40);
+// One view's gradients of splat i from its summed partials g: the per-view
+// means, log-scale, quaternion and logit gradients added into gm, gls, gq,
+// glog (which the caller zeroes), and the 48 SH gradients handed to
+// sink(q, value) in coefficient order.
+template <class ShSink>
+__device__ __forceinline__ void view_grads(const FrameParams& f, uint32_t i, const float* __restrict__ means,
+                                           const float* __restrict__ logScales, const float* __restrict__ quats,
+                                           const float* __restrict__ logits, const uint16_t* __restrict__ sh,
+                                           const float (&g)[9], float (&gm)[3], float (&gls)[3], float (&gq)[4],
+                                           float& glog, ShSink&& sink) {
+    const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
+
+    // ---- forward intermediates ------------------------------------------
+    const float px = means[3 * i], py = means[3 * i + 1], pz = means[3 * i + 2];
+    const float sig = 1.0f / (1.0f + lrt_exp(-logits[i]));
+    const float s0 = lrt_exp(logScales[3 * i]), s1 = lrt_exp(logScales[3 * i + 1]), s2 = lrt_exp(logScales[3 * i + 2]);
+    const float qw0 = quats[4 * i], qx0 = quats[4 * i + 1], qy0 = quats[4 * i + 2], qz0 = quats[4 * i + 3];
+    const float len = sqrtf(qw0 * qw0 + qx0 * qx0 + qy0 * qy0 + qz0 * qz0);
+    const bool unitQ = len > 0.0f;
+    const float x = unitQ ? qx0 / len : 0.0f, y = unitQ ? qy0 / len : 0.0f, z = unitQ ? qz0 / len : 0.0f,
+                w = unitQ ? qw0 / len : 1.0f;
+    const float3 t = to_view(f, make_float3(px, py, pz));
+    const float R[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
+                           {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
+                           {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}};
+    const float S[3] = {s0, s1, s2};
+    float M[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) M[a][b] = R[a][b] * S[b];
+    const float W[3][3] = {{f.m[0], f.m[1], f.m[2]}, {f.m[4], f.m[5], f.m[6]}, {f.m[8], f.m[9], f.m[10]}};
+    float jx0, jx2, jy1, jy2;
+    bool clampX = false, clampY = false;
+    float limX = 0.0f, limY = 0.0f;
+    const float invZ = 1.0f / t.z;
+    if (f.ortho) {
+        jx0 = f.focalX; jx2 = 0.0f; jy1 = f.focalY; jy2 = 0.0f;
+    } else {
+        const float limLoX = (-0.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+        const float limHiX = (1.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
+        const float limLoY = (-0.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+        const float limHiY = (1.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
+        const float ux = t.x * invZ, uy = t.y * invZ;
+        clampX = ux < limLoX || ux > limHiX;
+        clampY = uy < limLoY || uy > limHiY;
+        limX = ux < limLoX ? limLoX : limHiX;
+        limY = uy < limLoY ? limLoY : limHiY;
+        const float tx = clampf(ux, limLoX, limHiX) * t.z;
+        const float ty = clampf(uy, limLoY, limHiY) * t.z;
+        jx0 = f.focalX * invZ; jx2 = -f.focalX * tx * invZ * invZ;
+        jy1 = f.focalY * invZ; jy2 = -f.focalY * ty * invZ * invZ;
     }
+    float T2x[3], T2y[3], ax[3], ay[3];
+    for (int c = 0; c < 3; ++c) {
+        T2x[c] = jx0 * W[0][c] + jx2 * W[2][c];
+        T2y[c] = jy1 * W[1][c] + jy2 * W[2][c];
+    }
+    for (int c = 0; c < 3; ++c) {
+        ax[c] = T2x[0] * M[0][c] + T2x[1] * M[1][c] + T2x[2] * M[2][c];
+        ay[c] = T2y[0] * M[0][c] + T2y[1] * M[1][c] + T2y[2] * M[2][c];
+    }
+    const float ap = ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2];
+    const float bp = ax[0] * ay[0] + ax[1] * ay[1] + ax[2] * ay[2];
+    const float cp = ay[0] * ay[0] + ay[1] * ay[1] + ay[2] * ay[2];
+    const float detB = ap * cp - bp * bp;
+    const float a = ap + 0.3f, c = cp + 0.3f, b = bp;
+    const float det = a * c - b * b;
+    const float aa = f.antialias != 0 ? sqrtf(fmaxf(detB, 0.0f) / det) : 1.0f;
+    const float QA = c / det, QB = -b / det, QC = a / det;
+
+    // ---- colour ---------------------------------------------------------------
+    float coef[48];   // the fp16 coefficients, read as six 16-byte vectors
+    {
+        const uint4* rv = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(i) * 48);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const uint4 w4 = __ldg(rv + q);
+            const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                coef[q * 8 + 2 * h] = low_half(ws[h]);
+                coef[q * 8 + 2 * h + 1] = high_half(ws[h]);
+            }
+        }
+    }
+    float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
+    const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
+    const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
+    const uint32_t degree = min(3u, f.shLimit);   // bas[] is 0 above it
+    float bas[15], bgx[15], bgy[15], bgz[15];
+    sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
+    float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        constexpr float kSH0 = 0.28209479177387814f;
+        const float base = 0.5f + kSH0 * coef[ch];
+        float rest = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 15; ++k) rest += bas[k] * coef[3 + 3 * k + ch];
+        // colour = max(base + rest, 0): no gradient where clamped. Basis
+        // functions above the evaluated degree are 0, so their
+        // coefficients get 0.
+        const float gcol = base + rest > 0.0f ? g[6 + ch] : 0.0f;
+        sink(ch, kSH0 * gcol);
+#pragma unroll
+        for (int k = 0; k < 15; ++k) {
+            sink(3 + 3 * k + ch, bas[k] * gcol);
+            const float cg = coef[3 + 3 * k + ch] * gcol;
+            gdx += cg * bgx[k];
+            gdy += cg * bgy[k];
+            gdz += cg * bgz[k];
+        }
+    }
+    {   // dir = v / |v|, v = p - eye
+        const float dotd = gdx * dirx + gdy * diry + gdz * dirz;
+        gm[0] += (gdx - dotd * dirx) / vl;
+        gm[1] += (gdy - dotd * diry) / vl;
+        gm[2] += (gdz - dotd * dirz) / vl;
+    }
+
+    // ---- alpha0 = sigmoid(logit) * aa -----------------------------------------
+    glog = gAlpha * aa * sig * (1.0f - sig);
+    const float gAA = gAlpha * sig;
+    float gDetB = 0.0f, gDet = 0.0f;
+    if (f.antialias != 0 && detB > 0.0f && aa > 0.0f) {
+        gDetB = gAA / (2.0f * aa * det);
+        gDet = -gAA * aa / (2.0f * det);
+    }
+
+    // ---- conic = inverse of [[a, b], [b, c]] ------------------------------------
+    // G_Sigma = -Q G_Q Q with G_Q = [[gA, gB/2], [gB/2, gC]]
+    const float h = 0.5f * gB;
+    const float t00 = gA * QA + h * QB, t01 = gA * QB + h * QC;
+    const float t10 = h * QA + gC * QB, t11 = h * QB + gC * QC;
+    const float gS00 = -(QA * t00 + QB * t10), gS01 = -(QA * t01 + QB * t11);
+    const float gS11 = -(QB * t01 + QC * t11);
+    float ga = gS00 + gDet * c + gDetB * cp;
+    float gc = gS11 + gDet * a + gDetB * ap;
+    float gb = 2.0f * gS01 - gDet * 2.0f * b - gDetB * 2.0f * bp;
+
+    // ---- a' = ax.ax, b' = ax.ay, c' = ay.ay --------------------------------
+    float gax[3], gay[3];
+    for (int k = 0; k < 3; ++k) {
+        gax[k] = 2.0f * ga * ax[k] + gb * ay[k];
+        gay[k] = gb * ax[k] + 2.0f * gc * ay[k];
+    }
+    // ax = T2x M, ay = T2y M
+    float gT2x[3], gT2y[3], gM[3][3];
+    for (int r = 0; r < 3; ++r) {
+        gT2x[r] = gax[0] * M[r][0] + gax[1] * M[r][1] + gax[2] * M[r][2];
+        gT2y[r] = gay[0] * M[r][0] + gay[1] * M[r][1] + gay[2] * M[r][2];
+        for (int cc = 0; cc < 3; ++cc) gM[r][cc] = T2x[r] * gax[cc] + T2y[r] * gay[cc];
+    }
+    // M = R diag(S)
+    float gR[3][3];
+    for (int cc = 0; cc < 3; ++cc) {
+        float gs = 0.0f;
+        for (int r = 0; r < 3; ++r) {
+            gR[r][cc] = gM[r][cc] * S[cc];
+            gs += gM[r][cc] * R[r][cc];
+        }
+        gls[cc] = gs * S[cc];
+    }
+    // R(x, y, z, w)
+    const float gx = 2.0f * (gR[0][1] * y + gR[0][2] * z + gR[1][0] * y - 2.0f * gR[1][1] * x - gR[1][2] * w +
+                             gR[2][0] * z + gR[2][1] * w - 2.0f * gR[2][2] * x);
+    const float gy = 2.0f * (-2.0f * gR[0][0] * y + gR[0][1] * x + gR[0][2] * w + gR[1][0] * x + gR[1][2] * z -
+                             gR[2][0] * w + gR[2][1] * z - 2.0f * gR[2][2] * y);
+    const float gz = 2.0f * (-2.0f * gR[0][0] * z - gR[0][1] * w + gR[0][2] * x + gR[1][0] * w -
+                             2.0f * gR[1][1] * z + gR[1][2] * y + gR[2][0] * x + gR[2][1] * y);
+    const float gw = 2.0f * (-gR[0][1] * z + gR[0][2] * y + gR[1][0] * z - gR[1][2] * x - gR[2][0] * y +
+                             gR[2][1] * x);
+    if (unitQ) {   // q_n = q / |q|
+        const float dq = gx * x + gy * y + gz * z + gw * w;
+        gq[0] = (gw - dq * w) / len;
+        gq[1] = (gx - dq * x) / len;
+        gq[2] = (gy - dq * y) / len;
+        gq[3] = (gz - dq * z) / len;
+    }
+    // T2 = J W
+    float gjx0 = 0.0f, gjx2 = 0.0f, gjy1 = 0.0f, gjy2 = 0.0f;
+    for (int cc = 0; cc < 3; ++cc) {
+        gjx0 += gT2x[cc] * W[0][cc];
+        gjx2 += gT2x[cc] * W[2][cc];
+        gjy1 += gT2y[cc] * W[1][cc];
+        gjy2 += gT2y[cc] * W[2][cc];
+    }
+    float gt[3] = {0.0f, 0.0f, 0.0f};
+    if (f.ortho) {
+        gt[0] += gcx * f.focalX;
+        gt[1] += gcy * f.focalY;
+    } else {
+        // centre = focal t.xy / t.z + c
+        gt[0] += gcx * f.focalX * invZ;
+        gt[1] += gcy * f.focalY * invZ;
+        gt[2] += -(gcx * f.focalX * t.x + gcy * f.focalY * t.y) * invZ * invZ;
+        // J: jx0 = fx / tz, jx2 = -fx tx_c / tz^2 (tx_c = t.x, or lim tz when clamped)
+        gt[2] += -(gjx0 * f.focalX + gjy1 * f.focalY) * invZ * invZ;
+        if (clampX) {
+            gt[2] += gjx2 * f.focalX * limX * invZ * invZ;
+        } else {
+            gt[0] += -gjx2 * f.focalX * invZ * invZ;
+            gt[2] += 2.0f * gjx2 * f.focalX * t.x * invZ * invZ * invZ;
+        }
+        if (clampY) {
+            gt[2] += gjy2 * f.focalY * limY * invZ * invZ;
+        } else {
+            gt[1] += -gjy2 * f.focalY * invZ * invZ;
+            gt[2] += 2.0f * gjy2 * f.focalY * t.y * invZ * invZ * invZ;
+        }
+    }
+    // t = W p + t0
+    for (int k = 0; k < 3; ++k) gm[k] += W[0][k] * gt[0] + W[1][k] * gt[1] + W[2][k] * gt[2];
+}
+
+// The partials of the splat at `slot` in a frame (touched[slot] pairs from
+// pair offsets[slot] of `partials`), summed into g; every lane of the warp
+// takes part. nOut comes back 0 for a dead lane or a pair range outside the
+// buffer.
+__device__ __forceinline__ void splat_partials(bool live, uint32_t slot, uint32_t lane, const uint32_t* __restrict__ touched,
+                                               const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
+                                               uint32_t partialPairs, float (&g)[9], uint32_t& nOut) {
     uint32_t n = live ? touched[slot] : 0u;
     const uint32_t firstRaw = live ? offsets[slot] : 0u;   // loaded beside the count, not after it
     const uint32_t first = n != 0 ? firstRaw : 0u;
     // Reads stay inside the partials buffer even for a frame whose pairs
     // overflowed their buffer (the host reports that frame as an error).
     n = first >= partialPairs ? 0u : min(n, partialPairs - first);
-    float g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) g[q] = 0.0f;
     const float4* part4 = reinterpret_cast<const float4*>(partials);
     if (n <= kSolo) sum_partials(part4 + static_cast<size_t>(first) * 3, n, g);
     uint32_t many = __ballot_sync(0xFFFFFFFFu, n > kSolo);
@@ -130,8 +327,37 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
             for (int q = 0; q < 9; ++q) g[q] = h[q];
         }
     }
+    nOut = n;
+}
+
+// One frame: every splat's gradients written (zero for a splat the frame
+// does not touch).
+__global__ void __launch_bounds__(kThreads, 4)
+splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
+                      const float* __restrict__ quats, const float* __restrict__ logits,
+                      const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
+                      const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
+                      uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
+                      float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh) {
+    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool live = i < f.count;
+    const uint32_t slot = f.base + i;
+    // The parameters and SH row are read only after the partials are summed;
+    // ask for them now (into L2, no registers held), so their DRAM latency
+    // overlaps the count, offset and partial loads that each wait on the last.
+    if (live) {
+        prefetch_l2(means + 3 * static_cast<size_t>(i));
+        prefetch_l2(logScales + 3 * static_cast<size_t>(i));
+        prefetch_l2(quats + 4 * static_cast<size_t>(i));
+        prefetch_l2(logits + i);
+        prefetch_l2(sh + 48 * static_cast<size_t>(i));
+        prefetch_l2(sh + 48 * static_cast<size_t>(i) + 40);
+    }
+    float g[9];
+    uint32_t n = 0;
+    splat_partials(live, slot, lane, touched, offsets, partials, partialPairs, g, n);
     if (!live) return;
-    if (kAccumulate && n == 0) return;
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
     float* gshRow = gSh + static_cast<size_t>(i) * 48;
     if (n == 0) {
@@ -139,230 +365,12 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
 #pragma unroll
         for (int q = 0; q < 12; ++q) out[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
-        const float gcx = g[0], gcy = g[1], gA = g[2], gB = g[3], gC = g[4], gAlpha = g[5];
-
-        // ---- forward intermediates ------------------------------------------
-        const float px = means[3 * i], py = means[3 * i + 1], pz = means[3 * i + 2];
-        const float sig = 1.0f / (1.0f + lrt_exp(-logits[i]));
-        const float s0 = lrt_exp(logScales[3 * i]), s1 = lrt_exp(logScales[3 * i + 1]), s2 = lrt_exp(logScales[3 * i + 2]);
-        const float qw0 = quats[4 * i], qx0 = quats[4 * i + 1], qy0 = quats[4 * i + 2], qz0 = quats[4 * i + 3];
-        const float len = sqrtf(qw0 * qw0 + qx0 * qx0 + qy0 * qy0 + qz0 * qz0);
-        const bool unitQ = len > 0.0f;
-        const float x = unitQ ? qx0 / len : 0.0f, y = unitQ ? qy0 / len : 0.0f, z = unitQ ? qz0 / len : 0.0f,
-                    w = unitQ ? qw0 / len : 1.0f;
-        const float3 t = to_view(f, make_float3(px, py, pz));
-        const float R[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
-                               {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
-                               {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}};
-        const float S[3] = {s0, s1, s2};
-        float M[3][3];
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) M[a][b] = R[a][b] * S[b];
-        const float W[3][3] = {{f.m[0], f.m[1], f.m[2]}, {f.m[4], f.m[5], f.m[6]}, {f.m[8], f.m[9], f.m[10]}};
-        float jx0, jx2, jy1, jy2;
-        bool clampX = false, clampY = false;
-        float limX = 0.0f, limY = 0.0f;
-        const float invZ = 1.0f / t.z;
-        if (f.ortho) {
-            jx0 = f.focalX; jx2 = 0.0f; jy1 = f.focalY; jy2 = 0.0f;
-        } else {
-            const float limLoX = (-0.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
-            const float limHiX = (1.15f * static_cast<float>(f.width) - f.centreX) / f.focalX;
-            const float limLoY = (-0.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
-            const float limHiY = (1.15f * static_cast<float>(f.height) - f.centreY) / f.focalY;
-            const float ux = t.x * invZ, uy = t.y * invZ;
-            clampX = ux < limLoX || ux > limHiX;
-            clampY = uy < limLoY || uy > limHiY;
-            limX = ux < limLoX ? limLoX : limHiX;
-            limY = uy < limLoY ? limLoY : limHiY;
-            const float tx = clampf(ux, limLoX, limHiX) * t.z;
-            const float ty = clampf(uy, limLoY, limHiY) * t.z;
-            jx0 = f.focalX * invZ; jx2 = -f.focalX * tx * invZ * invZ;
-            jy1 = f.focalY * invZ; jy2 = -f.focalY * ty * invZ * invZ;
-        }
-        float T2x[3], T2y[3], ax[3], ay[3];
-        for (int c = 0; c < 3; ++c) {
-            T2x[c] = jx0 * W[0][c] + jx2 * W[2][c];
-            T2y[c] = jy1 * W[1][c] + jy2 * W[2][c];
-        }
-        for (int c = 0; c < 3; ++c) {
-            ax[c] = T2x[0] * M[0][c] + T2x[1] * M[1][c] + T2x[2] * M[2][c];
-            ay[c] = T2y[0] * M[0][c] + T2y[1] * M[1][c] + T2y[2] * M[2][c];
-        }
-        const float ap = ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2];
-        const float bp = ax[0] * ay[0] + ax[1] * ay[1] + ax[2] * ay[2];
-        const float cp = ay[0] * ay[0] + ay[1] * ay[1] + ay[2] * ay[2];
-        const float detB = ap * cp - bp * bp;
-        const float a = ap + 0.3f, c = cp + 0.3f, b = bp;
-        const float det = a * c - b * b;
-        const float aa = f.antialias != 0 ? sqrtf(fmaxf(detB, 0.0f) / det) : 1.0f;
-        const float QA = c / det, QB = -b / det, QC = a / det;
-
-        // ---- colour ---------------------------------------------------------------
-        float coef[48];   // the fp16 coefficients, read as six 16-byte vectors
-        {
-            const uint4* rv = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(i) * 48);
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const uint4 w4 = __ldg(rv + q);
-                const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    coef[q * 8 + 2 * h] = low_half(ws[h]);
-                    coef[q * 8 + 2 * h + 1] = high_half(ws[h]);
-                }
-            }
-        }
-        float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
-        const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
-        const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
-        const uint32_t degree = min(3u, f.shLimit);   // bas[] is 0 above it
-        float bas[15], bgx[15], bgy[15], bgz[15];
-        sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
-        float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
         float gsh[48];
+        view_grads(f, i, means, logScales, quats, logits, sh, g, gm, gls, gq, glog,
+                   [&](int q, float v) { gsh[q] = v; });
+        float4* out = reinterpret_cast<float4*>(gshRow);
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-            constexpr float kSH0 = 0.28209479177387814f;
-            const float base = 0.5f + kSH0 * coef[ch];
-            float rest = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 15; ++k) rest += bas[k] * coef[3 + 3 * k + ch];
-            // colour = max(base + rest, 0): no gradient where clamped. Basis
-            // functions above the evaluated degree are 0, so their
-            // coefficients get 0.
-            const float gcol = base + rest > 0.0f ? g[6 + ch] : 0.0f;
-            gsh[ch] = kSH0 * gcol;
-#pragma unroll
-            for (int k = 0; k < 15; ++k) {
-                gsh[3 + 3 * k + ch] = bas[k] * gcol;
-                const float cg = coef[3 + 3 * k + ch] * gcol;
-                gdx += cg * bgx[k];
-                gdy += cg * bgy[k];
-                gdz += cg * bgz[k];
-            }
-        }
-        {
-            float4* out = reinterpret_cast<float4*>(gshRow);
-#pragma unroll
-            for (int q = 0; q < 12; ++q) {
-                float4 v = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
-                if (kAccumulate) {
-                    const float4 o = out[q];
-                    v = make_float4(o.x + v.x, o.y + v.y, o.z + v.z, o.w + v.w);
-                }
-                out[q] = v;
-            }
-        }
-        {   // dir = v / |v|, v = p - eye
-            const float dotd = gdx * dirx + gdy * diry + gdz * dirz;
-            gm[0] += (gdx - dotd * dirx) / vl;
-            gm[1] += (gdy - dotd * diry) / vl;
-            gm[2] += (gdz - dotd * dirz) / vl;
-        }
-
-        // ---- alpha0 = sigmoid(logit) * aa -----------------------------------------
-        glog = gAlpha * aa * sig * (1.0f - sig);
-        const float gAA = gAlpha * sig;
-        float gDetB = 0.0f, gDet = 0.0f;
-        if (f.antialias != 0 && detB > 0.0f && aa > 0.0f) {
-            gDetB = gAA / (2.0f * aa * det);
-            gDet = -gAA * aa / (2.0f * det);
-        }
-
-        // ---- conic = inverse of [[a, b], [b, c]] ------------------------------------
-        // G_Sigma = -Q G_Q Q with G_Q = [[gA, gB/2], [gB/2, gC]]
-        const float h = 0.5f * gB;
-        const float t00 = gA * QA + h * QB, t01 = gA * QB + h * QC;
-        const float t10 = h * QA + gC * QB, t11 = h * QB + gC * QC;
-        const float gS00 = -(QA * t00 + QB * t10), gS01 = -(QA * t01 + QB * t11);
-        const float gS11 = -(QB * t01 + QC * t11);
-        float ga = gS00 + gDet * c + gDetB * cp;
-        float gc = gS11 + gDet * a + gDetB * ap;
-        float gb = 2.0f * gS01 - gDet * 2.0f * b - gDetB * 2.0f * bp;
-
-        // ---- a' = ax.ax, b' = ax.ay, c' = ay.ay --------------------------------
-        float gax[3], gay[3];
-        for (int k = 0; k < 3; ++k) {
-            gax[k] = 2.0f * ga * ax[k] + gb * ay[k];
-            gay[k] = gb * ax[k] + 2.0f * gc * ay[k];
-        }
-        // ax = T2x M, ay = T2y M
-        float gT2x[3], gT2y[3], gM[3][3];
-        for (int r = 0; r < 3; ++r) {
-            gT2x[r] = gax[0] * M[r][0] + gax[1] * M[r][1] + gax[2] * M[r][2];
-            gT2y[r] = gay[0] * M[r][0] + gay[1] * M[r][1] + gay[2] * M[r][2];
-            for (int cc = 0; cc < 3; ++cc) gM[r][cc] = T2x[r] * gax[cc] + T2y[r] * gay[cc];
-        }
-        // M = R diag(S)
-        float gR[3][3];
-        for (int cc = 0; cc < 3; ++cc) {
-            float gs = 0.0f;
-            for (int r = 0; r < 3; ++r) {
-                gR[r][cc] = gM[r][cc] * S[cc];
-                gs += gM[r][cc] * R[r][cc];
-            }
-            gls[cc] = gs * S[cc];
-        }
-        // R(x, y, z, w)
-        const float gx = 2.0f * (gR[0][1] * y + gR[0][2] * z + gR[1][0] * y - 2.0f * gR[1][1] * x - gR[1][2] * w +
-                                 gR[2][0] * z + gR[2][1] * w - 2.0f * gR[2][2] * x);
-        const float gy = 2.0f * (-2.0f * gR[0][0] * y + gR[0][1] * x + gR[0][2] * w + gR[1][0] * x + gR[1][2] * z -
-                                 gR[2][0] * w + gR[2][1] * z - 2.0f * gR[2][2] * y);
-        const float gz = 2.0f * (-2.0f * gR[0][0] * z - gR[0][1] * w + gR[0][2] * x + gR[1][0] * w -
-                                 2.0f * gR[1][1] * z + gR[1][2] * y + gR[2][0] * x + gR[2][1] * y);
-        const float gw = 2.0f * (-gR[0][1] * z + gR[0][2] * y + gR[1][0] * z - gR[1][2] * x - gR[2][0] * y +
-                                 gR[2][1] * x);
-        if (unitQ) {   // q_n = q / |q|
-            const float dq = gx * x + gy * y + gz * z + gw * w;
-            gq[0] = (gw - dq * w) / len;
-            gq[1] = (gx - dq * x) / len;
-            gq[2] = (gy - dq * y) / len;
-            gq[3] = (gz - dq * z) / len;
-        }
-        // T2 = J W
-        float gjx0 = 0.0f, gjx2 = 0.0f, gjy1 = 0.0f, gjy2 = 0.0f;
-        for (int cc = 0; cc < 3; ++cc) {
-            gjx0 += gT2x[cc] * W[0][cc];
-            gjx2 += gT2x[cc] * W[2][cc];
-            gjy1 += gT2y[cc] * W[1][cc];
-            gjy2 += gT2y[cc] * W[2][cc];
-        }
-        float gt[3] = {0.0f, 0.0f, 0.0f};
-        if (f.ortho) {
-            gt[0] += gcx * f.focalX;
-            gt[1] += gcy * f.focalY;
-        } else {
-            // centre = focal t.xy / t.z + c
-            gt[0] += gcx * f.focalX * invZ;
-            gt[1] += gcy * f.focalY * invZ;
-            gt[2] += -(gcx * f.focalX * t.x + gcy * f.focalY * t.y) * invZ * invZ;
-            // J: jx0 = fx / tz, jx2 = -fx tx_c / tz^2 (tx_c = t.x, or lim tz when clamped)
-            gt[2] += -(gjx0 * f.focalX + gjy1 * f.focalY) * invZ * invZ;
-            if (clampX) {
-                gt[2] += gjx2 * f.focalX * limX * invZ * invZ;
-            } else {
-                gt[0] += -gjx2 * f.focalX * invZ * invZ;
-                gt[2] += 2.0f * gjx2 * f.focalX * t.x * invZ * invZ * invZ;
-            }
-            if (clampY) {
-                gt[2] += gjy2 * f.focalY * limY * invZ * invZ;
-            } else {
-                gt[1] += -gjy2 * f.focalY * invZ * invZ;
-                gt[2] += 2.0f * gjy2 * f.focalY * t.y * invZ * invZ * invZ;
-            }
-        }
-        // t = W p + t0
-        for (int k = 0; k < 3; ++k) gm[k] += W[0][k] * gt[0] + W[1][k] * gt[1] + W[2][k] * gt[2];
-    }
-    if (kAccumulate) {
-        for (int k = 0; k < 3; ++k) {
-            gMeans[3 * i + k] = gMeans[3 * i + k] + gm[k];
-            gLogScales[3 * i + k] = gLogScales[3 * i + k] + gls[k];
-        }
-        for (int k = 0; k < 4; ++k) gQuats[4 * i + k] = gQuats[4 * i + k] + gq[k];
-        gLogits[i] = gLogits[i] + glog;
-        return;
+        for (int q = 0; q < 12; ++q) out[q] = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
     }
     for (int k = 0; k < 3; ++k) {
         gMeans[3 * i + k] = gm[k];
@@ -372,23 +380,113 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     gLogits[i] = glog;
 }
 
+// A chunk of views in one pass. Per splat, view after view in order, the
+// view's gradients (view_grads, as above) are added to running sums -- the
+// 48 SH ones in shared memory, a column per thread -- and the sums written
+// once at the end, so the gradient buffers are read and written once a chunk
+// rather than once a view. The sums start from what the buffers hold when
+// `accumulate` is set (a batch's later chunks), else from zero: the same
+// float additions, in the same order, as a view-by-view pass adding each
+// view to the buffers. touched / offsets: one array of `count` per view.
+__global__ void __launch_bounds__(kThreads, 3)
+splat_backward_views_kernel(const FrameParams* __restrict__ frames, uint32_t views, uint32_t count,
+                            const float* __restrict__ means, const float* __restrict__ logScales,
+                            const float* __restrict__ quats, const float* __restrict__ logits,
+                            const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
+                            const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
+                            uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
+                            float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh,
+                            uint32_t accumulate) {
+    __shared__ float sAcc[48][kThreads];
+    __shared__ FrameParams sF[kMaxChunkViews];
+    {
+        const uint32_t words = views * static_cast<uint32_t>(sizeof(FrameParams) / 4);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(frames);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sF);
+        for (uint32_t w = threadIdx.x; w < words; w += kThreads) dst[w] = src[w];
+    }
+    const uint32_t tid = threadIdx.x;
+    const uint32_t i = blockIdx.x * kThreads + tid;
+    const uint32_t lane = tid & 31u;
+    const bool live = i < count;
+    float am[3] = {0, 0, 0}, als[3] = {0, 0, 0}, aq[4] = {0, 0, 0, 0}, alog = 0.0f;
+    float4* shRow = reinterpret_cast<float4*>(gSh + static_cast<size_t>(i) * 48);
+    if (live && accumulate != 0) {
+        for (int k = 0; k < 3; ++k) {
+            am[k] = gMeans[3 * i + k];
+            als[k] = gLogScales[3 * i + k];
+        }
+        for (int k = 0; k < 4; ++k) aq[k] = gQuats[4 * i + k];
+        alog = gLogits[i];
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            const float4 v = shRow[q];
+            sAcc[4 * q][tid] = v.x;
+            sAcc[4 * q + 1][tid] = v.y;
+            sAcc[4 * q + 2][tid] = v.z;
+            sAcc[4 * q + 3][tid] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 48; ++q) sAcc[q][tid] = 0.0f;
+    }
+    __syncthreads();
+    for (uint32_t v = 0; v < views; ++v) {
+        const FrameParams& f = sF[v];
+        float g[9];
+        uint32_t n = 0;
+        splat_partials(live, f.base + i, lane, touched + static_cast<size_t>(v) * count,
+                       offsets + static_cast<size_t>(v) * count, partials, partialPairs, g, n);
+        if (!live || n == 0) continue;
+        float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
+        view_grads(f, i, means, logScales, quats, logits, sh, g, gm, gls, gq, glog,
+                   [&](int q, float x) { sAcc[q][tid] = sAcc[q][tid] + x; });
+        for (int k = 0; k < 3; ++k) {
+            am[k] = am[k] + gm[k];
+            als[k] = als[k] + gls[k];
+        }
+        for (int k = 0; k < 4; ++k) aq[k] = aq[k] + gq[k];
+        alog = alog + glog;
+    }
+    if (!live) return;
+    for (int k = 0; k < 3; ++k) {
+        gMeans[3 * i + k] = am[k];
+        gLogScales[3 * i + k] = als[k];
+    }
+    for (int k = 0; k < 4; ++k) gQuats[4 * i + k] = aq[k];
+    gLogits[i] = alog;
+#pragma unroll
+    for (int q = 0; q < 12; ++q)
+        shRow[q] = make_float4(sAcc[4 * q][tid], sAcc[4 * q + 1][tid], sAcc[4 * q + 2][tid], sAcc[4 * q + 3][tid]);
+}
+
 }  // namespace
+
+cudaError_t launch_splat_backward_views(const FrameParams* framesDev, uint32_t views, uint32_t count,
+                                        const float* means, const float* logScales, const float* quats,
+                                        const float* logits, const uint16_t* sh, const uint32_t* touched,
+                                        const uint32_t* offsets, const float* partials, uint32_t partialPairs,
+                                        float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
+                                        bool accumulate, cudaStream_t stream) {
+    if (views > kMaxChunkViews) return cudaErrorInvalidValue;
+    if (count == 0 || views == 0) return cudaSuccess;
+    const uint32_t blocks = (count + kThreads - 1) / kThreads;
+    splat_backward_views_kernel<<<blocks, kThreads, 0, stream>>>(
+        framesDev, views, count, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans,
+        gLogScales, gQuats, gLogits, gSh, accumulate ? 1u : 0u);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,
                                   const uint32_t* offsets, const float* partials, uint32_t partialPairs,
                                   float* gMeans, float* gLogScales, float* gQuats, float* gLogits, float* gSh,
-                                  cudaStream_t stream, bool accumulate) {
+                                  cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t blocks = (f.count + kThreads - 1) / kThreads;
-    if (accumulate)
-        splat_backward_kernel<true><<<blocks, kThreads, 0, stream>>>(
-            f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales,
-            gQuats, gLogits, gSh);
-    else
-        splat_backward_kernel<false><<<blocks, kThreads, 0, stream>>>(
-            f, means, logScales, quats, logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales,
-            gQuats, gLogits, gSh);
+    splat_backward_kernel<<<blocks, kThreads, 0, stream>>>(f, means, logScales, quats, logits, sh, touched, offsets,
+                                                           partials, partialPairs, gMeans, gLogScales, gQuats, gLogits,
+                                                           gSh);
     return cudaGetLastError();
 }
 

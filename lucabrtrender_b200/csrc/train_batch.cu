@@ -10,9 +10,9 @@
 //   value -> ranges -> one persistent training blend over (view, tile) items
 //   -> per view the L1 loss and its gradient -> one backward-blend launch
 //   over the chunk's (view, tile) items, writing per-pair partials at their
-//   emit indices -> one per-splat backward per view, the first view of the
-//   batch writing the gradients and every later one adding to them, in view
-//   order.
+//   emit indices -> one per-splat backward over the chunk's views: each
+//   splat's gradients summed view after view (from zero in the batch's first
+//   chunk, from the buffers' values in later ones) and written once.
 // Each view's pixels, and each view's gradient contribution, are the same
 // bits as a single-view training step of that view: within a tile the pairs
 // keep the single view's order, and a splat's pairs are contiguous at their
@@ -108,6 +108,7 @@ extern "C" int lrt_rast_train_batch(lrt_rast* r, const lrt_train_params* params,
     LRT_CUDA(r, ensure(r->trainBatchGrad, maxPixels * 16), "colour gradients");
     LRT_CUDA(r, ensure(r->trainBatchViews, size_t{perChunk} * sizeof(lrt::ViewParams) + 16), "view parameters");
     LRT_CUDA(r, ensure(r->trainBatchLoss, size_t{perChunk} * 4 + 16), "losses");
+    LRT_CUDA(r, ensure(r->trainBatchFrames, size_t{perChunk} * sizeof(FrameParams)), "frame parameters");
     LRT_CUDA(r, ensure(r->lossScratch, lrt::l1_scratch_bytes()), "loss scratch");
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     LRT_CUDA(r, ensure(r->ranges, size_t{maxTiles} * 8), "tile ranges");
@@ -176,10 +177,17 @@ extern "C" int lrt_rast_train_batch(lrt_rast* r, const lrt_train_params* params,
         const uint32_t keyBits = 24 + bits_for(chunkTiles);
         const uint32_t lastPartition = count * lrt::project_partitions(n) - 1;
         std::vector<lrt::ViewParams> hostViews(count);
-        for (uint32_t k = 0; k < count; ++k) hostViews[k] = cv[k].v;
+        std::vector<FrameParams> hostFrames(count);
+        for (uint32_t k = 0; k < count; ++k) {
+            hostViews[k] = cv[k].v;
+            hostFrames[k] = cv[k].f;
+        }
         LRT_CUDA(r, cudaMemcpyAsync(devViews, hostViews.data(), count * sizeof(lrt::ViewParams), cudaMemcpyHostToDevice,
                                     stream),
                  "view parameters");
+        LRT_CUDA(r, cudaMemcpyAsync(r->trainBatchFrames.ptr, hostFrames.data(), count * sizeof(FrameParams),
+                                    cudaMemcpyHostToDevice, stream),
+                 "frame parameters");
 
         // --- forward: project, sort, ranges, blend (drawn again if the pairs outgrew their buffer) ---
         const uint64_t* sorted = nullptr;
@@ -253,25 +261,25 @@ extern "C" int lrt_rast_train_batch(lrt_rast* r, const lrt_train_params* params,
                      "loss gradient");
         }
 
-        // --- backward: per-pair partials over the chunk's tiles, then per splat, view by view ---
+        // --- backward: per-pair partials over the chunk's tiles, then per splat over the chunk's views ---
         LRT_CUDA(r, ensure(r->partials, size_t{std::max(pairs, 1u)} * 48), "pair partials");
         LRT_CUDA(r,
                  lrt::launch_blend_backward_batch(bp, devViews, count, static_cast<uint2*>(r->ranges.ptr), sorted, emit,
                                                   static_cast<ProjRecord*>(r->proj.ptr), chunkTiles,
                                                   static_cast<float*>(r->partials.ptr), stream),
                  "blend backward");
-        for (uint32_t k = 0; k < count; ++k) {
-            LRT_CUDA(r,
-                     lrt::launch_splat_backward(cv[k].f, means, logScales, quats, logits, sh,
-                                                static_cast<uint32_t*>(r->touched.ptr) + size_t{k} * n,
-                                                static_cast<uint32_t*>(r->trainOffsets.ptr) + size_t{k} * n,
-                                                static_cast<float*>(r->partials.ptr), pairs,
-                                                static_cast<float*>(grads->means), static_cast<float*>(grads->log_scales),
-                                                static_cast<float*>(grads->quats),
-                                                static_cast<float*>(grads->opacity_logits),
-                                                static_cast<float*>(grads->sh), stream, c0 + k > 0),
-                     "projection backward");
-        }
+        LRT_CUDA(r,
+                 lrt::launch_splat_backward_views(static_cast<const FrameParams*>(r->trainBatchFrames.ptr), count, n,
+                                                  means, logScales, quats, logits, sh,
+                                                  static_cast<uint32_t*>(r->touched.ptr),
+                                                  static_cast<uint32_t*>(r->trainOffsets.ptr),
+                                                  static_cast<float*>(r->partials.ptr), pairs,
+                                                  static_cast<float*>(grads->means),
+                                                  static_cast<float*>(grads->log_scales),
+                                                  static_cast<float*>(grads->quats),
+                                                  static_cast<float*>(grads->opacity_logits),
+                                                  static_cast<float*>(grads->sh), c0 > 0, stream),
+                 "projection backward");
     }
     LRT_CUDA(r, cudaEventRecord(r->ev[7], stream), "event");
     LRT_CUDA(r, cudaEventRecord(r->frameDone, stream), "event");
