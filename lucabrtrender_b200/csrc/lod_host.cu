@@ -26,12 +26,15 @@ struct lrt_lod {
     uint32_t coarsest = 0, finest = 0, levels = 0, merged = 0, chunkSplats = 0;
     float boundsLo[3] = {0, 0, 0}, boundsHi[3] = {0, 0, 0}, extent = 0.0f;
     uint32_t levelBase[kLodLevels + 2] = {};           // first merged Gaussian of each stored level; [levels] = merged
-    DeviceBuffer positions, shape, sh, codes, starts;   // the store, Morton order
-    DeviceBuffer mPositions, mShape, mSh, cells;        // merged Gaussians, coarsest level first
+    // The store (Morton order) and the merged Gaussians (coarsest level
+    // first) with their cells and the finest groups' starts, each set carved
+    // from one allocation (storeArena, levelArena); codes is the build's own.
+    DeviceBuffer positions, shape, sh, codes, starts;
+    DeviceBuffer mPositions, mShape, mSh, cells;
+    DeviceBuffer storeArena, levelArena;
     ~lrt_lod() {
         DeviceScope scope(device);
-        for (DeviceBuffer* b : {&positions, &shape, &sh, &codes, &starts, &mPositions, &mShape, &mSh, &cells})
-            release(*b);
+        for (DeviceBuffer* b : {&codes, &storeArena, &levelArena}) release(*b);
     }
 };
 
@@ -53,19 +56,23 @@ void release_cut_frames(lrt_rast* r) {
 
 namespace {
 
-// The build's temporaries, freed on every return.
-struct BuildScratch {
-    int device = 0;
-    DeviceBuffer globals, partial, keys, keysAlt, order, orderAlt, sortScratch, status, firstChild, moments, err;
-    ~BuildScratch() {
-        DeviceScope scope(device);
-        for (DeviceBuffer* b : {&globals, &partial, &keys, &keysAlt, &order, &orderAlt, &sortScratch, &status,
-                                &firstChild, &moments, &err})
-            release(*b);
-    }
-};
-
 uint32_t sh_words_for(uint32_t rest) { return (rest * 3 + 1) / 2; }
+
+// One allocation for several buffers, each starting on a 256-byte boundary;
+// the parts point into `arena` and are not freed on their own.
+cudaError_t carve(DeviceBuffer& arena, std::initializer_list<std::pair<DeviceBuffer*, size_t>> parts) {
+    size_t total = 0;
+    for (const auto& p : parts) total += (std::max<size_t>(p.second, 16) + 255) & ~size_t{255};
+    const cudaError_t e = ensure(arena, total);
+    if (e != cudaSuccess) return e;
+    size_t at = 0;
+    for (const auto& p : parts) {
+        p.first->ptr = static_cast<char*>(arena.ptr) + at;
+        p.first->bytes = std::max<size_t>(p.second, 16);
+        at += (p.first->bytes + 255) & ~size_t{255};
+    }
+    return cudaSuccess;
+}
 
 LodSplatArrays arrays_of(DeviceBuffer& positions, DeviceBuffer& shape, DeviceBuffer& sh) {
     return {static_cast<float4*>(positions.ptr), static_cast<uint4*>(shape.ptr), static_cast<uint32_t*>(sh.ptr)};
@@ -190,16 +197,16 @@ int lrt_lod_build(lrt_rast* r, const lrt_gpu_splats* cloud, const float* bounds,
     lod->shWords = shWords;
     lod->coarsest = coarsest;
     lod->chunkSplats = std::max<uint32_t>(settings.chunk_splats, 1u);
-    BuildScratch t;
-    t.device = r->device;
+    LodBuildScratch& t = r->lodBuild;   // kept between builds: a build allocates only what it returns
     LRT_CUDA(r, ensure(t.globals, sizeof(LodGlobals)), "lod buffers");
     LRT_CUDA(r, ensure(t.partial, std::max<size_t>(lrt::lod_bounds_partial_bytes(), 64)), "lod buffers");
     for (DeviceBuffer* b : {&t.keys, &t.keysAlt, &t.order, &t.orderAlt}) LRT_CUDA(r, ensure(*b, size_t{n} * 4), "lod buffers");
     LRT_CUDA(r, ensure(t.sortScratch, lrt::sort_scratch_bytes(n, 30)), "lod buffers");
     LRT_CUDA(r, ensure(t.err, 16), "lod buffers");
-    LRT_CUDA(r, ensure(lod->positions, size_t{n} * 16), "lod buffers");
-    LRT_CUDA(r, ensure(lod->shape, size_t{n} * 16), "lod buffers");
-    LRT_CUDA(r, ensure(lod->sh, size_t{n} * shWords * 4), "lod buffers");
+    LRT_CUDA(r,
+             carve(lod->storeArena,
+                   {{&lod->positions, size_t{n} * 16}, {&lod->shape, size_t{n} * 16}, {&lod->sh, size_t{n} * shWords * 4}}),
+             "lod buffers");
 
     LodGlobals* globals = static_cast<LodGlobals*>(t.globals.ptr);
     uint32_t* err = static_cast<uint32_t*>(t.err.ptr);
@@ -264,11 +271,11 @@ int lrt_lod_build(lrt_rast* r, const lrt_gpu_splats* cloud, const float* bounds,
     lod->extent = host.extent;
     const uint32_t stride = kLodMomentsHead + 3 * rest;
     const uint32_t finestGroups = groups[finest];
-    LRT_CUDA(r, ensure(lod->mPositions, size_t{merged} * 16), "lod levels");
-    LRT_CUDA(r, ensure(lod->mShape, size_t{merged} * 16), "lod levels");
-    LRT_CUDA(r, ensure(lod->mSh, size_t{merged} * shWords * 4), "lod levels");
-    LRT_CUDA(r, ensure(lod->cells, size_t{merged} * 4), "lod levels");
-    LRT_CUDA(r, ensure(lod->starts, size_t{finestGroups} * 4), "lod levels");
+    LRT_CUDA(r,
+             carve(lod->levelArena, {{&lod->mPositions, size_t{merged} * 16}, {&lod->mShape, size_t{merged} * 16},
+                                     {&lod->mSh, size_t{merged} * shWords * 4}, {&lod->cells, size_t{merged} * 4},
+                                     {&lod->starts, size_t{finestGroups} * 4}}),
+             "lod levels");
     LRT_CUDA(r, ensure(t.firstChild, size_t{merged} * 4), "lod levels");
     LRT_CUDA(r, ensure(t.moments, size_t{merged} * stride * 4), "lod levels");
     // One status region per compaction: the finest level's over the splats,

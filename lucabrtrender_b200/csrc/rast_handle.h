@@ -19,6 +19,13 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
+// A level-of-detail build's temporaries (lod_host.cu): the bounds and
+// counters, the Morton sort's keys, indices and scratch, the look-back
+// status words, each group's first child and moments, the error word.
+struct LodBuildScratch {
+    DeviceBuffer globals, partial, keys, keysAlt, order, orderAlt, sortScratch, status, firstChild, moments, err;
+};
+
 struct lrt_rast {
     int device = 0;
     std::string error;
@@ -86,8 +93,10 @@ struct lrt_rast {
         std::vector<std::pair<uint64_t, std::pair<uint32_t, uint32_t>>> tuned;   // shape -> (views per chunk, blocks/SM)
     } batch;
     // Levels of detail: the clouds the last lrt_lod_select made, one per
-    // instance, rewritten by the next call (lod_host.cu).
+    // instance, rewritten by the next call, and the builds' temporaries, kept
+    // from one build to the next (lod_host.cu).
     std::vector<LodCutFrame*> cutFrames;
+    LodBuildScratch lodBuild;
 };
 
 // lod_host.cu: frees the cut clouds (called by lrt_rast_destroy).

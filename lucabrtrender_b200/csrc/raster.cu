@@ -62,7 +62,10 @@ void lrt_rast_destroy(lrt_rast* r) {
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
                             &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
-                            &r->trainBatchViews, &r->trainBatchLoss, &r->trainBatchFrames})
+                            &r->trainBatchViews, &r->trainBatchLoss, &r->trainBatchFrames, &r->lodBuild.globals,
+                            &r->lodBuild.partial, &r->lodBuild.keys, &r->lodBuild.keysAlt, &r->lodBuild.order,
+                            &r->lodBuild.orderAlt, &r->lodBuild.sortScratch, &r->lodBuild.status,
+                            &r->lodBuild.firstChild, &r->lodBuild.moments, &r->lodBuild.err})
         release(*b);
     if (r->ringTail < r->ringHead) cudaDeviceSynchronize();   // enqueued frames still write the ring
     if (r->hostCounters != nullptr) cudaFreeHost(r->hostCounters);
