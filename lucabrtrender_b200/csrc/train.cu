@@ -16,6 +16,7 @@ namespace {
 
 constexpr uint32_t kThreads = 128;
 constexpr uint32_t kMaxChunkViews = 16;   // views one splat_backward_views launch takes
+constexpr uint32_t kGradStrideFloats = 12;  // floats per pair in the partials buffer
 constexpr float kC1 = 0.4886025119029199f;
 __device__ constexpr float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
                           0.5462742152960396f};
@@ -286,15 +287,14 @@ __device__ __forceinline__ void view_grads(const FrameParams& f, uint32_t i, con
     for (int k = 0; k < 3; ++k) gm[k] += W[0][k] * gt[0] + W[1][k] * gt[1] + W[2][k] * gt[2];
 }
 
-// The partials of the splat at `slot` in a frame (touched[slot] pairs from
-// pair offsets[slot] of `partials`), summed into g; every lane of the warp
-// takes part. nOut comes back 0 for a dead lane or a pair range outside the
-// buffer.
-__device__ __forceinline__ void splat_partials(bool live, uint32_t slot, uint32_t lane, const uint32_t* __restrict__ touched,
-                                               const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
-                                               uint32_t partialPairs, float (&g)[9], uint32_t& nOut) {
-    uint32_t n = live ? touched[slot] : 0u;
-    const uint32_t firstRaw = live ? offsets[slot] : 0u;   // loaded beside the count, not after it
+// The partials of one splat in a frame (its touched count `count` of pairs
+// from pair `firstRaw` of `partials`; both 0 for a dead lane), summed into g;
+// every lane of the warp takes part. nOut comes back 0 for a dead lane or a
+// pair range outside the buffer.
+__device__ __forceinline__ void splat_partials(uint32_t count, uint32_t firstRaw, uint32_t lane,
+                                               const float* __restrict__ partials, uint32_t partialPairs,
+                                               float (&g)[9], uint32_t& nOut) {
+    uint32_t n = count;
     const uint32_t first = n != 0 ? firstRaw : 0u;
     // Reads stay inside the partials buffer even for a frame whose pairs
     // overflowed their buffer (the host reports that frame as an error).
@@ -356,7 +356,9 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
     }
     float g[9];
     uint32_t n = 0;
-    splat_partials(live, slot, lane, touched, offsets, partials, partialPairs, g, n);
+    const uint32_t count = live ? touched[slot] : 0u;
+    const uint32_t firstRaw = live ? offsets[slot] : 0u;   // loaded beside the count, not after it
+    splat_partials(count, firstRaw, lane, partials, partialPairs, g, n);
     if (!live) return;
     float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
     float* gshRow = gSh + static_cast<size_t>(i) * 48;
@@ -431,12 +433,27 @@ splat_backward_views_kernel(const FrameParams* __restrict__ frames, uint32_t vie
         for (int q = 0; q < 48; ++q) sAcc[q][tid] = 0.0f;
     }
     __syncthreads();
+    // The next view's count and first pair are loaded, and its first partials
+    // asked into L2, while this view's gradients are computed.
+    uint32_t nextCount = live ? touched[sF[0].base + i] : 0u;
+    uint32_t nextFirst = live ? offsets[sF[0].base + i] : 0u;
     for (uint32_t v = 0; v < views; ++v) {
         const FrameParams& f = sF[v];
+        const uint32_t thisCount = nextCount, thisFirst = nextFirst;
+        if (v + 1 < views && live) {
+            const size_t at = static_cast<size_t>(v + 1) * count + sF[v + 1].base + i;
+            nextCount = touched[at];
+            nextFirst = offsets[at];
+        }
         float g[9];
         uint32_t n = 0;
-        splat_partials(live, f.base + i, lane, touched + static_cast<size_t>(v) * count,
-                       offsets + static_cast<size_t>(v) * count, partials, partialPairs, g, n);
+        splat_partials(thisCount, thisFirst, lane, partials, partialPairs, g, n);
+        if (v + 1 < views && nextCount != 0 && nextFirst < partialPairs) {
+            const size_t at = static_cast<size_t>(nextFirst) * kGradStrideFloats;
+            prefetch_l2(partials + at);
+            if (nextCount > 1 && at + 32 < static_cast<size_t>(partialPairs) * kGradStrideFloats)
+                prefetch_l2(partials + at + 32);
+        }
         if (!live || n == 0) continue;
         float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
         view_grads(f, i, means, logScales, quats, logits, sh, g, gm, gls, gq, glog,
