@@ -128,19 +128,31 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     // items in order. Each item's group leader adds the group's size to the
     // warp's digit counter with a shared-memory atomic and passes the old
     // count to its peers. A warp's atomics on one address take effect in
-    // issue order, so the items need no barrier between them and their
-    // latencies overlap.
+    // issue order, so the items need no barrier between them: in groups of
+    // kRankGroup items, every item's peer mask is found first, then every
+    // leader's atomic is issued (their latencies overlap), then the old
+    // counts are passed on.
     uint32_t rank[kSortItems];
     const uint32_t lowerLanes = (1u << lane) - 1u;
+    constexpr uint32_t kRankGroup = 4;
 #pragma unroll
-    for (uint32_t j = 0; j < kSortItems; ++j) {
-        const uint32_t d = dig[j];
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers));
-        uint32_t prior = 0;
-        if (lane == leader && d < kDigits) prior = atomicAdd(&sWarpHist[warp][d], static_cast<uint32_t>(__popc(peers)));
-        rank[j] = __shfl_sync(0xFFFFFFFFu, prior, static_cast<int>(leader)) +
-                  static_cast<uint32_t>(__popc(peers & lowerLanes));
+    for (uint32_t j0 = 0; j0 < kSortItems; j0 += kRankGroup) {
+        uint32_t peers[kRankGroup];
+#pragma unroll
+        for (uint32_t q = 0; q < kRankGroup; ++q) peers[q] = __match_any_sync(0xFFFFFFFFu, dig[j0 + q]);
+#pragma unroll
+        for (uint32_t q = 0; q < kRankGroup; ++q) {
+            const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers[q]));
+            rank[j0 + q] = 0;
+            if (lane == leader && dig[j0 + q] < kDigits)
+                rank[j0 + q] = atomicAdd(&sWarpHist[warp][dig[j0 + q]], static_cast<uint32_t>(__popc(peers[q])));
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < kRankGroup; ++q) {
+            const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers[q]));
+            rank[j0 + q] = __shfl_sync(0xFFFFFFFFu, rank[j0 + q], static_cast<int>(leader)) +
+                           static_cast<uint32_t>(__popc(peers[q] & lowerLanes));
+        }
     }
     __syncthreads();
 
