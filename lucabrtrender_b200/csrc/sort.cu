@@ -7,7 +7,7 @@
 //
 // Here a sort is one histogram kernel that reads the keys once and counts
 // every pass's digits, then one kernel per 8-bit digit that:
-//   1. takes the next 4096-key partition by atomic ticket (launch order),
+//   1. takes the next 3072-key partition by atomic ticket (launch order),
 //   2. ranks its keys stably inside each warp with __match_any_sync (keys are
 //      warp-striped, so a warp's item j covers 32 consecutive keys and items
 //      are visited in order), and across warps with per-warp digit counts,
@@ -27,7 +27,7 @@ namespace {
 
 constexpr uint32_t kSortThreads = 256;
 constexpr uint32_t kSortWarps = kSortThreads / 32;
-constexpr uint32_t kSortItems = 16;
+constexpr uint32_t kSortItems = 12;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 constexpr uint32_t kDigits = 256;
 constexpr uint32_t kFlagAggregate = 1u << 30;
@@ -36,6 +36,7 @@ constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr uint32_t kMaxPasses = 8;
 constexpr uint32_t kHistThreads = 512;
+constexpr uint32_t kLookWords = 4;   // earlier partitions' status words a look-back step reads
 
 // 256-wide exclusive scan across the block (one value per thread).
 __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* sWarp) {
@@ -110,7 +111,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     const uint32_t base = part * kSortTile;
     if (base >= n) return;
 
-    // Warp-striped load: item j of lane l is key base + 512 warp + 32 j + l.
+    // Warp-striped load: item j of lane l is key base + 384 warp + 32 j + l.
     K key[kSortItems];
     uint32_t val[kSortItems];
     uint32_t dig[kSortItems];
@@ -174,24 +175,42 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     const uint32_t globalStart = block_exclusive_scan_256(hist[tid], sScan);
     sBlockStart[tid] = blockStart;
 
+    // The look-back reads kLookWords earlier partitions' words at once (their
+    // loads in flight together) and sums them in order up to the first one
+    // not yet published or the first inclusive one.
     uint32_t prefix = 0;
     if (part > 0) {
         int64_t p = static_cast<int64_t>(part) - 1;
         uint32_t spins = 0;
         while (p >= 0) {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> s(lookback[static_cast<size_t>(p) * kDigits + tid]);
-            const uint32_t word = s.load(cuda::memory_order_relaxed);
-            if ((word & ~kValueMask) == 0) {
+            uint32_t words[kLookWords];
+#pragma unroll
+            for (uint32_t q = 0; q < kLookWords; ++q) {
+                words[q] = kFlagInclusive;   // before partition 0: an inclusive zero
+                if (p - static_cast<int64_t>(q) >= 0) {
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> s(
+                        lookback[static_cast<size_t>(p - static_cast<int64_t>(q)) * kDigits + tid]);
+                    words[q] = s.load(cuda::memory_order_relaxed);
+                }
+            }
+            uint32_t used = 0;
+            bool inclusive = false;
+#pragma unroll
+            for (uint32_t q = 0; q < kLookWords; ++q) {
+                if (inclusive || used < q || (words[q] & ~kValueMask) == 0) continue;
+                prefix += words[q] & kValueMask;
+                used = q + 1;
+                inclusive = (words[q] & kFlagInclusive) != 0;
+            }
+            if (inclusive) break;
+            p -= used;
+            if (used == 0) {
                 if (++spins > kSpinLimit) {
                     atomicOr(err, kErrTimeout);
                     break;
                 }
                 __nanosleep(20);
-                continue;
             }
-            prefix += word & kValueMask;
-            if (word & kFlagInclusive) break;
-            --p;
         }
         mine.store(kFlagInclusive | (prefix + count), cuda::memory_order_relaxed);
     }
