@@ -380,11 +380,13 @@ typedef struct lrt_train_view {
  * the backward of that loss; `grads` receives the gradients of the sum of the
  * views' losses (written, not added to), accumulated view by view in the
  * given order, so they are the sum of the single-view gradients taken in that
- * order, bit for bit. Views go in chunks: each chunk is projected view by
- * view into one pair buffer (the views' tiles numbered one after another),
- * sorted once, blended by one persistent launch over (view, tile) items,
- * and taken back through one backward-blend launch over those items and one
- * per-splat backward per view. The settings' width and height are replaced
+ * order, bit for bit (up to the sign of a zero). Views go in chunks: each
+ * chunk is projected view by view into one pair buffer (the views' tiles
+ * numbered one after another), sorted once, blended by one persistent launch
+ * over (view, tile) items, and taken back through one backward-blend launch
+ * over those items and one per-splat backward over the chunk's views (each
+ * splat's view gradients summed in order, its gradient buffers written once
+ * a chunk). The settings' width and height are replaced
  * by each view's. Returns when the step is done; OVERFLOW cannot happen (a
  * chunk whose pairs outgrow their buffer is drawn again with more room). */
 int lrt_rast_train_batch(lrt_rast* rast, const lrt_train_params* params, const lrt_train_view* views,
