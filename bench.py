@@ -56,14 +56,13 @@ def orbit_camera(L, k: int):
     return L.square_pixel_camera(eye, (0.0, 0.0, 0.0), WIDTH, HEIGHT, 60.0, 0.01)
 
 
-def workload_config(extra: dict | None = None) -> dict:
-    cfg = {"workload": "plain forward, 1M splats, 1920x1080, 20-frame orbit at radius 4",
-           "splats": SPLATS, "width": WIDTH, "height": HEIGHT, "frames": FRAMES, "tile": 16, "sh_degree": 3,
-           "seed": SEED, "l2": "flushed before every device-timed step (256 MB write); the end-to-end steps run "
-                               "back to back with a 283 MB working set per frame, larger than L2"}
-    if extra:
-        cfg.update(extra)
-    return cfg
+def workload_config(world: int) -> dict:
+    """The workload, the same in both arms."""
+    return {"workload": "plain forward, 1M splats, 1920x1080, 20-frame orbit at radius 4",
+            "splats": SPLATS, "width": WIDTH, "height": HEIGHT, "frames": FRAMES, "tile": 16, "sh_degree": 3,
+            "seed": SEED, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "flushed before every device-timed step (256 MB write); the end-to-end steps run back to back "
+                  "with a 283 MB working set per frame, larger than L2"}
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -131,21 +130,14 @@ class Clocks:
                 "samples": len(sm), "samples_whole_run": len(rows)}
 
 
-def cpu_reference_frames(k_frames: int, threads: int, packed, log=print) -> tuple[float, list]:
-    """The oracle (CPU restatement) rendering full frames of the orbit."""
+def cpu_reference_frames(frame_ids, threads: int) -> tuple[float, list]:
+    """The oracle (CPU restatement of the reference's kernels) rendering full
+    frames of the orbit. The scene and the cameras are built by the oracle
+    too (oracle/bench_workload.py): this leg imports nothing from the package."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as ora
-    import lucabrtrender_b200 as L
-    from lucabrtrender_b200 import _abi  # noqa: F401
-
-    cloud = ora.HostCloud(packed.positions, packed.shape, packed.sh, packed.rest_per_colour)
-    st = L.RenderSettings(width=WIDTH, height=HEIGHT).struct()
-    times = []
-    for k in range(k_frames):
-        pr = L.projection_for(orbit_camera(L, k), WIDTH, HEIGHT).struct()
-        t = time.perf_counter()
-        ora.render(pr, [(cloud, np.eye(4), None)], st, threads, want_pairs=False)
-        times.append((time.perf_counter() - t) * 1e3)
+    import bench_workload as W
+    cloud = W.packed_cloud(SPLATS, SEED)
+    times = W.time_frames(cloud, frame_ids, FRAMES, RADIUS, WIDTH, HEIGHT, threads)
     return float(np.mean(times)), times
 
 
@@ -153,19 +145,18 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import lucabrtrender_b200 as L
     threads = os.cpu_count() or 1
-    packed = L.pack_splats(L.synthetic_records(SPLATS, SEED), 15, 3)
-    cpu_reference_frames(args.warmup, threads, packed)
-    mean_ms, _ = cpu_reference_frames(args.steps, threads, packed)
+    cpu_reference_frames(range(args.warmup), threads)
+    mean_ms, _ = cpu_reference_frames(range(args.steps), threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(mean_ms, 3), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config({"reference_arm": "oracle: C++ restatement of the reference's Slang raster "
-                                                    "kernels (the Slang itself cannot run here), CPU"}),
+        "config": workload_config(args.gpus),
+        "reference_arm": "the oracle: a C++ restatement of the reference's Slang raster kernels (the Slang itself "
+                         "cannot run here), on the host cores; scene and cameras built by the oracle",
         "cpu_baseline": {"value": round(mean_ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full frames of the orbit, {threads} threads"},
+                         "sample": f"frames 0-{args.steps - 1} of the orbit, {threads} threads"},
         "e2e": {"value": round(mean_ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -643,17 +634,20 @@ def run_ours(args) -> None:
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
+            # A bounded sample (about 25 s of CPU work on 16 host threads):
+            # the first frames of the same orbit; the --impl reference arm
+            # times every frame the GPU arm times.
             threads = os.cpu_count() or 1
-            ms, times = cpu_reference_frames(args.cpu_frames, threads, packed)
+            ms, times = cpu_reference_frames(range(args.cpu_frames), threads)
             cpu = {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{args.cpu_frames} full frames of the same orbit on the oracle (C++ restatement "
+                   "sample": f"frames 0-{args.cpu_frames - 1} of the same orbit on the oracle (C++ restatement "
                              f"of the reference's kernels), {threads} threads"}
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                       "pairs_per_frame": int(pairs), "visible_per_frame": int(visible)}),
+            "config": workload_config(world),
+            "frame": {"pairs": int(pairs), "visible": int(visible), "tiles": tiles, "pixels": pixels},
             "stages_ms": {k: round(v, 4) for k, v in stage.items()},
             "sort_gbs": round(sort_gbs, 1) if sort_gbs else None,
             "roofline": {"kernel": dom_name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
@@ -684,7 +678,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-frames", type=int, default=2)
+    ap.add_argument("--cpu-frames", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-backward", action="store_true")
     ap.add_argument("--no-batch", action="store_true")

@@ -406,6 +406,16 @@ int lrt_prefix_sum(lrt_rast* rast, const void* in, void* out, void* total, uint3
 int lrt_radix_sort(lrt_rast* rast, void* keys, void* values, uint32_t count, uint32_t key_bits,
                    uint32_t key_bytes, void* stream);
 
+/* Test hook for the bounded waits (no counterpart in the reference, whose
+ * sort never waits on another workgroup). While set on a handle, its
+ * lrt_radix_sort runs the last digit pass with partition 0 never taken, so
+ * the partition after it waits for counts nobody publishes. That wait gives
+ * up after `poll_limit` polls (0: the normal limit, 2^22), the call returns
+ * LRT_TIMEOUT, and the keys are left in an undefined order (every write stays
+ * inside the buffers). Clearing it (0, 0) restores normal sorts; the handle
+ * stays usable throughout. */
+int lrt_rast_debug_sort_fault(lrt_rast* rast, uint32_t skip_first_partition, uint32_t poll_limit);
+
 /* The prefix sum above for callers that cannot allocate device memory: a
  * plugin running inside a host application that owns every device allocation
  * (and its budget), or a frame-critical path where cudaMalloc would

@@ -149,8 +149,10 @@ __device__ __forceinline__ float4 cull_box(const ProjRecord& rec) {
 // the pixel. Pairs are in depth-key order, not exactly depth order, so that
 // first pair is found from a running maximum of the batch's depths (the first
 // index where it reaches the layer's depth), not from depth order.
+// Returns true when a bounded wait gave up (kErrTimeout is set): the
+// barriers' phases are then unknown, so a persistent caller must stop.
 template <bool kTrain, bool kComposite = false>
-__device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
+__device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
                                            const uint2* __restrict__ ranges,
                                            const unsigned long long* __restrict__ pairs,
                                            const uint32_t* __restrict__ emitSlot,
@@ -207,6 +209,7 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
     float depthSum = 0.0f;
     float depthAt = -1.0f;
     bool done = !inside;
+    bool gaveUp = false;
     uint32_t last = start;
     if (start < end) issue(0, start);
     uint32_t k = 0;
@@ -218,6 +221,7 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         if (!mbar_wait(&sBar[buf], parity)) {
             atomicOr(err, kErrTimeout);
             done = true;
+            gaveUp = true;
         }
         if (buf == 0) phase0 ^= 1u; else phase1 ^= 1u;
         const uint32_t cnt = min(kBatch, end - at);
@@ -322,13 +326,16 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
                 // Drain the batch already in flight, and count its phase: a
                 // persistent block blends its next tile with the same barriers.
                 const uint32_t nb = buf ^ 1u;
-                if (!mbar_wait(&sBar[nb], nb == 0 ? phase0 : phase1)) atomicOr(err, kErrTimeout);
+                if (!mbar_wait(&sBar[nb], nb == 0 ? phase0 : phase1)) {
+                    atomicOr(err, kErrTimeout);
+                    gaveUp = true;
+                }
                 if (nb == 0) phase0 ^= 1u; else phase1 ^= 1u;
             }
             break;
         }
     }
-    if (!inside) return;
+    if (!inside) return gaveUp;
     if constexpr (kComposite) {
         if (!opaqueHit && underHit) {
             opaqueHit = true;
@@ -356,6 +363,7 @@ __device__ __forceinline__ void blend_tile(const BlendParams& bp, uint32_t tile,
         pixState[pix] = make_float4(r, g, b, T);
         pixLast[pix] = last;
     }
+    return gaveUp;
 }
 
 
@@ -442,9 +450,13 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
         vbp.height = v.height;
         vbp.tilesX = v.tilesX;
         const uint32_t local = item - v.tileBase;
-        blend_tile<kTrain>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr, proj + v.recordBase,
-                           v.colour, v.depth, kTrain ? v.pixState : nullptr, kTrain ? v.pixLast : nullptr, err, sRec,
-                           sBox, sBar, phase0, phase1);
+        const bool gaveUp = blend_tile<kTrain>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr,
+                                               proj + v.recordBase, v.colour, v.depth,
+                                               kTrain ? v.pixState : nullptr, kTrain ? v.pixLast : nullptr, err,
+                                               sRec, sBox, sBar, phase0, phase1);
+        // After a wait gave up the barriers' phases are unknown: take no more
+        // items (the frame reports TIMEOUT and its output is undefined).
+        if (__syncthreads_or(gaveUp ? 1 : 0)) return;
     }
 }
 

@@ -48,13 +48,23 @@ size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
                                   uint32_t* err, cudaStream_t stream);
 
+// A planted look-back fault, for the test of the bounded waits: the last
+// pass's ticket counter starts at 1, so its partition 0 is never taken and
+// never publishes its counts; the partition after it polls at most
+// `pollLimit` times, gives up, sets kErrTimeout and carries on (the sort's
+// output is then undefined, every write still in bounds).
+struct SortFault {
+    uint32_t skipFirstPartition = 0;
+    uint32_t pollLimit = 0;   // 0: the normal limit
+};
+
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
-                            uint32_t* err, bool* resultInAlt, cudaStream_t stream);
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr);
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
-                            uint32_t* err, bool* resultInAlt, cudaStream_t stream);
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr);
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
                           uint2* ranges, uint32_t tiles, cudaStream_t stream);

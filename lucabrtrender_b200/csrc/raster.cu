@@ -985,13 +985,13 @@ int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32
         LRT_CUDA(r,
                  lrt::launch_sort_u64(static_cast<uint64_t*>(keys), static_cast<uint64_t*>(r->algoKeysAlt.ptr), vals,
                                       valsAlt, counters + 4, count, 0, keyBits, r->sortScratch.ptr, err, &inAlt,
-                                      stream),
+                                      stream, &r->sortFault),
                  "radix sort");
     } else {
         LRT_CUDA(r,
                  lrt::launch_sort_u32(static_cast<uint32_t*>(keys), static_cast<uint32_t*>(r->algoKeysAlt.ptr), vals,
                                       valsAlt, counters + 4, count, 0, keyBits, r->sortScratch.ptr, err, &inAlt,
-                                      stream),
+                                      stream, &r->sortFault),
                  "radix sort");
     }
     if (inAlt) {   // an odd pass count ends in the scratch buffers (RadixSort.cpp:146-155 copies back too)
@@ -1004,6 +1004,14 @@ int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32
     LRT_CUDA(r, cudaMemcpyAsync(r->hostCounters + 7, err, 4, cudaMemcpyDeviceToHost, stream), "status readback");
     LRT_CUDA(r, cudaStreamSynchronize(stream), "radix sort");
     if (r->hostCounters[7] & lrt::kErrTimeout) return fail(r, LRT_TIMEOUT, "radix sort look-back gave up");
+    return LRT_OK;
+}
+
+int lrt_rast_debug_sort_fault(lrt_rast* r, uint32_t skip_first_partition, uint32_t poll_limit) {
+    if (r == nullptr) return LRT_INVALID_ARGUMENT;
+    r->error.clear();
+    r->sortFault.skipFirstPartition = skip_first_partition != 0 ? 1u : 0u;
+    r->sortFault.pollLimit = poll_limit;
     return LRT_OK;
 }
 

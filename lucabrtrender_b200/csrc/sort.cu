@@ -30,9 +30,11 @@ constexpr uint32_t kSortWarps = kSortThreads / 32;
 constexpr uint32_t kSortItems = 12;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 constexpr uint32_t kDigits = 256;
-constexpr uint32_t kFlagAggregate = 1u << 30;
-constexpr uint32_t kFlagInclusive = 2u << 30;
-constexpr uint32_t kValueMask = (1u << 30) - 1;
+// Look-back words are 64 bits: a digit's running count (up to 2^32 - 1 keys)
+// in the low 32 bits, the status in bits 32-33.
+constexpr uint64_t kFlagAggregate = 1ull << 32;
+constexpr uint64_t kFlagInclusive = 2ull << 32;
+constexpr uint64_t kValueMask = 0xFFFFFFFFull;
 constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr uint32_t kMaxPasses = 8;
 constexpr uint32_t kHistThreads = 512;
@@ -90,8 +92,8 @@ template <typename K, bool kValues>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
 onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
-                const uint32_t* __restrict__ hist, uint32_t* __restrict__ lookback,
-                uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift) {
+                const uint32_t* __restrict__ hist, unsigned long long* __restrict__ lookback,
+                uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift, uint32_t spinLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
     K* sKeys = reinterpret_cast<K*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * kSortTile);
@@ -165,7 +167,8 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
         sWarpHist[w][tid] = count;
         count += c;
     }
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(lookback[static_cast<size_t>(part) * kDigits + tid]);
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(
+        lookback[static_cast<size_t>(part) * kDigits + tid]);
     if (part == 0) {
         mine.store(kFlagInclusive | count, cuda::memory_order_relaxed);
     } else {
@@ -183,12 +186,12 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
         int64_t p = static_cast<int64_t>(part) - 1;
         uint32_t spins = 0;
         while (p >= 0) {
-            uint32_t words[kLookWords];
+            unsigned long long words[kLookWords];
 #pragma unroll
             for (uint32_t q = 0; q < kLookWords; ++q) {
                 words[q] = kFlagInclusive;   // before partition 0: an inclusive zero
                 if (p - static_cast<int64_t>(q) >= 0) {
-                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> s(
+                    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> s(
                         lookback[static_cast<size_t>(p - static_cast<int64_t>(q)) * kDigits + tid]);
                     words[q] = s.load(cuda::memory_order_relaxed);
                 }
@@ -198,14 +201,14 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 #pragma unroll
             for (uint32_t q = 0; q < kLookWords; ++q) {
                 if (inclusive || used < q || (words[q] & ~kValueMask) == 0) continue;
-                prefix += words[q] & kValueMask;
+                prefix += static_cast<uint32_t>(words[q] & kValueMask);
                 used = q + 1;
                 inclusive = (words[q] & kFlagInclusive) != 0;
             }
             if (inclusive) break;
             p -= used;
             if (used == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spinLimit) {
                     atomicOr(err, kErrTimeout);
                     break;
                 }
@@ -242,7 +245,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 template <typename K, bool kValues>
 cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                       uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
-                      bool* resultInAlt, cudaStream_t stream) {
+                      bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
     *resultInAlt = false;
     if (cap == 0 || bits == 0) return cudaSuccess;
     const uint32_t passes = (bits + 7) / 8;
@@ -250,10 +253,18 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     char* s = static_cast<char*>(scratch);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(s);                     // kMaxPasses
     uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
-    uint32_t* lookback = reinterpret_cast<uint32_t*>(s + 64 + kMaxPasses * kDigits * 4);
+    unsigned long long* lookback = reinterpret_cast<unsigned long long*>(s + 64 + kMaxPasses * kDigits * 4);
     const size_t bytes = sort_scratch_bytes(cap, bits);
     cudaError_t e = cudaMemsetAsync(scratch, 0, bytes, stream);
     if (e != cudaSuccess) return e;
+    const uint32_t spinLimit = fault != nullptr && fault->pollLimit != 0 ? fault->pollLimit : kSpinLimit;
+    if (fault != nullptr && fault->skipFirstPartition != 0) {
+        // The last pass's tickets start at 1. Only the last pass: its input is
+        // whole, so a missing prefix only moves keys to earlier slots, never
+        // past the end; no later pass reads what it leaves undefined.
+        e = cudaMemsetAsync(tickets + (passes - 1), 1, 1, stream);
+        if (e != cudaSuccess) return e;
+    }
     const uint32_t histBlocks = std::max(1u, std::min(parts, 148u * 4u));
     histogram_kernel<K><<<histBlocks, kHistThreads, 0, stream>>>(keys, dCount, cap, firstBit, passes, hist);
     e = cudaGetLastError();
@@ -269,7 +280,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     for (uint32_t p = 0; p < passes; ++p) {
         onesweep_kernel<K, kValues><<<parts, kSortThreads, smem, stream>>>(
             src, dst, vsrc, vdst, dCount, cap, hist + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
-            tickets + p, err, firstBit + 8 * p);
+            tickets + p, err, firstBit + 8 * p, spinLimit);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         std::swap(src, dst);
@@ -284,29 +295,31 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits) {
     const size_t passes = (bits + 7) / 8;
     const size_t parts = (static_cast<size_t>(cap) + kSortTile - 1) / kSortTile;
-    return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * 4;
+    return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * 8;
 }
 
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
-                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream) {
+                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
+                            const SortFault* fault) {
     if (bits > 64 || firstBit + bits > 64 || (bits + 7) / 8 > kMaxPasses) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_impl<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream);
+                                         resultInAlt, stream, fault);
     return sort_impl<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream);
+                                      resultInAlt, stream, fault);
 }
 
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
-                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream) {
+                            void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
+                            const SortFault* fault) {
     if (bits > 32 || firstBit + bits > 32) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_impl<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream);
+                                         resultInAlt, stream, fault);
     return sort_impl<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream);
+                                      resultInAlt, stream, fault);
 }
 
 }  // namespace lrt

@@ -21,8 +21,11 @@ REF_LIB = HERE / "_ref" / "libref_camera.so"
 
 import sys  # noqa: E402
 
-sys.path.insert(0, str(HERE.parent))
-from lucabrtrender_b200 import _abi  # noqa: E402  (struct layouts of the public header)
+# The public header's struct layouts (its ctypes mirror beside it); the
+# oracle shares them with the package but imports nothing from the package.
+if str(HERE.parent / "include") not in sys.path:
+    sys.path.insert(0, str(HERE.parent / "include"))
+import lrt_raster_ctypes as _abi  # noqa: E402
 
 
 class FrameOut(C.Structure):
