@@ -1115,9 +1115,11 @@ int renderImpl(const lrt_projection* pr, uint64_t total, const lrt_render_settin
         depthTmp.resize(size_t{f.width} * f.height);
         depth = depthTmp.data();
     }
+    const uint8_t* blendTiles = out->blend_tiles;
     parallelFor(f.height, threads, [&](uint64_t b, uint64_t e) {
         for (uint64_t py = b; py < e; ++py)
             for (uint32_t px = 0; px < f.width; ++px) {
+                if (blendTiles != nullptr && blendTiles[(py / kTile) * f.tilesX + px / kTile] == 0) continue;
                 std::vector<uint32_t>* list = nullptr;
                 if (crop != nullptr && px >= crop->x0 && px < crop->x0 + crop->w && py >= crop->y0 &&
                     py < crop->y0 + crop->h)

@@ -44,6 +44,9 @@ typedef struct ora_frame_out {
     uint32_t visible;
     uint32_t slots;
     double stage_ms[6];   /* project, depth sort, counts, emit, tile sort+ranges, blend */
+    /* optional: one byte per tile; when set, only tiles with a nonzero byte
+       are blended (the other pixels are left as the caller filled them) */
+    const uint8_t* blend_tiles;
 } ora_frame_out;
 
 uint32_t ora_abi_version(void);

@@ -34,6 +34,7 @@ class FrameOut(C.Structure):
         ("touched", C.c_void_p), ("depth_keys", C.c_void_p), ("pair_tiles", C.c_void_p),
         ("pair_slots", C.c_void_p), ("ranges", C.c_void_p), ("pair_capacity", C.c_uint64),
         ("pairs", C.c_uint64), ("visible", C.c_uint32), ("slots", C.c_uint32), ("stage_ms", C.c_double * 6),
+        ("blend_tiles", C.c_void_p),
     ]
 
 
@@ -249,11 +250,22 @@ def _instances(instances):
     return arr, keep
 
 
+def tile_mask(settings, tiles) -> np.ndarray:
+    """One byte per tile of the frame, set for the given tile ids."""
+    tiles_x = (settings.width + 15) // 16
+    tiles_y = (settings.height + 15) // 16
+    m = np.zeros(tiles_x * tiles_y, np.uint8)
+    m[np.asarray(list(tiles), np.int64)] = 1
+    return m
+
+
 def render(projection: _abi.Projection, instances, settings: _abi.RenderSettingsStruct, threads: int = 0,
-           want_pairs: bool = True, points=(), under=None) -> dict:
+           want_pairs: bool = True, points=(), under=None, blend_tiles=None) -> dict:
     """The restated rasteriser; `points` (HostPoints, matrix, style) are drawn
     as discs after the splats, `under` is an optional (colour [H,W,4], depth
-    [H,W]) layer -- either makes the frame a composite one."""
+    [H,W]) layer -- either makes the frame a composite one. `blend_tiles`
+    (one byte per tile, see tile_mask) blends only the marked tiles; the
+    other pixels stay zero."""
     slots = sum(c.count for c, _, _ in instances) + sum(p.count for p, _, _ in points)
     tiles_x = (settings.width + 15) // 16
     tiles_y = (settings.height + 15) // 16
@@ -272,6 +284,9 @@ def render(projection: _abi.Projection, instances, settings: _abi.RenderSettings
     out.touched, out.depth_keys = touched.ctypes.data, keys.ctypes.data
     out.ranges = ranges.ctypes.data
     out.pair_capacity = cap
+    if blend_tiles is not None:
+        blend_tiles = np.ascontiguousarray(blend_tiles, np.uint8)
+        out.blend_tiles = blend_tiles.ctypes.data
     arr, keep = _instances(instances)
     parr, pkeep = _points(points)
     if under is not None:
@@ -297,6 +312,8 @@ def render(projection: _abi.Projection, instances, settings: _abi.RenderSettings
         ps = np.zeros(pairs, np.uint32)
         out2 = FrameOut()
         out2.pair_tiles, out2.pair_slots, out2.pair_capacity = pt.ctypes.data, ps.ctypes.data, pairs
+        no_blend = np.zeros(ranges.shape[0], np.uint8)   # the image is already drawn
+        out2.blend_tiles = no_blend.ctypes.data
         _check(run(out2), "render")
         result["pair_tiles"] = pt
         result["pair_slots"] = ps
@@ -397,7 +414,10 @@ class RawCloud:
 
 
 def train_render(projection: _abi.Projection, cloud: RawCloud, settings: _abi.RenderSettingsStruct,
-                 crop=(0, 0, 0, 0), threads: int = 0) -> dict:
+                 crop=(0, 0, 0, 0), threads: int = 0, crop_only: bool = False) -> dict:
+    """The restated training forward; with a crop, each crop pixel's
+    contributor list (its slots in blend order). `crop_only` blends only the
+    tiles the crop overlaps (the rest of the image stays zero)."""
     lib = load()
     lib.ora_train_render.argtypes = [C.POINTER(_abi.Projection), C.POINTER(_abi.TrainParams),
                                      C.POINTER(_abi.RenderSettingsStruct), C.POINTER(FrameOut), C.c_uint32,
@@ -420,10 +440,20 @@ def train_render(projection: _abi.Projection, cloud: RawCloud, settings: _abi.Re
     offsets = np.zeros(cw * ch + 1, np.uint32)
     total = C.c_uint64()
     p = cloud.struct()
+    crop_tiles = None
+    if cw > 0 and ch > 0:
+        tx = range(x0 // 16, (x0 + cw - 1) // 16 + 1)
+        ty = range(y0 // 16, (y0 + ch - 1) // 16 + 1)
+        crop_tiles = tile_mask(settings, [y * ((w + 15) // 16) + x for y in ty for x in tx])
+    if crop_only:
+        out.blend_tiles = crop_tiles.ctypes.data if crop_tiles is not None else None
     _check(lib.ora_train_render(C.byref(projection), C.byref(p), C.byref(settings), C.byref(out), threads, x0, y0, cw,
                                 ch, offsets.ctypes.data, None, 0, C.byref(total)), "train_render")
     slots = np.zeros(max(1, total.value), np.uint32)
     out2 = FrameOut()
+    # The second pass only fills the crop's lists: blend the crop's tiles alone.
+    second_mask = crop_tiles if crop_tiles is not None else np.zeros(tiles, np.uint8)
+    out2.blend_tiles = second_mask.ctypes.data
     _check(lib.ora_train_render(C.byref(projection), C.byref(p), C.byref(settings), C.byref(out2), threads, x0, y0,
                                 cw, ch, offsets.ctypes.data, slots.ctypes.data, total.value, C.byref(total)),
            "train_render")
