@@ -107,7 +107,15 @@ typedef struct lrt_splat_edit {
  *              [1] f16 log sx | f16 log sy << 16, [2] f16 log sz | f16 base r << 16,
  *              [3] f16 base g | f16 base b << 16
  *   sh         sh_words uint32 per splat: f16 rest coefficients, rgb per basis
- * All three are device pointers owned by the caller. */
+ * All three are device pointers owned by the caller.
+ *   filter3d   optional (null: off, the reference's behaviour): one float per
+ *              splat, the variance of the Mip-Splatting 3D smoothing filter
+ *              (Yu et al., "Mip-Splatting", CVPR 2024, section 4.1) in the
+ *              cloud's own units, e.g. from lrt_rast_filter3d. When set, the
+ *              projection widens each splat's scales to sqrt(s^2 + v) and
+ *              scales its opacity by sqrt(prod s^2 / prod (s^2 + v)) before
+ *              anything else reads them. No counterpart in the reference,
+ *              which has only the 2D filter. */
 typedef struct lrt_gpu_splats {
     uint32_t count;
     uint32_t rest_per_colour;   /* 0, 3, 8, 15 -> degree 0..3 */
@@ -116,6 +124,7 @@ typedef struct lrt_gpu_splats {
     const void* positions;
     const void* shape;
     const void* sh;
+    const void* filter3d;
 } lrt_gpu_splats;
 
 /* SplatInstance (TileRasterizer.h:52-67) without the relight fields. */
@@ -405,6 +414,20 @@ int lrt_prefix_sum(lrt_rast* rast, const void* in, void* out, void* total, uint3
  * one histogram pass, then one decoupled look-back pass per 8-bit digit. */
 int lrt_radix_sort(lrt_rast* rast, void* keys, void* values, uint32_t count, uint32_t key_bits,
                    uint32_t key_bytes, void* stream);
+
+/* The Mip-Splatting 3D filter's per-splat variance (Yu et al., CVPR 2024,
+ * section 4.1), from a set of cameras: a splat's sampling rate under a
+ * camera is focal_x / z (perspective; focal_x for an orthographic camera)
+ * where its centre lies in front of the near plane and projects within the
+ * image widened by 15% on each side; its variance is coefficient / r^2 with r
+ * the highest such rate (the paper's default coefficient is 0.2). Splats no
+ * camera sees get the largest variance among the seen ones; with none seen,
+ * 0. `cloud` and `variance` are device memory; cameras and sizes (width,
+ * height per camera) are host arrays; positions are taken in the cloud's
+ * own space (cameras given in that space). No counterpart in the reference. */
+int lrt_rast_filter3d(lrt_rast* rast, const lrt_gpu_splats* cloud, const lrt_projection* cameras,
+                      const uint32_t* sizes, uint32_t camera_count, float coefficient, float* variance,
+                      void* stream);
 
 /* Test hook for the bounded waits (no counterpart in the reference, whose
  * sort never waits on another workgroup). While set on a handle, its

@@ -19,7 +19,7 @@ LIB_DIR = PACKAGE / "lib"
 LIBRARY = LIB_DIR / "liblrt_raster.so"
 OBJ_DIR = ROOT / "_build" / "obj"
 
-SOURCES = ["project.cu", "scan.cu", "sort.cu", "blend.cu", "raster.cu", "math_eval.cu", "scan_noalloc.cu", "train.cu", "decode.cu", "compare.cu", "loss.cu", "lod.cu", "lod_host.cu", "train_batch.cu", "host.cpp"]
+SOURCES = ["project.cu", "scan.cu", "sort.cu", "blend.cu", "raster.cu", "math_eval.cu", "scan_noalloc.cu", "train.cu", "decode.cu", "compare.cu", "loss.cu", "lod.cu", "lod_host.cu", "train_batch.cu", "filter3d.cu", "host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-O3",
          "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]

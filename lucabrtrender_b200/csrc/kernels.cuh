@@ -26,7 +26,7 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
                                 ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                 uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
                                 uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
-                                const FrameParams* fDev = nullptr);
+                                const FrameParams* fDev = nullptr, const float* filter3d = nullptr);
 
 // The same for the differentiable parameters (means float3, log-scales
 // float3, quaternions w x y z, opacity logits, SH fp16 [16][3]); also writes

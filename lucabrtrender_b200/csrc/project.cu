@@ -151,6 +151,7 @@ struct PackedSource {
     const float4* positions;
     const uint4* shape;
     const uint32_t* sh;
+    const float* filter3d;   // optional: the 3D filter's variance per splat
     static constexpr bool kDisc = false;
     static constexpr uint32_t kRestOffset = 0;
     struct Loaded {
@@ -162,6 +163,19 @@ struct PackedSource {
         p = make_float3(po.x, po.y, po.z);
         opacity = po.w;
         scale = make_float3(lrt_exp(low_half(l.sw.y)), lrt_exp(high_half(l.sw.y)), lrt_exp(low_half(l.sw.z)));
+        if (filter3d != nullptr) apply_filter3d(__ldg(filter3d + i), scale, opacity);
+    }
+    // The Mip-Splatting 3D filter (Yu et al., CVPR 2024, section 4.1): the
+    // splat convolved with an isotropic Gaussian of variance v keeps its
+    // rotation, takes the scales sqrt(s^2 + v) and pays the spread-out
+    // energy back in opacity, sqrt(prod s^2 / prod (s^2 + v)).
+    __device__ __forceinline__ static void apply_filter3d(float v, float3& s, float& opacity) {
+        const float qx = s.x * s.x, qy = s.y * s.y, qz = s.z * s.z;
+        const float fx = qx + v, fy = qy + v, fz = qz + v;
+        const float before = qx * qy * qz;
+        const float after = fx * fy * fz;
+        opacity = opacity * sqrtf(before / after);
+        s = make_float3(sqrtf(fx), sqrtf(fy), sqrtf(fz));
     }
     // decodeQuaternion, packing.slang:52-69
     __device__ __forceinline__ void rotation(const Loaded& l, float& x, float& y, float& z, float& w) const {
@@ -776,12 +790,13 @@ cudaError_t launch_project_emit(const FrameParams& f, const float4* positions, c
                                 ProjRecord* proj, uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                 uint64_t* status, uint32_t* ticket, uint32_t partitionBase, uint32_t lastPartition,
                                 uint32_t slotBits, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
-                                const FrameParams* fDev) {
+                                const FrameParams* fDev, const float* filter3d) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
-    return launch(f, fDev, PackedSource{positions, shape, sh}, TrainOutputs{nullptr, nullptr, nullptr}, stage, proj, rects,
+    return launch(f, fDev, PackedSource{positions, shape, sh, filter3d}, TrainOutputs{nullptr, nullptr, nullptr}, stage,
+                  proj, rects,
                   touched, keys, counters, status, ticket, partitionBase, lastPartition, slotBits, pairs, capacity,
                   stream);
 }

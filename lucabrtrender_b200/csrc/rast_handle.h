@@ -36,6 +36,7 @@ struct lrt_rast {
     DeviceBuffer counters;                               // visible, pairs, err, algo err
     DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers
     lrt::SortFault sortFault;                            // lrt_radix_sort's planted fault (tests only)
+    DeviceBuffer filterCameras, filterScratch;           // lrt_rast_filter3d's cameras and lowest rate
     uint32_t* hostCounters = nullptr;                    // pinned
     cudaEvent_t ev[8] = {};
     uint32_t splatCap = 0, pairCap = 0, tileCap = 0;

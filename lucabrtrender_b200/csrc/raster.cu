@@ -239,7 +239,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
                              static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
                              status, tickets + launch, partitionBase, lastPartition, slotBits, pairBuf, r->pairCap,
-                             stream),
+                             stream, nullptr, static_cast<const float*>(c.packed->filter3d)),
                          "project");
             }
             base += c.count;
@@ -1095,7 +1095,8 @@ int enqueue_batch(lrt_rast* r, const std::vector<CloudDesc>& clouds, const lrt_v
                              static_cast<const uint4*>(c.packed->shape), static_cast<const uint32_t*>(c.packed->sh),
                              static_cast<ProjRecord*>(B.records.ptr), nullptr, nullptr, nullptr, counters, status,
                              tickets + launch, partitionBase, lastPartition, slotBits,
-                             static_cast<uint64_t*>(r->pairs.ptr), r->pairCap, B.stream, devF + li),
+                             static_cast<uint64_t*>(r->pairs.ptr), r->pairCap, B.stream, devF + li,
+                             static_cast<const float*>(c.packed->filter3d)),
                          "project");
                 partitionBase += lrt::project_partitions(c.count);
                 launch += 1;
@@ -1179,7 +1180,12 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
     uint64_t key = mix(0, nViews);
     key = mix(key, total);
     for (uint32_t v : shape.order) key = mix(mix(key, views[v].width), views[v].height);
-    for (const CloudDesc& c : clouds) key = mix(mix(key, reinterpret_cast<uintptr_t>(c.packed->positions)), c.count);
+    // Every pointer a captured launch bakes in is part of the key.
+    for (const CloudDesc& c : clouds) {
+        key = mix(mix(key, reinterpret_cast<uintptr_t>(c.packed->positions)), c.count);
+        key = mix(mix(key, reinterpret_cast<uintptr_t>(c.packed->shape)), reinterpret_cast<uintptr_t>(c.packed->sh));
+        key = mix(key, reinterpret_cast<uintptr_t>(c.packed->filter3d));
+    }
     key = mix(key, (uint64_t{s->antialias} << 1) ^ (uint64_t{s->max_sh_degree} << 3) ^ (uint64_t{s->linearise} << 7) ^
                        (uint64_t{s->depth_mode} << 9));
     shape.key = key;

@@ -430,6 +430,23 @@ class TileRasterizer:
             "visible": v.visible,
         }
 
+    def filter3d(self, cloud: GpuSplats, views: Sequence[tuple], coefficient: float = 0.2,
+                 stream=None) -> torch.Tensor:
+        """The Mip-Splatting 3D filter's variance per splat (lrt_rast_filter3d)
+        from cameras given as (Camera or Projection, width, height): assign
+        the result to ``cloud.filter3d`` to render with the filter."""
+        n = len(views)
+        cams = (_abi.Projection * max(n, 1))()
+        sizes = (C.c_uint32 * max(2 * n, 2))()
+        for k, (view, w, h) in enumerate(views):
+            cams[k] = (view if isinstance(view, Projection) else projection_for(view, w, h)).struct()
+            sizes[2 * k], sizes[2 * k + 1] = int(w), int(h)
+        out = torch.empty(cloud.count, dtype=torch.float32, device=cloud.positions.device)
+        cs = cloud.struct()
+        self._check(_abi.load().lrt_rast_filter3d(self._handle, C.byref(cs), cams, sizes, n, float(coefficient),
+                                                  out.data_ptr() if cloud.count else None, _stream_ptr(stream)))
+        return out
+
     def prefix_sum(self, values: torch.Tensor, out: torch.Tensor, total: torch.Tensor, stream=None) -> None:
         """PrefixSum::apply over uint32 bit patterns held in int32 tensors."""
         n = values.numel()

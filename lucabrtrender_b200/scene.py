@@ -49,11 +49,14 @@ class PackedSplats:
 
 @dataclass
 class GpuSplats:
-    """A packed cloud on the device. The tensors own the memory."""
+    """A packed cloud on the device. The tensors own the memory. `filter3d`
+    (optional, [N] float32): the Mip-Splatting 3D filter's variance per splat
+    (TileRasterizer.filter3d computes it); None leaves the filter off."""
     positions: torch.Tensor   # [N, 4] float32
     shape: torch.Tensor       # [N, 4] int32 (bit patterns)
     sh: torch.Tensor          # [N, sh_words] int32 (bit patterns)
     rest_per_colour: int
+    filter3d: torch.Tensor | None = None
 
     @property
     def count(self) -> int:
@@ -76,6 +79,11 @@ class GpuSplats:
         s.positions = self.positions.data_ptr() if self.count else None
         s.shape = self.shape.data_ptr() if self.count else None
         s.sh = self.sh.data_ptr() if self.count else None
+        if self.filter3d is not None and self.count:
+            if self.filter3d.dtype != torch.float32 or self.filter3d.numel() != self.count or \
+                    not self.filter3d.is_contiguous():
+                raise ValueError("filter3d must be a contiguous float32 tensor with one value per splat")
+            s.filter3d = self.filter3d.data_ptr()
         return s
 
     @property

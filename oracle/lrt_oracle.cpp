@@ -554,6 +554,17 @@ struct PackedSrc {
         p = {pos[0], pos[1], pos[2]};
         opacity = pos[3];
         scale = {expImpl(lowHalf(shape[1])), expImpl(highHalf(shape[1])), expImpl(lowHalf(shape[2]))};
+        if (c.filter3d != nullptr) {
+            // The Mip-Splatting 3D filter (Yu et al., CVPR 2024, section 4.1):
+            // scales sqrt(s^2 + v), opacity times sqrt(prod s^2 / prod (s^2 + v)).
+            const float v = static_cast<const float*>(c.filter3d)[i];
+            const float qx = scale.x * scale.x, qy = scale.y * scale.y, qz = scale.z * scale.z;
+            const float fx = qx + v, fy = qy + v, fz = qz + v;
+            const float before = qx * qy * qz;
+            const float after = fx * fy * fz;
+            opacity = opacity * std::sqrt(before / after);
+            scale = {std::sqrt(fx), std::sqrt(fy), std::sqrt(fz)};
+        }
     }
     void rotation(uint32_t i, float q[4]) const {
         decodeQuaternion(static_cast<const uint32_t*>(c.shape)[size_t{i} * 4], q);
@@ -1148,6 +1159,59 @@ int renderImpl(const lrt_projection* pr, uint64_t total, const lrt_render_settin
 }  // namespace
 
 extern "C" {
+
+// The Mip-Splatting 3D filter's variance per splat (Yu et al., CVPR 2024,
+// section 4.1), as lrt_rast_filter3d defines it: the highest sampling rate
+// focal_x / z (focal_x for an orthographic camera) over the cameras whose
+// near plane the centre is in front of and whose image, widened by 15% a
+// side, its projection falls in; variance coefficient / rate^2; unseen
+// splats take the lowest seen rate; none seen: 0.
+int ora_filter3d(const lrt_gpu_splats* cloud, const lrt_projection* cams, const uint32_t* sizes, uint32_t camCount,
+                 float coefficient, float* out) {
+    std::vector<Frame> frames(camCount);
+    lrt_splat_instance ident{};
+    const double id[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    std::memcpy(ident.object_to_world, id, sizeof(id));
+    for (uint32_t k = 0; k < camCount; ++k) {
+        lrt_render_settings s{};
+        s.width = sizes[2 * k];
+        s.height = sizes[2 * k + 1];
+        if (s.width == 0 || s.height == 0) return LRT_INVALID_ARGUMENT;
+        frames[k] = frameFor(cams[k], s);
+        setObject(frames[k], cams[k], ident);
+    }
+    const float* pos = static_cast<const float*>(cloud->positions);
+    float lowest = INFINITY;
+    for (uint32_t i = 0; i < cloud->count; ++i) {
+        const F3 p{pos[4 * i], pos[4 * i + 1], pos[4 * i + 2]};
+        float best = 0.0f;
+        for (const Frame& f : frames) {
+            const F3 t = toView(f, p);
+            if (!(t.z > f.nearZ)) continue;
+            const float invZ = f.ortho != 0 ? 1.0f : 1.0f / t.z;
+            const float sx = f.focalX * t.x * invZ + f.centreX;
+            const float sy = f.focalY * t.y * invZ + f.centreY;
+            const float w = static_cast<float>(f.width), h = static_cast<float>(f.height);
+            if (!(sx >= -0.15f * w && sx <= 1.15f * w && sy >= -0.15f * h && sy <= 1.15f * h)) continue;
+            const float r = f.focalX * invZ;
+            if (r > best) best = r;
+        }
+        out[i] = best;
+        if (best > 0.0f && best < lowest) lowest = best;
+    }
+    for (uint32_t i = 0; i < cloud->count; ++i) {
+        float r = out[i];
+        if (!(r > 0.0f)) {
+            if (!(lowest < INFINITY)) {
+                out[i] = 0.0f;
+                continue;
+            }
+            r = lowest;
+        }
+        out[i] = coefficient / (r * r);
+    }
+    return LRT_OK;
+}
 
 int ora_render(const lrt_projection* pr, const lrt_splat_instance* instances, uint32_t n,
                const lrt_render_settings* s, ora_frame_out* out, uint32_t threads) {

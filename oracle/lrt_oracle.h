@@ -66,6 +66,11 @@ int ora_pack_splats(const float* raw, uint32_t count, uint32_t floats_per_record
                     uint32_t file_per_colour, uint32_t keep_per_colour, float* positions,
                     uint32_t* shape, uint32_t* sh, uint32_t* kept);
 
+/* The Mip-Splatting 3D filter's variance per splat (lrt_rast_filter3d's
+ * definition; host pointers). */
+int ora_filter3d(const lrt_gpu_splats* cloud, const lrt_projection* cameras, const uint32_t* sizes,
+                 uint32_t camera_count, float coefficient, float* variance);
+
 /* The tile rasteriser (splats in lrt_gpu_splats are HOST pointers here). */
 int ora_render(const lrt_projection* projection, const lrt_splat_instance* instances,
                uint32_t instance_count, const lrt_render_settings* settings,

@@ -124,6 +124,23 @@ def projection_for(camera: _abi.CameraStruct, width: int, height: int) -> _abi.P
     return out
 
 
+def filter3d(cloud: "HostCloud", views, coefficient: float = 0.2) -> np.ndarray:
+    """The 3D filter's variance per splat from (Projection struct, width, height) views."""
+    n = len(views)
+    cams = (_abi.Projection * max(n, 1))()
+    sizes = (C.c_uint32 * max(2 * n, 2))()
+    for k, (pr, w, h) in enumerate(views):
+        cams[k] = pr
+        sizes[2 * k], sizes[2 * k + 1] = int(w), int(h)
+    out = np.zeros(cloud.count, np.float32)
+    cs = cloud.struct()
+    lib = load()
+    lib.ora_filter3d.argtypes = [C.POINTER(_abi.GpuSplatsStruct), C.POINTER(_abi.Projection), C.POINTER(C.c_uint32),
+                                 C.c_uint32, C.c_float, C.c_void_p]
+    _check(lib.ora_filter3d(C.byref(cs), cams, sizes, n, float(coefficient), out.ctypes.data), "filter3d")
+    return out
+
+
 # --------------------------------------------------------------- packing ----
 @dataclass
 class HostCloud:
@@ -131,6 +148,7 @@ class HostCloud:
     shape: np.ndarray       # [N, 4] uint32
     sh: np.ndarray          # [N, words] uint32
     rest_per_colour: int
+    filter3d: np.ndarray | None = None   # [N] float32, the 3D filter's variance
 
     @property
     def count(self) -> int:
@@ -144,6 +162,9 @@ class HostCloud:
         s.positions = self.positions.ctypes.data
         s.shape = self.shape.ctypes.data
         s.sh = self.sh.ctypes.data
+        if self.filter3d is not None:
+            assert self.filter3d.dtype == np.float32 and self.filter3d.flags["C_CONTIGUOUS"]
+            s.filter3d = self.filter3d.ctypes.data
         return s
 
 
