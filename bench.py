@@ -406,14 +406,14 @@ HEAVY_WIDTH, HEAVY_HEIGHT = 3840, 2160
 HEAVY_SEED = 7
 
 
-def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int) -> dict:
+def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int, splats: int = HEAVY_SPLATS) -> dict:
     """The sort-heavy frame: 6M splats with means N(0,2) and log-scales
     N(-3.5,0.7), 3840x2160, 16x16 tiles, camera 4 units out. Per-stage ms
     from the frame's own events, pairs, and the pair sort's algorithmic bytes
     per second against the HBM peak. The cloud is decoded on the device from
     its raw records (the same bytes as the host packing). The working set
     (about 4 GB of pair words) is far larger than L2, so no flush is needed."""
-    raw = L.synthetic_records(HEAVY_SPLATS, HEAVY_SEED, mean_sigma=2.0, log_scale_mean=-3.5, log_scale_sigma=0.7)
+    raw = L.synthetic_records(splats, HEAVY_SEED, mean_sigma=2.0, log_scale_mean=-3.5, log_scale_sigma=0.7)
     raw_dev = torch.from_numpy(raw).to(dev)
     del raw
     stream = torch.cuda.current_stream(dev)
@@ -445,7 +445,8 @@ def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int) -> dict:
     sort_ms = float(np.mean([x.tile_sort_ms for x in st]))
     sort_bytes = (passes * 16 + 8) * pairs
     gbs = sort_bytes / (sort_ms * 1e-3) / 1e9
-    out = {"workload": "6M splats, means N(0,2), log-scales N(-3.5,0.7), 3840x2160, 16x16 tiles, eye (0, 0, 4)",
+    out = {"workload": f"{splats / 1e6:g}M splats, means N(0,2), log-scales N(-3.5,0.7), 3840x2160, 16x16 tiles, "
+                       "eye (0, 0, 4)",
            "steps": steps, "ms_per_frame": round(float(np.mean(frame_ms)), 4),
            "stages_ms": {k: round(float(np.mean([getattr(x, k) for x in st])), 4)
                          for k in ("project_ms", "tile_sort_ms", "blend_ms")},
@@ -457,6 +458,22 @@ def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int) -> dict:
     del cloud, inst, targets
     torch.cuda.empty_cache()
     return out
+
+
+def run_heavy_only(args) -> None:
+    """Only the sort-heavy frame (for profiling that workload, or a smaller
+    one of the same distributions with --heavy-splats)."""
+    import torch
+    import lucabrtrender_b200 as L
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    clocks = Clocks(0).start()
+    raster = L.TileRasterizer.create(0)
+    heavy = run_sort_heavy(L, torch, dev, raster, measured_peaks()[0], clocks, args.steps, args.heavy_splats)
+    clocks.stop()
+    heavy["clocks"] = clocks.summary()
+    print(json.dumps(heavy), flush=True)
+    raster.close()
 
 
 def run_ours(args) -> None:
@@ -656,7 +673,8 @@ def run_ours(args) -> None:
     # --- the sort-heavy frame ---
     heavy = None
     if not args.no_heavy:
-        heavy = run_sort_heavy(L, torch, dev, raster, measured_peaks()[0], clocks, max(3, args.steps // 4))
+        heavy = run_sort_heavy(L, torch, dev, raster, measured_peaks()[0], clocks, max(3, args.steps // 4),
+                               args.heavy_splats)
 
     # --- many views: one batched call against sequential renders ---
     batch = None
@@ -748,10 +766,15 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-next", action="store_true")
     ap.add_argument("--no-heavy", action="store_true")
+    ap.add_argument("--heavy-only", action="store_true",
+                    help="run only the sort-heavy frame (--steps frames after 2 warm-up frames)")
+    ap.add_argument("--heavy-splats", type=int, default=HEAVY_SPLATS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.heavy_only:
+        run_heavy_only(args)
     else:
         run_ours(args)
 

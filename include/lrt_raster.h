@@ -402,6 +402,11 @@ int lrt_rast_train_batch(lrt_rast* rast, const lrt_train_params* params, const l
                          uint32_t view_count, const lrt_render_settings* settings, lrt_train_grads* grads,
                          lrt_batch_stats* stats, void* stream);
 
+/* Test hook of lrt_rast_train_batch (no counterpart in the reference): fixes
+ * its views per chunk and blend blocks per SM for the handle's later steps
+ * instead of timing candidates (0, 0: tune again). */
+int lrt_rast_debug_train_chunking(lrt_rast* rast, uint32_t views_per_chunk, uint32_t blocks_per_sm);
+
 
 /* PrefixSum::apply: exclusive scan of `count` uint32 at `in` into `out`, the
  * sum into `total` (all device pointers; `out` may alias `in`). Single pass,
@@ -429,15 +434,19 @@ int lrt_rast_filter3d(lrt_rast* rast, const lrt_gpu_splats* cloud, const lrt_pro
                       const uint32_t* sizes, uint32_t camera_count, float coefficient, float* variance,
                       void* stream);
 
-/* Test hook for the bounded waits (no counterpart in the reference, whose
- * sort never waits on another workgroup). While set on a handle, its
- * lrt_radix_sort runs the last digit pass with partition 0 never taken, so
- * the partition after it waits for counts nobody publishes. That wait gives
- * up after `poll_limit` polls (0: the normal limit, 2^22), the call returns
- * LRT_TIMEOUT, and the keys are left in an undefined order (every write stays
- * inside the buffers). Clearing it (0, 0) restores normal sorts; the handle
- * stays usable throughout. */
-int lrt_rast_debug_sort_fault(lrt_rast* rast, uint32_t skip_first_partition, uint32_t poll_limit);
+/* Test hooks of a handle's lrt_radix_sort (no counterpart in the reference,
+ * whose sort never waits on another workgroup):
+ *   skip_first_partition  the last digit pass runs with partition 0 never
+ *       taken, so the partition after it waits for counts nobody publishes.
+ *       That wait gives up after `poll_limit` polls (0: the normal limit,
+ *       2^22), the call returns LRT_TIMEOUT, and the keys are left in an
+ *       undefined order (every write stays inside the buffers);
+ *   wide_look_back  the 64-bit look-back words that sorts of 2^30 keys or
+ *       more use, at any size.
+ * Clearing them (0, 0, 0) restores normal sorts; the handle stays usable
+ * throughout. */
+int lrt_rast_debug_sort(lrt_rast* rast, uint32_t skip_first_partition, uint32_t poll_limit,
+                        uint32_t wide_look_back);
 
 /* The prefix sum above for callers that cannot allocate device memory: a
  * plugin running inside a host application that owns every device allocation

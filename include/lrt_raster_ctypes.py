@@ -41,7 +41,7 @@ EXPORTS = (
     "lrt_rast_decode_splats", "lrt_rast_decode_points", "lrt_rast_compare_images", "lrt_rast_compare_hdr",
     "lrt_rast_count_different", "lrt_rast_l1_loss", "lrt_l1_loss_grad", "lrt_lod_build_settings_default",
     "lrt_lod_build", "lrt_lod_destroy", "lrt_lod_get_info", "lrt_lod_splats", "lrt_lod_level", "lrt_lod_starts",
-    "lrt_lod_select", "lrt_rast_train_batch", "lrt_rast_debug_sort_fault", "lrt_rast_filter3d",
+    "lrt_lod_select", "lrt_rast_train_batch", "lrt_rast_debug_sort", "lrt_rast_filter3d", "lrt_rast_debug_train_chunking",
 )
 PREFIX_SUM_NOALLOC_MAX = 1 << 26
 

@@ -70,7 +70,8 @@ def load() -> C.CDLL:
     lib.lrt_prefix_sum.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     lib.lrt_radix_sort.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                    C.c_void_p]
-    lib.lrt_rast_debug_sort_fault.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.lrt_rast_debug_sort.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32]
+    lib.lrt_rast_debug_train_chunking.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
     lib.lrt_rast_filter3d.argtypes = [C.c_void_p, C.POINTER(GpuSplatsStruct), C.POINTER(Projection),
                                       C.POINTER(C.c_uint32), C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]
     lib.lrt_pack_splats.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,

@@ -42,7 +42,8 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
                                       uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
                                       uint32_t lastPartition, uint32_t lowBits, uint64_t* pairs, uint32_t* values,
-                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream);
+                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream,
+                                      const FrameParams* fDev = nullptr);
 
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
@@ -53,9 +54,12 @@ cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* t
 // never publishes its counts; the partition after it polls at most
 // `pollLimit` times, gives up, sets kErrTimeout and carries on (the sort's
 // output is then undefined, every write still in bounds).
+// `wideWords` makes a sort of fewer than 2^30 keys use the 64-bit look-back
+// words that larger sorts need, so that tests can check that form.
 struct SortFault {
     uint32_t skipFirstPartition = 0;
     uint32_t pollLimit = 0;   // 0: the normal limit
+    uint32_t wideWords = 0;
 };
 
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);

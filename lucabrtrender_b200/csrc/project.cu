@@ -278,6 +278,152 @@ struct TrainOutputs {
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
+
+// ---- Splats of more than kSmallArea tiles, one tile row at a time ----
+//
+// The tiles of a row that the exact test (tile_touched) accepts are those
+// whose box of pixel centres meets the ellipse {power <= cutoff}; within the
+// row's band of pixel centres, the ellipse spans one x interval [XL, XR]. In
+// double precision that interval gives, with a margin m covering every
+// rounding of the float test (its inputs' rounding and the power's, which
+// grows with the conic's condition number), the columns that are certainly
+// touched and the few around them that must be tested exactly. A row is then
+// counted in O(1) plus a handful of exact tests, and its pairs are the
+// certain run with the exact hits either side of it: the counts and pairs
+// are the per-tile test's own, at a cost that follows the pairs, not the
+// rectangle's area. Rows near the top or bottom of the ellipse, and
+// ill-conditioned conics, are tested tile by tile.
+struct Footprint {
+    float cx, cy, a, b, c, cut;
+    uint32_t x0, x1;      // the rectangle's columns
+    uint32_t y0;          // its first row
+    uint32_t tid;         // the splat's thread in the block
+    uint32_t shMasked;    // mask row shift | 0x100 when the splat keeps a tile mask
+};
+
+struct RowPlan {
+    int32_t lo, hi;           // candidate columns, inside the rectangle (none when lo > hi)
+    int32_t sureLo, sureHi;   // certainly touched columns, inside [lo, hi] (none when sureLo > sureHi)
+};
+
+// The x range of tile column t's pixel centres, relative to the centre, as
+// tile_touched forms it (the same float values, here exact in double).
+__device__ __forceinline__ double col_lo(int32_t t, float cx) {
+    return static_cast<double>(static_cast<float>(t * static_cast<int32_t>(kTile)) + 0.5f) - static_cast<double>(cx);
+}
+__device__ __forceinline__ double col_hi(int32_t t, uint32_t width, float cx) {
+    const int32_t last = min((t + 1) * static_cast<int32_t>(kTile), static_cast<int32_t>(width)) - 1;
+    return static_cast<double>(static_cast<float>(last) + 0.5f) - static_cast<double>(cx);
+}
+
+__device__ __forceinline__ RowPlan row_plan(const Footprint& fp, uint32_t ty, uint32_t width, uint32_t height) {
+    RowPlan p{static_cast<int32_t>(fp.x0), static_cast<int32_t>(fp.x1), 1, 0};   // default: every column exact
+    const double a = fp.a, b = fp.b, c = fp.c, k = fp.cut;
+    const double det = a * c - b * b;
+    if (!(a > 0.0) || !(c > 0.0) || !(k > 0.0) || !(det > 1e-6 * a * c)) return p;
+    const double hx = sqrt(k * c / det), hy = sqrt(k * a / det);
+    // Margin: the float test's power carries a relative error of a few
+    // roundings times the condition number kappa, which moves the boundary
+    // by at most that times the half-axes; its box coordinates carry one
+    // rounding of magnitudes up to |centre| + extent. Both with a factor of
+    // 16 to spare, plus a quarter pixel.
+    const double lmin = 0.5 * (a + c) - sqrt(0.25 * (a - c) * (a - c) + b * b);
+    if (!(lmin > 0.0)) return p;
+    const double kappa = (fabs(a) + 2.0 * fabs(b) + fabs(c)) / lmin;
+    const double reach = fabs(static_cast<double>(fp.cx)) + fabs(static_cast<double>(fp.cy)) + hx + hy + 64.0;
+    const double m = 0.25 + 16.0 * 6.0e-8 * (4.0 * kappa * (hx + hy) + reach);
+    if (!(m < 24.0)) return p;
+    const int32_t ity = static_cast<int32_t>(ty);
+    const double ylo = static_cast<double>(static_cast<float>(ity * static_cast<int32_t>(kTile)) + 0.5f) -
+                       static_cast<double>(fp.cy);
+    const int32_t lastRow = min((ity + 1) * static_cast<int32_t>(kTile), static_cast<int32_t>(height)) - 1;
+    const double yhi = static_cast<double>(static_cast<float>(lastRow) + 0.5f) - static_cast<double>(fp.cy);
+    if (yhi < -hy - m || ylo > hy + m) {   // the band misses the ellipse by more than the margin
+        p.lo = 1;
+        p.hi = 0;
+        return p;
+    }
+    if (yhi < -hy + m || ylo > hy - m) return p;   // near its top or bottom: every column exact
+    // The ellipse's x extent within the band: its leftmost and rightmost
+    // points (x = -+hx, y = -b x / c) clamped into the band.
+    const double yl = fmin(fmax(b * hx / c, ylo), yhi);
+    const double yr = fmin(fmax(-b * hx / c, ylo), yhi);
+    const double xl = (-b * yl - sqrt(fmax(k * a - det * yl * yl, 0.0))) / a;
+    const double xr = (-b * yr + sqrt(fmax(k * a - det * yr * yr, 0.0))) / a;
+    // First column whose hi >= v, and last whose lo <= v, within the
+    // rectangle (the estimate is exact but for the clipped last column; the
+    // adjustment steps are bounded and, if they do not settle, every column
+    // is tested exactly).
+    const int32_t x0 = static_cast<int32_t>(fp.x0), x1 = static_cast<int32_t>(fp.x1);
+    bool ok = true;
+    auto firstHiAtLeast = [&](double v) -> int32_t {
+        const double e = ceil((v + static_cast<double>(fp.cx) - 15.5) / 16.0);
+        int32_t t = static_cast<int32_t>(fmin(fmax(e, static_cast<double>(x0)), static_cast<double>(x1 + 1)));
+        for (int it = 0; it < 3 && t > x0 && col_hi(t - 1, width, fp.cx) >= v; ++it) --t;
+        for (int it = 0; it < 3 && t <= x1 && col_hi(t, width, fp.cx) < v; ++it) ++t;
+        if ((t > x0 && col_hi(t - 1, width, fp.cx) >= v) || (t <= x1 && col_hi(t, width, fp.cx) < v)) ok = false;
+        return t;
+    };
+    auto lastLoAtMost = [&](double v) -> int32_t {
+        const double e = floor((v + static_cast<double>(fp.cx) - 0.5) / 16.0);
+        int32_t t = static_cast<int32_t>(fmin(fmax(e, static_cast<double>(x0 - 1)), static_cast<double>(x1)));
+        for (int it = 0; it < 3 && t < x1 && col_lo(t + 1, fp.cx) <= v; ++it) ++t;
+        for (int it = 0; it < 3 && t >= x0 && col_lo(t, fp.cx) > v; ++it) --t;
+        if ((t < x1 && col_lo(t + 1, fp.cx) <= v) || (t >= x0 && col_lo(t, fp.cx) > v)) ok = false;
+        return t;
+    };
+    const int32_t lo = firstHiAtLeast(xl - m), hi = lastLoAtMost(xr + m);
+    const int32_t sureLo = firstHiAtLeast(xl + m), sureHi = lastLoAtMost(xr - m);
+    if (!ok) return p;
+    p.lo = lo;
+    p.hi = hi;
+    p.sureLo = max(sureLo, lo);
+    p.sureHi = min(sureHi, hi);
+    return p;
+}
+
+// A row's touched tiles in column order: `visit(t)` for each exact hit and
+// `run(t0, t1)` for the certain run [t0, t1].
+template <class Hit, class Run>
+__device__ __forceinline__ void row_walk(const Footprint& fp, uint32_t ty, uint32_t width, uint32_t height,
+                                         Hit&& visit, Run&& run) {
+    const RowPlan p = row_plan(fp, ty, width, height);
+    const bool sure = p.sureLo <= p.sureHi;
+    const int32_t leftEnd = sure ? p.sureLo - 1 : p.hi;
+    for (int32_t t = p.lo; t <= leftEnd; ++t)
+        if (tile_touched(width, height, fp.cx, fp.cy, fp.a, fp.b, fp.c, fp.cut, static_cast<uint32_t>(t), ty)) visit(t);
+    if (!sure) return;
+    run(p.sureLo, p.sureHi);
+    for (int32_t t = p.sureHi + 1; t <= p.hi; ++t)
+        if (tile_touched(width, height, fp.cx, fp.cy, fp.a, fp.b, fp.c, fp.cut, static_cast<uint32_t>(t), ty)) visit(t);
+}
+
+// One row: its count, first and last touched column, whether its hits are
+// one run, and (for a masked splat) its tiles' bits, rows `1 << sh` apart.
+struct RowCount {
+    uint32_t count;
+    int32_t first, last;
+    bool regular;
+    unsigned long long bits;
+};
+__device__ __forceinline__ RowCount row_count(const Footprint& fp, uint32_t r, uint32_t width, uint32_t height) {
+    RowCount rc{0, 0, -2, true, 0ull};
+    const bool masked = (fp.shMasked & 0x100u) != 0;
+    const uint32_t base = (r << (fp.shMasked & 0xFFu));
+    auto add = [&](int32_t t0, int32_t t1) {
+        if (rc.count != 0 && t0 != rc.last + 1) rc.regular = false;
+        if (rc.count == 0) rc.first = t0;
+        rc.count += static_cast<uint32_t>(t1 - t0 + 1);
+        rc.last = t1;
+        if (masked) {
+            const uint32_t n = static_cast<uint32_t>(t1 - t0 + 1);
+            const unsigned long long ones = n >= 64 ? ~0ull : (1ull << n) - 1ull;
+            rc.bits |= ones << (base + static_cast<uint32_t>(t0) - fp.x0);
+        }
+    };
+    row_walk(fp, fp.y0 + r, width, height, [&](int32_t t) { add(t, t); }, add);
+    return rc;
+}
 constexpr uint64_t kFlagAggregate = 1ull << 62;
 constexpr uint64_t kFlagInclusive = 2ull << 62;
 constexpr uint64_t kValueMask = (1ull << 62) - 1;
@@ -332,6 +478,96 @@ struct PairSink {
     }
 };
 
+// The block's large splats counted a tile row per thread per step (rows in
+// list order, splat after splat): counts added into counts[splat thread]
+// (bit 31 marks a splat with a row that is not one run), tile bits of masked
+// splats or-ed into masks[splat thread]. Kept out of line: the kernel's other
+// paths do not pay for its registers.
+__device__ __noinline__ void count_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
+                                              uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t* counts,
+                                              unsigned long long* masks) {
+    const uint32_t tid = threadIdx.x;
+    uint32_t fs = 0;   // the splat of row item j: found by search once, then advanced
+    {
+        uint32_t lo = 0, hi = bigTotal;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (footRow[mid] <= tid) lo = mid; else hi = mid;
+        }
+        fs = lo;
+    }
+    for (uint32_t j = tid; j < rowsTotal; j += kProjectThreads) {
+        while (footRow[fs + 1] <= j) ++fs;
+        const Footprint fp = foot[fs];
+        const RowCount rc = row_count(fp, j - footRow[fs], width, height);
+        if (rc.count != 0) atomicAdd(&counts[fp.tid], rc.count);
+        if (!rc.regular) atomicOr(&counts[fp.tid], 0x80000000u);
+        if (rc.bits != 0) atomicOr(&masks[fp.tid], rc.bits);
+    }
+}
+
+// The pairs of the block's large, unmasked splats whose rows are single runs:
+// a chunk of 256 rows at a time, each row's count and first column from its
+// row plan (as when counting), flattened so that consecutive threads write
+// consecutive pairs. takenStart[t]: the pairs of such splats before splat t.
+template <class Sink>
+__device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
+                                             uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t tileBase,
+                                             uint32_t tilesX, const uint32_t* widthBits, const uint32_t* start,
+                                             const uint32_t* takenStart, const unsigned long long* low,
+                                             uint32_t* rowOff, uint32_t* rowFirst, uint32_t* rowMeta,
+                                             uint32_t* scanScratch, unsigned long long blockBase, uint32_t tileShift,
+                                             uint32_t slotBase, const Sink& sink) {
+    const uint32_t tid = threadIdx.x;
+    uint32_t fs = 0;
+    {
+        uint32_t lo = 0, hi = bigTotal;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (footRow[mid] <= tid) lo = mid; else hi = mid;
+        }
+        fs = lo;
+    }
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < rowsTotal; c0 += kProjectThreads) {
+        const uint32_t j = c0 + tid;
+        uint32_t cnt = 0, first = 0, meta = 0;
+        if (j < rowsTotal) {
+            while (footRow[fs + 1] <= j) ++fs;
+            const Footprint fp = foot[fs];
+            if ((fp.shMasked & 0x100u) == 0 && (widthBits[fp.tid] & 0x80000000u) == 0) {
+                const uint32_t r = j - footRow[fs];
+                const RowCount rc = row_count(fp, r, width, height);
+                cnt = rc.count;
+                first = static_cast<uint32_t>(rc.first);
+                meta = (fp.y0 + r) | (fp.tid << 16);
+            }
+        }
+        uint32_t chunkTotal = 0;
+        const uint32_t off = block_exclusive_scan(cnt, scanScratch, &chunkTotal);
+        rowOff[tid] = off;
+        rowFirst[tid] = first;
+        rowMeta[tid] = meta;
+        if (tid == 0) rowOff[kProjectThreads] = chunkTotal;
+        __syncthreads();
+        for (uint32_t k = tid; k < chunkTotal; k += kProjectThreads) {
+            uint32_t lo = 0, hi = kProjectThreads;   // the last row q with rowOff[q] <= k
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (rowOff[mid] <= k) lo = mid; else hi = mid;
+            }
+            const uint32_t q = lo;
+            const uint32_t ty = rowMeta[q] & 0xFFFFu, owner = rowMeta[q] >> 16;
+            const uint32_t tx = rowFirst[q] + (k - rowOff[q]);
+            sink.put(blockBase + start[owner] + (carry + k - takenStart[owner]),
+                     (static_cast<unsigned long long>(tileBase + ty * tilesX + tx) << tileShift) | low[owner],
+                     slotBase + owner);
+        }
+        carry += chunkTotal;
+        __syncthreads();
+    }
+}
+
 template <class Src>
 __global__ void __launch_bounds__(kProjectThreads, 4)
 project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
@@ -349,6 +585,11 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     __shared__ unsigned long long sLow[kProjectThreads];   // depth key << lowBits
     __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
     __shared__ uint32_t sWidth[kProjectThreads];
+    __shared__ Footprint sFoot[kProjectThreads];           // the block's splats of more than kSmallArea tiles
+    __shared__ uint32_t sFootRow[kProjectThreads + 1];     // their first row in the block's row list
+    __shared__ uint32_t sRowFirst[kProjectThreads];        // emission: a chunk's rows, first column
+    __shared__ uint32_t sRowMeta[kProjectThreads];         // emission: tile row | splat thread << 16
+    __shared__ uint32_t sRowOff[kProjectThreads + 1];      // emission: the chunk's rows' pair offsets
     __shared__ unsigned long long sBase;
     // The frame's parameters: by value, or (when a captured graph replays a
     // batch with new cameras) read from device memory, once per block.
@@ -532,48 +773,14 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             }
         }
     }
-    uint32_t big = __ballot_sync(0xFFFFFFFFu, alive && area > kSmallArea);
-    while (big != 0) {
-        const int src = __ffs(big) - 1;
-        big &= big - 1;
-        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
-        const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
-        const uint32_t sSh = __shfl_sync(0xFFFFFFFFu, sh, src);
-        const bool sMasked = __shfl_sync(0xFFFFFFFFu, masked ? 1u : 0u, src) != 0;
-        const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
-        const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
-        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
-        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
-        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
-        // Lane l tests tiles l, l + 32, ... of the rectangle, row-major; its
-        // column and row advance by 32 tiles per step without a division.
-        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
-        uint32_t dx = lane % sW, dy = lane / sW;
-        uint32_t count = 0;
-        uint32_t mLo = 0, mHi = 0;
-        for (uint32_t base = 0; base < sArea; base += 32) {
-            const bool hit = base + lane < sArea &&
-                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + dx, sY + dy);
-            count += static_cast<uint32_t>(__popc(__ballot_sync(0xFFFFFFFFu, hit)));
-            if (sMasked) {
-                const uint32_t bit = (dy << sSh) | dx;
-                mLo |= __reduce_or_sync(0xFFFFFFFFu, hit && bit < 32u ? 1u << bit : 0u);
-                mHi |= __reduce_or_sync(0xFFFFFFFFu, hit && bit >= 32u ? 1u << (bit - 32u) : 0u);
-            }
-            dx += stepDx;
-            dy += stepDy;
-            if (dx >= sW) {
-                dx -= sW;
-                dy += 1;
-            }
-        }
-        if (lane == static_cast<uint32_t>(src)) {
-            touched = count;
-            mask = sMasked ? (static_cast<unsigned long long>(mHi) << 32) | mLo : 0ull;
-        }
+    // Splats of more than kSmallArea tiles are counted by the whole block
+    // below, after the records are written (so that the projection's values
+    // are no longer held in registers); the others are decided now.
+    const bool bigHere = alive && area > kSmallArea;
+    if (!bigHere) {
+        alive = alive && touched != 0;
+        if (!alive) touched = 0;
     }
-    alive = alive && touched != 0;
-    if (!alive) touched = 0;
 
     if (stageWords != 0) cp_async_wait_all();
     __syncthreads();
@@ -624,6 +831,49 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             proj[record] = rec;
             if (f.writeDebug) rects[record] = make_uint4(1, 1, 0, 0);
         }
+    }
+
+    // The block counts its large splats a tile row per thread per step, into
+    // sSmallStart (zeroed here; the block scan writes it later) and, for a
+    // masked splat, its tile bits into sMask. A row whose hits are not one
+    // run marks its splat (bit 31) for the per-tile emission.
+    uint32_t bigTotal = 0, rowsTotal = 0, bigIdx = 0;
+    const bool anyBig = __syncthreads_or(bigHere ? 1 : 0) != 0;   // most blocks have none
+    if (anyBig) {
+        bigIdx = block_exclusive_scan(bigHere ? 1u : 0u, sScan, &bigTotal);
+        const uint32_t rowStart = block_exclusive_scan(bigHere ? rh : 0u, sScan, &rowsTotal);
+        sSmallStart[tid] = 0;
+        sMask[tid] = 0ull;
+        if (bigHere) {
+            sFoot[bigIdx] = Footprint{cx, cy, ca, cb, cc, cutoff, rect.x, rect.z, rect.y, tid,
+                                      sh | (masked ? 0x100u : 0u)};
+            sFootRow[bigIdx] = rowStart;
+        }
+        if (tid == 0) sFootRow[bigTotal] = rowsTotal;
+        __syncthreads();
+    }
+    if (rowsTotal != 0) {
+        count_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, sSmallStart, sMask);
+        __syncthreads();
+    }
+    bool irregular = false;
+    if (bigHere) {
+        const uint32_t v = sSmallStart[tid];
+        touched = v & 0x7FFFFFFFu;
+        irregular = (v & 0x80000000u) != 0;
+        mask = masked ? sMask[tid] : 0ull;
+        if (touched == 0) {   // no tile holds a pixel centre inside it: culled after all
+            alive = false;
+            key = 0x00FFFFFFu;
+            ProjRecord rec;
+            rec.screen = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            rec.conic = rec.screen;
+            rec.colour = rec.screen;
+            proj[record] = rec;
+            if (f.writeDebug) rects[record] = make_uint4(1, 1, 0, 0);
+        }
+    }
+    if (inRange) {
         if (f.writeDebug || train.offsets != nullptr) touchedOut[record] = touched;
         if (f.writeDebug) keysOut[record] = key;
     }
@@ -640,7 +890,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     sMask[tid] = mask;
     sLow[tid] = static_cast<unsigned long long>(key) << lowBits;
     sRect[tid] = rect.x | (rect.y << 16);
-    sWidth[tid] = rw | (sh << 16);
+    sWidth[tid] = rw | (sh << 16) | (irregular ? 0x80000000u : 0u);
     if (tid == 0) {
         sStart[kProjectThreads] = blockTotal;
         sSmallStart[kProjectThreads] = smallTotal;
@@ -719,25 +969,42 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         unsigned long long m = sMask[s];
         for (; r > 0; --r) m &= m - 1;   // drop the r lowest set bits
         const uint32_t bit = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
-        const uint32_t bsh = sWidth[s] >> 16;
+        const uint32_t bsh = (sWidth[s] >> 16) & 0xFFu;
         const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
         const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
         sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
                  (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s],
                  slotBase + s);
     }
-    // The rest: their warp repeats the tile test 32 tiles at a time.
-    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && !masked);
+    // The rest (rectangles too large for a mask): the block writes their
+    // pairs a chunk of 256 tile rows at a time, each row's count and first
+    // column from its row plan (the same as when counting), flattened so
+    // that consecutive threads write consecutive pairs. A splat's rows are in
+    // order, so its pairs follow one another from its offset.
+    if (rowsTotal != 0) {
+        __syncthreads();   // the masked writes are done with sSmallStart
+        const bool taken = touched != 0 && !masked && !irregular;
+        uint32_t takenTotal = 0;
+        sSmallStart[tid] = block_exclusive_scan(taken ? touched : 0u, sScan, &takenTotal);
+        __syncthreads();
+        if (takenTotal != 0)
+            emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, f.tileBase, f.tilesX, sWidth,
+                            sStart, sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, blockBase, tileShift,
+                            slotBase, sink);
+    }
+    // A splat whose rows are not all single runs (possible only through the
+    // float test's rounding at the ellipse's edge): its warp repeats the exact
+    // tile test over the rectangle, 32 tiles at a time.
+    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && !masked && irregular);
     while (large != 0) {
         const int src = __ffs(large) - 1;
         large &= large - 1;
         const uint32_t s = (tid & ~31u) + static_cast<uint32_t>(src);
         const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
+        const Footprint sfp = sFoot[__shfl_sync(0xFFFFFFFFu, bigIdx, src)];
         const uint32_t sW = sWidth[s] & 0xFFFFu;
         const uint32_t sX = sRect[s] & 0xFFFFu, sY = sRect[s] >> 16;
-        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
-        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
-        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+        const float scx = sfp.cx, scy = sfp.cy, sa = sfp.a, sb = sfp.b, sc = sfp.c, scut = sfp.cut;
         unsigned long long at = blockBase + sStart[s];
         const unsigned long long low = sLow[s];
         const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
@@ -818,10 +1085,11 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* offsets,
                                       uint32_t* counters, uint64_t* status, uint32_t* ticket, uint32_t partitionBase,
                                       uint32_t lastPartition, uint32_t lowBits, uint64_t* pairs, uint32_t* values,
-                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream) {
+                                      uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream,
+                                      const FrameParams* fDev) {
     if (f.count == 0) return cudaSuccess;
     // The DC triple is read from the staged row too, so it is always staged.
-    return launch(f, nullptr, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
+    return launch(f, fDev, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
                   TrainOutputs{offsets, values, emitSlot}, true, proj, rects, touched, keys, counters, status, ticket,
                   partitionBase, lastPartition, lowBits, pairs, capacity, stream);
 }

@@ -45,10 +45,10 @@ struct lrt_rast {
     DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
     DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
     DeviceBuffer lossScratch;                            // the L1 loss's per-block sums
-    // Training batches (train_batch.cu): colour gradients, view parameters
-    // and queue, losses with no caller buffer, the chunk's frame parameters;
-    // their pair capacity.
-    DeviceBuffer trainBatchGrad, trainBatchViews, trainBatchLoss, trainBatchFrames;
+    // Training batches (train_batch.cu): colour gradients, every view's view
+    // and frame parameters with the chunks' queues, losses with no caller
+    // buffer; their pair capacity.
+    DeviceBuffer trainBatchGrad, trainBatchViews, trainBatchLoss;
     uint32_t trainBatchPairCap = 0;
     void* metricHost = nullptr;                          // pinned readback of the metrics
     size_t metricHostBytes = 0;
@@ -94,6 +94,24 @@ struct lrt_rast {
         bool graphFailed = false;
         std::vector<std::pair<uint64_t, std::pair<uint32_t, uint32_t>>> tuned;   // shape -> (views per chunk, blocks/SM)
     } batch;
+    // Training batches (train_batch.cu): a stream of their own, the views'
+    // and frames' parameters staged in pinned memory, per-chunk counters read
+    // back once a step, the captured step and the tuned shapes.
+    struct TrainBatch {
+        cudaStream_t stream = nullptr;
+        cudaEvent_t in = nullptr, out = nullptr, start = nullptr, end = nullptr;
+        DeviceBuffer counters;
+        void* hostParams = nullptr;        // pinned: ViewParams then FrameParams for every view
+        size_t hostParamsBytes = 0;
+        uint32_t* hostCounters = nullptr;  // pinned: 4 words per chunk
+        uint32_t hostCounterChunks = 0;
+        uint64_t generation = 0;           // bumped whenever a buffer the graph uses moves
+        cudaGraphExec_t graph = nullptr;
+        uint64_t graphKey = 0, graphGeneration = 0;
+        bool graphFailed = false;
+        std::vector<std::pair<uint64_t, std::pair<uint32_t, uint32_t>>> tuned;   // shape -> (views per chunk, blocks/SM)
+        uint32_t fixedChunk = 0, fixedBlocks = 0;   // set by the test hook: no tuning
+    } trainBatch;
     // Levels of detail: the clouds the last lrt_lod_select made, one per
     // instance, rewritten by the next call, and the builds' temporaries, kept
     // from one build to the next (lod_host.cu).

@@ -62,7 +62,7 @@ void lrt_rast_destroy(lrt_rast* r) {
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
                             &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
-                            &r->trainBatchViews, &r->trainBatchLoss, &r->trainBatchFrames, &r->lodBuild.globals,
+                            &r->trainBatchViews, &r->trainBatchLoss, &r->lodBuild.globals,
                             &r->lodBuild.partial, &r->lodBuild.keys, &r->lodBuild.keysAlt, &r->lodBuild.order,
                             &r->lodBuild.orderAlt, &r->lodBuild.sortScratch, &r->lodBuild.status,
                             &r->lodBuild.firstChild, &r->lodBuild.moments, &r->lodBuild.err})
@@ -84,6 +84,15 @@ void lrt_rast_destroy(lrt_rast* r) {
     for (cudaEvent_t e : {B.in, B.out, B.start, B.end})
         if (e != nullptr) cudaEventDestroy(e);
     if (B.stream != nullptr) cudaStreamDestroy(B.stream);
+    auto& TB = r->trainBatch;
+    release(TB.counters);
+    if (TB.hostParams != nullptr) cudaFreeHost(TB.hostParams);
+    if (TB.hostCounters != nullptr) cudaFreeHost(TB.hostCounters);
+    if (TB.graph != nullptr) cudaGraphExecDestroy(TB.graph);
+    for (cudaEvent_t e : {TB.in, TB.out, TB.start, TB.end})
+        if (e != nullptr) cudaEventDestroy(e);
+    if (TB.stream != nullptr) cudaStreamDestroy(TB.stream);
+    for (DeviceBuffer* b : {&r->filterCameras, &r->filterScratch}) release(*b);
     release_cut_frames(r);
     delete r;
 }
@@ -1007,11 +1016,12 @@ int lrt_radix_sort(lrt_rast* r, void* keys, void* values, uint32_t count, uint32
     return LRT_OK;
 }
 
-int lrt_rast_debug_sort_fault(lrt_rast* r, uint32_t skip_first_partition, uint32_t poll_limit) {
+int lrt_rast_debug_sort(lrt_rast* r, uint32_t skip_first_partition, uint32_t poll_limit, uint32_t wide_look_back) {
     if (r == nullptr) return LRT_INVALID_ARGUMENT;
     r->error.clear();
     r->sortFault.skipFirstPartition = skip_first_partition != 0 ? 1u : 0u;
     r->sortFault.pollLimit = poll_limit;
+    r->sortFault.wideWords = wide_look_back != 0 ? 1u : 0u;
     return LRT_OK;
 }
 
@@ -1376,7 +1386,12 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
         int code = reserve(perChunk);
         if (code != LRT_OK) return code;
         fill(perChunk);
-        const bool haveGraph = B.graph != nullptr && B.graphKey == key && B.graphGeneration == B.generation;
+        // The buffers the batch shares with single frames (which can move
+        // them between batches) are part of what a captured graph bakes in.
+        uint64_t gkey = key;
+        for (const void* q : {r->pairs.ptr, r->pairsAlt.ptr, r->scanScratch.ptr, r->sortScratch.ptr})
+            gkey = mix(gkey, reinterpret_cast<uintptr_t>(q));
+        const bool haveGraph = B.graph != nullptr && B.graphKey == gkey && B.graphGeneration == B.generation;
         if (!haveGraph && !B.graphFailed) {
             // Capture this shape's batch into a graph.
             if (B.graph != nullptr) {
@@ -1393,7 +1408,7 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
             if (graph != nullptr) cudaGraphDestroy(graph);
             cudaGetLastError();
             if (ok) {
-                B.graphKey = key;
+                B.graphKey = gkey;
                 B.graphGeneration = B.generation;
             } else {
                 B.graph = nullptr;
@@ -1402,7 +1417,7 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
             }
         }
         bool over = false;
-        if (B.graph != nullptr && B.graphKey == key && B.graphGeneration == B.generation) {
+        if (B.graph != nullptr && B.graphKey == gkey && B.graphGeneration == B.generation) {
             LRT_CUDA(r, cudaEventRecord(B.start, B.stream), "event");
             LRT_CUDA(r, cudaGraphLaunch(B.graph, B.stream), "graph launch");
             LRT_CUDA(r, cudaEventRecord(B.end, B.stream), "event");

@@ -30,11 +30,21 @@ constexpr uint32_t kSortWarps = kSortThreads / 32;
 constexpr uint32_t kSortItems = 12;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 constexpr uint32_t kDigits = 256;
-// Look-back words are 64 bits: a digit's running count (up to 2^32 - 1 keys)
-// in the low 32 bits, the status in bits 32-33.
-constexpr uint64_t kFlagAggregate = 1ull << 32;
-constexpr uint64_t kFlagInclusive = 2ull << 32;
-constexpr uint64_t kValueMask = 0xFFFFFFFFull;
+// A look-back word holds a digit's running count and, in its top bits, the
+// status (aggregate or inclusive). Sorts of fewer than 2^30 keys use 32-bit
+// words (30 bits of count); larger ones 64-bit words (a 32-bit count, the
+// status in bits 32-33), so no count can spill into the status bits.
+template <typename W>
+struct LookWord;
+template <>
+struct LookWord<uint32_t> {
+    static constexpr uint32_t kAggregate = 1u << 30, kInclusive = 2u << 30, kValue = (1u << 30) - 1;
+};
+template <>
+struct LookWord<unsigned long long> {
+    static constexpr unsigned long long kAggregate = 1ull << 32, kInclusive = 2ull << 32, kValue = 0xFFFFFFFFull;
+};
+constexpr uint32_t kSmallSortMax = (1u << 30) - 1;   // the most keys 32-bit words can count
 constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr uint32_t kMaxPasses = 8;
 constexpr uint32_t kHistThreads = 512;
@@ -88,11 +98,11 @@ histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount
         if (sHist[i] != 0) atomicAdd(&hist[i], sHist[i]);
 }
 
-template <typename K, bool kValues>
+template <typename K, bool kValues, typename W>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
 onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
-                const uint32_t* __restrict__ hist, unsigned long long* __restrict__ lookback,
+                const uint32_t* __restrict__ hist, W* __restrict__ lookback,
                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift, uint32_t spinLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
     K* sKeys = reinterpret_cast<K*>(smem);
@@ -167,12 +177,14 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
         sWarpHist[w][tid] = count;
         count += c;
     }
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(
-        lookback[static_cast<size_t>(part) * kDigits + tid]);
+    constexpr W kFlagAggregate = LookWord<W>::kAggregate;
+    constexpr W kFlagInclusive = LookWord<W>::kInclusive;
+    constexpr W kValueMask = LookWord<W>::kValue;
+    cuda::atomic_ref<W, cuda::thread_scope_device> mine(lookback[static_cast<size_t>(part) * kDigits + tid]);
     if (part == 0) {
-        mine.store(kFlagInclusive | count, cuda::memory_order_relaxed);
+        mine.store(kFlagInclusive | static_cast<W>(count), cuda::memory_order_relaxed);
     } else {
-        mine.store(kFlagAggregate | count, cuda::memory_order_relaxed);
+        mine.store(kFlagAggregate | static_cast<W>(count), cuda::memory_order_relaxed);
     }
     const uint32_t blockStart = block_exclusive_scan_256(count, sScan);
     const uint32_t globalStart = block_exclusive_scan_256(hist[tid], sScan);
@@ -186,12 +198,12 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
         int64_t p = static_cast<int64_t>(part) - 1;
         uint32_t spins = 0;
         while (p >= 0) {
-            unsigned long long words[kLookWords];
+            W words[kLookWords];
 #pragma unroll
             for (uint32_t q = 0; q < kLookWords; ++q) {
                 words[q] = kFlagInclusive;   // before partition 0: an inclusive zero
                 if (p - static_cast<int64_t>(q) >= 0) {
-                    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> s(
+                    cuda::atomic_ref<W, cuda::thread_scope_device> s(
                         lookback[static_cast<size_t>(p - static_cast<int64_t>(q)) * kDigits + tid]);
                     words[q] = s.load(cuda::memory_order_relaxed);
                 }
@@ -215,7 +227,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
                 __nanosleep(20);
             }
         }
-        mine.store(kFlagInclusive | (prefix + count), cuda::memory_order_relaxed);
+        mine.store(kFlagInclusive | static_cast<W>(prefix + count), cuda::memory_order_relaxed);
     }
     sGlobal[tid] = globalStart + prefix - blockStart;
     __syncthreads();
@@ -242,7 +254,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     }
 }
 
-template <typename K, bool kValues>
+template <typename K, bool kValues, typename W>
 cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                       uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
                       bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
@@ -253,7 +265,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     char* s = static_cast<char*>(scratch);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(s);                     // kMaxPasses
     uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
-    unsigned long long* lookback = reinterpret_cast<unsigned long long*>(s + 64 + kMaxPasses * kDigits * 4);
+    W* lookback = reinterpret_cast<W*>(s + 64 + kMaxPasses * kDigits * 4);
     const size_t bytes = sort_scratch_bytes(cap, bits);
     cudaError_t e = cudaMemsetAsync(scratch, 0, bytes, stream);
     if (e != cudaSuccess) return e;
@@ -270,7 +282,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t smem = sizeof(K) * kSortTile + (kValues ? sizeof(uint32_t) * kSortTile : 0);
-    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     K* src = keys;
@@ -278,7 +290,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* vsrc = vals;
     uint32_t* vdst = valsAlt;
     for (uint32_t p = 0; p < passes; ++p) {
-        onesweep_kernel<K, kValues><<<parts, kSortThreads, smem, stream>>>(
+        onesweep_kernel<K, kValues, W><<<parts, kSortThreads, smem, stream>>>(
             src, dst, vsrc, vdst, dCount, cap, hist + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
             tickets + p, err, firstBit + 8 * p, spinLimit);
         e = cudaGetLastError();
@@ -295,7 +307,20 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits) {
     const size_t passes = (bits + 7) / 8;
     const size_t parts = (static_cast<size_t>(cap) + kSortTile - 1) / kSortTile;
-    return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * 8;
+    const size_t word = 8;   // room for either word size (the 64-bit form can be asked for at any size)
+    return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * word;
+}
+
+template <typename K, bool kValues>
+cudaError_t sort_dispatch(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
+                          uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
+                          bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
+    const bool wide = cap > kSmallSortMax || (fault != nullptr && fault->wideWords != 0);
+    if (!wide)
+        return sort_impl<K, kValues, uint32_t>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch,
+                                               err, resultInAlt, stream, fault);
+    return sort_impl<K, kValues, unsigned long long>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
+                                                     scratch, err, resultInAlt, stream, fault);
 }
 
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
@@ -304,9 +329,9 @@ cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, u
                             const SortFault* fault) {
     if (bits > 64 || firstBit + bits > 64 || (bits + 7) / 8 > kMaxPasses) return cudaErrorInvalidValue;
     if (vals != nullptr)
-        return sort_impl<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
+        return sort_dispatch<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
                                          resultInAlt, stream, fault);
-    return sort_impl<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
+    return sort_dispatch<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
                                       resultInAlt, stream, fault);
 }
 
@@ -316,9 +341,9 @@ cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, u
                             const SortFault* fault) {
     if (bits > 32 || firstBit + bits > 32) return cudaErrorInvalidValue;
     if (vals != nullptr)
-        return sort_impl<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
+        return sort_dispatch<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
                                          resultInAlt, stream, fault);
-    return sort_impl<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
+    return sort_dispatch<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
                                       resultInAlt, stream, fault);
 }
 

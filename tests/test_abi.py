@@ -139,3 +139,114 @@ def test_device_entry_points_fail_cleanly_without_a_device():
     h = C.c_void_p()
     assert _abi.load().lrt_rast_create(C.byref(h), 0) == _abi.DEVICE_FAILURE
     assert not h.value
+
+
+@pytest.mark.gpu
+def test_cpp_host_renders_a_frame_through_the_header(tmp_path):
+    """A C++ host does what the reference-side binding does: packs raw
+    records with lrt_pack_splats, copies them into cudaMalloc'd buffers,
+    renders one frame with lrt_rast_render into cudaMalloc'd targets and reads
+    it back. Its image equals the Python path's bit for bit."""
+    import numpy as np
+    import torch
+    import lucabrtrender_b200 as L
+
+    raw = L.synthetic_records(30_000, 12)
+    raw_path = tmp_path / "raw.f32"
+    raw.astype(np.float32).tofile(raw_path)
+    W, H = 320, 240
+    src = tmp_path / "render_host.cpp"
+    src.write_text(r"""
+#include "lrt_raster.h"
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+int main(int argc, char** argv) {
+    const uint32_t W = 320, H = 240, fpr = 59;
+    FILE* f = std::fopen(argv[1], "rb");
+    std::vector<float> raw;
+    float v;
+    while (std::fread(&v, 4, 1, f) == 1) raw.push_back(v);
+    std::fclose(f);
+    const uint32_t count = static_cast<uint32_t>(raw.size() / fpr);
+    const uint32_t words = (15 * 3 + 1) / 2;
+    std::vector<float> pos(size_t{count} * 4);
+    std::vector<uint32_t> shape(size_t{count} * 4), sh(size_t{count} * words);
+    uint32_t kept = 0;
+    if (lrt_pack_splats(raw.data(), count, fpr, 15, 15, pos.data(), shape.data(), sh.data(), &kept) != LRT_OK) return 1;
+    void *dPos, *dShape, *dSh, *dColour, *dDepth;
+    cudaMalloc(&dPos, kept * 16ull);
+    cudaMalloc(&dShape, kept * 16ull);
+    cudaMalloc(&dSh, kept * 4ull * words);
+    cudaMalloc(&dColour, W * H * 16ull);
+    cudaMalloc(&dDepth, W * H * 4ull);
+    cudaMemcpy(dPos, pos.data(), kept * 16ull, cudaMemcpyHostToDevice);
+    cudaMemcpy(dShape, shape.data(), kept * 16ull, cudaMemcpyHostToDevice);
+    cudaMemcpy(dSh, sh.data(), kept * 4ull * words, cudaMemcpyHostToDevice);
+    lrt_gpu_splats cloud{};
+    cloud.count = kept;
+    cloud.rest_per_colour = 15;
+    cloud.sh_words = words;
+    cloud.positions = dPos;
+    cloud.shape = dShape;
+    cloud.sh = dSh;
+    lrt_splat_instance inst{};
+    inst.splats = &cloud;
+    for (int k = 0; k < 4; ++k) inst.object_to_world[5 * k] = 1.0;
+    lrt_camera cam;
+    const double eye[3] = {1.0, 0.5, 4.0}, target[3] = {0, 0, 0}, up[3] = {0, 1, 0};
+    if (lrt_camera_looking_at(eye, target, up, &cam) != LRT_OK) return 2;
+    const double focalPx = (H / 2.0) / std::tan(60.0 * (3.14159265358979323846 / 180.0) / 2.0);
+    cam.lens.focal = focalPx * cam.lens.haperture / W;
+    cam.lens.near_z = 0.01;
+    lrt_projection proj;
+    if (lrt_projection_for(&cam, W, H, &proj) != LRT_OK) return 3;
+    lrt_render_settings s{};
+    s.width = W;
+    s.height = H;
+    s.antialias = 1;
+    s.max_sh_degree = 3;
+    s.depth_threshold = 0.5f;
+    s.linearise = 1;
+    lrt_targets t{W, H, dColour, dDepth};
+    lrt_frame_stats stats{};
+    lrt_rast* r = nullptr;
+    if (lrt_rast_create(&r, 0) != LRT_OK) return 4;
+    if (lrt_rast_render(r, &proj, &inst, 1, &s, &t, &stats, nullptr) != LRT_OK) {
+        std::fprintf(stderr, "%s\n", lrt_rast_last_error(r));
+        return 5;
+    }
+    std::vector<float> colour(size_t{W} * H * 4);
+    cudaMemcpy(colour.data(), dColour, colour.size() * 4, cudaMemcpyDeviceToHost);
+    FILE* o = std::fopen(argv[2], "wb");
+    std::fwrite(colour.data(), 4, colour.size(), o);
+    std::fclose(o);
+    std::printf("%u %u %u\n", stats.splats, stats.visible, stats.pairs);
+    lrt_rast_destroy(r);
+    for (void* p : {dPos, dShape, dSh, dColour, dDepth}) cudaFree(p);
+    return 0;
+}
+""")
+    exe = tmp_path / "render_host"
+    cuda = "/usr/local/cuda"
+    subprocess.run(["g++", "-std=c++17", "-I", str(ROOT / "include"), "-I", f"{cuda}/include", str(src), "-o",
+                    str(exe), str(_abi.LIBRARY_PATH), f"-Wl,-rpath,{_abi.LIBRARY_PATH.parent}", f"-L{cuda}/lib64",
+                    "-lcudart", f"-Wl,-rpath,{cuda}/lib64"], check=True)
+    out_path = tmp_path / "colour.f32"
+    run = subprocess.run([str(exe), str(raw_path), str(out_path)], capture_output=True, text=True)
+    assert run.returncode == 0, run.stderr
+    splats, visible, pairs = map(int, run.stdout.split())
+    host_colour = np.fromfile(out_path, np.float32).reshape(H, W, 4)
+
+    packed = L.pack_splats(raw, 15, 3)
+    cam = L.square_pixel_camera((1.0, 0.5, 4.0), (0.0, 0.0, 0.0), W, H, 60.0, 0.01)
+    r = L.TileRasterizer.create(0)
+    try:
+        t = L.RenderTargets()
+        stats = r.render(cam, [L.SplatInstance(L.to_device(packed))], L.RenderSettings(width=W, height=H), t)
+        assert (stats.splats, stats.visible, stats.pairs) == (splats, visible, pairs)
+        assert pairs > 0
+        assert np.array_equal(t.colour.cpu().numpy().view(np.uint32), host_colour.view(np.uint32))
+    finally:
+        r.close()

@@ -4,8 +4,9 @@ For every view the batch must draw the single-view training forward's image
 and depth bit for bit and take the same L1 loss; its gradients must be the
 single-view gradients summed in view order in float32 (the order the batch
 accumulates them), equal up to the sign of zero. Runs with views of mixed
-sizes, and with more views than one chunk holds, so that the chunked path and
-its boundary are covered.
+sizes, with chunkings fixed by the test hook (several chunks, and chunk
+boundaries inside the views' list), and over repeated steps with new cameras,
+which replay the captured step.
 """
 from __future__ import annotations
 
@@ -14,6 +15,7 @@ import pytest
 import torch
 
 import lucabrtrender_b200 as L
+from lucabrtrender_b200 import _abi
 
 import train_fixtures as TF
 
@@ -71,7 +73,8 @@ def test_the_batch_equals_single_view_steps(raster, count, n, seed):
     views = views_for(count, seed)
     colours, depths, losses, grads, stats = L.train_batch(p["means"], p["log_scales"], p["quats"], p["logits"], p["sh"],
                                                           views, L.RenderSettings(), raster)
-    assert stats.views == count and stats.chunks == (count + 15) // 16
+    assert stats.views == count
+    assert stats.chunks == (count + stats.views_per_chunk - 1) // stats.views_per_chunk
     images, want_losses, want = single_view_steps(raster, p, views)
     for k, ((colour, depth), c, d) in enumerate(zip(images, colours, depths)):
         assert np.array_equal(c.cpu().numpy().view(np.uint32), colour.view(np.uint32)), k
@@ -98,3 +101,51 @@ def test_a_bucket_and_an_fp16_working_copy_give_the_same_batch(raster):
     for k in ga:
         assert gb[k].data_ptr() == bucket.views[k].data_ptr()
         assert torch.equal(ga[k].view(torch.int32), gb[k].view(torch.int32)), k
+
+
+def _check_equal(raster, p, views, out):
+    colours, depths, losses, grads, _ = out
+    images, want_losses, want = single_view_steps(raster, p, views)
+    for k, ((colour, depth), c, d) in enumerate(zip(images, colours, depths)):
+        assert np.array_equal(c.cpu().numpy().view(np.uint32), colour.view(np.uint32)), k
+        assert np.array_equal(d.cpu().numpy().view(np.uint32), depth.view(np.uint32)), k
+    assert losses.cpu().numpy().tolist() == pytest.approx(want_losses, rel=0, abs=0)
+    for name in NAMES:
+        assert np.array_equal(grads[GRAD_KEYS[name]].cpu().numpy(), want[name]), name
+
+
+@pytest.mark.parametrize("chunk,blocks", [(4, 2), (7, 8), (16, 4)])
+def test_fixed_chunkings_equal_single_view_steps(chunk, blocks):
+    r = L.TileRasterizer.create(0)
+    lib = _abi.load()
+    try:
+        assert lib.lrt_rast_debug_train_chunking(r._handle, chunk, blocks) == _abi.OK
+        p = params_of(9000, 40 + chunk)
+        views = views_for(19, 40 + chunk)
+        out = L.train_batch(p["means"], p["log_scales"], p["quats"], p["logits"], p["sh"], views,
+                            L.RenderSettings(), r)
+        stats = out[4]
+        assert stats.views_per_chunk == chunk and stats.blend_blocks_per_sm == blocks
+        assert stats.chunks == (19 + chunk - 1) // chunk
+        _check_equal(r, p, views, out)
+    finally:
+        r.close()
+
+
+def test_repeated_steps_replay_the_captured_step_with_new_cameras():
+    r = L.TileRasterizer.create(0)
+    try:
+        p = params_of(15000, 50)
+        outs = []
+        for step in range(4):   # tune, capture, replay, replay
+            views = views_for(6, 60 + step)
+            # the same view sizes every step: one shape
+            out = L.train_batch(p["means"], p["log_scales"], p["quats"], p["logits"], p["sh"], views,
+                                L.RenderSettings(), r)
+            outs.append((views, out))
+        replays = [o[4].graph_replayed for _, o in outs]
+        assert replays[0] == 0 and replays[-1] == 1, replays
+        for views, out in outs[2:]:
+            _check_equal(r, p, views, out)
+    finally:
+        r.close()
