@@ -401,6 +401,56 @@ def run_lod(L, torch, stream, raster, cloud, settings, peak) -> dict:
                             "select_ms includes its one count read back"}
 
 
+def sort_bytes(slots: float, pairs: float, tiles: int) -> dict:
+    """Algorithmic bytes of a frame's two sorts: the depth sort of one 8-byte
+    word per slot on 24 key bits, and the stable sort of one 8-byte word per
+    pair on the tile bits; per 8-bit pass 8 B read + 8 B written per word, plus
+    one 8 B read per word for the histograms."""
+    tile_bits = max(1, math.ceil(math.log2(tiles)))
+    depth_passes, tile_passes = 3, math.ceil(tile_bits / 8)
+    return {"depth": (16 * depth_passes + 8) * slots, "tile": (16 * tile_passes + 8) * pairs,
+            "depth_passes": depth_passes, "tile_passes": tile_passes}
+
+
+def run_standin(L, torch, dev, raster, cloud, frames: int) -> dict:
+    """The same orbit frames through the stand-in for the reference's GPU
+    path (baseline/standin: the reference's stage sequence and launch shapes
+    in CUDA -- one thread per chunk in its scans and radix sorts, a blocking
+    count readback, a per-pixel blend reading a 48-byte record per pair from
+    global memory), device-timed per frame after two warm-up frames, with the
+    last image checked equal to the product's."""
+    sys.path.insert(0, str(ROOT / "baseline" / "standin"))
+    import standin as S
+    s = S.Standin(dev.index or 0)
+    try:
+        settings = L.RenderSettings(width=WIDTH, height=HEIGHT)
+        theirs = L.RenderTargets(WIDTH, HEIGHT, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        times, stages = [], []
+        for k in range(frames + 2):
+            pr = L.projection_for(orbit_camera(L, k), WIDTH, HEIGHT)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            st = s.render(pr.struct(), cloud.struct(), settings.struct(), theirs.struct(), stream.cuda_stream)
+            b.record(stream)
+            b.synchronize()
+            if k >= 2:
+                times.append(a.elapsed_time(b))
+                stages.append(st)
+        ours = L.RenderTargets(WIDTH, HEIGHT, device=dev)
+        raster.render(pr, [L.SplatInstance(cloud)], settings, ours, stream)
+        torch.cuda.synchronize(dev)
+        equal = torch.equal(ours.colour, theirs.colour) and torch.equal(ours.depth, theirs.depth)
+        return {"label": "stand-in for the reference's Slang kernels on this GPU (they cannot run here): "
+                         "its stage sequence and launch shapes in CUDA, the same arithmetic",
+                "frames": frames, "ms_per_view": round(float(np.mean(times)), 4),
+                "stages_ms": {k: round(float(np.mean([x[k] for x in stages])), 4) for k in S.STAGES},
+                "images_equal_to_product": bool(equal)}
+    finally:
+        s.close()
+
+
 HEAVY_SPLATS = 6_000_000
 HEAVY_WIDTH, HEAVY_HEIGHT = 3840, 2160
 HEAVY_SEED = 7
@@ -440,19 +490,18 @@ def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int, splats: int 
     clocks.window(w0, time.time())
     pairs = float(np.mean([x.pairs for x in st]))
     tiles = ((HEAVY_WIDTH + 15) // 16) * ((HEAVY_HEIGHT + 15) // 16)
-    key_bits = 24 + max(1, math.ceil(math.log2(tiles)))
-    passes = math.ceil(key_bits / 8)
-    sort_ms = float(np.mean([x.tile_sort_ms for x in st]))
-    sort_bytes = (passes * 16 + 8) * pairs
-    gbs = sort_bytes / (sort_ms * 1e-3) / 1e9
+    sb = sort_bytes(splats, pairs, tiles)
+    sort_ms = float(np.mean([x.depth_sort_ms + x.tile_sort_ms for x in st]))
+    gbs = (sb["depth"] + sb["tile"]) / (sort_ms * 1e-3) / 1e9
     out = {"workload": f"{splats / 1e6:g}M splats, means N(0,2), log-scales N(-3.5,0.7), 3840x2160, 16x16 tiles, "
                        "eye (0, 0, 4)",
            "steps": steps, "ms_per_frame": round(float(np.mean(frame_ms)), 4),
            "stages_ms": {k: round(float(np.mean([getattr(x, k) for x in st])), 4)
-                         for k in ("project_ms", "tile_sort_ms", "blend_ms")},
+                         for k in ("project_ms", "depth_sort_ms", "emit_ms", "tile_sort_ms", "blend_ms")},
            "pairs": int(pairs), "visible": int(np.mean([x.visible for x in st])),
-           "key_bits": key_bits, "passes": passes,
-           "sort_bytes": "per pass 8 B read + 8 B written per pair, plus one 8 B/pair histogram read; "
+           "sort_passes": {"depth": sb["depth_passes"], "tile": sb["tile_passes"]},
+           "sort_bytes": "depth sort: 8 B words per slot, tile sort: 8 B words per pair; per 8-bit pass 8 B read "
+                         "+ 8 B written per word, plus one 8 B read per word for the histograms; "
                          "tile_sort_ms also holds the ranges pass",
            "sort_gbs": round(gbs, 1), "sort_frac_of_hbm": round(gbs / peak, 4)}
     del cloud, inst, targets
@@ -655,7 +704,8 @@ def run_ours(args) -> None:
         fb_value = fb_total / (args.steps * world)
         fwd_bwd = {"ms_per_view": round(fb_value, 4), "ratio_to_plain_forward": round(fb_value / value, 3),
                    "forward_stages_ms": {k: round(float(np.mean([getattr(x, k) for x in fwd_stats])), 4)
-                                         for k in ("project_ms", "tile_sort_ms", "blend_ms")},
+                                         for k in ("project_ms", "depth_sort_ms", "emit_ms", "tile_sort_ms",
+                                                   "blend_ms")},
                    "backward_blend_ms": round(float(np.mean(bwd_blend)), 4),
                    "backward_reduce_and_projection_ms": round(float(np.mean(bwd_proj)), 4),
                    "loss": "L1 vs a seeded uniform [0,1]^3 target, mean over pixels and channels "
@@ -669,6 +719,11 @@ def run_ours(args) -> None:
     next_rows = None
     if not args.no_next:
         next_rows = run_next_rows(L, torch, dev, raster, packed, cloud, measured_peaks()[0])
+
+    # --- the stand-in for the reference's GPU path, same orbit ---
+    standin = None
+    if not args.no_standin:
+        standin = run_standin(L, torch, dev, raster, cloud, 5)
 
     # --- the sort-heavy frame ---
     heavy = None
@@ -684,32 +739,39 @@ def run_ours(args) -> None:
     # --- roofline of the dominant kernel, measured live over the timed steps ---
     st = stats_list
     mean = lambda f: float(np.mean([getattr(s, f) for s in st]))  # noqa: E731
-    stage = {k: mean(k) for k in ("project_ms", "counts_ms", "emit_ms", "tile_sort_ms", "blend_ms")}
+    stage = {k: mean(k) for k in ("project_ms", "depth_sort_ms", "emit_ms", "tile_sort_ms", "blend_ms")}
     pairs = float(np.mean([s.pairs for s in st]))
     visible = float(np.mean([s.visible for s in st]))
     tiles = ((WIDTH + 15) // 16) * ((HEIGHT + 15) // 16)
     pixels = WIDTH * HEIGHT
-    key_bits = 24 + max(1, math.ceil(math.log2(tiles)))
-    passes = math.ceil(key_bits / 8)
+    sort = sort_bytes(SPLATS, pairs, tiles)
     # Algorithmic bytes per launch (per unit x units):
     #   blend:   ranges 8 B/tile + (8 B pair word + 48 B record) per pair + 20 B per pixel written
-    #   sort:    per 8-bit pass 8 B read + 8 B written per pair, plus one 8 B/pair histogram read
-    #   project (fused with counts and emission): 124 B per splat read (deg 3),
-    #            48+16+4+4 B per slot written, 8 B per pair written
+    #   project: 124 B per splat read (deg 3); 48 + 16 + 4 + 4 B record, rect, count, key
+    #            and 8 + 8 B depth and aux words written per slot
+    #   emit:    per slot its sorted depth word and count read and its offset written (depth-order
+    #            offsets: 8+4+4 B), then its count, rect, aux word and offset read (4+16+8+4 B;
+    #            records of unmasked splats not counted), 8 B per pair written
+    #   sorts:   see sort_bytes
     bytes_blend = 8 * tiles + 56 * pairs + 20 * pixels
-    bytes_sort = (passes * 16 + 8) * pairs
-    bytes_project = 124 * SPLATS + 72 * SPLATS + 8 * pairs
+    bytes_project = 124 * SPLATS + 88 * SPLATS
+    bytes_emit = 48 * SPLATS + 8 * pairs
     peak, peak_kind = measured_peaks()
     kernels = {
         "blend": (stage["blend_ms"], bytes_blend),
-        "pair sort + ranges": (stage["tile_sort_ms"], bytes_sort + 8 * pairs + 8 * tiles),
-        "project + counts + emit": (stage["project_ms"], bytes_project),
+        "tile sort + ranges": (stage["tile_sort_ms"], sort["tile"] + 8 * pairs + 8 * tiles),
+        "depth sort": (stage["depth_sort_ms"], sort["depth"]),
+        "emit": (stage["emit_ms"], bytes_emit),
+        "project + counts": (stage["project_ms"], bytes_project),
     }
     dom_name = max(kernels, key=lambda n: kernels[n][0])
     dom_ms, dom_bytes = kernels[dom_name]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    sort_gbs = bytes_sort / (stage["tile_sort_ms"] * 1e-3) / 1e9 if stage["tile_sort_ms"] > 0 else None
-    launches_per_frame = 1 + 1 + passes + 1 + 1   # project+emit, histogram, digit passes, ranges, blend
+    sort_ms = stage["depth_sort_ms"] + stage["tile_sort_ms"]
+    sort_gbs = (sort["depth"] + sort["tile"]) / (sort_ms * 1e-3) / 1e9 if sort_ms > 0 else None
+    # project, depth histogram + passes, depth-order offsets, pair writes,
+    # tile histogram + passes, ranges, blend
+    launches_per_frame = 1 + 1 + sort["depth_passes"] + 2 + 1 + sort["tile_passes"] + 1 + 1
 
     clocks.stop()
     if rank == 0:
@@ -745,6 +807,7 @@ def run_ours(args) -> None:
             "fwd_bwd": fwd_bwd,
             "batch": batch,
             "sort_heavy": heavy,
+            "standin": standin,
             "next_rows": next_rows,
         }
         print(json.dumps(line), flush=True)
@@ -766,6 +829,7 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-next", action="store_true")
     ap.add_argument("--no-heavy", action="store_true")
+    ap.add_argument("--no-standin", action="store_true")
     ap.add_argument("--heavy-only", action="store_true",
                     help="run only the sort-heavy frame (--steps frames after 2 warm-up frames)")
     ap.add_argument("--heavy-splats", type=int, default=HEAVY_SPLATS)

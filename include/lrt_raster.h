@@ -664,7 +664,8 @@ int lrt_lod_select(lrt_rast* rast, const lrt_projection* projection, const lrt_l
 /* Diagnostic: the library's own exp (fn 0), log (1), sRGB-to-linear (2),
  * cut-off power (3), float-to-half rounding (4, the binary16 bits in the
  * low 16 bits of each output word) and the half-pair packing of x and -x/2
- * (5, x in the low half), evaluated on the device over n floats (device pointers),
+ * (5, x in the low half) and the blend's exp without range checks (6,
+ * defined for -87 <= x <= 88), evaluated on the device over n floats (device pointers),
  * for comparing their bits with a host implementation. No reference
  * counterpart: the reference evaluates these through Slang's library. */
 int lrt_math_eval(int fn, const void* x, void* y, uint32_t n, void* stream);

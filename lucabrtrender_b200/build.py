@@ -4,8 +4,11 @@ Every kernel is compiled for sm_100a only. ``-fmad=false`` keeps each float
 product and sum a separate rounding, in source order, which is what makes the
 kernels' tile tests, depth keys and blend bit-identical to the CPU oracle.
 The files whose results are checked to a tolerance instead (the backward
-passes and the loss, CONTRACTED) are compiled with ``-fmad=true``: the
-compiler may fuse a product into the sum that follows it.
+blend and the loss, CONTRACTED) are compiled with ``-fmad=true``: the
+compiler may fuse a product into the sum that follows it. The per-splat
+backward (train.cu) is not: its single-view and per-chunk kernels inline
+the same chain rule and must give the same bits, and where the compiler
+fuses is decided per kernel after inlining, which made the two differ.
 """
 from __future__ import annotations
 
@@ -26,7 +29,7 @@ SOURCES = ["project.cu", "scan.cu", "sort.cu", "blend.cu", "blend_backward.cu", 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-I", str(ROOT / "include")]
-CONTRACTED = {"blend_backward.cu", "train.cu", "loss.cu"}
+CONTRACTED = {"blend_backward.cu", "loss.cu"}
 
 
 def fmad_flag(name: str) -> str:

@@ -1,12 +1,15 @@
 // Stages (d) tile ranges and (e) the front-to-back blend.
 //
-// Pair word (64 bits, sorted on its key bits only):
-//     tile << (24 + slotBits) | depthKey24 << slotBits | slot
-// A stable sort of the key bits [slotBits, slotBits + 24 + tileBits) over
-// pairs emitted in slot order leaves every tile's pairs in (depth key, slot)
-// order -- the order the reference gets from its depth sort followed by a
-// stable tile sort (shaders/lrt/splat/frame.slang:17-20,
-// modules/render/src/TileRasterizer.cpp:401-457).
+// Pair words (64 bits, sorted on their tile bits, or on tile and depth):
+//   single frames:  tile << 32 | slot (or emit index), emitted in depth order
+//                   and sorted stably on the tile bits -- the reference's
+//                   depth sort followed by a stable tile sort
+//                   (shaders/lrt/splat/frame.slang:17-20,
+//                   modules/render/src/TileRasterizer.cpp:401-457);
+//   batched views:  tile << (24 + slotBits) | depthKey24 << slotBits | slot,
+//                   emitted in slot order and sorted stably on the key bits.
+// Both leave every tile's pairs in (depth key, slot) order. BlendParams
+// carries the slot field's width (slotBits) and the tile field's shift.
 #include "kernels.cuh"
 #include "raster_common.cuh"
 #include "blend_common.cuh"
@@ -16,6 +19,8 @@ namespace {
 
 constexpr uint32_t kBatch = 256;
 constexpr uint32_t kWaitLimit = 1u << 22;
+// Pixels a thread in the splat blends (the composite blend keeps one).
+constexpr uint32_t kBlendPix = 2;
 
 // shaders/lrt/splat/splat_ranges.slang:11-25 (after a zeroing memset,
 // splat_tiles_clear.slang:8-17). Each thread takes kRangeRun consecutive
@@ -100,11 +105,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // shaders/lrt/splat/splat_blend.slang:23-108 (splat-only entry, :110-114).
-// One block per 16x16 tile, one thread per pixel; warp w covers the 8x4
-// pixel block ((w & 1) * 8, (w >> 1) * 4). The tile's pairs are read in
-// batches of 256: each thread copies one record into shared memory with a
-// bulk copy completing on the batch's mbarrier, and batch k+1 is in flight
-// while batch k is blended. Each record gets a conservative bounding box
+// One block per 16x16 tile, kPix pixels a thread (kBlendThreads / kPix
+// threads); warp w covers the 8 x 4kPix pixel block ((w & 1) * 8,
+// (w >> 1) * 4kPix), a lane's pixels 4 rows apart, so the per-record work a
+// warp shares (the walk, the record's loads, the votes) serves kPix pixels a
+// lane. The tile's pairs are read in batches of 256 / kPix, one record a
+// thread, each copied into shared memory by a bulk copy completing on the
+// batch's mbarrier; batch k+1 is in flight while batch k is blended. Each record gets a conservative bounding box
 // (cull_box); a warp skips, as a whole, every record whose box misses the
 // bounding box of its pixels that are still blending. Each pixel runs the
 // reference's loop unchanged over the records it is given, so it stops at
@@ -122,7 +129,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // index where it reaches the layer's depth), not from depth order.
 // Returns true when a bounded wait gave up (kErrTimeout is set): the
 // barriers' phases are then unknown, so a persistent caller must stop.
-template <bool kTrain, bool kComposite = false>
+template <bool kTrain, bool kComposite = false, uint32_t kPix = 1>
 __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile, uint32_t tx, uint32_t ty,
                                            const uint2* __restrict__ ranges,
                                            const unsigned long long* __restrict__ pairs,
@@ -130,27 +137,49 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
                                            const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut,
                                            float* __restrict__ depthOut, float4* __restrict__ pixState,
                                            uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
-                                           ProjRecord (&sRec)[2][kBatch], float4 (&sBox)[kBatch],
-                                           uint64_t (&sBar)[2], uint32_t& phase0, uint32_t& phase1,
-                                           const float4* __restrict__ underColour = nullptr,
+                                           ProjRecord (&sRec)[2][kBatch / kPix],
+                                           float4 (&sBox)[kBatch / kPix], uint64_t (&sBar)[2], uint32_t& phase0,
+                                           uint32_t& phase1, const float4* __restrict__ underColour = nullptr,
                                            const float* __restrict__ underDepth = nullptr,
                                            float* sZMax = nullptr, float* sWarpMax = nullptr) {
+    static_assert(!kComposite || kPix == 1, "the composite walk keeps one pixel a thread");
+    constexpr uint32_t kThreads = kBlendThreads / kPix;
+    constexpr uint32_t kB = kBatch / kPix;   // records a batch: one per thread
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
+    // Warp w covers the 8 x 4kPix block ((w & 1) * 8, (w >> 1) * 4kPix); a
+    // lane's pixel q sits 4q rows below its first.
     const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
-    const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
-    const bool inside = px < bp.width && py < bp.height;
+    const uint32_t py0 = ty * kTile + (warp >> 1) * (4u * kPix) + (lane >> 3);
     const uint2 range = ranges[tile];
     const uint32_t start = range.x, end = range.y;
     const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
-    const size_t pix = static_cast<size_t>(py) * bp.width + px;
-    // Composite state: the under layer's depth here, where the layer stops
-    // this pixel's walk (a pair index), and what ended the walk opaquely.
+    const float pxf = static_cast<float>(px) + 0.5f;
+    bool inside[kPix], done[kPix];
+    float pyf[kPix], r[kPix], g[kPix], b[kPix], T[kPix], depthSum[kPix], depthAt[kPix];
+    uint32_t last[kPix];
+#pragma unroll
+    for (uint32_t q = 0; q < kPix; ++q) {
+        const uint32_t py = py0 + 4u * q;
+        inside[q] = px < bp.width && py < bp.height;
+        done[q] = !inside[q];
+        pyf[q] = static_cast<float>(py) + 0.5f;
+        r[q] = 0.0f;
+        g[q] = 0.0f;
+        b[q] = 0.0f;
+        T[q] = 1.0f;
+        depthSum[q] = 0.0f;
+        depthAt[q] = -1.0f;
+        last[q] = start;
+    }
+    // Composite state (one pixel a thread): the under layer's depth here,
+    // where the layer stops this pixel's walk (a pair index), and what ended
+    // the walk opaquely.
     bool underHit = false;
     float underZ = 0.0f;
     if constexpr (kComposite) {
-        if (underColour != nullptr && inside) {
-            underZ = underDepth[pix];
+        if (underColour != nullptr && inside[0]) {
+            underZ = underDepth[static_cast<size_t>(py0) * bp.width + px];
             underHit = underZ > 0.0f;
         }
     }
@@ -161,43 +190,36 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
     float zCarry = -3.4e38f;   // the largest depth of the tile's earlier batches
 
     auto issue = [&](uint32_t buf, uint32_t at) {
-        const uint32_t cnt = min(kBatch, end - at);
+        const uint32_t cnt = min(kB, end - at);
         if (tid == 0) mbar_arrive_expect_tx(&sBar[buf], cnt * static_cast<uint32_t>(sizeof(ProjRecord)));
-        if (tid < cnt) {
-            uint32_t slot = static_cast<uint32_t>(pairs[at + tid] & slotMask);
+        for (uint32_t k = tid; k < cnt; k += kThreads) {
+            uint32_t slot = static_cast<uint32_t>(pairs[at + k] & slotMask);
             if constexpr (kTrain) {
                 if (emitSlot != nullptr) slot = emitSlot[slot];   // the low field is the emit index
             }
             fence_proxy_async_smem();
-            bulk_copy_record(&sRec[buf][tid], proj + slot, &sBar[buf]);
+            bulk_copy_record(&sRec[buf][k], proj + slot, &sBar[buf]);
         }
     };
 
-    const float pxf = static_cast<float>(px) + 0.5f;
-    const float pyf = static_cast<float>(py) + 0.5f;
-    float r = 0.0f, g = 0.0f, b = 0.0f;
-    float T = 1.0f;
-    float depthSum = 0.0f;
-    float depthAt = -1.0f;
-    bool done = !inside;
     bool gaveUp = false;
-    uint32_t last = start;
     if (start < end) issue(0, start);
     uint32_t k = 0;
-    for (uint32_t at = start; at < end; at += kBatch, ++k) {
+    for (uint32_t at = start; at < end; at += kB, ++k) {
         const uint32_t buf = k & 1u;
-        const bool more = at + kBatch < end;
-        if (more) issue(buf ^ 1u, at + kBatch);
+        const bool more = at + kB < end;
+        if (more) issue(buf ^ 1u, at + kB);
         const uint32_t parity = buf == 0 ? phase0 : phase1;
         if (!mbar_wait(&sBar[buf], parity)) {
             atomicOr(err, kErrTimeout);
-            done = true;
+#pragma unroll
+            for (uint32_t q = 0; q < kPix; ++q) done[q] = true;
             gaveUp = true;
         }
         if (buf == 0) phase0 ^= 1u; else phase1 ^= 1u;
-        const uint32_t cnt = min(kBatch, end - at);
+        const uint32_t cnt = min(kB, end - at);
         const ProjRecord* batch = sRec[buf];
-        if (tid < cnt) sBox[tid] = cull_box(batch[tid]);
+        for (uint32_t m = tid; m < cnt; m += kThreads) sBox[m] = cull_box(batch[m]);
         if constexpr (kComposite) {
             if (underColour != nullptr) {
                 // Running maximum of the depths, tile order, across batches.
@@ -230,15 +252,25 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
         // walks the ballot's set bits in record order.
         for (uint32_t c = 0; c < cnt; c += 32) {
             if constexpr (kComposite) {
-                if (at + c >= stopAt) done = true;
+                if (at + c >= stopAt) done[0] = true;
             }
-            const unsigned active = __ballot_sync(0xFFFFFFFFu, !done);
+            bool live = false;
+            uint32_t yLo = 0xFFFFFFFFu, yHi = 0u;
+#pragma unroll
+            for (uint32_t q = 0; q < kPix; ++q) {
+                if (!done[q]) {
+                    live = true;
+                    yLo = min(yLo, py0 + 4u * q);
+                    yHi = max(yHi, py0 + 4u * q);
+                }
+            }
+            const unsigned active = __ballot_sync(0xFFFFFFFFu, live);
             if (active == 0) break;
             const uint32_t big = 0xFFFFFFFFu;
-            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, done ? big : px);
-            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : px);
-            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, done ? big : py);
-            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, done ? 0u : py);
+            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, live ? px : big);
+            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, live ? px : 0u);
+            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, yLo);
+            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, yHi);
             const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
             const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
             bool overlap = false;
@@ -247,52 +279,67 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
                 overlap = !(box.x > bx1 || box.y < bx0 || box.z > by1 || box.w < by0);
             }
             uint32_t todo = __ballot_sync(0xFFFFFFFFu, overlap);
-            // Straight-line body with one warp-uniform skip: every lane computes
-            // the power, lanes still blending that pass the cut are candidates,
-            // and the rest of the reference's step runs predicated on a hit.
+            // Straight-line body with warp-uniform skips: every lane computes
+            // the power of each of its pixels, pixels still blending that pass
+            // the cut are candidates, and the rest of the reference's step
+            // runs predicated on a hit.
             while (todo != 0) {
                 const uint32_t j = c + static_cast<uint32_t>(__ffs(todo)) - 1u;
                 todo &= todo - 1u;
                 const float4 screen = batch[j].screen;
                 const float4 conic = batch[j].conic;
                 const float dx = pxf - screen.x;
-                const float dy = pyf - screen.y;
-                const float power = splat_power(conic, dx, dy);
-                const bool candidate = !done && !(power > screen.w) && (!kComposite || at + j < stopAt);
-                if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
-                bool blendIt = candidate;
-                if constexpr (kComposite) {
-                    if (candidate) {
-                        const float4 col = batch[j].colour;
-                        if (col.w > 0.5f) {   // a disc: opaque, the walk ends here
-                            opaqueHit = true;
-                            opaque = make_float4(col.x, col.y, col.z, 1.0f);
-                            opaqueZ = screen.z;
-                            done = true;
-                            blendIt = false;
+                float power[kPix];
+                bool candidate[kPix];
+                bool anyCandidate = false;
+#pragma unroll
+                for (uint32_t q = 0; q < kPix; ++q) {
+                    const float dy = pyf[q] - screen.y;
+                    power[q] = splat_power(conic, dx, dy);
+                    candidate[q] = !done[q] && !(power[q] > screen.w) && (!kComposite || at + j < stopAt);
+                    anyCandidate = anyCandidate || candidate[q];
+                }
+                if (!__any_sync(0xFFFFFFFFu, anyCandidate)) continue;
+#pragma unroll
+                for (uint32_t q = 0; q < kPix; ++q) {
+                    if (kPix > 1 && !__any_sync(0xFFFFFFFFu, candidate[q])) continue;
+                    bool blendIt = candidate[q];
+                    if constexpr (kComposite) {
+                        if (candidate[q]) {
+                            const float4 col = batch[j].colour;
+                            if (col.w > 0.5f) {   // a disc: opaque, the walk ends here
+                                opaqueHit = true;
+                                opaque = make_float4(col.x, col.y, col.z, 1.0f);
+                                opaqueZ = screen.z;
+                                done[q] = true;
+                                blendIt = false;
+                            }
                         }
                     }
-                }
-                // A candidate's power lies in [0, 9] (the cut is at most 9), so
-                // the exponent's argument is in range; others discard it.
-                const float alpha = fminf(0.99f, conic.w * lrt_exp_in_range(-0.5f * power));
-                if (blendIt && !(alpha < 1.0f / 255.0f)) {
-                    const float4 colour = batch[j].colour;
-                    const float weight = T * alpha;
-                    // rgb += weight colour, depthSum += weight z
-                    // (splat_blend.slang:72-74), each one multiply-add.
-                    r = __fmaf_rn(weight, colour.x, r);
-                    g = __fmaf_rn(weight, colour.y, g);
-                    b = __fmaf_rn(weight, colour.z, b);
-                    depthSum = __fmaf_rn(weight, screen.z, depthSum);
-                    T = T * (1.0f - alpha);
-                    if (depthAt < 0.0f && 1.0f - T >= bp.depthThreshold) depthAt = screen.z;
-                    if (kTrain) last = at + j + 1;
-                    if (T < 1e-4f) done = true;
+                    // A candidate's power lies in [0, 9] (the cut is at most 9), so
+                    // the exponent's argument is in range; others discard it.
+                    const float alpha = fminf(0.99f, conic.w * lrt_exp_in_range(-0.5f * power[q]));
+                    if (blendIt && !(alpha < 1.0f / 255.0f)) {
+                        const float4 colour = batch[j].colour;
+                        const float weight = T[q] * alpha;
+                        // rgb += weight colour, depthSum += weight z
+                        // (splat_blend.slang:72-74), each one multiply-add.
+                        r[q] = __fmaf_rn(weight, colour.x, r[q]);
+                        g[q] = __fmaf_rn(weight, colour.y, g[q]);
+                        b[q] = __fmaf_rn(weight, colour.z, b[q]);
+                        depthSum[q] = __fmaf_rn(weight, screen.z, depthSum[q]);
+                        T[q] = T[q] * (1.0f - alpha);
+                        if (depthAt[q] < 0.0f && 1.0f - T[q] >= bp.depthThreshold) depthAt[q] = screen.z;
+                        if (kTrain) last[q] = at + j + 1;
+                        if (T[q] < 1e-4f) done[q] = true;
+                    }
                 }
             }
         }
-        if (__syncthreads_and(done ? 1 : 0)) {
+        bool allDone = true;
+#pragma unroll
+        for (uint32_t q = 0; q < kPix; ++q) allDone = allDone && done[q];
+        if (__syncthreads_and(allDone ? 1 : 0)) {
             if (more) {
                 // Drain the batch already in flight, and count its phase: a
                 // persistent block blends its next tile with the same barriers.
@@ -306,46 +353,52 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
             break;
         }
     }
-    if (!inside) return gaveUp;
-    if constexpr (kComposite) {
-        if (!opaqueHit && underHit) {
-            opaqueHit = true;
-            opaque = underColour[pix];
-            opaqueZ = underZ;
+#pragma unroll
+    for (uint32_t q = 0; q < kPix; ++q) {
+        if (!inside[q]) continue;
+        const size_t pix = static_cast<size_t>(py0 + 4u * q) * bp.width + px;
+        if constexpr (kComposite) {
+            if (!opaqueHit && underHit) {
+                opaqueHit = true;
+                opaque = underColour[pix];
+                opaqueZ = underZ;
+            }
         }
-    }
-    const float coverage = 1.0f - T;
-    float lr = r, lg = g, lb = b;
-    if (bp.linearise != 0 && coverage > 1e-6f) {
-        lr = srgb_to_linear(r / coverage) * coverage;
-        lg = srgb_to_linear(g / coverage) * coverage;
-        lb = srgb_to_linear(b / coverage) * coverage;
-    }
-    float4 behind = make_float4(bp.bg[0], bp.bg[1], bp.bg[2], bp.bg[3]);
-    if (opaqueHit) {
-        behind = opaque;
-        depthSum = depthSum + T * opaqueZ;
-        if (depthAt < 0.0f) depthAt = opaqueZ;
-    }
-    const float total = opaqueHit ? 1.0f : coverage;
-    colourOut[pix] = make_float4(lr + T * behind.x, lg + T * behind.y, lb + T * behind.z, coverage + T * behind.w);
-    depthOut[pix] = bp.depthMode == 0 ? (total > 1e-6f ? depthSum / total : 0.0f) : fmaxf(depthAt, 0.0f);
-    if (kTrain) {
-        pixState[pix] = make_float4(r, g, b, T);
-        pixLast[pix] = last;
+        const float coverage = 1.0f - T[q];
+        float lr = r[q], lg = g[q], lb = b[q];
+        if (bp.linearise != 0 && coverage > 1e-6f) {
+            lr = srgb_to_linear(r[q] / coverage) * coverage;
+            lg = srgb_to_linear(g[q] / coverage) * coverage;
+            lb = srgb_to_linear(b[q] / coverage) * coverage;
+        }
+        float4 behind = make_float4(bp.bg[0], bp.bg[1], bp.bg[2], bp.bg[3]);
+        float dSum = depthSum[q], dAt = depthAt[q];
+        if (opaqueHit) {
+            behind = opaque;
+            dSum = dSum + T[q] * opaqueZ;
+            if (dAt < 0.0f) dAt = opaqueZ;
+        }
+        const float total = opaqueHit ? 1.0f : coverage;
+        colourOut[pix] = make_float4(lr + T[q] * behind.x, lg + T[q] * behind.y, lb + T[q] * behind.z,
+                                     coverage + T[q] * behind.w);
+        depthOut[pix] = bp.depthMode == 0 ? (total > 1e-6f ? dSum / total : 0.0f) : fmaxf(dAt, 0.0f);
+        if (kTrain) {
+            pixState[pix] = make_float4(r[q], g[q], b[q], T[q]);
+            pixLast[pix] = last[q];
+        }
     }
     return gaveUp;
 }
 
 
 template <bool kTrain>
-__global__ void __launch_bounds__(kBlendThreads)
+__global__ void __launch_bounds__(kBlendThreads / kBlendPix)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
              const uint32_t* __restrict__ emitSlot,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
              float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
-    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
-    __shared__ __align__(16) float4 sBox[kBatch];
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch / kBlendPix];
+    __shared__ __align__(16) float4 sBox[kBatch / kBlendPix];
     __shared__ __align__(8) uint64_t sBar[2];
     if (threadIdx.x == 0) {
         mbar_init(&sBar[0], 1);
@@ -355,8 +408,8 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
     const uint32_t tile = blockIdx.x;
-    blend_tile<kTrain>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emitSlot, proj, colourOut, depthOut,
-                       pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
+    blend_tile<kTrain, false, kBlendPix>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emitSlot, proj,
+                                         colourOut, depthOut, pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
 }
 
 // splatBlendComposite (splat_blend.slang:116-120): discs and an optional
@@ -389,13 +442,13 @@ blend_composite_kernel(BlendParams bp, const uint2* __restrict__ ranges, const u
 // another, largest views first -- and blend each as blend_kernel does
 // (kTrain: as blend_kernel<true>, keeping each view's per-pixel state).
 template <bool kTrain>
-__global__ void __launch_bounds__(kBlendThreads)
+__global__ void __launch_bounds__(kBlendThreads / kBlendPix)
 blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_t viewCount,
                    const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
                    const ProjRecord* __restrict__ proj, uint32_t totalTiles, uint32_t* __restrict__ queue,
                    uint32_t* __restrict__ err) {
-    __shared__ __align__(128) ProjRecord sRec[2][kBatch];
-    __shared__ __align__(16) float4 sBox[kBatch];
+    __shared__ __align__(128) ProjRecord sRec[2][kBatch / kBlendPix];
+    __shared__ __align__(16) float4 sBox[kBatch / kBlendPix];
     __shared__ __align__(8) uint64_t sBar[2];
     __shared__ uint32_t sItem;
     if (threadIdx.x == 0) {
@@ -421,10 +474,10 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
         vbp.height = v.height;
         vbp.tilesX = v.tilesX;
         const uint32_t local = item - v.tileBase;
-        const bool gaveUp = blend_tile<kTrain>(vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr,
-                                               proj + v.recordBase, v.colour, v.depth,
-                                               kTrain ? v.pixState : nullptr, kTrain ? v.pixLast : nullptr, err,
-                                               sRec, sBox, sBar, phase0, phase1);
+        const bool gaveUp = blend_tile<kTrain, false, kBlendPix>(
+            vbp, item, local % v.tilesX, local / v.tilesX, ranges, pairs, nullptr, proj + v.recordBase, v.colour,
+            v.depth, kTrain ? v.pixState : nullptr, kTrain ? v.pixLast : nullptr, err, sRec, sBox, sBar, phase0,
+            phase1);
         // After a wait gave up the barriers' phases are unknown: take no more
         // items (the frame reports TIMEOUT and its output is undefined).
         if (__syncthreads_or(gaveUp ? 1 : 0)) return;
@@ -447,7 +500,7 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_kernel<false><<<tiles, kBlendThreads, 0, stream>>>(
+    blend_kernel<false><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), nullptr, proj, colour, depth, nullptr, nullptr,
         err);
     return cudaGetLastError();
@@ -464,11 +517,13 @@ cudaError_t launch_blend_composite(const BlendParams& bp, const uint2* ranges, c
     return cudaGetLastError();
 }
 
+// `blocks` counts blocks of kBlendThreads threads; the grid has kBlendPix
+// times as many blocks of kBlendThreads / kBlendPix threads.
 cudaError_t launch_blend_batch(const BlendParams& bp, const ViewParams* views, uint32_t viewCount, const uint2* ranges,
                                const uint64_t* pairs, const ProjRecord* proj, uint32_t totalTiles, uint32_t* queue,
                                uint32_t* err, uint32_t blocks, cudaStream_t stream) {
     if (totalTiles == 0) return cudaSuccess;
-    blend_batch_kernel<false><<<blocks, kBlendThreads, 0, stream>>>(
+    blend_batch_kernel<false><<<blocks * kBlendPix, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, totalTiles, queue, err);
     return cudaGetLastError();
 }
@@ -478,7 +533,7 @@ cudaError_t launch_blend_batch_train(const BlendParams& bp, const ViewParams* vi
                                      uint32_t totalTiles, uint32_t* queue, uint32_t* err, uint32_t blocks,
                                      cudaStream_t stream) {
     if (totalTiles == 0) return cudaSuccess;
-    blend_batch_kernel<true><<<blocks, kBlendThreads, 0, stream>>>(
+    blend_batch_kernel<true><<<blocks * kBlendPix, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), proj, totalTiles, queue, err);
     return cudaGetLastError();
 }
@@ -488,7 +543,7 @@ cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const
                                float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_kernel<true><<<tiles, kBlendThreads, 0, stream>>>(
+    blend_kernel<true><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
         pixLast, err);
     return cudaGetLastError();

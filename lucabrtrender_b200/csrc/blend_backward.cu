@@ -24,6 +24,7 @@ __device__ __forceinline__ float srgb_to_linear_slope(float c) {
 
 constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
 constexpr uint32_t kGradStride = 12;   // floats per pair in the partials buffer (three 16-byte vectors)
+constexpr uint32_t kBwdPix = 2;        // pixels a thread
 
 // Sum of nine values over the warp by recursive halving (a reduce-scatter):
 // at each step a lane keeps part of its list, sends the rest to its partner
@@ -67,10 +68,13 @@ __device__ __forceinline__ float warp_reduce_scatter9(const float (&v)[9], uint3
 //   dL/dalpha_i = T_i sum_k dL/drgb_k (c_ik - B_k) - dL/dT * T / (1 - alpha_i)
 //   B          <- alpha_i c_i + (1 - alpha_i) B
 // then through alpha = min(0.99, alpha0 exp(-power / 2)) (no gradient when
-// clamped) and power = a dx^2 + 2 b dx dy + c dy^2. A pair's nine values are
-// summed over the warp's pixels by shuffles, over the block's warps in
-// warp order through shared memory, and written at the pair's emit index: a
-// splat's pairs are contiguous there, so a per-splat sum needs no atomics.
+// clamped) and power = a dx^2 + 2 b dx dy + c dy^2. kBwdPix pixels a thread
+// (warp w covers the 8 x 4kBwdPix block ((w & 1) * 8, (w >> 1) * 4kBwdPix), a
+// lane's pixels 4 rows apart): a lane first adds its pixels' nine values, so
+// one warp reduction serves 32 kBwdPix pixels. A pair's values are summed over
+// the warp by shuffles, over the block's warps in warp order through shared
+// memory, and written at the pair's emit index: a splat's pairs are
+// contiguous there, so a per-splat sum needs no atomics.
 // One tile: `item` indexes the ranges (the frame's tile, or a batch's
 // (view, tile) item); (tx, ty) is the tile within its view.
 __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint32_t item, uint32_t tx, uint32_t ty,
@@ -83,95 +87,127 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
                                                     const uint32_t* __restrict__ pixLast,
                                                     const float4* __restrict__ gradColour,
                                                     float* __restrict__ partials) {
-    constexpr uint32_t kB = 128;
+    constexpr uint32_t kP = kBwdPix;
+    constexpr uint32_t kThreads = kBlendThreads / kP;
+    constexpr uint32_t kWarps = kThreads / 32;
+    constexpr uint32_t kB = 128;   // records a batch
     __shared__ __align__(16) ProjRecord sRec[kB];
     __shared__ __align__(16) float4 sBox[kB];
     __shared__ uint32_t sEmit[kB];
-    __shared__ float sPart[kBlendThreads / 32][kB][kGrads];
-    __shared__ uint32_t sHit[kBlendThreads / 32][kB / 32];   // which sPart slots a warp wrote this batch
+    __shared__ float sPart[kWarps][kB][kGrads];
+    __shared__ uint32_t sHit[kWarps][kB / 32];   // which sPart slots a warp wrote this batch
     __shared__ uint32_t sMaxLast;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
     const uint32_t px = tx * kTile + (warp & 1u) * 8u + (lane & 7u);
-    const uint32_t py = ty * kTile + (warp >> 1) * 4u + (lane >> 3);
-    const bool inside = px < bp.width && py < bp.height;
+    const uint32_t py0 = ty * kTile + (warp >> 1) * (4u * kP) + (lane >> 3);
     const uint2 range = ranges[item];
     const uint32_t start = range.x;
     const unsigned long long slotMask = (1ull << bp.slotBits) - 1ull;
-    const size_t pix = static_cast<size_t>(py) * bp.width + px;
+    const float pxf = static_cast<float>(px) + 0.5f;
 
-    uint32_t myLast = start;
-    float gr = 0.0f, gg = 0.0f, gb = 0.0f, gT = 0.0f, T = 1.0f;
-    if (inside) {
-        myLast = pixLast[pix];
-        const float4 st = pixState[pix];
-        const float4 G = gradColour[pix];
-        T = st.w;
-        const float cov = 1.0f - T;
-        if (bp.linearise != 0 && cov > 1e-6f) {
-            const float u0 = st.x / cov, u1 = st.y / cov, u2 = st.z / cov;
-            const float d0 = srgb_to_linear_slope(u0), d1 = srgb_to_linear_slope(u1), d2 = srgb_to_linear_slope(u2);
-            gr = G.x * d0;
-            gg = G.y * d1;
-            gb = G.z * d2;
-            // out_k = s(u_k) cov + T bg_k with cov = 1 - T; alpha_out = cov + T bg_a
-            gT = G.x * (bp.bg[0] - (srgb_to_linear(u0) - d0 * u0)) + G.y * (bp.bg[1] - (srgb_to_linear(u1) - d1 * u1)) +
-                 G.z * (bp.bg[2] - (srgb_to_linear(u2) - d2 * u2)) + G.w * (bp.bg[3] - 1.0f);
-        } else {
-            gr = G.x;
-            gg = G.y;
-            gb = G.z;
-            gT = G.x * bp.bg[0] + G.y * bp.bg[1] + G.z * bp.bg[2] + G.w * (bp.bg[3] - 1.0f);
+    uint32_t myLast[kP];
+    float pyf[kP], gr[kP], gg[kP], gb[kP], T[kP], gTT[kP], Br[kP], Bg[kP], Bb[kP];
+    bool live[kP];
+    uint32_t laneMax = start;
+#pragma unroll
+    for (uint32_t q = 0; q < kP; ++q) {
+        const uint32_t py = py0 + 4u * q;
+        const bool inside = px < bp.width && py < bp.height;
+        pyf[q] = static_cast<float>(py) + 0.5f;
+        myLast[q] = start;
+        gr[q] = 0.0f;
+        gg[q] = 0.0f;
+        gb[q] = 0.0f;
+        T[q] = 1.0f;
+        float gT = 0.0f;
+        if (inside) {
+            const size_t pix = static_cast<size_t>(py) * bp.width + px;
+            myLast[q] = pixLast[pix];
+            const float4 st = pixState[pix];
+            const float4 G = gradColour[pix];
+            T[q] = st.w;
+            const float cov = 1.0f - T[q];
+            if (bp.linearise != 0 && cov > 1e-6f) {
+                const float u0 = st.x / cov, u1 = st.y / cov, u2 = st.z / cov;
+                const float d0 = srgb_to_linear_slope(u0), d1 = srgb_to_linear_slope(u1), d2 = srgb_to_linear_slope(u2);
+                gr[q] = G.x * d0;
+                gg[q] = G.y * d1;
+                gb[q] = G.z * d2;
+                // out_k = s(u_k) cov + T bg_k with cov = 1 - T; alpha_out = cov + T bg_a
+                gT = G.x * (bp.bg[0] - (srgb_to_linear(u0) - d0 * u0)) +
+                     G.y * (bp.bg[1] - (srgb_to_linear(u1) - d1 * u1)) +
+                     G.z * (bp.bg[2] - (srgb_to_linear(u2) - d2 * u2)) + G.w * (bp.bg[3] - 1.0f);
+            } else {
+                gr[q] = G.x;
+                gg[q] = G.y;
+                gb[q] = G.z;
+                gT = G.x * bp.bg[0] + G.y * bp.bg[1] + G.z * bp.bg[2] + G.w * (bp.bg[3] - 1.0f);
+            }
         }
+        gTT[q] = -gT * T[q];   // the final transmittance's share of every dL/dalpha
+        Br[q] = 0.0f;
+        Bg[q] = 0.0f;
+        Bb[q] = 0.0f;
+        live[q] = inside && myLast[q] > start;
+        laneMax = max(laneMax, myLast[q]);
     }
-    const float Tfinal = T;
-    const float gTT = -gT * Tfinal;   // the final transmittance's share of every dL/dalpha
     if (tid == 0) sMaxLast = start;
     __syncthreads();
-    if (inside) atomicMax(&sMaxLast, myLast);
+    const uint32_t warpMax = __reduce_max_sync(0xFFFFFFFFu, laneMax);
+    if (lane == 0) atomicMax(&sMaxLast, warpMax);
     __syncthreads();
     const uint32_t maxLast = sMaxLast;
-    bool live = inside && myLast > start;
     // Pairs past every pixel's last contributor get zero partials here, so the
     // buffer needs no clearing beforehand.
-    for (uint32_t k = maxLast + tid; k < range.y; k += kBlendThreads) {
+    for (uint32_t k = maxLast + tid; k < range.y; k += kThreads) {
         const uint32_t e = emitSlot != nullptr ? static_cast<uint32_t>(pairs[k] & slotMask) : emit[k];
         float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(e) * kGradStride);
         out[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         out[1] = out[0];
         out[2] = out[0];
     }
-    float Br = 0.0f, Bg = 0.0f, Bb = 0.0f;
-    const float pxf = static_cast<float>(px) + 0.5f;
-    const float pyf = static_cast<float>(py) + 0.5f;
 
     for (uint32_t bEnd = maxLast; bEnd > start;) {
         const uint32_t bStart = bEnd - start > kB ? bEnd - kB : start;
         const uint32_t cnt = bEnd - bStart;
-        if (tid < cnt) {
-            const uint32_t low = static_cast<uint32_t>(pairs[bStart + tid] & slotMask);
+        for (uint32_t m = tid; m < cnt; m += kThreads) {
+            const uint32_t low = static_cast<uint32_t>(pairs[bStart + m] & slotMask);
             // The emit index is the word's low field (and the slot comes from
             // the emit-slot map), or it travelled through the sort as a value.
             const uint32_t slot = emitSlot != nullptr ? emitSlot[low] : low;
-            sRec[tid] = proj[slot];
-            sEmit[tid] = emitSlot != nullptr ? low : emit[bStart + tid];
+            sRec[m] = proj[slot];
+            sEmit[m] = emitSlot != nullptr ? low : emit[bStart + m];
         }
-        if (tid < (kBlendThreads / 32) * (kB / 32)) (&sHit[0][0])[tid] = 0u;
+        if (tid < kWarps * (kB / 32)) (&sHit[0][0])[tid] = 0u;
         __syncthreads();
-        if (tid < cnt) sBox[tid] = cull_box(sRec[tid]);
+        for (uint32_t m = tid; m < cnt; m += kThreads) sBox[m] = cull_box(sRec[m]);
         __syncthreads();
         // Records from the back of the batch, 32 at a time.
         for (int c = static_cast<int>((cnt - 1) & ~31u); c >= 0; c -= 32) {
-            const unsigned any = __ballot_sync(0xFFFFFFFFu, live);
-            if (any == 0) break;
-            // Lanes whose pixel stopped before this chunk take no part in it.
-            const bool here = live && myLast > bStart + static_cast<uint32_t>(c);
-            if (__ballot_sync(0xFFFFFFFFu, here) == 0) continue;
+            bool anyLive = false;
+#pragma unroll
+            for (uint32_t q = 0; q < kP; ++q) anyLive = anyLive || live[q];
+            if (__ballot_sync(0xFFFFFFFFu, anyLive) == 0) break;
+            // Pixels that stopped before this chunk take no part in it.
+            bool here[kP];
+            bool hereAny = false;
+            uint32_t yLo = 0xFFFFFFFFu, yHi = 0u;
+#pragma unroll
+            for (uint32_t q = 0; q < kP; ++q) {
+                here[q] = live[q] && myLast[q] > bStart + static_cast<uint32_t>(c);
+                if (here[q]) {
+                    hereAny = true;
+                    yLo = min(yLo, py0 + 4u * q);
+                    yHi = max(yHi, py0 + 4u * q);
+                }
+            }
+            if (__ballot_sync(0xFFFFFFFFu, hereAny) == 0) continue;
             const uint32_t big = 0xFFFFFFFFu;
-            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, here ? px : big);
-            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, here ? px : 0u);
-            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, here ? py : big);
-            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, here ? py : 0u);
+            const uint32_t x0 = __reduce_min_sync(0xFFFFFFFFu, hereAny ? px : big);
+            const uint32_t x1 = __reduce_max_sync(0xFFFFFFFFu, hereAny ? px : 0u);
+            const uint32_t y0 = __reduce_min_sync(0xFFFFFFFFu, yLo);
+            const uint32_t y1 = __reduce_max_sync(0xFFFFFFFFu, yHi);
             const float bx0 = static_cast<float>(x0) + 0.5f, bx1 = static_cast<float>(x1) + 0.5f;
             const float by0 = static_cast<float>(y0) + 0.5f, by1 = static_cast<float>(y1) + 0.5f;
             bool overlap = false;
@@ -186,63 +222,76 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
                 const uint32_t bit = 31u - static_cast<uint32_t>(__clz(todo));
                 todo &= ~(1u << bit);
                 const uint32_t j = static_cast<uint32_t>(c) + bit;
-                float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                 const float4 screen = sRec[j].screen;
                 const float4 conic = sRec[j].conic;
                 const float dx = pxf - screen.x;
-                const float dy = pyf - screen.y;
-                const float power = splat_power(conic, dx, dy);
-                const bool candidate = live && bStart + j < myLast && !(power > screen.w);
-                if (!__any_sync(0xFFFFFFFFu, candidate)) continue;
-                // The forward's alpha decides who contributed, so it is taken
-                // from the exact exponential wherever the fast one (relative
-                // error below 1e-6 for these arguments) lies within 1e-5 of
-                // either threshold; elsewhere both sides of a threshold agree
-                // and the fast value serves.
-                float e = __expf(-0.5f * power);
-                float raw = conic.w * e;
-                if (candidate && (fabsf(raw - 1.0f / 255.0f) <= 1e-5f / 255.0f || fabsf(raw - 0.99f) <= 0.99e-5f)) {
-                    e = lrt_exp(-0.5f * power);
-                    raw = conic.w * e;
+                float dy[kP], power[kP];
+                bool candidate[kP];
+                bool anyCandidate = false;
+#pragma unroll
+                for (uint32_t q = 0; q < kP; ++q) {
+                    dy[q] = pyf[q] - screen.y;
+                    power[q] = splat_power(conic, dx, dy[q]);
+                    candidate[q] = live[q] && bStart + j < myLast[q] && !(power[q] > screen.w);
+                    anyCandidate = anyCandidate || candidate[q];
                 }
-                const float alpha = fminf(0.99f, raw);
-                const bool hit = candidate && !(alpha < 1.0f / 255.0f);
-                const unsigned hits = __ballot_sync(0xFFFFFFFFu, hit);
-                if (hits == 0) continue;
-                written |= 1u << bit;
-                if (hit) {
-                    // Gradients are checked against FP64 to a tolerance, not
-                    // bit for bit, so this part uses fused multiply-adds.
-                    const float4 col = sRec[j].colour;
-                    const float oneMinus = 1.0f - alpha;   // in [0.01, 1]
-                    float inv;   // 1 / (1 - alpha) to about 1 ulp
-                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(oneMinus));
-                    const float Ti = T * inv;
-                    const float w = Ti * alpha;
-                    v[6] = gr * w;
-                    v[7] = gg * w;
-                    v[8] = gb * w;
-                    const float behind =
-                        __fmaf_rn(gr, col.x - Br, __fmaf_rn(gg, col.y - Bg, gb * (col.z - Bb)));
-                    const float dAlpha = __fmaf_rn(Ti, behind, gTT * inv);
-                    Br = __fmaf_rn(alpha, col.x - Br, Br);
-                    Bg = __fmaf_rn(alpha, col.y - Bg, Bg);
-                    Bb = __fmaf_rn(alpha, col.z - Bb, Bb);
-                    T = Ti;
-                    if (raw <= 0.99f) {
-                        v[5] = dAlpha * e;
-                        const float dPower = -0.5f * alpha * dAlpha;
-                        const float pdx = dPower * dx, pdy = dPower * dy;
-                        v[2] = pdx * dx;
-                        v[3] = 2.0f * pdx * dy;
-                        v[4] = pdy * dy;
-                        v[0] = -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
-                        v[1] = -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
+                if (!__any_sync(0xFFFFFFFFu, anyCandidate)) continue;
+                float v[kGrads] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                bool hitAny = false;
+#pragma unroll
+                for (uint32_t q = 0; q < kP; ++q) {
+                    // The forward's alpha decides who contributed, so it is
+                    // taken from the exact exponential wherever the fast one
+                    // (relative error below 1e-6 for these arguments) lies
+                    // within 1e-5 of either threshold; elsewhere both sides of
+                    // a threshold agree and the fast value serves.
+                    float e = __expf(-0.5f * power[q]);
+                    float raw = conic.w * e;
+                    if (candidate[q] &&
+                        (fabsf(raw - 1.0f / 255.0f) <= 1e-5f / 255.0f || fabsf(raw - 0.99f) <= 0.99e-5f)) {
+                        e = lrt_exp(-0.5f * power[q]);
+                        raw = conic.w * e;
+                    }
+                    const float alpha = fminf(0.99f, raw);
+                    const bool hit = candidate[q] && !(alpha < 1.0f / 255.0f);
+                    if (hit) {
+                        hitAny = true;
+                        // Gradients are checked against FP64 to a tolerance, not
+                        // bit for bit, so this part uses fused multiply-adds.
+                        const float4 col = sRec[j].colour;
+                        const float oneMinus = 1.0f - alpha;   // in [0.01, 1]
+                        float inv;   // 1 / (1 - alpha) to about 1 ulp
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(oneMinus));
+                        const float Ti = T[q] * inv;
+                        const float w = Ti * alpha;
+                        v[6] += gr[q] * w;
+                        v[7] += gg[q] * w;
+                        v[8] += gb[q] * w;
+                        const float behind =
+                            __fmaf_rn(gr[q], col.x - Br[q], __fmaf_rn(gg[q], col.y - Bg[q], gb[q] * (col.z - Bb[q])));
+                        const float dAlpha = __fmaf_rn(Ti, behind, gTT[q] * inv);
+                        Br[q] = __fmaf_rn(alpha, col.x - Br[q], Br[q]);
+                        Bg[q] = __fmaf_rn(alpha, col.y - Bg[q], Bg[q]);
+                        Bb[q] = __fmaf_rn(alpha, col.z - Bb[q], Bb[q]);
+                        T[q] = Ti;
+                        if (raw <= 0.99f) {
+                            v[5] += dAlpha * e;
+                            const float dPower = -0.5f * alpha * dAlpha;
+                            const float pdx = dPower * dx, pdy = dPower * dy[q];
+                            v[2] += pdx * dx;
+                            v[3] += 2.0f * pdx * dy[q];
+                            v[4] += pdy * dy[q];
+                            v[0] += -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
+                            v[1] += -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
+                        }
                     }
                 }
+                const unsigned hits = __ballot_sync(0xFFFFFFFFu, hitAny);
+                if (hits == 0) continue;
+                written |= 1u << bit;
                 if ((hits & (hits - 1)) == 0) {
-                    // one pixel of the warp: its values are the warp's sums
-                    if (hit) {
+                    // one lane of the warp: its values are the warp's sums
+                    if (hitAny) {
 #pragma unroll
                         for (uint32_t k = 0; k < kGrads; ++k) sPart[warp][j][k] = v[k];
                     }
@@ -255,18 +304,18 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
             if (lane == 0) sHit[warp][static_cast<uint32_t>(c) >> 5] = written;
         }
         __syncthreads();
-        if (tid < cnt) {
+        for (uint32_t m = tid; m < cnt; m += kThreads) {
             // Warps that wrote nothing for this record are skipped: adding
             // their zeros would not change the sum.
             float sum[kGradStride] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (uint32_t w = 0; w < kBlendThreads / 32; ++w) {
-                if ((sHit[w][tid >> 5] >> (tid & 31u)) & 1u) {
+            for (uint32_t w = 0; w < kWarps; ++w) {
+                if ((sHit[w][m >> 5] >> (m & 31u)) & 1u) {
 #pragma unroll
-                    for (uint32_t k = 0; k < kGrads; ++k) sum[k] += sPart[w][tid][k];
+                    for (uint32_t k = 0; k < kGrads; ++k) sum[k] += sPart[w][m][k];
                 }
             }
-            float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(sEmit[tid]) * kGradStride);
+            float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(sEmit[m]) * kGradStride);
             out[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
             out[1] = make_float4(sum[4], sum[5], sum[6], sum[7]);
             out[2] = make_float4(sum[8], 0.0f, 0.0f, 0.0f);
@@ -276,7 +325,7 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
     }
 }
 
-__global__ void __launch_bounds__(kBlendThreads)
+__global__ void __launch_bounds__(kBlendThreads / kBwdPix)
 blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
                       const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
                       const ProjRecord* __restrict__ proj,
@@ -290,7 +339,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
 // The backward of a training batch: one block per (view, tile) item of the
 // chunk, each the tile of blend_backward_kernel in its own view (records at
 // the view's base, pixel state and colour gradient from the view's buffers).
-__global__ void __launch_bounds__(kBlendThreads)
+__global__ void __launch_bounds__(kBlendThreads / kBwdPix)
 blend_backward_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_t viewCount,
                             const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
                             const uint32_t* __restrict__ emit, const ProjRecord* __restrict__ proj,
@@ -318,7 +367,7 @@ cudaError_t launch_blend_backward_batch(const BlendParams& bp, const ViewParams*
                                         const ProjRecord* proj, uint32_t totalTiles, float* partials,
                                         cudaStream_t stream) {
     if (totalTiles == 0) return cudaSuccess;
-    blend_backward_batch_kernel<<<totalTiles, kBlendThreads, 0, stream>>>(
+    blend_backward_batch_kernel<<<totalTiles, kBlendThreads / kBwdPix, 0, stream>>>(
         bp, views, viewCount, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, proj, partials);
     return cudaGetLastError();
 }
@@ -329,7 +378,7 @@ cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, co
                                   float* partials, cudaStream_t stream) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_backward_kernel<<<tiles, kBlendThreads, 0, stream>>>(
+    blend_backward_kernel<<<tiles, kBlendThreads / kBwdPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
         gradColour, partials);
     return cudaGetLastError();

@@ -45,6 +45,35 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
                                       uint32_t* emitSlot, uint32_t capacity, cudaStream_t stream,
                                       const FrameParams* fDev = nullptr);
 
+// The reference's two-sort order in two steps around a depth sort: the
+// projection alone (records, rects, touched counts, depth keys; per slot the
+// depth word depthKey << 32 | slot and the aux word emit_sorted reads), then,
+// over the depth words sorted on bits 32-55, the pairs emitted in depth order
+// as tile << 32 | slot (counters[1]: their total; status and ticket as for
+// the projection, over project_partitions(n) partitions).
+cudaError_t launch_project_only(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
+                                const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
+                                uint64_t* depthWords, cudaStream_t stream);
+cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
+                                       const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                       uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
+                                       uint64_t* depthWords, cudaStream_t stream);
+// The pairs in depth order from the depth-sorted slot words: each slot's
+// first pair into offsets[slot] (the total into counters[1]), then the pair
+// words tile << 32 | slot. Training frames: the emit index as the word's low
+// field with emitSlot[index] = slot, or as values[] beside a slot (both null:
+// not a training frame).
+cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const ProjRecord* proj, const uint4* rects,
+                               const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
+                               uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
+                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
+                               uint32_t* values = nullptr, uint32_t* emitSlot = nullptr);
+cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,
+                                      const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
+                                      uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
+                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, cudaStream_t stream);
+
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
                                   uint32_t* err, cudaStream_t stream);

@@ -102,7 +102,31 @@ LRT_HD float lrt_exp(float x) {
 // lrt_exp without its range checks, for -87 <= x <= 88 (where no check
 // fires, so the result has the same bits); outside that range it returns an
 // unspecified value. For hot loops whose argument is known to be in range.
+// On the device n = rint(x log2 e) comes from adding 1.5 * 2^23 (the sum
+// rounds to the nearest integer, ties to even, as rint does, for
+// |x log2 e| < 2^22), and the sum's low bits are then n itself, so 2^n is one
+// shift-add of those bits: no float -> int conversion. The bits are those of
+// the form below.
 LRT_HD float lrt_exp_in_range(float x) {
+#if defined(__CUDA_ARCH__)
+    constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23, bits 0x4B400000
+    const float t = __fadd_rn(__fmul_rn(x, 1.44269504088896340736f), kMagic);
+    const float n = __fsub_rn(t, kMagic);
+    float r = __fmaf_rn(-n, 0.693147182464599609375f, x);
+    r = __fmaf_rn(-n, -1.904654299957768e-09f, r);
+    float p = 1.984126984126984e-4f;
+    p = __fmaf_rn(p, r, 1.388888888888889e-3f);
+    p = __fmaf_rn(p, r, 8.333333333333333e-3f);
+    p = __fmaf_rn(p, r, 4.166666666666666e-2f);
+    p = __fmaf_rn(p, r, 1.666666666666667e-1f);
+    p = __fmaf_rn(p, r, 0.5f);
+    p = __fmaf_rn(p, r, 1.0f);
+    p = __fmaf_rn(p, r, 1.0f);
+    // (bits(t) - 0x4B400000 + 127) << 23 = 2^n's bits, the subtraction folded
+    // into the constant (mod 2^32).
+    const uint32_t scale = (__float_as_uint(t) << 23) + ((127u - 0x4B400000u) << 23);
+    return __fmul_rn(p, __uint_as_float(scale));
+#else
     const float n = lrt_rint(x * 1.44269504088896340736f);
     float r = lrt_fma(-n, 0.693147182464599609375f, x);
     r = lrt_fma(-n, -1.904654299957768e-09f, r);
@@ -116,6 +140,7 @@ LRT_HD float lrt_exp_in_range(float x) {
     p = lrt_fma(p, r, 1.0f);
     const int e = static_cast<int>(n);
     return p * bits_float(static_cast<uint32_t>(e + 127) << 23);
+#endif
 }
 
 LRT_HD float lrt_log(float x) {

@@ -1,6 +1,5 @@
-// Diagnostic: the rasteriser's own exp / log / sRGB / cut-off / float-to-half
-// functions
-// evaluated on the device, so tests can compare their bits with the host's.
+// Diagnostic: the rasteriser's own exp (with and without its range checks),
+// log, sRGB, cut-off and float-to-half functions evaluated on the device, so tests can compare their bits with the host's.
 #include "../../include/lrt_raster.h"
 #include "kernels.cuh"
 #include "raster_common.cuh"
@@ -20,6 +19,7 @@ __global__ void math_eval_kernel(int fn, const float* __restrict__ x, float* __r
         case 3: out = cutoff_power(v); break;
         case 4: out = __uint_as_float(float_to_half(v)); break;
         case 5: out = __uint_as_float(pack_halves(v, -0.5f * v)); break;
+        case 6: out = lrt_exp_in_range(v); break;   // for -87 <= v <= 88 only
         default: out = NAN; break;
     }
     y[i] = out;
@@ -36,7 +36,7 @@ cudaError_t launch_math_eval(int fn, const float* x, float* y, uint32_t n, cudaS
 }  // namespace lrt
 
 extern "C" int lrt_math_eval(int fn, const void* x, void* y, uint32_t n, void* stream) {
-    if (fn < 0 || fn > 5 || (n > 0 && (x == nullptr || y == nullptr))) return LRT_INVALID_ARGUMENT;
+    if (fn < 0 || fn > 6 || (n > 0 && (x == nullptr || y == nullptr))) return LRT_INVALID_ARGUMENT;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = lrt::launch_math_eval(fn, static_cast<const float*>(x), static_cast<float*>(y), n, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -1,5 +1,5 @@
 // Stages (a) and (b): per-splat projection, the touched-tile count, the
-// pairs' offsets and the pairs themselves, in one kernel.
+// pairs' offsets and the pairs themselves.
 //
 // Projection restates shaders/lrt/splat/splat_project.slang:39-221 (the splat
 // route; relighting is not part of this path): SplatEdit fate, near/far cull,
@@ -8,10 +8,19 @@
 // opacity payback, conic and cut-off, tile rectangle, exact touched-tile
 // count, view-dependent colour from f16 spherical harmonics up to degree 3,
 // and the 24-bit depth key. The pairs are the reference's splat_emit
-// (shaders/lrt/splat/splat_emit.slang:17-50), written in slot order at
-// offsets that are the exclusive prefix of the touched counts
-// (TileRasterizer.cpp:383-438 computes the same with three scans and a
-// readback).
+// (shaders/lrt/splat/splat_emit.slang:17-50).
+//
+// Two schedules share the projection (project_emit_kernel<Src, kEmit>):
+//  - single frames (kEmit false) stop after the records and counts and write
+//    each slot's depth word (depth key << 32 | slot) and aux word (its tile
+//    mask, or whether a large splat's rows are all single runs); the depth
+//    sort orders the words, depth_offsets_kernel gives each slot its first
+//    pair in depth order and emit_pairs_kernel writes the pairs
+//    (tile << 32 | slot) -- the reference's own two-sort sequence
+//    (TileRasterizer.cpp:383-457);
+//  - batched views (kEmit true) write (tile | depth key | slot) words in slot
+//    order at offsets from a block scan and a decoupled look-back over the
+//    frame's partitions, for one sort per chunk of views.
 //
 // B200 layout: one thread per splat, 256 per block; a block takes the next
 // 256 splats by atomic ticket. Positions and shape are read as 16-byte
@@ -19,12 +28,15 @@
 // start on a 16-byte boundary) are staged into shared memory by 16-byte
 // cp.async copies issued first, so they land while the geometry runs. A
 // splat's exact tile test runs per thread when its rectangle holds at most 16
-// tiles, and across its warp (32 tiles at a time, ballots) when larger; up to
-// 64 tiles the result is kept as a bitmask. The block's pair offsets come
-// from a block scan and a decoupled look-back over all partitions of the
-// frame (bounded waits). Pairs of masked splats are then written by the whole
-// block, one pair per thread per step, so writes are contiguous; larger
-// splats are written by their own warp with the tile test repeated.
+// tiles and across its warp (32 tiles at a time, ballots) up to 512; up to
+// 64 tiles the result is kept as a bitmask. Larger splats are counted and
+// written a tile row at a time by the whole block: a row plan (the ellipse's
+// x-extent in double precision, widened by a margin that covers the float
+// test's rounding) gives each row a run that is certainly touched and a few
+// columns at its ends that are tested exactly. Pairs of masked splats are
+// written by the whole block, one pair per thread per step, so writes are
+// contiguous; the other splats up to 512 tiles by their own warp with the
+// tile test repeated.
 #include "kernels.cuh"
 #include "raster_common.cuh"
 
@@ -278,6 +290,7 @@ struct TrainOutputs {
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
+constexpr uint32_t kWarpArea = 512;   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
 
 // ---- Splats of more than kSmallArea tiles, one tile row at a time ----
 //
@@ -323,15 +336,15 @@ __device__ __forceinline__ RowPlan row_plan(const Footprint& fp, uint32_t ty, ui
     if (!(a > 0.0) || !(c > 0.0) || !(k > 0.0) || !(det > 1e-6 * a * c)) return p;
     const double hx = sqrt(k * c / det), hy = sqrt(k * a / det);
     // Margin: the float test's power carries a relative error of a few
-    // roundings times the condition number kappa, which moves the boundary
-    // by at most that times the half-axes; its box coordinates carry one
-    // rounding of magnitudes up to |centre| + extent. Both with a factor of
-    // 16 to spare, plus a quarter pixel.
+    // roundings (4 x 2^-24) times the condition number kappa, which moves
+    // the boundary by at most that times half the long axis; its box
+    // coordinates carry one rounding of magnitudes up to |centre| + extent.
+    // Both with a factor of 8 to spare, plus a quarter pixel.
     const double lmin = 0.5 * (a + c) - sqrt(0.25 * (a - c) * (a - c) + b * b);
     if (!(lmin > 0.0)) return p;
     const double kappa = (fabs(a) + 2.0 * fabs(b) + fabs(c)) / lmin;
     const double reach = fabs(static_cast<double>(fp.cx)) + fabs(static_cast<double>(fp.cy)) + hx + hy + 64.0;
-    const double m = 0.25 + 16.0 * 6.0e-8 * (4.0 * kappa * (hx + hy) + reach);
+    const double m = 0.25 + 1.0e-6 * kappa * (hx + hy) + 5.0e-7 * reach;
     if (!(m < 24.0)) return p;
     const int32_t ity = static_cast<int32_t>(ty);
     const double ylo = static_cast<double>(static_cast<float>(ity * static_cast<int32_t>(kTile)) + 0.5f) -
@@ -343,11 +356,17 @@ __device__ __forceinline__ RowPlan row_plan(const Footprint& fp, uint32_t ty, ui
         p.hi = 0;
         return p;
     }
-    if (yhi < -hy + m || ylo > hy - m) return p;   // near its top or bottom: every column exact
+    // Near the ellipse's top or bottom the band's x extent is ill-conditioned
+    // (it grows as the square root of the band's overlap): there the
+    // candidates are the x extent of the band widened by m on both sides,
+    // each tested exactly, and none is certain.
+    const bool tangent = yhi < -hy + m || ylo > hy - m;
+    const double bandLo = tangent ? fmax(ylo - m, -hy) : ylo;
+    const double bandHi = tangent ? fmin(yhi + m, hy) : yhi;
     // The ellipse's x extent within the band: its leftmost and rightmost
     // points (x = -+hx, y = -b x / c) clamped into the band.
-    const double yl = fmin(fmax(b * hx / c, ylo), yhi);
-    const double yr = fmin(fmax(-b * hx / c, ylo), yhi);
+    const double yl = fmin(fmax(b * hx / c, bandLo), bandHi);
+    const double yr = fmin(fmax(-b * hx / c, bandLo), bandHi);
     const double xl = (-b * yl - sqrt(fmax(k * a - det * yl * yl, 0.0))) / a;
     const double xr = (-b * yr + sqrt(fmax(k * a - det * yr * yr, 0.0))) / a;
     // First column whose hi >= v, and last whose lo <= v, within the
@@ -373,12 +392,12 @@ __device__ __forceinline__ RowPlan row_plan(const Footprint& fp, uint32_t ty, ui
         return t;
     };
     const int32_t lo = firstHiAtLeast(xl - m), hi = lastLoAtMost(xr + m);
-    const int32_t sureLo = firstHiAtLeast(xl + m), sureHi = lastLoAtMost(xr - m);
+    const int32_t sureLo = tangent ? 1 : firstHiAtLeast(xl + m), sureHi = tangent ? 0 : lastLoAtMost(xr - m);
     if (!ok) return p;
     p.lo = lo;
     p.hi = hi;
-    p.sureLo = max(sureLo, lo);
-    p.sureHi = min(sureHi, hi);
+    p.sureLo = tangent ? 1 : max(sureLo, lo);
+    p.sureHi = tangent ? 0 : min(sureHi, hi);
     return p;
 }
 
@@ -455,6 +474,93 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
     return before + x - v;
 }
 
+// The block's first pair in the frame: warp 0 publishes the block's total
+// and looks back 32 partitions at a time (lane l reads the status of
+// partition q - l); the nearest inclusive prefix ends the walk and the
+// aggregates up to it are summed across the warp. A partition in the window
+// that has published nothing yet makes the warp read the window again
+// (bounded: after kSpinLimit polls kErrTimeout is raised and the walk
+// ends). The frame's last partition writes the pair total to counters[1].
+// Called by warp 0 only; lane 0's result is the block's base.
+__device__ __forceinline__ unsigned long long frame_lookback(uint64_t* __restrict__ status, uint32_t g,
+                                                             uint32_t lastPartition, uint32_t blockTotal,
+                                                             uint32_t* __restrict__ counters,
+                                                             uint32_t* __restrict__ err) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint64_t prefix = 0;
+    if (lane == 0) {
+        cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
+        mine.store((g == 0 ? kFlagInclusive : kFlagAggregate) | blockTotal, cuda::memory_order_relaxed);
+    }
+    if (g > 0) {
+        int64_t q = static_cast<int64_t>(g) - 1;
+        uint32_t spins = 0;
+        while (true) {
+            const int64_t idx = q - static_cast<int64_t>(lane);
+            uint64_t word = kFlagInclusive;   // before partition 0: an empty inclusive prefix
+            if (idx >= 0) {
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[idx]);
+                word = sref.load(cuda::memory_order_relaxed);
+            }
+            const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, (word & kFlagInclusive) != 0);
+            const uint32_t empty = __ballot_sync(0xFFFFFFFFu, (word & ~kValueMask) == 0);
+            const uint32_t first = inclusive != 0 ? static_cast<uint32_t>(__ffs(inclusive)) - 1u : 32u;
+            const uint32_t upTo = first < 32u ? (2u << first) - 1u : 0xFFFFFFFFu;   // lanes 0..first
+            if ((empty & upTo) != 0) {
+                if (++spins > kSpinLimit) {
+                    if (lane == 0) atomicOr(err, kErrTimeout);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            uint64_t v = ((upTo >> lane) & 1u) ? (word & kValueMask) : 0ull;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            prefix += v;
+            if (first < 32u) break;
+            q -= 32;
+        }
+        if (lane == 0) {
+            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
+            mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
+        }
+    }
+    if (lane == 0 && g == lastPartition) {
+        const uint64_t all = prefix + blockTotal;
+        if (all > 0xFFFFFFFFull) atomicOr(err, kErrTooManyPairs);
+        counters[1] = static_cast<uint32_t>(all);
+    }
+    return prefix;
+}
+
+// The position of the r-th set bit (from 0, lowest first) of a 64-bit mask
+// that has more than r set bits: the half, then five halvings by population
+// count.
+__device__ __forceinline__ uint32_t nth_set_bit(unsigned long long m, uint32_t r) {
+    uint32_t w = static_cast<uint32_t>(m);
+    uint32_t base = 0;
+    const uint32_t lowCount = static_cast<uint32_t>(__popc(w));
+    if (r >= lowCount) {
+        r -= lowCount;
+        w = static_cast<uint32_t>(m >> 32);
+        base = 32;
+    }
+#pragma unroll
+    for (uint32_t width = 16; width > 0; width >>= 1) {
+        const uint32_t lowBits = w & ((1u << width) - 1u);
+        const uint32_t c = static_cast<uint32_t>(__popc(lowBits));
+        if (r >= c) {
+            r -= c;
+            w >>= width;
+            base += width;
+        } else {
+            w = lowBits;
+        }
+    }
+    return base;
+}
+
 struct PairSink {
     unsigned long long* pairs;
     uint32_t* values;     // training, emit index as a sort value
@@ -510,6 +616,7 @@ __device__ __noinline__ void count_large_rows(const Footprint* foot, const uint3
 // a chunk of 256 rows at a time, each row's count and first column from its
 // row plan (as when counting), flattened so that consecutive threads write
 // consecutive pairs. takenStart[t]: the pairs of such splats before splat t.
+// slotOf[t]: the slot of the block's splat t (null: slotBase + t).
 template <class Sink>
 __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
                                              uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t tileBase,
@@ -517,7 +624,7 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
                                              const uint32_t* takenStart, const unsigned long long* low,
                                              uint32_t* rowOff, uint32_t* rowFirst, uint32_t* rowMeta,
                                              uint32_t* scanScratch, unsigned long long blockBase, uint32_t tileShift,
-                                             uint32_t slotBase, const Sink& sink) {
+                                             uint32_t slotBase, const uint32_t* slotOf, const Sink& sink) {
     const uint32_t tid = threadIdx.x;
     uint32_t fs = 0;
     {
@@ -561,21 +668,80 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
             const uint32_t tx = rowFirst[q] + (k - rowOff[q]);
             sink.put(blockBase + start[owner] + (carry + k - takenStart[owner]),
                      (static_cast<unsigned long long>(tileBase + ty * tilesX + tx) << tileShift) | low[owner],
-                     slotBase + owner);
+                     slotOf != nullptr ? slotOf[owner] : slotBase + owner);
         }
         carry += chunkTotal;
         __syncthreads();
     }
 }
 
-template <class Src>
+// The pairs of a warp's splats whose tiles are tested one by one (unmasked
+// splats of up to kWarpArea tiles, and larger ones with a row that is not
+// one run, possible only through the float test's rounding at the
+// ellipse's edge): for each such splat the warp repeats the exact tile test
+// over its rectangle, 32 tiles at a time, and writes the hits in row-major
+// order. The splat's record is read back from `records` (written earlier by
+// its thread): records[slotOf ? slotOf[s] : s].
+template <class Sink>
+__device__ __noinline__ void emit_by_warp(bool mine, uint32_t area, const uint32_t* widthBits,
+                                          const uint32_t* rectBits, const uint32_t* start,
+                                          const unsigned long long* low, const ProjRecord* records, uint32_t width,
+                                          uint32_t height, uint32_t tileBase, uint32_t tilesX,
+                                          unsigned long long blockBase, uint32_t tileShift, uint32_t slotBase,
+                                          const uint32_t* slotOf, const Sink& sink) {
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    uint32_t todo = __ballot_sync(0xFFFFFFFFu, mine);
+    while (todo != 0) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t s = (tid & ~31u) + static_cast<uint32_t>(src);
+        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
+        const ProjRecord rec = records[slotOf != nullptr ? slotOf[s] : s];
+        const uint32_t sW = widthBits[s] & 0xFFFFu;
+        const uint32_t sX = rectBits[s] & 0xFFFFu, sY = rectBits[s] >> 16;
+        unsigned long long at = blockBase + start[s];
+        const unsigned long long lowWord = low[s];
+        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
+        uint32_t dx = lane % sW, dy = lane / sW;
+        for (uint32_t base = 0; base < sArea; base += 32) {
+            const uint32_t tx = sX + dx, ty = sY + dy;
+            const bool hit = base + lane < sArea &&
+                             tile_touched(width, height, rec.screen.x, rec.screen.y, rec.conic.x, rec.conic.y,
+                                          rec.conic.z, rec.screen.w, tx, ty);
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+            if (hit) {
+                sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
+                         (static_cast<unsigned long long>(tileBase + ty * tilesX + tx) << tileShift) | lowWord,
+                         slotOf != nullptr ? slotOf[s] : slotBase + s);
+            }
+            at += static_cast<uint32_t>(__popc(bal));
+            dx += stepDx;
+            dy += stepDy;
+            if (dx >= sW) {
+                dx -= sW;
+                dy += 1;
+            }
+        }
+    }
+}
+
+
+// kEmit: emit the pairs (offsets by look-back over the frame's partitions).
+// Otherwise stop after the records and counts, and write per slot the
+// depth word (depth key << 32 | slot) the depth sort orders and the aux word
+// emit_sorted_kernel reads: the tile mask of a masked splat, else 1 when a
+// row of the splat's hits is not one run.
+template <class Src, bool kEmit = true>
 __global__ void __launch_bounds__(kProjectThreads, 4)
 project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
                     uint32_t stageWords, uint32_t shVector,
                     ProjRecord* __restrict__ proj, uint4* __restrict__ rects, uint32_t* __restrict__ touchedOut,
                     uint32_t* __restrict__ keysOut, uint32_t* __restrict__ counters, uint64_t* __restrict__ status,
                     uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t lowBits,
-                    unsigned long long* __restrict__ pairs, uint32_t capacity) {
+                    unsigned long long* __restrict__ pairs, uint32_t capacity,
+                    unsigned long long* __restrict__ auxOut = nullptr,
+                    unsigned long long* __restrict__ depthWordsOut = nullptr) {
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
@@ -773,10 +939,52 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             }
         }
     }
-    // Splats of more than kSmallArea tiles are counted by the whole block
-    // below, after the records are written (so that the projection's values
+    // Splats of up to kWarpArea tiles: their warp tests 32 tiles of the
+    // rectangle a step (row-major, lane l tiles l, l + 32, ...; column and row
+    // advance by 32 tiles a step without a division), building the mask of a
+    // masked splat.
+    uint32_t medium = __ballot_sync(0xFFFFFFFFu, alive && area > kSmallArea && area <= kWarpArea);
+    while (medium != 0) {
+        const int src = __ffs(medium) - 1;
+        medium &= medium - 1;
+        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
+        const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
+        const uint32_t sSh = __shfl_sync(0xFFFFFFFFu, sh, src);
+        const bool sMasked = __shfl_sync(0xFFFFFFFFu, masked ? 1u : 0u, src) != 0;
+        const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
+        const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
+        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
+        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
+        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
+        uint32_t dx = lane % sW, dy = lane / sW;
+        uint32_t count = 0;
+        uint32_t mLo = 0, mHi = 0;
+        for (uint32_t base = 0; base < sArea; base += 32) {
+            const bool hit = base + lane < sArea &&
+                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + dx, sY + dy);
+            count += static_cast<uint32_t>(__popc(__ballot_sync(0xFFFFFFFFu, hit)));
+            if (sMasked) {
+                const uint32_t bit = (dy << sSh) | dx;
+                mLo |= __reduce_or_sync(0xFFFFFFFFu, hit && bit < 32u ? 1u << bit : 0u);
+                mHi |= __reduce_or_sync(0xFFFFFFFFu, hit && bit >= 32u ? 1u << (bit - 32u) : 0u);
+            }
+            dx += stepDx;
+            dy += stepDy;
+            if (dx >= sW) {
+                dx -= sW;
+                dy += 1;
+            }
+        }
+        if (lane == static_cast<uint32_t>(src)) {
+            touched = count;
+            mask = sMasked ? (static_cast<unsigned long long>(mHi) << 32) | mLo : 0ull;
+        }
+    }
+    // Larger splats are counted by the whole block below, a tile row at a
+    // time, after the records are written (so that the projection's values
     // are no longer held in registers); the others are decided now.
-    const bool bigHere = alive && area > kSmallArea;
+    const bool bigHere = alive && area > kWarpArea;
     if (!bigHere) {
         alive = alive && touched != 0;
         if (!alive) touched = 0;
@@ -879,6 +1087,13 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
     const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, inRange && alive);
     if (lane == 0 && ballot != 0) atomicAdd(counters, static_cast<uint32_t>(__popc(ballot)));
+    if constexpr (!kEmit) {
+        if (inRange) {
+            auxOut[record] = masked ? mask : (irregular ? 1ull : 0ull);
+            depthWordsOut[record] = (static_cast<unsigned long long>(key) << 32) | slot;
+        }
+        return;
+    }
 
     // Offsets: block scan, then decoupled look-back over the frame's partitions.
     uint32_t blockTotal = 0, smallTotal = 0;
@@ -895,61 +1110,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         sStart[kProjectThreads] = blockTotal;
         sSmallStart[kProjectThreads] = smallTotal;
     }
-    if (tid < 32) {
-        // Warp 0 looks back 32 partitions at a time: lane l reads the status
-        // of partition q - l; the nearest inclusive prefix ends the walk, and
-        // the aggregates up to it are summed across the warp. A partition in
-        // the window that has published nothing yet makes the warp read the
-        // window again (bounded).
-        const uint32_t g = partitionBase + part;
-        uint64_t prefix = 0;
-        if (lane == 0) {
-            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
-            mine.store((g == 0 ? kFlagInclusive : kFlagAggregate) | blockTotal, cuda::memory_order_relaxed);
-        }
-        if (g > 0) {
-            int64_t q = static_cast<int64_t>(g) - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const int64_t idx = q - static_cast<int64_t>(lane);
-                uint64_t word = kFlagInclusive;   // before partition 0: an empty inclusive prefix
-                if (idx >= 0) {
-                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> sref(status[idx]);
-                    word = sref.load(cuda::memory_order_relaxed);
-                }
-                const uint32_t inclusive = __ballot_sync(0xFFFFFFFFu, (word & kFlagInclusive) != 0);
-                const uint32_t empty = __ballot_sync(0xFFFFFFFFu, (word & ~kValueMask) == 0);
-                const uint32_t first = inclusive != 0 ? static_cast<uint32_t>(__ffs(inclusive)) - 1u : 32u;
-                const uint32_t upTo = first < 32u ? (2u << first) - 1u : 0xFFFFFFFFu;   // lanes 0..first
-                if ((empty & upTo) != 0) {
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0) atomicOr(err, kErrTimeout);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                uint64_t v = ((upTo >> lane) & 1u) ? (word & kValueMask) : 0ull;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-                prefix += v;
-                if (first < 32u) break;
-                q -= 32;
-            }
-            if (lane == 0) {
-                cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[g]);
-                mine.store(kFlagInclusive | (prefix + blockTotal), cuda::memory_order_relaxed);
-            }
-        }
-        if (lane == 0) {
-            sBase = prefix;
-            if (g == lastPartition) {
-                const uint64_t all = prefix + blockTotal;
-                if (all > 0xFFFFFFFFull) atomicOr(err, kErrTooManyPairs);
-                counters[1] = static_cast<uint32_t>(all);
-            }
-        }
-    }
+    if (tid < 32) sBase = frame_lookback(status, partitionBase + part, lastPartition, blockTotal, counters, err);
     __syncthreads();
     const unsigned long long blockBase = sBase;
     if (writeOffset) train.offsets[slot] = static_cast<uint32_t>(blockBase + start);
@@ -965,10 +1126,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             if (sSmallStart[mid] <= j) lo = mid; else hi = mid;
         }
         const uint32_t s = lo;
-        uint32_t r = j - sSmallStart[s];
-        unsigned long long m = sMask[s];
-        for (; r > 0; --r) m &= m - 1;   // drop the r lowest set bits
-        const uint32_t bit = static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
+        const uint32_t bit = nth_set_bit(sMask[s], j - sSmallStart[s]);
         const uint32_t bsh = (sWidth[s] >> 16) & 0xFFu;
         const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
         const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
@@ -983,50 +1141,173 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     // order, so its pairs follow one another from its offset.
     if (rowsTotal != 0) {
         __syncthreads();   // the masked writes are done with sSmallStart
-        const bool taken = touched != 0 && !masked && !irregular;
+        // Only the splats the rows walk (those in sFoot): their pairs' offsets
+        // among the rows' pairs.
+        const bool taken = touched != 0 && !masked && !irregular && area > kWarpArea;
         uint32_t takenTotal = 0;
         sSmallStart[tid] = block_exclusive_scan(taken ? touched : 0u, sScan, &takenTotal);
         __syncthreads();
         if (takenTotal != 0)
             emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, f.tileBase, f.tilesX, sWidth,
                             sStart, sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, blockBase, tileShift,
-                            slotBase, sink);
+                            slotBase, nullptr, sink);
     }
     // A splat whose rows are not all single runs (possible only through the
     // float test's rounding at the ellipse's edge): its warp repeats the exact
     // tile test over the rectangle, 32 tiles at a time.
-    uint32_t large = __ballot_sync(0xFFFFFFFFu, touched != 0 && !masked && irregular);
-    while (large != 0) {
-        const int src = __ffs(large) - 1;
-        large &= large - 1;
-        const uint32_t s = (tid & ~31u) + static_cast<uint32_t>(src);
-        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
-        const Footprint sfp = sFoot[__shfl_sync(0xFFFFFFFFu, bigIdx, src)];
-        const uint32_t sW = sWidth[s] & 0xFFFFu;
-        const uint32_t sX = sRect[s] & 0xFFFFu, sY = sRect[s] >> 16;
-        const float scx = sfp.cx, scy = sfp.cy, sa = sfp.a, sb = sfp.b, sc = sfp.c, scut = sfp.cut;
-        unsigned long long at = blockBase + sStart[s];
-        const unsigned long long low = sLow[s];
-        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
-        uint32_t dx = lane % sW, dy = lane / sW;
-        for (uint32_t base = 0; base < sArea; base += 32) {
-            const uint32_t tx = sX + dx, ty = sY + dy;
-            const bool hit = base + lane < sArea && tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, tx, ty);
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
-            if (hit) {
-                sink.put(at + static_cast<uint32_t>(__popc(bal & ((1u << lane) - 1u))),
-                         (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | low,
-                         slotBase + s);
-            }
-            at += static_cast<uint32_t>(__popc(bal));
-            dx += stepDx;
-            dy += stepDy;
-            if (dx >= sW) {
-                dx -= sW;
-                dy += 1;
-            }
-        }
+    // Unmasked splats of up to kWarpArea tiles, and larger ones whose rows
+    // are not all single runs: their warp writes their pairs, repeating the
+    // exact tile test over the rectangle 32 tiles at a time.
+    const bool byWarp = touched != 0 && !masked && (area <= kWarpArea || irregular);
+    if (__ballot_sync(0xFFFFFFFFu, byWarp) != 0)
+        emit_by_warp(byWarp, area, sWidth, sRect, sStart, sLow, proj + f.recordBase + slotBase, f.width, f.height,
+                     f.tileBase, f.tilesX, blockBase, tileShift, slotBase, nullptr, sink);
+}
+
+// Stage (b) in depth order, as the reference emits (splat_emit.slang:17-50
+// over the depth-sorted visible splats, TileRasterizer.cpp:418-438), in two
+// kernels so that the pair writing keeps the projection's load balance:
+//  - depth_offsets_kernel: each slot's first pair, the exclusive prefix of
+//    the touched counts over the slots in depth order (block scan, then the
+//    frame look-back; the last partition writes the total to counters[1]);
+//  - emit_pairs_kernel: the pairs, written in slot order, each splat's at
+//    its offset, as words tile << 32 | slot, its tiles in row-major order.
+// Depth order puts the near splats, which are the large ones, together:
+// writing their pairs in that order left a few blocks with most of a
+// sort-heavy frame's pairs. In slot order they are spread over the grid as
+// in the projection. A stable sort of the words on their tile bits then
+// leaves every tile's pairs in (depth key, slot) order: the reference's
+// two-sort order. Training frames keep the offsets (each slot's emit range
+// is [offset, offset + touched)) and a way back from every pair to its emit
+// index: the word's low field itself, with an emit index -> slot map
+// (train.emitSlot), or a sort value beside a slot (train.values).
+constexpr uint32_t kOffsetItems = 4;   // depth positions a thread
+
+__global__ void __launch_bounds__(kProjectThreads)
+depth_offsets_kernel(const unsigned long long* __restrict__ sortedWords, uint32_t n,
+                     const uint32_t* __restrict__ touchedIn, uint32_t* __restrict__ counters,
+                     uint64_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t lastPartition,
+                     uint32_t* __restrict__ offsets) {
+    __shared__ uint32_t sPart;
+    __shared__ uint32_t sScan[kProjectThreads / 32];
+    __shared__ unsigned long long sBase;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) sPart = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t part = sPart;
+    const uint32_t d0 = (part * kProjectThreads + tid) * kOffsetItems;
+    uint32_t slot[kOffsetItems], count[kOffsetItems];
+    uint32_t mine = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kOffsetItems; ++k) {
+        const bool in = d0 + k < n;
+        slot[k] = in ? static_cast<uint32_t>(__ldg(sortedWords + d0 + k)) : 0u;
+        count[k] = in ? __ldg(touchedIn + slot[k]) : 0u;
+        mine += count[k];
     }
+    uint32_t blockTotal = 0;
+    uint32_t at = block_exclusive_scan(mine, sScan, &blockTotal);
+    if (tid < 32) sBase = frame_lookback(status, part, lastPartition, blockTotal, counters, counters + 2);
+    __syncthreads();
+    const unsigned long long base = sBase;
+#pragma unroll
+    for (uint32_t k = 0; k < kOffsetItems; ++k) {
+        if (d0 + k < n) offsets[slot[k]] = static_cast<uint32_t>(base + at);
+        at += count[k];
+    }
+}
+
+// Block b writes the pairs of slots [256 b, 256 b + 256): it reads each
+// one's touched count, rectangle, aux word (project_emit_kernel<.., false>)
+// and offset, and, for a splat written row by row or tile by tile, its
+// record.
+__global__ void __launch_bounds__(kProjectThreads, 4)
+emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* __restrict__ rectsIn,
+                  const uint32_t* __restrict__ touchedIn, const unsigned long long* __restrict__ aux,
+                  const uint32_t* __restrict__ offsets, uint32_t width, uint32_t height, uint32_t tilesX,
+                  uint32_t* __restrict__ err, unsigned long long* __restrict__ pairs, uint32_t capacity,
+                  TrainOutputs train) {
+    __shared__ uint32_t sScan[kProjectThreads / 32];
+    __shared__ uint32_t sStart[kProjectThreads + 1];
+    __shared__ uint32_t sSmallStart[kProjectThreads + 1];
+    __shared__ unsigned long long sMask[kProjectThreads];
+    __shared__ unsigned long long sLow[kProjectThreads];
+    __shared__ uint32_t sRect[kProjectThreads];
+    __shared__ uint32_t sWidth[kProjectThreads];
+    __shared__ Footprint sFoot[kProjectThreads];
+    __shared__ uint32_t sFootRow[kProjectThreads + 1];
+    __shared__ uint32_t sRowFirst[kProjectThreads];
+    __shared__ uint32_t sRowMeta[kProjectThreads];
+    __shared__ uint32_t sRowOff[kProjectThreads + 1];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t slotBase = blockIdx.x * kProjectThreads;
+    const uint32_t slot = slotBase + tid;
+    const bool inRange = slot < n;
+    const uint32_t touched = inRange ? __ldg(touchedIn + slot) : 0u;
+    const bool alive = touched != 0;
+    const uint4 rect = alive ? __ldg(rectsIn + slot) : make_uint4(1, 1, 0, 0);
+    const uint32_t rw = alive ? rect.z - rect.x + 1 : 0;
+    const uint32_t rh = alive ? rect.w - rect.y + 1 : 0;
+    const uint32_t area = rw * rh;
+    const uint32_t sh = rw <= 1 ? 0u : 32u - static_cast<uint32_t>(__clz(rw - 1));
+    const bool masked = alive && rh <= (64u >> sh);
+    const unsigned long long a = alive ? __ldg(aux + slot) : 0ull;
+    const bool irregular = alive && !masked && (a & 1ull) != 0;
+    // The splats written a row at a time: unmasked, of more than kWarpArea
+    // tiles, every row one run. The other unmasked ones go tile by tile.
+    const bool rowsHere = alive && !masked && !irregular && area > kWarpArea;
+    const bool byWarp = alive && !masked && !rowsHere;
+    uint32_t bigTotal = 0, rowsTotal = 0;
+    const uint32_t bigIdx = block_exclusive_scan(rowsHere ? 1u : 0u, sScan, &bigTotal);
+    const uint32_t rowStart = block_exclusive_scan(rowsHere ? rh : 0u, sScan, &rowsTotal);
+    if (rowsHere) {
+        const ProjRecord rec = proj[slot];
+        sFoot[bigIdx] = Footprint{rec.screen.x, rec.screen.y, rec.conic.x, rec.conic.y, rec.conic.z, rec.screen.w,
+                                  rect.x, rect.z, rect.y, tid, sh};
+        sFootRow[bigIdx] = rowStart;
+    }
+    if (tid == 0) sFootRow[bigTotal] = rowsTotal;
+    uint32_t smallTotal = 0;
+    const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
+    sStart[tid] = alive ? __ldg(offsets + slot) : 0u;
+    sSmallStart[tid] = smallStart;
+    sMask[tid] = masked ? a : 0ull;
+    sLow[tid] = 0ull;
+    sRect[tid] = rect.x | (rect.y << 16);
+    sWidth[tid] = rw | (sh << 16) | (irregular ? 0x80000000u : 0u);
+    if (tid == 0) sSmallStart[kProjectThreads] = smallTotal;
+    __syncthreads();
+    const PairSink sink{pairs, train.values, train.emitSlot, capacity, err};
+    constexpr uint32_t tileShift = 32;
+
+    // Masked splats: the whole block writes their pairs, one per thread per step.
+    for (uint32_t j = tid; j < smallTotal; j += kProjectThreads) {
+        uint32_t lo = 0, hi = kProjectThreads;   // the splat s with sSmallStart[s] <= j < sSmallStart[s + 1]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sSmallStart[mid] <= j) lo = mid; else hi = mid;
+        }
+        const uint32_t s = lo;
+        const uint32_t bit = nth_set_bit(sMask[s], j - sSmallStart[s]);
+        const uint32_t bsh = (sWidth[s] >> 16) & 0xFFu;
+        const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
+        const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
+        sink.put(static_cast<unsigned long long>(sStart[s]) + (j - sSmallStart[s]),
+                 static_cast<unsigned long long>(ty * tilesX + tx) << tileShift, slotBase + s);
+    }
+    if (rowsTotal != 0) {
+        __syncthreads();   // the masked writes are done with sSmallStart
+        uint32_t takenTotal = 0;
+        sSmallStart[tid] = block_exclusive_scan(rowsHere ? touched : 0u, sScan, &takenTotal);
+        __syncthreads();
+        if (takenTotal != 0)
+            emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, width, height, 0u, tilesX, sWidth, sStart,
+                            sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, 0ull, tileShift, slotBase,
+                            nullptr, sink);
+    }
+    if (__ballot_sync(0xFFFFFFFFu, byWarp) != 0)
+        emit_by_warp(byWarp, area, sWidth, sRect, sStart, sLow, proj + slotBase, width, height, 0u, tilesX, 0ull,
+                     tileShift, slotBase, nullptr, sink);
 }
 
 template <class Src>
@@ -1045,6 +1326,25 @@ cudaError_t launch(const FrameParams& f, const FrameParams* fDev, const Src& src
     project_emit_kernel<Src><<<blocks, kProjectThreads, smem, stream>>>(
         f, fDev, src, train, stageWords, shVector, proj, rects, touched, keys, counters, status, ticket, partitionBase,
         lastPartition, slotBits, reinterpret_cast<unsigned long long*>(pairs), capacity);
+    return cudaGetLastError();
+}
+
+// The projection without its emission (project_emit_kernel<Src, false>).
+template <class Src>
+cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRecord* proj, uint4* rects,
+                        uint32_t* touched, uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
+                        uint64_t* depthWords, cudaStream_t stream) {
+    const uint32_t stageWords = stage ? f.shWords : 0u;
+    const uint32_t shVector = (reinterpret_cast<uintptr_t>(src.sh) & 15u) == 0 ? 1u : 0u;
+    const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
+    cudaError_t e = cudaFuncSetAttribute(project_emit_kernel<Src, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(std::max<size_t>(smem, 1)));
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = project_partitions(f.count);
+    project_emit_kernel<Src, false><<<blocks, kProjectThreads, smem, stream>>>(
+        f, nullptr, src, TrainOutputs{nullptr, nullptr, nullptr}, stageWords, shVector, proj, rects, touched, keys,
+        counters, nullptr, ticket, 0, 0, 0, nullptr, 0, reinterpret_cast<unsigned long long*>(aux),
+        reinterpret_cast<unsigned long long*>(depthWords));
     return cudaGetLastError();
 }
 
@@ -1092,6 +1392,57 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
     return launch(f, fDev, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)},
                   TrainOutputs{offsets, values, emitSlot}, true, proj, rects, touched, keys, counters, status, ticket,
                   partitionBase, lastPartition, lowBits, pairs, capacity, stream);
+}
+
+cudaError_t launch_project_only(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
+                                const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
+                                uint64_t* depthWords, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    const uint32_t rpc = f.restPerColour;
+    const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
+    const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
+    return launch_only(f, PackedSource{positions, shape, sh, filter3d}, stage, proj, rects, touched, keys, counters,
+                       ticket, aux, depthWords, stream);
+}
+
+cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
+                                       const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
+                                       uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
+                                       uint64_t* depthWords, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    PointSource src{positions, reinterpret_cast<const uint2*>(colours), nullptr, style.size_mode, style.size,
+                    style.constant_colour, {style.colour[0], style.colour[1], style.colour[2]}};
+    return launch_only(f, src, false, proj, rects, touched, keys, counters, ticket, aux, depthWords, stream);
+}
+
+cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const ProjRecord* proj, const uint4* rects,
+                               const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
+                               uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
+                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
+                               uint32_t* values, uint32_t* emitSlot) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t perBlock = kProjectThreads * kOffsetItems;
+    const uint32_t offsetBlocks = (n + perBlock - 1) / perBlock;
+    depth_offsets_kernel<<<offsetBlocks, kProjectThreads, 0, stream>>>(
+        reinterpret_cast<const unsigned long long*>(sortedWords), n, touched, counters, status, ticket,
+        offsetBlocks - 1, offsets);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    emit_pairs_kernel<<<project_partitions(n), kProjectThreads, 0, stream>>>(
+        n, proj, rects, touched, reinterpret_cast<const unsigned long long*>(aux), offsets, width, height, tilesX,
+        counters + 2, reinterpret_cast<unsigned long long*>(pairs), capacity, TrainOutputs{nullptr, values, emitSlot});
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,
+                                      const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
+                                      uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
+                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, cudaStream_t stream) {
+    if (f.count == 0) return cudaSuccess;
+    // The DC triple is read from the staged row too, so it is always staged.
+    return launch_only(f, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)}, true,
+                       proj, rects, touched, keys, counters, ticket, aux, depthWords, stream);
 }
 
 }  // namespace lrt

@@ -35,6 +35,7 @@ struct lrt_rast {
     DeviceBuffer scanScratch, sortScratch;               // look-back status words, tickets
     DeviceBuffer counters;                               // visible, pairs, err, algo err
     DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers
+    DeviceBuffer depthWords, depthWordsAlt, splatAux;    // per slot: depth words (two-step frames), aux words
     lrt::SortFault sortFault;                            // lrt_radix_sort's planted fault (tests only)
     DeviceBuffer filterCameras, filterScratch;           // lrt_rast_filter3d's cameras and lowest rate
     uint32_t* hostCounters = nullptr;                    // pinned
@@ -42,7 +43,7 @@ struct lrt_rast {
     uint32_t splatCap = 0, pairCap = 0, tileCap = 0;
     lrt_debug_view debug{};
     // Training: what the backward pass needs from its forward.
-    DeviceBuffer pairValues, pairValuesAlt, trainOffsets, pixState, pixLast, partials;
+    DeviceBuffer pairValues, pairValuesAlt, pairOffsets, pixState, pixLast, partials;
     DeviceBuffer metricScratch;                          // parity metrics: histograms, row errors
     DeviceBuffer lossScratch;                            // the L1 loss's per-block sums
     // Training batches (train_batch.cu): colour gradients, every view's view

@@ -60,7 +60,7 @@ void lrt_rast_destroy(lrt_rast* r) {
     DeviceScope scope(r->device);
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
-                            &r->algoValsAlt, &r->pairValues, &r->pairValuesAlt, &r->trainOffsets, &r->pixState,
+                            &r->algoValsAlt, &r->depthWords, &r->depthWordsAlt, &r->splatAux, &r->pairValues, &r->pairValuesAlt, &r->pairOffsets, &r->pixState,
                             &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
                             &r->trainBatchViews, &r->trainBatchLoss, &r->lodBuild.globals,
                             &r->lodBuild.partial, &r->lodBuild.keys, &r->lodBuild.keysAlt, &r->lodBuild.order,
@@ -136,11 +136,11 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     const uint32_t tilesX = (s->width + lrt::kTile - 1) / lrt::kTile;
     const uint32_t tilesY = (s->height + lrt::kTile - 1) / lrt::kTile;
     const uint32_t tiles = tilesX * tilesY;
-    const uint32_t slotBits = bits_for(std::max<uint64_t>(slots, 1));
     const uint32_t tileBits = bits_for(tiles);
-    const uint32_t keyBits = 24 + tileBits;
-    if (slotBits + keyBits > 64)
-        return fail(r, LRT_UNSUPPORTED, "splat slots and tile count do not fit one 64-bit pair word");
+    // A frame takes the reference's two sorts: the projection alone, a sort
+    // of the slots' depth words, the pairs emitted in depth order as
+    // tile << 32 | slot (or emit index), and a stable sort of those on the tile
+    // bits (TileRasterizer.cpp:401-457).
 
     // Buffers (TileRasterizer.cpp:105-177).
     if (slots > r->splatCap) {
@@ -151,12 +151,17 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         LRT_CUDA(r, ensure(r->keys, size_t{cap} * 4), "depth keys");
         r->splatCap = cap;
     }
+    LRT_CUDA(r, ensure(r->depthWords, size_t{r->splatCap} * 8), "depth words");
+    LRT_CUDA(r, ensure(r->depthWordsAlt, size_t{r->splatCap} * 8), "depth words");
+    LRT_CUDA(r, ensure(r->splatAux, size_t{r->splatCap} * 8), "tile masks");
+    LRT_CUDA(r, ensure(r->pairOffsets, size_t{std::max(slots, 1u)} * 4), "pair offsets");
     if (train) {
-        LRT_CUDA(r, ensure(r->trainOffsets, size_t{std::max(slots, 1u)} * 4), "pair offsets");
         LRT_CUDA(r, ensure(r->pixState, size_t{s->width} * s->height * 16), "pixel state");
         LRT_CUDA(r, ensure(r->pixLast, size_t{s->width} * s->height * 4), "pixel state");
     }
-    const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches} * 4;
+    // Look-back status words and a ticket per projection launch, plus one
+    // for the emission over the frame's slots in depth order.
+    const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches + 1} * 4;
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
         LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
@@ -186,90 +191,102 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     bp.depthThreshold = s->depth_threshold;
     for (int a = 0; a < 4; ++a) bp.bg[a] = s->background[a];
     FrameParams lastParams{};
-    // Training frames carry each pair's emit index to the backward pass. It is
-    // the pair word's low field (with an emit-index -> slot map for the blend)
-    // when tile, depth key and index fit 64 bits, else a sort value beside the
-    // word. The low field is the slot otherwise.
+    // Training frames carry each pair's emit index to the backward pass: the
+    // pair word's low field (with an emit index -> slot map for the blend),
+    // or, when asked for, a sort value beside a word whose low field is the
+    // slot. Other frames' words hold the slot.
     const bool valuesAsked = train && !clouds.empty() && clouds[0].train != nullptr &&
                              (clouds[0].train->flags & LRT_TRAIN_SORT_VALUES) != 0;
-    bool lowIsEmit = false;
-    uint32_t lowBits = slotBits;
+    const bool lowIsEmit = train && !valuesAsked;
+    bp.slotBits = 32;
+    bp.tileShift = 32;
     for (int attempt = 0; attempt < 2; ++attempt) {
-        lowIsEmit = train && !valuesAsked && keyBits + bits_for(r->pairCap) <= 64;
-        lowBits = lowIsEmit ? bits_for(r->pairCap) : slotBits;
-        bp.slotBits = lowBits;
-        bp.tileShift = 24 + lowBits;
         LRT_CUDA(r, ensure(r->pairs, size_t{r->pairCap} * 8), "pairs");
         LRT_CUDA(r, ensure(r->pairsAlt, size_t{r->pairCap} * 8), "pairs");
         if (train) {
             LRT_CUDA(r, ensure(r->pairValues, size_t{r->pairCap} * 4), "pair values");
             if (!lowIsEmit) LRT_CUDA(r, ensure(r->pairValuesAlt, size_t{r->pairCap} * 4), "pair values");
         }
-        LRT_CUDA(r, ensure(r->sortScratch, lrt::sort_scratch_bytes(r->pairCap, keyBits)), "sort scratch");
+        LRT_CUDA(r,
+                 ensure(r->sortScratch,
+                        std::max(lrt::sort_scratch_bytes(r->pairCap, tileBits), lrt::sort_scratch_bytes(slots, 24))),
+                 "sort scratch");
         LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
         LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, stream), "projection scratch");
         uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
         uint32_t* valueBuf = train && !lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
         uint32_t* emitSlot = train && lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
 
-        // --- project, count, emit --------------------------------------------
+        // --- project, count -------------------------------------------------------
         LRT_CUDA(r, cudaEventRecord(r->ev[0], stream), "event");
-        uint32_t base = 0, partitionBase = 0, launch = 0;
+        uint32_t base = 0, launch = 0;
+        uint64_t* depthWords = static_cast<uint64_t*>(r->depthWords.ptr);
+        uint64_t* aux = static_cast<uint64_t*>(r->splatAux.ptr);
         for (const CloudDesc& c : clouds) {
             const FrameParams f = frame_params(pr, s, c, tilesX, tilesY, base);
             lastParams = f;
             if (c.point != nullptr) {
                 const lrt_gpu_points& g = *c.point->points;
                 LRT_CUDA(r,
-                         lrt::launch_project_points(
+                         lrt::launch_project_points_only(
                              f, static_cast<const float4*>(g.positions), static_cast<const uint32_t*>(g.colours),
                              c.point->style, static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
                              static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
-                             status, tickets + launch, partitionBase, lastPartition, lowBits, pairBuf, r->pairCap,
-                             stream),
+                             tickets + launch, aux, depthWords, stream),
                          "points");
             } else if (c.train != nullptr) {
                 const lrt_train_params& t = *c.train;
                 LRT_CUDA(r,
-                         lrt::launch_project_emit_train(
+                         lrt::launch_project_only_train(
                              f, static_cast<const float*>(t.means), static_cast<const float*>(t.log_scales),
                              static_cast<const float*>(t.quats), static_cast<const float*>(t.opacity_logits),
                              static_cast<const uint16_t*>(t.sh), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                             static_cast<uint32_t*>(r->keys.ptr), static_cast<uint32_t*>(r->trainOffsets.ptr),
-                             counters, status, tickets + launch, partitionBase, lastPartition, lowBits, pairBuf,
-                             valueBuf, emitSlot, r->pairCap, stream),
+                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords, stream),
                          "project");
             } else {
                 LRT_CUDA(r,
-                         lrt::launch_project_emit(
+                         lrt::launch_project_only(
                              f, static_cast<const float4*>(c.packed->positions),
                              static_cast<const uint4*>(c.packed->shape), static_cast<const uint32_t*>(c.packed->sh),
-                             static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
-                             static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
-                             status, tickets + launch, partitionBase, lastPartition, slotBits, pairBuf, r->pairCap,
-                             stream, nullptr, static_cast<const float*>(c.packed->filter3d)),
+                             static_cast<const float*>(c.packed->filter3d), static_cast<ProjRecord*>(r->proj.ptr),
+                             static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords, stream),
                          "project");
             }
             base += c.count;
-            partitionBase += lrt::project_partitions(c.count);
             launch += 1;
         }
         LRT_CUDA(r, cudaEventRecord(r->ev[1], stream), "event");
-
-        // --- sort + ranges ------------------------------------------------------
+        // --- depth sort of the slots (24-bit keys; ties stay in slot order) ------------
+        bool depthInAlt = false;
+        LRT_CUDA(r,
+                 lrt::launch_sort_u64(depthWords, static_cast<uint64_t*>(r->depthWordsAlt.ptr), nullptr, nullptr,
+                                      nullptr, slots, 32, 24, r->sortScratch.ptr, err, &depthInAlt, stream),
+                 "depth sort");
+        const uint64_t* byDepth = depthInAlt ? static_cast<const uint64_t*>(r->depthWordsAlt.ptr) : depthWords;
+        LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
+        // --- pairs in depth order ----------------------------------------------------------
+        LRT_CUDA(r,
+                 lrt::launch_emit_sorted(byDepth, slots, static_cast<ProjRecord*>(r->proj.ptr),
+                                         static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
+                                         aux, s->width, s->height, tilesX, counters, status, tickets + launches,
+                                         static_cast<uint32_t*>(r->pairOffsets.ptr), pairBuf, r->pairCap, stream,
+                                         valueBuf, emitSlot),
+                 "emit");
+        LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
+        // --- stable sort on the tile bits + ranges -------------------------------------------
         bool inAlt = false;
         LRT_CUDA(r,
                  lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), valueBuf,
                                       valueBuf != nullptr ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr,
-                                      counters + 1, r->pairCap, lowBits, keyBits, r->sortScratch.ptr, err, &inAlt,
-                                      stream),
-                 "pair sort");
+                                      counters + 1, r->pairCap, 32, tileBits, r->sortScratch.ptr, err, &inAlt, stream),
+                 "tile sort");
         sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
         if (valueBuf != nullptr) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;
         LRT_CUDA(r,
-                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 24 + lowBits,
-                                    static_cast<uint2*>(r->ranges.ptr), tiles, stream),
+                 lrt::launch_ranges(sorted, counters + 1, r->pairCap, 32, static_cast<uint2*>(r->ranges.ptr), tiles,
+                                    stream),
                  "ranges");
         LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
 
@@ -320,8 +337,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
             r->debug.ranges = r->ranges.ptr;
             r->debug.slots = slots;
             r->debug.tiles = tiles;
-            r->debug.slot_bits = lowBits;
-            r->debug.depth_bits = 24;
+            r->debug.slot_bits = 32u;
+            r->debug.depth_bits = 0u;
             r->debug.tile_bits = tileBits;
             r->pendingStream = stream;
             if (train) {
@@ -361,8 +378,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     r->debug.slots = slots;
     r->debug.pairs_count = pairs;
     r->debug.tiles = tiles;
-    r->debug.slot_bits = lowBits;
-    r->debug.depth_bits = 24;
+    r->debug.slot_bits = 32u;
+    r->debug.depth_bits = 0u;
     r->debug.tile_bits = tileBits;
     r->debug.visible = visible;
     r->trainReady = false;
@@ -384,7 +401,9 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         stats->pairs = pairs;
         if (s->time_stages) {
             stats->project_ms = event_ms(r->ev[0], r->ev[1]);
-            stats->tile_sort_ms = event_ms(r->ev[1], r->ev[2]);
+            stats->depth_sort_ms = event_ms(r->ev[1], r->ev[4]);
+            stats->emit_ms = event_ms(r->ev[4], r->ev[5]);
+            stats->tile_sort_ms = event_ms(r->ev[5], r->ev[2]);
             stats->blend_ms = event_ms(r->ev[2], r->ev[3]);
         }
         stats->total_ms =
@@ -903,7 +922,7 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
                                         static_cast<const float*>(p.log_scales), static_cast<const float*>(p.quats),
                                         static_cast<const float*>(p.opacity_logits),
                                         static_cast<const uint16_t*>(p.sh), static_cast<uint32_t*>(r->touched.ptr),
-                                        static_cast<uint32_t*>(r->trainOffsets.ptr),
+                                        static_cast<uint32_t*>(r->pairOffsets.ptr),
                                         static_cast<float*>(r->partials.ptr), r->trainPairs,
                                         static_cast<float*>(grads->means),
                                         static_cast<float*>(grads->log_scales), static_cast<float*>(grads->quats),

@@ -16,7 +16,8 @@
 //   4. scatters keys (and values) into shared memory in digit order, then
 //      writes them out so that consecutive threads write consecutive slots.
 // Only the key bits asked for are sorted: the pass count is ceil(bits / 8).
-// Key types: uint32 and uint64, with or without uint32 values.
+// Key types: uint32 and uint64, with or without uint32 values. The key count
+// is read on the device (at most `cap`), or is `cap` when no count is given.
 #include "kernels.cuh"
 #include "raster_common.cuh"
 
@@ -88,7 +89,7 @@ histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount
     __shared__ uint32_t sHist[kMaxPasses * kDigits];
     for (uint32_t i = threadIdx.x; i < passes * kDigits; i += blockDim.x) sHist[i] = 0;
     __syncthreads();
-    const uint32_t n = min(*dCount, cap);
+    const uint32_t n = dCount != nullptr ? min(*dCount, cap) : cap;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const K key = keys[i];
         for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p * kDigits + digit_of(key, firstBit + 8 * p)], 1u);
@@ -118,7 +119,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     if (tid == 0) sPart = atomicAdd(ticket, 1u);
     for (uint32_t i = tid; i < kSortWarps * kDigits; i += kSortThreads) (&sWarpHist[0][0])[i] = 0;
     __syncthreads();
-    const uint32_t n = min(*dCount, cap);
+    const uint32_t n = dCount != nullptr ? min(*dCount, cap) : cap;
     const uint32_t part = sPart;
     const uint32_t base = part * kSortTile;
     if (base >= n) return;

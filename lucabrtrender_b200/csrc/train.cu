@@ -23,33 +23,55 @@ __device__ constexpr float kC2[5] = {1.0925484305920792f, -1.0925484305920792f, 
 __device__ constexpr float kC3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f, 0.3731763325901154f,
                           -0.4570457994644658f, 1.445305721320277f, -0.5900435899266435f};
 
-// The 15 rest basis functions (sh.slang:25-51 order) and their gradients.
-__device__ __forceinline__ void sh_basis(float x, float y, float z, uint32_t degree, float (&b)[15], float (&gx)[15],
-                                         float (&gy)[15], float (&gz)[15]) {
-#pragma unroll
-    for (int k = 0; k < 15; ++k) b[k] = gx[k] = gy[k] = gz[k] = 0.0f;
-    if (degree == 0) return;
-    b[0] = -kC1 * y; gy[0] = -kC1;
-    b[1] = kC1 * z;  gz[1] = kC1;
-    b[2] = -kC1 * x; gx[2] = -kC1;
-    if (degree < 2) return;
+// Rest basis function k of sh.slang:25-51 (k in 0..14, in its order) at the
+// unit direction (x, y, z); k is a constant wherever these are called (the
+// callers' loops are unrolled), so each call is a short polynomial.
+__device__ __forceinline__ float sh_basis_at(int k, float x, float y, float z) {
     const float xx = x * x, yy = y * y, zz = z * z;
-    b[3] = kC2[0] * x * y;  gx[3] = kC2[0] * y; gy[3] = kC2[0] * x;
-    b[4] = kC2[1] * y * z;  gy[4] = kC2[1] * z; gz[4] = kC2[1] * y;
-    b[5] = kC2[2] * (2.0f * zz - xx - yy); gx[5] = -2.0f * kC2[2] * x; gy[5] = -2.0f * kC2[2] * y; gz[5] = 4.0f * kC2[2] * z;
-    b[6] = kC2[3] * x * z;  gx[6] = kC2[3] * z; gz[6] = kC2[3] * x;
-    b[7] = kC2[4] * (xx - yy); gx[7] = 2.0f * kC2[4] * x; gy[7] = -2.0f * kC2[4] * y;
-    if (degree < 3) return;
-    b[8] = kC3[0] * y * (3.0f * xx - yy);  gx[8] = 6.0f * kC3[0] * x * y; gy[8] = kC3[0] * (3.0f * xx - 3.0f * yy);
-    b[9] = kC3[1] * x * y * z; gx[9] = kC3[1] * y * z; gy[9] = kC3[1] * x * z; gz[9] = kC3[1] * x * y;
-    b[10] = kC3[2] * y * (4.0f * zz - xx - yy);
-    gx[10] = -2.0f * kC3[2] * x * y; gy[10] = kC3[2] * (4.0f * zz - xx - 3.0f * yy); gz[10] = 8.0f * kC3[2] * y * z;
-    b[11] = kC3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
-    gx[11] = -6.0f * kC3[3] * x * z; gy[11] = -6.0f * kC3[3] * y * z; gz[11] = kC3[3] * (6.0f * zz - 3.0f * xx - 3.0f * yy);
-    b[12] = kC3[4] * x * (4.0f * zz - xx - yy);
-    gx[12] = kC3[4] * (4.0f * zz - 3.0f * xx - yy); gy[12] = -2.0f * kC3[4] * x * y; gz[12] = 8.0f * kC3[4] * x * z;
-    b[13] = kC3[5] * z * (xx - yy); gx[13] = 2.0f * kC3[5] * x * z; gy[13] = -2.0f * kC3[5] * y * z; gz[13] = kC3[5] * (xx - yy);
-    b[14] = kC3[6] * x * (xx - 3.0f * yy); gx[14] = kC3[6] * (3.0f * xx - 3.0f * yy); gy[14] = -6.0f * kC3[6] * x * y;
+    switch (k) {
+        case 0: return -kC1 * y;
+        case 1: return kC1 * z;
+        case 2: return -kC1 * x;
+        case 3: return kC2[0] * x * y;
+        case 4: return kC2[1] * y * z;
+        case 5: return kC2[2] * (2.0f * zz - xx - yy);
+        case 6: return kC2[3] * x * z;
+        case 7: return kC2[4] * (xx - yy);
+        case 8: return kC3[0] * y * (3.0f * xx - yy);
+        case 9: return kC3[1] * x * y * z;
+        case 10: return kC3[2] * y * (4.0f * zz - xx - yy);
+        case 11: return kC3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+        case 12: return kC3[4] * x * (4.0f * zz - xx - yy);
+        case 13: return kC3[5] * z * (xx - yy);
+        default: return kC3[6] * x * (xx - 3.0f * yy);
+    }
+}
+
+// The same function and its gradient (d/dx, d/dy, d/dz).
+__device__ __forceinline__ void sh_basis_grad_at(int k, float x, float y, float z, float& b, float& gx, float& gy,
+                                                 float& gz) {
+    const float xx = x * x, yy = y * y, zz = z * z;
+    b = sh_basis_at(k, x, y, z);
+    gx = gy = gz = 0.0f;
+    switch (k) {
+        case 0: gy = -kC1; break;
+        case 1: gz = kC1; break;
+        case 2: gx = -kC1; break;
+        case 3: gx = kC2[0] * y; gy = kC2[0] * x; break;
+        case 4: gy = kC2[1] * z; gz = kC2[1] * y; break;
+        case 5: gx = -2.0f * kC2[2] * x; gy = -2.0f * kC2[2] * y; gz = 4.0f * kC2[2] * z; break;
+        case 6: gx = kC2[3] * z; gz = kC2[3] * x; break;
+        case 7: gx = 2.0f * kC2[4] * x; gy = -2.0f * kC2[4] * y; break;
+        case 8: gx = 6.0f * kC3[0] * x * y; gy = kC3[0] * (3.0f * xx - 3.0f * yy); break;
+        case 9: gx = kC3[1] * y * z; gy = kC3[1] * x * z; gz = kC3[1] * x * y; break;
+        case 10: gx = -2.0f * kC3[2] * x * y; gy = kC3[2] * (4.0f * zz - xx - 3.0f * yy); gz = 8.0f * kC3[2] * y * z; break;
+        case 11:
+            gx = -6.0f * kC3[3] * x * z; gy = -6.0f * kC3[3] * y * z; gz = kC3[3] * (6.0f * zz - 3.0f * xx - 3.0f * yy);
+            break;
+        case 12: gx = kC3[4] * (4.0f * zz - 3.0f * xx - yy); gy = -2.0f * kC3[4] * x * y; gz = 8.0f * kC3[4] * x * z; break;
+        case 13: gx = 2.0f * kC3[5] * x * z; gy = -2.0f * kC3[5] * y * z; gz = kC3[5] * (xx - yy); break;
+        default: gx = kC3[6] * (3.0f * xx - 3.0f * yy); gy = -6.0f * kC3[6] * x * y; break;
+    }
 }
 
 // A splat's partials summed in a fixed order. Splats with few pairs are summed
@@ -143,47 +165,62 @@ __device__ __forceinline__ void view_grads(const FrameParams& f, uint32_t i, con
     const float QA = c / det, QB = -b / det, QC = a / det;
 
     // ---- colour ---------------------------------------------------------------
-    float coef[48];   // the fp16 coefficients, read as six 16-byte vectors
+    // The fp16 coefficients stay packed (24 words, read as six 16-byte
+    // vectors) and are unpacked where used; each basis function and its
+    // gradient is formed where it is used, in two passes over the 15 rest
+    // functions (the rest sum, then the gradients), so that no 48-value
+    // arrays are held at once.
+    uint32_t cw[24];
     {
         const uint4* rv = reinterpret_cast<const uint4*>(sh + static_cast<size_t>(i) * 48);
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
             const uint4 w4 = __ldg(rv + q);
-            const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                coef[q * 8 + 2 * h] = low_half(ws[h]);
-                coef[q * 8 + 2 * h + 1] = high_half(ws[h]);
-            }
+            cw[4 * q] = w4.x;
+            cw[4 * q + 1] = w4.y;
+            cw[4 * q + 2] = w4.z;
+            cw[4 * q + 3] = w4.w;
         }
     }
+    auto coef = [&](int q) { return (q & 1) != 0 ? high_half(cw[q >> 1]) : low_half(cw[q >> 1]); };
     float vx = px - f.eye[0], vy = py - f.eye[1], vz = pz - f.eye[2];
     const float vl = sqrtf(vx * vx + vy * vy + vz * vz);
     const float dirx = vx / vl, diry = vy / vl, dirz = vz / vl;
-    const uint32_t degree = min(3u, f.shLimit);   // bas[] is 0 above it
-    float bas[15], bgx[15], bgy[15], bgz[15];
-    sh_basis(dirx, diry, dirz, degree, bas, bgx, bgy, bgz);
-    float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
+    const uint32_t degree = min(3u, f.shLimit);   // basis functions above it are 0
+    const int used = degree == 0 ? 0 : degree == 1 ? 3 : degree == 2 ? 8 : 15;
+    constexpr float kSH0 = 0.28209479177387814f;
+    float rest[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        if (k < used) {
+            const float b = sh_basis_at(k, dirx, diry, dirz);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) rest[ch] += b * coef(3 + 3 * k + ch);
+        }
+    }
+    // colour = max(base + rest, 0): no gradient where clamped. Basis
+    // functions above the evaluated degree are 0, so their coefficients get 0.
+    float gcol[3];
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
-        constexpr float kSH0 = 0.28209479177387814f;
-        const float base = 0.5f + kSH0 * coef[ch];
-        float rest = 0.0f;
+        const float base = 0.5f + kSH0 * coef(ch);
+        gcol[ch] = base + rest[ch] > 0.0f ? g[6 + ch] : 0.0f;
+        sink(ch, kSH0 * gcol[ch]);
+    }
+    float gdx = 0.0f, gdy = 0.0f, gdz = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 15; ++k) rest += bas[k] * coef[3 + 3 * k + ch];
-        // colour = max(base + rest, 0): no gradient where clamped. Basis
-        // functions above the evaluated degree are 0, so their
-        // coefficients get 0.
-        const float gcol = base + rest > 0.0f ? g[6 + ch] : 0.0f;
-        sink(ch, kSH0 * gcol);
+    for (int k = 0; k < 15; ++k) {
+        float b = 0.0f, bx = 0.0f, by = 0.0f, bz = 0.0f;
+        if (k < used) sh_basis_grad_at(k, dirx, diry, dirz, b, bx, by, bz);
+        float cg = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 15; ++k) {
-            sink(3 + 3 * k + ch, bas[k] * gcol);
-            const float cg = coef[3 + 3 * k + ch] * gcol;
-            gdx += cg * bgx[k];
-            gdy += cg * bgy[k];
-            gdz += cg * bgz[k];
+        for (int ch = 0; ch < 3; ++ch) {
+            sink(3 + 3 * k + ch, b * gcol[ch]);
+            cg += coef(3 + 3 * k + ch) * gcol[ch];
         }
+        gdx += cg * bx;
+        gdy += cg * by;
+        gdz += cg * bz;
     }
     {   // dir = v / |v|, v = p - eye
         const float dotd = gdx * dirx + gdy * diry + gdz * dirz;
@@ -332,13 +369,14 @@ __device__ __forceinline__ void splat_partials(uint32_t count, uint32_t firstRaw
 
 // One frame: every splat's gradients written (zero for a splat the frame
 // does not touch).
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 5)
 splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
                       const float* __restrict__ quats, const float* __restrict__ logits,
                       const uint16_t* __restrict__ sh, const uint32_t* __restrict__ touched,
                       const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
                       uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
                       float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh) {
+    __shared__ float sGsh[48][kThreads];
     const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const bool live = i < f.count;
@@ -367,12 +405,15 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
 #pragma unroll
         for (int q = 0; q < 12; ++q) out[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
-        float gsh[48];
+        // The 48 SH gradients go through shared memory (a column per thread)
+        // rather than registers, then out as 16-byte stores.
         view_grads(f, i, means, logScales, quats, logits, sh, g, gm, gls, gq, glog,
-                   [&](int q, float v) { gsh[q] = v; });
+                   [&](int q, float v) { sGsh[q][threadIdx.x] = v; });
         float4* out = reinterpret_cast<float4*>(gshRow);
 #pragma unroll
-        for (int q = 0; q < 12; ++q) out[q] = make_float4(gsh[4 * q], gsh[4 * q + 1], gsh[4 * q + 2], gsh[4 * q + 3]);
+        for (int q = 0; q < 12; ++q)
+            out[q] = make_float4(sGsh[4 * q][threadIdx.x], sGsh[4 * q + 1][threadIdx.x], sGsh[4 * q + 2][threadIdx.x],
+                                 sGsh[4 * q + 3][threadIdx.x]);
     }
     for (int k = 0; k < 3; ++k) {
         gMeans[3 * i + k] = gm[k];
@@ -457,13 +498,16 @@ splat_backward_views_kernel(const FrameParams* __restrict__ frames, uint32_t vie
         if (!live || n == 0) continue;
         float gm[3] = {0, 0, 0}, gls[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0}, glog = 0.0f;
         view_grads(f, i, means, logScales, quats, logits, sh, g, gm, gls, gq, glog,
-                   [&](int q, float x) { sAcc[q][tid] = sAcc[q][tid] + x; });
+                   [&](int q, float x) { sAcc[q][tid] = __fadd_rn(sAcc[q][tid], x); });
+        // The running sums are plain rounded additions (never fused with the
+        // product that formed a term), so that they equal the single-view
+        // gradients summed in view order.
         for (int k = 0; k < 3; ++k) {
-            am[k] = am[k] + gm[k];
-            als[k] = als[k] + gls[k];
+            am[k] = __fadd_rn(am[k], gm[k]);
+            als[k] = __fadd_rn(als[k], gls[k]);
         }
-        for (int k = 0; k < 4; ++k) aq[k] = aq[k] + gq[k];
-        alog = alog + glog;
+        for (int k = 0; k < 4; ++k) aq[k] = __fadd_rn(aq[k], gq[k]);
+        alog = __fadd_rn(alog, glog);
     }
     if (!live) return;
     for (int k = 0; k < 3; ++k) {

@@ -141,7 +141,7 @@ int reserve_step(lrt_rast* r, const StepArgs& a, const Layout& L, uint32_t cap) 
     const uint32_t keyBits = 24 + bits_for(L.maxTiles);
     LRT_CUDA(r, ensure_tb(r, r->proj, slots * sizeof(ProjRecord)), "splat records");
     LRT_CUDA(r, ensure_tb(r, r->touched, slots * 4), "touched counts");
-    LRT_CUDA(r, ensure_tb(r, r->trainOffsets, slots * 4), "pair offsets");
+    LRT_CUDA(r, ensure_tb(r, r->pairOffsets, slots * 4), "pair offsets");
     LRT_CUDA(r, ensure_tb(r, r->pixState, L.maxPixels * 16), "pixel state");
     LRT_CUDA(r, ensure_tb(r, r->pixLast, L.maxPixels * 4), "pixel state");
     LRT_CUDA(r, ensure_tb(r, r->trainBatchGrad, L.maxPixels * 16), "colour gradients");
@@ -241,7 +241,7 @@ int enqueue_step(lrt_rast* r, const StepArgs& a, const Layout& L, uint32_t cap, 
                      lrt::launch_project_emit_train(
                          L.frames[v], means, logScales, quats, logits, sh, static_cast<ProjRecord*>(r->proj.ptr),
                          nullptr, static_cast<uint32_t*>(r->touched.ptr), nullptr,
-                         static_cast<uint32_t*>(r->trainOffsets.ptr) + size_t{k} * n, counters, status, tickets + k,
+                         static_cast<uint32_t*>(r->pairOffsets.ptr) + size_t{k} * n, counters, status, tickets + k,
                          partitionBase, lastPartition, slotBits, pairBuf, valueBuf, nullptr, cap, st, devFrames + v),
                      "project");
             partitionBase += lrt::project_partitions(n);
@@ -290,7 +290,7 @@ int enqueue_step(lrt_rast* r, const StepArgs& a, const Layout& L, uint32_t cap, 
                      lrt::launch_splat_backward_views(
                          devFrames + v0 + b0, bn, n, means, logScales, quats, logits, sh,
                          static_cast<uint32_t*>(r->touched.ptr) + size_t{b0} * n,
-                         static_cast<uint32_t*>(r->trainOffsets.ptr) + size_t{b0} * n,
+                         static_cast<uint32_t*>(r->pairOffsets.ptr) + size_t{b0} * n,
                          static_cast<float*>(r->partials.ptr), cap, static_cast<float*>(a.grads->means),
                          static_cast<float*>(a.grads->log_scales), static_cast<float*>(a.grads->quats),
                          static_cast<float*>(a.grads->opacity_logits), static_cast<float*>(a.grads->sh),
@@ -324,7 +324,7 @@ uint64_t step_key(const lrt_rast* r, const StepArgs& a, const Layout& L, uint32_
     }
     // The handle's buffers, which single-view steps and frames share and can
     // move between batches.
-    for (const DeviceBuffer* b : {&r->proj, &r->touched, &r->trainOffsets, &r->pixState, &r->pixLast,
+    for (const DeviceBuffer* b : {&r->proj, &r->touched, &r->pairOffsets, &r->pixState, &r->pixLast,
                                   &r->trainBatchGrad, &r->trainBatchViews, &r->trainBatchLoss, &r->lossScratch,
                                   &r->scanScratch, &r->ranges, &r->pairs, &r->pairsAlt, &r->pairValues,
                                   &r->pairValuesAlt, &r->sortScratch, &r->partials, &r->trainBatch.counters})

@@ -426,6 +426,7 @@ class TileRasterizer:
             "pairs": grab(v.pairs, v.pairs_count, torch.int64),
             "ranges": grab(v.ranges, v.tiles, torch.int32, 2),
             "slot_bits": v.slot_bits,
+            "depth_bits": v.depth_bits,
             "tile_bits": v.tile_bits,
             "visible": v.visible,
         }

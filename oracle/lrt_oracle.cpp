@@ -887,6 +887,7 @@ void ora_math_eval(int fn, const float* x, float* y, uint32_t n) {
     for (uint32_t i = 0; i < n; ++i) {
         switch (fn) {
             case 0: y[i] = expImpl(x[i]); break;
+            case 6: y[i] = expImpl(x[i]); break;   // the device's in-range form, -87 <= x <= 88
             case 1: y[i] = logImpl(x[i]); break;
             case 2: y[i] = srgbToLinear(x[i]); break;
             case 3: y[i] = cutoffPower(x[i]); break;

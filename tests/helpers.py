@@ -166,11 +166,16 @@ def synthetic_scene(count: int, width: int, height: int, seed: int = 1, eye=(0.0
                  settings(width=width, height=height))
 
 
-def pair_words_to_tile_slot(words: np.ndarray, slot_bits: int):
+def pair_words_to_tile_slot(words: np.ndarray, slot_bits: int, depth_bits: int = 24):
+    """A sorted pair word is tile << (depth_bits + slot_bits) | depth key <<
+    slot_bits | slot: training frames carry the 24-bit depth key, other
+    frames (depth_bits 0) only tile << 32 | slot. keys is None without one."""
     w = words.astype(np.uint64)
     slots = (w & np.uint64((1 << slot_bits) - 1)).astype(np.uint32)
-    keys = ((w >> np.uint64(slot_bits)) & np.uint64(0xFFFFFF)).astype(np.uint32)
-    tiles = (w >> np.uint64(24 + slot_bits)).astype(np.uint32)
+    keys = None
+    if depth_bits:
+        keys = ((w >> np.uint64(slot_bits)) & np.uint64((1 << depth_bits) - 1)).astype(np.uint32)
+    tiles = (w >> np.uint64(depth_bits + slot_bits)).astype(np.uint32)
     return tiles, keys, slots
 
 

@@ -56,7 +56,7 @@ def test_a_filtered_frame_equals_the_oracle_and_an_unfiltered_one_is_unchanged(r
     ref = ora.render(scene.projection().struct(), [(host, np.eye(4), None)], scene.settings.struct(), 0)
     assert stats.pairs == ref["pairs"]
     assert np.array_equal(dbg["proj"].cpu().numpy().view(np.uint32), ref["proj"].view(np.uint32))
-    tiles, _, slots = H.pair_words_to_tile_slot(dbg["pairs"].cpu().numpy().view(np.uint64), dbg["slot_bits"])
+    tiles, _, slots = H.pair_words_to_tile_slot(dbg["pairs"].cpu().numpy().view(np.uint64), dbg["slot_bits"], dbg["depth_bits"])
     assert np.array_equal(tiles, ref["pair_tiles"]) and np.array_equal(slots, ref["pair_slots"])
     assert np.abs(targets.colour.cpu().numpy() - ref["colour"]).max() <= 1e-5
     # the filter changed the frame; the same cloud without it renders as before

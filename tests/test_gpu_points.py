@@ -37,7 +37,7 @@ def check_frame(rasterizer, out, ref, targets):
     assert np.array_equal(dbg["touched"].cpu().numpy().view(np.uint32), ref["touched"])
     assert np.array_equal(dbg["depth_keys"].cpu().numpy().view(np.uint32), ref["depth_keys"])
     assert np.array_equal(dbg["ranges"].cpu().numpy().view(np.uint32), ref["ranges"])
-    tiles, slots = H.pair_words_to_tile_slot(dbg["pairs"].cpu().numpy().view(np.uint64), dbg["slot_bits"])[::2]
+    tiles, slots = H.pair_words_to_tile_slot(dbg["pairs"].cpu().numpy().view(np.uint64), dbg["slot_bits"], dbg["depth_bits"])[::2]
     assert np.array_equal(tiles, ref["pair_tiles"]) and np.array_equal(slots, ref["pair_slots"])
     assert np.array_equal(targets.colour.cpu().numpy().view(np.uint32), ref["colour"].view(np.uint32))
     assert np.array_equal(targets.depth.cpu().numpy().view(np.uint32), ref["depth"].view(np.uint32))

@@ -25,15 +25,17 @@ def test_the_sort_heavy_frame_keeps_every_invariant(rasterizer):
     stats = rasterizer.render(cam, [L.SplatInstance(cloud)], settings, a)
     dbg = rasterizer.debug_arrays()
     words = dbg["pairs"].cpu().numpy().view(np.uint64)
-    sb = dbg["slot_bits"]
+    sb, db = dbg["slot_bits"], dbg["depth_bits"]
     assert stats.pairs == words.size > 50_000_000
     assert int(dbg["touched"].cpu().numpy().astype(np.int64).sum()) == words.size
-    key = words >> np.uint64(sb)
+    slots = words & np.uint64((1 << sb) - 1)
+    tiles = (words >> np.uint64(db + sb)).astype(np.int64)
+    # (tile, 24-bit depth key, slot) ascending
+    depth = dbg["depth_keys"].cpu().numpy().view(np.uint32)[slots.astype(np.int64)].astype(np.uint64)
+    key = (tiles.astype(np.uint64) << np.uint64(24)) | depth
     assert np.all(key[1:] >= key[:-1])
     ties = key[1:] == key[:-1]
-    slots = words & np.uint64((1 << sb) - 1)
     assert np.all(slots[1:][ties] > slots[:-1][ties])
-    tiles = (words >> np.uint64(24 + sb)).astype(np.int64)
     ranges = dbg["ranges"].cpu().numpy().astype(np.int64)
     lengths = ranges[:, 1] - ranges[:, 0]
     assert lengths.sum() == words.size and np.all(lengths >= 0)
