@@ -364,10 +364,12 @@ int lrt_rast_train_forward(lrt_rast* rast, const lrt_projection* projection, con
  * (device); gradients of the parameters are written to `grads`. A
  * reverse-order re-blend per pixel, per-pair partials written at each pair's
  * emit index, then a per-splat ordered sum and the projection's chain rule:
- * no atomics. */
+ * no atomics. It waits only for an enqueued forward's counts (to report an
+ * overflow before reading its pairs) and returns once its kernels are
+ * enqueued on `stream`: the gradients are ready in that stream's order. */
 int lrt_rast_train_backward(lrt_rast* rast, const void* grad_colour, lrt_train_grads* grads, void* stream);
 /* CUDA-event times of the last backward: the blend backward and the
- * per-splat reduction + projection backward. */
+ * per-splat reduction + projection backward (waits for the backward). */
 int lrt_rast_backward_times(const lrt_rast* rast, double* blend_ms, double* project_ms);
 
 /* One view of a training batch: a batch view (its images written by the

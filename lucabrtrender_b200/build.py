@@ -60,7 +60,8 @@ def _compile(src: Path, obj: Path, verbose_ptxas: bool) -> None:
 def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     OBJ_DIR.mkdir(parents=True, exist_ok=True)
     LIB_DIR.mkdir(parents=True, exist_ok=True)
-    newest_header = max(p.stat().st_mtime for p in _headers())
+    # The headers and this file (its flags) are inputs of every object.
+    newest_header = max([p.stat().st_mtime for p in _headers()] + [Path(__file__).stat().st_mtime])
     jobs = []
     objs = []
     for name in SOURCES:

@@ -290,7 +290,7 @@ struct TrainOutputs {
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
-constexpr uint32_t kWarpArea = 512;   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
+constexpr uint32_t kWarpArea = 128;   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
 
 // ---- Splats of more than kSmallArea tiles, one tile row at a time ----
 //
@@ -614,8 +614,9 @@ __device__ __noinline__ void count_large_rows(const Footprint* foot, const uint3
 
 // The pairs of the block's large, unmasked splats whose rows are single runs:
 // a chunk of 256 rows at a time, each row's count and first column from its
-// row plan (as when counting), flattened so that consecutive threads write
-// consecutive pairs. takenStart[t]: the pairs of such splats before splat t.
+// row plan (as when counting) and its pairs' place among the chunk's by a
+// block scan; then each warp writes whole rows, its lanes on consecutive
+// pairs of a row. takenStart[t]: the pairs of such splats before splat t.
 // slotOf[t]: the slot of the block's splat t (null: slotBase + t).
 template <class Sink>
 __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
@@ -626,6 +627,7 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
                                              uint32_t* scanScratch, unsigned long long blockBase, uint32_t tileShift,
                                              uint32_t slotBase, const uint32_t* slotOf, const Sink& sink) {
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u, warp = tid >> 5;
     uint32_t fs = 0;
     {
         uint32_t lo = 0, hi = bigTotal;
@@ -657,18 +659,18 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
         rowMeta[tid] = meta;
         if (tid == 0) rowOff[kProjectThreads] = chunkTotal;
         __syncthreads();
-        for (uint32_t k = tid; k < chunkTotal; k += kProjectThreads) {
-            uint32_t lo = 0, hi = kProjectThreads;   // the last row q with rowOff[q] <= k
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (rowOff[mid] <= k) lo = mid; else hi = mid;
-            }
-            const uint32_t q = lo;
+        const uint32_t rows = min(kProjectThreads, rowsTotal - c0);
+        for (uint32_t q = warp; q < rows; q += kProjectThreads / 32) {
+            const uint32_t o = rowOff[q], n = rowOff[q + 1] - o;
+            if (n == 0) continue;
             const uint32_t ty = rowMeta[q] & 0xFFFFu, owner = rowMeta[q] >> 16;
-            const uint32_t tx = rowFirst[q] + (k - rowOff[q]);
-            sink.put(blockBase + start[owner] + (carry + k - takenStart[owner]),
-                     (static_cast<unsigned long long>(tileBase + ty * tilesX + tx) << tileShift) | low[owner],
-                     slotOf != nullptr ? slotOf[owner] : slotBase + owner);
+            const uint32_t tx0 = rowFirst[q];
+            const unsigned long long at = blockBase + start[owner] + (carry + o - takenStart[owner]);
+            const unsigned long long word0 = (static_cast<unsigned long long>(tileBase + ty * tilesX) << tileShift) |
+                                             low[owner];
+            const uint32_t slot = slotOf != nullptr ? slotOf[owner] : slotBase + owner;
+            for (uint32_t k = lane; k < n; k += 32)
+                sink.put(at + k, word0 + (static_cast<unsigned long long>(tx0 + k) << tileShift), slot);
         }
         carry += chunkTotal;
         __syncthreads();
@@ -1096,20 +1098,14 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
 
     // Offsets: block scan, then decoupled look-back over the frame's partitions.
-    uint32_t blockTotal = 0, smallTotal = 0;
+    uint32_t blockTotal = 0;
     const uint32_t start = block_exclusive_scan(touched, sScan, &blockTotal);
-    const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
     sStart[tid] = start;
-    sSmallStart[tid] = smallStart;
     const bool writeOffset = train.offsets != nullptr && inRange;
-    sMask[tid] = mask;
     sLow[tid] = static_cast<unsigned long long>(key) << lowBits;
     sRect[tid] = rect.x | (rect.y << 16);
     sWidth[tid] = rw | (sh << 16) | (irregular ? 0x80000000u : 0u);
-    if (tid == 0) {
-        sStart[kProjectThreads] = blockTotal;
-        sSmallStart[kProjectThreads] = smallTotal;
-    }
+    if (tid == 0) sStart[kProjectThreads] = blockTotal;
     if (tid < 32) sBase = frame_lookback(status, partitionBase + part, lastPartition, blockTotal, counters, err);
     __syncthreads();
     const unsigned long long blockBase = sBase;
@@ -1118,21 +1114,49 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     const uint32_t tileShift = 24 + lowBits;
     const uint32_t slotBase = slot - tid;   // the slot of the block's first splat
 
-    // Masked splats: the whole block writes their pairs, one per thread per step.
-    for (uint32_t j = tid; j < smallTotal; j += kProjectThreads) {
-        uint32_t lo = 0, hi = kProjectThreads;   // the splat s with sSmallStart[s] <= j < sSmallStart[s + 1]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (sSmallStart[mid] <= j) lo = mid; else hi = mid;
+    // Masked splats: each warp writes its own splats' pairs, 32 at a time,
+    // consecutive lanes on consecutive pairs (a warp's splats' pairs follow
+    // one another, so the writes are contiguous). A lane finds its pair's
+    // splat by a binary search over the warp's running pair counts
+    // (shuffles: the last lane whose count starts at or before the pair,
+    // which always has pairs), and the tile as that splat's mask bit of the
+    // same rank.
+    {
+        const uint32_t mine = masked ? touched : 0u;
+        uint32_t incl = mine;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += o;
         }
-        const uint32_t s = lo;
-        const uint32_t bit = nth_set_bit(sMask[s], j - sSmallStart[s]);
-        const uint32_t bsh = (sWidth[s] >> 16) & 0xFFu;
-        const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
-        const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
-        sink.put(blockBase + sStart[s] + (j - sSmallStart[s]),
-                 (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | sLow[s],
-                 slotBase + s);
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - mine;
+        const uint32_t mRect = rect.x | (rect.y << 16);
+        const unsigned long long mLow = static_cast<unsigned long long>(key) << lowBits;
+        const uint32_t warpBase = slotBase + (tid & ~31u);
+        for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+            const uint32_t pos = c0 + lane;
+            uint32_t l = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l + step));
+                if (e <= pos) l += step;
+            }
+            const uint32_t r = pos - __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l));
+            const unsigned long long m = __shfl_sync(0xFFFFFFFFu, mask, static_cast<int>(l));
+            const uint32_t oRect = __shfl_sync(0xFFFFFFFFu, mRect, static_cast<int>(l));
+            const uint32_t oSh = __shfl_sync(0xFFFFFFFFu, sh, static_cast<int>(l));
+            const uint32_t oStart = __shfl_sync(0xFFFFFFFFu, start, static_cast<int>(l));
+            const unsigned long long oLow = __shfl_sync(0xFFFFFFFFu, mLow, static_cast<int>(l));
+            if (pos < total) {
+                const uint32_t bit = nth_set_bit(m, r);
+                const uint32_t tx = (oRect & 0xFFFFu) + (bit & ((1u << oSh) - 1u));
+                const uint32_t ty = (oRect >> 16) + (bit >> oSh);
+                sink.put(blockBase + oStart + r,
+                         (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | oLow,
+                         warpBase + l);
+            }
+        }
     }
     // The rest (rectangles too large for a mask): the block writes their
     // pairs a chunk of 256 tile rows at a time, each row's count and first
@@ -1140,7 +1164,6 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     // that consecutive threads write consecutive pairs. A splat's rows are in
     // order, so its pairs follow one another from its offset.
     if (rowsTotal != 0) {
-        __syncthreads();   // the masked writes are done with sSmallStart
         // Only the splats the rows walk (those in sFoot): their pairs' offsets
         // among the rows' pairs.
         const bool taken = touched != 0 && !masked && !irregular && area > kWarpArea;
@@ -1181,7 +1204,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
 // is [offset, offset + touched)) and a way back from every pair to its emit
 // index: the word's low field itself, with an emit index -> slot map
 // (train.emitSlot), or a sort value beside a slot (train.values).
-constexpr uint32_t kOffsetItems = 4;   // depth positions a thread
+constexpr uint32_t kOffsetItems = 16;   // depth positions a thread
 
 __global__ void __launch_bounds__(kProjectThreads)
 depth_offsets_kernel(const unsigned long long* __restrict__ sortedWords, uint32_t n,
@@ -1230,7 +1253,6 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];
-    __shared__ unsigned long long sMask[kProjectThreads];
     __shared__ unsigned long long sLow[kProjectThreads];
     __shared__ uint32_t sRect[kProjectThreads];
     __shared__ uint32_t sWidth[kProjectThreads];
@@ -1267,36 +1289,56 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
         sFootRow[bigIdx] = rowStart;
     }
     if (tid == 0) sFootRow[bigTotal] = rowsTotal;
-    uint32_t smallTotal = 0;
-    const uint32_t smallStart = block_exclusive_scan(masked ? touched : 0u, sScan, &smallTotal);
-    sStart[tid] = alive ? __ldg(offsets + slot) : 0u;
-    sSmallStart[tid] = smallStart;
-    sMask[tid] = masked ? a : 0ull;
+    const uint32_t first = alive ? __ldg(offsets + slot) : 0u;
+    sStart[tid] = first;
     sLow[tid] = 0ull;
     sRect[tid] = rect.x | (rect.y << 16);
     sWidth[tid] = rw | (sh << 16) | (irregular ? 0x80000000u : 0u);
-    if (tid == 0) sSmallStart[kProjectThreads] = smallTotal;
     __syncthreads();
     const PairSink sink{pairs, train.values, train.emitSlot, capacity, err};
     constexpr uint32_t tileShift = 32;
 
-    // Masked splats: the whole block writes their pairs, one per thread per step.
-    for (uint32_t j = tid; j < smallTotal; j += kProjectThreads) {
-        uint32_t lo = 0, hi = kProjectThreads;   // the splat s with sSmallStart[s] <= j < sSmallStart[s + 1]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (sSmallStart[mid] <= j) lo = mid; else hi = mid;
+    // Masked splats: each warp writes its own splats' pairs, 32 at a time,
+    // consecutive lanes on consecutive pairs. A lane finds its pair's splat by
+    // a binary search over the warp's running pair counts (shuffles: the
+    // last lane whose count starts at or before the pair, which always has
+    // pairs), and the pair's tile as that splat's mask bit of the same rank.
+    {
+        const uint32_t lane = tid & 31u;
+        const uint32_t mine = masked ? touched : 0u;
+        uint32_t incl = mine;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += o;
         }
-        const uint32_t s = lo;
-        const uint32_t bit = nth_set_bit(sMask[s], j - sSmallStart[s]);
-        const uint32_t bsh = (sWidth[s] >> 16) & 0xFFu;
-        const uint32_t tx = (sRect[s] & 0xFFFFu) + (bit & ((1u << bsh) - 1u));
-        const uint32_t ty = (sRect[s] >> 16) + (bit >> bsh);
-        sink.put(static_cast<unsigned long long>(sStart[s]) + (j - sSmallStart[s]),
-                 static_cast<unsigned long long>(ty * tilesX + tx) << tileShift, slotBase + s);
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - mine;
+        const uint32_t mRect = rect.x | (rect.y << 16);
+        const uint32_t warpBase = slotBase + (tid & ~31u);
+        for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+            const uint32_t pos = c0 + lane;
+            uint32_t l = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l + step));
+                if (e <= pos) l += step;
+            }
+            const uint32_t r = pos - __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l));
+            const unsigned long long m = __shfl_sync(0xFFFFFFFFu, a, static_cast<int>(l));
+            const uint32_t oRect = __shfl_sync(0xFFFFFFFFu, mRect, static_cast<int>(l));
+            const uint32_t oSh = __shfl_sync(0xFFFFFFFFu, sh, static_cast<int>(l));
+            const uint32_t oFirst = __shfl_sync(0xFFFFFFFFu, first, static_cast<int>(l));
+            if (pos < total) {
+                const uint32_t bit = nth_set_bit(m, r);
+                const uint32_t tx = (oRect & 0xFFFFu) + (bit & ((1u << oSh) - 1u));
+                const uint32_t ty = (oRect >> 16) + (bit >> oSh);
+                sink.put(static_cast<unsigned long long>(oFirst) + r,
+                         static_cast<unsigned long long>(ty * tilesX + tx) << tileShift, warpBase + l);
+            }
+        }
     }
     if (rowsTotal != 0) {
-        __syncthreads();   // the masked writes are done with sSmallStart
         uint32_t takenTotal = 0;
         sSmallStart[tid] = block_exclusive_scan(rowsHere ? touched : 0u, sScan, &takenTotal);
         __syncthreads();

@@ -39,7 +39,9 @@ struct lrt_rast {
     lrt::SortFault sortFault;                            // lrt_radix_sort's planted fault (tests only)
     DeviceBuffer filterCameras, filterScratch;           // lrt_rast_filter3d's cameras and lowest rate
     uint32_t* hostCounters = nullptr;                    // pinned
-    cudaEvent_t ev[8] = {};
+    // ev[0..5]: a frame's stage times; ev[6]: an enqueued training frame's
+    // counts copied to the host; ev[7..9]: the training backward's times.
+    cudaEvent_t ev[10] = {};
     uint32_t splatCap = 0, pairCap = 0, tileCap = 0;
     lrt_debug_view debug{};
     // Training: what the backward pass needs from its forward.
@@ -66,7 +68,7 @@ struct lrt_rast {
     const uint32_t* trainSortedValues = nullptr;   // emit index per sorted pair (value layout)
     const uint32_t* trainEmitSlot = nullptr;       // slot per emit index (low-field layout)
     uint32_t trainPairs = 0;
-    double lastBackwardMs[2] = {0.0, 0.0};
+    bool backwardTimed = false;   // ev[7..9] hold a training backward's times
     // Plain frames enqueued by lrt_rast_render_async: their counts land in a
     // ring of pinned slots, each with the event that marks its frame done.
     static constexpr uint32_t kRing = 16;

@@ -58,6 +58,7 @@ int lrt_rast_create(lrt_rast** out, int device) {
 void lrt_rast_destroy(lrt_rast* r) {
     if (r == nullptr) return;
     DeviceScope scope(r->device);
+    if (r->frameDoneSet) cudaEventSynchronize(r->frameDone);   // a backward may still read the buffers
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
                             &r->algoValsAlt, &r->depthWords, &r->depthWordsAlt, &r->splatAux, &r->pairValues, &r->pairValuesAlt, &r->pairOffsets, &r->pixState,
@@ -341,6 +342,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
             r->debug.depth_bits = 0u;
             r->debug.tile_bits = tileBits;
             r->pendingStream = stream;
+            if (train) LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
             if (train) {
                 r->trainFrame = lastParams;
                 r->trainBlend = bp;
@@ -904,11 +906,20 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
         return fail(r, LRT_INVALID_ARGUMENT, "the SH gradient must be 16-byte aligned");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    if (r->trainPending) {
+        // The forward ran without waiting: wait for its counts only (its
+        // copy to the host is done; the loss kernels after it may still
+        // run), so that an overflow or timeout is reported before anything
+        // reads its pairs.
+        LRT_CUDA(r, cudaEventSynchronize(r->ev[6]), "frame");
+        const int code = settle_pending_frame(r);
+        if (code != LRT_OK) return code;
+    }
     // Every pair's partials are written by the blend backward (zeros for those
     // it does not walk), so the buffer is not cleared.
     const size_t partialBytes = std::max<size_t>(size_t{r->trainPairs} * 12 * sizeof(float), 16);
     LRT_CUDA(r, ensure(r->partials, partialBytes), "partials");
-    LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
+    LRT_CUDA(r, cudaEventRecord(r->ev[7], stream), "event");
     LRT_CUDA(r,
              lrt::launch_blend_backward(r->trainBlend, static_cast<uint2*>(r->ranges.ptr), r->trainSorted,
                                         r->trainSortedValues, r->trainEmitSlot, static_cast<ProjRecord*>(r->proj.ptr),
@@ -916,7 +927,7 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
                                         static_cast<const float4*>(gradColour), static_cast<float*>(r->partials.ptr),
                                         stream),
              "blend backward");
-    LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
+    LRT_CUDA(r, cudaEventRecord(r->ev[8], stream), "event");
     LRT_CUDA(r,
              lrt::launch_splat_backward(r->trainFrame, static_cast<const float*>(p.means),
                                         static_cast<const float*>(p.log_scales), static_cast<const float*>(p.quats),
@@ -929,21 +940,24 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
                                         static_cast<float*>(grads->opacity_logits), static_cast<float*>(grads->sh),
                                         stream),
              "projection backward");
-    LRT_CUDA(r, cudaEventRecord(r->ev[6], stream), "event");
-    LRT_CUDA(r, cudaStreamSynchronize(stream), "backward");
-    if (r->trainPending) {   // the forward ran without waiting: its status is read here
-        const int code = settle_pending_frame(r);
-        if (code != LRT_OK) return code;
-    }
-    r->lastBackwardMs[0] = event_ms(r->ev[4], r->ev[5]);
-    r->lastBackwardMs[1] = event_ms(r->ev[5], r->ev[6]);
+    LRT_CUDA(r, cudaEventRecord(r->ev[9], stream), "event");
+    // No wait here: the gradients are ready in stream order. Later calls on
+    // the handle (any stream) wait for this event before touching its buffers.
+    LRT_CUDA(r, cudaEventRecord(r->frameDone, stream), "event");
+    r->frameDoneSet = true;
+    r->backwardTimed = true;
     return LRT_OK;
 }
 
 int lrt_rast_backward_times(const lrt_rast* r, double* blendMs, double* projectMs) {
     if (r == nullptr || blendMs == nullptr || projectMs == nullptr) return LRT_INVALID_ARGUMENT;
-    *blendMs = r->lastBackwardMs[0];
-    *projectMs = r->lastBackwardMs[1];
+    *blendMs = 0.0;
+    *projectMs = 0.0;
+    if (!r->backwardTimed) return LRT_OK;
+    DeviceScope scope(r->device);
+    if (cudaEventSynchronize(r->ev[9]) != cudaSuccess) return LRT_DEVICE_FAILURE;
+    *blendMs = event_ms(r->ev[7], r->ev[8]);
+    *projectMs = event_ms(r->ev[8], r->ev[9]);
     return LRT_OK;
 }
 

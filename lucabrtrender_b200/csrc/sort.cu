@@ -7,7 +7,8 @@
 //
 // Here a sort is one histogram kernel that reads the keys once and counts
 // every pass's digits, then one kernel per 8-bit digit that:
-//   1. takes the next 3072-key partition by atomic ticket (launch order),
+//   1. takes the next partition (3072 keys, 4096 in sorts of more than 2^23
+//      keys) by atomic ticket (launch order),
 //   2. ranks its keys stably inside each warp with __match_any_sync (keys are
 //      warp-striped, so a warp's item j covers 32 consecutive keys and items
 //      are visited in order), and across warps with per-warp digit counts,
@@ -30,6 +31,13 @@ constexpr uint32_t kSortThreads = 256;
 constexpr uint32_t kSortWarps = kSortThreads / 32;
 constexpr uint32_t kSortItems = 12;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+// Sorts of more than kLargeKeys keys take kLargeItems keys a thread: fewer,
+// longer partitions (measured: the 256M-pair tile sort of a 6M-splat 4K
+// frame 5.36 against 5.79 ms), while smaller sorts keep 12 (16 was slower
+// for the 1M-slot depth sort).
+constexpr uint32_t kLargeItems = 16;
+constexpr uint32_t kLargeKeys = 1u << 23;
+constexpr uint32_t kLargeTile = kSortThreads * kLargeItems;
 constexpr uint32_t kDigits = 256;
 // A look-back word holds a digit's running count and, in its top bits, the
 // status (aggregate or inclusive). Sorts of fewer than 2^30 keys use 32-bit
@@ -99,7 +107,7 @@ histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount
         if (sHist[i] != 0) atomicAdd(&hist[i], sHist[i]);
 }
 
-template <typename K, bool kValues, typename W>
+template <typename K, bool kValues, typename W, uint32_t kItems>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
 onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
@@ -107,7 +115,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift, uint32_t spinLimit) {
     extern __shared__ __align__(16) unsigned char smem[];
     K* sKeys = reinterpret_cast<K*>(smem);
-    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * kSortTile);
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * (kItems * kSortThreads));
     __shared__ uint32_t sWarpHist[kSortWarps][kDigits];
     __shared__ uint32_t sBlockStart[kDigits];
     __shared__ uint32_t sGlobal[kDigits];
@@ -121,16 +129,16 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     __syncthreads();
     const uint32_t n = dCount != nullptr ? min(*dCount, cap) : cap;
     const uint32_t part = sPart;
-    const uint32_t base = part * kSortTile;
+    const uint32_t base = part * (kItems * kSortThreads);
     if (base >= n) return;
 
     // Warp-striped load: item j of lane l is key base + 384 warp + 32 j + l.
-    K key[kSortItems];
-    uint32_t val[kSortItems];
-    uint32_t dig[kSortItems];
-    const uint32_t wbase = base + warp * (kSortItems * 32);
+    K key[kItems];
+    uint32_t val[kItems];
+    uint32_t dig[kItems];
+    const uint32_t wbase = base + warp * (kItems * 32);
 #pragma unroll
-    for (uint32_t j = 0; j < kSortItems; ++j) {
+    for (uint32_t j = 0; j < kItems; ++j) {
         const uint32_t idx = wbase + j * 32 + lane;
         const bool ok = idx < n;
         key[j] = ok ? kin[idx] : K(0);
@@ -146,11 +154,11 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     // kRankGroup items, every item's peer mask is found first, then every
     // leader's atomic is issued (their latencies overlap), then the old
     // counts are passed on.
-    uint32_t rank[kSortItems];
+    uint32_t rank[kItems];
     const uint32_t lowerLanes = (1u << lane) - 1u;
     constexpr uint32_t kRankGroup = 4;
 #pragma unroll
-    for (uint32_t j0 = 0; j0 < kSortItems; j0 += kRankGroup) {
+    for (uint32_t j0 = 0; j0 < kItems; j0 += kRankGroup) {
         uint32_t peers[kRankGroup];
 #pragma unroll
         for (uint32_t q = 0; q < kRankGroup; ++q) peers[q] = __match_any_sync(0xFFFFFFFFu, dig[j0 + q]);
@@ -235,7 +243,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 
     // Scatter into shared memory in digit order.
 #pragma unroll
-    for (uint32_t j = 0; j < kSortItems; ++j) {
+    for (uint32_t j = 0; j < kItems; ++j) {
         const uint32_t d = dig[j];
         if (d < kDigits) {
             const uint32_t at = sBlockStart[d] + sWarpHist[warp][d] + rank[j];
@@ -246,7 +254,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     __syncthreads();
 
     // Write out: slot i of the block goes to sGlobal[digit] + i.
-    const uint32_t valid = min(kSortTile, n - base);
+    const uint32_t valid = min((kItems * kSortThreads), n - base);
     for (uint32_t i = tid; i < valid; i += kSortThreads) {
         const K k = sKeys[i];
         const uint32_t at = sGlobal[digit_of(k, shift)] + i;
@@ -255,14 +263,15 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     }
 }
 
-template <typename K, bool kValues, typename W>
+template <typename K, bool kValues, typename W, uint32_t kItems>
 cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                       uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
                       bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
     *resultInAlt = false;
     if (cap == 0 || bits == 0) return cudaSuccess;
+    constexpr uint32_t kTile = kItems * kSortThreads;
     const uint32_t passes = (bits + 7) / 8;
-    const uint32_t parts = (cap + kSortTile - 1) / kSortTile;
+    const uint32_t parts = (cap + kTile - 1) / kTile;
     char* s = static_cast<char*>(scratch);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(s);                     // kMaxPasses
     uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
@@ -282,8 +291,8 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     histogram_kernel<K><<<histBlocks, kHistThreads, 0, stream>>>(keys, dCount, cap, firstBit, passes, hist);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(K) * kSortTile + (kValues ? sizeof(uint32_t) * kSortTile : 0);
-    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = sizeof(K) * kTile + (kValues ? sizeof(uint32_t) * kTile : 0);
+    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues, W, kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     K* src = keys;
@@ -291,7 +300,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* vsrc = vals;
     uint32_t* vdst = valsAlt;
     for (uint32_t p = 0; p < passes; ++p) {
-        onesweep_kernel<K, kValues, W><<<parts, kSortThreads, smem, stream>>>(
+        onesweep_kernel<K, kValues, W, kItems><<<parts, kSortThreads, smem, stream>>>(
             src, dst, vsrc, vdst, dCount, cap, hist + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
             tickets + p, err, firstBit + 8 * p, spinLimit);
         e = cudaGetLastError();
@@ -307,7 +316,8 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
 
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits) {
     const size_t passes = (bits + 7) / 8;
-    const size_t parts = (static_cast<size_t>(cap) + kSortTile - 1) / kSortTile;
+    const size_t tile = cap > kLargeKeys ? kLargeTile : kSortTile;
+    const size_t parts = (static_cast<size_t>(cap) + tile - 1) / tile;
     const size_t word = 8;   // room for either word size (the 64-bit form can be asked for at any size)
     return 64 + kMaxPasses * kDigits * 4 + std::max<size_t>(passes, 1) * std::max<size_t>(parts, 1) * kDigits * word;
 }
@@ -317,11 +327,19 @@ cudaError_t sort_dispatch(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt
                           uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
                           bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
     const bool wide = cap > kSmallSortMax || (fault != nullptr && fault->wideWords != 0);
+    const bool large = cap > kLargeKeys;
+    if (!wide && !large)
+        return sort_impl<K, kValues, uint32_t, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
+                                                           scratch, err, resultInAlt, stream, fault);
     if (!wide)
-        return sort_impl<K, kValues, uint32_t>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch,
-                                               err, resultInAlt, stream, fault);
-    return sort_impl<K, kValues, unsigned long long>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
-                                                     scratch, err, resultInAlt, stream, fault);
+        return sort_impl<K, kValues, uint32_t, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
+                                                            scratch, err, resultInAlt, stream, fault);
+    if (!large)
+        return sort_impl<K, kValues, unsigned long long, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap,
+                                                                     firstBit, bits, scratch, err, resultInAlt, stream,
+                                                                     fault);
+    return sort_impl<K, kValues, unsigned long long, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit,
+                                                                  bits, scratch, err, resultInAlt, stream, fault);
 }
 
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
