@@ -54,25 +54,31 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
 cudaError_t launch_project_only(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
                                 const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                 uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                                uint64_t* depthWords, cudaStream_t stream);
+                                uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream);
 cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
                                        const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                        uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                                       uint64_t* depthWords, cudaStream_t stream);
+                                       uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream);
 // The pairs in depth order from the depth-sorted slot words: each slot's
 // first pair into offsets[slot] (the total into counters[1]), then the pair
 // words tile << 32 | slot. Training frames: the emit index as the word's low
 // field with emitSlot[index] = slot, or as values[] beside a slot (both null:
 // not a training frame).
+// tileDigits (tilePasses x 256, tilePasses 1 or 2): the tile sort's digit
+// counts of the pairs written, added up there for the sort.
 cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const ProjRecord* proj, const uint4* rects,
                                const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
                                uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
-                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
-                               uint32_t* values = nullptr, uint32_t* emitSlot = nullptr);
+                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, uint32_t* tileDigits,
+                               uint32_t tilePasses, cudaStream_t stream, uint32_t* values = nullptr,
+                               uint32_t* emitSlot = nullptr);
 cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
-                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, cudaStream_t stream);
+                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream);
 
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,
@@ -92,12 +98,17 @@ struct SortFault {
 };
 
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);
+// presetHist: the digit counts of every pass (256 a pass, from firstBit up),
+// already counted by the kernel that wrote the keys; the sort then skips its
+// own counting pass over the keys.
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
-                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr);
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr,
+                            const uint32_t* presetHist = nullptr);
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
-                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr);
+                            uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr,
+                            const uint32_t* presetHist = nullptr);
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
                           uint2* ranges, uint32_t tiles, cudaStream_t stream);

@@ -12,7 +12,7 @@
 //
 // Two schedules share the projection (project_emit_kernel<Src, kEmit>):
 //  - single frames (kEmit false) stop after the records and counts and write
-//    each slot's depth word (depth key << 32 | slot) and aux word (its tile
+//    each slot's depth word (depth key << 32 | slot) and aux words (its tile
 //    mask, or whether a large splat's rows are all single runs); the depth
 //    sort orders the words, depth_offsets_kernel gives each slot its first
 //    pair in depth order and emit_pairs_kernel writes the pairs
@@ -28,15 +28,14 @@
 // start on a 16-byte boundary) are staged into shared memory by 16-byte
 // cp.async copies issued first, so they land while the geometry runs. A
 // splat's exact tile test runs per thread when its rectangle holds at most 16
-// tiles and across its warp (32 tiles at a time, ballots) up to 512; up to
-// 64 tiles the result is kept as a bitmask. Larger splats are counted and
-// written a tile row at a time by the whole block: a row plan (the ellipse's
-// x-extent in double precision, widened by a margin that covers the float
-// test's rounding) gives each row a run that is certainly touched and a few
-// columns at its ends that are tested exactly. Pairs of masked splats are
-// written by the whole block, one pair per thread per step, so writes are
-// contiguous; the other splats up to 512 tiles by their own warp with the
-// tile test repeated.
+// tiles and across its warp (32 tiles at a time, ballots) up to 128, and the
+// result is kept as a 128-bit mask of the rectangle's tiles in row-major
+// order. Larger splats are counted and written a tile row at a time by the
+// whole block: a row plan (the ellipse's x-extent in double precision,
+// widened by a margin that covers the float test's rounding) gives each row
+// a run that is certainly touched and a few columns at its ends that are
+// tested exactly. Pairs of masked splats are written by their warp, lanes on
+// consecutive pairs, each pair's tile from the mask bit of its rank.
 #include "kernels.cuh"
 #include "raster_common.cuh"
 
@@ -290,7 +289,9 @@ struct TrainOutputs {
 };
 
 constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
-constexpr uint32_t kWarpArea = 128;   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
+constexpr uint32_t kWarpArea = 128;
+constexpr uint32_t kMaskArea = kWarpArea;   // splats of up to this many tiles keep a 128-bit tile mask
+static_assert(kMaskArea <= 128, "a tile mask has 128 bits");   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
 
 // ---- Splats of more than kSmallArea tiles, one tile row at a time ----
 //
@@ -561,6 +562,20 @@ __device__ __forceinline__ uint32_t nth_set_bit(unsigned long long m, uint32_t r
     return base;
 }
 
+// The same over a 128-bit mask (lo, hi) with more than r set bits.
+__device__ __forceinline__ uint32_t nth_set_bit128(unsigned long long lo, unsigned long long hi, uint32_t r) {
+    const uint32_t lowCount = static_cast<uint32_t>(__popcll(lo));
+    return r < lowCount ? nth_set_bit(lo, r) : 64u + nth_set_bit(hi, r - lowCount);
+}
+
+// Row and column of bit `bit` of a row-major mask of width w (w <= 128,
+// bit < 128): (bit + 1/2) / w in float lies at least 1/256 away from an
+// integer, far more than its rounding error, so the floor is exact.
+__device__ __forceinline__ void mask_bit_tile(uint32_t bit, uint32_t w, float invW, uint32_t& dx, uint32_t& dy) {
+    dy = static_cast<uint32_t>((static_cast<float>(bit) + 0.5f) * invW);
+    dx = bit - dy * w;
+}
+
 struct PairSink {
     unsigned long long* pairs;
     uint32_t* values;     // training, emit index as a sort value
@@ -581,6 +596,23 @@ struct PairSink {
         } else {
             atomicOr(err, kErrOverflow);
         }
+    }
+};
+
+// A PairSink that also counts, in shared memory, the tile sort's digits of
+// every pair it writes (the tile's low byte, and its second byte when the
+// sort takes two passes), so that the sort needs no counting pass of its own.
+struct CountingSink {
+    PairSink inner;
+    uint32_t* digits;   // shared: 256 a pass
+    uint32_t passes;    // 1 or 2
+    __device__ __forceinline__ void put(uint64_t at, unsigned long long word, uint32_t slot) const {
+        if (at < inner.capacity) {
+            const uint32_t tile = static_cast<uint32_t>(word >> 32);
+            atomicAdd(&digits[tile & 0xFFu], 1u);
+            if (passes > 1) atomicAdd(&digits[256 + ((tile >> 8) & 0xFFu)], 1u);
+        }
+        inner.put(at, word, slot);
     }
 };
 
@@ -677,10 +709,10 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
     }
 }
 
-// The pairs of a warp's splats whose tiles are tested one by one (unmasked
-// splats of up to kWarpArea tiles, and larger ones with a row that is not
-// one run, possible only through the float test's rounding at the
-// ellipse's edge): for each such splat the warp repeats the exact tile test
+// The pairs of a warp's splats whose tiles are tested one by one (large
+// splats with a row that is not one run, possible only through the float
+// test's rounding at the ellipse's edge): for each such splat the warp
+// repeats the exact tile test
 // over its rectangle, 32 tiles at a time, and writes the hits in row-major
 // order. The splat's record is read back from `records` (written earlier by
 // its thread): records[slotOf ? slotOf[s] : s].
@@ -731,9 +763,9 @@ __device__ __noinline__ void emit_by_warp(bool mine, uint32_t area, const uint32
 
 // kEmit: emit the pairs (offsets by look-back over the frame's partitions).
 // Otherwise stop after the records and counts, and write per slot the
-// depth word (depth key << 32 | slot) the depth sort orders and the aux word
-// emit_sorted_kernel reads: the tile mask of a masked splat, else 1 when a
-// row of the splat's hits is not one run.
+// depth word (depth key << 32 | slot) the depth sort orders and the two aux
+// words emit_pairs_kernel reads: the tile mask of a masked splat, else 1 when
+// a row of a large splat's hits is not one run.
 template <class Src, bool kEmit = true>
 __global__ void __launch_bounds__(kProjectThreads, 4)
 project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
@@ -743,7 +775,8 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                     uint32_t* __restrict__ ticket, uint32_t partitionBase, uint32_t lastPartition, uint32_t lowBits,
                     unsigned long long* __restrict__ pairs, uint32_t capacity,
                     unsigned long long* __restrict__ auxOut = nullptr,
-                    unsigned long long* __restrict__ depthWordsOut = nullptr) {
+                    unsigned long long* __restrict__ depthWordsOut = nullptr,
+                    uint32_t* __restrict__ depthDigits = nullptr) {
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
@@ -762,12 +795,18 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     // The frame's parameters: by value, or (when a captured graph replays a
     // batch with new cameras) read from device memory, once per block.
     __shared__ FrameParams sF;
+    // Without emission: the block's counts of the depth keys' three bytes
+    // (the depth sort's digits), added to depthDigits at the end.
+    __shared__ uint32_t sDigits[kEmit ? 1 : 3 * 256];
     uint32_t* err = counters + 2;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     if (tid == 0) {
         sPart = atomicAdd(ticket, 1u);
         sF = fDev != nullptr ? *fDev : fArg;
+    }
+    if constexpr (!kEmit) {
+        for (uint32_t k = tid; k < 3 * 256; k += kProjectThreads) sDigits[k] = 0;
     }
     __syncthreads();
     const FrameParams& f = sF;
@@ -918,21 +957,21 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
 
     // The exact touched count (splat_project.slang:148-160), row-major over
-    // the rectangle. Where it fits, a bitmask of the touched tiles is kept with
-    // rows `1 << sh` bits apart (sh: bits of the rectangle's width), so that a
-    // bit's tile is found by shifts; such splats are "masked".
+    // the rectangle. Up to kMaskArea tiles a bitmask of the touched tiles is
+    // kept, bit k for the rectangle's k-th tile in row-major order (two
+    // words); such splats are "masked" and their pairs are written from it.
     const uint32_t rw = alive ? rect.z - rect.x + 1 : 0;
     const uint32_t rh = alive ? rect.w - rect.y + 1 : 0;
     const uint32_t area = rw * rh;
     const uint32_t sh = rw <= 1 ? 0u : 32u - static_cast<uint32_t>(__clz(rw - 1));
-    const bool masked = alive && rh <= (64u >> sh);
+    const bool masked = alive && area <= kMaskArea;
     uint32_t touched = 0;
-    unsigned long long mask = 0;
-    if (alive && area <= kSmallArea) {   // always masked: rh * 2^sh < 2 * area
+    unsigned long long mask = 0, maskHi = 0;
+    if (alive && area <= kSmallArea) {
         uint32_t dx = 0, dy = 0;
         for (uint32_t k = 0; k < area; ++k) {
             if (tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, rect.x + dx, rect.y + dy)) {
-                mask |= 1ull << ((dy << sh) | dx);
+                mask |= 1ull << k;
                 touched += 1;
             }
             if (++dx == rw) {
@@ -943,16 +982,14 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
     // Splats of up to kWarpArea tiles: their warp tests 32 tiles of the
     // rectangle a step (row-major, lane l tiles l, l + 32, ...; column and row
-    // advance by 32 tiles a step without a division), building the mask of a
-    // masked splat.
+    // advance by 32 tiles a step without a division); step j's ballot is the
+    // mask's bits [32 j, 32 j + 32).
     uint32_t medium = __ballot_sync(0xFFFFFFFFu, alive && area > kSmallArea && area <= kWarpArea);
     while (medium != 0) {
         const int src = __ffs(medium) - 1;
         medium &= medium - 1;
         const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
         const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
-        const uint32_t sSh = __shfl_sync(0xFFFFFFFFu, sh, src);
-        const bool sMasked = __shfl_sync(0xFFFFFFFFu, masked ? 1u : 0u, src) != 0;
         const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
         const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
         const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
@@ -961,16 +998,14 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
         uint32_t dx = lane % sW, dy = lane / sW;
         uint32_t count = 0;
-        uint32_t mLo = 0, mHi = 0;
+        unsigned long long mLo = 0, mHi = 0;
         for (uint32_t base = 0; base < sArea; base += 32) {
             const bool hit = base + lane < sArea &&
                              tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + dx, sY + dy);
-            count += static_cast<uint32_t>(__popc(__ballot_sync(0xFFFFFFFFu, hit)));
-            if (sMasked) {
-                const uint32_t bit = (dy << sSh) | dx;
-                mLo |= __reduce_or_sync(0xFFFFFFFFu, hit && bit < 32u ? 1u << bit : 0u);
-                mHi |= __reduce_or_sync(0xFFFFFFFFu, hit && bit >= 32u ? 1u << (bit - 32u) : 0u);
-            }
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+            count += static_cast<uint32_t>(__popc(bal));
+            if (base < 64) mLo |= static_cast<unsigned long long>(bal) << base;
+            else mHi |= static_cast<unsigned long long>(bal) << (base - 64);
             dx += stepDx;
             dy += stepDy;
             if (dx >= sW) {
@@ -980,7 +1015,8 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         }
         if (lane == static_cast<uint32_t>(src)) {
             touched = count;
-            mask = sMasked ? (static_cast<unsigned long long>(mHi) << 32) | mLo : 0ull;
+            mask = mLo;
+            maskHi = mHi;
         }
     }
     // Larger splats are counted by the whole block below, a tile row at a
@@ -1091,8 +1127,17 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     if (lane == 0 && ballot != 0) atomicAdd(counters, static_cast<uint32_t>(__popc(ballot)));
     if constexpr (!kEmit) {
         if (inRange) {
-            auxOut[record] = masked ? mask : (irregular ? 1ull : 0ull);
+            reinterpret_cast<ulonglong2*>(auxOut)[record] =
+                masked ? make_ulonglong2(mask, maskHi) : make_ulonglong2(irregular ? 1ull : 0ull, 0ull);
             depthWordsOut[record] = (static_cast<unsigned long long>(key) << 32) | slot;
+            atomicAdd(&sDigits[key & 0xFFu], 1u);
+            atomicAdd(&sDigits[256 + ((key >> 8) & 0xFFu)], 1u);
+            atomicAdd(&sDigits[512 + (key >> 16)], 1u);
+        }
+        __syncthreads();
+        for (uint32_t k = tid; k < 3 * 256; k += kProjectThreads) {
+            const uint32_t v = sDigits[k];
+            if (v != 0 && depthDigits != nullptr) atomicAdd(depthDigits + k, v);
         }
         return;
     }
@@ -1133,6 +1178,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         const uint32_t excl = incl - mine;
         const uint32_t mRect = rect.x | (rect.y << 16);
         const unsigned long long mLow = static_cast<unsigned long long>(key) << lowBits;
+        const float mInvW = masked ? 1.0f / static_cast<float>(rw) : 0.0f;
         const uint32_t warpBase = slotBase + (tid & ~31u);
         for (uint32_t c0 = 0; c0 < total; c0 += 32) {
             const uint32_t pos = c0 + lane;
@@ -1144,14 +1190,17 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             }
             const uint32_t r = pos - __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l));
             const unsigned long long m = __shfl_sync(0xFFFFFFFFu, mask, static_cast<int>(l));
+            const unsigned long long mH = __shfl_sync(0xFFFFFFFFu, maskHi, static_cast<int>(l));
             const uint32_t oRect = __shfl_sync(0xFFFFFFFFu, mRect, static_cast<int>(l));
-            const uint32_t oSh = __shfl_sync(0xFFFFFFFFu, sh, static_cast<int>(l));
+            const uint32_t oW = __shfl_sync(0xFFFFFFFFu, rw, static_cast<int>(l));
+            const float oInvW = __shfl_sync(0xFFFFFFFFu, mInvW, static_cast<int>(l));
             const uint32_t oStart = __shfl_sync(0xFFFFFFFFu, start, static_cast<int>(l));
             const unsigned long long oLow = __shfl_sync(0xFFFFFFFFu, mLow, static_cast<int>(l));
             if (pos < total) {
-                const uint32_t bit = nth_set_bit(m, r);
-                const uint32_t tx = (oRect & 0xFFFFu) + (bit & ((1u << oSh) - 1u));
-                const uint32_t ty = (oRect >> 16) + (bit >> oSh);
+                uint32_t dx, dy;
+                mask_bit_tile(nth_set_bit128(m, mH, r), oW, oInvW, dx, dy);
+                const uint32_t tx = (oRect & 0xFFFFu) + dx;
+                const uint32_t ty = (oRect >> 16) + dy;
                 sink.put(blockBase + oStart + r,
                          (static_cast<unsigned long long>(f.tileBase + ty * f.tilesX + tx) << tileShift) | oLow,
                          warpBase + l);
@@ -1249,7 +1298,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
                   const uint32_t* __restrict__ touchedIn, const unsigned long long* __restrict__ aux,
                   const uint32_t* __restrict__ offsets, uint32_t width, uint32_t height, uint32_t tilesX,
                   uint32_t* __restrict__ err, unsigned long long* __restrict__ pairs, uint32_t capacity,
-                  TrainOutputs train) {
+                  TrainOutputs train, uint32_t* __restrict__ tileDigits, uint32_t tilePasses) {
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];
@@ -1261,7 +1310,10 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     __shared__ uint32_t sRowFirst[kProjectThreads];
     __shared__ uint32_t sRowMeta[kProjectThreads];
     __shared__ uint32_t sRowOff[kProjectThreads + 1];
+    __shared__ uint32_t sDigits[2 * 256];
     const uint32_t tid = threadIdx.x;
+    sDigits[tid] = 0;
+    sDigits[256 + tid] = 0;
     const uint32_t slotBase = blockIdx.x * kProjectThreads;
     const uint32_t slot = slotBase + tid;
     const bool inRange = slot < n;
@@ -1272,9 +1324,9 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     const uint32_t rh = alive ? rect.w - rect.y + 1 : 0;
     const uint32_t area = rw * rh;
     const uint32_t sh = rw <= 1 ? 0u : 32u - static_cast<uint32_t>(__clz(rw - 1));
-    const bool masked = alive && rh <= (64u >> sh);
-    const unsigned long long a = alive ? __ldg(aux + slot) : 0ull;
-    const bool irregular = alive && !masked && (a & 1ull) != 0;
+    const bool masked = alive && area <= kMaskArea;
+    const ulonglong2 a = alive ? __ldg(reinterpret_cast<const ulonglong2*>(aux) + slot) : make_ulonglong2(0ull, 0ull);
+    const bool irregular = alive && !masked && (a.x & 1ull) != 0;
     // The splats written a row at a time: unmasked, of more than kWarpArea
     // tiles, every row one run. The other unmasked ones go tile by tile.
     const bool rowsHere = alive && !masked && !irregular && area > kWarpArea;
@@ -1295,7 +1347,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     sRect[tid] = rect.x | (rect.y << 16);
     sWidth[tid] = rw | (sh << 16) | (irregular ? 0x80000000u : 0u);
     __syncthreads();
-    const PairSink sink{pairs, train.values, train.emitSlot, capacity, err};
+    const CountingSink sink{PairSink{pairs, train.values, train.emitSlot, capacity, err}, sDigits, tilePasses};
     constexpr uint32_t tileShift = 32;
 
     // Masked splats: each warp writes its own splats' pairs, 32 at a time,
@@ -1315,6 +1367,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
         const uint32_t excl = incl - mine;
         const uint32_t mRect = rect.x | (rect.y << 16);
+        const float mInvW = masked ? 1.0f / static_cast<float>(rw) : 0.0f;
         const uint32_t warpBase = slotBase + (tid & ~31u);
         for (uint32_t c0 = 0; c0 < total; c0 += 32) {
             const uint32_t pos = c0 + lane;
@@ -1325,14 +1378,17 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
                 if (e <= pos) l += step;
             }
             const uint32_t r = pos - __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l));
-            const unsigned long long m = __shfl_sync(0xFFFFFFFFu, a, static_cast<int>(l));
+            const unsigned long long m = __shfl_sync(0xFFFFFFFFu, a.x, static_cast<int>(l));
+            const unsigned long long mH = __shfl_sync(0xFFFFFFFFu, a.y, static_cast<int>(l));
             const uint32_t oRect = __shfl_sync(0xFFFFFFFFu, mRect, static_cast<int>(l));
-            const uint32_t oSh = __shfl_sync(0xFFFFFFFFu, sh, static_cast<int>(l));
+            const uint32_t oW = __shfl_sync(0xFFFFFFFFu, rw, static_cast<int>(l));
+            const float oInvW = __shfl_sync(0xFFFFFFFFu, mInvW, static_cast<int>(l));
             const uint32_t oFirst = __shfl_sync(0xFFFFFFFFu, first, static_cast<int>(l));
             if (pos < total) {
-                const uint32_t bit = nth_set_bit(m, r);
-                const uint32_t tx = (oRect & 0xFFFFu) + (bit & ((1u << oSh) - 1u));
-                const uint32_t ty = (oRect >> 16) + (bit >> oSh);
+                uint32_t dx, dy;
+                mask_bit_tile(nth_set_bit128(m, mH, r), oW, oInvW, dx, dy);
+                const uint32_t tx = (oRect & 0xFFFFu) + dx;
+                const uint32_t ty = (oRect >> 16) + dy;
                 sink.put(static_cast<unsigned long long>(oFirst) + r,
                          static_cast<unsigned long long>(ty * tilesX + tx) << tileShift, warpBase + l);
             }
@@ -1350,6 +1406,11 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     if (__ballot_sync(0xFFFFFFFFu, byWarp) != 0)
         emit_by_warp(byWarp, area, sWidth, sRect, sStart, sLow, proj + slotBase, width, height, 0u, tilesX, 0ull,
                      tileShift, slotBase, nullptr, sink);
+    __syncthreads();
+    for (uint32_t d = tid; d < tilePasses * 256; d += kProjectThreads) {
+        const uint32_t v = sDigits[d];
+        if (v != 0) atomicAdd(tileDigits + d, v);
+    }
 }
 
 template <class Src>
@@ -1375,7 +1436,7 @@ cudaError_t launch(const FrameParams& f, const FrameParams* fDev, const Src& src
 template <class Src>
 cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRecord* proj, uint4* rects,
                         uint32_t* touched, uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                        uint64_t* depthWords, cudaStream_t stream) {
+                        uint64_t* depthWords, uint32_t* depthDigits, cudaStream_t stream) {
     const uint32_t stageWords = stage ? f.shWords : 0u;
     const uint32_t shVector = (reinterpret_cast<uintptr_t>(src.sh) & 15u) == 0 ? 1u : 0u;
     const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
@@ -1386,7 +1447,7 @@ cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRe
     project_emit_kernel<Src, false><<<blocks, kProjectThreads, smem, stream>>>(
         f, nullptr, src, TrainOutputs{nullptr, nullptr, nullptr}, stageWords, shVector, proj, rects, touched, keys,
         counters, nullptr, ticket, 0, 0, 0, nullptr, 0, reinterpret_cast<unsigned long long*>(aux),
-        reinterpret_cast<unsigned long long*>(depthWords));
+        reinterpret_cast<unsigned long long*>(depthWords), depthDigits);
     return cudaGetLastError();
 }
 
@@ -1439,30 +1500,33 @@ cudaError_t launch_project_emit_train(const FrameParams& f, const float* means, 
 cudaError_t launch_project_only(const FrameParams& f, const float4* positions, const uint4* shape, const uint32_t* sh,
                                 const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                 uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                                uint64_t* depthWords, cudaStream_t stream) {
+                                uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
     return launch_only(f, PackedSource{positions, shape, sh, filter3d}, stage, proj, rects, touched, keys, counters,
-                       ticket, aux, depthWords, stream);
+                       ticket, aux, depthWords, depthDigits, stream);
 }
 
 cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
                                        const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                        uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                                       uint64_t* depthWords, cudaStream_t stream) {
+                                       uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     PointSource src{positions, reinterpret_cast<const uint2*>(colours), nullptr, style.size_mode, style.size,
                     style.constant_colour, {style.colour[0], style.colour[1], style.colour[2]}};
-    return launch_only(f, src, false, proj, rects, touched, keys, counters, ticket, aux, depthWords, stream);
+    return launch_only(f, src, false, proj, rects, touched, keys, counters, ticket, aux, depthWords, depthDigits,
+                       stream);
 }
 
 cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const ProjRecord* proj, const uint4* rects,
                                const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
                                uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
-                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, cudaStream_t stream,
-                               uint32_t* values, uint32_t* emitSlot) {
+                               uint32_t* offsets, uint64_t* pairs, uint32_t capacity, uint32_t* tileDigits,
+                               uint32_t tilePasses, cudaStream_t stream, uint32_t* values, uint32_t* emitSlot) {
     if (n == 0) return cudaSuccess;
     const uint32_t perBlock = kProjectThreads * kOffsetItems;
     const uint32_t offsetBlocks = (n + perBlock - 1) / perBlock;
@@ -1473,18 +1537,20 @@ cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const Pr
     if (e != cudaSuccess) return e;
     emit_pairs_kernel<<<project_partitions(n), kProjectThreads, 0, stream>>>(
         n, proj, rects, touched, reinterpret_cast<const unsigned long long*>(aux), offsets, width, height, tilesX,
-        counters + 2, reinterpret_cast<unsigned long long*>(pairs), capacity, TrainOutputs{nullptr, values, emitSlot});
+        counters + 2, reinterpret_cast<unsigned long long*>(pairs), capacity, TrainOutputs{nullptr, values, emitSlot},
+        tileDigits, tilePasses);
     return cudaGetLastError();
 }
 
 cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
-                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, cudaStream_t stream) {
+                                      uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, uint32_t* depthDigits,
+                                cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     // The DC triple is read from the staged row too, so it is always staged.
     return launch_only(f, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)}, true,
-                       proj, rects, touched, keys, counters, ticket, aux, depthWords, stream);
+                       proj, rects, touched, keys, counters, ticket, aux, depthWords, depthDigits, stream);
 }
 
 }  // namespace lrt

@@ -154,15 +154,19 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     }
     LRT_CUDA(r, ensure(r->depthWords, size_t{r->splatCap} * 8), "depth words");
     LRT_CUDA(r, ensure(r->depthWordsAlt, size_t{r->splatCap} * 8), "depth words");
-    LRT_CUDA(r, ensure(r->splatAux, size_t{r->splatCap} * 8), "tile masks");
+    LRT_CUDA(r, ensure(r->splatAux, size_t{r->splatCap} * 16), "tile masks");
     LRT_CUDA(r, ensure(r->pairOffsets, size_t{std::max(slots, 1u)} * 4), "pair offsets");
     if (train) {
         LRT_CUDA(r, ensure(r->pixState, size_t{s->width} * s->height * 16), "pixel state");
         LRT_CUDA(r, ensure(r->pixLast, size_t{s->width} * s->height * 4), "pixel state");
     }
     // Look-back status words and a ticket per projection launch, plus one
-    // for the emission over the frame's slots in depth order.
-    const size_t statusBytes = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches + 1} * 4;
+    // for the emission over the frame's slots in depth order; then the two
+    // sorts' digit counts (3 passes of the depth sort, up to 2 of the tile
+    // sort), counted by the kernels that write the keys.
+    const size_t ticketsEnd = lrt::project_status_bytes(static_cast<uint32_t>(partitions)) + size_t{launches + 1} * 4;
+    const size_t digitsAt = (ticketsEnd + 15) & ~size_t{15};
+    const size_t statusBytes = digitsAt + 5 * 256 * 4;
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
         LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
@@ -178,6 +182,9 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     uint64_t* status = static_cast<uint64_t*>(r->scanScratch.ptr);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(static_cast<char*>(r->scanScratch.ptr) +
                                                     lrt::project_status_bytes(static_cast<uint32_t>(partitions)));
+    uint32_t* depthDigits = reinterpret_cast<uint32_t*>(static_cast<char*>(r->scanScratch.ptr) + digitsAt);
+    uint32_t* tileDigits = depthDigits + 3 * 256;
+    const uint32_t tilePasses = (tileBits + 7) / 8 <= 2 ? (tileBits + 7) / 8 : 0u;
     const uint32_t lastPartition = partitions > 0 ? static_cast<uint32_t>(partitions - 1) : 0u;
     uint32_t visible = 0, pairs = 0, statusBits = 0;
     const uint64_t* sorted = nullptr;
@@ -233,7 +240,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              f, static_cast<const float4*>(g.positions), static_cast<const uint32_t*>(g.colours),
                              c.point->style, static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
                              static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
-                             tickets + launch, aux, depthWords, stream),
+                             tickets + launch, aux, depthWords, depthDigits, stream),
                          "points");
             } else if (c.train != nullptr) {
                 const lrt_train_params& t = *c.train;
@@ -243,7 +250,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<const float*>(t.quats), static_cast<const float*>(t.opacity_logits),
                              static_cast<const uint16_t*>(t.sh), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords, stream),
+                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords,
+                             depthDigits, stream),
                          "project");
             } else {
                 LRT_CUDA(r,
@@ -252,7 +260,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<const uint4*>(c.packed->shape), static_cast<const uint32_t*>(c.packed->sh),
                              static_cast<const float*>(c.packed->filter3d), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
-                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords, stream),
+                             static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords,
+                             depthDigits, stream),
                          "project");
             }
             base += c.count;
@@ -263,7 +272,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         bool depthInAlt = false;
         LRT_CUDA(r,
                  lrt::launch_sort_u64(depthWords, static_cast<uint64_t*>(r->depthWordsAlt.ptr), nullptr, nullptr,
-                                      nullptr, slots, 32, 24, r->sortScratch.ptr, err, &depthInAlt, stream),
+                                      nullptr, slots, 32, 24, r->sortScratch.ptr, err, &depthInAlt, stream, nullptr,
+                                      depthDigits),
                  "depth sort");
         const uint64_t* byDepth = depthInAlt ? static_cast<const uint64_t*>(r->depthWordsAlt.ptr) : depthWords;
         LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
@@ -272,8 +282,9 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                  lrt::launch_emit_sorted(byDepth, slots, static_cast<ProjRecord*>(r->proj.ptr),
                                          static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
                                          aux, s->width, s->height, tilesX, counters, status, tickets + launches,
-                                         static_cast<uint32_t*>(r->pairOffsets.ptr), pairBuf, r->pairCap, stream,
-                                         valueBuf, emitSlot),
+                                         static_cast<uint32_t*>(r->pairOffsets.ptr), pairBuf, r->pairCap,
+                                         tilePasses != 0 ? tileDigits : nullptr, tilePasses, stream, valueBuf,
+                                         emitSlot),
                  "emit");
         LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
         // --- stable sort on the tile bits + ranges -------------------------------------------
@@ -281,7 +292,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         LRT_CUDA(r,
                  lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), valueBuf,
                                       valueBuf != nullptr ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr,
-                                      counters + 1, r->pairCap, 32, tileBits, r->sortScratch.ptr, err, &inAlt, stream),
+                                      counters + 1, r->pairCap, 32, tileBits, r->sortScratch.ptr, err, &inAlt, stream,
+                                      nullptr, tilePasses != 0 ? tileDigits : nullptr),
                  "tile sort");
         sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
         if (valueBuf != nullptr) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;

@@ -266,7 +266,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 template <typename K, bool kValues, typename W, uint32_t kItems>
 cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                       uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
-                      bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
+                      bool* resultInAlt, cudaStream_t stream, const SortFault* fault, const uint32_t* presetHist) {
     *resultInAlt = false;
     if (cap == 0 || bits == 0) return cudaSuccess;
     constexpr uint32_t kTile = kItems * kSortThreads;
@@ -287,10 +287,15 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
         e = cudaMemsetAsync(tickets + (passes - 1), 1, 1, stream);
         if (e != cudaSuccess) return e;
     }
-    const uint32_t histBlocks = std::max(1u, std::min(parts, 148u * 4u));
-    histogram_kernel<K><<<histBlocks, kHistThreads, 0, stream>>>(keys, dCount, cap, firstBit, passes, hist);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    const uint32_t* digitCounts = hist;
+    if (presetHist != nullptr) {
+        digitCounts = presetHist;
+    } else {
+        const uint32_t histBlocks = std::max(1u, std::min(parts, 148u * 4u));
+        histogram_kernel<K><<<histBlocks, kHistThreads, 0, stream>>>(keys, dCount, cap, firstBit, passes, hist);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const size_t smem = sizeof(K) * kTile + (kValues ? sizeof(uint32_t) * kTile : 0);
     e = cudaFuncSetAttribute(onesweep_kernel<K, kValues, W, kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
@@ -301,7 +306,8 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* vdst = valsAlt;
     for (uint32_t p = 0; p < passes; ++p) {
         onesweep_kernel<K, kValues, W, kItems><<<parts, kSortThreads, smem, stream>>>(
-            src, dst, vsrc, vdst, dCount, cap, hist + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
+            src, dst, vsrc, vdst, dCount, cap, digitCounts + p * kDigits,
+            lookback + static_cast<size_t>(p) * parts * kDigits,
             tickets + p, err, firstBit + 8 * p, spinLimit);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -325,45 +331,46 @@ size_t sort_scratch_bytes(uint32_t cap, uint32_t bits) {
 template <typename K, bool kValues>
 cudaError_t sort_dispatch(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                           uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
-                          bool* resultInAlt, cudaStream_t stream, const SortFault* fault) {
+                          bool* resultInAlt, cudaStream_t stream, const SortFault* fault,
+                          const uint32_t* presetHist) {
     const bool wide = cap > kSmallSortMax || (fault != nullptr && fault->wideWords != 0);
     const bool large = cap > kLargeKeys;
     if (!wide && !large)
         return sort_impl<K, kValues, uint32_t, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
-                                                           scratch, err, resultInAlt, stream, fault);
+                                                           scratch, err, resultInAlt, stream, fault, presetHist);
     if (!wide)
         return sort_impl<K, kValues, uint32_t, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
-                                                            scratch, err, resultInAlt, stream, fault);
+                                                            scratch, err, resultInAlt, stream, fault, presetHist);
     if (!large)
         return sort_impl<K, kValues, unsigned long long, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap,
                                                                      firstBit, bits, scratch, err, resultInAlt, stream,
-                                                                     fault);
+                                                                     fault, presetHist);
     return sort_impl<K, kValues, unsigned long long, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit,
-                                                                  bits, scratch, err, resultInAlt, stream, fault);
+                                                                  bits, scratch, err, resultInAlt, stream, fault, presetHist);
 }
 
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
                             void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
-                            const SortFault* fault) {
+                            const SortFault* fault, const uint32_t* presetHist) {
     if (bits > 64 || firstBit + bits > 64 || (bits + 7) / 8 > kMaxPasses) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_dispatch<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream, fault);
+                                         resultInAlt, stream, fault, presetHist);
     return sort_dispatch<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream, fault);
+                                      resultInAlt, stream, fault, presetHist);
 }
 
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
                             void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
-                            const SortFault* fault) {
+                            const SortFault* fault, const uint32_t* presetHist) {
     if (bits > 32 || firstBit + bits > 32) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_dispatch<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream, fault);
+                                         resultInAlt, stream, fault, presetHist);
     return sort_dispatch<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream, fault);
+                                      resultInAlt, stream, fault, presetHist);
 }
 
 }  // namespace lrt
