@@ -404,11 +404,11 @@ def run_lod(L, torch, stream, raster, cloud, settings, peak) -> dict:
 def sort_bytes(slots: float, pairs: float, tiles: int) -> dict:
     """Algorithmic bytes of a frame's two sorts: the depth sort of one 8-byte
     word per slot on 24 key bits, and the stable sort of one 8-byte word per
-    pair on the tile bits; per 8-bit pass 8 B read + 8 B written per word, plus
-    one 8 B read per word for the histograms."""
+    pair on the tile bits; per 8-bit pass 8 B read + 8 B written per word (the
+    digit counts come from the kernels that write the keys)."""
     tile_bits = max(1, math.ceil(math.log2(tiles)))
     depth_passes, tile_passes = 3, math.ceil(tile_bits / 8)
-    return {"depth": (16 * depth_passes + 8) * slots, "tile": (16 * tile_passes + 8) * pairs,
+    return {"depth": 16 * depth_passes * slots, "tile": 16 * tile_passes * pairs,
             "depth_passes": depth_passes, "tile_passes": tile_passes}
 
 
@@ -501,7 +501,7 @@ def run_sort_heavy(L, torch, dev, raster, peak, clocks, steps: int, splats: int 
            "pairs": int(pairs), "visible": int(np.mean([x.visible for x in st])),
            "sort_passes": {"depth": sb["depth_passes"], "tile": sb["tile_passes"]},
            "sort_bytes": "depth sort: 8 B words per slot, tile sort: 8 B words per pair; per 8-bit pass 8 B read "
-                         "+ 8 B written per word, plus one 8 B read per word for the histograms; "
+                         "+ 8 B written per word (the digit counts come from the kernels that write the keys); "
                          "tile_sort_ms also holds the ranges pass",
            "sort_gbs": round(gbs, 1), "sort_frac_of_hbm": round(gbs / peak, 4)}
     del cloud, inst, targets
@@ -748,14 +748,14 @@ def run_ours(args) -> None:
     # Algorithmic bytes per launch (per unit x units):
     #   blend:   ranges 8 B/tile + (8 B pair word + 48 B record) per pair + 20 B per pixel written
     #   project: 124 B per splat read (deg 3); 48 + 16 + 4 + 4 B record, rect, count, key
-    #            and 8 + 8 B depth and aux words written per slot
+    #            and 8 + 16 B depth and aux words written per slot
     #   emit:    per slot its sorted depth word and count read and its offset written (depth-order
-    #            offsets: 8+4+4 B), then its count, rect, aux word and offset read (4+16+8+4 B;
-    #            records of unmasked splats not counted), 8 B per pair written
+    #            offsets: 8+4+4 B), then its count, rect, aux words and offset read (4+16+16+4 B;
+    #            records of large splats not counted), 8 B per pair written
     #   sorts:   see sort_bytes
     bytes_blend = 8 * tiles + 56 * pairs + 20 * pixels
-    bytes_project = 124 * SPLATS + 88 * SPLATS
-    bytes_emit = 48 * SPLATS + 8 * pairs
+    bytes_project = 124 * SPLATS + 96 * SPLATS
+    bytes_emit = 56 * SPLATS + 8 * pairs
     peak, peak_kind = measured_peaks()
     kernels = {
         "blend": (stage["blend_ms"], bytes_blend),
@@ -769,9 +769,9 @@ def run_ours(args) -> None:
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     sort_ms = stage["depth_sort_ms"] + stage["tile_sort_ms"]
     sort_gbs = (sort["depth"] + sort["tile"]) / (sort_ms * 1e-3) / 1e9 if sort_ms > 0 else None
-    # project, depth histogram + passes, depth-order offsets, pair writes,
-    # tile histogram + passes, ranges, blend
-    launches_per_frame = 1 + 1 + sort["depth_passes"] + 2 + 1 + sort["tile_passes"] + 1 + 1
+    # project, depth passes, depth-order offsets, pair writes, tile passes,
+    # ranges, blend
+    launches_per_frame = 1 + sort["depth_passes"] + 2 + sort["tile_passes"] + 1 + 1
 
     clocks.stop()
     if rank == 0:

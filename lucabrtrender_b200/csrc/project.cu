@@ -619,11 +619,10 @@ struct CountingSink {
 // The block's large splats counted a tile row per thread per step (rows in
 // list order, splat after splat): counts added into counts[splat thread]
 // (bit 31 marks a splat with a row that is not one run), tile bits of masked
-// splats or-ed into masks[splat thread]. Kept out of line: the kernel's other
-// paths do not pay for its registers.
-__device__ __noinline__ void count_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
-                                              uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t* counts,
-                                              unsigned long long* masks) {
+// splats or-ed into masks[splat thread].
+__device__ __forceinline__ void count_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
+                                                 uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t* counts,
+                                                 unsigned long long* masks) {
     const uint32_t tid = threadIdx.x;
     uint32_t fs = 0;   // the splat of row item j: found by search once, then advanced
     {
@@ -651,7 +650,7 @@ __device__ __noinline__ void count_large_rows(const Footprint* foot, const uint3
 // pairs of a row. takenStart[t]: the pairs of such splats before splat t.
 // slotOf[t]: the slot of the block's splat t (null: slotBase + t).
 template <class Sink>
-__device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
+__device__ __forceinline__ void emit_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
                                              uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t tileBase,
                                              uint32_t tilesX, const uint32_t* widthBits, const uint32_t* start,
                                              const uint32_t* takenStart, const unsigned long long* low,
@@ -717,7 +716,7 @@ __device__ __noinline__ void emit_large_rows(const Footprint* foot, const uint32
 // order. The splat's record is read back from `records` (written earlier by
 // its thread): records[slotOf ? slotOf[s] : s].
 template <class Sink>
-__device__ __noinline__ void emit_by_warp(bool mine, uint32_t area, const uint32_t* widthBits,
+__device__ __forceinline__ void emit_by_warp(bool mine, uint32_t area, const uint32_t* widthBits,
                                           const uint32_t* rectBits, const uint32_t* start,
                                           const unsigned long long* low, const ProjRecord* records, uint32_t width,
                                           uint32_t height, uint32_t tileBase, uint32_t tilesX,
