@@ -42,12 +42,12 @@ SEED = 1
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + written) of one launch, from ncu (`dram__bytes_read.sum +
 # dram__bytes_write.sum`) on frame 3 of this orbit; the capture and its command
-# are summarised under profiles/.
-PROFILED_DRAM_BYTES = {"blend": 63.438080e6 + 17.494784e6}
+# are summarised under profiles/ (blend_1M_1080p.md).
+PROFILED_DRAM_BYTES = {"blend": 54.031104e6 + 12.246784e6}
 # The blend is bound by instruction issue, not by HBM: its issue-active
 # fraction (`smsp__issue_active.avg.pct_of_peak_sustained_active`) from the
 # same capture, the secondary roofline its HBM fraction is read beside.
-PROFILED_ISSUE_ACTIVE = {"blend": 0.8889}
+PROFILED_ISSUE_ACTIVE = {"blend": 0.8643}
 
 
 def orbit_camera(L, k: int):
