@@ -364,9 +364,11 @@ int lrt_rast_train_forward(lrt_rast* rast, const lrt_projection* projection, con
  * (device); gradients of the parameters are written to `grads`. A
  * reverse-order re-blend per pixel, per-pair partials written at each pair's
  * emit index, then a per-splat ordered sum and the projection's chain rule:
- * no atomics. It waits only for an enqueued forward's counts (to report an
- * overflow before reading its pairs) and returns once its kernels are
- * enqueued on `stream`: the gradients are ready in that stream's order. */
+ * no atomics. It enqueues its kernels on `stream` (the gradients are ready
+ * in that stream's order), then, after a forward that was only enqueued,
+ * waits for that forward's counts: if that frame emitted more pairs than the
+ * buffers held it returns LRT_OVERFLOW and the gradients it wrote are not to
+ * be used (run the step again; the buffers are grown). */
 int lrt_rast_train_backward(lrt_rast* rast, const void* grad_colour, lrt_train_grads* grads, void* stream);
 /* CUDA-event times of the last backward: the blend backward and the
  * per-splat reduction + projection backward (waits for the backward). */
@@ -459,7 +461,7 @@ int lrt_rast_debug_sort(lrt_rast* rast, uint32_t skip_first_partition, uint32_t 
  * every GPU that loads the library holds until the process exits. Counts
  * above LRT_PREFIX_SUM_NOALLOC_MAX are rejected with LRT_INVALID_ARGUMENT.
  * The first call on each device looks up that array's device address (with
- * the device current), so make the first call before any stream capture.
+ * the device current).
  * All calls on a device share the array and clear it on their stream first;
  * calls whose work overlaps on the GPU race on it. Blocks until done, like
  * lrt_prefix_sum. No counterpart in the reference: its PrefixSum always

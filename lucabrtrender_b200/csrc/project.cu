@@ -966,16 +966,52 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     const bool masked = alive && area <= kMaskArea;
     uint32_t touched = 0;
     unsigned long long mask = 0, maskHi = 0;
-    if (alive && area <= kSmallArea) {
-        uint32_t dx = 0, dy = 0;
-        for (uint32_t k = 0; k < area; ++k) {
-            if (tile_touched(f.width, f.height, cx, cy, ca, cb, cc, cutoff, rect.x + dx, rect.y + dy)) {
-                mask |= 1ull << k;
-                touched += 1;
+    // Splats of up to kSmallArea tiles: the warp tests their tiles together,
+    // 32 (splat, tile) pairs a step in lane and row-major tile order, so that
+    // no lane waits on a neighbour with more tiles. A lane finds its pair's
+    // splat by a binary search over the warp's running tile counts
+    // (shuffles: the last lane whose count starts at or before the pair,
+    // which always has tiles), and each splat's lane takes its run of the
+    // step's ballot as mask bits.
+    {
+        const uint32_t mine = alive && area <= kSmallArea ? area : 0u;
+        uint32_t incl = mine;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - mine;
+        const float invW = mine != 0 ? 1.0f / static_cast<float>(rw) : 0.0f;
+        for (uint32_t c0 = 0; c0 < total; c0 += 32) {
+            const uint32_t pos = c0 + lane;
+            uint32_t l = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l + step));
+                if (e <= pos) l += step;
             }
-            if (++dx == rw) {
-                dx = 0;
-                ++dy;
+            const int src = static_cast<int>(l);
+            const uint32_t k = pos - __shfl_sync(0xFFFFFFFFu, excl, src);
+            const uint32_t oW = __shfl_sync(0xFFFFFFFFu, rw, src);
+            const float oInv = __shfl_sync(0xFFFFFFFFu, invW, src);
+            const uint32_t oX = __shfl_sync(0xFFFFFFFFu, rect.x, src), oY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
+            const float ocx = __shfl_sync(0xFFFFFFFFu, cx, src), ocy = __shfl_sync(0xFFFFFFFFu, cy, src);
+            const float oa = __shfl_sync(0xFFFFFFFFu, ca, src), ob = __shfl_sync(0xFFFFFFFFu, cb, src);
+            const float oc = __shfl_sync(0xFFFFFFFFu, cc, src), ocut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+            uint32_t dx = 0, dy = 0;
+            mask_bit_tile(k, oW, oInv, dx, dy);
+            const bool hit = pos < total && tile_touched(f.width, f.height, ocx, ocy, oa, ob, oc, ocut, oX + dx, oY + dy);
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+            if (mine != 0) {
+                const uint32_t lo = max(excl, c0), hi = min(incl, c0 + 32);
+                if (lo < hi) {
+                    const unsigned long long run = ((static_cast<unsigned long long>(bal) >> (lo - c0)) &
+                                                    ((1ull << (hi - lo)) - 1ull));
+                    mask |= run << (lo - excl);
+                    touched += static_cast<uint32_t>(__popcll(run));
+                }
             }
         }
     }

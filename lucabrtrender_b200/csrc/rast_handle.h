@@ -156,7 +156,12 @@ inline uint32_t grow(uint32_t have, uint32_t need) {
 
 inline cudaError_t ensure(DeviceBuffer& b, size_t bytes) {
     if (b.bytes >= bytes && b.ptr != nullptr) return cudaSuccess;
-    if (b.ptr != nullptr) cudaFree(b.ptr);
+    // Work still queued (an enqueued frame, a backward that returned without
+    // waiting) may read the old buffer: it finishes before the buffer goes.
+    if (b.ptr != nullptr) {
+        cudaDeviceSynchronize();
+        cudaFree(b.ptr);
+    }
     b.ptr = nullptr;
     b.bytes = 0;
     cudaError_t e = cudaMalloc(&b.ptr, std::max<size_t>(bytes, 16));

@@ -918,18 +918,17 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
         return fail(r, LRT_INVALID_ARGUMENT, "the SH gradient must be 16-byte aligned");
     DeviceScope scope(r->device);
     cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
-    if (r->trainPending) {
-        // The forward ran without waiting: wait for its counts only (its
-        // copy to the host is done; the loss kernels after it may still
-        // run), so that an overflow or timeout is reported before anything
-        // reads its pairs.
-        LRT_CUDA(r, cudaEventSynchronize(r->ev[6]), "frame");
-        const int code = settle_pending_frame(r);
-        if (code != LRT_OK) return code;
-    }
+    // A forward that ran without waiting has not reported its pair count yet:
+    // the backward is enqueued over the pair buffer's capacity (every read
+    // stays inside the buffers), and the forward's counts are read once the
+    // backward is queued behind it, so the device never waits for the host
+    // here. If that frame overflowed, the call returns OVERFLOW and the
+    // gradients it wrote are not to be used.
+    const bool pending = r->trainPending;
+    const uint32_t pairBound = pending ? r->pairCap : r->trainPairs;
     // Every pair's partials are written by the blend backward (zeros for those
     // it does not walk), so the buffer is not cleared.
-    const size_t partialBytes = std::max<size_t>(size_t{r->trainPairs} * 12 * sizeof(float), 16);
+    const size_t partialBytes = std::max<size_t>(size_t{pairBound} * 12 * sizeof(float), 16);
     LRT_CUDA(r, ensure(r->partials, partialBytes), "partials");
     LRT_CUDA(r, cudaEventRecord(r->ev[7], stream), "event");
     LRT_CUDA(r,
@@ -946,18 +945,23 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
                                         static_cast<const float*>(p.opacity_logits),
                                         static_cast<const uint16_t*>(p.sh), static_cast<uint32_t*>(r->touched.ptr),
                                         static_cast<uint32_t*>(r->pairOffsets.ptr),
-                                        static_cast<float*>(r->partials.ptr), r->trainPairs,
+                                        static_cast<float*>(r->partials.ptr), pairBound,
                                         static_cast<float*>(grads->means),
                                         static_cast<float*>(grads->log_scales), static_cast<float*>(grads->quats),
                                         static_cast<float*>(grads->opacity_logits), static_cast<float*>(grads->sh),
                                         stream),
              "projection backward");
     LRT_CUDA(r, cudaEventRecord(r->ev[9], stream), "event");
-    // No wait here: the gradients are ready in stream order. Later calls on
-    // the handle (any stream) wait for this event before touching its buffers.
+    // The gradients are ready in stream order. Later calls on the handle (any
+    // stream) wait for this event before touching its buffers.
     LRT_CUDA(r, cudaEventRecord(r->frameDone, stream), "event");
     r->frameDoneSet = true;
     r->backwardTimed = true;
+    if (pending) {
+        LRT_CUDA(r, cudaEventSynchronize(r->ev[6]), "frame");
+        const int code = settle_pending_frame(r);
+        if (code != LRT_OK) return code;
+    }
     return LRT_OK;
 }
 

@@ -9,11 +9,10 @@
 // library holds its 128 KB until the process exits. In host code its name is
 // only a host-side stand-in, so its device address is looked up once per
 // device with cudaGetSymbolAddress (with that device current) and cached.
-// That lookup happens on the first call on each device; make that first call
-// before any stream capture. Every call on a device shares the one array and
-// leaves the last call's contents behind, so each call clears it first on its
-// stream; calls whose work overlaps on the GPU (different streams, no
-// ordering between them) race on it.
+// That lookup happens on the first call on each device. Every call on a
+// device shares the one array and leaves the last call's contents behind, so
+// each call clears it first on its stream; calls whose work overlaps on the
+// GPU (different streams, no ordering between them) race on it.
 #include "../../include/lrt_raster.h"
 #include "kernels.cuh"
 #include "raster_common.cuh"
