@@ -26,9 +26,10 @@
 // 256 splats by atomic ticket. Positions and shape are read as 16-byte
 // vectors. The block's harmonics rows (92 bytes a splat at degree 3; 256 rows
 // start on a 16-byte boundary) are staged into shared memory by 16-byte
-// cp.async copies issued first, so they land while the geometry runs. A
-// splat's exact tile test runs per thread when its rectangle holds at most 16
-// tiles and across its warp (32 tiles at a time, ballots) up to 128, and the
+// cp.async copies issued first, so they land while the geometry runs. The
+// exact tile tests of splats whose rectangles hold at most 16 tiles run
+// across the warp together, 32 (splat, tile) pairs a step; larger ones up to
+// 128 tiles run across their warp one splat at a time, 32 tiles a step; the
 // result is kept as a 128-bit mask of the rectangle's tiles in row-major
 // order. Larger splats are counted and written a tile row at a time by the
 // whole block: a row plan (the ellipse's x-extent in double precision,
