@@ -27,10 +27,9 @@
 // vectors. The block's harmonics rows (92 bytes a splat at degree 3; 256 rows
 // start on a 16-byte boundary) are staged into shared memory by 16-byte
 // cp.async copies issued first, so they land while the geometry runs. The
-// exact tile tests of splats whose rectangles hold at most 16 tiles run
-// across the warp together, 32 (splat, tile) pairs a step; larger ones up to
-// 128 tiles run across their warp one splat at a time, 32 tiles a step; the
-// result is kept as a 128-bit mask of the rectangle's tiles in row-major
+// exact tile tests of the warp's splats whose rectangles hold at most 128
+// tiles run across the warp together, 32 (splat, tile) pairs a step, and each
+// such splat keeps a 128-bit mask of its rectangle's tiles in row-major
 // order. Larger splats are counted and written a tile row at a time by the
 // whole block: a row plan (the ellipse's x-extent in double precision,
 // widened by a margin that covers the float test's rounding) gives each row
@@ -289,12 +288,14 @@ struct TrainOutputs {
     uint32_t* emitSlot;
 };
 
-constexpr uint32_t kSmallArea = 16;   // per-thread tile test up to this many tiles
+// Splats of up to kWarpArea tiles have their tiles tested by their warp (32
+// (splat, tile) pairs a step) and keep a 128-bit tile mask; larger ones are
+// counted and written a tile row at a time.
 constexpr uint32_t kWarpArea = 128;
-constexpr uint32_t kMaskArea = kWarpArea;   // splats of up to this many tiles keep a 128-bit tile mask
-static_assert(kMaskArea <= 128, "a tile mask has 128 bits");   // per-warp tile test (32 tiles a step) up to this many; a tile row at a time above
+constexpr uint32_t kMaskArea = kWarpArea;
+static_assert(kMaskArea <= 128, "a tile mask has 128 bits");
 
-// ---- Splats of more than kSmallArea tiles, one tile row at a time ----
+// ---- Splats of more than kWarpArea tiles, one tile row at a time ----
 //
 // The tiles of a row that the exact test (tile_touched) accepts are those
 // whose box of pixel centres meets the ellipse {power <= cutoff}; within the
@@ -786,7 +787,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     __shared__ unsigned long long sLow[kProjectThreads];   // depth key << lowBits
     __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
     __shared__ uint32_t sWidth[kProjectThreads];
-    __shared__ Footprint sFoot[kProjectThreads];           // the block's splats of more than kSmallArea tiles
+    __shared__ Footprint sFoot[kProjectThreads];           // the block's splats of more than kWarpArea tiles
     __shared__ uint32_t sFootRow[kProjectThreads + 1];     // their first row in the block's row list
     __shared__ uint32_t sRowFirst[kProjectThreads];        // emission: a chunk's rows, first column
     __shared__ uint32_t sRowMeta[kProjectThreads];         // emission: tile row | splat thread << 16
@@ -967,15 +968,15 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     const bool masked = alive && area <= kMaskArea;
     uint32_t touched = 0;
     unsigned long long mask = 0, maskHi = 0;
-    // Splats of up to kSmallArea tiles: the warp tests their tiles together,
+    // Splats of up to kWarpArea tiles: the warp tests their tiles together,
     // 32 (splat, tile) pairs a step in lane and row-major tile order, so that
-    // no lane waits on a neighbour with more tiles. A lane finds its pair's
-    // splat by a binary search over the warp's running tile counts
-    // (shuffles: the last lane whose count starts at or before the pair,
-    // which always has tiles), and each splat's lane takes its run of the
-    // step's ballot as mask bits.
+    // no lane waits on a neighbour with more tiles and no step is left part
+    // empty at the end of a splat. A lane finds its pair's splat by a binary
+    // search over the warp's running tile counts (shuffles: the last lane
+    // whose count starts at or before the pair, which always has tiles), and
+    // each splat's lane takes its run of the step's ballot as mask bits.
     {
-        const uint32_t mine = alive && area <= kSmallArea ? area : 0u;
+        const uint32_t mine = alive && area <= kWarpArea ? area : 0u;
         uint32_t incl = mine;
 #pragma unroll
         for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -1010,49 +1011,16 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                 if (lo < hi) {
                     const unsigned long long run = ((static_cast<unsigned long long>(bal) >> (lo - c0)) &
                                                     ((1ull << (hi - lo)) - 1ull));
-                    mask |= run << (lo - excl);
+                    const uint32_t at = lo - excl;   // the run's first bit in the 128-bit mask
+                    if (at < 64) {
+                        mask |= run << at;
+                        if (at != 0) maskHi |= run >> (64 - at);   // bits past 63 (a run is at most 32 bits)
+                    } else {
+                        maskHi |= run << (at - 64);
+                    }
                     touched += static_cast<uint32_t>(__popcll(run));
                 }
             }
-        }
-    }
-    // Splats of up to kWarpArea tiles: their warp tests 32 tiles of the
-    // rectangle a step (row-major, lane l tiles l, l + 32, ...; column and row
-    // advance by 32 tiles a step without a division); step j's ballot is the
-    // mask's bits [32 j, 32 j + 32).
-    uint32_t medium = __ballot_sync(0xFFFFFFFFu, alive && area > kSmallArea && area <= kWarpArea);
-    while (medium != 0) {
-        const int src = __ffs(medium) - 1;
-        medium &= medium - 1;
-        const uint32_t sArea = __shfl_sync(0xFFFFFFFFu, area, src);
-        const uint32_t sW = __shfl_sync(0xFFFFFFFFu, rw, src);
-        const uint32_t sX = __shfl_sync(0xFFFFFFFFu, rect.x, src);
-        const uint32_t sY = __shfl_sync(0xFFFFFFFFu, rect.y, src);
-        const float scx = __shfl_sync(0xFFFFFFFFu, cx, src), scy = __shfl_sync(0xFFFFFFFFu, cy, src);
-        const float sa = __shfl_sync(0xFFFFFFFFu, ca, src), sb = __shfl_sync(0xFFFFFFFFu, cb, src);
-        const float sc = __shfl_sync(0xFFFFFFFFu, cc, src), scut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
-        const uint32_t stepDy = 32u / sW, stepDx = 32u % sW;
-        uint32_t dx = lane % sW, dy = lane / sW;
-        uint32_t count = 0;
-        unsigned long long mLo = 0, mHi = 0;
-        for (uint32_t base = 0; base < sArea; base += 32) {
-            const bool hit = base + lane < sArea &&
-                             tile_touched(f.width, f.height, scx, scy, sa, sb, sc, scut, sX + dx, sY + dy);
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
-            count += static_cast<uint32_t>(__popc(bal));
-            if (base < 64) mLo |= static_cast<unsigned long long>(bal) << base;
-            else mHi |= static_cast<unsigned long long>(bal) << (base - 64);
-            dx += stepDx;
-            dy += stepDy;
-            if (dx >= sW) {
-                dx -= sW;
-                dy += 1;
-            }
-        }
-        if (lane == static_cast<uint32_t>(src)) {
-            touched = count;
-            mask = mLo;
-            maskHi = mHi;
         }
     }
     // Larger splats are counted by the whole block below, a tile row at a
