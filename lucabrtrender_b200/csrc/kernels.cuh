@@ -55,12 +55,15 @@ cudaError_t launch_project_only(const FrameParams& f, const float4* positions, c
                                 const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                 uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
                                 uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream);
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream);
 cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
                                        const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                        uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
                                        uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream);
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream);
+// rowTable (rowCap entries; counters[3] counts the entries asked for): each
+// large splat's rows (first column, count), kept by the projection for the
+// pair writes; null: none kept.
 // The pairs in depth order from the depth-sorted slot words: each slot's
 // first pair into offsets[slot] (the total into counters[1]), then the pair
 // words tile << 32 | slot. Training frames: the emit index as the word's low
@@ -72,13 +75,13 @@ cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const Pr
                                const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
                                uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
                                uint32_t* offsets, uint64_t* pairs, uint32_t capacity, uint32_t* tileDigits,
-                               uint32_t tilePasses, cudaStream_t stream, uint32_t* values = nullptr,
-                               uint32_t* emitSlot = nullptr);
+                               uint32_t tilePasses, const uint2* rowTable, cudaStream_t stream,
+                               uint32_t* values = nullptr, uint32_t* emitSlot = nullptr);
 cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                       uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream);
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream);
 
 size_t scan_scratch_bytes(uint32_t n);
 cudaError_t launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t n, void* scratch,

@@ -314,8 +314,9 @@ struct Footprint {
     uint32_t x0, x1;      // the rectangle's columns
     uint32_t y0;          // its first row
     uint32_t tid;         // the splat's thread in the block
-    uint32_t shMasked;    // mask row shift | 0x100 when the splat keeps a tile mask
+    uint32_t table;       // the splat's first row in the row table, or kNoTable
 };
+constexpr uint32_t kNoTable = 0xFFFFFFFFu;
 
 struct RowPlan {
     int32_t lo, hi;           // candidate columns, inside the rectangle (none when lo > hi)
@@ -420,28 +421,20 @@ __device__ __forceinline__ void row_walk(const Footprint& fp, uint32_t ty, uint3
         if (tile_touched(width, height, fp.cx, fp.cy, fp.a, fp.b, fp.c, fp.cut, static_cast<uint32_t>(t), ty)) visit(t);
 }
 
-// One row: its count, first and last touched column, whether its hits are
-// one run, and (for a masked splat) its tiles' bits, rows `1 << sh` apart.
+// One row: its count, first and last touched column, and whether its hits
+// are one run.
 struct RowCount {
     uint32_t count;
     int32_t first, last;
     bool regular;
-    unsigned long long bits;
 };
 __device__ __forceinline__ RowCount row_count(const Footprint& fp, uint32_t r, uint32_t width, uint32_t height) {
-    RowCount rc{0, 0, -2, true, 0ull};
-    const bool masked = (fp.shMasked & 0x100u) != 0;
-    const uint32_t base = (r << (fp.shMasked & 0xFFu));
+    RowCount rc{0, 0, -2, true};
     auto add = [&](int32_t t0, int32_t t1) {
         if (rc.count != 0 && t0 != rc.last + 1) rc.regular = false;
         if (rc.count == 0) rc.first = t0;
         rc.count += static_cast<uint32_t>(t1 - t0 + 1);
         rc.last = t1;
-        if (masked) {
-            const uint32_t n = static_cast<uint32_t>(t1 - t0 + 1);
-            const unsigned long long ones = n >= 64 ? ~0ull : (1ull << n) - 1ull;
-            rc.bits |= ones << (base + static_cast<uint32_t>(t0) - fp.x0);
-        }
     };
     row_walk(fp, fp.y0 + r, width, height, [&](int32_t t) { add(t, t); }, add);
     return rc;
@@ -620,11 +613,12 @@ struct CountingSink {
 
 // The block's large splats counted a tile row per thread per step (rows in
 // list order, splat after splat): counts added into counts[splat thread]
-// (bit 31 marks a splat with a row that is not one run), tile bits of masked
-// splats or-ed into masks[splat thread].
+// (bit 31 marks a splat with a row that is not one run); each row's first
+// column and count also kept in the row table for a splat that has a place
+// there, so that writing its pairs needs no second row plan.
 __device__ __forceinline__ void count_large_rows(const Footprint* foot, const uint32_t* footRow, uint32_t bigTotal,
                                                  uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t* counts,
-                                                 unsigned long long* masks) {
+                                                 uint2* __restrict__ rowTable) {
     const uint32_t tid = threadIdx.x;
     uint32_t fs = 0;   // the splat of row item j: found by search once, then advanced
     {
@@ -638,10 +632,11 @@ __device__ __forceinline__ void count_large_rows(const Footprint* foot, const ui
     for (uint32_t j = tid; j < rowsTotal; j += kProjectThreads) {
         while (footRow[fs + 1] <= j) ++fs;
         const Footprint fp = foot[fs];
-        const RowCount rc = row_count(fp, j - footRow[fs], width, height);
+        const uint32_t r = j - footRow[fs];
+        const RowCount rc = row_count(fp, r, width, height);
         if (rc.count != 0) atomicAdd(&counts[fp.tid], rc.count);
         if (!rc.regular) atomicOr(&counts[fp.tid], 0x80000000u);
-        if (rc.bits != 0) atomicOr(&masks[fp.tid], rc.bits);
+        if (fp.table != kNoTable) rowTable[fp.table + r] = make_uint2(static_cast<uint32_t>(rc.first), rc.count);
     }
 }
 
@@ -658,7 +653,8 @@ __device__ __forceinline__ void emit_large_rows(const Footprint* foot, const uin
                                              const uint32_t* takenStart, const unsigned long long* low,
                                              uint32_t* rowOff, uint32_t* rowFirst, uint32_t* rowMeta,
                                              uint32_t* scanScratch, unsigned long long blockBase, uint32_t tileShift,
-                                             uint32_t slotBase, const uint32_t* slotOf, const Sink& sink) {
+                                             uint32_t slotBase, const uint32_t* slotOf, const Sink& sink,
+                                             const uint2* __restrict__ rowTable = nullptr) {
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
     uint32_t fs = 0;
@@ -677,11 +673,17 @@ __device__ __forceinline__ void emit_large_rows(const Footprint* foot, const uin
         if (j < rowsTotal) {
             while (footRow[fs + 1] <= j) ++fs;
             const Footprint fp = foot[fs];
-            if ((fp.shMasked & 0x100u) == 0 && (widthBits[fp.tid] & 0x80000000u) == 0) {
+            if ((widthBits[fp.tid] & 0x80000000u) == 0) {
                 const uint32_t r = j - footRow[fs];
-                const RowCount rc = row_count(fp, r, width, height);
-                cnt = rc.count;
-                first = static_cast<uint32_t>(rc.first);
+                if (fp.table != kNoTable) {   // kept by the projection's count
+                    const uint2 e = rowTable[fp.table + r];
+                    cnt = e.y;
+                    first = e.x;
+                } else {
+                    const RowCount rc = row_count(fp, r, width, height);
+                    cnt = rc.count;
+                    first = static_cast<uint32_t>(rc.first);
+                }
                 meta = (fp.y0 + r) | (fp.tid << 16);
             }
         }
@@ -777,13 +779,13 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                     unsigned long long* __restrict__ pairs, uint32_t capacity,
                     unsigned long long* __restrict__ auxOut = nullptr,
                     unsigned long long* __restrict__ depthWordsOut = nullptr,
-                    uint32_t* __restrict__ depthDigits = nullptr) {
+                    uint32_t* __restrict__ depthDigits = nullptr, uint2* __restrict__ rowTable = nullptr,
+                    uint32_t rowCap = 0) {
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];       // block-relative pair offset of each splat
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];  // the same over masked splats only
-    __shared__ unsigned long long sMask[kProjectThreads];
     __shared__ unsigned long long sLow[kProjectThreads];   // depth key << lowBits
     __shared__ uint32_t sRect[kProjectThreads];            // x0 | y0 << 16
     __shared__ uint32_t sWidth[kProjectThreads];
@@ -1084,26 +1086,32 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     }
 
     // The block counts its large splats a tile row per thread per step, into
-    // sSmallStart (zeroed here; the block scan writes it later) and, for a
-    // masked splat, its tile bits into sMask. A row whose hits are not one
-    // run marks its splat (bit 31) for the per-tile emission.
+    // sSmallStart (zeroed here; the block scan writes it later). A row whose
+    // hits are not one run marks its splat (bit 31) for the per-tile
+    // emission.
     uint32_t bigTotal = 0, rowsTotal = 0, bigIdx = 0;
+    uint32_t rowTableAt = kNoTable;
     const bool anyBig = __syncthreads_or(bigHere ? 1 : 0) != 0;   // most blocks have none
     if (anyBig) {
         bigIdx = block_exclusive_scan(bigHere ? 1u : 0u, sScan, &bigTotal);
         const uint32_t rowStart = block_exclusive_scan(bigHere ? rh : 0u, sScan, &rowsTotal);
         sSmallStart[tid] = 0;
-        sMask[tid] = 0ull;
         if (bigHere) {
-            sFoot[bigIdx] = Footprint{cx, cy, ca, cb, cc, cutoff, rect.x, rect.z, rect.y, tid,
-                                      sh | (masked ? 0x100u : 0u)};
+            // A place for the splat's rows in the row table (counters[3]
+            // counts the rows asked for; a splat past the table's end keeps
+            // none and its rows are planned again when its pairs are written).
+            if (rowTable != nullptr) {
+                const uint32_t at = atomicAdd(counters + 3, rh);
+                if (at <= rowCap && rh <= rowCap - at) rowTableAt = at;
+            }
+            sFoot[bigIdx] = Footprint{cx, cy, ca, cb, cc, cutoff, rect.x, rect.z, rect.y, tid, rowTableAt};
             sFootRow[bigIdx] = rowStart;
         }
         if (tid == 0) sFootRow[bigTotal] = rowsTotal;
         __syncthreads();
     }
     if (rowsTotal != 0) {
-        count_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, sSmallStart, sMask);
+        count_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, sSmallStart, rowTable);
         __syncthreads();
     }
     bool irregular = false;
@@ -1111,7 +1119,6 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         const uint32_t v = sSmallStart[tid];
         touched = v & 0x7FFFFFFFu;
         irregular = (v & 0x80000000u) != 0;
-        mask = masked ? sMask[tid] : 0ull;
         if (touched == 0) {   // no tile holds a pixel centre inside it: culled after all
             alive = false;
             key = 0x00FFFFFFu;
@@ -1132,7 +1139,9 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     if constexpr (!kEmit) {
         if (inRange) {
             reinterpret_cast<ulonglong2*>(auxOut)[record] =
-                masked ? make_ulonglong2(mask, maskHi) : make_ulonglong2(irregular ? 1ull : 0ull, 0ull);
+                masked ? make_ulonglong2(mask, maskHi)
+                       : make_ulonglong2((irregular ? 1ull : 0ull) | (static_cast<unsigned long long>(rowTableAt) << 32),
+                                         0ull);
             depthWordsOut[record] = (static_cast<unsigned long long>(key) << 32) | slot;
             atomicAdd(&sDigits[key & 0xFFu], 1u);
             atomicAdd(&sDigits[256 + ((key >> 8) & 0xFFu)], 1u);
@@ -1302,7 +1311,8 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
                   const uint32_t* __restrict__ touchedIn, const unsigned long long* __restrict__ aux,
                   const uint32_t* __restrict__ offsets, uint32_t width, uint32_t height, uint32_t tilesX,
                   uint32_t* __restrict__ err, unsigned long long* __restrict__ pairs, uint32_t capacity,
-                  TrainOutputs train, uint32_t* __restrict__ tileDigits, uint32_t tilePasses) {
+                  TrainOutputs train, uint32_t* __restrict__ tileDigits, uint32_t tilePasses,
+                  const uint2* __restrict__ rowTable) {
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];
@@ -1341,7 +1351,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     if (rowsHere) {
         const ProjRecord rec = proj[slot];
         sFoot[bigIdx] = Footprint{rec.screen.x, rec.screen.y, rec.conic.x, rec.conic.y, rec.conic.z, rec.screen.w,
-                                  rect.x, rect.z, rect.y, tid, sh};
+                                  rect.x, rect.z, rect.y, tid, static_cast<uint32_t>(a.x >> 32)};
         sFootRow[bigIdx] = rowStart;
     }
     if (tid == 0) sFootRow[bigTotal] = rowsTotal;
@@ -1405,7 +1415,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
         if (takenTotal != 0)
             emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, width, height, 0u, tilesX, sWidth, sStart,
                             sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, 0ull, tileShift, slotBase,
-                            nullptr, sink);
+                            nullptr, sink, rowTable);
     }
     if (__ballot_sync(0xFFFFFFFFu, byWarp) != 0)
         emit_by_warp(byWarp, area, sWidth, sRect, sStart, sLow, proj + slotBase, width, height, 0u, tilesX, 0ull,
@@ -1440,7 +1450,8 @@ cudaError_t launch(const FrameParams& f, const FrameParams* fDev, const Src& src
 template <class Src>
 cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRecord* proj, uint4* rects,
                         uint32_t* touched, uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
-                        uint64_t* depthWords, uint32_t* depthDigits, cudaStream_t stream) {
+                        uint64_t* depthWords, uint32_t* depthDigits, uint2* rowTable, uint32_t rowCap,
+                        cudaStream_t stream) {
     const uint32_t stageWords = stage ? f.shWords : 0u;
     const uint32_t shVector = (reinterpret_cast<uintptr_t>(src.sh) & 15u) == 0 ? 1u : 0u;
     const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
@@ -1451,7 +1462,7 @@ cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRe
     project_emit_kernel<Src, false><<<blocks, kProjectThreads, smem, stream>>>(
         f, nullptr, src, TrainOutputs{nullptr, nullptr, nullptr}, stageWords, shVector, proj, rects, touched, keys,
         counters, nullptr, ticket, 0, 0, 0, nullptr, 0, reinterpret_cast<unsigned long long*>(aux),
-        reinterpret_cast<unsigned long long*>(depthWords), depthDigits);
+        reinterpret_cast<unsigned long long*>(depthWords), depthDigits, rowTable, rowCap);
     return cudaGetLastError();
 }
 
@@ -1505,32 +1516,33 @@ cudaError_t launch_project_only(const FrameParams& f, const float4* positions, c
                                 const float* filter3d, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                 uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
                                 uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream) {
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t rpc = f.restPerColour;
     const uint32_t stored = rpc >= 15 ? 3u : rpc >= 8 ? 2u : rpc >= 3 ? 1u : 0u;
     const bool stage = std::min(stored, f.shLimit) > 0 && f.shWords > 0;
     return launch_only(f, PackedSource{positions, shape, sh, filter3d}, stage, proj, rects, touched, keys, counters,
-                       ticket, aux, depthWords, depthDigits, stream);
+                       ticket, aux, depthWords, depthDigits, rowTable, rowCap, stream);
 }
 
 cudaError_t launch_project_points_only(const FrameParams& f, const float4* positions, const uint32_t* colours,
                                        const lrt_point_style& style, ProjRecord* proj, uint4* rects, uint32_t* touched,
                                        uint32_t* keys, uint32_t* counters, uint32_t* ticket, uint64_t* aux,
                                        uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream) {
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     PointSource src{positions, reinterpret_cast<const uint2*>(colours), nullptr, style.size_mode, style.size,
                     style.constant_colour, {style.colour[0], style.colour[1], style.colour[2]}};
     return launch_only(f, src, false, proj, rects, touched, keys, counters, ticket, aux, depthWords, depthDigits,
-                       stream);
+                       rowTable, rowCap, stream);
 }
 
 cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const ProjRecord* proj, const uint4* rects,
                                const uint32_t* touched, const uint64_t* aux, uint32_t width, uint32_t height,
                                uint32_t tilesX, uint32_t* counters, uint64_t* status, uint32_t* ticket,
                                uint32_t* offsets, uint64_t* pairs, uint32_t capacity, uint32_t* tileDigits,
-                               uint32_t tilePasses, cudaStream_t stream, uint32_t* values, uint32_t* emitSlot) {
+                               uint32_t tilePasses, const uint2* rowTable, cudaStream_t stream, uint32_t* values,
+                               uint32_t* emitSlot) {
     if (n == 0) return cudaSuccess;
     const uint32_t perBlock = kProjectThreads * kOffsetItems;
     const uint32_t offsetBlocks = (n + perBlock - 1) / perBlock;
@@ -1542,7 +1554,7 @@ cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const Pr
     emit_pairs_kernel<<<project_partitions(n), kProjectThreads, 0, stream>>>(
         n, proj, rects, touched, reinterpret_cast<const unsigned long long*>(aux), offsets, width, height, tilesX,
         counters + 2, reinterpret_cast<unsigned long long*>(pairs), capacity, TrainOutputs{nullptr, values, emitSlot},
-        tileDigits, tilePasses);
+        tileDigits, tilePasses, rowTable);
     return cudaGetLastError();
 }
 
@@ -1550,11 +1562,12 @@ cudaError_t launch_project_only_train(const FrameParams& f, const float* means, 
                                       const float* quats, const float* logits, const uint16_t* sh, ProjRecord* proj,
                                       uint4* rects, uint32_t* touched, uint32_t* keys, uint32_t* counters,
                                       uint32_t* ticket, uint64_t* aux, uint64_t* depthWords, uint32_t* depthDigits,
-                                cudaStream_t stream) {
+                                uint2* rowTable, uint32_t rowCap, cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     // The DC triple is read from the staged row too, so it is always staged.
     return launch_only(f, RawSource{means, logScales, quats, logits, reinterpret_cast<const uint32_t*>(sh)}, true,
-                       proj, rects, touched, keys, counters, ticket, aux, depthWords, depthDigits, stream);
+                       proj, rects, touched, keys, counters, ticket, aux, depthWords, depthDigits, rowTable, rowCap,
+                       stream);
 }
 
 }  // namespace lrt

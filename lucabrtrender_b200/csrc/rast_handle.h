@@ -36,6 +36,8 @@ struct lrt_rast {
     DeviceBuffer counters;                               // visible, pairs, err, algo err
     DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers
     DeviceBuffer depthWords, depthWordsAlt, splatAux;    // per slot: depth words (two-step frames), aux words
+    DeviceBuffer rowTable;                               // large splats' rows (first column, count)
+    uint32_t rowCap = 0;                                 // its entries
     lrt::SortFault sortFault;                            // lrt_radix_sort's planted fault (tests only)
     DeviceBuffer filterCameras, filterScratch;           // lrt_rast_filter3d's cameras and lowest rate
     uint32_t* hostCounters = nullptr;                    // pinned

@@ -61,8 +61,8 @@ void lrt_rast_destroy(lrt_rast* r) {
     if (r->frameDoneSet) cudaEventSynchronize(r->frameDone);   // a backward may still read the buffers
     for (DeviceBuffer* b : {&r->proj, &r->rects, &r->touched, &r->keys, &r->pairs, &r->pairsAlt,
                             &r->ranges, &r->scanScratch, &r->sortScratch, &r->counters, &r->algoKeysAlt,
-                            &r->algoValsAlt, &r->depthWords, &r->depthWordsAlt, &r->splatAux, &r->pairValues, &r->pairValuesAlt, &r->pairOffsets, &r->pixState,
-                            &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
+                            &r->algoValsAlt, &r->depthWords, &r->depthWordsAlt, &r->splatAux, &r->rowTable,
+                            &r->pairValues, &r->pairValuesAlt, &r->pairOffsets, &r->pixState, &r->pixLast, &r->partials, &r->metricScratch, &r->lossScratch, &r->trainBatchGrad,
                             &r->trainBatchViews, &r->trainBatchLoss, &r->lodBuild.globals,
                             &r->lodBuild.partial, &r->lodBuild.keys, &r->lodBuild.keysAlt, &r->lodBuild.order,
                             &r->lodBuild.orderAlt, &r->lodBuild.sortScratch, &r->lodBuild.status,
@@ -155,6 +155,10 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     LRT_CUDA(r, ensure(r->depthWords, size_t{r->splatCap} * 8), "depth words");
     LRT_CUDA(r, ensure(r->depthWordsAlt, size_t{r->splatCap} * 8), "depth words");
     LRT_CUDA(r, ensure(r->splatAux, size_t{r->splatCap} * 16), "tile masks");
+    // The row table: one entry a slot to start with, grown to what a frame
+    // asked for (a splat past its end is planned again when written).
+    if (r->rowCap == 0) r->rowCap = std::max<uint32_t>(r->splatCap, 1024);
+    LRT_CUDA(r, ensure(r->rowTable, size_t{r->rowCap} * sizeof(uint2)), "row table");
     LRT_CUDA(r, ensure(r->pairOffsets, size_t{std::max(slots, 1u)} * 4), "pair offsets");
     if (train) {
         LRT_CUDA(r, ensure(r->pixState, size_t{s->width} * s->height * 16), "pixel state");
@@ -240,7 +244,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              f, static_cast<const float4*>(g.positions), static_cast<const uint32_t*>(g.colours),
                              c.point->style, static_cast<ProjRecord*>(r->proj.ptr), static_cast<uint4*>(r->rects.ptr),
                              static_cast<uint32_t*>(r->touched.ptr), static_cast<uint32_t*>(r->keys.ptr), counters,
-                             tickets + launch, aux, depthWords, depthDigits, stream),
+                             tickets + launch, aux, depthWords, depthDigits, static_cast<uint2*>(r->rowTable.ptr),
+                             r->rowCap, stream),
                          "points");
             } else if (c.train != nullptr) {
                 const lrt_train_params& t = *c.train;
@@ -251,7 +256,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<const uint16_t*>(t.sh), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
                              static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords,
-                             depthDigits, stream),
+                             depthDigits, static_cast<uint2*>(r->rowTable.ptr), r->rowCap, stream),
                          "project");
             } else {
                 LRT_CUDA(r,
@@ -261,7 +266,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                              static_cast<const float*>(c.packed->filter3d), static_cast<ProjRecord*>(r->proj.ptr),
                              static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
                              static_cast<uint32_t*>(r->keys.ptr), counters, tickets + launch, aux, depthWords,
-                             depthDigits, stream),
+                             depthDigits, static_cast<uint2*>(r->rowTable.ptr), r->rowCap, stream),
                          "project");
             }
             base += c.count;
@@ -283,8 +288,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                                          static_cast<uint4*>(r->rects.ptr), static_cast<uint32_t*>(r->touched.ptr),
                                          aux, s->width, s->height, tilesX, counters, status, tickets + launches,
                                          static_cast<uint32_t*>(r->pairOffsets.ptr), pairBuf, r->pairCap,
-                                         tilePasses != 0 ? tileDigits : nullptr, tilePasses, stream, valueBuf,
-                                         emitSlot),
+                                         tilePasses != 0 ? tileDigits : nullptr, tilePasses,
+                                         static_cast<const uint2*>(r->rowTable.ptr), stream, valueBuf, emitSlot),
                  "emit");
         LRT_CUDA(r, cudaEventRecord(r->ev[5], stream), "event");
         // --- stable sort on the tile bits + ranges -------------------------------------------
@@ -382,6 +387,9 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         r->pairCap = grow(r->pairCap, pairs);   // draw again with room for every pair
         statusBits &= ~lrt::kErrOverflow;
     }
+    // Rows the frame's large splats asked for beyond the row table: the next
+    // frame's table holds them (this one planned those rows again).
+    if (r->hostCounters[3] > r->rowCap) r->rowCap = grow(r->rowCap, r->hostCounters[3]);
 
     r->debug.proj = r->proj.ptr;
     r->debug.rects = r->rects.ptr;
