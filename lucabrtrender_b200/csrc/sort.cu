@@ -9,9 +9,11 @@
 // every pass's digits, then one kernel per 8-bit digit that:
 //   1. takes the next partition (3072 keys, 4096 in sorts of more than 2^23
 //      keys) by atomic ticket (launch order),
-//   2. ranks its keys stably inside each warp with __match_any_sync (keys are
-//      warp-striped, so a warp's item j covers 32 consecutive keys and items
-//      are visited in order), and across warps with per-warp digit counts,
+//   2. ranks its keys stably inside each warp (the lanes sharing a digit
+//      from nine ballots: one per digit bit, one for lanes without a key;
+//      keys are warp-striped, so a warp's item j covers 32 consecutive keys
+//      and items are visited in order), and across warps with per-warp
+//      digit counts,
 //   3. publishes its per-digit counts and resolves the prefix of all earlier
 //      partitions by decoupled look-back (bounded waits),
 //   4. scatters keys (and values) into shared memory in digit order, then
@@ -83,6 +85,20 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_
     const uint32_t before = warp == 0 ? 0 : sWarp[warp - 1];
     __syncthreads();
     return before + x - v;
+}
+
+// The lanes of the warp holding the same digit d (0..255, or kDigits for no
+// key), from one ballot per digit bit and one for the no-key lanes.
+__device__ __forceinline__ uint32_t match_digit(uint32_t d) {
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, d >= kDigits);
+    m = d >= kDigits ? m : ~m;
+#pragma unroll
+    for (uint32_t b = 0; b < 8; ++b) {
+        const bool bit = ((d >> b) & 1u) != 0;
+        const uint32_t v = __ballot_sync(0xFFFFFFFFu, bit);
+        m &= bit ? v : ~v;
+    }
+    return m;
 }
 
 template <typename K>
@@ -161,7 +177,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     for (uint32_t j0 = 0; j0 < kItems; j0 += kRankGroup) {
         uint32_t peers[kRankGroup];
 #pragma unroll
-        for (uint32_t q = 0; q < kRankGroup; ++q) peers[q] = __match_any_sync(0xFFFFFFFFu, dig[j0 + q]);
+        for (uint32_t q = 0; q < kRankGroup; ++q) peers[q] = match_digit(dig[j0 + q]);
 #pragma unroll
         for (uint32_t q = 0; q < kRankGroup; ++q) {
             const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers[q]));
