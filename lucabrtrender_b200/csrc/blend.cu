@@ -488,11 +488,23 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
                           uint2* ranges, uint32_t tiles, cudaStream_t stream) {
-    cudaError_t e = cudaMemsetAsync(ranges, 0, sizeof(uint2) * tiles, stream);
+    cudaError_t e = launch_zero(ranges, sizeof(uint2) * tiles, stream);
     if (e != cudaSuccess || cap == 0) return e;
     const uint32_t threads = (cap + kRangeRun - 1) / kRangeRun;
     ranges_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs),
                                                              dCount, cap, tileShift, ranges);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void publish_counters_kernel(const uint32_t* __restrict__ counters, uint32_t* hostMapped) {
+    if (threadIdx.x < 4) hostMapped[threadIdx.x] = counters[threadIdx.x];
+    __threadfence_system();
+}
+}  // namespace
+
+cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapped, cudaStream_t stream) {
+    publish_counters_kernel<<<1, 32, 0, stream>>>(counters, hostMapped);
     return cudaGetLastError();
 }
 

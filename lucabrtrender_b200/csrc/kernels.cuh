@@ -116,6 +116,19 @@ cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, u
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
                           uint2* ranges, uint32_t tiles, cudaStream_t stream);
 
+// `bytes` (a multiple of 4, from a 4-byte aligned `p`) set to zero by a
+// kernel. The frame path clears its scratch this way rather than by
+// cudaMemsetAsync, which the driver may hand to a copy engine, where it
+// would queue behind a caller's device-to-host copies.
+cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t stream);
+
+// The frame's four counters stored into pinned host memory by a kernel
+// (`hostMapped` is the device's address of that memory), not by a copy: a
+// device-to-host copy queues behind whatever the copy engine already holds,
+// such as a caller's readback of the previous image, and the frame's stream
+// would wait for it.
+cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapped, cudaStream_t stream);
+
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream);
 

@@ -41,6 +41,7 @@ struct lrt_rast {
     lrt::SortFault sortFault;                            // lrt_radix_sort's planted fault (tests only)
     DeviceBuffer filterCameras, filterScratch;           // lrt_rast_filter3d's cameras and lowest rate
     uint32_t* hostCounters = nullptr;                    // pinned
+    uint32_t* hostCountersDev = nullptr;                 // the device's address of hostCounters
     // ev[0..5]: a frame's stage times; ev[6]: an enqueued training frame's
     // counts copied to the host; ev[7..9]: the training backward's times.
     cudaEvent_t ev[10] = {};
@@ -75,6 +76,7 @@ struct lrt_rast {
     // ring of pinned slots, each with the event that marks its frame done.
     static constexpr uint32_t kRing = 16;
     uint32_t* ringHost = nullptr;               // pinned, 4 words per slot
+    uint32_t* ringHostDev = nullptr;            // the device's address of ringHost
     cudaEvent_t ringEvent[kRing] = {};
     uint32_t ringCap[kRing] = {};               // the pair capacity each frame ran with
     uint64_t ringHead = 0, ringTail = 0;        // next slot to fill; oldest slot not read

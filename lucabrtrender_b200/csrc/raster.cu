@@ -42,6 +42,9 @@ int lrt_rast_create(lrt_rast** out, int device) {
     r->device = device;
     bool ok = cudaMallocHost(reinterpret_cast<void**>(&r->hostCounters), 64) == cudaSuccess &&
               cudaMallocHost(reinterpret_cast<void**>(&r->ringHost), lrt_rast::kRing * 16) == cudaSuccess &&
+              cudaHostGetDevicePointer(reinterpret_cast<void**>(&r->hostCountersDev), r->hostCounters, 0) ==
+                  cudaSuccess &&
+              cudaHostGetDevicePointer(reinterpret_cast<void**>(&r->ringHostDev), r->ringHost, 0) == cudaSuccess &&
               ensure(r->counters, 64) == cudaSuccess;
     for (auto& e : r->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
     for (auto& e : r->ringEvent) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
@@ -223,8 +226,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                  ensure(r->sortScratch,
                         std::max(lrt::sort_scratch_bytes(r->pairCap, tileBits), lrt::sort_scratch_bytes(slots, 24))),
                  "sort scratch");
-        LRT_CUDA(r, cudaMemsetAsync(counters, 0, 16, stream), "counters");
-        LRT_CUDA(r, cudaMemsetAsync(r->scanScratch.ptr, 0, statusBytes, stream), "projection scratch");
+        LRT_CUDA(r, lrt::launch_zero(counters, 16, stream), "counters");
+        LRT_CUDA(r, lrt::launch_zero(r->scanScratch.ptr, statusBytes, stream), "projection scratch");
         uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
         uint32_t* valueBuf = train && !lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
         uint32_t* emitSlot = train && lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
@@ -335,9 +338,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
         const bool ring = deferred && !train;
         const uint32_t slot = static_cast<uint32_t>(r->ringHead % lrt_rast::kRing);
-        LRT_CUDA(r,
-                 cudaMemcpyAsync(ring ? r->ringHost + 4 * slot : r->hostCounters, counters, 16,
-                                 cudaMemcpyDeviceToHost, stream),
+        LRT_CUDA(r, lrt::launch_publish_counters(counters, ring ? r->ringHostDev + 4 * slot : r->hostCountersDev, stream),
                  "readback");
         LRT_CUDA(r, cudaEventRecord(r->frameDone, stream), "event");
         r->frameDoneSet = true;
@@ -809,11 +810,16 @@ int lrt_rast_render_async(lrt_rast* r, const lrt_projection* pr, const lrt_splat
         return fail(r, LRT_DEVICE_FAILURE, "waiting for an enqueued frame failed");
     // Enqueued only when a frame of this shape has run with a wait and the
     // last counts read leave a quarter of the pair buffer free; otherwise the
-    // frame waits (and draws again with grown buffers if it has to).
+    // frame waits (and draws again with grown buffers if it has to). A frame
+    // of a known shape whose last counts leave less than that grows the
+    // buffer first, so that the frames after it are enqueued again.
     const uint32_t slots = total_slots(clouds);
     const uint64_t wanted = uint64_t{r->plainSeenPairs} + r->plainSeenPairs / 4;
-    const bool deferred = r->plainSized && r->plainSlots == slots && r->plainWidth == s->width &&
-                          r->plainHeight == s->height && !s->time_stages && wanted <= r->pairCap;
+    const bool sameShape = r->plainSized && r->plainSlots == slots && r->plainWidth == s->width &&
+                           r->plainHeight == s->height;
+    const bool deferred = sameShape && !s->time_stages && wanted <= r->pairCap;
+    if (sameShape && !s->time_stages && wanted > r->pairCap)
+        r->pairCap = grow(r->pairCap, static_cast<uint32_t>(std::min<uint64_t>(wanted, 0xFFFFFFFFull)));
     if (!deferred) {
         lrt_frame_stats stats{};
         const int code = render_frame(r, pr, clouds, s, targets, &stats, streamPtr, false, frameStart);

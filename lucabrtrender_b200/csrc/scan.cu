@@ -135,7 +135,31 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_
     }
 }
 
+__global__ void zero_kernel(uint32_t* __restrict__ p, size_t words) {
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    // Words before the first 16-byte boundary, then 16-byte stores, then the
+    // tail.
+    const size_t head = min(words, static_cast<size_t>((16u - (reinterpret_cast<uintptr_t>(p) & 15u)) & 15u) / 4u);
+    if (i < head) p[i] = 0u;
+    const size_t quads = (words - head) / 4;
+    uint4* q = reinterpret_cast<uint4*>(p + head);
+    for (size_t k = i; k < quads; k += stride) q[k] = make_uint4(0u, 0u, 0u, 0u);
+    const size_t tail = head + quads * 4;
+    if (i < words - tail) p[tail + i] = 0u;
+}
+
 }  // namespace
+
+cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0) return cudaSuccess;
+    if ((bytes & 3u) != 0 || (reinterpret_cast<uintptr_t>(p) & 3u) != 0) return cudaErrorInvalidValue;
+    const size_t words = bytes / 4;
+    const size_t quads = (words + 3) / 4;
+    const uint32_t blocks = static_cast<uint32_t>(std::min<size_t>(std::max<size_t>((quads + 255) / 256, 1), 148 * 8));
+    zero_kernel<<<blocks, 256, 0, stream>>>(static_cast<uint32_t*>(p), words);
+    return cudaGetLastError();
+}
 
 size_t scan_scratch_bytes(uint32_t n) {
     const size_t parts = (static_cast<size_t>(n) + kScanTile - 1) / kScanTile;

@@ -293,7 +293,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
     W* lookback = reinterpret_cast<W*>(s + 64 + kMaxPasses * kDigits * 4);
     const size_t bytes = sort_scratch_bytes(cap, bits);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, bytes, stream);
+    cudaError_t e = launch_zero(scratch, bytes, stream);
     if (e != cudaSuccess) return e;
     const uint32_t spinLimit = fault != nullptr && fault->pollLimit != 0 ? fault->pollLimit : kSpinLimit;
     if (fault != nullptr && fault->skipFirstPartition != 0) {

@@ -94,3 +94,42 @@ def test_an_enqueued_frame_that_overflows_is_reported_and_redrawn_exactly():
     finally:
         raster.close()
         reference.close()
+
+
+def test_a_shape_whose_pairs_crowd_the_buffer_grows_it_and_stays_exact():
+    # 20k splats: the first frame's pair buffer holds 80k pairs. A view that
+    # emits between 64k and 80k fits it, but leaves less than a quarter free,
+    # so the next enqueued frame of that view grows the buffer (and waits);
+    # every image stays equal to a fresh handle's.
+    scene = H.synthetic_scene(20_000, 64, 64, seed=33, log_scale_mean=-3.0)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings(width=256, height=256)
+    probe = L.TileRasterizer.create(0)
+    try:
+        view = None
+        t = L.RenderTargets(256, 256)
+        for k in range(60):
+            radius = 9.0 * (1.6 / 9.0) ** (k / 59)
+            pairs = probe.render(orbit(0, 256, 256, radius=radius), instances, settings, t).pairs
+            if 64_000 < pairs <= 80_000:
+                view = orbit(0, 256, 256, radius=radius)
+                break
+    finally:
+        probe.close()
+    assert view is not None, "no view of this scene emits between 64k and 80k pairs"
+    raster = L.TileRasterizer.create(0)
+    reference = L.TileRasterizer.create(0)
+    try:
+        want = L.RenderTargets(256, 256)
+        reference.render(view, instances, settings, want)
+        first = L.RenderTargets(256, 256)
+        raster.render(view, instances, settings, first)   # sizes the shape: 80k pairs of buffer
+        got = [L.RenderTargets(256, 256) for _ in range(4)]
+        for g in got:
+            raster.render_async(view, instances, settings, g)
+        raster.settle()
+        for g in [first] + got:
+            assert torch.equal(g.colour, want.colour) and torch.equal(g.depth, want.depth)
+    finally:
+        raster.close()
+        reference.close()
