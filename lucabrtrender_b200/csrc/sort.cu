@@ -10,7 +10,8 @@
 //   1. takes the next partition (3072 keys, 4096 in sorts of more than 2^23
 //      keys) by atomic ticket (launch order),
 //   2. ranks its keys stably inside each warp (the lanes sharing a digit
-//      from nine ballots: one per digit bit, one for lanes without a key;
+//      from eight ballots, one per digit bit; a partial last partition is
+//      padded with all-ones keys, which sort after every real key;
 //      keys are warp-striped, so a warp's item j covers 32 consecutive keys
 //      and items are visited in order), and across warps with per-warp
 //      digit counts,
@@ -87,11 +88,10 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_
     return before + x - v;
 }
 
-// The lanes of the warp holding the same digit d (0..255, or kDigits for no
-// key), from one ballot per digit bit and one for the no-key lanes.
+// The lanes of the warp holding the same digit d (0..255), from one ballot
+// per digit bit.
 __device__ __forceinline__ uint32_t match_digit(uint32_t d) {
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, d >= kDigits);
-    m = d >= kDigits ? m : ~m;
+    uint32_t m = 0xFFFFFFFFu;
 #pragma unroll
     for (uint32_t b = 0; b < 8; ++b) {
         const bool bit = ((d >> b) & 1u) != 0;
@@ -157,9 +157,14 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     for (uint32_t j = 0; j < kItems; ++j) {
         const uint32_t idx = wbase + j * 32 + lane;
         const bool ok = idx < n;
-        key[j] = ok ? kin[idx] : K(0);
+        // Past the end (only in the last partition): all-ones keys, digit
+        // 255 in every pass. They rank after every real key (the ranking is
+        // stable and they come last), so they take the block's last places,
+        // which the write-out never reaches; their count only inflates the
+        // last partition's own digit-255 total, which no partition reads.
+        key[j] = ok ? kin[idx] : ~K(0);
         if (kValues) val[j] = ok ? vin[idx] : 0u;
-        dig[j] = ok ? digit_of(key[j], shift) : kDigits;
+        dig[j] = digit_of(key[j], shift);
     }
 
     // Stable rank inside the warp: peers with equal digits, lower lanes first;
@@ -182,7 +187,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
         for (uint32_t q = 0; q < kRankGroup; ++q) {
             const uint32_t leader = 31u - static_cast<uint32_t>(__clz(peers[q]));
             rank[j0 + q] = 0;
-            if (lane == leader && dig[j0 + q] < kDigits)
+            if (lane == leader)
                 rank[j0 + q] = atomicAdd(&sWarpHist[warp][dig[j0 + q]], static_cast<uint32_t>(__popc(peers[q])));
         }
 #pragma unroll
@@ -261,11 +266,9 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 #pragma unroll
     for (uint32_t j = 0; j < kItems; ++j) {
         const uint32_t d = dig[j];
-        if (d < kDigits) {
-            const uint32_t at = sBlockStart[d] + sWarpHist[warp][d] + rank[j];
-            sKeys[at] = key[j];
-            if (kValues) sVals[at] = val[j];
-        }
+        const uint32_t at = sBlockStart[d] + sWarpHist[warp][d] + rank[j];
+        sKeys[at] = key[j];
+        if (kValues) sVals[at] = val[j];
     }
     __syncthreads();
 
