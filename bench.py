@@ -674,23 +674,29 @@ def run_ours(args) -> None:
         for k in range(max(3, args.warmup)):
             train_step(k)
         torch.cuda.synchronize(dev)
-        fb_ms, bwd_blend, bwd_proj, fwd_stats = [], [], [], []
+        bwd_blend, bwd_proj, fwd_stats = [], [], []
+        # Steps run back to back, as a training loop runs them (the host
+        # waits only inside each backward, for its forward's counts); each
+        # step is timed on the device from after its L2 flush to its end.
+        fb_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        fb_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        torch.cuda.synchronize(dev)
         w0 = time.time()
         for k in range(args.steps):
             flush.fill_(float(k))
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
+            fb_start[k].record(stream)
             train_step(k)
-            b.record(stream)
-            b.synchronize()
-            fb_ms.append(a.elapsed_time(b))
+            fb_end[k].record(stream)
+        torch.cuda.synchronize(dev)
+        clocks.window(w0, time.time())
+        fb_ms = [a.elapsed_time(b) for a, b in zip(fb_start, fb_end)]
+        # The backward's and the forward's stage breakdowns, from extra steps
+        # (not part of the timed steps above).
+        for k in range(3):
+            train_step(k)
             t_blend, t_proj = L.train.backward_times(raster)
             bwd_blend.append(t_blend)
             bwd_proj.append(t_proj)
-        clocks.window(w0, time.time())
-        # The forward's stage breakdown, from extra steps that wait per stage
-        # (not part of the timed steps above).
         train_settings.time_stages = True
         for k in range(3):
             train_step(k)
