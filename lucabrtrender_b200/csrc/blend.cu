@@ -487,8 +487,8 @@ blend_batch_kernel(BlendParams bp, const ViewParams* __restrict__ views, uint32_
 }  // namespace
 
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
-                          uint2* ranges, uint32_t tiles, cudaStream_t stream) {
-    cudaError_t e = launch_zero(ranges, sizeof(uint2) * tiles, stream);
+                          uint2* ranges, uint32_t tiles, cudaStream_t stream, bool rangesZeroed) {
+    cudaError_t e = rangesZeroed ? cudaSuccess : launch_zero(ranges, sizeof(uint2) * tiles, stream);
     if (e != cudaSuccess || cap == 0) return e;
     const uint32_t threads = (cap + kRangeRun - 1) / kRangeRun;
     ranges_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs),

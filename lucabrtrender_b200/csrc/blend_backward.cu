@@ -22,7 +22,11 @@ __device__ __forceinline__ float srgb_to_linear_slope(float c) {
     return 2.4f / 1.055f * lrt_pow((c + 0.055f) / 1.055f, 1.4f);
 }
 
-constexpr uint32_t kGrads = 9;   // d/d(centre x, centre y, conic a, b, c, alpha, r, g, b) per pair
+// Per pair, as written: d/d(centre x, centre y, conic a, b, c, alpha, r, g,
+// b). While a batch is summed, slots 0, 1 and 3 hold the sums of pdx, pdy
+// and pdx dy (pdx = dL/dpower dx, pdy = dL/dpower dy); the record's conic
+// and the factor 2 are applied when the partials are written.
+constexpr uint32_t kGrads = 9;
 constexpr uint32_t kGradStride = 12;   // floats per pair in the partials buffer (three 16-byte vectors)
 constexpr uint32_t kBwdPix = 2;        // pixels a thread
 
@@ -275,14 +279,19 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
                         Bb[q] = __fmaf_rn(alpha, col.z - Bb[q], Bb[q]);
                         T[q] = Ti;
                         if (raw <= 0.99f) {
+                            // The centre's gradient, -2 (a pdx + b pdy, b pdx + c pdy),
+                            // is linear in (pdx, pdy) with the record's conic: the
+                            // pixels' pdx and pdy are summed here and the conic
+                            // applied once per record when the partials are written
+                            // (and the factor 2 of the b term likewise).
                             v[5] += dAlpha * e;
                             const float dPower = -0.5f * alpha * dAlpha;
                             const float pdx = dPower * dx, pdy = dPower * dy[q];
                             v[2] += pdx * dx;
-                            v[3] += 2.0f * pdx * dy[q];
+                            v[3] += pdx * dy[q];
                             v[4] += pdy * dy[q];
-                            v[0] += -2.0f * __fmaf_rn(conic.x, pdx, conic.y * pdy);
-                            v[1] += -2.0f * __fmaf_rn(conic.y, pdx, conic.z * pdy);
+                            v[0] += pdx;
+                            v[1] += pdy;
                         }
                     }
                 }
@@ -315,8 +324,11 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
                     for (uint32_t k = 0; k < kGrads; ++k) sum[k] += sPart[w][m][k];
                 }
             }
+            const float4 conic = sRec[m].conic;
+            const float gx = -2.0f * __fmaf_rn(conic.x, sum[0], conic.y * sum[1]);
+            const float gy = -2.0f * __fmaf_rn(conic.y, sum[0], conic.z * sum[1]);
             float4* out = reinterpret_cast<float4*>(partials + static_cast<size_t>(sEmit[m]) * kGradStride);
-            out[0] = make_float4(sum[0], sum[1], sum[2], sum[3]);
+            out[0] = make_float4(gx, gy, sum[2], 2.0f * sum[3]);
             out[1] = make_float4(sum[4], sum[5], sum[6], sum[7]);
             out[2] = make_float4(sum[8], 0.0f, 0.0f, 0.0f);
         }

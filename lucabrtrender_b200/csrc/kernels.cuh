@@ -103,24 +103,33 @@ struct SortFault {
 size_t sort_scratch_bytes(uint32_t cap, uint32_t bits);
 // presetHist: the digit counts of every pass (256 a pass, from firstBit up),
 // already counted by the kernel that wrote the keys; the sort then skips its
-// own counting pass over the keys.
+// own counting pass over the keys. scratchZeroed: the caller has zeroed the
+// sort_scratch_bytes(cap, bits) bytes of scratch on the stream already.
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
                             uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr,
-                            const uint32_t* presetHist = nullptr);
+                            const uint32_t* presetHist = nullptr, bool scratchZeroed = false);
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch,
                             uint32_t* err, bool* resultInAlt, cudaStream_t stream, const SortFault* fault = nullptr,
-                            const uint32_t* presetHist = nullptr);
+                            const uint32_t* presetHist = nullptr, bool scratchZeroed = false);
 
+// rangesZeroed: the caller has zeroed the `tiles` ranges on the stream already.
 cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_t cap, uint32_t tileShift,
-                          uint2* ranges, uint32_t tiles, cudaStream_t stream);
+                          uint2* ranges, uint32_t tiles, cudaStream_t stream, bool rangesZeroed = false);
 
 // `bytes` (a multiple of 4, from a 4-byte aligned `p`) set to zero by a
 // kernel. The frame path clears its scratch this way rather than by
 // cudaMemsetAsync, which the driver may hand to a copy engine, where it
 // would queue behind a caller's device-to-host copies.
 cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t stream);
+// Up to kZeroRegions such regions in one launch.
+struct ZeroRegion {
+    void* p;
+    size_t bytes;
+};
+constexpr uint32_t kZeroRegions = 6;
+cudaError_t launch_zero_regions(const ZeroRegion* regions, uint32_t count, cudaStream_t stream);
 
 // The frame's four counters stored into pinned host memory by a kernel
 // (`hostMapped` is the device's address of that memory), not by a copy: a

@@ -222,12 +222,19 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
             LRT_CUDA(r, ensure(r->pairValues, size_t{r->pairCap} * 4), "pair values");
             if (!lowIsEmit) LRT_CUDA(r, ensure(r->pairValuesAlt, size_t{r->pairCap} * 4), "pair values");
         }
-        LRT_CUDA(r,
-                 ensure(r->sortScratch,
-                        std::max(lrt::sort_scratch_bytes(r->pairCap, tileBits), lrt::sort_scratch_bytes(slots, 24))),
-                 "sort scratch");
-        LRT_CUDA(r, lrt::launch_zero(counters, 16, stream), "counters");
-        LRT_CUDA(r, lrt::launch_zero(r->scanScratch.ptr, statusBytes, stream), "projection scratch");
+        // The two sorts' scratch side by side, so that one launch clears it
+        // with the counters, the projection's scratch and the tile ranges.
+        const size_t depthScratch = lrt::sort_scratch_bytes(slots, 24);
+        const size_t tileScratchAt = (depthScratch + 255) & ~size_t{255};
+        const size_t tileScratch = lrt::sort_scratch_bytes(r->pairCap, tileBits);
+        LRT_CUDA(r, ensure(r->sortScratch, tileScratchAt + tileScratch), "sort scratch");
+        void* tileSortScratch = static_cast<char*>(r->sortScratch.ptr) + tileScratchAt;
+        const lrt::ZeroRegion clear[] = {{counters, 16},
+                                         {r->scanScratch.ptr, statusBytes},
+                                         {r->sortScratch.ptr, depthScratch},
+                                         {tileSortScratch, tileScratch},
+                                         {r->ranges.ptr, size_t{tiles} * sizeof(uint2)}};
+        LRT_CUDA(r, lrt::launch_zero_regions(clear, 5, stream), "frame scratch");
         uint64_t* pairBuf = static_cast<uint64_t*>(r->pairs.ptr);
         uint32_t* valueBuf = train && !lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
         uint32_t* emitSlot = train && lowIsEmit ? static_cast<uint32_t*>(r->pairValues.ptr) : nullptr;
@@ -281,7 +288,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         LRT_CUDA(r,
                  lrt::launch_sort_u64(depthWords, static_cast<uint64_t*>(r->depthWordsAlt.ptr), nullptr, nullptr,
                                       nullptr, slots, 32, 24, r->sortScratch.ptr, err, &depthInAlt, stream, nullptr,
-                                      depthDigits),
+                                      depthDigits, true),
                  "depth sort");
         const uint64_t* byDepth = depthInAlt ? static_cast<const uint64_t*>(r->depthWordsAlt.ptr) : depthWords;
         LRT_CUDA(r, cudaEventRecord(r->ev[4], stream), "event");
@@ -300,14 +307,14 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
         LRT_CUDA(r,
                  lrt::launch_sort_u64(pairBuf, static_cast<uint64_t*>(r->pairsAlt.ptr), valueBuf,
                                       valueBuf != nullptr ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : nullptr,
-                                      counters + 1, r->pairCap, 32, tileBits, r->sortScratch.ptr, err, &inAlt, stream,
-                                      nullptr, tilePasses != 0 ? tileDigits : nullptr),
+                                      counters + 1, r->pairCap, 32, tileBits, tileSortScratch, err, &inAlt, stream,
+                                      nullptr, tilePasses != 0 ? tileDigits : nullptr, true),
                  "tile sort");
         sorted = inAlt ? static_cast<uint64_t*>(r->pairsAlt.ptr) : pairBuf;
         if (valueBuf != nullptr) sortedValues = inAlt ? static_cast<uint32_t*>(r->pairValuesAlt.ptr) : valueBuf;
         LRT_CUDA(r,
                  lrt::launch_ranges(sorted, counters + 1, r->pairCap, 32, static_cast<uint2*>(r->ranges.ptr), tiles,
-                                    stream),
+                                    stream, true),
                  "ranges");
         LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
 

@@ -135,9 +135,9 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_
     }
 }
 
-__global__ void zero_kernel(uint32_t* __restrict__ p, size_t words) {
+__device__ __forceinline__ void zero_words(uint32_t* __restrict__ p, size_t words) {
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
-    size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     // Words before the first 16-byte boundary, then 16-byte stores, then the
     // tail.
     const size_t head = min(words, static_cast<size_t>((16u - (reinterpret_cast<uintptr_t>(p) & 15u)) & 15u) / 4u);
@@ -149,15 +149,43 @@ __global__ void zero_kernel(uint32_t* __restrict__ p, size_t words) {
     if (i < words - tail) p[tail + i] = 0u;
 }
 
+__global__ void zero_kernel(uint32_t* __restrict__ p, size_t words) { zero_words(p, words); }
+
+struct ZeroList {
+    ZeroRegion r[kZeroRegions];
+    uint32_t count;
+};
+__global__ void zero_regions_kernel(ZeroList list) {
+    for (uint32_t k = 0; k < list.count; ++k) zero_words(static_cast<uint32_t*>(list.r[k].p), list.r[k].bytes / 4);
+}
+
+uint32_t zero_blocks(size_t bytes) {
+    const size_t quads = (bytes / 4 + 3) / 4;
+    return static_cast<uint32_t>(std::min<size_t>(std::max<size_t>((quads + 255) / 256, 1), 148 * 8));
+}
+
 }  // namespace
 
 cudaError_t launch_zero(void* p, size_t bytes, cudaStream_t stream) {
     if (bytes == 0) return cudaSuccess;
     if ((bytes & 3u) != 0 || (reinterpret_cast<uintptr_t>(p) & 3u) != 0) return cudaErrorInvalidValue;
-    const size_t words = bytes / 4;
-    const size_t quads = (words + 3) / 4;
-    const uint32_t blocks = static_cast<uint32_t>(std::min<size_t>(std::max<size_t>((quads + 255) / 256, 1), 148 * 8));
-    zero_kernel<<<blocks, 256, 0, stream>>>(static_cast<uint32_t*>(p), words);
+    zero_kernel<<<zero_blocks(bytes), 256, 0, stream>>>(static_cast<uint32_t*>(p), bytes / 4);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_regions(const ZeroRegion* regions, uint32_t count, cudaStream_t stream) {
+    if (count > kZeroRegions) return cudaErrorInvalidValue;
+    ZeroList list{};
+    size_t largest = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        if ((regions[k].bytes & 3u) != 0 || (reinterpret_cast<uintptr_t>(regions[k].p) & 3u) != 0)
+            return cudaErrorInvalidValue;
+        list.r[k] = regions[k];
+        largest = std::max(largest, regions[k].bytes);
+    }
+    list.count = count;
+    if (largest == 0) return cudaSuccess;
+    zero_regions_kernel<<<zero_blocks(largest), 256, 0, stream>>>(list);
     return cudaGetLastError();
 }
 

@@ -285,7 +285,8 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
 template <typename K, bool kValues, typename W, uint32_t kItems>
 cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                       uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
-                      bool* resultInAlt, cudaStream_t stream, const SortFault* fault, const uint32_t* presetHist) {
+                      bool* resultInAlt, cudaStream_t stream, const SortFault* fault, const uint32_t* presetHist,
+                      bool scratchZeroed) {
     *resultInAlt = false;
     if (cap == 0 || bits == 0) return cudaSuccess;
     constexpr uint32_t kTile = kItems * kSortThreads;
@@ -296,7 +297,7 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* hist = reinterpret_cast<uint32_t*>(s + 64);                   // passes x 256
     W* lookback = reinterpret_cast<W*>(s + 64 + kMaxPasses * kDigits * 4);
     const size_t bytes = sort_scratch_bytes(cap, bits);
-    cudaError_t e = launch_zero(scratch, bytes, stream);
+    cudaError_t e = scratchZeroed ? cudaSuccess : launch_zero(scratch, bytes, stream);
     if (e != cudaSuccess) return e;
     const uint32_t spinLimit = fault != nullptr && fault->pollLimit != 0 ? fault->pollLimit : kSpinLimit;
     if (fault != nullptr && fault->skipFirstPartition != 0) {
@@ -351,45 +352,45 @@ template <typename K, bool kValues>
 cudaError_t sort_dispatch(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, const uint32_t* dCount,
                           uint32_t cap, uint32_t firstBit, uint32_t bits, void* scratch, uint32_t* err,
                           bool* resultInAlt, cudaStream_t stream, const SortFault* fault,
-                          const uint32_t* presetHist) {
+                          const uint32_t* presetHist, bool scratchZeroed) {
     const bool wide = cap > kSmallSortMax || (fault != nullptr && fault->wideWords != 0);
     const bool large = cap > kLargeKeys;
     if (!wide && !large)
         return sort_impl<K, kValues, uint32_t, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
-                                                           scratch, err, resultInAlt, stream, fault, presetHist);
+                                                           scratch, err, resultInAlt, stream, fault, presetHist, scratchZeroed);
     if (!wide)
         return sort_impl<K, kValues, uint32_t, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits,
-                                                            scratch, err, resultInAlt, stream, fault, presetHist);
+                                                            scratch, err, resultInAlt, stream, fault, presetHist, scratchZeroed);
     if (!large)
         return sort_impl<K, kValues, unsigned long long, kSortItems>(keys, keysAlt, vals, valsAlt, dCount, cap,
                                                                      firstBit, bits, scratch, err, resultInAlt, stream,
-                                                                     fault, presetHist);
+                                                                     fault, presetHist, scratchZeroed);
     return sort_impl<K, kValues, unsigned long long, kLargeItems>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit,
-                                                                  bits, scratch, err, resultInAlt, stream, fault, presetHist);
+                                                                  bits, scratch, err, resultInAlt, stream, fault, presetHist, scratchZeroed);
 }
 
 cudaError_t launch_sort_u64(uint64_t* keys, uint64_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
                             void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
-                            const SortFault* fault, const uint32_t* presetHist) {
+                            const SortFault* fault, const uint32_t* presetHist, bool scratchZeroed) {
     if (bits > 64 || firstBit + bits > 64 || (bits + 7) / 8 > kMaxPasses) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_dispatch<uint64_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream, fault, presetHist);
+                                         resultInAlt, stream, fault, presetHist, scratchZeroed);
     return sort_dispatch<uint64_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream, fault, presetHist);
+                                      resultInAlt, stream, fault, presetHist, scratchZeroed);
 }
 
 cudaError_t launch_sort_u32(uint32_t* keys, uint32_t* keysAlt, uint32_t* vals, uint32_t* valsAlt,
                             const uint32_t* dCount, uint32_t cap, uint32_t firstBit, uint32_t bits,
                             void* scratch, uint32_t* err, bool* resultInAlt, cudaStream_t stream,
-                            const SortFault* fault, const uint32_t* presetHist) {
+                            const SortFault* fault, const uint32_t* presetHist, bool scratchZeroed) {
     if (bits > 32 || firstBit + bits > 32) return cudaErrorInvalidValue;
     if (vals != nullptr)
         return sort_dispatch<uint32_t, true>(keys, keysAlt, vals, valsAlt, dCount, cap, firstBit, bits, scratch, err,
-                                         resultInAlt, stream, fault, presetHist);
+                                         resultInAlt, stream, fault, presetHist, scratchZeroed);
     return sort_dispatch<uint32_t, false>(keys, keysAlt, nullptr, nullptr, dCount, cap, firstBit, bits, scratch, err,
-                                      resultInAlt, stream, fault, presetHist);
+                                      resultInAlt, stream, fault, presetHist, scratchZeroed);
 }
 
 }  // namespace lrt
