@@ -178,6 +178,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
     uint32_t rank[kItems];
     const uint32_t lowerLanes = (1u << lane) - 1u;
     constexpr uint32_t kRankGroup = 4;
+    static_assert(kItems % kRankGroup == 0, "the rank groups must cover the items exactly");
 #pragma unroll
     for (uint32_t j0 = 0; j0 < kItems; j0 += kRankGroup) {
         uint32_t peers[kRankGroup];
