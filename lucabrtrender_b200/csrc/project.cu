@@ -651,12 +651,11 @@ __device__ __forceinline__ void emit_large_rows(const Footprint* foot, const uin
                                              uint32_t rowsTotal, uint32_t width, uint32_t height, uint32_t tileBase,
                                              uint32_t tilesX, const uint32_t* widthBits, const uint32_t* start,
                                              const uint32_t* takenStart, const unsigned long long* low,
-                                             uint32_t* rowOff, uint32_t* rowFirst, uint32_t* rowMeta,
                                              uint32_t* scanScratch, unsigned long long blockBase, uint32_t tileShift,
                                              uint32_t slotBase, const uint32_t* slotOf, const Sink& sink,
                                              const uint2* __restrict__ rowTable = nullptr) {
     const uint32_t tid = threadIdx.x;
-    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    const uint32_t lane = tid & 31u;
     uint32_t fs = 0;
     {
         uint32_t lo = 0, hi = bigTotal;
@@ -689,23 +688,41 @@ __device__ __forceinline__ void emit_large_rows(const Footprint* foot, const uin
         }
         uint32_t chunkTotal = 0;
         const uint32_t off = block_exclusive_scan(cnt, scanScratch, &chunkTotal);
-        rowOff[tid] = off;
-        rowFirst[tid] = first;
-        rowMeta[tid] = meta;
-        if (tid == 0) rowOff[kProjectThreads] = chunkTotal;
-        __syncthreads();
-        const uint32_t rows = min(kProjectThreads, rowsTotal - c0);
-        for (uint32_t q = warp; q < rows; q += kProjectThreads / 32) {
-            const uint32_t o = rowOff[q], n = rowOff[q + 1] - o;
-            if (n == 0) continue;
-            const uint32_t ty = rowMeta[q] & 0xFFFFu, owner = rowMeta[q] >> 16;
-            const uint32_t tx0 = rowFirst[q];
-            const unsigned long long at = blockBase + start[owner] + (carry + o - takenStart[owner]);
-            const unsigned long long word0 = (static_cast<unsigned long long>(tileBase + ty * tilesX) << tileShift) |
-                                             low[owner];
-            const uint32_t slot = slotOf != nullptr ? slotOf[owner] : slotBase + owner;
-            for (uint32_t k = lane; k < n; k += 32)
-                sink.put(at + k, word0 + (static_cast<unsigned long long>(tx0 + k) << tileShift), slot);
+        // Each warp writes the pairs of its 32 rows (a lane's own row) 32 at a
+        // time, lanes on consecutive pairs: a lane finds its pair's row by a
+        // binary search over the warp's running counts (shuffles: the last
+        // lane whose count starts at or before the pair, which always has
+        // pairs), so short rows leave no lane idle.
+        unsigned long long at0 = 0, word0 = 0;
+        uint32_t slot = 0;
+        if (cnt != 0) {
+            const uint32_t ty = meta & 0xFFFFu, owner = meta >> 16;
+            at0 = blockBase + start[owner] + (carry + off - takenStart[owner]);
+            word0 = (static_cast<unsigned long long>(tileBase + ty * tilesX + first) << tileShift) | low[owner];
+            slot = slotOf != nullptr ? slotOf[owner] : slotBase + owner;
+        }
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const uint32_t warpTotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - cnt;
+        for (uint32_t p0 = 0; p0 < warpTotal; p0 += 32) {
+            const uint32_t pos = p0 + lane;
+            uint32_t l = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xFFFFFFFFu, excl, static_cast<int>(l + step));
+                if (e <= pos) l += step;
+            }
+            const int src = static_cast<int>(l);
+            const uint32_t k = pos - __shfl_sync(0xFFFFFFFFu, excl, src);
+            const unsigned long long at = __shfl_sync(0xFFFFFFFFu, at0, src);
+            const unsigned long long word = __shfl_sync(0xFFFFFFFFu, word0, src);
+            const uint32_t slotHere = __shfl_sync(0xFFFFFFFFu, slot, src);
+            if (pos < warpTotal) sink.put(at + k, word + (static_cast<unsigned long long>(k) << tileShift), slotHere);
         }
         carry += chunkTotal;
         __syncthreads();
@@ -791,9 +808,6 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
     __shared__ uint32_t sWidth[kProjectThreads];
     __shared__ Footprint sFoot[kProjectThreads];           // the block's splats of more than kWarpArea tiles
     __shared__ uint32_t sFootRow[kProjectThreads + 1];     // their first row in the block's row list
-    __shared__ uint32_t sRowFirst[kProjectThreads];        // emission: a chunk's rows, first column
-    __shared__ uint32_t sRowMeta[kProjectThreads];         // emission: tile row | splat thread << 16
-    __shared__ uint32_t sRowOff[kProjectThreads + 1];      // emission: the chunk's rows' pair offsets
     __shared__ unsigned long long sBase;
     // The frame's parameters: by value, or (when a captured graph replays a
     // batch with new cameras) read from device memory, once per block.
@@ -1234,7 +1248,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         __syncthreads();
         if (takenTotal != 0)
             emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, f.width, f.height, f.tileBase, f.tilesX, sWidth,
-                            sStart, sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, blockBase, tileShift,
+                            sStart, sSmallStart, sLow, sScan, blockBase, tileShift,
                             slotBase, nullptr, sink);
     }
     // A splat whose rows are not all single runs (possible only through the
@@ -1321,9 +1335,6 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
     __shared__ uint32_t sWidth[kProjectThreads];
     __shared__ Footprint sFoot[kProjectThreads];
     __shared__ uint32_t sFootRow[kProjectThreads + 1];
-    __shared__ uint32_t sRowFirst[kProjectThreads];
-    __shared__ uint32_t sRowMeta[kProjectThreads];
-    __shared__ uint32_t sRowOff[kProjectThreads + 1];
     __shared__ uint32_t sDigits[2 * 256];
     const uint32_t tid = threadIdx.x;
     sDigits[tid] = 0;
@@ -1414,7 +1425,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
         __syncthreads();
         if (takenTotal != 0)
             emit_large_rows(sFoot, sFootRow, bigTotal, rowsTotal, width, height, 0u, tilesX, sWidth, sStart,
-                            sSmallStart, sLow, sRowOff, sRowFirst, sRowMeta, sScan, 0ull, tileShift, slotBase,
+                            sSmallStart, sLow, sScan, 0ull, tileShift, slotBase,
                             nullptr, sink, rowTable);
     }
     if (__ballot_sync(0xFFFFFFFFu, byWarp) != 0)
