@@ -1002,6 +1002,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
         const uint32_t excl = incl - mine;
         const float invW = mine != 0 ? 1.0f / static_cast<float>(rw) : 0.0f;
+        const float gate = mine != 0 ? far_edge_gate(ca, cb, cc, cutoff) : INFINITY;
         for (uint32_t c0 = 0; c0 < total; c0 += 32) {
             const uint32_t pos = c0 + lane;
             uint32_t l = 0;
@@ -1018,9 +1019,11 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
             const float ocx = __shfl_sync(0xFFFFFFFFu, cx, src), ocy = __shfl_sync(0xFFFFFFFFu, cy, src);
             const float oa = __shfl_sync(0xFFFFFFFFu, ca, src), ob = __shfl_sync(0xFFFFFFFFu, cb, src);
             const float oc = __shfl_sync(0xFFFFFFFFu, cc, src), ocut = __shfl_sync(0xFFFFFFFFu, cutoff, src);
+            const float ogate = __shfl_sync(0xFFFFFFFFu, gate, src);
             uint32_t dx = 0, dy = 0;
             mask_bit_tile(k, oW, oInv, dx, dy);
-            const bool hit = pos < total && tile_touched(f.width, f.height, ocx, ocy, oa, ob, oc, ocut, oX + dx, oY + dy);
+            const bool hit = pos < total && tile_touched(f.width, f.height, ocx, ocy, oa, ob, oc, ocut, oX + dx, oY + dy,
+                                                         ogate);
             const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
             if (mine != 0) {
                 const uint32_t lo = max(excl, c0), hi = min(incl, c0 + 32);

@@ -100,35 +100,65 @@ __device__ __forceinline__ float cutoff_power(float alpha) {   // frame.slang:10
 // the reference's expression, and the first within the cutoff answers. The edges nearer the centre go
 // first, since a touched tile is usually decided by one of them; an untouched
 // tile still evaluates all four.
+//
+// farGate (far_edge_gate) lets an untouched tile stop after the two nearer
+// edges. The power is a quadratic form, q(t p) = t^2 q(p), so the segment
+// from any point of the far edges towards the centre leaves the box through
+// a nearer edge, where the power is no larger: the exact minimum over the
+// box is on the nearer edges. Their two values, each the float power at a
+// few ulps from the edge's exact minimiser, exceed that minimum by less than
+// a relative 5u kappa (kappa = (|a| + |b| + |c|) / lambda_min bounds the
+// terms' sum against the power), and a far candidate's float value falls
+// below its exact one by no more. So when both nearer values are above the
+// gate, cutoff (1 + 64u kappa), every far candidate is above the cutoff too
+// and the answer (false) is the one the four candidates give.
 __device__ __forceinline__ bool power_within_over_box(float a, float b, float c, float lox, float loy, float hix,
-                                                      float hiy, float cutoff) {
+                                                      float hiy, float cutoff, float farGate = INFINITY) {
     if (lox <= 0.0f && hix >= 0.0f && loy <= 0.0f && hiy >= 0.0f) return 0.0f <= cutoff;
     const bool xNearHi = fabsf(hix) < fabsf(lox), yNearHi = fabsf(hiy) < fabsf(loy);
+    bool nearAbove = true;
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         {
             const float x = (e == 0) == xNearHi ? hix : lox;
             const float y = c > 1e-12f ? clampf(-b * x / c, loy, hiy) : loy;
-            if (a * x * x + 2.0f * b * x * y + c * y * y <= cutoff) return true;
+            const float q = a * x * x + 2.0f * b * x * y + c * y * y;
+            if (q <= cutoff) return true;
+            if (e == 0) nearAbove = q > farGate;
         }
         {
             const float y = (e == 0) == yNearHi ? hiy : loy;
             const float x = a > 1e-12f ? clampf(-b * y / a, lox, hix) : lox;
-            if (a * x * x + 2.0f * b * x * y + c * y * y <= cutoff) return true;
+            const float q = a * x * x + 2.0f * b * x * y + c * y * y;
+            if (q <= cutoff) return true;
+            if (e == 0) nearAbove = nearAbove && q > farGate;
         }
+        if (e == 0 && nearAbove) return false;
     }
     return false;
+}
+
+// The gate for power_within_over_box: infinite (never used) unless the conic
+// is positive definite with kappa <= 1e4 and both stationary points are
+// computed (a, c > 1e-12).
+__device__ __forceinline__ float far_edge_gate(float a, float b, float c, float cutoff) {
+    if (!(a > 1e-12f) || !(c > 1e-12f) || !(cutoff >= 0.0f)) return INFINITY;
+    const float lmin = 0.5f * (a + c) - sqrtf(0.25f * (a - c) * (a - c) + b * b);
+    if (!(lmin > 0.0f)) return INFINITY;
+    const float kappa = (a + fabsf(b) + c) / lmin;
+    if (!(kappa <= 1.0e4f)) return INFINITY;
+    return cutoff * (1.0f + 64.0f * 5.9604645e-08f * kappa);
 }
 
 // frame.slang:133-138: does tile (tx, ty) hold a pixel centre inside the footprint?
 __device__ __forceinline__ bool tile_touched(uint32_t width, uint32_t height, float cx, float cy,
                                              float ca, float cb, float cc, float cutoff, uint32_t tx,
-                                             uint32_t ty) {
+                                             uint32_t ty, float farGate = INFINITY) {
     const float firstX = static_cast<float>(tx * kTile) + 0.5f;
     const float firstY = static_cast<float>(ty * kTile) + 0.5f;
     const float lastX = static_cast<float>(min((tx + 1) * kTile, width) - 1) + 0.5f;
     const float lastY = static_cast<float>(min((ty + 1) * kTile, height) - 1) + 0.5f;
-    return power_within_over_box(ca, cb, cc, firstX - cx, firstY - cy, lastX - cx, lastY - cy, cutoff);
+    return power_within_over_box(ca, cb, cc, firstX - cx, firstY - cy, lastX - cx, lastY - cy, cutoff, farGate);
 }
 
 // shaders/lrt/common/color.slang:7-10
