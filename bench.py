@@ -41,13 +41,13 @@ RADIUS = 4.0
 SEED = 1
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + written) of one launch, from ncu (`dram__bytes_read.sum +
-# dram__bytes_write.sum`) on frame 3 of this orbit; the capture and its command
+# dram__bytes_write.sum`) on one frame of this orbit; the capture and its command
 # are summarised under profiles/ (blend_1M_1080p.md).
-PROFILED_DRAM_BYTES = {"blend": 54.031104e6 + 12.246784e6}
+PROFILED_DRAM_BYTES = {"blend": 54.170624e6 + 12.898048e6}
 # The blend is bound by instruction issue, not by HBM: its issue-active
 # fraction (`smsp__issue_active.avg.pct_of_peak_sustained_active`) from the
 # same capture, the secondary roofline its HBM fraction is read beside.
-PROFILED_ISSUE_ACTIVE = {"blend": 0.8643}
+PROFILED_ISSUE_ACTIVE = {"blend": 0.8633}
 
 
 def orbit_camera(L, k: int):
