@@ -776,10 +776,10 @@ def run_ours(args) -> None:
     sort_ms = stage["depth_sort_ms"] + stage["tile_sort_ms"]
     sort_gbs = (sort["depth"] + sort["tile"]) / (sort_ms * 1e-3) / 1e9 if sort_ms > 0 else None
     # project, depth passes, depth-order offsets, pair writes, tile passes,
-    # ranges, blend, the counters' store into host memory; and one launch
-    # that zeroes the counters, the projection's scratch, both sorts' scratch
-    # and the ranges
-    launches_per_frame = (1 + sort["depth_passes"] + 2 + sort["tile_passes"] + 1 + 1 + 1) + 1
+    # ranges, the tiles' busiest-first order (two kernels), blend, the
+    # counters' store into host memory; and one launch that zeroes the
+    # counters, the projection's scratch, both sorts' scratch and the ranges
+    launches_per_frame = (1 + sort["depth_passes"] + 2 + sort["tile_passes"] + 1 + 2 + 1 + 1) + 1
 
     clocks.stop()
     if rank == 0:

@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(kBlendThreads / kBlendPix)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
              const uint32_t* __restrict__ emitSlot,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
-             float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err) {
+             float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
+             const uint32_t* __restrict__ order) {
     __shared__ __align__(128) ProjRecord sRec[2][kBatch / kBlendPix];
     __shared__ __align__(16) float4 sBox[kBatch / kBlendPix];
     __shared__ __align__(8) uint64_t sBar[2];
@@ -407,7 +408,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
     }
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = order != nullptr ? order[blockIdx.x] : blockIdx.x;
     blend_tile<kTrain, false, kBlendPix>(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emitSlot, proj,
                                          colourOut, depthOut, pixState, pixLast, err, sRec, sBox, sBar, phase0, phase1);
 }
@@ -508,13 +509,106 @@ cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapp
     return cudaGetLastError();
 }
 
+namespace {
+constexpr uint32_t kOrderThreads = 256;
+constexpr uint32_t kOrderBuckets = 16;
+
+__device__ __forceinline__ uint32_t order_bucket(uint2 r) {   // floor(log2(pairs + 1)), at most 15
+    return min(31u - static_cast<uint32_t>(__clz(r.y - r.x + 1u)), kOrderBuckets - 1u);
+}
+
+// A block's tiles per bucket: per warp by ballots, then in shared memory.
+__device__ __forceinline__ uint32_t order_block_counts(const uint2* __restrict__ ranges, uint32_t tiles,
+                                                       uint32_t (&sWarp)[kOrderThreads / 32][kOrderBuckets],
+                                                       uint32_t& rank) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t t = blockIdx.x * kOrderThreads + threadIdx.x;
+    const uint32_t b = t < tiles ? order_bucket(ranges[t]) : kOrderBuckets;
+    rank = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kOrderBuckets; ++q) {
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, b == q);
+        if (lane == 0) sWarp[warp][q] = static_cast<uint32_t>(__popc(m));
+        if (b == q) rank = static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)));
+    }
+    __syncthreads();
+    return b;
+}
+
+__global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const uint2* __restrict__ ranges,
+                                                                         uint32_t tiles,
+                                                                         uint32_t* __restrict__ blockCounts) {
+    __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
+    uint32_t rank;
+    order_block_counts(ranges, tiles, sWarp, rank);
+    if (threadIdx.x < kOrderBuckets) {
+        uint32_t n = 0;
+        for (uint32_t w = 0; w < kOrderThreads / 32; ++w) n += sWarp[w][threadIdx.x];
+        blockCounts[blockIdx.x * kOrderBuckets + threadIdx.x] = n;
+    }
+}
+
+// The tiles in the order the blend launches them: busiest first, by buckets
+// of floor(log2(pairs + 1)), index order within a bucket. Blocks start in
+// launch order, so the long tiles start early and the short ones fill in at
+// the end. Each block reads every block's counts (from the kernel above):
+// the buckets' totals give their bases, the earlier blocks' counts its own
+// places in each bucket.
+__global__ void __launch_bounds__(kOrderThreads) tile_order_place_kernel(const uint2* __restrict__ ranges,
+                                                                         uint32_t tiles,
+                                                                         const uint32_t* __restrict__ blockCounts,
+                                                                         uint32_t* __restrict__ order) {
+    __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
+    __shared__ uint32_t sTotal[kOrderBuckets], sBefore[kOrderBuckets];
+    if (threadIdx.x < kOrderBuckets) {
+        sTotal[threadIdx.x] = 0;
+        sBefore[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < gridDim.x * kOrderBuckets; k += kOrderThreads) {
+        const uint32_t v = blockCounts[k];
+        if (v == 0) continue;
+        atomicAdd(&sTotal[k % kOrderBuckets], v);
+        if (k / kOrderBuckets < blockIdx.x) atomicAdd(&sBefore[k % kOrderBuckets], v);
+    }
+    uint32_t rank;
+    const uint32_t b = order_block_counts(ranges, tiles, sWarp, rank);   // (its barrier also ends the sums above)
+    if (threadIdx.x < kOrderBuckets) {
+        const uint32_t q = threadIdx.x;
+        uint32_t run = sBefore[q];
+        for (uint32_t h = q + 1; h < kOrderBuckets; ++h) run += sTotal[h];   // the busier buckets come first
+        for (uint32_t w = 0; w < kOrderThreads / 32; ++w) {
+            const uint32_t n = sWarp[w][q];
+            sWarp[w][q] = run;
+            run += n;
+        }
+    }
+    __syncthreads();
+    const uint32_t t = blockIdx.x * kOrderThreads + threadIdx.x;
+    if (t < tiles) order[sWarp[threadIdx.x >> 5][b] + rank] = t;
+}
+}  // namespace
+
+size_t tile_order_scratch_bytes(uint32_t tiles) {
+    return size_t{(tiles + kOrderThreads - 1) / kOrderThreads} * kOrderBuckets * sizeof(uint32_t);
+}
+
+cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* order, uint32_t* scratch,
+                              cudaStream_t stream) {
+    if (tiles == 0) return cudaSuccess;
+    const uint32_t blocks = (tiles + kOrderThreads - 1) / kOrderThreads;
+    tile_order_count_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, tiles, scratch);
+    tile_order_place_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, tiles, scratch, order);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
-                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream) {
+                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_kernel<false><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), nullptr, proj, colour, depth, nullptr, nullptr,
-        err);
+        err, order);
     return cudaGetLastError();
 }
 
@@ -552,12 +646,13 @@ cudaError_t launch_blend_batch_train(const BlendParams& bp, const ViewParams* vi
 
 cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
                                const uint32_t* emitSlot, const ProjRecord* proj, float4* colour, float* depth,
-                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream) {
+                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream,
+                               const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_kernel<true><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
-        pixLast, err);
+        pixLast, err, order);
     return cudaGetLastError();
 }
 

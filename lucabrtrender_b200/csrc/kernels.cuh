@@ -138,8 +138,15 @@ cudaError_t launch_zero_regions(const ZeroRegion* regions, uint32_t count, cudaS
 // would wait for it.
 cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapped, cudaStream_t stream);
 
+// The frame's tiles busiest first (by buckets of log2 of their pair counts),
+// the order the blends below launch them in when given one; scratch holds
+// tile_order_scratch_bytes(tiles).
+size_t tile_order_scratch_bytes(uint32_t tiles);
+cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* order, uint32_t* scratch,
+                              cudaStream_t stream);
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
-                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream);
+                         float4* colour, float* depth, uint32_t* err, cudaStream_t stream,
+                         const uint32_t* order = nullptr);
 
 // The views' tiles in one persistent launch; `queue` is a zeroed counter and
 // `blocks` the grid size (a multiple of the SM count).
@@ -167,7 +174,8 @@ cudaError_t launch_blend_backward_batch(const BlendParams& bp, const ViewParams*
 // `emit` holds each sorted pair's emit index.
 cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
                                const uint32_t* emitSlot, const ProjRecord* proj, float4* colour, float* depth,
-                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream);
+                               float4* pixState, uint32_t* pixLast, uint32_t* err, cudaStream_t stream,
+                               const uint32_t* order = nullptr);
 cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
                                   const uint32_t* emit, const uint32_t* emitSlot, const ProjRecord* proj,
                                   const float4* pixState, const uint32_t* pixLast, const float4* gradColour,

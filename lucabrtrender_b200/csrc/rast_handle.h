@@ -32,6 +32,7 @@ struct lrt_rast {
     DeviceBuffer proj, rects, touched, keys;            // per slot
     DeviceBuffer pairs, pairsAlt;                        // per pair
     DeviceBuffer ranges;                                 // per tile
+    DeviceBuffer tileOrder;                              // per tile: the blend's launch order
     DeviceBuffer scanScratch, sortScratch;               // look-back status words, tickets
     DeviceBuffer counters;                               // visible, pairs, err, algo err
     DeviceBuffer algoKeysAlt, algoValsAlt;               // lrt_radix_sort's ping-pong buffers

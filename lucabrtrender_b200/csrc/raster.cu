@@ -177,6 +177,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
         LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
+        LRT_CUDA(r, ensure(r->tileOrder, size_t{tiles} * 4 + lrt::tile_order_scratch_bytes(tiles)), "tile order");
         r->tileCap = tiles;
     }
     // Pairs are emitted on the device into a buffer of the capacity known
@@ -316,6 +317,13 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                  lrt::launch_ranges(sorted, counters + 1, r->pairCap, 32, static_cast<uint2*>(r->ranges.ptr), tiles,
                                     stream, true),
                  "ranges");
+        // The blend takes the tiles busiest first (the composite blend keeps
+        // index order).
+        uint32_t* tileOrder = composite ? nullptr : static_cast<uint32_t*>(r->tileOrder.ptr);
+        if (tileOrder != nullptr)
+            LRT_CUDA(r, lrt::launch_tile_order(static_cast<uint2*>(r->ranges.ptr), tiles, tileOrder, tileOrder + tiles,
+                                               stream),
+                     "tile order");
         LRT_CUDA(r, cudaEventRecord(r->ev[2], stream), "event");
 
         // --- blend ------------------------------------------------------------------
@@ -325,7 +333,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                                              static_cast<ProjRecord*>(r->proj.ptr),
                                              static_cast<float4*>(targets->colour), static_cast<float*>(targets->depth),
                                              static_cast<float4*>(r->pixState.ptr),
-                                             static_cast<uint32_t*>(r->pixLast.ptr), err, stream),
+                                             static_cast<uint32_t*>(r->pixLast.ptr), err, stream, tileOrder),
                      "blend");
         } else if (composite) {
             LRT_CUDA(r,
@@ -339,7 +347,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
             LRT_CUDA(r,
                      lrt::launch_blend(bp, static_cast<uint2*>(r->ranges.ptr), sorted,
                                        static_cast<ProjRecord*>(r->proj.ptr), static_cast<float4*>(targets->colour),
-                                       static_cast<float*>(targets->depth), err, stream),
+                                       static_cast<float*>(targets->depth), err, stream, tileOrder),
                      "blend");
         }
         LRT_CUDA(r, cudaEventRecord(r->ev[3], stream), "event");
