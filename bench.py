@@ -43,11 +43,11 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + written) of one launch, from ncu (`dram__bytes_read.sum +
 # dram__bytes_write.sum`) on one frame of this orbit; the capture and its command
 # are summarised under profiles/ (blend_1M_1080p.md).
-PROFILED_DRAM_BYTES = {"blend": 54.170624e6 + 12.898048e6}
+PROFILED_DRAM_BYTES = {"blend": 53.549312e6 + 7.519232e6}
 # The blend is bound by instruction issue, not by HBM: its issue-active
 # fraction (`smsp__issue_active.avg.pct_of_peak_sustained_active`) from the
 # same capture, the secondary roofline its HBM fraction is read beside.
-PROFILED_ISSUE_ACTIVE = {"blend": 0.8633}
+PROFILED_ISSUE_ACTIVE = {"blend": 0.9007}
 
 
 def orbit_camera(L, k: int):

@@ -235,8 +235,9 @@ int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
  * a blocking submit. A frame is only enqueued when a frame of the same shape
  * (splat count, width, height) has run with lrt_rast_render or this call's
  * waiting path and the last pair count read leaves a quarter of the pair
- * buffer free; otherwise this call waits like lrt_rast_render. time_stages
- * also makes it wait. Enqueued frames are ordered after every earlier call on
+ * buffer free; otherwise this call waits like lrt_rast_render (a frame of
+ * a known shape that leaves less free first grows the buffer, so that the
+ * frames after it are enqueued again). time_stages also makes it wait. Enqueued frames are ordered after every earlier call on
  * the handle, on any stream; targets belong to the caller until the frame is
  * done (an event the caller records on `stream` after this call marks it).
  * Counts and device status of enqueued frames are read by lrt_rast_settle. */
