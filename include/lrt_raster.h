@@ -223,7 +223,8 @@ const char* lrt_rast_last_error(const lrt_rast* rast);
  * concatenated into slots base + i in the order given; the slot breaks depth
  * ties. Like the reference's render (which ends with a blocking submit) the
  * call returns when the frame is done; it reads back the counts and the
- * device status once, at the end. */
+ * device status once, at the end. A frame (or view) side above 2^19 pixels
+ * returns LRT_UNSUPPORTED, as do more than 2^32 splats or pairs. */
 int lrt_rast_render(lrt_rast* rast, const lrt_projection* projection,
                     const lrt_splat_instance* instances, uint32_t instance_count,
                     const lrt_render_settings* settings, lrt_targets* targets,

@@ -120,6 +120,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
                  bool train, std::chrono::steady_clock::time_point frameStart, bool deferred = false,
                  const lrt_targets* under = nullptr, bool composite = false) {
     if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
+    if (s->width > lrt::kMaxFrameSide || s->height > lrt::kMaxFrameSide)
+        return fail(r, LRT_UNSUPPORTED, "a frame side above 2^19 pixels");
     if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
         targets->depth == nullptr)
         return fail(r, LRT_INVALID_ARGUMENT, "the targets are not the frame's size");
@@ -1241,6 +1243,8 @@ extern "C" int lrt_rast_render_batch(lrt_rast* r, const lrt_splat_instance* inst
     if (total > 0xFFFFFFFFull) return fail(r, LRT_UNSUPPORTED, "more than 2^32 splats in one view");
     for (uint32_t v = 0; v < nViews; ++v) {
         if (views[v].width == 0 || views[v].height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a view needs a size");
+        if (views[v].width > lrt::kMaxFrameSide || views[v].height > lrt::kMaxFrameSide)
+            return fail(r, LRT_UNSUPPORTED, "a view side above 2^19 pixels");
         if (views[v].colour == nullptr || views[v].depth == nullptr)
             return fail(r, LRT_INVALID_ARGUMENT, "a view without its images");
     }

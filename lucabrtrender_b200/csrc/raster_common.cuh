@@ -13,6 +13,9 @@
 namespace lrt {
 
 constexpr uint32_t kTile = 16;   // shaders/lrt/splat/frame.slang:31
+// The largest frame side: the projection packs a splat's tile rectangle
+// into 16-bit fields (its height into 15), so a side holds at most 2^15 tiles.
+constexpr uint32_t kMaxFrameSide = (1u << 15) * kTile;
 
 struct EditParams {   // shaders/lrt/common/edit.slang:23-37
     uint32_t active, shape, mode, invert;

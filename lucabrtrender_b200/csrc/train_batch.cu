@@ -365,6 +365,8 @@ extern "C" int lrt_rast_train_batch(lrt_rast* r, const lrt_train_params* params,
         return fail(r, LRT_INVALID_ARGUMENT, "the SH gradient must be 16-byte aligned");
     for (uint32_t v = 0; v < nViews; ++v) {
         if (views[v].width == 0 || views[v].height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a view needs a size");
+        if (views[v].width > lrt::kMaxFrameSide || views[v].height > lrt::kMaxFrameSide)
+            return fail(r, LRT_UNSUPPORTED, "a view side above 2^19 pixels");
         if (views[v].colour == nullptr || views[v].depth == nullptr || views[v].target == nullptr)
             return fail(r, LRT_INVALID_ARGUMENT, "a view without its images or target");
     }

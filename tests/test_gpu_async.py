@@ -133,3 +133,22 @@ def test_a_shape_whose_pairs_crowd_the_buffer_grows_it_and_stays_exact():
     finally:
         raster.close()
         reference.close()
+
+
+def test_a_frame_side_above_the_limit_is_unsupported():
+    # The projection packs tile rectangles into 16-bit fields: a frame side
+    # holds at most 2^15 tiles of 16 pixels.
+    scene = H.synthetic_scene(1000, 64, 64, seed=34)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    raster = L.TileRasterizer.create(0)
+    try:
+        wide = (1 << 19) + 1
+        settings = L.RenderSettings(width=wide, height=1)
+        with pytest.raises(L.LrtError) as info:
+            raster.render(orbit(0, wide, 1), instances, settings, L.RenderTargets(wide, 1))
+        assert info.value.code == _abi.UNSUPPORTED
+        # The handle still renders a frame of an ordinary size.
+        t = L.RenderTargets(64, 64)
+        assert raster.render(orbit(0, 64, 64), instances, L.RenderSettings(width=64, height=64), t).splats == 1000
+    finally:
+        raster.close()
