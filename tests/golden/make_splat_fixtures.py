@@ -8,7 +8,7 @@ x y z, logit opacity, three log scales, rotation w x y z, three DC, then the
 rest coefficients all red, then green, then blue), stored as base64 float32.
 The reference tree is read only here; the tests use the JSON.
 
-    python tests/golden/make_splat_fixtures.py [reference root]
+    python tests/golden/make_splat_fixtures.py <reference root>
 """
 from __future__ import annotations
 
@@ -49,7 +49,9 @@ def records(fields: dict[str, np.ndarray]) -> tuple[np.ndarray, int]:
 
 
 def main() -> None:
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_splat_fixtures.py <reference root>")
+    root = Path(sys.argv[1])
     out = {}
     for name in ("tiny", "sh3"):
         recs, per_colour = records(read_ply(root / "tests" / "data" / "splats" / f"{name}.ply"))
