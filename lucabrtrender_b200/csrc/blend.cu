@@ -513,17 +513,25 @@ namespace {
 constexpr uint32_t kOrderThreads = 256;
 constexpr uint32_t kOrderBuckets = 16;
 
-__device__ __forceinline__ uint32_t order_bucket(uint2 r) {   // floor(log2(pairs + 1)), at most 15
-    return min(31u - static_cast<uint32_t>(__clz(r.y - r.x + 1u)), kOrderBuckets - 1u);
+__device__ __forceinline__ uint32_t order_bucket(uint32_t work) {   // floor(log2(work + 1)), at most 15
+    return min(31u - static_cast<uint32_t>(__clz(work + 1u)), kOrderBuckets - 1u);
+}
+// A tile's work: its pair count, or (work != null) the given value.
+__device__ __forceinline__ uint32_t tile_work(const uint2* __restrict__ ranges, const uint32_t* __restrict__ work,
+                                              uint32_t t) {
+    if (work != nullptr) return work[t];
+    const uint2 r = ranges[t];
+    return r.y - r.x;
 }
 
 // A block's tiles per bucket: per warp by ballots, then in shared memory.
-__device__ __forceinline__ uint32_t order_block_counts(const uint2* __restrict__ ranges, uint32_t tiles,
+__device__ __forceinline__ uint32_t order_block_counts(const uint2* __restrict__ ranges,
+                                                       const uint32_t* __restrict__ work, uint32_t tiles,
                                                        uint32_t (&sWarp)[kOrderThreads / 32][kOrderBuckets],
                                                        uint32_t& rank) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t t = blockIdx.x * kOrderThreads + threadIdx.x;
-    const uint32_t b = t < tiles ? order_bucket(ranges[t]) : kOrderBuckets;
+    const uint32_t b = t < tiles ? order_bucket(tile_work(ranges, work, t)) : kOrderBuckets;
     rank = 0;
 #pragma unroll
     for (uint32_t q = 0; q < kOrderBuckets; ++q) {
@@ -536,11 +544,12 @@ __device__ __forceinline__ uint32_t order_block_counts(const uint2* __restrict__
 }
 
 __global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const uint2* __restrict__ ranges,
+                                                                         const uint32_t* __restrict__ work,
                                                                          uint32_t tiles,
                                                                          uint32_t* __restrict__ blockCounts) {
     __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
     uint32_t rank;
-    order_block_counts(ranges, tiles, sWarp, rank);
+    order_block_counts(ranges, work, tiles, sWarp, rank);
     if (threadIdx.x < kOrderBuckets) {
         uint32_t n = 0;
         for (uint32_t w = 0; w < kOrderThreads / 32; ++w) n += sWarp[w][threadIdx.x];
@@ -555,6 +564,7 @@ __global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const u
 // the buckets' totals give their bases, the earlier blocks' counts its own
 // places in each bucket.
 __global__ void __launch_bounds__(kOrderThreads) tile_order_place_kernel(const uint2* __restrict__ ranges,
+                                                                         const uint32_t* __restrict__ work,
                                                                          uint32_t tiles,
                                                                          const uint32_t* __restrict__ blockCounts,
                                                                          uint32_t* __restrict__ order) {
@@ -572,7 +582,7 @@ __global__ void __launch_bounds__(kOrderThreads) tile_order_place_kernel(const u
         if (k / kOrderBuckets < blockIdx.x) atomicAdd(&sBefore[k % kOrderBuckets], v);
     }
     uint32_t rank;
-    const uint32_t b = order_block_counts(ranges, tiles, sWarp, rank);   // (its barrier also ends the sums above)
+    const uint32_t b = order_block_counts(ranges, work, tiles, sWarp, rank);   // (its barrier also ends the sums above)
     if (threadIdx.x < kOrderBuckets) {
         const uint32_t q = threadIdx.x;
         uint32_t run = sBefore[q];
@@ -594,12 +604,47 @@ size_t tile_order_scratch_bytes(uint32_t tiles) {
 }
 
 cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* order, uint32_t* scratch,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, const uint32_t* work) {
     if (tiles == 0) return cudaSuccess;
     const uint32_t blocks = (tiles + kOrderThreads - 1) / kOrderThreads;
-    tile_order_count_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, tiles, scratch);
-    tile_order_place_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, tiles, scratch, order);
+    tile_order_count_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, work, tiles, scratch);
+    tile_order_place_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, work, tiles, scratch, order);
     return cudaGetLastError();
+}
+
+namespace {
+// A training frame's tile work for the backward blend: the pairs up to the
+// tile's last contributor (the largest of its pixels' saved last indices),
+// a warp a tile.
+__global__ void __launch_bounds__(256) tile_backward_work_kernel(const uint2* __restrict__ ranges,
+                                                                 const uint32_t* __restrict__ pixLast, uint32_t width,
+                                                                 uint32_t height, uint32_t tilesX, uint32_t tiles,
+                                                                 uint32_t* __restrict__ work) {
+    const uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31u;
+    if (t >= tiles) return;
+    const uint32_t x0 = (t % tilesX) * kTile, y0 = (t / tilesX) * kTile;
+    const uint32_t start = ranges[t].x;
+    uint32_t last = start;
+#pragma unroll
+    for (uint32_t k = 0; k < kTile * kTile / 32; ++k) {
+        const uint32_t p = k * 32u + lane;
+        const uint32_t px = x0 + (p & (kTile - 1u)), py = y0 + p / kTile;
+        if (px < width && py < height) last = max(last, pixLast[static_cast<size_t>(py) * width + px]);
+    }
+    last = __reduce_max_sync(0xFFFFFFFFu, last);
+    if (lane == 0) work[t] = last - start;
+}
+}  // namespace
+
+cudaError_t launch_tile_backward_order(const uint2* ranges, const uint32_t* pixLast, uint32_t width, uint32_t height,
+                                       uint32_t tilesX, uint32_t tiles, uint32_t* order, uint32_t* scratch,
+                                       uint32_t* work, cudaStream_t stream) {
+    if (tiles == 0) return cudaSuccess;
+    tile_backward_work_kernel<<<(tiles + 7) / 8, 256, 0, stream>>>(ranges, pixLast, width, height, tilesX, tiles, work);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_tile_order(ranges, tiles, order, scratch, stream, work);
 }
 
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,

@@ -342,8 +342,9 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                       const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
                       const ProjRecord* __restrict__ proj,
                       const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
-                      const float4* __restrict__ gradColour, float* __restrict__ partials) {
-    const uint32_t tile = blockIdx.x;
+                      const float4* __restrict__ gradColour, float* __restrict__ partials,
+                      const uint32_t* __restrict__ order) {
+    const uint32_t tile = order != nullptr ? order[blockIdx.x] : blockIdx.x;
     blend_backward_tile(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emit, emitSlot, proj, pixState,
                         pixLast, gradColour, partials);
 }
@@ -387,12 +388,12 @@ cudaError_t launch_blend_backward_batch(const BlendParams& bp, const ViewParams*
 cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
                                   const uint32_t* emit, const uint32_t* emitSlot, const ProjRecord* proj,
                                   const float4* pixState, const uint32_t* pixLast, const float4* gradColour,
-                                  float* partials, cudaStream_t stream) {
+                                  float* partials, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
     blend_backward_kernel<<<tiles, kBlendThreads / kBwdPix, 0, stream>>>(
         bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
-        gradColour, partials);
+        gradColour, partials, order);
     return cudaGetLastError();
 }
 

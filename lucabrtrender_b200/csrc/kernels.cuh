@@ -143,7 +143,13 @@ cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapp
 // tile_order_scratch_bytes(tiles).
 size_t tile_order_scratch_bytes(uint32_t tiles);
 cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* order, uint32_t* scratch,
-                              cudaStream_t stream);
+                              cudaStream_t stream, const uint32_t* work = nullptr);
+// The same for a training frame's backward blend, by the pairs up to each
+// tile's last contributor (from the forward's per-pixel last indices);
+// `work` holds a word per tile.
+cudaError_t launch_tile_backward_order(const uint2* ranges, const uint32_t* pixLast, uint32_t width, uint32_t height,
+                                       uint32_t tilesX, uint32_t tiles, uint32_t* order, uint32_t* scratch,
+                                       uint32_t* work, cudaStream_t stream);
 cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs, const ProjRecord* proj,
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream,
                          const uint32_t* order = nullptr);
@@ -179,7 +185,7 @@ cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const
 cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
                                   const uint32_t* emit, const uint32_t* emitSlot, const ProjRecord* proj,
                                   const float4* pixState, const uint32_t* pixLast, const float4* gradColour,
-                                  float* partials, cudaStream_t stream);
+                                  float* partials, cudaStream_t stream, const uint32_t* order = nullptr);
 
 cudaError_t launch_splat_backward(const FrameParams& f, const float* means, const float* logScales, const float* quats,
                                   const float* logits, const uint16_t* sh, const uint32_t* touched,

@@ -179,7 +179,8 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     LRT_CUDA(r, ensure(r->scanScratch, std::max<size_t>(statusBytes, 16)), "projection scratch");
     if (tiles > r->tileCap) {
         LRT_CUDA(r, ensure(r->ranges, size_t{tiles} * 8), "tile ranges");
-        LRT_CUDA(r, ensure(r->tileOrder, size_t{tiles} * 4 + lrt::tile_order_scratch_bytes(tiles)), "tile order");
+        // order, its scratch, and the backward's per-tile work
+        LRT_CUDA(r, ensure(r->tileOrder, size_t{tiles} * 8 + lrt::tile_order_scratch_bytes(tiles)), "tile order");
         r->tileCap = tiles;
     }
     // Pairs are emitted on the device into a buffer of the capacity known
@@ -962,12 +963,23 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
     const size_t partialBytes = std::max<size_t>(size_t{pairBound} * 12 * sizeof(float), 16);
     LRT_CUDA(r, ensure(r->partials, partialBytes), "partials");
     LRT_CUDA(r, cudaEventRecord(r->ev[7], stream), "event");
+    // The backward takes the tiles busiest first by its own work: the pairs
+    // up to each tile's last contributor.
+    const BlendParams& tb = r->trainBlend;
+    const uint32_t bTiles = tb.tilesX * tb.tilesY;
+    uint32_t* bOrder = static_cast<uint32_t*>(r->tileOrder.ptr);
+    uint32_t* bScratch = bOrder + bTiles;
+    uint32_t* bWork = bScratch + lrt::tile_order_scratch_bytes(bTiles) / 4;
+    LRT_CUDA(r,
+             lrt::launch_tile_backward_order(static_cast<uint2*>(r->ranges.ptr), static_cast<uint32_t*>(r->pixLast.ptr),
+                                             tb.width, tb.height, tb.tilesX, bTiles, bOrder, bScratch, bWork, stream),
+             "backward tile order");
     LRT_CUDA(r,
              lrt::launch_blend_backward(r->trainBlend, static_cast<uint2*>(r->ranges.ptr), r->trainSorted,
                                         r->trainSortedValues, r->trainEmitSlot, static_cast<ProjRecord*>(r->proj.ptr),
                                         static_cast<float4*>(r->pixState.ptr), static_cast<uint32_t*>(r->pixLast.ptr),
                                         static_cast<const float4*>(gradColour), static_cast<float*>(r->partials.ptr),
-                                        stream),
+                                        stream, bOrder),
              "blend backward");
     LRT_CUDA(r, cudaEventRecord(r->ev[8], stream), "event");
     LRT_CUDA(r,
