@@ -28,6 +28,7 @@ constexpr uint32_t kBlendPix = 2;
 constexpr uint32_t kRangeRun = 8;
 __global__ void ranges_kernel(const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ dCount,
                               uint32_t cap, uint32_t tileShift, uint2* __restrict__ ranges) {
+    chained_entry();
     const uint32_t n = min(*dCount, cap);
     const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) * kRangeRun;
     if (first >= n) return;
@@ -398,6 +399,7 @@ blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned lo
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
              float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
              const uint32_t* __restrict__ order) {
+    chained_entry();
     __shared__ __align__(128) ProjRecord sRec[2][kBatch / kBlendPix];
     __shared__ __align__(16) float4 sBox[kBatch / kBlendPix];
     __shared__ __align__(8) uint64_t sBar[2];
@@ -492,21 +494,20 @@ cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_
     cudaError_t e = rangesZeroed ? cudaSuccess : launch_zero(ranges, sizeof(uint2) * tiles, stream);
     if (e != cudaSuccess || cap == 0) return e;
     const uint32_t threads = (cap + kRangeRun - 1) / kRangeRun;
-    ranges_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const unsigned long long*>(pairs),
-                                                             dCount, cap, tileShift, ranges);
-    return cudaGetLastError();
+    return launch_chained(ranges_kernel, dim3((threads + 255) / 256), dim3(256), 0, stream,
+                          reinterpret_cast<const unsigned long long*>(pairs), dCount, cap, tileShift, ranges);
 }
 
 namespace {
 __global__ void publish_counters_kernel(const uint32_t* __restrict__ counters, uint32_t* hostMapped) {
+    chained_entry();
     if (threadIdx.x < 4) hostMapped[threadIdx.x] = counters[threadIdx.x];
     __threadfence_system();
 }
 }  // namespace
 
 cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapped, cudaStream_t stream) {
-    publish_counters_kernel<<<1, 32, 0, stream>>>(counters, hostMapped);
-    return cudaGetLastError();
+    return launch_chained(publish_counters_kernel, dim3(1), dim3(32), 0, stream, counters, hostMapped);
 }
 
 namespace {
@@ -547,6 +548,7 @@ __global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const u
                                                                          const uint32_t* __restrict__ work,
                                                                          uint32_t tiles,
                                                                          uint32_t* __restrict__ blockCounts) {
+    chained_entry();
     __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
     uint32_t rank;
     order_block_counts(ranges, work, tiles, sWarp, rank);
@@ -568,6 +570,7 @@ __global__ void __launch_bounds__(kOrderThreads) tile_order_place_kernel(const u
                                                                          uint32_t tiles,
                                                                          const uint32_t* __restrict__ blockCounts,
                                                                          uint32_t* __restrict__ order) {
+    chained_entry();
     __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
     __shared__ uint32_t sTotal[kOrderBuckets], sBefore[kOrderBuckets];
     if (threadIdx.x < kOrderBuckets) {
@@ -607,9 +610,11 @@ cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* ord
                               cudaStream_t stream, const uint32_t* work) {
     if (tiles == 0) return cudaSuccess;
     const uint32_t blocks = (tiles + kOrderThreads - 1) / kOrderThreads;
-    tile_order_count_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, work, tiles, scratch);
-    tile_order_place_kernel<<<blocks, kOrderThreads, 0, stream>>>(ranges, work, tiles, scratch, order);
-    return cudaGetLastError();
+    cudaError_t e = launch_chained(tile_order_count_kernel, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work,
+                                   tiles, scratch);
+    if (e != cudaSuccess) return e;
+    return launch_chained(tile_order_place_kernel, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work, tiles,
+                          static_cast<const uint32_t*>(scratch), order);
 }
 
 namespace {
@@ -651,10 +656,9 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_kernel<false><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), nullptr, proj, colour, depth, nullptr, nullptr,
-        err, order);
-    return cudaGetLastError();
+    return launch_chained(blend_kernel<false>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
+                          reinterpret_cast<const unsigned long long*>(pairs), static_cast<const uint32_t*>(nullptr), proj,
+                          colour, depth, static_cast<float4*>(nullptr), static_cast<uint32_t*>(nullptr), err, order);
 }
 
 cudaError_t launch_blend_composite(const BlendParams& bp, const uint2* ranges, const uint64_t* pairs,
@@ -695,10 +699,9 @@ cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const
                                const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_kernel<true><<<tiles, kBlendThreads / kBlendPix, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
-        pixLast, err, order);
-    return cudaGetLastError();
+    return launch_chained(blend_kernel<true>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
+                          reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
+                          pixLast, err, order);
 }
 
 }  // namespace lrt

@@ -798,6 +798,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                     unsigned long long* __restrict__ depthWordsOut = nullptr,
                     uint32_t* __restrict__ depthDigits = nullptr, uint2* __restrict__ rowTable = nullptr,
                     uint32_t rowCap = 0) {
+    chained_entry();
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
@@ -1290,6 +1291,7 @@ depth_offsets_kernel(const unsigned long long* __restrict__ sortedWords, uint32_
                      const uint32_t* __restrict__ touchedIn, uint32_t* __restrict__ counters,
                      uint64_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t lastPartition,
                      uint32_t* __restrict__ offsets) {
+    chained_entry();
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ unsigned long long sBase;
@@ -1330,6 +1332,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
                   uint32_t* __restrict__ err, unsigned long long* __restrict__ pairs, uint32_t capacity,
                   TrainOutputs train, uint32_t* __restrict__ tileDigits, uint32_t tilePasses,
                   const uint2* __restrict__ rowTable) {
+    chained_entry();
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];
@@ -1473,11 +1476,12 @@ cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRe
                                          static_cast<int>(std::max<size_t>(smem, 1)));
     if (e != cudaSuccess) return e;
     const uint32_t blocks = project_partitions(f.count);
-    project_emit_kernel<Src, false><<<blocks, kProjectThreads, smem, stream>>>(
-        f, nullptr, src, TrainOutputs{nullptr, nullptr, nullptr}, stageWords, shVector, proj, rects, touched, keys,
-        counters, nullptr, ticket, 0, 0, 0, nullptr, 0, reinterpret_cast<unsigned long long*>(aux),
-        reinterpret_cast<unsigned long long*>(depthWords), depthDigits, rowTable, rowCap);
-    return cudaGetLastError();
+    return launch_chained(project_emit_kernel<Src, false>, dim3(blocks), dim3(kProjectThreads), smem, stream, f,
+                          static_cast<const FrameParams*>(nullptr), src, TrainOutputs{nullptr, nullptr, nullptr},
+                          stageWords, shVector, proj, rects, touched, keys, counters,
+                          static_cast<uint64_t*>(nullptr), ticket, 0u, 0u, 0u, static_cast<unsigned long long*>(nullptr),
+                          0u, reinterpret_cast<unsigned long long*>(aux),
+                          reinterpret_cast<unsigned long long*>(depthWords), depthDigits, rowTable, rowCap);
 }
 
 }  // namespace
@@ -1560,16 +1564,15 @@ cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const Pr
     if (n == 0) return cudaSuccess;
     const uint32_t perBlock = kProjectThreads * kOffsetItems;
     const uint32_t offsetBlocks = (n + perBlock - 1) / perBlock;
-    depth_offsets_kernel<<<offsetBlocks, kProjectThreads, 0, stream>>>(
-        reinterpret_cast<const unsigned long long*>(sortedWords), n, touched, counters, status, ticket,
-        offsetBlocks - 1, offsets);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_chained(depth_offsets_kernel, dim3(offsetBlocks), dim3(kProjectThreads), 0, stream,
+                                   reinterpret_cast<const unsigned long long*>(sortedWords), n, touched, counters,
+                                   status, ticket, offsetBlocks - 1, offsets);
     if (e != cudaSuccess) return e;
-    emit_pairs_kernel<<<project_partitions(n), kProjectThreads, 0, stream>>>(
-        n, proj, rects, touched, reinterpret_cast<const unsigned long long*>(aux), offsets, width, height, tilesX,
-        counters + 2, reinterpret_cast<unsigned long long*>(pairs), capacity, TrainOutputs{nullptr, values, emitSlot},
-        tileDigits, tilePasses, rowTable);
-    return cudaGetLastError();
+    return launch_chained(emit_pairs_kernel, dim3(project_partitions(n)), dim3(kProjectThreads), 0, stream, n, proj,
+                          rects, touched, reinterpret_cast<const unsigned long long*>(aux),
+                          static_cast<const uint32_t*>(offsets), width, height, tilesX, counters + 2,
+                          reinterpret_cast<unsigned long long*>(pairs), capacity,
+                          TrainOutputs{nullptr, values, emitSlot}, tileDigits, tilePasses, rowTable);
 }
 
 cudaError_t launch_project_only_train(const FrameParams& f, const float* means, const float* logScales,

@@ -10,7 +10,36 @@
 
 #include "lrt_math.cuh"
 
+#include <utility>
+
 namespace lrt {
+
+// Programmatic dependent launch. A kernel launched by launch_chained may
+// have its blocks scheduled while the kernel before it on the stream is
+// still finishing: chained_entry(), its first statement, waits until that
+// kernel has completed and its writes are visible (which also covers every
+// kernel before it), then lets the next chained kernel begin launching once
+// all of this grid's blocks are running. Launched the usual way, a kernel
+// passes through it at once.
+__device__ __forceinline__ void chained_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... Params, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                  Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr = {};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 constexpr uint32_t kTile = 16;   // shaders/lrt/splat/frame.slang:31
 // The largest frame side: the projection packs a splat's tile rectangle

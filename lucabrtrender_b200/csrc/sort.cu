@@ -129,6 +129,7 @@ onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t*
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
                 const uint32_t* __restrict__ hist, W* __restrict__ lookback,
                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift, uint32_t spinLimit) {
+    chained_entry();
     extern __shared__ __align__(16) unsigned char smem[];
     K* sKeys = reinterpret_cast<K*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * (kItems * kSortThreads));
@@ -326,11 +327,10 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
     uint32_t* vsrc = vals;
     uint32_t* vdst = valsAlt;
     for (uint32_t p = 0; p < passes; ++p) {
-        onesweep_kernel<K, kValues, W, kItems><<<parts, kSortThreads, smem, stream>>>(
-            src, dst, vsrc, vdst, dCount, cap, digitCounts + p * kDigits,
-            lookback + static_cast<size_t>(p) * parts * kDigits,
-            tickets + p, err, firstBit + 8 * p, spinLimit);
-        e = cudaGetLastError();
+        e = launch_chained(onesweep_kernel<K, kValues, W, kItems>, dim3(parts), dim3(kSortThreads), smem, stream,
+                           static_cast<const K*>(src), dst, static_cast<const uint32_t*>(vsrc), vdst, dCount, cap,
+                           digitCounts + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
+                           tickets + p, err, firstBit + 8 * p, spinLimit);
         if (e != cudaSuccess) return e;
         std::swap(src, dst);
         std::swap(vsrc, vdst);
