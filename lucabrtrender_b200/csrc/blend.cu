@@ -625,6 +625,7 @@ __global__ void __launch_bounds__(256) tile_backward_work_kernel(const uint2* __
                                                                  const uint32_t* __restrict__ pixLast, uint32_t width,
                                                                  uint32_t height, uint32_t tilesX, uint32_t tiles,
                                                                  uint32_t* __restrict__ work) {
+    chained_entry();
     const uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31u;
     if (t >= tiles) return;
@@ -646,8 +647,8 @@ cudaError_t launch_tile_backward_order(const uint2* ranges, const uint32_t* pixL
                                        uint32_t tilesX, uint32_t tiles, uint32_t* order, uint32_t* scratch,
                                        uint32_t* work, cudaStream_t stream) {
     if (tiles == 0) return cudaSuccess;
-    tile_backward_work_kernel<<<(tiles + 7) / 8, 256, 0, stream>>>(ranges, pixLast, width, height, tilesX, tiles, work);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_chained(tile_backward_work_kernel, dim3((tiles + 7) / 8), dim3(256), 0, stream, ranges,
+                                   pixLast, width, height, tilesX, tiles, work);
     if (e != cudaSuccess) return e;
     return launch_tile_order(ranges, tiles, order, scratch, stream, work);
 }

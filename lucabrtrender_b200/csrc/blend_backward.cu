@@ -344,6 +344,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                       const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
                       const float4* __restrict__ gradColour, float* __restrict__ partials,
                       const uint32_t* __restrict__ order) {
+    chained_entry();
     const uint32_t tile = order != nullptr ? order[blockIdx.x] : blockIdx.x;
     blend_backward_tile(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emit, emitSlot, proj, pixState,
                         pixLast, gradColour, partials);
@@ -391,10 +392,9 @@ cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, co
                                   float* partials, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    blend_backward_kernel<<<tiles, kBlendThreads / kBwdPix, 0, stream>>>(
-        bp, ranges, reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
-        gradColour, partials, order);
-    return cudaGetLastError();
+    return launch_chained(blend_backward_kernel, dim3(tiles), dim3(kBlendThreads / kBwdPix), 0, stream, bp, ranges,
+                          reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
+                          gradColour, partials, order);
 }
 
 }  // namespace lrt

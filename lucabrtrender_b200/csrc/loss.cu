@@ -19,6 +19,7 @@ constexpr uint32_t kLossBlocks = 148 * 4;
 __global__ void __launch_bounds__(kLossThreads)
 l1_partial_kernel(const float4* __restrict__ colour, const float* __restrict__ target, uint32_t pixels,
                   float* __restrict__ partials) {
+    chained_entry();
     __shared__ float sWarp[kLossThreads / 32];
     float s = 0.0f;
     for (uint32_t i = blockIdx.x * kLossThreads + threadIdx.x; i < pixels; i += gridDim.x * kLossThreads) {
@@ -40,6 +41,7 @@ l1_partial_kernel(const float4* __restrict__ colour, const float* __restrict__ t
 
 __global__ void l1_total_kernel(const float* __restrict__ partials, uint32_t count, float scale,
                                 float* __restrict__ loss) {
+    chained_entry();
     __shared__ float sWarp[32];
     float s = 0.0f;
     for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) s += partials[i];
@@ -57,6 +59,7 @@ __global__ void l1_total_kernel(const float* __restrict__ partials, uint32_t cou
 __global__ void __launch_bounds__(kLossThreads)
 l1_grad_kernel(const float4* __restrict__ colour, const float* __restrict__ target, uint32_t pixels, float scale,
                const float* __restrict__ gradLoss, float4* __restrict__ gradColour) {
+    chained_entry();
     const float g = scale * (gradLoss != nullptr ? __ldg(gradLoss) : 1.0f);
     for (uint32_t i = blockIdx.x * kLossThreads + threadIdx.x; i < pixels; i += gridDim.x * kLossThreads) {
         const float4 c = __ldg(colour + i);
@@ -75,17 +78,19 @@ size_t l1_scratch_bytes() { return kLossBlocks * sizeof(float); }
 cudaError_t launch_l1_loss(const float4* colour, const float* target, uint32_t pixels, float* scratch, float* loss,
                            cudaStream_t stream) {
     const float scale = pixels > 0 ? 1.0f / (3.0f * static_cast<float>(pixels)) : 0.0f;
-    l1_partial_kernel<<<kLossBlocks, kLossThreads, 0, stream>>>(colour, target, pixels, scratch);
-    l1_total_kernel<<<1, 256, 0, stream>>>(scratch, kLossBlocks, scale, loss);
-    return cudaGetLastError();
+    cudaError_t e = launch_chained(l1_partial_kernel, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target,
+                                   pixels, scratch);
+    if (e != cudaSuccess) return e;
+    return launch_chained(l1_total_kernel, dim3(1), dim3(256), 0, stream, static_cast<const float*>(scratch),
+                          kLossBlocks, scale, loss);
 }
 
 cudaError_t launch_l1_grad(const float4* colour, const float* target, uint32_t pixels, const float* gradLoss,
                            float4* gradColour, cudaStream_t stream) {
     if (pixels == 0) return cudaSuccess;
     const float scale = 1.0f / (3.0f * static_cast<float>(pixels));
-    l1_grad_kernel<<<kLossBlocks, kLossThreads, 0, stream>>>(colour, target, pixels, scale, gradLoss, gradColour);
-    return cudaGetLastError();
+    return launch_chained(l1_grad_kernel, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target, pixels,
+                          scale, gradLoss, gradColour);
 }
 
 }  // namespace lrt
