@@ -152,3 +152,41 @@ def test_a_frame_side_above_the_limit_is_unsupported():
         assert raster.render(orbit(0, 64, 64), instances, L.RenderSettings(width=64, height=64), t).splats == 1000
     finally:
         raster.close()
+
+
+def test_many_enqueued_frames_back_to_back_stay_exact():
+    # Frames enqueued back to back run their kernels chained (each waits for
+    # the one before it as its first step); 48 of them over two views, each
+    # image copied out on another stream as the next frame renders, must
+    # equal the waiting renders bit for bit.
+    scene = H.synthetic_scene(80_000, 64, 64, seed=35)
+    instances = [L.SplatInstance(L.to_device(scene.clouds[0][0]))]
+    settings = L.RenderSettings(width=400, height=300)
+    views = [orbit(1, 400, 300), orbit(5, 400, 300)]
+    raster = L.TileRasterizer.create(0)
+    try:
+        want = []
+        for v in views:
+            t = L.RenderTargets(400, 300)
+            raster.render(v, instances, settings, t)
+            want.append((t.colour.clone(), t.depth.clone()))
+        targets = [L.RenderTargets(400, 300) for _ in range(2)]
+        copies = [[torch.empty_like(want[0][0]), torch.empty_like(want[0][1])] for _ in range(48)]
+        stream = torch.cuda.current_stream()
+        side = torch.cuda.Stream()
+        for k in range(48):
+            t = targets[k % 2]
+            raster.render_async(views[k % 2], instances, settings, t, stream)
+            done = torch.cuda.Event()
+            done.record(stream)
+            side.wait_event(done)
+            with torch.cuda.stream(side):
+                copies[k][0].copy_(t.colour)
+                copies[k][1].copy_(t.depth)
+            stream.wait_stream(side)   # the next frame into these targets waits for the copy
+        raster.settle()
+        torch.cuda.synchronize()
+        for k in range(48):
+            assert torch.equal(copies[k][0], want[k % 2][0]) and torch.equal(copies[k][1], want[k % 2][1]), k
+    finally:
+        raster.close()
