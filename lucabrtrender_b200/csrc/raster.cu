@@ -109,7 +109,7 @@ namespace {
 
 // One projection launch of a frame: a packed cloud instance, or the
 // differentiable parameters of the training path.
-// One frame, TileRasterizer.cpp:188-484 in this build's stage order. `train`
+// One frame, TileRasterizer.cpp:188-484 in this library's stage order. `train`
 // selects the training variants (emit indices carried through the sort,
 // per-slot pair offsets, per-pixel blend state for the backward pass).
 // `deferred`: enqueue the frame and return without waiting (training frames
