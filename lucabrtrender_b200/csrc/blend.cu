@@ -26,9 +26,10 @@ constexpr uint32_t kBlendPix = 2;
 // splat_tiles_clear.slang:8-17). Each thread takes kRangeRun consecutive
 // pairs (two 16-byte loads per pair pair) and the one before them.
 constexpr uint32_t kRangeRun = 8;
+template <bool kChained>
 __global__ void ranges_kernel(const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ dCount,
                               uint32_t cap, uint32_t tileShift, uint2* __restrict__ ranges) {
-    chained_entry();
+    chained_entry<kChained>();
     const uint32_t n = min(*dCount, cap);
     const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) * kRangeRun;
     if (first >= n) return;
@@ -392,14 +393,14 @@ __device__ __forceinline__ bool blend_tile(const BlendParams& bp, uint32_t tile,
 }
 
 
-template <bool kTrain>
+template <bool kTrain, bool kChained>
 __global__ void __launch_bounds__(kBlendThreads / kBlendPix)
 blend_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
              const uint32_t* __restrict__ emitSlot,
              const ProjRecord* __restrict__ proj, float4* __restrict__ colourOut, float* __restrict__ depthOut,
              float4* __restrict__ pixState, uint32_t* __restrict__ pixLast, uint32_t* __restrict__ err,
              const uint32_t* __restrict__ order) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ __align__(128) ProjRecord sRec[2][kBatch / kBlendPix];
     __shared__ __align__(16) float4 sBox[kBatch / kBlendPix];
     __shared__ __align__(8) uint64_t sBar[2];
@@ -494,20 +495,21 @@ cudaError_t launch_ranges(const uint64_t* pairs, const uint32_t* dCount, uint32_
     cudaError_t e = rangesZeroed ? cudaSuccess : launch_zero(ranges, sizeof(uint2) * tiles, stream);
     if (e != cudaSuccess || cap == 0) return e;
     const uint32_t threads = (cap + kRangeRun - 1) / kRangeRun;
-    return launch_chained(ranges_kernel, dim3((threads + 255) / 256), dim3(256), 0, stream,
+    return launch_chained(ranges_kernel<true>, ranges_kernel<false>, dim3((threads + 255) / 256), dim3(256), 0, stream,
                           reinterpret_cast<const unsigned long long*>(pairs), dCount, cap, tileShift, ranges);
 }
 
 namespace {
+template <bool kChained>
 __global__ void publish_counters_kernel(const uint32_t* __restrict__ counters, uint32_t* hostMapped) {
-    chained_entry();
+    chained_entry<kChained>();
     if (threadIdx.x < 4) hostMapped[threadIdx.x] = counters[threadIdx.x];
     __threadfence_system();
 }
 }  // namespace
 
 cudaError_t launch_publish_counters(const uint32_t* counters, uint32_t* hostMapped, cudaStream_t stream) {
-    return launch_chained(publish_counters_kernel, dim3(1), dim3(32), 0, stream, counters, hostMapped);
+    return launch_chained(publish_counters_kernel<true>, publish_counters_kernel<false>, dim3(1), dim3(32), 0, stream, counters, hostMapped);
 }
 
 namespace {
@@ -544,11 +546,12 @@ __device__ __forceinline__ uint32_t order_block_counts(const uint2* __restrict__
     return b;
 }
 
+template <bool kChained>
 __global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const uint2* __restrict__ ranges,
                                                                          const uint32_t* __restrict__ work,
                                                                          uint32_t tiles,
                                                                          uint32_t* __restrict__ blockCounts) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
     uint32_t rank;
     order_block_counts(ranges, work, tiles, sWarp, rank);
@@ -565,12 +568,13 @@ __global__ void __launch_bounds__(kOrderThreads) tile_order_count_kernel(const u
 // the end. Each block reads every block's counts (from the kernel above):
 // the buckets' totals give their bases, the earlier blocks' counts its own
 // places in each bucket.
+template <bool kChained>
 __global__ void __launch_bounds__(kOrderThreads) tile_order_place_kernel(const uint2* __restrict__ ranges,
                                                                          const uint32_t* __restrict__ work,
                                                                          uint32_t tiles,
                                                                          const uint32_t* __restrict__ blockCounts,
                                                                          uint32_t* __restrict__ order) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ uint32_t sWarp[kOrderThreads / 32][kOrderBuckets];
     __shared__ uint32_t sTotal[kOrderBuckets], sBefore[kOrderBuckets];
     if (threadIdx.x < kOrderBuckets) {
@@ -610,10 +614,10 @@ cudaError_t launch_tile_order(const uint2* ranges, uint32_t tiles, uint32_t* ord
                               cudaStream_t stream, const uint32_t* work) {
     if (tiles == 0) return cudaSuccess;
     const uint32_t blocks = (tiles + kOrderThreads - 1) / kOrderThreads;
-    cudaError_t e = launch_chained(tile_order_count_kernel, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work,
+    cudaError_t e = launch_chained(tile_order_count_kernel<true>, tile_order_count_kernel<false>, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work,
                                    tiles, scratch);
     if (e != cudaSuccess) return e;
-    return launch_chained(tile_order_place_kernel, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work, tiles,
+    return launch_chained(tile_order_place_kernel<true>, tile_order_place_kernel<false>, dim3(blocks), dim3(kOrderThreads), 0, stream, ranges, work, tiles,
                           static_cast<const uint32_t*>(scratch), order);
 }
 
@@ -621,11 +625,12 @@ namespace {
 // A training frame's tile work for the backward blend: the pairs up to the
 // tile's last contributor (the largest of its pixels' saved last indices),
 // a warp a tile.
+template <bool kChained>
 __global__ void __launch_bounds__(256) tile_backward_work_kernel(const uint2* __restrict__ ranges,
                                                                  const uint32_t* __restrict__ pixLast, uint32_t width,
                                                                  uint32_t height, uint32_t tilesX, uint32_t tiles,
                                                                  uint32_t* __restrict__ work) {
-    chained_entry();
+    chained_entry<kChained>();
     const uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31u;
     if (t >= tiles) return;
@@ -647,7 +652,7 @@ cudaError_t launch_tile_backward_order(const uint2* ranges, const uint32_t* pixL
                                        uint32_t tilesX, uint32_t tiles, uint32_t* order, uint32_t* scratch,
                                        uint32_t* work, cudaStream_t stream) {
     if (tiles == 0) return cudaSuccess;
-    cudaError_t e = launch_chained(tile_backward_work_kernel, dim3((tiles + 7) / 8), dim3(256), 0, stream, ranges,
+    cudaError_t e = launch_chained(tile_backward_work_kernel<true>, tile_backward_work_kernel<false>, dim3((tiles + 7) / 8), dim3(256), 0, stream, ranges,
                                    pixLast, width, height, tilesX, tiles, work);
     if (e != cudaSuccess) return e;
     return launch_tile_order(ranges, tiles, order, scratch, stream, work);
@@ -657,7 +662,7 @@ cudaError_t launch_blend(const BlendParams& bp, const uint2* ranges, const uint6
                          float4* colour, float* depth, uint32_t* err, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    return launch_chained(blend_kernel<false>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
+    return launch_chained(blend_kernel<false, true>, blend_kernel<false, false>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
                           reinterpret_cast<const unsigned long long*>(pairs), static_cast<const uint32_t*>(nullptr), proj,
                           colour, depth, static_cast<float4*>(nullptr), static_cast<uint32_t*>(nullptr), err, order);
 }
@@ -700,7 +705,7 @@ cudaError_t launch_blend_train(const BlendParams& bp, const uint2* ranges, const
                                const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    return launch_chained(blend_kernel<true>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
+    return launch_chained(blend_kernel<true, true>, blend_kernel<true, false>, dim3(tiles), dim3(kBlendThreads / kBlendPix), 0, stream, bp, ranges,
                           reinterpret_cast<const unsigned long long*>(pairs), emitSlot, proj, colour, depth, pixState,
                           pixLast, err, order);
 }

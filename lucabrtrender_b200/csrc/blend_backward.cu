@@ -337,6 +337,7 @@ __device__ __forceinline__ void blend_backward_tile(const BlendParams& bp, uint3
     }
 }
 
+template <bool kChained>
 __global__ void __launch_bounds__(kBlendThreads / kBwdPix)
 blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const unsigned long long* __restrict__ pairs,
                       const uint32_t* __restrict__ emit, const uint32_t* __restrict__ emitSlot,
@@ -344,7 +345,7 @@ blend_backward_kernel(BlendParams bp, const uint2* __restrict__ ranges, const un
                       const float4* __restrict__ pixState, const uint32_t* __restrict__ pixLast,
                       const float4* __restrict__ gradColour, float* __restrict__ partials,
                       const uint32_t* __restrict__ order) {
-    chained_entry();
+    chained_entry<kChained>();
     const uint32_t tile = order != nullptr ? order[blockIdx.x] : blockIdx.x;
     blend_backward_tile(bp, tile, tile % bp.tilesX, tile / bp.tilesX, ranges, pairs, emit, emitSlot, proj, pixState,
                         pixLast, gradColour, partials);
@@ -392,7 +393,7 @@ cudaError_t launch_blend_backward(const BlendParams& bp, const uint2* ranges, co
                                   float* partials, cudaStream_t stream, const uint32_t* order) {
     const uint32_t tiles = bp.tilesX * bp.tilesY;
     if (tiles == 0) return cudaSuccess;
-    return launch_chained(blend_backward_kernel, dim3(tiles), dim3(kBlendThreads / kBwdPix), 0, stream, bp, ranges,
+    return launch_chained(blend_backward_kernel<true>, blend_backward_kernel<false>, dim3(tiles), dim3(kBlendThreads / kBwdPix), 0, stream, bp, ranges,
                           reinterpret_cast<const unsigned long long*>(pairs), emit, emitSlot, proj, pixState, pixLast,
                           gradColour, partials, order);
 }

@@ -16,10 +16,11 @@ namespace {
 constexpr uint32_t kLossThreads = 256;
 constexpr uint32_t kLossBlocks = 148 * 4;
 
+template <bool kChained>
 __global__ void __launch_bounds__(kLossThreads)
 l1_partial_kernel(const float4* __restrict__ colour, const float* __restrict__ target, uint32_t pixels,
                   float* __restrict__ partials) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ float sWarp[kLossThreads / 32];
     float s = 0.0f;
     for (uint32_t i = blockIdx.x * kLossThreads + threadIdx.x; i < pixels; i += gridDim.x * kLossThreads) {
@@ -39,9 +40,10 @@ l1_partial_kernel(const float4* __restrict__ colour, const float* __restrict__ t
     }
 }
 
+template <bool kChained>
 __global__ void l1_total_kernel(const float* __restrict__ partials, uint32_t count, float scale,
                                 float* __restrict__ loss) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ float sWarp[32];
     float s = 0.0f;
     for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) s += partials[i];
@@ -56,10 +58,11 @@ __global__ void l1_total_kernel(const float* __restrict__ partials, uint32_t cou
     }
 }
 
+template <bool kChained>
 __global__ void __launch_bounds__(kLossThreads)
 l1_grad_kernel(const float4* __restrict__ colour, const float* __restrict__ target, uint32_t pixels, float scale,
                const float* __restrict__ gradLoss, float4* __restrict__ gradColour) {
-    chained_entry();
+    chained_entry<kChained>();
     const float g = scale * (gradLoss != nullptr ? __ldg(gradLoss) : 1.0f);
     for (uint32_t i = blockIdx.x * kLossThreads + threadIdx.x; i < pixels; i += gridDim.x * kLossThreads) {
         const float4 c = __ldg(colour + i);
@@ -78,10 +81,11 @@ size_t l1_scratch_bytes() { return kLossBlocks * sizeof(float); }
 cudaError_t launch_l1_loss(const float4* colour, const float* target, uint32_t pixels, float* scratch, float* loss,
                            cudaStream_t stream) {
     const float scale = pixels > 0 ? 1.0f / (3.0f * static_cast<float>(pixels)) : 0.0f;
-    cudaError_t e = launch_chained(l1_partial_kernel, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target,
+    const ChainScope chain(pixels >= kChainMinPixels);
+    cudaError_t e = launch_chained(l1_partial_kernel<true>, l1_partial_kernel<false>, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target,
                                    pixels, scratch);
     if (e != cudaSuccess) return e;
-    return launch_chained(l1_total_kernel, dim3(1), dim3(256), 0, stream, static_cast<const float*>(scratch),
+    return launch_chained(l1_total_kernel<true>, l1_total_kernel<false>, dim3(1), dim3(256), 0, stream, static_cast<const float*>(scratch),
                           kLossBlocks, scale, loss);
 }
 
@@ -89,7 +93,8 @@ cudaError_t launch_l1_grad(const float4* colour, const float* target, uint32_t p
                            float4* gradColour, cudaStream_t stream) {
     if (pixels == 0) return cudaSuccess;
     const float scale = 1.0f / (3.0f * static_cast<float>(pixels));
-    return launch_chained(l1_grad_kernel, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target, pixels,
+    const ChainScope chain(pixels >= kChainMinPixels);
+    return launch_chained(l1_grad_kernel<true>, l1_grad_kernel<false>, dim3(kLossBlocks), dim3(kLossThreads), 0, stream, colour, target, pixels,
                           scale, gradLoss, gradColour);
 }
 

@@ -786,7 +786,7 @@ __device__ __forceinline__ void emit_by_warp(bool mine, uint32_t area, const uin
 // depth word (depth key << 32 | slot) the depth sort orders and the two aux
 // words emit_pairs_kernel reads: the tile mask of a masked splat, else 1 when
 // a row of a large splat's hits is not one run.
-template <class Src, bool kEmit = true>
+template <class Src, bool kEmit = true, bool kChained = false>
 __global__ void __launch_bounds__(kProjectThreads, 4)
 project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src src, TrainOutputs train,
                     uint32_t stageWords, uint32_t shVector,
@@ -798,7 +798,7 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
                     unsigned long long* __restrict__ depthWordsOut = nullptr,
                     uint32_t* __restrict__ depthDigits = nullptr, uint2* __restrict__ rowTable = nullptr,
                     uint32_t rowCap = 0) {
-    chained_entry();
+    chained_entry<kChained>();
     extern __shared__ __align__(16) uint32_t shStage[];
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
@@ -1286,12 +1286,13 @@ project_emit_kernel(FrameParams fArg, const FrameParams* __restrict__ fDev, Src 
 // (train.emitSlot), or a sort value beside a slot (train.values).
 constexpr uint32_t kOffsetItems = 16;   // depth positions a thread
 
+template <bool kChained>
 __global__ void __launch_bounds__(kProjectThreads)
 depth_offsets_kernel(const unsigned long long* __restrict__ sortedWords, uint32_t n,
                      const uint32_t* __restrict__ touchedIn, uint32_t* __restrict__ counters,
                      uint64_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t lastPartition,
                      uint32_t* __restrict__ offsets) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ uint32_t sPart;
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ unsigned long long sBase;
@@ -1325,6 +1326,7 @@ depth_offsets_kernel(const unsigned long long* __restrict__ sortedWords, uint32_
 // one's touched count, rectangle, aux word (project_emit_kernel<.., false>)
 // and offset, and, for a splat written row by row or tile by tile, its
 // record.
+template <bool kChained>
 __global__ void __launch_bounds__(kProjectThreads, 4)
 emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* __restrict__ rectsIn,
                   const uint32_t* __restrict__ touchedIn, const unsigned long long* __restrict__ aux,
@@ -1332,7 +1334,7 @@ emit_pairs_kernel(uint32_t n, const ProjRecord* __restrict__ proj, const uint4* 
                   uint32_t* __restrict__ err, unsigned long long* __restrict__ pairs, uint32_t capacity,
                   TrainOutputs train, uint32_t* __restrict__ tileDigits, uint32_t tilePasses,
                   const uint2* __restrict__ rowTable) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ uint32_t sScan[kProjectThreads / 32];
     __shared__ uint32_t sStart[kProjectThreads + 1];
     __shared__ uint32_t sSmallStart[kProjectThreads + 1];
@@ -1472,11 +1474,13 @@ cudaError_t launch_only(const FrameParams& f, const Src& src, bool stage, ProjRe
     const uint32_t stageWords = stage ? f.shWords : 0u;
     const uint32_t shVector = (reinterpret_cast<uintptr_t>(src.sh) & 15u) == 0 ? 1u : 0u;
     const size_t smem = stage ? size_t{kProjectThreads} * f.shWords * 4 : 0;
-    cudaError_t e = cudaFuncSetAttribute(project_emit_kernel<Src, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(std::max<size_t>(smem, 1)));
-    if (e != cudaSuccess) return e;
+    for (auto kernel : {project_emit_kernel<Src, false, true>, project_emit_kernel<Src, false, false>}) {
+        const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(std::max<size_t>(smem, 1)));
+        if (e != cudaSuccess) return e;
+    }
     const uint32_t blocks = project_partitions(f.count);
-    return launch_chained(project_emit_kernel<Src, false>, dim3(blocks), dim3(kProjectThreads), smem, stream, f,
+    return launch_chained(project_emit_kernel<Src, false, true>, project_emit_kernel<Src, false, false>, dim3(blocks), dim3(kProjectThreads), smem, stream, f,
                           static_cast<const FrameParams*>(nullptr), src, TrainOutputs{nullptr, nullptr, nullptr},
                           stageWords, shVector, proj, rects, touched, keys, counters,
                           static_cast<uint64_t*>(nullptr), ticket, 0u, 0u, 0u, static_cast<unsigned long long*>(nullptr),
@@ -1564,11 +1568,11 @@ cudaError_t launch_emit_sorted(const uint64_t* sortedWords, uint32_t n, const Pr
     if (n == 0) return cudaSuccess;
     const uint32_t perBlock = kProjectThreads * kOffsetItems;
     const uint32_t offsetBlocks = (n + perBlock - 1) / perBlock;
-    cudaError_t e = launch_chained(depth_offsets_kernel, dim3(offsetBlocks), dim3(kProjectThreads), 0, stream,
+    cudaError_t e = launch_chained(depth_offsets_kernel<true>, depth_offsets_kernel<false>, dim3(offsetBlocks), dim3(kProjectThreads), 0, stream,
                                    reinterpret_cast<const unsigned long long*>(sortedWords), n, touched, counters,
                                    status, ticket, offsetBlocks - 1, offsets);
     if (e != cudaSuccess) return e;
-    return launch_chained(emit_pairs_kernel, dim3(project_partitions(n)), dim3(kProjectThreads), 0, stream, n, proj,
+    return launch_chained(emit_pairs_kernel<true>, emit_pairs_kernel<false>, dim3(project_partitions(n)), dim3(kProjectThreads), 0, stream, n, proj,
                           rects, touched, reinterpret_cast<const unsigned long long*>(aux),
                           static_cast<const uint32_t*>(offsets), width, height, tilesX, counters + 2,
                           reinterpret_cast<unsigned long long*>(pairs), capacity,

@@ -122,6 +122,7 @@ int render_frame(lrt_rast* r, const lrt_projection* pr, const std::vector<CloudD
     if (s->width == 0 || s->height == 0) return fail(r, LRT_INVALID_ARGUMENT, "a frame needs a size");
     if (s->width > lrt::kMaxFrameSide || s->height > lrt::kMaxFrameSide)
         return fail(r, LRT_UNSUPPORTED, "a frame side above 2^19 pixels");
+    const lrt::ChainScope chain(uint64_t{s->width} * s->height >= lrt::kChainMinPixels);
     if (targets->width != s->width || targets->height != s->height || targets->colour == nullptr ||
         targets->depth == nullptr)
         return fail(r, LRT_INVALID_ARGUMENT, "the targets are not the frame's size");
@@ -967,6 +968,7 @@ int lrt_rast_train_backward(lrt_rast* r, const void* gradColour, lrt_train_grads
     // up to each tile's last contributor.
     const BlendParams& tb = r->trainBlend;
     const uint32_t bTiles = tb.tilesX * tb.tilesY;
+    const lrt::ChainScope chain(uint64_t{tb.width} * tb.height >= lrt::kChainMinPixels);
     uint32_t* bOrder = static_cast<uint32_t*>(r->tileOrder.ptr);
     uint32_t* bScratch = bOrder + bTiles;
     uint32_t* bWork = bScratch + lrt::tile_order_scratch_bytes(bTiles) / 4;

@@ -155,8 +155,9 @@ struct ZeroList {
     ZeroRegion r[kZeroRegions];
     uint32_t count;
 };
+template <bool kChained>
 __global__ void zero_regions_kernel(ZeroList list) {
-    chained_entry();
+    chained_entry<kChained>();
     for (uint32_t k = 0; k < list.count; ++k) zero_words(static_cast<uint32_t*>(list.r[k].p), list.r[k].bytes / 4);
 }
 
@@ -186,7 +187,7 @@ cudaError_t launch_zero_regions(const ZeroRegion* regions, uint32_t count, cudaS
     }
     list.count = count;
     if (largest == 0) return cudaSuccess;
-    return launch_chained(zero_regions_kernel, dim3(zero_blocks(largest)), dim3(256), 0, stream, list);
+    return launch_chained(zero_regions_kernel<true>, zero_regions_kernel<false>, dim3(zero_blocks(largest)), dim3(256), 0, stream, list);
 }
 
 size_t scan_scratch_bytes(uint32_t n) {

@@ -123,13 +123,13 @@ histogram_kernel(const K* __restrict__ keys, const uint32_t* __restrict__ dCount
         if (sHist[i] != 0) atomicAdd(&hist[i], sHist[i]);
 }
 
-template <typename K, bool kValues, typename W, uint32_t kItems>
+template <typename K, bool kValues, typename W, uint32_t kItems, bool kChained>
 __global__ void __launch_bounds__(kSortThreads, kValues ? 3 : 4)
 onesweep_kernel(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, const uint32_t* __restrict__ dCount, uint32_t cap,
                 const uint32_t* __restrict__ hist, W* __restrict__ lookback,
                 uint32_t* __restrict__ ticket, uint32_t* __restrict__ err, uint32_t shift, uint32_t spinLimit) {
-    chained_entry();
+    chained_entry<kChained>();
     extern __shared__ __align__(16) unsigned char smem[];
     K* sKeys = reinterpret_cast<K*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * (kItems * kSortThreads));
@@ -319,15 +319,16 @@ cudaError_t sort_impl(K* keys, K* keysAlt, uint32_t* vals, uint32_t* valsAlt, co
         if (e != cudaSuccess) return e;
     }
     const size_t smem = sizeof(K) * kTile + (kValues ? sizeof(uint32_t) * kTile : 0);
-    e = cudaFuncSetAttribute(onesweep_kernel<K, kValues, W, kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
+    for (auto kernel : {onesweep_kernel<K, kValues, W, kItems, true>, onesweep_kernel<K, kValues, W, kItems, false>}) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
     K* src = keys;
     K* dst = keysAlt;
     uint32_t* vsrc = vals;
     uint32_t* vdst = valsAlt;
     for (uint32_t p = 0; p < passes; ++p) {
-        e = launch_chained(onesweep_kernel<K, kValues, W, kItems>, dim3(parts), dim3(kSortThreads), smem, stream,
+        e = launch_chained(onesweep_kernel<K, kValues, W, kItems, true>, onesweep_kernel<K, kValues, W, kItems, false>, dim3(parts), dim3(kSortThreads), smem, stream,
                            static_cast<const K*>(src), dst, static_cast<const uint32_t*>(vsrc), vdst, dCount, cap,
                            digitCounts + p * kDigits, lookback + static_cast<size_t>(p) * parts * kDigits,
                            tickets + p, err, firstBit + 8 * p, spinLimit);

@@ -369,6 +369,7 @@ __device__ __forceinline__ void splat_partials(uint32_t count, uint32_t firstRaw
 
 // One frame: every splat's gradients written (zero for a splat the frame
 // does not touch).
+template <bool kChained>
 __global__ void __launch_bounds__(kThreads, 5)
 splat_backward_kernel(FrameParams f, const float* __restrict__ means, const float* __restrict__ logScales,
                       const float* __restrict__ quats, const float* __restrict__ logits,
@@ -376,7 +377,7 @@ splat_backward_kernel(FrameParams f, const float* __restrict__ means, const floa
                       const uint32_t* __restrict__ offsets, const float* __restrict__ partials,
                       uint32_t partialPairs, float* __restrict__ gMeans, float* __restrict__ gLogScales,
                       float* __restrict__ gQuats, float* __restrict__ gLogits, float* __restrict__ gSh) {
-    chained_entry();
+    chained_entry<kChained>();
     __shared__ float sGsh[48][kThreads];
     const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
@@ -546,7 +547,7 @@ cudaError_t launch_splat_backward(const FrameParams& f, const float* means, cons
                                   cudaStream_t stream) {
     if (f.count == 0) return cudaSuccess;
     const uint32_t blocks = (f.count + kThreads - 1) / kThreads;
-    return launch_chained(splat_backward_kernel, dim3(blocks), dim3(kThreads), 0, stream, f, means, logScales, quats,
+    return launch_chained(splat_backward_kernel<true>, splat_backward_kernel<false>, dim3(blocks), dim3(kThreads), 0, stream, f, means, logScales, quats,
                           logits, sh, touched, offsets, partials, partialPairs, gMeans, gLogScales, gQuats, gLogits,
                           gSh);
 }
